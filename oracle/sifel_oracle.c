@@ -1,0 +1,622 @@
+/*
+ * sifel_oracle.c -- CPU restatement of SIFEL's linear FE hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle the GPU path is checked
+ * against: tests/, __graft_entry__.smoke() and the cpu_baseline leg of
+ * bench.py may call it; the product library never does.  Every routine
+ * restates one reference routine in plain C, in the same operation order so
+ * that, compiled with the reference's own flags (g++/gcc -O3, no FMA
+ * contraction on x86-64), results agree with the compiled reference to the
+ * last bit or very nearly so.  The restatement is pinned against the
+ * compiled reference (oracle/_ref) by tests/test_oracle_vs_reference.py and
+ * against committed golden fixtures by tests/test_oracle_golden.py.
+ *
+ * Conventions: `long` is int64 as in the reference; code numbers are 1-based,
+ * 0 (or negative) means "no equation" (gtopology.cpp:1619-1680); matrices are
+ * dense row-major.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------ */
+/* Gauss rule of order 2, 15-digit constants (GEFEL/intp.cpp:15-40)          */
+/* ------------------------------------------------------------------------ */
+static const double GP2[2] = {-0.577350269189626, 0.577350269189626};
+static const double GW2[2] = {1.0, 1.0};
+
+/* trilinear hexahedron, GEFEL/basefun.cpp:2299-2370 */
+static void bf_lin_hex_3d(double *n, double x, double y, double z) {
+  n[0] = (1.0 + x) * (1.0 + y) * (1.0 + z) / 8.0;
+  n[1] = (1.0 - x) * (1.0 + y) * (1.0 + z) / 8.0;
+  n[2] = (1.0 - x) * (1.0 - y) * (1.0 + z) / 8.0;
+  n[3] = (1.0 + x) * (1.0 - y) * (1.0 + z) / 8.0;
+  n[4] = (1.0 + x) * (1.0 + y) * (1.0 - z) / 8.0;
+  n[5] = (1.0 - x) * (1.0 + y) * (1.0 - z) / 8.0;
+  n[6] = (1.0 - x) * (1.0 - y) * (1.0 - z) / 8.0;
+  n[7] = (1.0 + x) * (1.0 - y) * (1.0 - z) / 8.0;
+}
+static void dx_bf_lin_hex_3d(double *n, double y, double z) {
+  n[0] = (1.0 + y) * (1.0 + z) / 8.0;
+  n[1] = (1.0 + y) * (1.0 + z) / (-8.0);
+  n[2] = (1.0 - y) * (1.0 + z) / (-8.0);
+  n[3] = (1.0 - y) * (1.0 + z) / 8.0;
+  n[4] = (1.0 + y) * (1.0 - z) / 8.0;
+  n[5] = (1.0 + y) * (1.0 - z) / (-8.0);
+  n[6] = (1.0 - y) * (1.0 - z) / (-8.0);
+  n[7] = (1.0 - y) * (1.0 - z) / 8.0;
+}
+static void dy_bf_lin_hex_3d(double *n, double x, double z) {
+  n[0] = (1.0 + x) * (1.0 + z) / 8.0;
+  n[1] = (1.0 - x) * (1.0 + z) / 8.0;
+  n[2] = (1.0 - x) * (1.0 + z) / (-8.0);
+  n[3] = (1.0 + x) * (1.0 + z) / (-8.0);
+  n[4] = (1.0 + x) * (1.0 - z) / 8.0;
+  n[5] = (1.0 - x) * (1.0 - z) / 8.0;
+  n[6] = (1.0 - x) * (1.0 - z) / (-8.0);
+  n[7] = (1.0 + x) * (1.0 - z) / (-8.0);
+}
+static void dz_bf_lin_hex_3d(double *n, double x, double y) {
+  n[0] = (1.0 + x) * (1.0 + y) / 8.0;
+  n[1] = (1.0 - x) * (1.0 + y) / 8.0;
+  n[2] = (1.0 - x) * (1.0 - y) / 8.0;
+  n[3] = (1.0 + x) * (1.0 - y) / 8.0;
+  n[4] = (1.0 + x) * (1.0 + y) / (-8.0);
+  n[5] = (1.0 - x) * (1.0 + y) / (-8.0);
+  n[6] = (1.0 - x) * (1.0 - y) / (-8.0);
+  n[7] = (1.0 + x) * (1.0 - y) / (-8.0);
+}
+
+/* bilinear quadrilateral, GEFEL/basefun.cpp:609-655 */
+static void bf_lin_4_2d(double *n, double x, double y) {
+  n[0] = 0.25 * (1.0 + x) * (1.0 + y);
+  n[1] = 0.25 * (1.0 - x) * (1.0 + y);
+  n[2] = 0.25 * (1.0 - x) * (1.0 - y);
+  n[3] = 0.25 * (1.0 + x) * (1.0 - y);
+}
+static void dx_bf_lin_4_2d(double *n, double y) {
+  n[0] = 0.25 * (1.0 + y);
+  n[1] = 0.25 * (-1.0 - y);
+  n[2] = 0.25 * (-1.0 + y);
+  n[3] = 0.25 * (1.0 - y);
+}
+static void dy_bf_lin_4_2d(double *n, double x) {
+  n[0] = 0.25 * (1.0 + x);
+  n[1] = 0.25 * (1.0 - x);
+  n[2] = 0.25 * (-1.0 + x);
+  n[3] = 0.25 * (-1.0 - x);
+}
+
+/* derivatives_3d, GEFEL/difcalc.cpp:487-565 (8-node case): natural
+ * derivatives in dx,dy,dz are replaced by Cartesian ones; returns detJ. */
+static double derivatives_3d(double *dx, double *dy, double *dz, const double *x, const double *y,
+                             const double *z, double xi, double eta, double zeta) {
+  double nx[8], ny[8], nz[8];
+  double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0, jac;
+  dx_bf_lin_hex_3d(nx, eta, zeta);
+  dy_bf_lin_hex_3d(ny, xi, zeta);
+  dz_bf_lin_hex_3d(nz, xi, eta);
+  for (int i = 0; i < 8; i++) {
+    d1 += nx[i] * x[i]; d2 += ny[i] * x[i]; d3 += nz[i] * x[i];
+    d4 += nx[i] * y[i]; d5 += ny[i] * y[i]; d6 += nz[i] * y[i];
+    d7 += nx[i] * z[i]; d8 += ny[i] * z[i]; d9 += nz[i] * z[i];
+  }
+  jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+  for (int i = 0; i < 8; i++) {
+    double ddx = dx[i], ddy = dy[i], ddz = dz[i];
+    dx[i] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
+    dy[i] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
+    dz[i] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+  }
+  return jac;
+}
+
+/* derivatives_2d, GEFEL/difcalc.cpp:86-138 (4-node case) */
+static double derivatives_2d(double *dx, double *dy, const double *x, const double *y, double xi,
+                             double eta) {
+  double nx[4], ny[4], d1 = 0, d2 = 0, d3 = 0, d4 = 0, jac;
+  dx_bf_lin_4_2d(nx, eta);
+  dy_bf_lin_4_2d(ny, xi);
+  for (int i = 0; i < 4; i++) {
+    d1 += nx[i] * x[i]; d2 += ny[i] * x[i];
+    d3 += nx[i] * y[i]; d4 += ny[i] * y[i];
+  }
+  jac = d1 * d4 - d2 * d3;
+  for (int i = 0; i < 4; i++) {
+    double ddx = dx[i], ddy = dy[i];
+    dx[i] = (ddx * d4 - ddy * d3) / jac;
+    dy[i] = (ddy * d1 - ddx * d2) / jac;
+  }
+  return jac;
+}
+
+/* bdbjac, GEFEL/matrix.cpp:3126: d += (A^T B) C * jac with mtxm then mxm
+ * (matrix.cpp:1362, 1184), then cmulm and addm (y + d). A, C: m x n; B: m x m */
+static void bdbjac(double *d, const double *a, const double *b, const double *c, double jac,
+                   int m, int n) {
+  double x[24 * 6];
+  double y;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < m; j++) {
+      double s = 0.0;
+      for (int k = 0; k < m; k++) s += a[k * n + i] * b[k * m + j];
+      x[i * m + j] = s;
+    }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      double s = 0.0;
+      for (int k = 0; k < m; k++) s += x[i * m + k] * c[k * n + j];
+      y = s * jac;
+      d[i * n + j] = y + d[i * n + j];
+    }
+}
+
+/* elastisomat::matstiff_spacestr, MEFEL/SRC/elastisomat.cpp:395-420 */
+static void matstiff_spacestr(double e, double nu, double *d) {
+  double g = e / 2.0 / (1.0 + nu);
+  double s = e / (1.0 + nu) / (1.0 - 2.0 * nu);
+  memset(d, 0, 36 * sizeof(double));
+  d[0] = s * (1 - nu); d[1] = s * nu; d[2] = s * nu;
+  d[6] = d[1]; d[7] = d[0]; d[8] = d[1];
+  d[12] = d[1]; d[13] = d[1]; d[14] = d[0];
+  d[21] = g; d[28] = g; d[35] = g;
+}
+
+/* elastisomat::matstiff_plstress, MEFEL/SRC/elastisomat.cpp:255-266 */
+static void matstiff_plstress(double e, double nu, double *d) {
+  double c = e / (1.0 - nu * nu);
+  d[0] = c; d[1] = c * nu; d[2] = 0.0;
+  d[3] = c * nu; d[4] = c; d[5] = 0.0;
+  d[6] = 0.0; d[7] = 0.0; d[8] = e / 2.0 / (1.0 + nu);
+}
+
+/* linhex::gl_stiffness_matrix, MEFEL/SRC/linhex.cpp:583-630, with
+ * linhex::geom_matrix (linhex.cpp:153-186).  xyz: 8 x (x,y,z). */
+void or_hex8_ke(const double *xyz, double e, double nu, double *ke) {
+  double x[8], y[8], z[8], dx[8], dy[8], dz[8], gm[6 * 24], d[36];
+  for (int i = 0; i < 8; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
+  memset(ke, 0, 576 * sizeof(double));
+  for (int i = 0; i < 2; i++) {
+    double xi = GP2[i];
+    for (int j = 0; j < 2; j++) {
+      double eta = GP2[j];
+      for (int k = 0; k < 2; k++) {
+        double zeta = GP2[k];
+        dx_bf_lin_hex_3d(dx, eta, zeta);
+        dy_bf_lin_hex_3d(dy, xi, zeta);
+        dz_bf_lin_hex_3d(dz, xi, eta);
+        double jac = derivatives_3d(dx, dy, dz, x, y, z, xi, eta, zeta);
+        memset(gm, 0, sizeof(gm));
+        for (int a = 0; a < 8; a++) {
+          int jj = 3 * a, kk = 3 * a + 1, ll = 3 * a + 2;
+          gm[0 * 24 + jj] = dx[a];
+          gm[1 * 24 + kk] = dy[a];
+          gm[2 * 24 + ll] = dz[a];
+          gm[3 * 24 + kk] = dz[a]; gm[3 * 24 + ll] = dy[a];
+          gm[4 * 24 + jj] = dz[a]; gm[4 * 24 + ll] = dx[a];
+          gm[5 * 24 + jj] = dy[a]; gm[5 * 24 + kk] = dx[a];
+        }
+        matstiff_spacestr(e, nu, d);
+        jac *= GW2[i] * GW2[j] * GW2[k];
+        if (jac < 0.0) jac = fabs(jac);
+        bdbjac(ke, gm, d, gm, jac, 6, 24);
+      }
+    }
+  }
+}
+
+/* planeelemlq::gl_stiffness_matrix, MEFEL/SRC/plelemlq.cpp:611-690 with
+ * geom_matrix (294-320); thickness interpolated from nodal values t[4]
+ * (planeelemlq::approx, plelemlq.cpp:127). xy: 4 x (x,y). */
+void or_quad4_ke(const double *xy, double e, double nu, const double *t, double *ke) {
+  double x[4], y[4], dx[4], dy[4], gm[3 * 8], d[9], bf[4];
+  for (int i = 0; i < 4; i++) { x[i] = xy[2 * i]; y[i] = xy[2 * i + 1]; }
+  memset(ke, 0, 64 * sizeof(double));
+  for (int i = 0; i < 2; i++) {
+    double xi = GP2[i];
+    for (int j = 0; j < 2; j++) {
+      double eta = GP2[j];
+      dx_bf_lin_4_2d(dx, eta);
+      dy_bf_lin_4_2d(dy, xi);
+      double jac = derivatives_2d(dx, dy, x, y, xi, eta);
+      memset(gm, 0, sizeof(gm));
+      for (int a = 0; a < 4; a++) {
+        gm[0 * 8 + 2 * a] = dx[a];
+        gm[1 * 8 + 2 * a + 1] = dy[a];
+        gm[2 * 8 + 2 * a] = dy[a];
+        gm[2 * 8 + 2 * a + 1] = dx[a];
+      }
+      matstiff_plstress(e, nu, d);
+      bf_lin_4_2d(bf, xi, eta);
+      double thick = 0.0;
+      for (int a = 0; a < 4; a++) thick += bf[a] * t[a];
+      jac *= thick * GW2[i] * GW2[j];
+      if (jac < 0.0) jac = fabs(jac);
+      bdbjac(ke, gm, d, gm, jac, 3, 8);
+    }
+  }
+}
+
+/* bdbj, GEFEL/matrix.cpp:3066-3110: symmetric fill of B^T D B jac */
+static void bdbj(double *k, const double *b, const double *d, double jac, int m, int n) {
+  double am[3 * 8];
+  int ll = 0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < m; j++) {
+      double s = 0.0;
+      int ii = i, jj = j;
+      for (int l = 0; l < m; l++) { s += b[ii] * d[jj]; ii += n; jj += m; }
+      am[ll++] = s;
+    }
+  for (int i = 0; i < n; i++) {
+    int ii = i * n + i, mm = ii, l0 = i * m, ul = l0 + m, jj = i;
+    double s = 0.0;
+    for (int l = l0; l < ul; l++) { s += am[l] * b[jj]; jj += n; }
+    k[ii] += s * jac;
+    ii++; mm += n;
+    for (int j = i + 1; j < n; j++) {
+      s = 0.0; jj = j;
+      for (int l = l0; l < ul; l++) { s += am[l] * b[jj]; jj += n; }
+      k[ii] += s * jac; k[mm] += s * jac;
+      ii++; mm += n;
+    }
+  }
+}
+
+/* nnj, GEFEL/matrix.cpp:3149-3174 (single row N) */
+static void nnj(double *m, const double *n, double jac, int nn) {
+  for (int i = 0; i < nn; i++) {
+    int kk = i * nn + i, ll = kk;
+    double s = 0.0 + n[i] * n[i];
+    m[kk] += s * jac;
+    kk++; ll += nn;
+    for (int j = i + 1; j < nn; j++) {
+      s = 0.0 + n[i] * n[j];
+      m[kk] += s * jac; m[ll] += s * jac;
+      kk++; ll += nn;
+    }
+  }
+}
+
+/* linhext::conductivity_matrix (TRFEL/SRC/linhext.cpp:774-840) for an
+ * isotropic material D = k I3 (isotrmat::matcond3d, isotrmat.cpp:124) and
+ * linhext::capacity_matrix (linhext.cpp:979-1030) with capacity c and
+ * density rho (nodal values, interpolated by linhext::approx). */
+void or_hex8t_kc(const double *xyz, double kcond, double c, const double *rho, double *ke,
+                 double *ce) {
+  double x[8], y[8], z[8], dx[8], dy[8], dz[8], gm[3 * 8], d[9], nb[8];
+  for (int i = 0; i < 8; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
+  if (ke) {
+    memset(ke, 0, 64 * sizeof(double));
+    for (int i = 0; i < 2; i++)
+      for (int j = 0; j < 2; j++)
+        for (int k = 0; k < 2; k++) {
+          double xi = GP2[i], eta = GP2[j], zeta = GP2[k];
+          dx_bf_lin_hex_3d(dx, eta, zeta);
+          dy_bf_lin_hex_3d(dy, xi, zeta);
+          dz_bf_lin_hex_3d(dz, xi, eta);
+          double jac = derivatives_3d(dx, dy, dz, x, y, z, xi, eta, zeta);
+          for (int a = 0; a < 8; a++) { gm[a] = dx[a]; gm[8 + a] = dy[a]; gm[16 + a] = dz[a]; }
+          memset(d, 0, sizeof(d));
+          d[0] = kcond; d[4] = kcond; d[8] = kcond;
+          if (jac < 0.0) jac = fabs(jac);
+          jac *= GW2[i] * GW2[j] * GW2[k];
+          bdbj(ke, gm, d, jac, 3, 8);
+        }
+  }
+  if (ce) {
+    memset(ce, 0, 64 * sizeof(double));
+    for (int i = 0; i < 2; i++)
+      for (int j = 0; j < 2; j++)
+        for (int k = 0; k < 2; k++) {
+          double xi = GP2[i], eta = GP2[j], zeta = GP2[k];
+          /* jac_3d (GEFEL/difcalc.cpp:650): same Jacobian as derivatives_3d */
+          double nx[8], ny[8], nz[8];
+          double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0;
+          dx_bf_lin_hex_3d(nx, eta, zeta);
+          dy_bf_lin_hex_3d(ny, xi, zeta);
+          dz_bf_lin_hex_3d(nz, xi, eta);
+          for (int a = 0; a < 8; a++) {
+            d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nz[a] * x[a];
+            d4 += nx[a] * y[a]; d5 += ny[a] * y[a]; d6 += nz[a] * y[a];
+            d7 += nx[a] * z[a]; d8 += ny[a] * z[a]; d9 += nz[a] * z[a];
+          }
+          double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 -
+                       d9 * d4 * d2;
+          bf_lin_hex_3d(nb, xi, eta, zeta);
+          double r = 0.0;
+          for (int a = 0; a < 8; a++) r += nb[a] * rho[a];
+          if (jac < 0.0) jac = fabs(jac);
+          jac *= GW2[i] * GW2[j] * GW2[k] * r * c;
+          nnj(ce, nb, jac, 8);
+        }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Storage patterns (CR and SCR) and localisation                           */
+/* ------------------------------------------------------------------------ */
+
+/* comparison for qsort of long */
+static int cmp_long(const void *a, const void *b) {
+  long x = *(const long *)a, y = *(const long *)b;
+  return (x > y) - (x < y);
+}
+
+/* Row-wise column sets of the global matrix from element code numbers:
+ * symcomprow::initiate (GEFEL/scr.cpp:556; numcontr, addresses, fillarray,
+ * sort_and_colindex_tko at 112-420) when sym != 0 (columns <= row, sorted, so
+ * the diagonal is last), comprow::initiate (cr.cpp:454; sort_and_colindex at
+ * 247) otherwise.  cn: ne x ndofe, 1-based, <= 0 skipped.
+ * Two-phase: call with ci == NULL to get negm (adr filled), then again with
+ * ci of that size. */
+long or_pattern(long n, long ne, long ndofe, const long *cn, int sym, long *adr, long *ci) {
+  long *cnt = (long *)calloc((size_t)n + 1, sizeof(long));
+  for (long e = 0; e < ne; e++) {
+    const long *c = cn + e * ndofe;
+    for (long i = 0; i < ndofe; i++) {
+      long ii = c[i] - 1;
+      if (ii < 0) continue;
+      for (long j = 0; j < ndofe; j++) {
+        long jj = c[j] - 1;
+        if (jj < 0) continue;
+        if (sym && jj > ii) continue;
+        cnt[ii]++;
+      }
+    }
+  }
+  long *start = (long *)malloc(((size_t)n + 1) * sizeof(long));
+  start[0] = 0;
+  for (long i = 0; i < n; i++) start[i + 1] = start[i] + cnt[i];
+  long *aux = (long *)malloc((size_t)start[n] * sizeof(long) + 8);
+  memset(cnt, 0, ((size_t)n + 1) * sizeof(long));
+  for (long e = 0; e < ne; e++) {
+    const long *c = cn + e * ndofe;
+    for (long i = 0; i < ndofe; i++) {
+      long ii = c[i] - 1;
+      if (ii < 0) continue;
+      for (long j = 0; j < ndofe; j++) {
+        long jj = c[j] - 1;
+        if (jj < 0) continue;
+        if (sym && jj > ii) continue;
+        aux[start[ii] + cnt[ii]++] = jj;
+      }
+    }
+  }
+  long negm = 0;
+  for (long i = 0; i < n; i++) {
+    long *row = aux + start[i];
+    long m = cnt[i];
+    qsort(row, (size_t)m, sizeof(long), cmp_long);
+    long u = 0;
+    for (long k = 0; k < m; k++)
+      if (u == 0 || row[k] != row[u - 1]) row[u++] = row[k];
+    cnt[i] = u;
+    negm += u;
+  }
+  adr[0] = 0;
+  for (long i = 0; i < n; i++) adr[i + 1] = adr[i] + cnt[i];
+  if (ci)
+    for (long i = 0; i < n; i++) memcpy(ci + adr[i], aux + start[i], (size_t)cnt[i] * sizeof(long));
+  free(aux);
+  free(start);
+  free(cnt);
+  return negm;
+}
+
+/* symcomprow::localize, GEFEL/scr.cpp:422-470 (searches restated as a direct
+ * search from the row start; the entry hit is the same unique position). */
+void or_scr_localize(long *adr, long *ci, double *a, const double *b, const long *cn, long m) {
+  for (long i = 0; i < m; i++) {
+    long ii = cn[i] - 1;
+    if (ii < 0) continue;
+    for (long j = 0; j < m; j++) {
+      long jj = cn[j] - 1;
+      if (jj < 0 || ii < jj) continue;
+      for (long k = adr[ii]; k < adr[ii + 1]; k++)
+        if (ci[k] == jj) { a[k] += b[i * m + j]; break; }
+    }
+  }
+}
+
+/* comprow::localize, GEFEL/cr.cpp:327-372 */
+void or_cr_localize(long *adr, long *ci, double *a, const double *b, const long *cn, long m) {
+  for (long i = 0; i < m; i++) {
+    long ii = cn[i] - 1;
+    if (ii < 0) continue;
+    for (long j = 0; j < m; j++) {
+      long jj = cn[j] - 1;
+      if (jj < 0) continue;
+      for (long k = adr[ii]; k < adr[ii + 1]; k++)
+        if (ci[k] == jj) { a[k] += b[i * m + j]; break; }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Whole-mesh assembly: stiffness_matrix (MEFEL/SRC/globmat.cpp:41-143) and  */
+/* conductivity_matrix / capacity_matrix (TRFEL/SRC/globmatt.cpp:19/92)     */
+/* ------------------------------------------------------------------------ */
+
+/* kind 0 = hex8 elasticity, 1 = quad4 plane stress, 2 = hex8 conduction,
+ * 3 = hex8 capacity.  coords: nn x 3; elems: ne x nne; cn: ne x ndofe;
+ * mats: per element material row (E,nu) or (k,c); thick: per element (quad4)
+ * or NULL; rho: per element density (capacity) or NULL (then 1). */
+void or_assemble(int kind, int sym, long ne, const double *coords, const long *elems,
+                 const long *cn, const double *emat, const double *thick, const double *rho,
+                 long *adr, long *ci, double *a) {
+  long nne = (kind == 1) ? 4 : 8;
+  long ndofe = (kind == 0) ? 24 : (kind == 1 ? 8 : 8);
+  double xyz[24], xy[8], t[4], r[8], ke[576];
+  for (long e = 0; e < ne; e++) {
+    const long *nd = elems + e * nne;
+    if (kind == 1) {
+      for (int i = 0; i < 4; i++) { xy[2 * i] = coords[3 * nd[i]]; xy[2 * i + 1] = coords[3 * nd[i] + 1]; t[i] = thick[e]; }
+      or_quad4_ke(xy, emat[2 * e], emat[2 * e + 1], t, ke);
+    } else {
+      for (int i = 0; i < 8; i++)
+        for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
+      if (kind == 0) {
+        or_hex8_ke(xyz, emat[2 * e], emat[2 * e + 1], ke);
+      } else {
+        for (int i = 0; i < 8; i++) r[i] = rho ? rho[e] : 1.0;
+        if (kind == 2) or_hex8t_kc(xyz, emat[2 * e], emat[2 * e + 1], r, ke, NULL);
+        else or_hex8t_kc(xyz, emat[2 * e], emat[2 * e + 1], r, NULL, ke);
+      }
+    }
+    if (sym) or_scr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
+    else or_cr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Matrix-vector products                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* symcomprow::mxv_scr, GEFEL/scr.cpp:655-672 */
+void or_scr_mxv(long n, const long *adr, const long *ci, const double *a, const double *b,
+                double *c) {
+  for (long i = 0; i < n; i++) {
+    long lj = adr[i], uj = adr[i + 1];
+    double s = 0.0, d = b[i];
+    for (long j = lj; j < uj; j++) {
+      long ii = ci[j];
+      s += a[j] * b[ii];
+      c[ii] += a[j] * d;
+    }
+    c[i] = s;
+  }
+}
+
+/* comprow::mxv_cr, GEFEL/cr.cpp:653-700 (serial branch) */
+void or_cr_mxv(long n, const long *adr, const long *ci, const double *a, const double *b,
+               double *c) {
+  for (long i = 0; i < n; i++) {
+    double s = 0.0;
+    for (long j = adr[i]; j < adr[i + 1]; j++) s += a[j] * b[ci[j]];
+    c[i] = s;
+  }
+}
+
+/* ss, GEFEL/vector.cpp:2052: plain serial dot product */
+static double ss(const double *a, const double *b, long n) {
+  double s = 0.0;
+  for (long i = 0; i < n; i++) s += a[i] * b[i];
+  return s;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Conjugate gradients                                                      */
+/* Status: 0 converged, 1 iteration limit, 2 breakdown |d.p| < zero,        */
+/*         5 zero right-hand side                                           */
+/* ------------------------------------------------------------------------ */
+
+/* symcomprow::cg_prec with tprec = 1 (Jacobi), GEFEL/scr.cpp:1093-1205.
+ * Stops when (r.r)/(f.f) < res; on convergence ani = i, ares = (r.h)/(f.f);
+ * otherwise ani/ares are left untouched (as in the reference). */
+int or_scr_cg_prec(long n, const long *adr, const long *ci, const double *a, double *x,
+                   const double *y, long ni, double res, double zero, long iv, long *ani,
+                   double *ares) {
+  double *d = (double *)malloc(n * sizeof(double)), *r = (double *)malloc(n * sizeof(double));
+  double *p = (double *)malloc(n * sizeof(double)), *h = (double *)malloc(n * sizeof(double));
+  int status = 1;
+  if (iv == 0)
+    for (long i = 0; i < n; i++) x[i] = 0.0;
+  or_scr_mxv(n, adr, ci, a, x, p);
+  double nory = 0.0;
+  for (long i = 0; i < n; i++) { nory += y[i] * y[i]; r[i] = y[i] - p[i]; }
+  if (nory < zero) { *ares = nory; *ani = 0; status = 5; }
+  for (long i = 0; i < n; i++) h[i] = r[i] / a[adr[i + 1] - 1];
+  double nom = ss(r, h, n);
+  for (long i = 0; i < n; i++) d[i] = h[i];
+  for (long it = 0; it < ni; it++) {
+    or_scr_mxv(n, adr, ci, a, d, p);
+    double denom = ss(d, p, n);
+    if (fabs(denom) < zero) { *ares = nom; *ani = it; status = 2; break; }
+    double alpha = nom / denom, rr = 0.0;
+    for (long j = 0; j < n; j++) {
+      x[j] += alpha * d[j];
+      r[j] -= alpha * p[j];
+      rr += r[j] * r[j];
+    }
+    for (long j = 0; j < n; j++) h[j] = r[j] / a[adr[j + 1] - 1];
+    denom = nom;
+    nom = ss(r, h, n);
+    double beta = nom / denom;
+    if (fabs(rr / nory) < res) { *ani = it; *ares = nom / nory; status = 0; break; }
+    for (long j = 0; j < n; j++) d[j] = beta * d[j] + h[j];
+  }
+  free(h); free(p); free(r); free(d);
+  return status;
+}
+
+/* comprow::cg_prec with a noprecond preconditioner (h = r, precond.cpp:166),
+ * GEFEL/cr.cpp:1124-1240.  Stops when sqrt((r.h)/(f.f)) < res; then
+ * ani = i, ares = r.h (the final assignment at cr.cpp:1236 overrides the
+ * in-loop one); on exhaustion ani = ni, ares = r.h. */
+int or_cr_cg_prec(long n, const long *adr, const long *ci, const double *a, double *x,
+                  const double *y, long ni, double res, double zero, long iv, long *ani,
+                  double *ares) {
+  double *d = (double *)malloc(n * sizeof(double)), *r = (double *)malloc(n * sizeof(double));
+  double *p = (double *)malloc(n * sizeof(double)), *h = (double *)malloc(n * sizeof(double));
+  int status = 1;
+  long it;
+  if (iv == 0)
+    for (long i = 0; i < n; i++) x[i] = 0.0;
+  or_cr_mxv(n, adr, ci, a, x, p);
+  double nory = 0.0;
+  for (long i = 0; i < n; i++) { nory += y[i] * y[i]; r[i] = y[i] - p[i]; }
+  if (nory < zero) {
+    *ares = nory; *ani = 0;
+    free(h); free(p); free(r); free(d);
+    return 5;
+  }
+  for (long i = 0; i < n; i++) h[i] = r[i];
+  double nom = ss(r, h, n);
+  for (long i = 0; i < n; i++) d[i] = h[i];
+  for (it = 0; it < ni; it++) {
+    or_cr_mxv(n, adr, ci, a, d, p);
+    double denom = ss(d, p, n);
+    if (fabs(denom) < zero) { status = 2; break; }
+    double alpha = nom / denom;
+    for (long j = 0; j < n; j++) { x[j] += alpha * d[j]; r[j] -= alpha * p[j]; }
+    for (long j = 0; j < n; j++) h[j] = r[j];
+    denom = nom;
+    nom = ss(r, h, n);
+    double beta = nom / denom;
+    if (sqrt(nom / nory) < res) { status = 0; break; }
+    for (long j = 0; j < n; j++) d[j] = beta * d[j] + h[j];
+  }
+  *ani = it;
+  *ares = nom;
+  free(h); free(p); free(r); free(d);
+  return status;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Transient d-form trapezoid, one step (TRFEL/SRC/npsolvert.cpp:1146-1230)  */
+/* ------------------------------------------------------------------------ */
+
+/* Given K and C in the same SCR pattern, the step's nodal flux vector rhs,
+ * and (d, v) at t_n: builds A = alpha dt K + C (scalgm/addgm, index-aligned,
+ * scr.cpp:760/682), p = C (d + (1-alpha) dt v) (mxv_scr), f = alpha dt rhs + p,
+ * solves A d' = f by symcomprow::cg_prec (x starts from d when iv = 1, as the
+ * reference passes lhs), sets v' = (d' - dd)/dt/alpha.  A is written into
+ * `work_a` (length negm). */
+int or_trfel_step(long n, const long *adr, const long *ci, const double *ka, const double *ca,
+                  double *work_a, const double *rhs, double *d, double *v, double dt,
+                  double alpha, long ni, double res, double zero, long iv, long *ani,
+                  double *ares) {
+  long negm = adr[n];
+  double *dd = (double *)malloc(n * sizeof(double)), *p = (double *)malloc(n * sizeof(double));
+  double *f = (double *)malloc(n * sizeof(double));
+  for (long j = 0; j < n; j++) dd[j] = d[j] + (1.0 - alpha) * dt * v[j];
+  or_scr_mxv(n, adr, ci, ca, dd, p);
+  for (long k = 0; k < negm; k++) work_a[k] = ka[k] * (dt * alpha);
+  for (long k = 0; k < negm; k++) work_a[k] += 1.0 * ca[k];
+  for (long j = 0; j < n; j++) f[j] = rhs[j] * alpha * dt + p[j];
+  int st = or_scr_cg_prec(n, adr, ci, work_a, d, f, ni, res, zero, iv, ani, ares);
+  for (long j = 0; j < n; j++) v[j] = (d[j] - dd[j]) / dt / alpha;
+  free(f); free(p); free(dd);
+  return st;
+}

@@ -1,0 +1,300 @@
+"""Synthetic SIFEL problems: structured meshes, loads and positional decks.
+
+The benchmark problems of this project are generated, never downloaded:
+
+* ``cantilever_hex``   -- 3D linear-elastic cantilever of 8-node hexahedra,
+  clamped at x = 0, uniform traction on the x = L face as consistent nodal
+  forces (each face quad gives a quarter of its force to each corner);
+* ``cantilever_top_loads`` -- independent N(0,1) x 1 kN z-forces on every
+  free node of the top face, one column per load case;
+* ``plate_quad``       -- 2D plane-stress plate of 4-node quads, left edge
+  clamped, unit traction x thickness on the right edge;
+* ``heat_cube``        -- unit cube of linear hexahedra for transient
+  conduction with one conductivity per element.
+
+``write_mefel_deck`` writes a deck in SIFEL's positional (``-kwd`` absent)
+MEFEL input format, token order as read by ``probdesc::read``
+(MEFEL/SRC/probdesc.cpp:204-452), ``mechtop::read`` (mechtop.cpp:124-262),
+``element::read`` (element.cpp:90-350), ``mechmat::read`` (mechmat.cpp:1042),
+``mechcrsec::read`` (mechcrsec.cpp:74), ``mechbclc::read`` / ``loadcase::read``
+(mechbclc.cpp:99, loadcase.cpp:114) and ``outdriverm::read``
+(outdriverm.cpp:96).  ``write_trfel_deck`` does the same for TRFEL.
+
+Node order of a hexahedron follows SIFEL (GEFEL/basefun.cpp:2299):
+n0 (+,+,+), n1 (-,+,+), n2 (-,-,+), n3 (+,-,+), n4..n7 likewise at zeta = -1.
+Quadrilaterals: n0 (+,+), n1 (-,+), n2 (-,-), n3 (+,-) (basefun.cpp:609).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Mesh:
+    """A mesh with nodal DOF flags, per-element materials and nodal loads.
+
+    coords   (nn, 3) float64 node coordinates (z = 0 for 2D meshes)
+    elems    (ne, nne) int64 0-based node ids in SIFEL element node order
+    dofflag  (nn, ndofn) int64 constraint codes as in the deck: 1 free, 0 fixed
+    emat     (ne,) int64 0-based material instance per element
+    mats     (nmat, k) float64 material parameters ((E, nu) or (k, c))
+    thick    (ne,) float64 element thickness (plane stress) or None
+    loads    (nlc, nn, ndofn) float64 nodal forces per load case
+    """
+
+    kind: str
+    coords: np.ndarray
+    elems: np.ndarray
+    dofflag: np.ndarray
+    emat: np.ndarray
+    mats: np.ndarray
+    loads: np.ndarray
+    thick: np.ndarray | None = None
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def nn(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def ne(self) -> int:
+        return int(self.elems.shape[0])
+
+    @property
+    def ndofn(self) -> int:
+        return int(self.dofflag.shape[1])
+
+    def code_numbers(self) -> np.ndarray:
+        """DOF numbering of ``gtopology::gencodnum`` (GEFEL/gtopology.cpp:1619).
+
+        Nodes in order, DOFs of a node in order; every free DOF (flag 1) gets
+        the next 1-based number, fixed DOFs get 0.
+        """
+        flat = self.dofflag.reshape(-1)
+        cn = np.zeros_like(flat)
+        free = flat == 1
+        cn[free] = np.arange(1, int(free.sum()) + 1)
+        return cn.reshape(self.dofflag.shape)
+
+    @property
+    def ndof(self) -> int:
+        return int((self.dofflag == 1).sum())
+
+
+def _hex_grid(nx, ny, nz, lx, ly, lz):
+    xs = np.linspace(0.0, lx, nx + 1)
+    ys = np.linspace(0.0, ly, ny + 1)
+    zs = np.linspace(0.0, lz, nz + 1)
+    # node id = i + (nx+1)*(j + (ny+1)*k): x fastest
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+    def nid(i, j, k):
+        return i + (nx + 1) * (j + (ny + 1) * k)
+
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    elems = np.stack(
+        [
+            nid(i + 1, j + 1, k + 1),
+            nid(i, j + 1, k + 1),
+            nid(i, j, k + 1),
+            nid(i + 1, j, k + 1),
+            nid(i + 1, j + 1, k),
+            nid(i, j + 1, k),
+            nid(i, j, k),
+            nid(i + 1, j, k),
+        ],
+        axis=1,
+    ).astype(np.int64)
+    return coords, elems, nid
+
+
+def cantilever_hex(nx=20, ny=4, nz=4, L=1.0, B=0.2, H=0.2, E=210e9, nu=0.3,
+                   traction=1.0e6) -> Mesh:
+    """Clamped cantilever of linear hexahedra with an end traction in -z."""
+    coords, elems, nid = _hex_grid(nx, ny, nz, L, B, H)
+    nn = coords.shape[0]
+    dofflag = np.ones((nn, 3), dtype=np.int64)
+    dofflag[np.isclose(coords[:, 0], 0.0)] = 0
+    loads = np.zeros((1, nn, 3))
+    # consistent nodal forces of a uniform traction on bilinear face quads
+    fq = traction * (B / ny) * (H / nz) / 4.0
+    for k in range(nz):
+        for j in range(ny):
+            for (jj, kk) in ((j, k), (j + 1, k), (j + 1, k + 1), (j, k + 1)):
+                loads[0, nid(nx, jj, kk), 2] -= fq
+    return Mesh(
+        kind="hex8",
+        coords=coords,
+        elems=elems,
+        dofflag=dofflag,
+        emat=np.zeros(elems.shape[0], dtype=np.int64),
+        mats=np.array([[E, nu]]),
+        loads=loads,
+        meta=dict(nx=nx, ny=ny, nz=nz, L=L, B=B, H=H),
+    )
+
+
+def cantilever_top_loads(mesh: Mesh, nlc: int, seed: int = 1234, scale: float = 1.0e3) -> Mesh:
+    """Replace the loads by ``nlc`` cases of N(0,1)*scale z-forces on the
+    free nodes of the top face (z = H)."""
+    H = mesh.meta["H"]
+    rng = np.random.default_rng(seed)
+    top = np.where(np.isclose(mesh.coords[:, 2], H) & (mesh.dofflag[:, 2] == 1))[0]
+    loads = np.zeros((nlc, mesh.nn, 3))
+    loads[:, top, 2] = rng.standard_normal((nlc, top.size)) * scale
+    out = Mesh(**{**mesh.__dict__})
+    out.loads = loads
+    return out
+
+
+def plate_quad(nx, ny, Lx=None, Ly=None, E=1.0e10, nu=0.25, t=0.01, traction=1.0) -> Mesh:
+    """Plane-stress plate of bilinear quads; left edge clamped, uniform
+    traction (per unit area) x thickness on the right edge, in +x."""
+    Lx = float(nx) if Lx is None else Lx
+    Ly = float(ny) if Ly is None else Ly
+    xs = np.linspace(0.0, Lx, nx + 1)
+    ys = np.linspace(0.0, Ly, ny + 1)
+    Y, X = np.meshgrid(ys, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel(), np.zeros(X.size)], axis=1)
+
+    def nid(i, j):
+        return i + (nx + 1) * j
+
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    i, j = i.ravel(), j.ravel()
+    elems = np.stack([nid(i + 1, j + 1), nid(i, j + 1), nid(i, j), nid(i + 1, j)], axis=1)
+    nn = coords.shape[0]
+    dofflag = np.ones((nn, 2), dtype=np.int64)
+    dofflag[np.isclose(coords[:, 0], 0.0)] = 0
+    loads = np.zeros((1, nn, 2))
+    fe = traction * t * (Ly / ny) / 2.0
+    for jj in range(ny):
+        loads[0, nid(nx, jj), 0] += fe
+        loads[0, nid(nx, jj + 1), 0] += fe
+    return Mesh(
+        kind="quad4",
+        coords=coords,
+        elems=elems.astype(np.int64),
+        dofflag=dofflag,
+        emat=np.zeros(elems.shape[0], dtype=np.int64),
+        mats=np.array([[E, nu]]),
+        loads=loads,
+        thick=np.full(elems.shape[0], t),
+        meta=dict(nx=nx, ny=ny, Lx=Lx, Ly=Ly),
+    )
+
+
+def plate_batch(count=512, seed=0, lo=16, hi=128):
+    """The uneven batch: ``count`` plates with side counts uniform in
+    [lo, hi], E uniform in [1e9, 1e11], nu uniform in [0.2, 0.35]."""
+    rng = np.random.default_rng(seed)
+    nx = rng.integers(lo, hi + 1, size=count)
+    ny = rng.integers(lo, hi + 1, size=count)
+    E = rng.uniform(1.0e9, 1.0e11, size=count)
+    nu = rng.uniform(0.2, 0.35, size=count)
+    return [plate_quad(int(a), int(b), E=float(e), nu=float(v)) for a, b, e, v in zip(nx, ny, E, nu)]
+
+
+def heat_cube(n=8, L=1.0, sigma=1.0, mu=0.0, seed=1234, rhoc=2.0e6, T_left=1.0) -> Mesh:
+    """Unit cube of n^3 linear hexahedra; per-element conductivity
+    exp(N(mu, sigma)) from ``seed`` in element order (x fastest); T fixed
+    to ``T_left`` on the x = 0 face (prescribed-value DOFs)."""
+    coords, elems, _ = _hex_grid(n, n, n, L, L, L)
+    rng = np.random.default_rng(seed)
+    k = np.exp(rng.normal(mu, sigma, size=elems.shape[0]))
+    nn = coords.shape[0]
+    dofflag = np.ones((nn, 1), dtype=np.int64)
+    left = np.isclose(coords[:, 0], 0.0)
+    dofflag[left] = 0
+    presc = np.zeros((nn, 1))
+    presc[left, 0] = T_left
+    return Mesh(
+        kind="hex8t",
+        coords=coords,
+        elems=elems,
+        dofflag=dofflag,
+        emat=np.arange(elems.shape[0], dtype=np.int64),
+        mats=np.stack([k, np.full_like(k, rhoc)], axis=1),
+        loads=np.zeros((1, nn, 1)),
+        meta=dict(n=n, L=L, prescribed=presc),
+    )
+
+
+# ----------------------------------------------------------------------------
+# deck writers
+# ----------------------------------------------------------------------------
+
+def _fmt(v: float) -> str:
+    return repr(float(v))
+
+
+def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
+                     res: float = 1.0e-20, iv: int = 0, precond: int = 1,
+                     title: str = "sifel-b200 synthetic deck") -> None:
+    """Write a linear-statics MEFEL deck (positional format).
+
+    storage 11 = symm_comp_rows, 10 = compressed_rows; solver cg (20);
+    precond 1 = diagprec, 0 = noprecond.  For SCR + diagprec the reference
+    stops on (r.r)/(f.f) < res, so res = 1e-20 means relative residual 1e-10.
+    """
+    nd = mesh.ndofn
+    lines: list[str] = [title]
+    # mespr problemtype straincomp stresscomp othercomp reactcomp
+    # adaptivity stochasticcalc homogenization noderenumber
+    lines.append("0\n1\n0 0 0 0\n0 0 0\n0")
+    lines.append(f"{storage}")
+    lines.append(f"20 {ni} {_fmt(res)} {iv}")
+    lines.append(f"{precond}")
+    lines.append(f"{mesh.nn}")
+    is2d = mesh.kind == "quad4"
+    for i, (x, y, z) in enumerate(mesh.coords):
+        lines.append(f"{i + 1} {_fmt(x)} {_fmt(y)} {_fmt(z)} {nd} 0 0")
+    con = np.where((mesh.dofflag != 1).any(axis=1))[0]
+    lines.append(f"{con.size}")
+    for i in con:
+        lines.append(f"{i + 1} " + " ".join(str(int(c)) for c in mesh.dofflag[i]))
+    lines.append(f"{mesh.ne}")
+    for e, nodes in enumerate(mesh.elems):
+        ns = " ".join(str(int(v) + 1) for v in nodes)
+        m = int(mesh.emat[e]) + 1
+        if is2d:
+            # type planeelementlq (23), strastrestate planestress (10),
+            # cne 0, crst csplanestr (10) instance e+1... one thickness set
+            lines.append(f"{e + 1} 23 10 {ns} 0 10 {int(mesh.meta.get('tset', [0] * mesh.ne)[e]) + 1 if 'tset' in mesh.meta else 1} 1 1 {m}")
+        else:
+            # type linearhex (102), cne 0, crst 0, one material elisomat (1)
+            lines.append(f"{e + 1} 102 {ns} 0 0 1 1 {m}")
+    # materials: one type (elisomat = 1), mats.shape[0] instances "id e nu"
+    lines.append("1")
+    lines.append(f"1 {mesh.mats.shape[0]}")
+    for k, (E, nu) in enumerate(mesh.mats):
+        lines.append(f"{k + 1} {_fmt(E)} {_fmt(nu)}")
+    # cross sections
+    if is2d:
+        tvals = mesh.meta.get("tvals", [float(mesh.thick[0])])
+        lines.append("1")
+        lines.append(f"10 {len(tvals)}")
+        for k, t in enumerate(tvals):
+            lines.append(f"{k + 1} {_fmt(t)}")
+    else:
+        lines.append("0")
+    # load cases
+    nlc = mesh.loads.shape[0]
+    lines.append(f"{nlc}")
+    for lc in range(nlc):
+        ld = np.where(np.abs(mesh.loads[lc]).sum(axis=1) != 0.0)[0]
+        lines.append(f"{ld.size}")
+        for i in ld:
+            lines.append(f"{i + 1} " + " ".join(_fmt(v) for v in mesh.loads[lc, i]))
+        lines.append("0")  # loaded elements
+        lines.append("0")  # prescribed displacements
+        lines.append("0")  # temperature changes
+    lines.append("0")  # eigenstrains
+    lines.append("0")  # textout
+    lines.append("0")  # outgr_format
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
