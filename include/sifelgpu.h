@@ -1,0 +1,214 @@
+/*
+ * sifelgpu.h -- C ABI of libsifelgpu.so, the B200 (sm_100a) implementation of
+ * SIFEL's linear finite-element hot path: element integration, assembly into
+ * GEFEL compressed-row storage and the Jacobi-preconditioned CG solve.
+ *
+ * Conventions shared by every entry point:
+ *  - plain C types only; `int64_t` stands for the reference's `long`;
+ *  - matrix storages are GEFEL's: CR (`comprow`, GEFEL/cr.h:96-109) holds all
+ *    entries of each row with sorted columns; SCR (`symcomprow`,
+ *    GEFEL/scr.h:83-96) holds the lower triangle of each row with sorted
+ *    columns, so the diagonal is the last entry of its row; `adr` has n+1
+ *    entries and adr[n] = negm;
+ *  - code numbers are 1-based; 0 (or negative) means "no equation", as
+ *    produced by gtopology::gencodnum (GEFEL/gtopology.cpp:1619);
+ *  - pointers without a `_d` suffix on the function name are HOST pointers;
+ *    the library copies in, computes on the current CUDA device and copies
+ *    results back before returning;
+ *  - every call returns an sgpu_status; nothing throws across the ABI;
+ *    sgpu_last_error() gives a one-line description of the last failure.
+ */
+#ifndef SIFELGPU_H
+#define SIFELGPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SGPU_API __attribute__((visibility("default")))
+#else
+#define SGPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports through print_err (GEFEL/iotools.cpp:25)
+ * and returns early; here every condition is a return value. */
+typedef enum {
+  SGPU_OK = 0,
+  SGPU_NOT_CONVERGED = 1, /* iteration limit reached (reference: ani/ares untouched) */
+  SGPU_BREAKDOWN = 2,     /* |d.p| < zero (scr.cpp:1146-1151, cr.cpp:1177-1181) */
+  SGPU_BAD_INPUT = 3,     /* malformed storage, sizes, non-positive diagonal, ... */
+  SGPU_CUDA_ERROR = 4,    /* a CUDA runtime call failed */
+  SGPU_ZERO_RHS = 5       /* (f.f) < zero (scr.cpp:1117-1120, cr.cpp:1160-1164) */
+} sgpu_status;
+
+/* Stopping criteria of the reference routines (each keeps its own). */
+typedef enum {
+  SGPU_CRIT_SCR_PREC = 0, /* (r.r)/(f.f) < res   symcomprow::cg_prec, GEFEL/scr.cpp:1188 */
+  SGPU_CRIT_CR_PREC = 1,  /* sqrt((r.h)/(f.f)) < res  comprow::cg_prec, GEFEL/cr.cpp:1217 */
+  SGPU_CRIT_TRUE = 2      /* ||f - K x|| / ||f|| < res with the residual recomputed in FP64 */
+} sgpu_criterion;
+
+/* Arithmetic of the iteration. */
+typedef enum {
+  SGPU_FP64 = 0,  /* plain FP64 PCG: the drop-in for the reference call */
+  SGPU_MIXED = 1  /* FP32 inner PCG on the Jacobi-scaled matrix, with the true
+                     residual and the solution update recomputed in FP64
+                     (reliable-update iterative refinement) */
+} sgpu_mode;
+
+/* Solve report; every field is written by every solve entry point. */
+typedef struct {
+  int64_t iterations;       /* PCG iterations performed (all inner ones for MIXED) */
+  int64_t refinements;      /* FP64 residual recomputations (MIXED), else 0 */
+  double crit_value;        /* value of the routine's own criterion at exit */
+  double rh_over_ff;        /* (r.h)/(f.f) at exit, the reference's `ares` on convergence */
+  double true_relres;       /* ||f - K x||_2 / ||f||_2, recomputed in FP64 on the GPU */
+  double setup_ms;          /* upload + format conversion, device timed */
+  double solve_ms;          /* iteration, device timed */
+  double spmv_bytes;        /* algorithmic bytes of one SpMV of the iteration's format */
+  int32_t spmv_format;      /* 0 = CSR, 3 = 3x3 block rows (BSR3) */
+  int32_t spmv_variant;     /* autotuned kernel variant id */
+} sgpu_solve_info;
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in solver entry points (host arrays)                                */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces symcomprow::cg_prec (GEFEL/scr.cpp:1093-1205) with tprec = 1, as
+ * dispatched by gmatrix::solve_system (GEFEL/gmatrix.cpp:1225-1227).
+ * Same arguments and meaning: x (in/out; used as start vector when iv = 1),
+ * y = right-hand side (not modified), ni iteration limit, res threshold on
+ * (r.r)/(f.f), zero = the gmatrix's computer zero (1e-30).  As in the
+ * reference, *ani = i and *ares = (r.h)/(f.f) are written only on
+ * convergence.  mode: SGPU_FP64 reproduces the reference's iteration;
+ * SGPU_MIXED runs the FP32-inner / FP64-refined form to the same threshold
+ * measured on the true FP64 residual.  info may be NULL. */
+SGPU_API int sgpu_scr_cg_prec(int64_t n, const int64_t *adr, const int64_t *ci, const double *a, double *x,
+                     const double *y, int64_t ni, double res, int64_t *ani, double *ares,
+                     double zero, int64_t iv, int32_t mode, sgpu_solve_info *info);
+
+/* Replaces comprow::cg_prec (GEFEL/cr.cpp:1124-1240) with a `noprecond`
+ * preconditioner (h = r, GEFEL/precond.cpp:166-171), the only CR case the
+ * reference can run (gmatrix.cpp:1213-1214).  Stops on sqrt((r.h)/(f.f)) < res;
+ * afterwards *ani = i and *ares = r.h as the reference leaves them (cr.cpp:1236).
+ * prec = 1 selects Jacobi instead (the reference's CR path has no working
+ * Jacobi; the criterion is unchanged). */
+SGPU_API int sgpu_cr_cg_prec(int64_t n, const int64_t *adr, const int64_t *ci, const double *a, double *x,
+                    const double *y, int64_t ni, double res, int64_t *ani, double *ares,
+                    double zero, int64_t iv, int32_t prec, int32_t mode, sgpu_solve_info *info);
+
+/* ------------------------------------------------------------------------ */
+/* Device-resident matrices                                                 */
+/* ------------------------------------------------------------------------ */
+
+typedef struct sgpu_matrix_s *sgpu_matrix;
+
+/* Upload a GEFEL storage (symmetric != 0: SCR, else CR) and build the device
+ * formats (full CSR with int32 indices; the FP32 Jacobi-scaled copy and the
+ * 3x3 block form are built on first use).  Replaces the matrix half of
+ * gmatrix::initiate + localize (GEFEL/gmatrix.cpp:268/499) for callers that
+ * assemble on the host. */
+SGPU_API int sgpu_matrix_create(int64_t n, const int64_t *adr, const int64_t *ci, const double *a,
+                       int32_t symmetric, sgpu_matrix *out);
+/* New values in the same pattern (the storage the handle was created from). */
+SGPU_API int sgpu_matrix_update_values(sgpu_matrix m, const double *a);
+SGPU_API int sgpu_matrix_destroy(sgpu_matrix m);
+/* n and the number of stored entries of the full CSR form. */
+SGPU_API int sgpu_matrix_info(sgpu_matrix m, int64_t *n, int64_t *nnz_full);
+/* Copy the matrix back in GEFEL storage (symmetric != 0: SCR arrays of size
+ * n+1 / negm; else CR).  Pass ci = a = NULL to get the sizes first. */
+SGPU_API int sgpu_matrix_download(sgpu_matrix m, int32_t symmetric, int64_t *adr, int64_t *ci, double *a,
+                         int64_t *negm);
+
+/* y = A x (mxv_scr / mxv_cr semantics, GEFEL/scr.cpp:655, cr.cpp:653).
+ * Host vectors. */
+SGPU_API int sgpu_matrix_mxv(sgpu_matrix m, const double *x, double *y);
+/* Same on device pointers (FP64), on the handle's stream. */
+SGPU_API int sgpu_matrix_mxv_d(sgpu_matrix m, const double *x_d, double *y_d);
+
+/* Run the handle's work on a caller's CUDA stream (cudaStream_t passed as a
+ * pointer; NULL restores the handle's own stream). */
+SGPU_API int sgpu_matrix_set_stream(sgpu_matrix m, void *stream);
+/* y = (S A S) x in FP32 with S = diag(A)^-1/2: the operator of the mixed
+ * iteration, device pointers, autotuned format/kernel. */
+SGPU_API int sgpu_matrix_mxv32_d(sgpu_matrix m, const float *x_d, float *y_d);
+/* Algorithmic bytes of one SpMV (precision 64 or 32) in the tuned format,
+ * the format id (0 CSR, 3 BSR3) and the kernel variant; tunes if needed. */
+SGPU_API int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *bytes, int32_t *format,
+                                   int32_t *variant);
+
+/* Jacobi-PCG on a device-resident matrix, host vectors.  crit selects the
+ * reference routine whose criterion is kept. */
+SGPU_API int sgpu_matrix_pcg(sgpu_matrix m, double *x, const double *f, int64_t ni, double res,
+                    double zero, int64_t iv, int32_t crit, int32_t prec, int32_t mode,
+                    int64_t *ani, double *ares, sgpu_solve_info *info);
+/* Same on device vectors (x_d in/out, f_d read-only), no host copies. */
+SGPU_API int sgpu_matrix_pcg_d(sgpu_matrix m, double *x_d, const double *f_d, int64_t ni, double res,
+                      double zero, int64_t iv, int32_t crit, int32_t prec, int32_t mode,
+                      int64_t *ani, double *ares, sgpu_solve_info *info);
+
+/* ------------------------------------------------------------------------ */
+/* Assembly on the GPU                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Element kinds of the hot path. */
+typedef enum {
+  SGPU_ELEM_HEX8 = 0,    /* linhex, 3D elasticity, 2x2x2 Gauss (MEFEL/SRC/linhex.cpp:583) */
+  SGPU_ELEM_QUAD4 = 1,   /* planeelemlq, plane stress, 2x2 Gauss (MEFEL/SRC/plelemlq.cpp:611) */
+  SGPU_ELEM_HEX8T_K = 2, /* linhext conductivity (TRFEL/SRC/linhext.cpp:774) */
+  SGPU_ELEM_HEX8T_C = 3  /* linhext capacity (TRFEL/SRC/linhext.cpp:979) */
+} sgpu_elem_kind;
+
+/* A mesh in SIFEL's terms.  Node order inside an element follows SIFEL
+ * (GEFEL/basefun.cpp:2299 for hexahedra, :609 for quadrilaterals). */
+typedef struct {
+  int32_t kind;          /* sgpu_elem_kind */
+  int32_t ndofn;         /* DOFs per node: 3 (hex8), 2 (quad4), 1 (hex8t) */
+  int64_t nn;            /* nodes */
+  const double *coords;  /* nn x 3 (z ignored for quad4) */
+  int64_t ne;            /* elements */
+  const int64_t *elems;  /* ne x nne, 0-based node ids */
+  const int64_t *cn;     /* nn x ndofn code numbers (1-based, <= 0: no equation) */
+  const double *emat;    /* ne x 2: (E, nu) for elasticity, (k, c) for hex8t */
+  const double *thick;   /* ne thicknesses (quad4), else NULL */
+  const double *rho;     /* ne densities (capacity), NULL = 1 */
+} sgpu_mesh;
+
+typedef struct {
+  int64_t n;          /* equations */
+  int64_t negm_scr;   /* entries of the SCR (lower-triangle) storage */
+  int64_t nnz_full;   /* entries of the full CSR on the device */
+  int32_t colours;    /* element colours of the atomic-free scatter */
+  double pattern_ms;  /* pattern build (device timed) */
+  double integrate_ms;/* element integration + scatter (device timed) */
+} sgpu_assembly_info;
+
+/* Assemble the global matrix of a mesh on the GPU into a new device-resident
+ * handle.  Replaces stiffness_matrix (MEFEL/SRC/globmat.cpp:41) and
+ * conductivity_matrix / capacity_matrix (TRFEL/SRC/globmatt.cpp:19/92)
+ * including the storage initiation (symcomprow::initiate, GEFEL/scr.cpp:556).
+ * sgpu_matrix_download gives the SCR or CR arrays the reference would hold. */
+SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembly_info *info);
+/* Re-integrate the values of a handle made by sgpu_assemble, on the same
+ * pattern: new per-element parameters (emat, rho; NULL keeps the old ones) or,
+ * for hex8t handles, the other matrix (kind K <-> C). */
+SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,
+                             sgpu_assembly_info *info);
+
+/* ------------------------------------------------------------------------ */
+/* Library state                                                            */
+/* ------------------------------------------------------------------------ */
+
+SGPU_API const char *sgpu_last_error(void);
+SGPU_API const char *sgpu_version(void);
+/* Number of kernels this library launched in the calling process so far. */
+SGPU_API int64_t sgpu_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIFELGPU_H */

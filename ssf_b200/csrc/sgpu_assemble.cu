@@ -1,0 +1,688 @@
+// Batched element integration fused with an atomic-free, colour-ordered
+// scatter into the device CSR.
+//
+// Reference path: stiffness_matrix (MEFEL/SRC/globmat.cpp:41-143) loops over
+// elements, calls linhex::res_stiffness_matrix (MEFEL/SRC/linhex.cpp:741 ->
+// gl_stiffness_matrix :583) or planeelemlq::res_stiffness_matrix
+// (MEFEL/SRC/plelemlq.cpp:785 -> :611), and localises each element matrix
+// with symcomprow::localize (GEFEL/scr.cpp:422) / comprow::localize
+// (GEFEL/cr.cpp:327).  TRFEL does the same with linhext::conductivity_matrix
+// and capacity_matrix (TRFEL/SRC/linhext.cpp:774/979) in
+// conductivity_matrix / capacity_matrix (TRFEL/SRC/globmatt.cpp:19/92).
+//
+// Here:
+//  1. pattern: every element emits its (row, col <= row) equation pairs as
+//     64-bit keys; one radix sort + unique gives the SCR pattern
+//     (symcomprow::initiate, GEFEL/scr.cpp:556), from which the full CSR is
+//     built (sgpu_matrix.cu);
+//  2. colouring: greedy first-fit on the host over node masks -- elements of
+//     one colour share no node, so their element matrices can be added into
+//     the CSR without atomics, and the sum order is fixed (deterministic);
+//  3. one launch per colour: one warp per element; lanes 0..G-1 compute the
+//     Jacobian and Cartesian shape-function gradients of one Gauss point each
+//     (derivatives_3d, GEFEL/difcalc.cpp:487) into shared memory, then every
+//     lane forms whole node-pair blocks B_a^T D B_b summed over the Gauss
+//     points and adds them into the CSR rows (binary search per row).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "sgpu_internal.cuh"
+
+namespace sgpu {
+
+namespace {
+
+constexpr int TPB = 256;
+constexpr int WPB = TPB / 32;
+
+inline int blocks_for(int64_t n, int tpb = TPB) {
+  int64_t b = (n + tpb - 1) / tpb;
+  return (int)(b < 1 ? 1 : (b > 1048576 ? 1048576 : b));
+}
+
+// Gauss rule of order 2 with the reference's 15-digit constant (GEFEL/intp.cpp:26-27)
+__constant__ double c_gp2[2] = {-0.577350269189626, 0.577350269189626};
+
+// ---------------------------------------------------------------------------
+// pattern
+// ---------------------------------------------------------------------------
+__global__ void k_elem_codes(int64_t ne, int nne, int ndofn, const int64_t *__restrict__ elems,
+                             const int64_t *__restrict__ cn, int *__restrict__ cne, unsigned *err, int64_t nn) {
+  const int ndofe = nne * ndofn;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ne * ndofe;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / ndofe;
+    const int q = (int)(t % ndofe), a = q / ndofn, i = q % ndofn;
+    const int64_t node = elems[e * nne + a];
+    int code = -1;
+    if (node < 0 || node >= nn) {
+      atomicOr(err, 1u);
+    } else {
+      const int64_t c = cn[node * ndofn + i];
+      code = c > 0 ? (int)(c - 1) : -1;
+    }
+    cne[t] = code;
+  }
+}
+
+// lower-triangle (row >= col) equation pairs of every element
+__global__ void k_elem_pairs(int64_t ne, int ndofe, const int *__restrict__ cne,
+                             unsigned long long *__restrict__ keys) {
+  const int npair = ndofe * ndofe;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ne * npair;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / npair;
+    const int q = (int)(t % npair), i = q / ndofe, j = q % ndofe;
+    const int r = cne[e * ndofe + i], c = cne[e * ndofe + j];
+    unsigned long long k = ~0ull;  // sorts last, dropped
+    if (r >= 0 && c >= 0 && c <= r) k = ((unsigned long long)(unsigned)r << 32) | (unsigned)c;
+    keys[t] = k;
+  }
+}
+
+__global__ void k_keys_to_scr(int64_t m, int64_t n, const unsigned long long *__restrict__ keys,
+                              int64_t *__restrict__ adr, int64_t *__restrict__ ci) {
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < m; s += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long k = keys[s];
+    const int64_t r = (int64_t)(k >> 32);
+    ci[s] = (int64_t)(k & 0xffffffffull);
+    if (s == 0 || (keys[s - 1] >> 32) != (unsigned long long)r) adr[r] = s;
+    if (s == m - 1) adr[n] = m;
+  }
+}
+
+__global__ void k_check_adr(int64_t n, const int64_t *__restrict__ adr, unsigned *err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (adr[i] < 0) atomicOr(err, 2u);  // an equation no element touches
+}
+
+// ---------------------------------------------------------------------------
+// element kernels
+// ---------------------------------------------------------------------------
+
+// position of column c in the sorted CSR row [b, e), or -1
+__device__ __forceinline__ int find_col(const int *__restrict__ col, int b, int e, int c) {
+  int lo = b, hi = e - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = __ldg(col + mid);
+    if (v == c) return mid;
+    if (v < c) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+// dN/dxi, dN/deta, dN/dzeta of the trilinear hexahedron (GEFEL/basefun.cpp:2316-2370)
+__device__ __forceinline__ void hex_dnat(double xi, double eta, double zeta, double *nx, double *ny, double *nz) {
+  const double sx[8] = {1, -1, -1, 1, 1, -1, -1, 1};
+  const double sy[8] = {1, 1, -1, -1, 1, 1, -1, -1};
+  const double sz[8] = {1, 1, 1, 1, -1, -1, -1, -1};
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    nx[a] = sx[a] * (1.0 + sy[a] * eta) * (1.0 + sz[a] * zeta) / 8.0;
+    ny[a] = sy[a] * (1.0 + sx[a] * xi) * (1.0 + sz[a] * zeta) / 8.0;
+    nz[a] = sz[a] * (1.0 + sx[a] * xi) * (1.0 + sy[a] * eta) / 8.0;
+  }
+}
+
+__device__ __forceinline__ void hex_n(double xi, double eta, double zeta, double *n) {
+  const double sx[8] = {1, -1, -1, 1, 1, -1, -1, 1};
+  const double sy[8] = {1, 1, -1, -1, 1, 1, -1, -1};
+  const double sz[8] = {1, 1, 1, 1, -1, -1, -1, -1};
+#pragma unroll
+  for (int a = 0; a < 8; a++) n[a] = (1.0 + sx[a] * xi) * (1.0 + sy[a] * eta) * (1.0 + sz[a] * zeta) / 8.0;
+}
+
+// Per-warp shared storage: Cartesian gradients at the Gauss points and
+// |detJ| * weight (times the point's extra factor).
+struct HexShared {
+  double g[8][8][3];  // [gp][node][x,y,z]
+  double w[8];
+  double nb[8][8];    // shape functions at the Gauss points (capacity)
+};
+
+// lanes 0..7: Gauss point `lane` (reference loop order xi, eta, zeta)
+__device__ __forceinline__ void hex_gauss_point(int lane, const double *x, const double *y, const double *z,
+                                                HexShared &sh, bool want_n) {
+  if (lane < 8) {
+    const double xi = c_gp2[(lane >> 2) & 1], eta = c_gp2[(lane >> 1) & 1], zeta = c_gp2[lane & 1];
+    double nx[8], ny[8], nz[8];
+    hex_dnat(xi, eta, zeta, nx, ny, nz);
+    double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0;
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nz[a] * x[a];
+      d4 += nx[a] * y[a]; d5 += ny[a] * y[a]; d6 += nz[a] * y[a];
+      d7 += nx[a] * z[a]; d8 += ny[a] * z[a]; d9 += nz[a] * z[a];
+    }
+    const double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      const double ddx = nx[a], ddy = ny[a], ddz = nz[a];
+      sh.g[lane][a][0] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
+      sh.g[lane][a][1] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
+      sh.g[lane][a][2] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+    }
+    sh.w[lane] = fabs(jac);  // weights are 1 for the order-2 rule
+    if (want_n) {
+      double n[8];
+      hex_n(xi, eta, zeta, n);
+#pragma unroll
+      for (int a = 0; a < 8; a++) sh.nb[lane][a] = n[a];
+    }
+  }
+}
+
+// add v into CSR entry (r, c); both >= 0
+__device__ __forceinline__ void csr_add(const int *__restrict__ rowptr, const int *__restrict__ col,
+                                        double *__restrict__ val, int r, int c, double v, unsigned *err) {
+  const int p = find_col(col, __ldg(rowptr + r), __ldg(rowptr + r + 1), c);
+  if (p >= 0) val[p] += v;
+  else atomicOr(err, 4u);
+}
+
+// hex8 elasticity (linhex::gl_stiffness_matrix): block (a,b) of
+// sum_gp |J| B_a^T D B_b with B rows [xx, yy, zz, yz, xz, xy]
+// (linhex::geom_matrix, MEFEL/SRC/linhex.cpp:153-186) and isotropic D
+// (elastisomat::matstiff_spacestr, MEFEL/SRC/elastisomat.cpp:395-420)
+__global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__restrict__ elist,
+                                                      const double *__restrict__ coords,
+                                                      const int64_t *__restrict__ elems,
+                                                      const int *__restrict__ cne, const double *__restrict__ emat,
+                                                      const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                      double *__restrict__ val, unsigned *err) {
+  __shared__ HexShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexShared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double x[8], y[8], z[8];
+    double cx = 0, cy = 0, cz = 0;
+    if (lane < 8) {
+      const int64_t nd = elems[(int64_t)e * 8 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1]; cz = coords[3 * nd + 2];
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+      z[a] = __shfl_sync(0xffffffffu, cz, a);
+    }
+    hex_gauss_point(lane, x, y, z, sh, false);
+    __syncwarp();
+    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+    const double G = E / 2.0 / (1.0 + nu);
+    const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
+    const double d0 = s * (1 - nu), d1 = s * nu;
+    int code[24];
+#pragma unroll
+    for (int q = 0; q < 24; q++) code[q] = __ldg(cne + (int64_t)e * 24 + q);
+    for (int blk = lane; blk < 64; blk += 32) {
+      const int a = blk >> 3, b = blk & 7;
+      double k[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+      for (int gp = 0; gp < 8; gp++) {
+        const double ax = sh.g[gp][a][0], ay = sh.g[gp][a][1], az = sh.g[gp][a][2];
+        const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1], bz = sh.g[gp][b][2];
+        const double w = sh.w[gp];
+        // D B_b: columns (u, v, w) of node b
+        // rows: xx, yy, zz, yz, xz, xy
+        const double db[6][3] = {{d0 * bx, d1 * by, d1 * bz}, {d1 * bx, d0 * by, d1 * bz}, {d1 * bx, d1 * by, d0 * bz},
+                                 {0.0, G * bz, G * by},        {G * bz, 0.0, G * bx},        {G * by, G * bx, 0.0}};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          // B_a^T rows: u -> (xx: ax, xz: az, xy: ay); v -> (yy: ay, yz: az, xy: ax); w -> (zz: az, yz: ay, xz: ax)
+          k[0][j] += w * (ax * db[0][j] + az * db[4][j] + ay * db[5][j]);
+          k[1][j] += w * (ay * db[1][j] + az * db[3][j] + ax * db[5][j]);
+          k[2][j] += w * (az * db[2][j] + ay * db[3][j] + ax * db[4][j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int r = code[3 * a + i];
+        if (r < 0) continue;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          const int c = code[3 * b + j];
+          if (c >= 0) csr_add(rowptr, col, val, r, c, k[i][j], err);
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// quad4 plane stress (planeelemlq::gl_stiffness_matrix, MEFEL/SRC/plelemlq.cpp:611-690):
+// B rows [xx, yy, xy] (geom_matrix, :294-320), D plane stress
+// (elastisomat::matstiff_plstress, MEFEL/SRC/elastisomat.cpp:255), thickness
+// interpolated at the Gauss point from nodal values (here all equal to the
+// element's cross-section thickness, mechcrsec::give_thickness :397-411)
+struct QuadShared {
+  double g[4][4][2];
+  double w[4];
+};
+
+__global__ void __launch_bounds__(TPB) k_quad4_elastic(int ne_c, const int *__restrict__ elist,
+                                                       const double *__restrict__ coords,
+                                                       const int64_t *__restrict__ elems,
+                                                       const int *__restrict__ cne, const double *__restrict__ emat,
+                                                       const double *__restrict__ thick,
+                                                       const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                       double *__restrict__ val, unsigned *err) {
+  __shared__ QuadShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  QuadShared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double x[4], y[4], cx = 0, cy = 0;
+    if (lane < 4) {
+      const int64_t nd = elems[(int64_t)e * 4 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+    }
+    const double t_e = thick[e];
+    if (lane < 4) {
+      const double xi = c_gp2[(lane >> 1) & 1], eta = c_gp2[lane & 1];
+      // bf_lin_4_2d derivatives (GEFEL/basefun.cpp:609-655)
+      const double nx[4] = {0.25 * (1.0 + eta), 0.25 * (-1.0 - eta), 0.25 * (-1.0 + eta), 0.25 * (1.0 - eta)};
+      const double ny[4] = {0.25 * (1.0 + xi), 0.25 * (1.0 - xi), 0.25 * (-1.0 + xi), 0.25 * (-1.0 - xi)};
+      const double n[4] = {0.25 * (1.0 + xi) * (1.0 + eta), 0.25 * (1.0 - xi) * (1.0 + eta),
+                           0.25 * (1.0 - xi) * (1.0 - eta), 0.25 * (1.0 + xi) * (1.0 - eta)};
+      double d1 = 0, d2 = 0, d3 = 0, d4 = 0, th = 0;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nx[a] * y[a]; d4 += ny[a] * y[a];
+        th += n[a] * t_e;
+      }
+      const double jac = d1 * d4 - d2 * d3;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        sh.g[lane][a][0] = (nx[a] * d4 - ny[a] * d3) / jac;
+        sh.g[lane][a][1] = (ny[a] * d1 - nx[a] * d2) / jac;
+      }
+      sh.w[lane] = fabs(jac * th);
+    }
+    __syncwarp();
+    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+    const double c = E / (1.0 - nu * nu), d01 = c * nu, g3 = E / 2.0 / (1.0 + nu);
+    if (lane < 16) {
+      const int a = lane >> 2, b = lane & 3;
+      double k00 = 0, k01 = 0, k10 = 0, k11 = 0;
+#pragma unroll
+      for (int gp = 0; gp < 4; gp++) {
+        const double ax = sh.g[gp][a][0], ay = sh.g[gp][a][1];
+        const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1];
+        const double w = sh.w[gp];
+        // D B_b (rows xx, yy, xy; columns u, v)
+        const double db00 = c * bx, db01 = d01 * by, db10 = d01 * bx, db11 = c * by, db20 = g3 * by, db21 = g3 * bx;
+        k00 += w * (ax * db00 + ay * db20);
+        k01 += w * (ax * db01 + ay * db21);
+        k10 += w * (ay * db10 + ax * db20);
+        k11 += w * (ay * db11 + ax * db21);
+      }
+      const int r0 = __ldg(cne + (int64_t)e * 8 + 2 * a), r1 = __ldg(cne + (int64_t)e * 8 + 2 * a + 1);
+      const int c0 = __ldg(cne + (int64_t)e * 8 + 2 * b), c1 = __ldg(cne + (int64_t)e * 8 + 2 * b + 1);
+      if (r0 >= 0) {
+        if (c0 >= 0) csr_add(rowptr, col, val, r0, c0, k00, err);
+        if (c1 >= 0) csr_add(rowptr, col, val, r0, c1, k01, err);
+      }
+      if (r1 >= 0) {
+        if (c0 >= 0) csr_add(rowptr, col, val, r1, c0, k10, err);
+        if (c1 >= 0) csr_add(rowptr, col, val, r1, c1, k11, err);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// hex8 conduction (linhext::conductivity_matrix, TRFEL/SRC/linhext.cpp:774-840,
+// isotropic D = k I, isotrmat::matcond3d) or capacity
+// (linhext::capacity_matrix, :979-1030: N^T N rho c |J| w)
+template <bool CAPACITY>
+__global__ void __launch_bounds__(TPB) k_hex8_scalar(int ne_c, const int *__restrict__ elist,
+                                                     const double *__restrict__ coords,
+                                                     const int64_t *__restrict__ elems,
+                                                     const int *__restrict__ cne, const double *__restrict__ emat,
+                                                     const double *__restrict__ rho,
+                                                     const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                     double *__restrict__ val, unsigned *err) {
+  __shared__ HexShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexShared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double x[8], y[8], z[8], cx = 0, cy = 0, cz = 0;
+    if (lane < 8) {
+      const int64_t nd = elems[(int64_t)e * 8 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1]; cz = coords[3 * nd + 2];
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+      z[a] = __shfl_sync(0xffffffffu, cz, a);
+    }
+    hex_gauss_point(lane, x, y, z, sh, CAPACITY);
+    __syncwarp();
+    const double kc = emat[2 * (int64_t)e], cc = emat[2 * (int64_t)e + 1];
+    const double re = rho ? rho[e] : 1.0;
+    for (int blk = lane; blk < 64; blk += 32) {
+      const int a = blk >> 3, b = blk & 7;
+      double v = 0.0;
+#pragma unroll
+      for (int gp = 0; gp < 8; gp++) {
+        if (CAPACITY) {
+          // rho interpolated from equal nodal densities: sum_a N_a rho
+          double r = 0.0;
+#pragma unroll
+          for (int q = 0; q < 8; q++) r += sh.nb[gp][q] * re;
+          v += (sh.nb[gp][a] * sh.nb[gp][b]) * (sh.w[gp] * r * cc);
+        } else {
+          const double gg = sh.g[gp][a][0] * sh.g[gp][b][0] + sh.g[gp][a][1] * sh.g[gp][b][1] +
+                            sh.g[gp][a][2] * sh.g[gp][b][2];
+          v += gg * kc * sh.w[gp];
+        }
+      }
+      const int r = __ldg(cne + (int64_t)e * 8 + a), c = __ldg(cne + (int64_t)e * 8 + b);
+      if (r >= 0 && c >= 0) csr_add(rowptr, col, val, r, c, v, err);
+    }
+    __syncwarp();
+  }
+}
+
+int read_err(const unsigned *err_d, cudaStream_t s, unsigned *out) {
+  SGPU_CUDA(cudaMemcpyAsync(out, err_d, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  return SGPU_OK;
+}
+
+// greedy first-fit colouring over per-node colour masks: an element takes the
+// lowest colour no element sharing one of its nodes already has
+int colour_elements(int64_t nn, int64_t ne, int nne, const int64_t *elems, std::vector<int> &order,
+                    std::vector<int> &offsets) {
+  std::vector<uint64_t> mask((size_t)nn, 0);
+  std::vector<int> colour((size_t)ne);
+  int ncol = 0;
+  for (int64_t e = 0; e < ne; e++) {
+    uint64_t used = 0;
+    for (int a = 0; a < nne; a++) used |= mask[(size_t)elems[e * nne + a]];
+    if (used == ~0ull) return fail(SGPU_BAD_INPUT, "mesh needs more than 64 element colours");
+    const int c = __builtin_ctzll(~used);
+    colour[(size_t)e] = c;
+    ncol = std::max(ncol, c + 1);
+    for (int a = 0; a < nne; a++) mask[(size_t)elems[e * nne + a]] |= (1ull << c);
+  }
+  offsets.assign(ncol + 1, 0);
+  for (int64_t e = 0; e < ne; e++) offsets[colour[(size_t)e] + 1]++;
+  for (int c = 0; c < ncol; c++) offsets[c + 1] += offsets[c];
+  order.resize((size_t)ne);
+  std::vector<int> fill(offsets.begin(), offsets.end() - 1);
+  for (int64_t e = 0; e < ne; e++) order[(size_t)fill[colour[(size_t)e]]++] = (int)e;
+  return SGPU_OK;
+}
+
+}  // namespace
+
+// Assembly state kept with the matrix handle so that values can be
+// re-integrated (new materials, the capacity form) on the same pattern.
+struct AssemblyData {
+  int kind = 0, nne = 0, ndofn = 0;
+  int64_t nn = 0, ne = 0;
+  DevBuf<double> coords, emat, thick, rho;
+  DevBuf<int64_t> elems;
+  DevBuf<int> cne, elist;
+  std::vector<int> offsets;
+};
+
+int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
+  cudaStream_t s = m->stream;
+  Csr &c = m->csr;
+  DevBuf<unsigned> err;
+  SGPU_TRY(err.alloc(1));
+  SGPU_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
+  SGPU_CUDA(cudaMemsetAsync(c.val.p, 0, (size_t)c.nnz * sizeof(double), s));
+  SGPU_CUDA(cudaEventRecord(m->ev0, s));
+  const int ncol = (int)ad.offsets.size() - 1;
+  for (int col = 0; col < ncol; col++) {
+    const int beg = ad.offsets[col], cnt = ad.offsets[col + 1] - beg;
+    if (cnt == 0) continue;
+    const int grid = std::min((cnt + WPB - 1) / WPB, kNumSMs * 16);
+    const int *el = ad.elist.p + beg;
+    switch (kind) {
+      case 0:
+        k_hex8_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, c.rowptr.p,
+                                            c.col.p, c.val.p, err.p);
+        break;
+      case 1:
+        k_quad4_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,
+                                             c.rowptr.p, c.col.p, c.val.p, err.p);
+        break;
+      case 2:
+        k_hex8_scalar<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, nullptr,
+                                                  c.rowptr.p, c.col.p, c.val.p, err.p);
+        break;
+      default:
+        k_hex8_scalar<true><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                 ad.rho.p ? ad.rho.p : nullptr, c.rowptr.p, c.col.p, c.val.p,
+                                                 err.p);
+        break;
+    }
+    count_launches(1);
+    SGPU_CUDA(cudaGetLastError());
+  }
+  SGPU_CUDA(cudaEventRecord(m->ev1, s));
+  unsigned e = 0;
+  SGPU_TRY(read_err(err.p, s, &e));
+  if (e) return fail(SGPU_BAD_INPUT, "element scatter found no CSR entry (bits " + std::to_string(e) + ")");
+  float ms = 0.f;
+  SGPU_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+  if (ms_out) *ms_out = ms;
+  return SGPU_OK;
+}
+
+}  // namespace sgpu
+
+using namespace sgpu;
+
+struct sgpu_assembly_s {
+  sgpu::AssemblyData d;
+};
+
+extern "C" {
+
+SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembly_info *info) {
+  if (!mesh || !out) return fail(SGPU_BAD_INPUT, "null argument");
+  *out = nullptr;
+  if (info) memset(info, 0, sizeof(*info));
+  const int kind = mesh->kind;
+  int nne, ndofn;
+  switch (kind) {
+    case SGPU_ELEM_HEX8: nne = 8; ndofn = 3; break;
+    case SGPU_ELEM_QUAD4: nne = 4; ndofn = 2; break;
+    case SGPU_ELEM_HEX8T_K:
+    case SGPU_ELEM_HEX8T_C: nne = 8; ndofn = 1; break;
+    default: return fail(SGPU_BAD_INPUT, "unknown element kind");
+  }
+  if (mesh->ndofn != ndofn) return fail(SGPU_BAD_INPUT, "ndofn does not match the element kind");
+  if (mesh->nn <= 0 || mesh->ne <= 0 || !mesh->coords || !mesh->elems || !mesh->cn || !mesh->emat)
+    return fail(SGPU_BAD_INPUT, "empty mesh");
+  if (kind == SGPU_ELEM_QUAD4 && !mesh->thick) return fail(SGPU_BAD_INPUT, "quad4 needs thicknesses");
+  if (mesh->ne > (1LL << 31) - 1) return fail(SGPU_BAD_INPUT, "too many elements");
+  const int64_t nn = mesh->nn, ne = mesh->ne;
+  const int ndofe = nne * ndofn;
+  // number of equations = largest code number
+  int64_t n = 0;
+  for (int64_t q = 0; q < nn * ndofn; q++) n = std::max<int64_t>(n, mesh->cn[q]);
+  if (n <= 0) return fail(SGPU_BAD_INPUT, "no free equations");
+  for (int64_t q = 0; q < ne * nne; q++)
+    if (mesh->elems[q] < 0 || mesh->elems[q] >= nn) return fail(SGPU_BAD_INPUT, "element node out of range");
+
+  sgpu_matrix m = new sgpu_matrix_s();
+  m->n = n;
+  m->src_sym = 1;
+  auto bail = [&](int st) {
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    cudaStream_t s = m->own_stream;
+    cudaEvent_t a = m->ev0, b = m->ev1;
+    delete m;
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (s) cudaStreamDestroy(s);
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&m->ev0) != cudaSuccess || cudaEventCreate(&m->ev1) != cudaSuccess)
+    return bail(fail(SGPU_CUDA_ERROR, "stream/event creation failed"));
+  m->stream = m->own_stream;
+  cudaStream_t s = m->stream;
+  m->asm_data = new sgpu_assembly_s();
+  AssemblyData &ad = m->asm_data->d;
+  ad.kind = kind; ad.nne = nne; ad.ndofn = ndofn; ad.nn = nn; ad.ne = ne;
+  int st;
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, s);
+#define BAIL_ON(x)                        \
+  do {                                    \
+    st = (x);                             \
+    if (st != SGPU_OK) {                  \
+      cudaEventDestroy(t0);               \
+      cudaEventDestroy(t1);               \
+      return bail(st);                    \
+    }                                     \
+  } while (0)
+  BAIL_ON(ad.coords.alloc(nn * 3));
+  BAIL_ON(ad.elems.alloc(ne * nne));
+  BAIL_ON(ad.emat.alloc(ne * 2));
+  DevBuf<int64_t> cn_d;
+  BAIL_ON(cn_d.alloc(nn * ndofn));
+  BAIL_ON(ad.cne.alloc(ne * ndofe));
+  cudaMemcpyAsync(ad.coords.p, mesh->coords, nn * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(ad.elems.p, mesh->elems, ne * nne * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(ad.emat.p, mesh->emat, ne * 2 * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(cn_d.p, mesh->cn, nn * ndofn * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+  if (mesh->thick) {
+    BAIL_ON(ad.thick.alloc(ne));
+    cudaMemcpyAsync(ad.thick.p, mesh->thick, ne * sizeof(double), cudaMemcpyHostToDevice, s);
+  }
+  if (mesh->rho) {
+    BAIL_ON(ad.rho.alloc(ne));
+    cudaMemcpyAsync(ad.rho.p, mesh->rho, ne * sizeof(double), cudaMemcpyHostToDevice, s);
+  }
+  DevBuf<unsigned> err;
+  BAIL_ON(err.alloc(1));
+  cudaMemsetAsync(err.p, 0, sizeof(unsigned), s);
+  k_elem_codes<<<blocks_for(ne * ndofe), TPB, 0, s>>>(ne, nne, ndofn, ad.elems.p, cn_d.p, ad.cne.p, err.p, nn);
+  count_launches(1);
+
+  // pattern: lower-triangle pairs -> sort -> unique -> SCR
+  {
+    const int64_t npairs = ne * (int64_t)ndofe * ndofe;
+    if (npairs > (1LL << 31) - 1) return bail(fail(SGPU_BAD_INPUT, "mesh too large for one pattern sort"));
+    DevBuf<unsigned long long> keys, skeys;
+    BAIL_ON(keys.alloc(npairs));
+    BAIL_ON(skeys.alloc(npairs));
+    k_elem_pairs<<<blocks_for(npairs), TPB, 0, s>>>(ne, ndofe, ad.cne.p, keys.p);
+    count_launches(1);
+    const int end_bit = 64;  // invalid keys (~0) must sort last
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tmp, keys.p, skeys.p, (int)npairs, 0, end_bit, s);
+    DevBuf<unsigned char> t;
+    BAIL_ON(t.alloc(tmp));
+    cub::DeviceRadixSort::SortKeys(t.p, tmp, keys.p, skeys.p, (int)npairs, 0, end_bit, s);
+    DevBuf<int> nsel;
+    BAIL_ON(nsel.alloc(1));
+    size_t tmp2 = 0;
+    cub::DeviceSelect::Unique(nullptr, tmp2, skeys.p, keys.p, nsel.p, (int)npairs, s);
+    DevBuf<unsigned char> t2;
+    BAIL_ON(t2.alloc(tmp2));
+    cub::DeviceSelect::Unique(t2.p, tmp2, skeys.p, keys.p, nsel.p, (int)npairs, s);
+    count_launches(6);
+    int nuniq = 0;
+    cudaMemcpyAsync(&nuniq, nsel.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(SGPU_CUDA_ERROR, "pattern sort failed"));
+    // drop the trailing invalid key, if any
+    unsigned long long lastk = 0;
+    cudaMemcpy(&lastk, keys.p + nuniq - 1, sizeof(lastk), cudaMemcpyDeviceToHost);
+    const int64_t negm = (lastk == ~0ull) ? nuniq - 1 : nuniq;
+    m->src_negm = negm;
+    BAIL_ON(m->src_adr.alloc(n + 1));
+    BAIL_ON(m->src_ci.alloc(negm));
+    cudaMemsetAsync(m->src_adr.p, 0xff, (n + 1) * sizeof(int64_t), s);
+    k_keys_to_scr<<<blocks_for(negm), TPB, 0, s>>>(negm, n, keys.p, m->src_adr.p, m->src_ci.p);
+    k_check_adr<<<blocks_for(n), TPB, 0, s>>>(n, m->src_adr.p, err.p);
+    count_launches(2);
+    unsigned e = 0;
+    BAIL_ON(read_err(err.p, s, &e));
+    if (e) return bail(fail(SGPU_BAD_INPUT, "code numbers: element node out of range or unused equation"));
+  }
+  BAIL_ON(matrix_build_from_device_src(m));
+  cudaEventRecord(t1, s);
+  cudaEventSynchronize(t1);
+  float pattern_ms = 0.f;
+  cudaEventElapsedTime(&pattern_ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+
+  // colouring (host) and the per-colour element lists
+  std::vector<int> order;
+  st = colour_elements(nn, ne, nne, mesh->elems, order, ad.offsets);
+  if (st != SGPU_OK) return bail(st);
+  if (ad.elist.alloc(ne) != SGPU_OK) return bail(SGPU_CUDA_ERROR);
+  cudaMemcpyAsync(ad.elist.p, order.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s);
+  float asm_ms = 0.f;
+  st = assemble_values(m, ad, kind, &asm_ms);
+  if (st != SGPU_OK) return bail(st);
+  st = finish_values(m);
+  if (st != SGPU_OK) return bail(st);
+  if (info) {
+    info->n = n;
+    info->negm_scr = m->src_negm;
+    info->nnz_full = m->csr.nnz;
+    info->colours = (int32_t)ad.offsets.size() - 1;
+    info->pattern_ms = pattern_ms;
+    info->integrate_ms = asm_ms;
+  }
+  *out = m;
+  return SGPU_OK;
+#undef BAIL_ON
+}
+
+SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,
+                             sgpu_assembly_info *info) {
+  if (!m || !m->asm_data) return fail(SGPU_BAD_INPUT, "handle was not created by sgpu_assemble");
+  AssemblyData &ad = m->asm_data->d;
+  const bool scalar_ok = (ad.kind == SGPU_ELEM_HEX8T_K || ad.kind == SGPU_ELEM_HEX8T_C) &&
+                         (kind == SGPU_ELEM_HEX8T_K || kind == SGPU_ELEM_HEX8T_C);
+  if (kind != ad.kind && !scalar_ok) return fail(SGPU_BAD_INPUT, "element kind differs from the pattern's");
+  cudaStream_t s = m->stream;
+  if (emat) SGPU_CUDA(cudaMemcpyAsync(ad.emat.p, emat, ad.ne * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (rho) {
+    SGPU_TRY(ad.rho.alloc(ad.ne));
+    SGPU_CUDA(cudaMemcpyAsync(ad.rho.p, rho, ad.ne * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  float ms = 0.f;
+  SGPU_TRY(assemble_values(m, ad, kind, &ms));
+  SGPU_TRY(finish_values(m));
+  if (info) {
+    memset(info, 0, sizeof(*info));
+    info->n = m->n;
+    info->negm_scr = m->src_negm;
+    info->nnz_full = m->csr.nnz;
+    info->colours = (int32_t)ad.offsets.size() - 1;
+    info->integrate_ms = ms;
+  }
+  return SGPU_OK;
+}
+
+}  // extern "C"
+
+void sgpu_free_assembly(sgpu_assembly_s *a) { delete a; }

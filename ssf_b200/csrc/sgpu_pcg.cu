@@ -1,0 +1,961 @@
+// SpMV kernels, fused PCG vector kernels and the PCG drivers.
+//
+// Reference iteration (symcomprow::cg_prec, GEFEL/scr.cpp:1093-1205):
+//   p = A d; denom = d.p; alpha = nom/denom; x += alpha d; r -= alpha p;
+//   rr = r.r; h = r/diag; nom' = r.h; beta = nom'/nom; stop on rr/(f.f) < res;
+//   d = beta d + h.
+// Here one iteration is three kernels:
+//   K_A  spmv + d.p  (last block: alpha, breakdown test)
+//   K_B  x,r update, h = r/diag, r.r and r.h (last block: beta, stop test)
+//   K_C  d = beta d + h
+// Reductions are deterministic: every block writes one partial, the last block
+// to arrive (atomic ticket, no waiting) sums the partials in block order.
+// G iterations are captured in one CUDA graph; every kernel returns at once
+// when the device-side state says the iteration has stopped, so a graph
+// launched past convergence costs only empty launches.
+//
+// The mixed form iterates CG in FP32 on the Jacobi-scaled matrix
+// S K S (S = diag^-1/2, unit diagonal), accumulating the solution correction
+// in FP32 and folding it into the FP64 solution at "reliable updates"
+// (van der Vorst & Ye, SIAM J. Sci. Comput. 22, 2000): whenever the iterated
+// residual has dropped by a factor delta, or predicts convergence, the true
+// residual f - K x is recomputed with the FP64 matrix and replaces the
+// iterated one.  Those FP64 steps (x update, residual, their norms) are the
+// only ones whose stability needs FP64.
+#include <cfloat>
+#include <cmath>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "sgpu_internal.cuh"
+
+namespace sgpu {
+
+// ---------------------------------------------------------------------------
+// device-side solver state
+// ---------------------------------------------------------------------------
+struct PcgState {
+  // configuration
+  int64_t ni;
+  double res, zero, tol2, delta2;
+  int crit, prec;
+  // FP64 iteration scalars
+  double nory, nom, denom, alpha, beta, rr;
+  // mixed iteration scalars
+  double ff, rho, rho_prev, rr_ref, kappa2, true_rr, true_rel;
+  double sigma;  // scale of the FP32 residual: the first one has unit norm
+  int64_t it, it_last_update, refinements;
+  // outputs in the reference's conventions
+  int64_t ani;
+  double ares;
+  int ani_set;
+  // control
+  int done, pause, status;
+  double last_dot;
+};
+
+namespace {
+
+constexpr int TPB = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// sum over the block; result valid in thread 0
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+  __shared__ double sh[NV][TPB / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) v[q] = warp_sum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) sh[q][wid] = v[q];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      double t = (lane < (int)(blockDim.x >> 5)) ? sh[q][lane] : 0.0;
+      v[q] = warp_sum(t);
+    }
+  }
+}
+
+// Writes the block's NV partial sums, then reports whether this block is the
+// last one to finish.  The last block sums the partials of all blocks in block
+// order into tot[] (deterministic) and resets the ticket.
+template <int NV>
+__device__ __forceinline__ bool reduce_grid(double (&v)[NV], double *partials, unsigned *ticket,
+                                            double (&tot)[NV]) {
+  __shared__ bool am_last;
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) partials[(size_t)q * gridDim.x + blockIdx.x] = v[q];
+    __threadfence();
+    unsigned t = atomicAdd(ticket, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double s[NV];
+#pragma unroll
+  for (int q = 0; q < NV; q++) s[q] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) s[q] += __ldcg(partials + (size_t)q * gridDim.x + b);
+  }
+  block_sum<NV>(s);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) tot[q] = s[q];
+    *ticket = 0u;
+  }
+  return threadIdx.x == 0;
+}
+
+__device__ __forceinline__ bool stopped(const PcgState *st) { return st->done | st->pause; }
+
+// ---------------------------------------------------------------------------
+// epilogues of the SpMV kernels (run by thread 0 of the last block)
+// ---------------------------------------------------------------------------
+struct EpiNone {
+  static constexpr bool kDot = false;
+  static constexpr bool kGate = false;
+  __device__ static void finish(PcgState *, double) {}
+};
+struct EpiDot {  // plain dot x.y into st->last_dot
+  static constexpr bool kDot = true;
+  static constexpr bool kGate = false;
+  __device__ static void finish(PcgState *st, double t) { st->last_dot = t; }
+};
+struct EpiAlpha64 {  // reference: denom = d.p; breakdown test; alpha = nom/denom
+  static constexpr bool kDot = true;
+  static constexpr bool kGate = true;
+  __device__ static void finish(PcgState *st, double denom) {
+    st->denom = denom;
+    if (fabs(denom) < st->zero) {
+      // scr.cpp:1146-1151 (ares = nom, ani = i); cr.cpp:1177-1181 leaves the
+      // loop and then assigns ani = i, ares = nom as well
+      st->ani = st->it;
+      st->ares = st->nom;
+      st->ani_set = 1;
+      if (st->status == 0) st->status = SGPU_BREAKDOWN;
+      st->done = 1;
+      return;
+    }
+    st->alpha = st->nom / denom;
+  }
+};
+struct EpiAlpha32 {  // mixed: alpha = rho / (p.q)
+  static constexpr bool kDot = true;
+  static constexpr bool kGate = true;
+  __device__ static void finish(PcgState *st, double pq) {
+    st->denom = pq;
+    if (!(pq > 0.0)) {  // S K S is SPD: a non-positive (or NaN) p.q is a breakdown
+      st->status = SGPU_BREAKDOWN;
+      st->done = 1;
+      return;
+    }
+    st->alpha = st->rho / pq;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// SpMV: CSR, L lanes per row; the row loop is uniform per warp so that every
+// lane takes part in the shuffles
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T *p) { return __ldcs(p); }
+
+template <typename AccT, int L>
+__device__ __forceinline__ AccT group_sum(AccT s) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, L);
+  return s;
+}
+
+template <typename VT, typename XT, typename AccT, int L, class Epi>
+__global__ void __launch_bounds__(TPB) k_spmv_csr(int n, const int *__restrict__ rowptr,
+                                                  const int *__restrict__ col, const VT *__restrict__ val,
+                                                  const XT *__restrict__ x, XT *__restrict__ y,
+                                                  PcgState *st, double *partials, unsigned *ticket) {
+  if (Epi::kGate && stopped(st)) return;
+  constexpr int GPW = 32 / L;  // rows per warp step
+  const int lane = threadIdx.x & 31;
+  const int g = lane / L, sub = lane % L;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc = 0.0;
+  for (int base = warp * GPW; base < n; base += nwarps * GPW) {
+    const int i = base + g;
+    int b = 0, e = 0;
+    if (i < n) { b = __ldg(rowptr + i); e = __ldg(rowptr + i + 1); }
+    AccT s = AccT(0);
+#pragma unroll 4
+    for (int k = b + sub; k < e; k += L) s += (AccT)ld_stream(val + k) * (AccT)__ldg(x + ld_stream(col + k));
+    s = group_sum<AccT, L>(s);
+    if (sub == 0 && i < n) {
+      y[i] = (XT)s;
+      if (Epi::kDot) acc += (double)__ldg(x + i) * (double)(XT)s;
+    }
+  }
+  if (Epi::kDot) {
+    double v[1] = {acc}, t[1];
+    if (reduce_grid<1>(v, partials, ticket, t)) Epi::finish(st, t[0]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SpMV: BSR3, one warp per block row, lanes over the row's 3x3 blocks.
+// Values are stored component-major per block row (see sgpu_matrix.cu) so a
+// warp reading one component of consecutive blocks is fully coalesced.
+// ---------------------------------------------------------------------------
+template <typename VT, typename XT, typename AccT, class Epi>
+__global__ void __launch_bounds__(TPB) k_spmv_bsr3(int nb, const int *__restrict__ browptr,
+                                                   const int *__restrict__ bcol, const VT *__restrict__ bval,
+                                                   const XT *__restrict__ x, XT *__restrict__ y,
+                                                   PcgState *st, double *partials, unsigned *ticket) {
+  if (Epi::kGate && stopped(st)) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc = 0.0;
+  for (int br = warp; br < nb; br += nwarps) {
+    const int s = __ldg(browptr + br), e = __ldg(browptr + br + 1), nbr = e - s;
+    const VT *bv = bval + 9ll * s;
+    AccT y0 = 0, y1 = 0, y2 = 0;
+    for (int j = lane; j < nbr; j += 32) {
+      const int c = ld_stream(bcol + s + j);
+      VT v[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) v[q] = ld_stream(bv + q * nbr + j);
+      const AccT x0 = (AccT)__ldg(x + 3 * c), x1 = (AccT)__ldg(x + 3 * c + 1), x2 = (AccT)__ldg(x + 3 * c + 2);
+      y0 += (AccT)v[0] * x0 + (AccT)v[1] * x1 + (AccT)v[2] * x2;
+      y1 += (AccT)v[3] * x0 + (AccT)v[4] * x1 + (AccT)v[5] * x2;
+      y2 += (AccT)v[6] * x0 + (AccT)v[7] * x1 + (AccT)v[8] * x2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+      y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+      y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+    }
+    if (lane < 3) {
+      const AccT yv = lane == 0 ? y0 : (lane == 1 ? y1 : y2);
+      y[3 * br + lane] = (XT)yv;
+      if (Epi::kDot) acc += (double)__ldg(x + 3 * br + lane) * (double)(XT)yv;
+    }
+  }
+  if (Epi::kDot) {
+    double v[1] = {acc}, t[1];
+    if (reduce_grid<1>(v, partials, ticket, t)) Epi::finish(st, t[0]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 PCG vector kernels (the reference iteration)
+// ---------------------------------------------------------------------------
+
+// r = f - p, h = r/diag (or r), d = h; nory = f.f, nom = r.h
+__global__ void __launch_bounds__(TPB) k_pcg64_init(int n, const double *__restrict__ f, const double *__restrict__ p,
+                                                    const double *__restrict__ diag, double *__restrict__ r,
+                                                    double *__restrict__ h, double *__restrict__ d, PcgState *st,
+                                                    double *partials, unsigned *ticket) {
+  const int prec = st->prec;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double fi = f[i];
+    const double ri = fi - p[i];
+    const double hi = prec ? ri / diag[i] : ri;
+    r[i] = ri;
+    h[i] = hi;
+    d[i] = hi;
+    v[0] += fi * fi;
+    v[1] += ri * hi;
+  }
+  double t[2];
+  if (reduce_grid<2>(v, partials, ticket, t)) {
+    st->nory = t[0];
+    st->nom = t[1];
+    st->it = 0;
+    st->done = 0;
+    st->pause = 0;
+    st->status = 0;
+    if (t[0] < st->zero) {
+      // scr.cpp:1117-1120: reported, the iteration continues (and then stops
+      // on the zero denominator); cr.cpp:1160-1164 returns at once
+      st->status = SGPU_ZERO_RHS;
+      st->ares = t[0];
+      st->ani = 0;
+      st->ani_set = 1;
+      if (st->crit == SGPU_CRIT_CR_PREC) st->done = 1;
+    }
+    if (st->ni <= 0) st->done = 1;
+  }
+}
+
+// x += alpha d; r -= alpha p; h = r/diag; rr = r.r; nom' = r.h; stop test
+__global__ void __launch_bounds__(TPB) k_pcg64_update(int n, double *__restrict__ x, double *__restrict__ r,
+                                                      double *__restrict__ h, const double *__restrict__ d,
+                                                      const double *__restrict__ p, const double *__restrict__ diag,
+                                                      PcgState *st, double *partials, unsigned *ticket) {
+  if (stopped(st)) return;
+  const double alpha = st->alpha;
+  const int prec = st->prec;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double di = d[i];
+    x[i] += alpha * di;
+    const double ri = r[i] - alpha * p[i];
+    r[i] = ri;
+    const double hi = prec ? ri / diag[i] : ri;
+    h[i] = hi;
+    v[0] += ri * ri;
+    v[1] += ri * hi;
+  }
+  double t[2];
+  if (reduce_grid<2>(v, partials, ticket, t)) {
+    const double rr = t[0], nom_new = t[1];
+    st->rr = rr;
+    st->beta = nom_new / st->nom;
+    st->nom = nom_new;
+    const int64_t it = st->it;
+    bool conv;
+    if (st->crit == SGPU_CRIT_SCR_PREC) {
+      conv = fabs(rr / st->nory) < st->res;  // scr.cpp:1188
+      if (conv) { st->ani = it; st->ares = nom_new / st->nory; st->ani_set = 1; }
+    } else if (st->crit == SGPU_CRIT_CR_PREC) {
+      conv = sqrt(nom_new / st->nory) < st->res;  // cr.cpp:1217
+      if (conv) { st->ani = it; st->ares = nom_new; st->ani_set = 1; }
+    } else {
+      conv = rr < st->tol2 * st->nory;
+      if (conv) { st->ani = it; st->ares = nom_new / st->nory; st->ani_set = 1; }
+    }
+    st->it = it + 1;
+    if (conv) {
+      st->done = 1;
+    } else if (it + 1 >= st->ni) {
+      st->done = 1;
+      if (st->status == 0) st->status = SGPU_NOT_CONVERGED;
+      if (st->crit == SGPU_CRIT_CR_PREC) { st->ani = st->ni; st->ares = nom_new; st->ani_set = 1; }
+    }
+  }
+}
+
+// d = beta d + h
+__global__ void __launch_bounds__(TPB) k_pcg64_dir(int n, double *__restrict__ d, const double *__restrict__ h,
+                                                   const PcgState *st) {
+  if (stopped(st)) return;
+  const double beta = st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    d[i] = beta * d[i] + h[i];
+}
+
+// ||f - p||^2 and ||f||^2 (true residual after the iteration)
+__global__ void __launch_bounds__(TPB) k_resid_norm(int n, const double *__restrict__ f, const double *__restrict__ p,
+                                                    PcgState *st, double *partials, unsigned *ticket) {
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = f[i] - p[i];
+    v[0] += ri * ri;
+    v[1] += f[i] * f[i];
+  }
+  double t[2];
+  if (reduce_grid<2>(v, partials, ticket, t)) {
+    st->true_rr = t[0];
+    st->ff = t[1];
+    st->true_rel = t[1] > 0.0 ? sqrt(t[0] / t[1]) : sqrt(t[0]);
+  }
+}
+
+__global__ void k_fill(int n, double *__restrict__ a, double v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// mixed-precision kernels
+// ---------------------------------------------------------------------------
+
+// reliable update, part 1: xhat += y / sigma; y = 0; t = S xhat (the unscaled x)
+__global__ void __launch_bounds__(TPB) k_ru_fold(int n, double *__restrict__ xhat, float *__restrict__ y32,
+                                                 const double *__restrict__ dscale, double *__restrict__ t,
+                                                 const PcgState *st) {
+  const double inv_sigma = st->sigma > 0.0 ? 1.0 / st->sigma : 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double xv = xhat[i] + (double)y32[i] * inv_sigma;
+    xhat[i] = xv;
+    y32[i] = 0.0f;
+    t[i] = dscale[i] * xv;
+  }
+}
+
+// reliable update, part 2: r = f - K x (p = K x); r32 = sigma S r;
+// true norms; convergence test on ||r||/||f||.  sigma is fixed at the
+// first update so that the FP32 residual starts with unit norm (far from the
+// FP32 underflow range whatever the units of f).
+__global__ void __launch_bounds__(TPB) k_ru_sigma(int n, const double *__restrict__ f, const double *__restrict__ p,
+                                                  const double *__restrict__ dscale, PcgState *st,
+                                                  double *partials, unsigned *ticket) {
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double rh = dscale[i] * (f[i] - p[i]);
+    v[0] += rh * rh;
+  }
+  double t[1];
+  if (reduce_grid<1>(v, partials, ticket, t)) st->sigma = t[0] > 0.0 ? 1.0 / sqrt(t[0]) : 1.0;
+}
+
+__global__ void __launch_bounds__(TPB) k_ru_resid(int n, const double *__restrict__ f, const double *__restrict__ p,
+                                                  const double *__restrict__ dscale, float *__restrict__ r32,
+                                                  PcgState *st, double *partials, unsigned *ticket) {
+  const double sigma = st->sigma;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double fi = f[i];
+    const double ri = fi - p[i];
+    const float rh = (float)(sigma * dscale[i] * ri);
+    r32[i] = rh;
+    v[0] += ri * ri;
+    v[1] += (double)rh * (double)rh;
+    v[2] += fi * fi;
+  }
+  double t[3];
+  if (reduce_grid<3>(v, partials, ticket, t)) {
+    st->true_rr = t[0];
+    st->ff = t[2];
+    st->true_rel = t[2] > 0.0 ? sqrt(t[0] / t[2]) : sqrt(t[0]);
+    // rho_prev keeps r.r of the iteration before the one that paused (set by
+    // k_cg32_update), so k_ru_dir's beta = rho_true / rho_prev is the CG beta
+    // with the replaced residual
+    st->rho = t[1];
+    st->rr_ref = t[1];
+    st->kappa2 = t[1] > 0.0 ? t[0] / t[1] : 1.0;
+    st->it_last_update = st->it;
+    st->refinements += 1;
+    st->pause = 0;
+    if (t[2] < st->zero) {
+      st->status = SGPU_ZERO_RHS;
+      st->done = 1;
+    } else if (t[0] < st->tol2 * t[2]) {
+      st->done = 1;
+    }
+  }
+}
+
+// after a reliable update: p = r + beta p, beta = rho_true / rho_before
+__global__ void __launch_bounds__(TPB) k_ru_dir(int n, float *__restrict__ p32, const float *__restrict__ r32,
+                                                const PcgState *st, int first) {
+  if (st->done) return;
+  if (first) {  // p = r (p's memory is not initialised: no 0 * p)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p32[i] = r32[i];
+    return;
+  }
+  const float beta = (float)(st->rho / st->rho_prev);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p32[i] = r32[i] + beta * p32[i];
+}
+
+// y += alpha p; r -= alpha q; rho' = r.r; decide on a reliable update
+__global__ void __launch_bounds__(TPB) k_cg32_update(int n, float *__restrict__ y32, float *__restrict__ r32,
+                                                     const float *__restrict__ p32, const float *__restrict__ q32,
+                                                     PcgState *st, double *partials, unsigned *ticket) {
+  if (stopped(st)) return;
+  const float alpha = (float)st->alpha;
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    y32[i] += alpha * p32[i];
+    const float ri = r32[i] - alpha * q32[i];
+    r32[i] = ri;
+    v[0] += (double)ri * (double)ri;
+  }
+  double t[1];
+  if (reduce_grid<1>(v, partials, ticket, t)) {
+    const double rr = t[0];
+    st->rho_prev = st->rho;
+    st->rho = rr;
+    st->beta = rr / st->rho_prev;
+    st->it += 1;
+    const bool dropped = rr < st->delta2 * st->rr_ref;
+    const bool predicts = st->kappa2 * rr < st->tol2 * st->ff;
+    const bool stale = st->it - st->it_last_update >= 256;
+    if (dropped || predicts || stale) st->pause = 1;
+    if (st->it >= st->ni) {
+      st->pause = 1;
+    }
+  }
+}
+
+// p = r + beta p
+__global__ void __launch_bounds__(TPB) k_cg32_dir(int n, float *__restrict__ p32, const float *__restrict__ r32,
+                                                  const PcgState *st) {
+  if (stopped(st)) return;
+  const float beta = (float)st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p32[i] = r32[i] + beta * p32[i];
+}
+
+__global__ void k_x_to_xhat(int n, const double *__restrict__ x, const double *__restrict__ dscale,
+                            double *__restrict__ xhat) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) xhat[i] = x[i] / dscale[i];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int g_vec_blocks = 0, g_spmv_blocks = 0;
+
+int grid_for_vectors() {
+  if (!g_vec_blocks) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg64_update, TPB, 0);
+    g_vec_blocks = kNumSMs * (nb > 0 ? nb : 4);
+  }
+  return g_vec_blocks;
+}
+
+int ensure_work(sgpu_matrix m, bool mixed) {
+  Work &w = m->w;
+  const size_t n = (size_t)m->n;
+  SGPU_TRY(w.r.alloc(n));
+  SGPU_TRY(w.h.alloc(n));
+  SGPU_TRY(w.d.alloc(n));
+  SGPU_TRY(w.p.alloc(n));
+  SGPU_TRY(w.x.alloc(n));
+  SGPU_TRY(w.f.alloc(n));
+  SGPU_TRY(w.t.alloc(n));
+  if (mixed) {
+    SGPU_TRY(w.r32.alloc(n));
+    SGPU_TRY(w.p32.alloc(n));
+    SGPU_TRY(w.q32.alloc(n));
+    SGPU_TRY(w.y32.alloc(n));
+  }
+  if (!w.partials.p) {
+    SGPU_TRY(w.partials.alloc(4 * 8192));
+    SGPU_TRY(w.counters.alloc(16));
+    SGPU_CUDA(cudaMemsetAsync(w.counters.p, 0, 16 * sizeof(unsigned), m->stream));
+    SGPU_TRY(w.scal.alloc(sizeof(PcgState)));
+  }
+  return SGPU_OK;
+}
+
+inline PcgState *state_of(sgpu_matrix m) { return reinterpret_cast<PcgState *>(m->w.scal.p); }
+
+// grid of a grid-stride kernel (all resident blocks), capped so the partials
+// fit; queried once per kernel and cached, so no query runs during capture
+template <class K>
+int occ_grid(K kern, int cap = 8192) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find((const void *)kern);
+  if (it != cache.end()) return it->second;
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TPB, 0);
+  int g = kNumSMs * (nb > 0 ? nb : 4);
+  g = g > cap ? cap : g;
+  cache[(const void *)kern] = g;
+  return g;
+}
+
+// one SpMV launch of the planned kernel, with an epilogue
+template <class Epi>
+int launch_spmv64(sgpu_matrix m, int format, int variant, const double *x, double *y, cudaStream_t s,
+                  int ticket_slot) {
+  PcgState *st = state_of(m);
+  unsigned *tk = m->w.counters.p + ticket_slot;
+  double *part = m->w.partials.p;
+  if (format == 3) {
+    auto k = k_spmv_bsr3<double, double, double, Epi>;
+    k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval.p, x, y, st, part, tk);
+  } else {
+    const Csr &c = m->csr;
+    switch (variant) {
+      case 8: { auto k = k_spmv_csr<double, double, double, 8, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val.p, x, y, st, part, tk); break; }
+      case 16: { auto k = k_spmv_csr<double, double, double, 16, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val.p, x, y, st, part, tk); break; }
+      case 4: { auto k = k_spmv_csr<double, double, double, 4, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val.p, x, y, st, part, tk); break; }
+      default: { auto k = k_spmv_csr<double, double, double, 32, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val.p, x, y, st, part, tk); break; }
+    }
+  }
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+template <class Epi>
+int launch_spmv32(sgpu_matrix m, int format, int variant, const float *x, float *y, cudaStream_t s,
+                  int ticket_slot) {
+  PcgState *st = state_of(m);
+  unsigned *tk = m->w.counters.p + ticket_slot;
+  double *part = m->w.partials.p;
+  if (format == 3) {
+    auto k = k_spmv_bsr3<float, float, float, Epi>;
+    k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval32s.p, x, y, st, part, tk);
+  } else {
+    const Csr &c = m->csr;
+    switch (variant) {
+      case 8: { auto k = k_spmv_csr<float, float, float, 8, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val32s.p, x, y, st, part, tk); break; }
+      case 16: { auto k = k_spmv_csr<float, float, float, 16, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val32s.p, x, y, st, part, tk); break; }
+      case 4: { auto k = k_spmv_csr<float, float, float, 4, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val32s.p, x, y, st, part, tk); break; }
+      default: { auto k = k_spmv_csr<float, float, float, 32, Epi>;
+        k<<<occ_grid(k), TPB, 0, s>>>(c.n, c.rowptr.p, c.col.p, c.val32s.p, x, y, st, part, tk); break; }
+    }
+  }
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+double spmv_bytes(sgpu_matrix m, int format, int precision) {
+  const double sv = precision == 64 ? 8.0 : 4.0;
+  const double n = (double)m->n;
+  if (format == 3)
+    return (double)m->bsr.nblk * (9.0 * sv + 4.0) + (m->bsr.nb + 1.0) * 4.0 + 2.0 * n * sv;
+  return (double)m->csr.nnz * (sv + 4.0) + (n + 1.0) * 4.0 + 2.0 * n * sv;
+}
+
+}  // namespace
+
+// Plain FP64 SpMV with the tuned kernel (public: sgpu_matrix_mxv_d).
+int spmv64(sgpu_matrix m, const double *x, double *y, cudaStream_t s) {
+  SGPU_TRY(ensure_work(m, false));
+  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
+  return launch_spmv64<EpiNone>(m, m->plan64.format, m->plan64.variant, x, y, s, 0);
+}
+
+int spmv32(sgpu_matrix m, const float *x, float *y, cudaStream_t s) {
+  SGPU_TRY(ensure_work(m, true));
+  if (!m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "scaled operator needs a positive diagonal");
+  SGPU_TRY(ensure_fp32(m));
+  if (!m->plan32.tuned) SGPU_TRY(spmv_autotune(m, 32));
+  return launch_spmv32<EpiNone>(m, m->plan32.format, m->plan32.variant, x, y, s, 0);
+}
+
+int spmv_plan(sgpu_matrix m, int precision, double *bytes, int *format, int *variant) {
+  SpmvPlan &p = precision == 64 ? m->plan64 : m->plan32;
+  if (!p.tuned) {
+    SGPU_TRY(ensure_work(m, precision == 32));
+    if (precision == 32) {
+      if (!m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "scaled operator needs a positive diagonal");
+      SGPU_TRY(ensure_fp32(m));
+    }
+    SGPU_TRY(spmv_autotune(m, precision));
+  }
+  if (bytes) *bytes = spmv_bytes(m, p.format, precision);
+  if (format) *format = p.format;
+  if (variant) *variant = p.variant;
+  return SGPU_OK;
+}
+
+// Times every applicable SpMV variant on the handle's matrix (a few
+// repetitions each, CUDA events on the handle's stream) and keeps the fastest.
+int spmv_autotune(sgpu_matrix m, int precision) {
+  SGPU_TRY(ensure_work(m, precision == 32));
+  SGPU_TRY(ensure_bsr3(m));
+  if (precision == 32) SGPU_TRY(ensure_fp32(m));
+  cudaStream_t s = m->stream;
+  struct Cand { int format, variant; };
+  std::vector<Cand> cands = {{0, 4}, {0, 8}, {0, 16}, {0, 32}};
+  if (m->bsr.valid) cands.push_back({3, 0});
+  // x = 1, y scratch
+  const int n = (int)m->n;
+  k_fill<<<grid_for_vectors(), TPB, 0, s>>>(n, m->w.t.p, 1.0);
+  count_launches(1);
+  float best = FLT_MAX;
+  Cand pick = cands[0];
+  const int reps = 5;
+  for (const Cand &c : cands) {
+    float ms = 0.f;
+    for (int rep = 0; rep < reps + 1; rep++) {
+      if (rep == 1) SGPU_CUDA(cudaEventRecord(m->ev0, s));
+      if (precision == 64)
+        SGPU_TRY(launch_spmv64<EpiNone>(m, c.format, c.variant, m->w.t.p, m->w.p.p, s, 0));
+      else
+        SGPU_TRY(launch_spmv32<EpiNone>(m, c.format, c.variant, reinterpret_cast<const float *>(m->w.t.p),
+                                        m->w.q32.p, s, 0));
+    }
+    SGPU_CUDA(cudaEventRecord(m->ev1, s));
+    SGPU_CUDA(cudaEventSynchronize(m->ev1));
+    SGPU_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+    if (ms < best) { best = ms; pick = c; }
+  }
+  SpmvPlan &p = precision == 64 ? m->plan64 : m->plan32;
+  p.format = pick.format;
+  p.variant = pick.variant;
+  p.tuned = true;
+  return SGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the drivers
+// ---------------------------------------------------------------------------
+
+namespace {
+
+int read_state(sgpu_matrix m, PcgState *h) {
+  SGPU_CUDA(cudaMemcpyAsync(h, state_of(m), sizeof(PcgState), cudaMemcpyDeviceToHost, m->stream));
+  SGPU_CUDA(cudaStreamSynchronize(m->stream));
+  return SGPU_OK;
+}
+
+int write_state(sgpu_matrix m, const PcgState *h) {
+  SGPU_CUDA(cudaMemcpyAsync(state_of(m), h, sizeof(PcgState), cudaMemcpyHostToDevice, m->stream));
+  SGPU_CUDA(cudaStreamSynchronize(m->stream));
+  return SGPU_OK;
+}
+
+// Builds a graph of `iters` FP64 iterations (3 kernels each).
+int capture_fp64_chunk(sgpu_matrix m, int iters, cudaGraphExec_t *exec, int64_t *nodes) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int n = (int)m->n;
+  const int vg = grid_for_vectors();
+  PcgState *st = state_of(m);
+  cudaGraph_t g;
+  SGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  for (int it = 0; it < iters; it++) {
+    int rc = launch_spmv64<EpiAlpha64>(m, m->plan64.format, m->plan64.variant, w.d.p, w.p.p, s, 1);
+    if (rc != SGPU_OK) { cudaStreamEndCapture(s, &g); return rc; }
+    k_pcg64_update<<<vg, TPB, 0, s>>>(n, w.x.p, w.r.p, w.h.p, w.d.p, w.p.p, m->csr.diag.p, st, w.partials.p,
+                                      w.counters.p + 2);
+    k_pcg64_dir<<<vg, TPB, 0, s>>>(n, w.d.p, w.h.p, st);
+  }
+  SGPU_CUDA(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  *nodes = 3LL * iters;
+  return SGPU_OK;
+}
+
+int capture_fp32_chunk(sgpu_matrix m, int iters, cudaGraphExec_t *exec, int64_t *nodes) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int n = (int)m->n;
+  const int vg = grid_for_vectors();
+  PcgState *st = state_of(m);
+  cudaGraph_t g;
+  SGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  for (int it = 0; it < iters; it++) {
+    int rc = launch_spmv32<EpiAlpha32>(m, m->plan32.format, m->plan32.variant, w.p32.p, w.q32.p, s, 1);
+    if (rc != SGPU_OK) { cudaStreamEndCapture(s, &g); return rc; }
+    k_cg32_update<<<vg, TPB, 0, s>>>(n, w.y32.p, w.r32.p, w.p32.p, w.q32.p, st, w.partials.p, w.counters.p + 2);
+    k_cg32_dir<<<vg, TPB, 0, s>>>(n, w.p32.p, w.r32.p, st);
+  }
+  SGPU_CUDA(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  *nodes = 3LL * iters;
+  return SGPU_OK;
+}
+
+// true residual of the current w.x against w.f, into st->true_rel
+int true_residual(sgpu_matrix m, const double *x) {
+  cudaStream_t s = m->stream;
+  SGPU_TRY(launch_spmv64<EpiNone>(m, m->plan64.format, m->plan64.variant, x, m->w.p.p, s, 0));
+  k_resid_norm<<<grid_for_vectors(), TPB, 0, s>>>((int)m->n, m->w.f.p, m->w.p.p, state_of(m), m->w.partials.p,
+                                                  m->w.counters.p + 3);
+  count_launches(1);
+  return SGPU_OK;
+}
+
+constexpr int kChunk = 32;
+
+int solve_fp64(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int prec,
+               PcgState *hs) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int n = (int)m->n;
+  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
+  PcgState init{};
+  init.ni = ni;
+  init.res = res;
+  init.zero = zero;
+  init.tol2 = res * res;
+  init.crit = crit;
+  init.prec = prec;
+  SGPU_TRY(write_state(m, &init));
+  // p = A x0 (x0 = 0 when iv == 0, as the reference zeroes x and multiplies)
+  if (iv == 0) SGPU_CUDA(cudaMemsetAsync(w.x.p, 0, (size_t)n * sizeof(double), s));
+  SGPU_TRY(launch_spmv64<EpiNone>(m, m->plan64.format, m->plan64.variant, w.x.p, w.p.p, s, 0));
+  k_pcg64_init<<<grid_for_vectors(), TPB, 0, s>>>(n, w.f.p, w.p.p, m->csr.diag.p, w.r.p, w.h.p, w.d.p,
+                                                  state_of(m), w.partials.p, w.counters.p + 2);
+  count_launches(1);
+  cudaGraphExec_t exec = nullptr;
+  int64_t nodes = 0;
+  SGPU_TRY(capture_fp64_chunk(m, kChunk, &exec, &nodes));
+  int rc = SGPU_OK;
+  for (;;) {
+    cudaError_t e = cudaGraphLaunch(exec, s);
+    if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
+    count_launches(nodes);
+    rc = read_state(m, hs);
+    if (rc != SGPU_OK) break;
+    if (hs->done) break;
+  }
+  cudaGraphExecDestroy(exec);
+  return rc;
+}
+
+int reliable_update(sgpu_matrix m, bool first) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int n = (int)m->n;
+  const int vg = grid_for_vectors();
+  // xhat lives in w.d, the unscaled solution in w.x
+  k_ru_fold<<<vg, TPB, 0, s>>>(n, w.d.p, w.y32.p, m->csr.dscale.p, w.x.p, state_of(m));
+  count_launches(1);
+  SGPU_TRY(launch_spmv64<EpiNone>(m, m->plan64.format, m->plan64.variant, w.x.p, w.p.p, s, 0));
+  if (first) {
+    k_ru_sigma<<<vg, TPB, 0, s>>>(n, w.f.p, w.p.p, m->csr.dscale.p, state_of(m), w.partials.p, w.counters.p + 3);
+    count_launches(1);
+  }
+  k_ru_resid<<<vg, TPB, 0, s>>>(n, w.f.p, w.p.p, m->csr.dscale.p, w.r32.p, state_of(m), w.partials.p,
+                                w.counters.p + 3);
+  count_launches(1);
+  return SGPU_OK;
+}
+
+int solve_mixed(sgpu_matrix m, int64_t ni, double tol, double zero, int64_t iv, PcgState *hs) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int n = (int)m->n;
+  const int vg = grid_for_vectors();
+  if (!m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "mixed mode needs a positive diagonal (Jacobi scaling)");
+  SGPU_TRY(ensure_fp32(m));
+  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
+  if (!m->plan32.tuned) SGPU_TRY(spmv_autotune(m, 32));
+  PcgState init{};
+  init.ni = ni;
+  init.res = tol;
+  init.zero = zero;
+  init.tol2 = tol * tol;
+  init.delta2 = 0.1 * 0.1;
+  init.crit = SGPU_CRIT_TRUE;
+  init.prec = 1;
+  SGPU_TRY(write_state(m, &init));
+  // xhat = x0 / S (x0 = 0 unless iv); y = 0
+  if (iv == 0) {
+    SGPU_CUDA(cudaMemsetAsync(w.d.p, 0, (size_t)n * sizeof(double), s));
+  } else {
+    k_x_to_xhat<<<vg, TPB, 0, s>>>(n, w.x.p, m->csr.dscale.p, w.d.p);
+    count_launches(1);
+  }
+  SGPU_CUDA(cudaMemsetAsync(w.y32.p, 0, (size_t)n * sizeof(float), s));
+  SGPU_TRY(reliable_update(m, true));
+  k_ru_dir<<<vg, TPB, 0, s>>>(n, w.p32.p, w.r32.p, state_of(m), 1);
+  count_launches(1);
+  SGPU_TRY(read_state(m, hs));
+  if (hs->done) return SGPU_OK;
+  cudaGraphExec_t exec = nullptr;
+  int64_t nodes = 0;
+  SGPU_TRY(capture_fp32_chunk(m, kChunk / 2, &exec, &nodes));
+  int rc = SGPU_OK;
+  for (;;) {
+    cudaError_t e = cudaGraphLaunch(exec, s);
+    if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
+    count_launches(nodes);
+    rc = read_state(m, hs);
+    if (rc != SGPU_OK || hs->done) break;
+    if (hs->pause) {
+      rc = reliable_update(m, false);
+      if (rc != SGPU_OK) break;
+      k_ru_dir<<<vg, TPB, 0, s>>>(n, w.p32.p, w.r32.p, state_of(m), 0);
+      count_launches(1);
+      rc = read_state(m, hs);
+      if (rc != SGPU_OK || hs->done) break;
+      if (hs->it >= ni) {
+        PcgState t = *hs;
+        t.status = SGPU_NOT_CONVERGED;
+        t.done = 1;
+        rc = write_state(m, &t);
+        *hs = t;
+        break;
+      }
+    }
+  }
+  cudaGraphExecDestroy(exec);
+  if (rc != SGPU_OK) return rc;
+  // a breakdown inside a chunk leaves a correction in y: fold it in
+  if (!(hs->done && hs->status == 0 && hs->pause == 0)) {
+    PcgState keep = *hs;
+    SGPU_TRY(reliable_update(m, false));
+    SGPU_TRY(read_state(m, hs));
+    hs->status = keep.status;
+    hs->done = 1;
+  }
+  return SGPU_OK;
+}
+
+}  // namespace
+
+// Runs one solve on the handle: w.f holds f, w.x holds x0 (iv = 1) and gets x.
+int pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int prec, int mode,
+            int64_t *ani, double *ares, sgpu_solve_info *info) {
+  cudaStream_t s = m->stream;
+  PcgState hs{};
+  if (prec && !m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "Jacobi preconditioner needs a positive diagonal");
+  SGPU_CUDA(cudaEventRecord(m->ev0, s));
+  int rc;
+  if (mode == SGPU_MIXED) {
+    double tol = (crit == SGPU_CRIT_SCR_PREC) ? sqrt(res) : res;
+    rc = solve_mixed(m, ni, tol, zero, iv, &hs);
+  } else {
+    rc = solve_fp64(m, ni, res, zero, iv, crit, prec, &hs);
+  }
+  SGPU_CUDA(cudaEventRecord(m->ev1, s));
+  if (rc != SGPU_OK) return rc;
+  float solve_ms = 0.f;
+  SGPU_CUDA(cudaEventSynchronize(m->ev1));
+  SGPU_CUDA(cudaEventElapsedTime(&solve_ms, m->ev0, m->ev1));
+  // true FP64 residual of the returned x
+  SGPU_TRY(true_residual(m, m->w.x.p));
+  PcgState fin{};
+  SGPU_TRY(read_state(m, &fin));
+  if (mode == SGPU_MIXED) {
+    if (fin.status == 0 && fin.done) {
+      if (ani) *ani = fin.it;
+      if (ares) *ares = fin.true_rr / (fin.ff > 0 ? fin.ff : 1.0);
+    }
+  } else if (hs.ani_set) {
+    if (ani) *ani = hs.ani;
+    if (ares) *ares = hs.ares;
+  }
+  if (info) {
+    info->iterations = hs.it;
+    info->refinements = mode == SGPU_MIXED ? hs.refinements : 0;
+    info->rh_over_ff = mode == SGPU_MIXED ? fin.true_rr / (fin.ff > 0 ? fin.ff : 1.0)
+                                          : hs.nom / (hs.nory > 0 ? hs.nory : 1.0);
+    if (mode == SGPU_MIXED) info->crit_value = fin.true_rel;
+    else if (crit == SGPU_CRIT_SCR_PREC) info->crit_value = hs.rr / (hs.nory > 0 ? hs.nory : 1.0);
+    else if (crit == SGPU_CRIT_CR_PREC) info->crit_value = sqrt(hs.nom / (hs.nory > 0 ? hs.nory : 1.0));
+    else info->crit_value = sqrt(hs.rr / (hs.nory > 0 ? hs.nory : 1.0));
+    info->true_relres = fin.true_rel;
+    info->solve_ms = solve_ms;
+    const SpmvPlan &pl = mode == SGPU_MIXED ? m->plan32 : m->plan64;
+    info->spmv_format = pl.format;
+    info->spmv_variant = pl.variant;
+    info->spmv_bytes = spmv_bytes(m, pl.format, mode == SGPU_MIXED ? 32 : 64);
+  }
+  return hs.status;
+}
+
+int pcg_prepare(sgpu_matrix m, bool mixed) { return ensure_work(m, mixed); }
+double *work_x(sgpu_matrix m) { return m->w.x.p; }
+double *work_f(sgpu_matrix m) { return m->w.f.p; }
+
+}  // namespace sgpu

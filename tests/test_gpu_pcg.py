@@ -1,0 +1,121 @@
+"""GPU parity of the drop-in solvers against the oracle (CPU restatement of
+GEFEL's CG routines) and the committed golden fixtures."""
+import numpy as np
+import pytest
+
+from ssf_b200 import decks, gefel
+from ssf_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(oracle, nx=20, ny=4, nz=4, sym=True):
+    m = decks.cantilever_hex(nx, ny, nz)
+    adr, ci, a = oracle.assemble(m, sym=sym)
+    f = oracle.load_vector(m)
+    return m, adr, ci, a, f
+
+
+def test_scr_spmv_matches_oracle(oracle, gpu_lib):
+    m, adr, ci, a, f = _system(oracle)
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal(adr.size - 1)
+    ref = oracle.scr_mxv(adr, ci, a, b)
+    got = gefel.symcomprow(adr, ci, a).mxv_scr(b)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def test_cr_spmv_matches_oracle(oracle, gpu_lib):
+    m, adr, ci, a, f = _system(oracle, sym=False)
+    b = np.random.default_rng(1).standard_normal(adr.size - 1)
+    ref = oracle.cr_mxv(adr, ci, a, b)
+    got = gefel.comprow(adr, ci, a).mxv_cr(b)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def test_scr_cg_prec_fp64_parity(oracle, gpu_lib):
+    m, adr, ci, a, f = _system(oracle)
+    xo, st, ani_o, ares_o = oracle.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert st == 0
+    x = np.zeros_like(f)
+    r = gefel.symcomprow(adr, ci, a).cg_prec(x, f, 20000, 1e-20)
+    assert r.status == L.OK
+    # same iteration within rounding of the dot products
+    assert abs(r.ani - ani_o) <= 2
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+    assert r.info["true_relres"] < 1e-9
+
+
+def test_scr_cg_prec_mixed_parity(oracle, gpu_lib):
+    m, adr, ci, a, f = _system(oracle)
+    xo, st, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-24)
+    x = np.zeros_like(f)
+    r = gefel.symcomprow(adr, ci, a).cg_prec(x, f, 20000, 1e-20, mode="mixed")
+    assert r.status == L.OK
+    assert r.info["true_relres"] < 1e-10
+    # solution error against a tight FP64 oracle solve: the refined mixed form
+    # reaches the same relative residual, so its error is bounded alike
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-7
+    assert r.info["refinements"] >= 2
+
+
+def test_cr_cg_noprec_parity(oracle, gpu_lib):
+    m, adr, ci, a, f = _system(oracle, nx=10, ny=2, nz=2, sym=False)
+    xo, st, ani_o, ares_o = oracle.cr_cg_prec(adr, ci, a, f, ni=20000, res=1e-10)
+    assert st == 0
+    x = np.zeros_like(f)
+    r = gefel.comprow(adr, ci, a).cg_prec(x, f, 20000, 1e-10)
+    assert r.status == L.OK
+    assert abs(r.ani - ani_o) <= 2
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_hex8_assembly_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex(6, 3, 2)
+    # distort the nodes so every element differs
+    rng = np.random.default_rng(3)
+    m.coords = m.coords + rng.uniform(-0.01, 0.01, m.coords.shape)
+    m.emat = np.arange(m.ne) % 2
+    m.mats = np.array([[210e9, 0.3], [70e9, 0.25]])
+    adr, ci, a = oracle.assemble(m, sym=True)
+    with mefel.stiffness_matrix(m) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+    assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+def test_quad4_assembly_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    m = decks.plate_quad(7, 5, E=3e10, nu=0.22)
+    rng = np.random.default_rng(4)
+    m.coords[:, :2] += rng.uniform(-0.1, 0.1, (m.nn, 2))
+    adr, ci, a = oracle.assemble(m, sym=True)
+    with mefel.stiffness_matrix(m) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+    assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+def test_hex8t_assembly_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    m = decks.heat_cube(4)
+    rng = np.random.default_rng(5)
+    m.coords = m.coords + rng.uniform(-0.02, 0.02, m.coords.shape)
+    for kind, fn in (("hex8t_k", mefel.conductivity_matrix), ("hex8t_c", mefel.capacity_matrix)):
+        adr, ci, a = oracle.assemble(m, sym=True, kind=kind)
+        with fn(m) as K:
+            g_adr, g_ci, g_a = K.download(symmetric=1)
+        assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+        assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+def test_linear_statics_end_to_end(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex(20, 4, 4)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    f = oracle.load_vector(m)
+    xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    X, res = mefel.solve_linear_statics(m, res=1e-20)
+    assert res[0].status == L.OK
+    assert np.linalg.norm(X[0] - xo) / np.linalg.norm(xo) <= 1e-8
