@@ -71,6 +71,8 @@ typedef struct {
   double spmv_bytes;        /* algorithmic bytes of one SpMV of the iteration's format */
   int32_t spmv_format;      /* 0 = CSR, 3 = 3x3 block rows (BSR3) */
   int32_t spmv_variant;     /* autotuned kernel variant id */
+  int32_t fallback;         /* MIXED: 1 if the FP32 iteration stagnated and the
+                               solve was finished in FP64 from its iterate */
 } sgpu_solve_info;
 
 /* ------------------------------------------------------------------------ */
@@ -139,6 +141,11 @@ SGPU_API int sgpu_matrix_mxv32_d(sgpu_matrix m, const float *x_d, float *y_d);
  * the format id (0 CSR, 3 BSR3) and the kernel variant; tunes if needed. */
 SGPU_API int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *bytes, int32_t *format,
                                    int32_t *variant);
+
+/* Override the autotuner: use SpMV `format` (0 CSR, 3 BSR3) and `variant`
+ * (CSR: lanes per row 4/8/16/32) for `precision` (64 or 32).  For tests and
+ * tuning studies; BAD_INPUT if the format is not available for the matrix. */
+SGPU_API int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32_t variant);
 
 /* Jacobi-PCG on a device-resident matrix, host vectors.  crit selects the
  * reference routine whose criterion is kept. */

@@ -33,6 +33,7 @@ class SolveInfo(C.Structure):
         ("spmv_bytes", C.c_double),
         ("spmv_format", C.c_int32),
         ("spmv_variant", C.c_int32),
+        ("fallback", C.c_int32),
     ]
 
     def as_dict(self):
@@ -102,6 +103,7 @@ SIGNATURES = {
     "sgpu_matrix_set_stream": ([_vp, _vp], C.c_int),
     "sgpu_matrix_mxv32_d": ([_vp, _vp, _vp], C.c_int),
     "sgpu_matrix_spmv_plan": ([_vp, _i32, C.POINTER(_dbl), C.POINTER(_i32), C.POINTER(_i32)], C.c_int),
+    "sgpu_matrix_set_spmv": ([_vp, _i32, _i32, _i32], C.c_int),
     "sgpu_assemble": ([C.POINTER(Mesh), C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_reassemble": ([_vp, _i32, _vp, _vp, C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_last_error": ([], C.c_char_p),

@@ -211,6 +211,26 @@ int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *bytes, int32
   return SGPU_OK;
 }
 
+int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32_t variant) {
+  if (!m) return fail(SGPU_BAD_INPUT, "null handle");
+  if (precision != 64 && precision != 32) return fail(SGPU_BAD_INPUT, "precision must be 64 or 32");
+  if (format != 0 && format != 3) return fail(SGPU_BAD_INPUT, "format must be 0 (CSR) or 3 (BSR3)");
+  if (format == 0 && variant != 4 && variant != 8 && variant != 16 && variant != 32)
+    return fail(SGPU_BAD_INPUT, "CSR variant must be 4, 8, 16 or 32 lanes per row");
+  SGPU_TRY(pcg_prepare(m, precision == 32));
+  if (precision == 32) {
+    if (!m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "scaled operator needs a positive diagonal");
+    SGPU_TRY(ensure_fp32(m));
+  }
+  SGPU_TRY(ensure_bsr3(m));
+  if (format == 3 && !m->bsr.valid) return fail(SGPU_BAD_INPUT, "matrix has no 3x3 block-row form");
+  SpmvPlan &p = precision == 64 ? m->plan64 : m->plan32;
+  p.format = format;
+  p.variant = variant;
+  p.tuned = true;
+  return SGPU_OK;
+}
+
 int sgpu_matrix_pcg(sgpu_matrix m, double *x, const double *f, int64_t ni, double res, double zero, int64_t iv,
                     int32_t crit, int32_t prec, int32_t mode, int64_t *ani, double *ares, sgpu_solve_info *info) {
   if (!m) return fail(SGPU_BAD_INPUT, "null handle");

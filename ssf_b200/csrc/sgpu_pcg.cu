@@ -324,6 +324,7 @@ __global__ void __launch_bounds__(TPB) k_pcg64_update(int n, double *__restrict_
   if (reduce_grid<2>(v, partials, ticket, t)) {
     const double rr = t[0], nom_new = t[1];
     st->rr = rr;
+    st->rho_prev = st->nom;
     st->beta = nom_new / st->nom;
     st->nom = nom_new;
     const int64_t it = st->it;
@@ -339,7 +340,9 @@ __global__ void __launch_bounds__(TPB) k_pcg64_update(int n, double *__restrict_
       if (conv) { st->ani = it; st->ares = nom_new / st->nory; st->ani_set = 1; }
     }
     st->it = it + 1;
-    if (conv) {
+    if (conv && st->crit == SGPU_CRIT_TRUE) {
+      st->pause = 1;  // the host confirms on the true residual (k_pcg64_confirm)
+    } else if (conv) {
       st->done = 1;
     } else if (it + 1 >= st->ni) {
       st->done = 1;
@@ -356,6 +359,44 @@ __global__ void __launch_bounds__(TPB) k_pcg64_dir(int n, double *__restrict__ d
   const double beta = st->beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     d[i] = beta * d[i] + h[i];
+}
+
+// SGPU_CRIT_TRUE: after the iterated residual met the threshold, p = K x.
+// Stop if the true residual meets it too; otherwise replace r by the true
+// residual (h, r.h with it) and go on: beta = (r.h)_true / (r.h)_previous.
+__global__ void __launch_bounds__(TPB) k_pcg64_confirm(int n, const double *__restrict__ f,
+                                                       const double *__restrict__ p, const double *__restrict__ diag,
+                                                       double *__restrict__ r, double *__restrict__ h, PcgState *st,
+                                                       double *partials, unsigned *ticket) {
+  const int prec = st->prec;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = f[i] - p[i];
+    const double hi = prec ? ri / diag[i] : ri;
+    r[i] = ri;
+    h[i] = hi;
+    v[0] += ri * ri;
+    v[1] += ri * hi;
+  }
+  double t[2];
+  if (reduce_grid<2>(v, partials, ticket, t)) {
+    st->refinements += 1;
+    st->true_rr = t[0];
+    st->rr = t[0];
+    if (t[0] < st->tol2 * st->nory) {
+      st->done = 1;
+      st->ares = t[1] / st->nory;
+    } else {
+      st->beta = t[1] / st->rho_prev;
+      st->nom = t[1];
+      st->pause = 0;
+      st->ani_set = 0;
+      if (st->it >= st->ni) {
+        st->done = 1;
+        if (st->status == 0) st->status = SGPU_NOT_CONVERGED;
+      }
+    }
+  }
 }
 
 // ||f - p||^2 and ||f||^2 (true residual after the iteration)
@@ -799,6 +840,7 @@ int solve_fp64(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, i
   int64_t nodes = 0;
   SGPU_TRY(capture_fp64_chunk(m, kChunk, &exec, &nodes));
   int rc = SGPU_OK;
+  std::vector<double> confirms;
   for (;;) {
     cudaError_t e = cudaGraphLaunch(exec, s);
     if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
@@ -806,6 +848,31 @@ int solve_fp64(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, i
     rc = read_state(m, hs);
     if (rc != SGPU_OK) break;
     if (hs->done) break;
+    if (hs->pause) {  // SGPU_CRIT_TRUE: confirm on the true residual
+      rc = launch_spmv64<EpiNone>(m, m->plan64.format, m->plan64.variant, w.x.p, w.p.p, s, 0);
+      if (rc != SGPU_OK) break;
+      k_pcg64_confirm<<<grid_for_vectors(), TPB, 0, s>>>(n, w.f.p, w.p.p, m->csr.diag.p, w.r.p, w.h.p,
+                                                         state_of(m), w.partials.p, w.counters.p + 2);
+      count_launches(1);
+      rc = read_state(m, hs);
+      if (rc != SGPU_OK || hs->done) break;
+      // The true residual of an FP64 iterate cannot fall below the rounding
+      // floor of f - K x itself (about 2^-53 ||K|| ||x|| / ||f||).  When
+      // replacing the residual stops paying (no halving over three
+      // confirmations), the iterate is as good as FP64 holds: stop there.
+      confirms.push_back(hs->true_rr);
+      const size_t k = confirms.size();
+      if (k > 3 && confirms[k - 1] > 0.25 * confirms[k - 4]) {
+        PcgState t = *hs;
+        t.done = 1;
+        t.ares = t.nom / t.nory;
+        rc = write_state(m, &t);
+        *hs = t;
+        break;
+      }
+      k_pcg64_dir<<<grid_for_vectors(), TPB, 0, s>>>(n, w.d.p, w.h.p, state_of(m));
+      count_launches(1);
+    }
   }
   cudaGraphExecDestroy(exec);
   return rc;
@@ -829,6 +896,8 @@ int reliable_update(sgpu_matrix m, bool first) {
   count_launches(1);
   return SGPU_OK;
 }
+
+constexpr int kFallback = 1000;  // solve_mixed: continue in FP64
 
 int solve_mixed(sgpu_matrix m, int64_t ni, double tol, double zero, int64_t iv, PcgState *hs) {
   cudaStream_t s = m->stream;
@@ -865,6 +934,11 @@ int solve_mixed(sgpu_matrix m, int64_t ni, double tol, double zero, int64_t iv, 
   int64_t nodes = 0;
   SGPU_TRY(capture_fp32_chunk(m, kChunk / 2, &exec, &nodes));
   int rc = SGPU_OK;
+  // true relative residual at every reliable update: when the FP32 iteration
+  // stops making progress (the FP32 operator's error dominates, which happens
+  // when cond(S K S) * 2^-24 is not small), the solve falls back to FP64
+  std::vector<double> hist{hs->true_rel};
+  bool stagnated = false;
   for (;;) {
     cudaError_t e = cudaGraphLaunch(exec, s);
     if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
@@ -878,6 +952,12 @@ int solve_mixed(sgpu_matrix m, int64_t ni, double tol, double zero, int64_t iv, 
       count_launches(1);
       rc = read_state(m, hs);
       if (rc != SGPU_OK || hs->done) break;
+      hist.push_back(hs->true_rel);
+      const size_t k = hist.size();
+      if (!std::isfinite(hs->true_rel) || (k > 4 && hist[k - 1] > 0.5 * hist[k - 4])) {
+        stagnated = true;
+        break;
+      }
       if (hs->it >= ni) {
         PcgState t = *hs;
         t.status = SGPU_NOT_CONVERGED;
@@ -890,6 +970,7 @@ int solve_mixed(sgpu_matrix m, int64_t ni, double tol, double zero, int64_t iv, 
   }
   cudaGraphExecDestroy(exec);
   if (rc != SGPU_OK) return rc;
+  if (stagnated) return kFallback;
   // a breakdown inside a chunk leaves a correction in y: fold it in
   if (!(hs->done && hs->status == 0 && hs->pause == 0)) {
     PcgState keep = *hs;
@@ -911,9 +992,20 @@ int pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int 
   if (prec && !m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "Jacobi preconditioner needs a positive diagonal");
   SGPU_CUDA(cudaEventRecord(m->ev0, s));
   int rc;
+  int fallback = 0;
+  int64_t mixed_its = 0, mixed_refs = 0;
   if (mode == SGPU_MIXED) {
     double tol = (crit == SGPU_CRIT_SCR_PREC) ? sqrt(res) : res;
     rc = solve_mixed(m, ni, tol, zero, iv, &hs);
+    if (rc == kFallback) {
+      // FP64 from the current solution (w.x is up to date after a reliable update)
+      fallback = 1;
+      mixed_its = hs.it;
+      mixed_refs = hs.refinements;
+      rc = solve_fp64(m, ni > hs.it ? ni - hs.it : 1, tol * tol, zero, 1, SGPU_CRIT_SCR_PREC, 1, &hs);
+      hs.it += mixed_its;
+      hs.refinements += mixed_refs;
+    }
   } else {
     rc = solve_fp64(m, ni, res, zero, iv, crit, prec, &hs);
   }
@@ -928,7 +1020,7 @@ int pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int 
   SGPU_TRY(read_state(m, &fin));
   if (mode == SGPU_MIXED) {
     if (fin.status == 0 && fin.done) {
-      if (ani) *ani = fin.it;
+      if (ani) *ani = hs.it;
       if (ares) *ares = fin.true_rr / (fin.ff > 0 ? fin.ff : 1.0);
     }
   } else if (hs.ani_set) {
@@ -950,6 +1042,7 @@ int pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int 
     info->spmv_format = pl.format;
     info->spmv_variant = pl.variant;
     info->spmv_bytes = spmv_bytes(m, pl.format, mode == SGPU_MIXED ? 32 : 64);
+    info->fallback = fallback;
   }
   return hs.status;
 }

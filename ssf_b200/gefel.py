@@ -164,6 +164,15 @@ class DeviceMatrix:
     def update_values(self, a):
         L.check(L.lib().sgpu_matrix_update_values(self.h, _f64(a)))
 
+    def set_spmv(self, precision, fmt, variant=0):
+        """Pin the SpMV kernel (format 0 CSR / 3 BSR3, CSR lanes per row)."""
+        L.check(L.lib().sgpu_matrix_set_spmv(self.h, int(precision), int(fmt), int(variant)))
+
+    def spmv_plan(self, precision):
+        b, f, v = C.c_double(), C.c_int32(), C.c_int32()
+        L.check(L.lib().sgpu_matrix_spmv_plan(self.h, int(precision), C.byref(b), C.byref(f), C.byref(v)))
+        return {"bytes": b.value, "format": f.value, "variant": v.value}
+
     def mxv(self, b):
         y = np.zeros(self.n)
         L.check(L.lib().sgpu_matrix_mxv(self.h, _f64(b), y))

@@ -119,3 +119,35 @@ def test_linear_statics_end_to_end(oracle, gpu_lib):
     X, res = mefel.solve_linear_statics(m, res=1e-20)
     assert res[0].status == L.OK
     assert np.linalg.norm(X[0] - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+@pytest.mark.parametrize("fmt,variant", [(0, 4), (0, 8), (0, 16), (0, 32), (3, 0)])
+def test_every_spmv_kernel_fp64(oracle, gpu_lib, fmt, variant):
+    m, adr, ci, a, f = _system(oracle, nx=12, ny=3, nz=3)
+    b = np.random.default_rng(7).standard_normal(adr.size - 1)
+    ref = oracle.scr_mxv(adr, ci, a, b)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as d:
+        d.set_spmv(64, fmt, variant)
+        got = d.mxv(b)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("fmt,variant", [(0, 4), (0, 8), (0, 16), (0, 32), (3, 0)])
+def test_every_spmv_kernel_fp32_scaled(oracle, gpu_lib, fmt, variant):
+    import ctypes
+    import torch
+    m, adr, ci, a, f = _system(oracle, nx=12, ny=3, nz=3)
+    K = oracle.scr_to_dense(adr, ci, a)
+    s = 1.0 / np.sqrt(np.diag(K))
+    Ah = K * s[:, None] * s[None, :]
+    b = np.random.default_rng(8).standard_normal(K.shape[0]).astype(np.float32)
+    ref = Ah @ b.astype(np.float64)
+    xd = torch.from_numpy(b).cuda()
+    yd = torch.empty_like(xd)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as d:
+        d.set_spmv(32, fmt, variant)
+        L.check(L.lib().sgpu_matrix_mxv32_d(d.h, ctypes.c_void_p(xd.data_ptr()), ctypes.c_void_p(yd.data_ptr())))
+        torch.cuda.synchronize()
+    got = yd.cpu().numpy().astype(np.float64)
+    # FP32 values and accumulation: a few ulps of the row's magnitude
+    assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
