@@ -23,6 +23,8 @@
 // iterated one.  Those FP64 steps (x update, residual, their norms) are the
 // only ones whose stability needs FP64.
 #include <cfloat>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <mutex>
 #include <unordered_map>
@@ -722,11 +724,12 @@ int spmv_autotune(sgpu_matrix m, int precision) {
     float ms = 0.f;
     for (int rep = 0; rep < reps + 1; rep++) {
       if (rep == 1) SGPU_CUDA(cudaEventRecord(m->ev0, s));
+      // with the dot-product epilogue of the iteration's SpMV
       if (precision == 64)
-        SGPU_TRY(launch_spmv64<EpiNone>(m, c.format, c.variant, m->w.t.p, m->w.p.p, s, 0));
+        SGPU_TRY(launch_spmv64<EpiDot>(m, c.format, c.variant, m->w.t.p, m->w.p.p, s, 4));
       else
-        SGPU_TRY(launch_spmv32<EpiNone>(m, c.format, c.variant, reinterpret_cast<const float *>(m->w.t.p),
-                                        m->w.q32.p, s, 0));
+        SGPU_TRY(launch_spmv32<EpiDot>(m, c.format, c.variant, reinterpret_cast<const float *>(m->w.t.p),
+                                       m->w.q32.p, s, 4));
     }
     SGPU_CUDA(cudaEventRecord(m->ev1, s));
     SGPU_CUDA(cudaEventSynchronize(m->ev1));
@@ -737,6 +740,16 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   p.format = pick.format;
   p.variant = pick.variant;
   p.tuned = true;
+  // SGPU_SPMV64 / SGPU_SPMV32 = "<format>:<variant>" pins the choice (profiling
+  // runs need the same kernel as the timed run, whatever the timings say)
+  const char *pin = getenv(precision == 64 ? "SGPU_SPMV64" : "SGPU_SPMV32");
+  if (pin) {
+    int f = -1, v = 0;
+    if (sscanf(pin, "%d:%d", &f, &v) >= 1) {
+      for (const Cand &c : cands)
+        if (c.format == f && (f == 3 || c.variant == v)) { p.format = f; p.variant = c.variant; }
+    }
+  }
   return SGPU_OK;
 }
 
