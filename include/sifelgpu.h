@@ -206,6 +206,30 @@ SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, co
                              sgpu_assembly_info *info);
 
 /* ------------------------------------------------------------------------ */
+/* Solving without allocating device memory                                 */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference: an addition for callers that cannot
+ * allocate GPU memory while they solve (an application that owns the whole
+ * device memory pool through its own allocator, or one that must not call
+ * cudaMalloc/cudaFree because they synchronise the device).  Jacobi-PCG with
+ * the criterion of symcomprow::cg_prec on a caller-owned device CSR (full
+ * rows, int32 indices, sorted columns, diagonal present): rowptr_d[n+1],
+ * col_d/val_d[rowptr_d[n]], f_d[n] read, x_d[n] in/out (start vector when
+ * iv = 1), all device pointers, work enqueued on `stream` (NULL = legacy
+ * default stream).  The work vectors live in one static device array of the
+ * library (about 5 MiB, held by every GPU that loads it until exit), so
+ * n <= 131072 (BAD_INPUT beyond).  Nothing is allocated.  Every call uses the
+ * same array: calls that overlap on the GPU race and must be serialised.  The
+ * first call on each device looks up the array's device address; make it
+ * before any stream capture.  *ani/*ares as in sgpu_scr_cg_prec (written only
+ * on convergence); *iterations (may be NULL) gets the iterations done. */
+SGPU_API int sgpu_csr_pcg_noalloc_d(int32_t n, const int32_t *rowptr_d, const int32_t *col_d,
+                                    const double *val_d, const double *f_d, double *x_d, int64_t ni,
+                                    double res, double zero, int64_t iv, void *stream, int64_t *ani,
+                                    double *ares, int64_t *iterations);
+
+/* ------------------------------------------------------------------------ */
 /* Library state                                                            */
 /* ------------------------------------------------------------------------ */
 
