@@ -143,7 +143,8 @@ SGPU_API int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *byt
                                    int32_t *variant);
 
 /* Override the autotuner: use SpMV `format` (0 CSR, 3 BSR3) and `variant`
- * (CSR: lanes per row 4/8/16/32) for `precision` (64 or 32).  For tests and
+ * (lanes per row: 4/8/16/32 for CSR, 8/16/32 for BSR3) for `precision`
+ * (64 or 32).  For tests and
  * tuning studies; BAD_INPUT if the format is not available for the matrix. */
 SGPU_API int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32_t variant);
 

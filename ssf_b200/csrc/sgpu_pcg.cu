@@ -219,21 +219,43 @@ __global__ void __launch_bounds__(TPB) k_spmv_csr(int n, const int *__restrict__
 // Values are stored component-major per block row (see sgpu_matrix.cu) so a
 // warp reading one component of consecutive blocks is fully coalesced.
 // ---------------------------------------------------------------------------
-template <typename VT, typename XT, typename AccT, class Epi>
+template <typename VT, typename XT, typename AccT, int LPR, class Epi>
 __global__ void __launch_bounds__(TPB) k_spmv_bsr3(int nb, const int *__restrict__ browptr,
                                                    const int *__restrict__ bcol, const VT *__restrict__ bval,
                                                    const XT *__restrict__ x, XT *__restrict__ y,
                                                    PcgState *st, double *partials, unsigned *ticket) {
+  // LPR lanes per block row (32, 16 or 8): 32/LPR block rows per warp step;
+  // each lane takes blocks sub, sub+LPR, ... of its row, two at a time so
+  // that the loads of two blocks are in flight together
   if (Epi::kGate && stopped(st)) return;
-  const int lane = threadIdx.x & 31;
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, g = lane / LPR, sub = lane % LPR;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double acc = 0.0;
-  for (int br = warp; br < nb; br += nwarps) {
-    const int s = __ldg(browptr + br), e = __ldg(browptr + br + 1), nbr = e - s;
+  for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
+    const int br = base + g;
+    int s = 0, nbr = 0;
+    if (br < nb) { s = __ldg(browptr + br); nbr = __ldg(browptr + br + 1) - s; }
     const VT *bv = bval + 9ll * s;
     AccT y0 = 0, y1 = 0, y2 = 0;
-    for (int j = lane; j < nbr; j += 32) {
+    int j = sub;
+    for (; j + LPR < nbr; j += 2 * LPR) {
+      const int j2 = j + LPR;
+      const int c = ld_stream(bcol + s + j), c2 = ld_stream(bcol + s + j2);
+      VT v[9], w[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) { v[q] = ld_stream(bv + q * nbr + j); w[q] = ld_stream(bv + q * nbr + j2); }
+      const AccT x0 = (AccT)__ldg(x + 3 * c), x1 = (AccT)__ldg(x + 3 * c + 1), x2 = (AccT)__ldg(x + 3 * c + 2);
+      const AccT z0 = (AccT)__ldg(x + 3 * c2), z1 = (AccT)__ldg(x + 3 * c2 + 1), z2 = (AccT)__ldg(x + 3 * c2 + 2);
+      y0 += (AccT)v[0] * x0 + (AccT)v[1] * x1 + (AccT)v[2] * x2;
+      y1 += (AccT)v[3] * x0 + (AccT)v[4] * x1 + (AccT)v[5] * x2;
+      y2 += (AccT)v[6] * x0 + (AccT)v[7] * x1 + (AccT)v[8] * x2;
+      y0 += (AccT)w[0] * z0 + (AccT)w[1] * z1 + (AccT)w[2] * z2;
+      y1 += (AccT)w[3] * z0 + (AccT)w[4] * z1 + (AccT)w[5] * z2;
+      y2 += (AccT)w[6] * z0 + (AccT)w[7] * z1 + (AccT)w[8] * z2;
+    }
+    if (j < nbr) {
       const int c = ld_stream(bcol + s + j);
       VT v[9];
 #pragma unroll
@@ -244,15 +266,15 @@ __global__ void __launch_bounds__(TPB) k_spmv_bsr3(int nb, const int *__restrict
       y2 += (AccT)v[6] * x0 + (AccT)v[7] * x1 + (AccT)v[8] * x2;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      y0 += __shfl_xor_sync(0xffffffffu, y0, o);
-      y1 += __shfl_xor_sync(0xffffffffu, y1, o);
-      y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      y0 += __shfl_xor_sync(0xffffffffu, y0, o, LPR);
+      y1 += __shfl_xor_sync(0xffffffffu, y1, o, LPR);
+      y2 += __shfl_xor_sync(0xffffffffu, y2, o, LPR);
     }
-    if (lane < 3) {
-      const AccT yv = lane == 0 ? y0 : (lane == 1 ? y1 : y2);
-      y[3 * br + lane] = (XT)yv;
-      if (Epi::kDot) acc += (double)__ldg(x + 3 * br + lane) * (double)(XT)yv;
+    if (sub < 3 && br < nb) {
+      const AccT yv = sub == 0 ? y0 : (sub == 1 ? y1 : y2);
+      y[3 * br + sub] = (XT)yv;
+      if (Epi::kDot) acc += (double)__ldg(x + 3 * br + sub) * (double)(XT)yv;
     }
   }
   if (Epi::kDot) {
@@ -615,7 +637,9 @@ int launch_spmv64(sgpu_matrix m, int format, int variant, const double *x, doubl
   unsigned *tk = m->w.counters.p + ticket_slot;
   double *part = m->w.partials.p;
   if (format == 3) {
-    auto k = k_spmv_bsr3<double, double, double, Epi>;
+    auto k = variant == 8    ? k_spmv_bsr3<double, double, double, 8, Epi>
+             : variant == 16 ? k_spmv_bsr3<double, double, double, 16, Epi>
+                             : k_spmv_bsr3<double, double, double, 32, Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval.p, x, y, st, part, tk);
   } else {
     const Csr &c = m->csr;
@@ -642,7 +666,9 @@ int launch_spmv32(sgpu_matrix m, int format, int variant, const float *x, float 
   unsigned *tk = m->w.counters.p + ticket_slot;
   double *part = m->w.partials.p;
   if (format == 3) {
-    auto k = k_spmv_bsr3<float, float, float, Epi>;
+    auto k = variant == 8    ? k_spmv_bsr3<float, float, float, 8, Epi>
+             : variant == 16 ? k_spmv_bsr3<float, float, float, 16, Epi>
+                             : k_spmv_bsr3<float, float, float, 32, Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval32s.p, x, y, st, part, tk);
   } else {
     const Csr &c = m->csr;
@@ -712,7 +738,11 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   cudaStream_t s = m->stream;
   struct Cand { int format, variant; };
   std::vector<Cand> cands = {{0, 4}, {0, 8}, {0, 16}, {0, 32}};
-  if (m->bsr.valid) cands.push_back({3, 0});
+  if (m->bsr.valid) {
+    cands.push_back({3, 32});
+    cands.push_back({3, 16});
+    cands.push_back({3, 8});
+  }
   // x = 1, y scratch
   const int n = (int)m->n;
   k_fill<<<grid_for_vectors(), TPB, 0, s>>>(n, m->w.t.p, 1.0);
@@ -747,7 +777,7 @@ int spmv_autotune(sgpu_matrix m, int precision) {
     int f = -1, v = 0;
     if (sscanf(pin, "%d:%d", &f, &v) >= 1) {
       for (const Cand &c : cands)
-        if (c.format == f && (f == 3 || c.variant == v)) { p.format = f; p.variant = c.variant; }
+        if (c.format == f && c.variant == v) { p.format = f; p.variant = v; }
     }
   }
   return SGPU_OK;
