@@ -158,6 +158,18 @@ SGPU_API int sgpu_matrix_pcg_d(sgpu_matrix m, double *x_d, const double *f_d, in
                       double zero, int64_t iv, int32_t crit, int32_t prec, int32_t mode,
                       int64_t *ani, double *ares, sgpu_solve_info *info);
 
+/* All load cases at once (solve_linear_statics, MEFEL/SRC/lssolver.cpp:78-80,
+ * solves them one after the other): nrhs (<= 128) independent Jacobi-PCG
+ * iterations with the criterion of symcomprow::cg_prec, advanced together so
+ * that one sparse-matrix-times-block product per iteration reads the matrix
+ * once for all of them.  X, F: nrhs column blocks of n (the lhsrhs layout,
+ * lhsrhs.cpp:72-74), host; per column ani/ares as the reference (written only
+ * on convergence) and status[c] (may be NULL).  Returns the first non-OK
+ * column status, else OK. */
+SGPU_API int sgpu_matrix_pcg_multi(sgpu_matrix m, int32_t nrhs, double *X, const double *F, int64_t ni,
+                                   double res, double zero, int64_t iv, int64_t *ani, double *ares,
+                                   int32_t *status, sgpu_solve_info *info);
+
 /* ------------------------------------------------------------------------ */
 /* Assembly on the GPU                                                      */
 /* ------------------------------------------------------------------------ */
@@ -205,6 +217,35 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
  * for hex8t handles, the other matrix (kind K <-> C). */
 SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,
                              sgpu_assembly_info *info);
+
+/* Dirichlet lifting of TRFEL's assemble_init (TRFEL/SRC/globmatt.cpp:1635):
+ * for a hex8 conduction handle made by sgpu_assemble, add -K_e r_e of every
+ * element into rhs[n] (host, accumulated) at its free DOFs, where rnode[nn]
+ * holds the nodal values prescvalues() gives (globmatt.cpp:1057): prescribed
+ * values on prescribed nodes, initial values on free ones.  Time-constant
+ * prescribed values only (the capacity part of the lifting is then zero). */
+SGPU_API int sgpu_assembly_lift(sgpu_matrix m, const double *rnode, double *rhs);
+
+/* ------------------------------------------------------------------------ */
+/* Linear transient conduction                                              */
+/* ------------------------------------------------------------------------ */
+
+/* out = a K + b C on the common pattern of two handles (gmatrix::scalgm and
+ * addgm, GEFEL/gmatrix.cpp:1848/1791, index-aligned); a new handle. */
+SGPU_API int sgpu_matrix_combine(sgpu_matrix K, sgpu_matrix C, double a, double b, sgpu_matrix *out);
+/* nsteps steps of the d-form generalized trapezoid of
+ * linear_nonstat_solv_dform (TRFEL/SRC/npsolvert.cpp:1071-1272) with a fixed
+ * dt and alpha: dd = d + (1-alpha) dt v; A = alpha dt K + C; f = alpha dt rhs
+ * + C dd; A d = f by Jacobi-PCG with the reference's criterion (ni, res,
+ * zero, iv as for sgpu_scr_cg_prec; x starts from the previous d when
+ * iv = 1); v = (d - dd)/dt/alpha.  rhs[n] is the step's right-hand side
+ * (constant: the lifting of time-constant prescribed values), d and v (host,
+ * n) are read and overwritten; step_iterations (may be NULL) gets the
+ * iterations of every step.  Everything between the first and the last copy
+ * stays on the device. */
+SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v,
+                                  double dt, double alpha, int64_t nsteps, int64_t ni, double res, double zero,
+                                  int64_t iv, int32_t mode, int64_t *step_iterations, sgpu_solve_info *info);
 
 /* ------------------------------------------------------------------------ */
 /* Solving without allocating device memory                                 */

@@ -60,6 +60,7 @@ def lib():
         L.or_trfel_step.argtypes = [_L, _pL, _pL, _pD, _pD, _pD, _pD, _pD, _pD, _D, _D, _L, _D, _D,
                                     _L, C.POINTER(_L), C.POINTER(_D)]
         L.or_trfel_step.restype = C.c_int
+        L.or_trfel_lift.argtypes = [_L, _pD, _pL, _pL, _pD, _pD, _pD]
         _lib = L
     return _lib
 
@@ -180,6 +181,37 @@ def cr_cg_prec(adr, ci, a, f, ni=100000, res=1e-10, zero=1e-30, x0=None):
     st = lib().or_cr_cg_prec(n, _i64(adr), _i64(ci), _f64(a), x, _f64(f), ni, res, zero,
                              0 if x0 is None else 1, C.byref(ani), C.byref(ares))
     return x, st, ani.value, ares.value
+
+
+def trfel_lift(mesh, rnode):
+    """-K r lifting of assemble_init over all elements, in equation order."""
+    cne = element_code_numbers(mesh)
+    rhs = np.zeros(mesh.ndof)
+    lib().or_trfel_lift(mesh.ne, _f64(mesh.coords), _i64(mesh.elems), cne, _f64(mesh.mats[mesh.emat]),
+                        _f64(rnode), rhs)
+    return rhs
+
+
+def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1, rnode=None):
+    """nsteps of linear_nonstat_solv_dform (TRFEL/SRC/npsolvert.cpp:1146-1230)
+    with K and C assembled once (their values do not change for linear
+    materials) and the lifting of time-constant prescribed values."""
+    adr, ci, ka = assemble(mesh, sym=True, kind="hex8t_k")
+    _, _, ca = assemble(mesh, sym=True, kind="hex8t_c")
+    n = adr.size - 1
+    if rnode is None:
+        rnode = mesh.meta["prescribed"][:, 0]
+    rhs = trfel_lift(mesh, rnode)
+    d = np.zeros(n)
+    v = np.zeros(n)
+    work = np.zeros(ka.size)
+    its = []
+    for _ in range(nsteps):
+        ani, ares = _L(-1), _D(0.0)
+        st = lib().or_trfel_step(n, adr, ci, ka, ca, work, rhs, d, v, dt, alpha, ni, res, zero, iv,
+                                 C.byref(ani), C.byref(ares))
+        its.append((st, ani.value))
+    return d, v, its
 
 
 def scr_to_dense(adr, ci, a):

@@ -620,3 +620,31 @@ int or_trfel_step(long n, const long *adr, const long *ci, const double *ka, con
   free(f); free(p); free(dd);
   return st;
 }
+
+/* Dirichlet lifting of assemble_init (TRFEL/SRC/globmatt.cpp:1635-1760) for
+ * linear hexahedra with isotropic conduction: r_e = nodal values given by
+ * prescvalues() (globmatt.cpp:1057: prescribed values on prescribed DOFs,
+ * initial values on free ones); f = -K_e r_e (mxv then cmulv(-1)); locglob
+ * adds f at DOFs with code number > 0.  emat: ne x (k, c); cne: ne x 8. */
+void or_trfel_lift(long ne, const double *coords, const long *elems, const long *cne, const double *emat,
+                   const double *rnode, double *rhs) {
+  double xyz[24], ke[64], r[8], f[8];
+  for (long e = 0; e < ne; e++) {
+    const long *nd = elems + e * 8;
+    for (int i = 0; i < 8; i++) {
+      for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
+      r[i] = rnode[nd[i]];
+    }
+    double rho1[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+    or_hex8t_kc(xyz, emat[2 * e], emat[2 * e + 1], rho1, ke, NULL);
+    for (int i = 0; i < 8; i++) {
+      double s = 0.0;
+      for (int j = 0; j < 8; j++) s += ke[i * 8 + j] * r[j];
+      f[i] = -1.0 * s;
+    }
+    for (int i = 0; i < 8; i++) {
+      long ii = cne[e * 8 + i] - 1;
+      if (ii >= 0) rhs[ii] += f[i];
+    }
+  }
+}

@@ -397,6 +397,60 @@ __global__ void __launch_bounds__(TPB) k_hex8_scalar(int ne_c, const int *__rest
   }
 }
 
+// Dirichlet lifting of TRFEL's assemble_init (TRFEL/SRC/globmatt.cpp:1635-1760):
+// for every element, r_e = the nodal values prescvalues() gives (prescribed
+// values on prescribed DOFs, the initial values on free DOFs,
+// globmatt.cpp:1057-1075), f_e = -K_e r_e, added to rhs at the free DOFs
+// (locglob).  With time-constant prescribed values the capacity term of
+// assemble_init, -C_e (r - r_prev)/dt, is zero and is not formed.
+__global__ void __launch_bounds__(TPB) k_hex8t_lift(int ne_c, const int *__restrict__ elist,
+                                                    const double *__restrict__ coords,
+                                                    const int64_t *__restrict__ elems,
+                                                    const int *__restrict__ cne, const double *__restrict__ emat,
+                                                    const double *__restrict__ rnode, double *__restrict__ rhs) {
+  __shared__ HexShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexShared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double x[8], y[8], z[8], cx = 0, cy = 0, cz = 0, rv = 0;
+    if (lane < 8) {
+      const int64_t nd = elems[(int64_t)e * 8 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1]; cz = coords[3 * nd + 2];
+      rv = rnode[nd];
+    }
+    double r[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+      z[a] = __shfl_sync(0xffffffffu, cz, a);
+      r[a] = __shfl_sync(0xffffffffu, rv, a);
+    }
+    hex_gauss_point(lane, x, y, z, sh, false);
+    __syncwarp();
+    const double kc = emat[2 * (int64_t)e];
+    if (lane < 8) {
+      const int a = lane;
+      double f = 0.0;
+#pragma unroll
+      for (int b = 0; b < 8; b++) {
+        double kab = 0.0;
+#pragma unroll
+        for (int gp = 0; gp < 8; gp++) {
+          const double gg = sh.g[gp][a][0] * sh.g[gp][b][0] + sh.g[gp][a][1] * sh.g[gp][b][1] +
+                            sh.g[gp][a][2] * sh.g[gp][b][2];
+          kab += gg * kc * sh.w[gp];
+        }
+        f += kab * r[b];
+      }
+      const int row = __ldg(cne + (int64_t)e * 8 + a);
+      if (row >= 0) rhs[row] -= f;
+    }
+    __syncwarp();
+  }
+}
+
 int read_err(const unsigned *err_d, cudaStream_t s, unsigned *out) {
   SGPU_CUDA(cudaMemcpyAsync(out, err_d, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
@@ -654,6 +708,33 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   *out = m;
   return SGPU_OK;
 #undef BAIL_ON
+}
+
+SGPU_API int sgpu_assembly_lift(sgpu_matrix m, const double *rnode, double *rhs) {
+  if (!m || !m->asm_data) return fail(SGPU_BAD_INPUT, "handle was not created by sgpu_assemble");
+  if (!rnode || !rhs) return fail(SGPU_BAD_INPUT, "null argument");
+  AssemblyData &ad = m->asm_data->d;
+  if (ad.kind != SGPU_ELEM_HEX8T_K && ad.kind != SGPU_ELEM_HEX8T_C)
+    return fail(SGPU_BAD_INPUT, "lifting is defined for the hex8 conduction handles");
+  cudaStream_t s = m->stream;
+  DevBuf<double> rn, f;
+  SGPU_TRY(rn.alloc(ad.nn));
+  SGPU_TRY(f.alloc(m->n));
+  SGPU_CUDA(cudaMemcpyAsync(rn.p, rnode, ad.nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  SGPU_CUDA(cudaMemcpyAsync(f.p, rhs, m->n * sizeof(double), cudaMemcpyHostToDevice, s));
+  const int ncol = (int)ad.offsets.size() - 1;
+  for (int col = 0; col < ncol; col++) {
+    const int beg = ad.offsets[col], cnt = ad.offsets[col + 1] - beg;
+    if (cnt == 0) continue;
+    const int grid = std::min((cnt + WPB - 1) / WPB, kNumSMs * 16);
+    k_hex8t_lift<<<grid, TPB, 0, s>>>(cnt, ad.elist.p + beg, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, rn.p,
+                                      f.p);
+    count_launches(1);
+  }
+  SGPU_CUDA(cudaGetLastError());
+  SGPU_CUDA(cudaMemcpyAsync(rhs, f.p, m->n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  return SGPU_OK;
 }
 
 SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,

@@ -202,6 +202,26 @@ class DeviceMatrix:
         return xx, Result(st, ani.value if got else None, ares.value if got else None, info.as_dict())
 
 
+def pcg_multi(dm: "DeviceMatrix", F, ni=100000, res=1e-20, zero=1e-30, X0=None):
+    """Every column of F (n x R, or R column blocks) solved together by the
+    batched Jacobi-PCG (one SpMM per iteration).  Returns X (n x R) and a
+    list of per-column Results."""
+    F = np.asarray(F, dtype=np.float64)
+    R = F.shape[1]
+    Fc = np.ascontiguousarray(F.T)  # R column blocks of n
+    Xc = np.zeros_like(Fc) if X0 is None else np.ascontiguousarray(np.asarray(X0, dtype=np.float64).T)
+    ani = np.full(R, -1, dtype=np.int64)
+    ares = np.full(R, np.nan)
+    st = np.zeros(R, dtype=np.int32)
+    info = L.SolveInfo()
+    rc = L.lib().sgpu_matrix_pcg_multi(dm.h, R, Xc, Fc, int(ni), float(res), float(zero), 0 if X0 is None else 1,
+                                       ani.ctypes.data, ares.ctypes.data, st.ctypes.data, C.byref(info))
+    L.check(rc, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN, L.ZERO_RHS))
+    out = [Result(int(st[c]), int(ani[c]) if ani[c] >= 0 else None, float(ares[c]) if ani[c] >= 0 else None,
+                  info.as_dict()) for c in range(R)]
+    return Xc.T.copy(), out
+
+
 class gmatrix:
     """The solver-dispatch facade of GEFEL/gmatrix.cpp for the CG cases.
 

@@ -71,12 +71,22 @@ def mefel_right_hand_side(mesh, lc: int = 0) -> np.ndarray:
     return f
 
 
-def solve_linear_statics(mesh, ni=100000, res=1e-20, mode="fp64"):
-    """Assemble K once, then solve every load case (lssolver.cpp:78-80)."""
+def solve_linear_statics(mesh, ni=100000, res=1e-20, mode="fp64", batched=None):
+    """Assemble K once, then solve every load case (lssolver.cpp:78-80).
+    With several load cases (and FP64) they are solved together by the
+    batched PCG unless batched=False."""
+    from .gefel import pcg_multi
     K = stiffness_matrix(mesh)
+    nlc = mesh.loads.shape[0]
+    if batched is None:
+        batched = nlc > 1 and mode == "fp64"
     out, results = [], []
     try:
-        for lc in range(mesh.loads.shape[0]):
+        if batched:
+            F = np.stack([mefel_right_hand_side(mesh, lc) for lc in range(nlc)], axis=1)
+            X, results = pcg_multi(K, F, ni=ni, res=res)
+            return X.T.copy(), results
+        for lc in range(nlc):
             f = mefel_right_hand_side(mesh, lc)
             x, r = K.pcg(f, ni=ni, res=res, crit="scr", prec=1, mode=mode)
             out.append(x)
@@ -84,3 +94,36 @@ def solve_linear_statics(mesh, ni=100000, res=1e-20, mode="fp64"):
     finally:
         K.close()
     return np.stack(out), results
+
+
+def trfel_lift(K: DeviceMatrix, rnode) -> np.ndarray:
+    """Right-hand side of TRFEL's assemble_init for time-constant prescribed
+    values: -sum_e K_e r_e at the free DOFs (TRFEL/SRC/globmatt.cpp:1635)."""
+    rhs = np.zeros(K.n)
+    L.check(L.lib().sgpu_assembly_lift(K.h, _c(rnode, np.float64), rhs))
+    return rhs
+
+
+def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1,
+                              mode="fp64", rnode=None, d0=None, v0=None):
+    """The d-form generalized trapezoid (TRFEL/SRC/npsolvert.cpp:1071) on the
+    GPU: K and C assembled once, `nsteps` steps with everything on the device.
+    Returns (d, v, per-step iterations, solve info)."""
+    K = conductivity_matrix(mesh)
+    Cm = capacity_matrix(mesh)
+    try:
+        if rnode is None:
+            rnode = mesh.meta["prescribed"][:, 0]
+        rhs = trfel_lift(K, rnode)
+        d = np.zeros(K.n) if d0 is None else _c(d0, np.float64).copy()
+        v = np.zeros(K.n) if v0 is None else _c(v0, np.float64).copy()
+        its = np.zeros(max(nsteps, 1), dtype=np.int64)
+        info = L.SolveInfo()
+        m = {"fp64": L.FP64, "mixed": L.MIXED}[mode]
+        st = L.lib().sgpu_transient_dform(K.h, Cm.h, rhs, d, v, float(dt), float(alpha), int(nsteps), int(ni),
+                                          float(res), float(zero), int(iv), m, its.ctypes.data, C.byref(info))
+        L.check(st, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN))
+        return d, v, its[:nsteps], info.as_dict()
+    finally:
+        K.close()
+        Cm.close()

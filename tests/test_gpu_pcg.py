@@ -151,3 +151,25 @@ def test_every_spmv_kernel_fp32_scaled(oracle, gpu_lib, fmt, variant):
     got = yd.cpu().numpy().astype(np.float64)
     # FP32 values and accumulation: a few ulps of the row's magnitude
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("nrhs,sym", [(5, True), (40, True), (7, False)])
+def test_batched_load_cases_match_oracle(oracle, gpu_lib, nrhs, sym):
+    from ssf_b200.gefel import DeviceMatrix, pcg_multi
+    m = decks.cantilever_top_loads(decks.cantilever_hex(12, 3, 3, H=0.2), nrhs, seed=9)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    F = np.stack([oracle.load_vector(m, lc) for lc in range(nrhs)], axis=1)
+    if not sym:  # a matrix without the 3x3 block form takes the CSR product
+        adr, ci, a = oracle.assemble(m, sym=False)
+        with DeviceMatrix(adr, ci, a, 0) as d:
+            X, res = pcg_multi(d, F, res=1e-20)
+        sadr, sci, sa = oracle.assemble(m, sym=True)
+    else:
+        with DeviceMatrix(adr, ci, a, 1) as d:
+            X, res = pcg_multi(d, F, res=1e-20)
+        sadr, sci, sa = adr, ci, a
+    for c in range(nrhs):
+        xo, st, ani_o, _ = oracle.scr_cg_prec(sadr, sci, sa, F[:, c], ni=20000, res=1e-20)
+        assert st == 0 and res[c].status == L.OK
+        assert abs(res[c].ani - ani_o) <= 2
+        assert np.linalg.norm(X[:, c] - xo) / np.linalg.norm(xo) <= 1e-8
