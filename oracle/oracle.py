@@ -281,6 +281,16 @@ def run_mefel_dump(deck_path: str, outdir: str, solve: bool = True) -> dict:
     return read_dump(outdir)
 
 
+def run_trfel_dump(deck_path: str, outdir: str, solve: bool = True) -> dict:
+    """Run the reference TRFEL pipeline on a deck; return its dumped arrays."""
+    os.makedirs(outdir, exist_ok=True)
+    exe = os.path.join(REF_DIR, "trfel_dump")
+    args = [exe, os.path.abspath(deck_path), "."] + ([] if solve else ["nosolve"])
+    with open(os.path.join(outdir, "run.log"), "w") as log:
+        subprocess.run(args, cwd=outdir, stdout=log, stderr=subprocess.STDOUT, check=True)
+    return read_dump(outdir)
+
+
 def read_dump(outdir: str) -> dict:
     meta = {}
     with open(os.path.join(outdir, "meta.txt")) as fh:

@@ -298,3 +298,69 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
     lines.append("0")  # outgr_format
     with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
+
+
+def write_trfel_deck(mesh: Mesh, path: str, dt: float, nsteps: int, alpha: float = 1.0, ni: int = 20000,
+                     res: float = 1.0e-20, iv: int = 1, precond: int = 1, rho: float = 1.0,
+                     title: str = "sifel-b200 synthetic transport deck") -> None:
+    """Write a linear nonstationary heat-conduction TRFEL deck (positional).
+
+    Token order as read by probdesct::read (TRFEL/SRC/probdesct.cpp:177-560;
+    timecontr::read, GEFEL/timecontr.cpp:70), transtop::read
+    (transtop.cpp:93), elementt::read (elementt.cpp:72), transmat::read
+    (transmat.cpp:794; isotrmat "c k", isotrmat.cpp:444), transcrsec::read
+    (transcrsec.cpp:33), transbclc::read / loadcaset::read (transbclc.cpp:33,
+    loadcaset.cpp:133; one constant prescribed value per distinct value),
+    lhsrhst::initcond (lhsrhst.cpp:157) and outdrivert::read.  Every element
+    has its own isotropic material instance (mesh.mats rows (k, c)); storage
+    SCR (11) for K and C, cg (20) with the diagonal preconditioner.
+    """
+    presc = mesh.meta["prescribed"][:, 0]
+    end = dt * nsteps
+    L = [title]
+    # mesprt problemtype(nonstationary 60) transmatter(onemedium 1) mednames(heat 1) scale
+    L.append("0\n60\n1\n1\n1.0")
+    # gradcomp fluxcomp othercomp eqothercomp gravity adaptivity stochastic homog noderenumber advection reaction
+    L.append("0\n0\n0\n0\n0\n0\n0\n0\n0\n0\n0")
+    # nonstatsolver trapezoidd(1) alpha; timecontr fixed(0) start end, one important time, constant dt
+    L.append(f"1 {_fmt(alpha)}")
+    L.append(f"0 0.0 {_fmt(end)} 1 {_fmt(end)} 0 {_fmt(dt)}")
+    # timetypeprint, hdbackup, storages, solver, capdiagonalization
+    L.append("1\n0\n11 11")
+    L.append(f"20 {ni} {_fmt(res)} {iv}")
+    L.append(f"{precond}\n0")
+    L.append(f"{mesh.nn}")
+    for i, (x, y, z) in enumerate(mesh.coords):
+        L.append(f"{i + 1} {_fmt(x)} {_fmt(y)} {_fmt(z)} 1 0")
+    # constraints: prescribed nodes get code -(index of their prescribed value)
+    fixed = np.where(mesh.dofflag[:, 0] != 1)[0]
+    values = sorted(set(float(presc[i]) for i in fixed))
+    pv_index = {v: k + 1 for k, v in enumerate(values)}
+    L.append(f"{fixed.size}")
+    for i in fixed:
+        L.append(f"{i + 1} {-pv_index[float(presc[i])]}")
+    L.append(f"{mesh.ne}")
+    for e, nodes in enumerate(mesh.elems):
+        ns = " ".join(str(int(v) + 1) for v in nodes)
+        # cne 0, cross section crsec3dt (3) instance 1 (the density), material isotransmat (100)
+        L.append(f"{e + 1} 225 {ns} 0 3 1 100 {int(mesh.emat[e]) + 1}")
+    # materials: isotransmat (100), one instance per row of mats: "id c k"
+    L.append("1")
+    L.append(f"100 {mesh.mats.shape[0]}")
+    for k, (kc, c) in enumerate(mesh.mats):
+        L.append(f"{k + 1} {_fmt(c)} {_fmt(kc)}")
+    # cross sections: one 3D section carrying the density (capacity = rho c N^T N)
+    L.append("1\n3 1")
+    L.append(f"1 {_fmt(rho)}")
+    # one load case: prescribed values, no sources / element loads / nodal values / climatic conditions
+    L.append("1")
+    L.append(f"{len(values)}")
+    for v in values:
+        L.append(f"{_fmt(v)} 0 {_fmt(v)}")
+    L.append("0\n0\n0\n0\n0\n0")  # nqs neb nnv ncc ncc2 nmultfunc
+    L.append("0")  # boundary fluxes: neb
+    for i in range(mesh.nn):  # initial values
+        L.append(f"{i + 1} 0.0")
+    L.append("0\n0\n0")  # textout outgr_format numdiag
+    with open(path, "w") as fh:
+        fh.write("\n".join(L) + "\n")

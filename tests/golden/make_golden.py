@@ -87,6 +87,21 @@ def main(big=False):
     np.savez_compressed(os.path.join(HERE, "cr_cantilever.npz"), adr=d["K_adr"], ci=d["K_ci"], a=d["K_a"],
                         f=d["f"], u=d["u"], ani=d["meta"]["ani_0"], ares=d["meta"]["ares_0"])
 
+    # TRFEL: 4^3 heat cube, lognormal conductivity per element, T = 1 on x = 0,
+    # implicit Euler, dt = 10 s: K, C and (T, V) after 1 and 3 steps
+    cube = decks.heat_cube(4)
+    res = {}
+    for nsteps in (1, 3):
+        with tempfile.TemporaryDirectory() as td:
+            deck = os.path.join(td, "cube.in")
+            decks.write_trfel_deck(cube, deck, dt=10.0, nsteps=nsteps)
+            dd = O.run_trfel_dump(deck, td)
+        res[nsteps] = dd
+    d1, d3 = res[1], res[3]
+    np.savez_compressed(os.path.join(HERE, "trfel_cube.npz"), K_adr=d3["K_adr"], K_ci=d3["K_ci"], K_a=d3["K_a"],
+                        C_adr=d3["C_adr"], C_ci=d3["C_ci"], C_a=d3["C_a"], T1=d1["T"], V1=d1["V"], T3=d3["T"],
+                        V3=d3["V"], ani3=d3["meta"]["ani"], dt=10.0)
+
     for (nx, ny, nz), key in (((100, 20, 20), "cantilever_100x20x20"),) + (
             (((200, 40, 40), "cantilever_200x40x40"),) if big else ()):
         d = run(decks.cantilever_hex(nx, ny, nz), key)

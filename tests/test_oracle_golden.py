@@ -107,3 +107,21 @@ def test_iteration_limit_leaves_ani_untouched(oracle):
     g = load("c1_cantilever.npz")
     x, st, ani, ares = oracle.scr_cg_prec(g["adr"], g["ci"], g["a"], g["f"], ni=5, res=1e-20)
     assert st == 1 and ani == -1
+
+
+def test_trfel_cube_matrices_and_steps(oracle):
+    """TRFEL conductivity/capacity (linhext, TRFEL/SRC/linhext.cpp:774/979),
+    Dirichlet lifting (globmatt.cpp:1635) and the d-form trapezoid
+    (npsolvert.cpp:1071): bit-exact with the compiled reference."""
+    g = load("trfel_cube.npz")
+    m = decks.heat_cube(4)
+    adr, ci, ka = oracle.assemble(m, sym=True, kind="hex8t_k")
+    assert np.array_equal(adr, g["K_adr"]) and np.array_equal(ci, g["K_ci"])
+    assert np.array_equal(ka, g["K_a"])
+    _, _, ca = oracle.assemble(m, sym=True, kind="hex8t_c")
+    assert np.array_equal(ca, g["C_a"])
+    T1, V1, _ = oracle.trfel_steps(m, 1, float(g["dt"]), iv=1)
+    assert np.array_equal(T1, g["T1"]) and np.array_equal(V1, g["V1"])
+    T3, V3, its = oracle.trfel_steps(m, 3, float(g["dt"]), iv=1)
+    assert np.array_equal(T3, g["T3"]) and np.array_equal(V3, g["V3"])
+    assert its[-1][1] == int(g["ani3"])

@@ -1,0 +1,55 @@
+"""The oracle against the compiled SIFEL reference on fresh decks (skipped
+where oracle/_ref has not been built: the reference sources are needed)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from ssf_b200 import decks
+
+
+@pytest.fixture(scope="module")
+def ref(oracle):
+    if not oracle.ref_available():
+        pytest.skip("compiled reference (oracle/_ref) not built")
+    return oracle
+
+
+def test_random_distorted_cantilever_bit_exact(ref):
+    m = decks.cantilever_hex(7, 3, 2)
+    rng = np.random.default_rng(42)
+    inner = ~np.isclose(m.coords[:, 0], 0.0)
+    m.coords[inner] += rng.uniform(-0.01, 0.01, (inner.sum(), 3))
+    m.emat = rng.integers(0, 3, m.ne)
+    m.mats = np.array([[210e9, 0.3], [70e9, 0.33], [30e9, 0.2]])
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    assert np.array_equal(a, d["K_a"])
+    f = ref.load_vector(m)
+    x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
+
+
+def test_reference_solver_library_matches_oracle(ref):
+    """libsifelref.so runs the reference's own symcomprow::cg_prec."""
+    m = decks.cantilever_hex(10, 2, 2)
+    adr, ci, a = ref.assemble(m, sym=True)
+    f = ref.load_vector(m)
+    x_o, _, ani_o, ares_o = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    x_r, ani_r, ares_r = ref.ref_scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani_r == ani_o and ares_r == ares_o and np.array_equal(x_r, x_o)
+
+
+def test_trfel_random_cube_bit_exact(ref):
+    m = decks.heat_cube(3, seed=77)
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "c.in")
+        decks.write_trfel_deck(m, deck, dt=25.0, nsteps=2, alpha=0.5)
+        d = ref.run_trfel_dump(deck, td)
+    T, V, its = ref.trfel_steps(m, 2, 25.0, alpha=0.5, iv=1)
+    assert np.array_equal(T, d["T"]) and np.array_equal(V, d["V"])
