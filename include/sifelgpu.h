@@ -73,6 +73,7 @@ typedef struct {
   int32_t spmv_variant;     /* autotuned kernel variant id */
   int32_t fallback;         /* MIXED: 1 if the FP32 iteration stagnated and the
                                solve was finished in FP64 from its iterate */
+  int32_t tile_rows;        /* batched solves: rows per work segment picked by the tuner */
 } sgpu_solve_info;
 
 /* ------------------------------------------------------------------------ */
@@ -169,6 +170,21 @@ SGPU_API int sgpu_matrix_pcg_d(sgpu_matrix m, double *x_d, const double *f_d, in
 SGPU_API int sgpu_matrix_pcg_multi(sgpu_matrix m, int32_t nrhs, double *X, const double *F, int64_t ni,
                                    double res, double zero, int64_t iv, int64_t *ani, double *ares,
                                    int32_t *status, sgpu_solve_info *info);
+
+/* Many independent systems of uneven size (the diagonal blocks of m, in
+ * order; sys_rows[k] equations each, summing to n) solved together: every
+ * system its own Jacobi-PCG with the criterion of symcomprow::cg_prec, all
+ * advanced by the same kernels (one block-diagonal SpMV and two vector
+ * kernels per iteration, captured in a CUDA graph and relaunched until every
+ * system has stopped); converged systems drop out of the work.  tune != 0
+ * first times a few iterations with each segment size / lanes-per-row pair
+ * and keeps the fastest.  x: n (host, out; the iteration starts from 0);
+ * f: n; per system ani/ares (reference conventions), status and iterations
+ * (arrays of nsys, may be NULL). */
+SGPU_API int sgpu_matrix_pcg_batch(sgpu_matrix m, int32_t nsys, const int64_t *sys_rows, double *x,
+                                   const double *f, int64_t ni, double res, double zero, int32_t tune,
+                                   int64_t *ani, double *ares, int32_t *status, int64_t *iterations,
+                                   sgpu_solve_info *info);
 
 /* ------------------------------------------------------------------------ */
 /* Assembly on the GPU                                                      */

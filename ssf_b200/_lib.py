@@ -34,6 +34,7 @@ class SolveInfo(C.Structure):
         ("spmv_format", C.c_int32),
         ("spmv_variant", C.c_int32),
         ("fallback", C.c_int32),
+        ("tile_rows", C.c_int32),
     ]
 
     def as_dict(self):
@@ -112,6 +113,8 @@ SIGNATURES = {
                               C.POINTER(SolveInfo)], C.c_int),
     "sgpu_matrix_pcg_multi": ([_vp, _i32, _pD, _pD, _i64, _dbl, _dbl, _i64, _vp, _vp, _vp, C.POINTER(SolveInfo)],
                               C.c_int),
+    "sgpu_matrix_pcg_batch": ([_vp, _i32, _pL, _pD, _pD, _i64, _dbl, _dbl, _i32, _vp, _vp, _vp, _vp,
+                               C.POINTER(SolveInfo)], C.c_int),
     "sgpu_assemble": ([C.POINTER(Mesh), C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_reassemble": ([_vp, _i32, _vp, _vp, C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_last_error": ([], C.c_char_p),

@@ -364,3 +364,34 @@ def write_trfel_deck(mesh: Mesh, path: str, dt: float, nsteps: int, alpha: float
     L.append("0\n0\n0")  # textout outgr_format numdiag
     with open(path, "w") as fh:
         fh.write("\n".join(L) + "\n")
+
+
+def merge_meshes(meshes) -> tuple[Mesh, np.ndarray]:
+    """Concatenate independent meshes of one kind into one mesh with disjoint
+    node ranges (node ids shifted, one material row per mesh kept).  The code
+    numbers of the merged mesh run mesh by mesh, so every mesh is a
+    contiguous diagonal block of the global matrix.  Returns the merged mesh
+    and the equation count of each part."""
+    kind = meshes[0].kind
+    coords, elems, dofflag, emat, mats, thick, loads, rows = [], [], [], [], [], [], [], []
+    node0 = 0
+    mat0 = 0
+    for m in meshes:
+        if m.kind != kind:
+            raise ValueError("meshes of different kinds")
+        coords.append(m.coords)
+        elems.append(m.elems + node0)
+        dofflag.append(m.dofflag)
+        emat.append(m.emat + mat0)
+        mats.append(m.mats)
+        if m.thick is not None:
+            thick.append(m.thick)
+        loads.append(m.loads[0])
+        rows.append(m.ndof)
+        node0 += m.nn
+        mat0 += m.mats.shape[0]
+    merged = Mesh(kind=kind, coords=np.concatenate(coords), elems=np.concatenate(elems),
+                  dofflag=np.concatenate(dofflag), emat=np.concatenate(emat), mats=np.concatenate(mats),
+                  loads=np.concatenate(loads)[None], thick=np.concatenate(thick) if thick else None,
+                  meta=dict(parts=len(meshes)))
+    return merged, np.asarray(rows, dtype=np.int64)

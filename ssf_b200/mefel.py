@@ -127,3 +127,31 @@ def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20,
     finally:
         K.close()
         Cm.close()
+
+
+def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True):
+    """Many independent meshes (e.g. the uneven plate batch) assembled in one
+    call and solved by the batched PCG in one launch sequence.  Returns the
+    list of solutions, per-system (status, ani, ares, iterations) and info."""
+    from .decks import merge_meshes
+    merged, rows = merge_meshes(meshes)
+    K = stiffness_matrix(merged)
+    try:
+        f = mefel_right_hand_side(merged)
+        x = np.zeros(K.n)
+        nsys = rows.size
+        ani = np.full(nsys, -1, dtype=np.int64)
+        ares = np.full(nsys, np.nan)
+        st = np.zeros(nsys, dtype=np.int32)
+        its = np.zeros(nsys, dtype=np.int64)
+        info = L.SolveInfo()
+        rc = L.lib().sgpu_matrix_pcg_batch(K.h, nsys, rows, x, f, int(ni), float(res), float(zero), int(tune),
+                                           ani.ctypes.data, ares.ctypes.data, st.ctypes.data, its.ctypes.data,
+                                           C.byref(info))
+        L.check(rc, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN, L.ZERO_RHS))
+        offs = np.concatenate([[0], np.cumsum(rows)])
+        xs = [x[offs[k]:offs[k + 1]] for k in range(nsys)]
+        out = dict(status=st, ani=ani, ares=ares, iterations=its, info=info.as_dict(), assembly=K.assembly)
+        return xs, out
+    finally:
+        K.close()

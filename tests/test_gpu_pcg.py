@@ -173,3 +173,19 @@ def test_batched_load_cases_match_oracle(oracle, gpu_lib, nrhs, sym):
         assert st == 0 and res[c].status == L.OK
         assert abs(res[c].ani - ani_o) <= 2
         assert np.linalg.norm(X[:, c] - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_uneven_batch_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    rng = np.random.default_rng(21)
+    plates = [decks.plate_quad(int(a), int(b), E=float(e), nu=float(v), traction=1e6)
+              for a, b, e, v in zip(rng.integers(3, 12, 9), rng.integers(3, 12, 9), rng.uniform(1e9, 1e11, 9),
+                                    rng.uniform(0.2, 0.35, 9))]
+    xs, out = mefel.solve_batch(plates, res=1e-20, tune=True)
+    for k, p in enumerate(plates):
+        adr, ci, a = oracle.assemble(p, sym=True)
+        f = oracle.load_vector(p)
+        xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+        assert st == 0 and out["status"][k] == L.OK
+        assert abs(int(out["ani"][k]) - ani_o) <= 2
+        assert np.linalg.norm(xs[k] - xo) / np.linalg.norm(xo) <= 1e-8
