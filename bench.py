@@ -52,6 +52,8 @@ WORKLOADS = {
     "cantilever_100x20x20": (100, 20, 20),
     "cantilever_20x4x4": (20, 4, 4),
 }
+# the other benchmark configurations, one JSON line each when asked for
+EXTRA = ("cantilever_100x20x20_64rhs", "heat_cube_128_50steps", "plates_512")
 METRIC = "solve time to relative residual 1e-10 (fastest GPU form; mixed-refined and FP64 PCG both reported)"
 TOL = 1.0e-10
 # Iterations SIFEL's own Jacobi-PCG (symcomprow::cg_prec, SCR storage,
@@ -387,6 +389,172 @@ def run_ours(args, ws, rank):
 
 
 # ----------------------------------------------------------------------------
+# the other configurations: many load cases, transient conduction, plate batch
+# ----------------------------------------------------------------------------
+
+def _timed_calls(fn, steps, warmup, ws):
+    """Wall-clock of synchronous library calls bracketed by device syncs and
+    CUDA events on the current stream (the calls finish their own streams
+    before returning); max over ranks."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    l0 = L.kernel_launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    outs = [fn() for _ in range(steps)]
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    return dist_max(e0.elapsed_time(e1) / steps, ws), outs, L.kernel_launches() - l0
+
+
+def run_extra(args, ws, rank):
+    import torch
+    from ssf_b200 import gefel, mefel
+    from oracle import oracle as O  # CPU baseline leg only
+    torch.cuda.set_device(torch.cuda.current_device())
+    peak, peak_kind = measured_peak()
+    out = {"n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated meshes)", "unit": "ms"}
+    clocks = Clocks(torch.cuda.current_device())
+    if args.workload == "cantilever_100x20x20_64rhs":
+        mesh = decks.cantilever_top_loads(decks.cantilever_hex(100, 20, 20), 64, seed=1234)
+        K = mefel.stiffness_matrix(mesh)
+        F = np.stack([mefel.mefel_right_hand_side(mesh, lc) for lc in range(64)], axis=1)
+        clocks.start()
+        ms, outs, launches = _timed_calls(lambda: gefel.pcg_multi(K, F, res=1e-20), args.steps, args.warmup, ws)
+        clk = clocks.stop()
+        X, res = outs[-1]
+        # the same 64 cases one after the other (the reference's order), device-resident matrix
+        t0 = time.perf_counter()
+        seq_its = []
+        for c in range(64):
+            _, r = K.pcg(F[:, c], res=1e-20, crit="scr", prec=1, mode="fp64")
+            seq_its.append(r.info["iterations"])
+        torch.cuda.synchronize()
+        seq_ms = (time.perf_counter() - t0) * 1e3
+        n = K.n
+        adr_h, ci_h, a_h = K.download(symmetric=1)
+        K.close()
+        per_it = None
+        if rank == 0 and O.ref_available():
+            t0 = time.perf_counter()
+            O.ref_scr_cg_prec(adr_h, ci_h, a_h, F[:, 0], ni=20, res=1e-20)
+            per_it = (time.perf_counter() - t0) / 21
+        its = [r.info["iterations"] for r in res]
+        out.update({"metric": "64 load cases to (r.r)/(f.f) < 1e-20 each: batched PCG with SpMM", "value": round(ms, 3),
+                    "ms_per_step": round(ms, 3),
+                    "config": {"workload": args.workload, "n_equations": n, "load_cases": 64,
+                               "parallelism": "single GPU" if ws == 1 else f"replicas x{ws}"},
+                    "batched": {"solve_ms": round(ms, 3), "iterations_max": int(max(its)),
+                                "all_converged": all(r.status == L.OK for r in res)},
+                    "sequential_fp64": {"solve_ms": round(seq_ms, 3), "iterations_total": int(sum(seq_its)),
+                                        "speedup_batched": round(seq_ms / ms, 2)},
+                    "gpu_launches": int(launches), "clocks": clk})
+        if per_it is not None:
+            out["cpu_baseline"] = {"value": round(per_it * 1e3 * (sum(seq_its)), 1), "unit": "ms", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": "20 iterations of SIFEL's symcomprow::cg_prec on load case 0, scaled to "
+                                             f"the {int(sum(seq_its))} iterations of the 64 sequential solves"}
+    elif args.workload == "heat_cube_128_50steps":
+        mesh = decks.heat_cube(128, seed=1234)
+        Kt = mefel.conductivity_matrix(mesh)
+        Ct = mefel.capacity_matrix(mesh, rho=np.ones(mesh.ne))
+        rhs = mefel.trfel_lift(Kt, mesh.meta["prescribed"][:, 0])
+        n = Kt.n
+        st_holder = {}
+
+        def run():
+            d = np.zeros(n)
+            v = np.zeros(n)
+            its = np.zeros(50, dtype=np.int64)
+            info = L.SolveInfo()
+            rc = L.lib().sgpu_transient_dform(Kt.h, Ct.h, rhs, d, v, 10.0, 1.0, 50, 100000, 1e-20, 1e-30, 1, L.FP64,
+                                              its.ctypes.data, C.byref(info))
+            L.check(rc)
+            st_holder["its"] = its
+            st_holder["info"] = info.as_dict()
+            return d
+        clocks.start()
+        ms, outs, launches = _timed_calls(run, args.steps, max(1, args.warmup // 3), ws)
+        clk = clocks.stop()
+        its = st_holder["its"]
+        out.update({"metric": "50 implicit-Euler steps of (C + dt K) T = f, each to (r.r)/(f.f) < 1e-20, K and C "
+                              "assembled on the GPU", "value": round(ms, 3), "ms_per_step": round(ms, 3),
+                    "config": {"workload": args.workload, "n_equations": n, "elements": int(mesh.ne), "dt_s": 10.0,
+                               "parallelism": "single GPU" if ws == 1 else f"replicas x{ws}"},
+                    "iterations_total": int(its.sum()), "iterations_per_step": [int(i) for i in its[:5]] + ["..."],
+                    "solve_ms_device": round(st_holder["info"]["solve_ms"], 3), "assembly": Kt.assembly,
+                    "gpu_launches": int(launches), "clocks": clk})
+        Kt.close()
+        Ct.close()
+        if rank == 0 and ws == 1 and not args.no_cpu:
+            t0 = time.perf_counter()
+            adr, ci, ka = O.assemble(mesh, sym=True, kind="hex8t_k")
+            _, _, ca = O.assemble(mesh, sym=True, kind="hex8t_c")
+            t_asm = time.perf_counter() - t0
+            d, v, sits = O.trfel_steps(mesh, 1, 10.0, iv=1, ni=100000)
+            t_step = time.perf_counter() - t0 - t_asm
+            # the reference integrates K and C (and the lifting) again in every step
+            est = 50 * (1.5 * t_asm + t_step) * 1e3
+            out["cpu_baseline"] = {"value": round(est, 1), "unit": "ms", "cores": 1, "kind": "port",
+                                   "sample": "the oracle's K and C integration and one step on this mesh, scaled "
+                                             "to 50 steps that each integrate K, C and the lifting again as "
+                                             "the reference does"}
+    else:  # plates_512
+        plates = decks.plate_batch(512, seed=0)
+        nd = sum(p.ndof for p in plates)
+        state = {}
+
+        def run():
+            xs, o = mefel.solve_batch(plates, res=1e-20, zero=1e-300, tune=state.get("tune", True))
+            state["tune"] = False
+            state["o"] = o
+            return xs
+        clocks.start()
+        ms, outs, launches = _timed_calls(run, args.steps, args.warmup, ws)
+        clk = clocks.stop()
+        o = state["o"]
+        out.update({"metric": "512 uneven plane-stress plates merged, assembled and solved together (each to "
+                              "(r.r)/(f.f) < 1e-20), host mesh to host solution", "value": round(ms, 3),
+                    "ms_per_step": round(ms, 3),
+                    "config": {"workload": args.workload, "plates": 512, "n_equations": int(nd),
+                               "parallelism": "single GPU" if ws == 1 else f"replicas x{ws}",
+                               "zero": "1e-300 (the reference's 1e-30 absolute |d.p| test stops these "
+                                       "unit-traction plates before 1e-10)"},
+                    "solve_ms_device": round(o["info"]["solve_ms"], 3), "assembly": o["assembly"],
+                    "iterations_max": int(o["iterations"].max()), "iterations_total": int(o["iterations"].sum()),
+                    "all_converged": bool((o["status"] == 0).all()),
+                    "tuned": {"lanes_per_row": o["info"]["spmv_variant"], "segment_rows": o["info"]["tile_rows"]},
+                    "gpu_launches": int(launches), "clocks": clk})
+        if rank == 0 and ws == 1 and not args.no_cpu and O.ref_available():
+            # sample: 8 plates spread over the size range, reference solve timed, scaled by nnz x iterations
+            order = np.argsort([p.ndof for p in plates])
+            pick = order[np.linspace(0, len(order) - 1, 8).astype(int)]
+            t_s, work_s = 0.0, 0.0
+            for k in pick:
+                adr, ci, a = O.assemble(plates[k], sym=True)
+                f = O.load_vector(plates[k])
+                t0 = time.perf_counter()
+                O.ref_scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-20, zero=1e-300)
+                t_s += time.perf_counter() - t0
+                work_s += plates[k].ndof * float(o["iterations"][k])
+            work_all = float(sum(p.ndof * float(o["iterations"][k]) for k, p in enumerate(plates)))
+            out["cpu_baseline"] = {"value": round(t_s * work_all / work_s * 1e3, 1),
+                                   "unit": "ms", "cores": 1, "kind": "reference",
+                                   "sample": "SIFEL's symcomprow::cg_prec on 8 of the 512 plates (sizes spread), "
+                                             "scaled by equations x iterations to the whole batch "
+                                             "(solve only)"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------------
 # the reference arm: SIFEL's own CPU solver on the same workload
 # ----------------------------------------------------------------------------
 
@@ -438,7 +606,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cantilever_200x40x40", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cantilever_200x40x40", choices=sorted(WORKLOADS) + list(EXTRA))
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--forms", default="both", choices=["both", "fp64", "mixed"],
@@ -450,7 +618,15 @@ def main():
         args.warmup = 3
     ws, rank = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.workload in EXTRA:
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "workload": args.workload,
+                                      "unavailable": "the reference arm is timed on the default workload; "
+                                                     "this line's cpu_baseline carries the CPU estimate"}))
+            else:
+                run_extra(args, ws, rank)
+        elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:
             run_ours(args, ws, rank)
