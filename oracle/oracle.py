@@ -214,6 +214,16 @@ def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, i
     return d, v, its
 
 
+def trfel_stationary(mesh, ni=100000, res=1e-20, zero=1e-30, rnode=None):
+    """solve_stationary_problem (TRFEL/SRC/spsolvert.cpp:13): K assembled,
+    right-hand side = the lifting of assemble_init, Jacobi-PCG."""
+    adr, ci, ka = assemble(mesh, sym=True, kind="hex8t_k")
+    if rnode is None:
+        rnode = mesh.meta["prescribed"][:, 0]
+    rhs = trfel_lift(mesh, rnode)
+    return scr_cg_prec(adr, ci, ka, rhs, ni=ni, res=res, zero=zero)
+
+
 def scr_to_dense(adr, ci, a):
     n = adr.size - 1
     K = np.zeros((n, n))

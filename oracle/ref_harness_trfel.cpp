@@ -82,18 +82,22 @@ int main(int argc, const char *argv[]) {
     double t2 = now_s();
     fprintf(m, "t_solve_total %.9f\n", t2 - t1);
     if (Kmat) fprintf(m, "ani %ld\nares %.17e\n", Kmat->ani, Kmat->ares);
+    fflush(m);
     dump(out + "/T.f64", Lsrst->give_lhs(0), sizeof(double) * n);
-    dump(out + "/V.f64", Lsrst->give_tdlhs(0), sizeof(double) * n);
+    // a stationary problem keeps no time derivatives
+    if (Tp->tprob != stationary_problem && Lsrst->give_tdlhs(0))
+      dump(out + "/V.f64", Lsrst->give_tdlhs(0), sizeof(double) * n);
   }
   double t3 = now_s();
   conductivity_matrix(0);
   double t4 = now_s();
-  capacity_matrix(0);
+  const bool transient = Tp->tprob != stationary_problem;
+  if (transient) capacity_matrix(0);
   double t5 = now_s();
   long nk = dump_matrix(out, "K", Kmat, n);
-  long nc = dump_matrix(out, "C", Cmat, n);
+  long nc = transient ? dump_matrix(out, "C", Cmat, n) : 0;
   fprintf(m, "negm_K %ld\nnegm_C %ld\nstorage_K %d\nstorage_C %d\n", nk, nc, (int)Kmat->ts,
-          (int)Cmat->ts);
+          transient ? (int)Cmat->ts : -1);
   fprintf(m, "t_conductivity %.9f\nt_capacity %.9f\n", t4 - t3, t5 - t4);
   fclose(m);
   return 0;

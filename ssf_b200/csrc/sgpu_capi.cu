@@ -216,8 +216,10 @@ int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32
   if (precision != 64 && precision != 32) return fail(SGPU_BAD_INPUT, "precision must be 64 or 32");
   if (format != 0 && format != 3) return fail(SGPU_BAD_INPUT, "format must be 0 (CSR) or 3 (BSR3)");
   if ((format == 0 && variant != 4 && variant != 8 && variant != 16 && variant != 32) ||
-      (format == 3 && variant != 8 && variant != 16 && variant != 32))
-    return fail(SGPU_BAD_INPUT, "variant = lanes per row: 4, 8, 16 or 32 for CSR; 8, 16 or 32 for BSR3");
+      (format == 3 && variant != 8 && variant != 16 && variant != 32 && variant != 132 && variant != 232 &&
+       variant != 116 && variant != 216 && variant != 108 && variant != 208))
+    return fail(SGPU_BAD_INPUT,
+                "variant = lanes per row: 4, 8, 16 or 32 for CSR; 8, 16, 32 (+100/+200: register caps) for BSR3");
   SGPU_TRY(pcg_prepare(m, precision == 32));
   if (precision == 32) {
     if (!m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "scaled operator needs a positive diagonal");

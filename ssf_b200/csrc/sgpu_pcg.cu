@@ -219,8 +219,8 @@ __global__ void __launch_bounds__(TPB) k_spmv_csr(int n, const int *__restrict__
 // Values are stored component-major per block row (see sgpu_matrix.cu) so a
 // warp reading one component of consecutive blocks is fully coalesced.
 // ---------------------------------------------------------------------------
-template <typename VT, typename XT, typename AccT, int LPR, class Epi>
-__global__ void __launch_bounds__(TPB) k_spmv_bsr3(int nb, const int *__restrict__ browptr,
+template <typename VT, typename XT, typename AccT, int LPR, int MINB, class Epi>
+__global__ void __launch_bounds__(TPB, MINB) k_spmv_bsr3(int nb, const int *__restrict__ browptr,
                                                    const int *__restrict__ bcol, const VT *__restrict__ bval,
                                                    const XT *__restrict__ x, XT *__restrict__ y,
                                                    PcgState *st, double *partials, unsigned *ticket) {
@@ -637,9 +637,17 @@ int launch_spmv64(sgpu_matrix m, int format, int variant, const double *x, doubl
   unsigned *tk = m->w.counters.p + ticket_slot;
   double *part = m->w.partials.p;
   if (format == 3) {
-    auto k = variant == 8    ? k_spmv_bsr3<double, double, double, 8, Epi>
-             : variant == 16 ? k_spmv_bsr3<double, double, double, 16, Epi>
-                             : k_spmv_bsr3<double, double, double, 32, Epi>;
+    // variant = lanes per block row, + 100 for a register cap that allows 6
+    // resident blocks per SM, + 200 for 8
+    auto k = variant == 8     ? k_spmv_bsr3<double, double, double, 8, 1, Epi>
+             : variant == 16  ? k_spmv_bsr3<double, double, double, 16, 1, Epi>
+             : variant == 132 ? k_spmv_bsr3<double, double, double, 32, 6, Epi>
+             : variant == 232 ? k_spmv_bsr3<double, double, double, 32, 8, Epi>
+             : variant == 116 ? k_spmv_bsr3<double, double, double, 16, 6, Epi>
+             : variant == 216 ? k_spmv_bsr3<double, double, double, 16, 8, Epi>
+             : variant == 108 ? k_spmv_bsr3<double, double, double, 8, 6, Epi>
+             : variant == 208 ? k_spmv_bsr3<double, double, double, 8, 8, Epi>
+                              : k_spmv_bsr3<double, double, double, 32, 1, Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval.p, x, y, st, part, tk);
   } else {
     const Csr &c = m->csr;
@@ -666,9 +674,15 @@ int launch_spmv32(sgpu_matrix m, int format, int variant, const float *x, float 
   unsigned *tk = m->w.counters.p + ticket_slot;
   double *part = m->w.partials.p;
   if (format == 3) {
-    auto k = variant == 8    ? k_spmv_bsr3<float, float, float, 8, Epi>
-             : variant == 16 ? k_spmv_bsr3<float, float, float, 16, Epi>
-                             : k_spmv_bsr3<float, float, float, 32, Epi>;
+    auto k = variant == 8     ? k_spmv_bsr3<float, float, float, 8, 1, Epi>
+             : variant == 16  ? k_spmv_bsr3<float, float, float, 16, 1, Epi>
+             : variant == 132 ? k_spmv_bsr3<float, float, float, 32, 6, Epi>
+             : variant == 232 ? k_spmv_bsr3<float, float, float, 32, 8, Epi>
+             : variant == 116 ? k_spmv_bsr3<float, float, float, 16, 6, Epi>
+             : variant == 216 ? k_spmv_bsr3<float, float, float, 16, 8, Epi>
+             : variant == 108 ? k_spmv_bsr3<float, float, float, 8, 6, Epi>
+             : variant == 208 ? k_spmv_bsr3<float, float, float, 8, 8, Epi>
+                              : k_spmv_bsr3<float, float, float, 32, 1, Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval32s.p, x, y, st, part, tk);
   } else {
     const Csr &c = m->csr;
@@ -738,11 +752,8 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   cudaStream_t s = m->stream;
   struct Cand { int format, variant; };
   std::vector<Cand> cands = {{0, 4}, {0, 8}, {0, 16}, {0, 32}};
-  if (m->bsr.valid) {
-    cands.push_back({3, 32});
-    cands.push_back({3, 16});
-    cands.push_back({3, 8});
-  }
+  if (m->bsr.valid)
+    for (int v : {32, 16, 8, 132, 232, 116, 216, 108, 208}) cands.push_back({3, v});
   // x = 1, y scratch
   const int n = (int)m->n;
   k_fill<<<grid_for_vectors(), TPB, 0, s>>>(n, m->w.t.p, 1.0);

@@ -300,9 +300,9 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
         fh.write("\n".join(lines) + "\n")
 
 
-def write_trfel_deck(mesh: Mesh, path: str, dt: float, nsteps: int, alpha: float = 1.0, ni: int = 20000,
+def write_trfel_deck(mesh: Mesh, path: str, dt: float = 1.0, nsteps: int = 1, alpha: float = 1.0, ni: int = 20000,
                      res: float = 1.0e-20, iv: int = 1, precond: int = 1, rho: float = 1.0,
-                     title: str = "sifel-b200 synthetic transport deck") -> None:
+                     title: str = "sifel-b200 synthetic transport deck", stationary: bool = False) -> None:
     """Write a linear nonstationary heat-conduction TRFEL deck (positional).
 
     Token order as read by probdesct::read (TRFEL/SRC/probdesct.cpp:177-560;
@@ -319,16 +319,21 @@ def write_trfel_deck(mesh: Mesh, path: str, dt: float, nsteps: int, alpha: float
     end = dt * nsteps
     L = [title]
     # mesprt problemtype(nonstationary 60) transmatter(onemedium 1) mednames(heat 1) scale
-    L.append("0\n60\n1\n1\n1.0")
+    L.append(f"0\n{50 if stationary else 60}\n1\n1\n1.0")
     # gradcomp fluxcomp othercomp eqothercomp gravity adaptivity stochastic homog noderenumber advection reaction
     L.append("0\n0\n0\n0\n0\n0\n0\n0\n0\n0\n0")
-    # nonstatsolver trapezoidd(1) alpha; timecontr fixed(0) start end, one important time, constant dt
-    L.append(f"1 {_fmt(alpha)}")
-    L.append(f"0 0.0 {_fmt(end)} 1 {_fmt(end)} 0 {_fmt(dt)}")
-    # timetypeprint, hdbackup, storages, solver, capdiagonalization
-    L.append("1\n0\n11 11")
-    L.append(f"20 {ni} {_fmt(res)} {iv}")
-    L.append(f"{precond}\n0")
+    if stationary:  # conductmatstor, solver (probdesct.cpp:189-196)
+        L.append("11")
+        L.append(f"20 {ni} {_fmt(res)} {iv}")
+        L.append(f"{precond}")
+    else:
+        # nonstatsolver trapezoidd(1) alpha; timecontr fixed(0) start end, one important time, constant dt
+        L.append(f"1 {_fmt(alpha)}")
+        L.append(f"0 0.0 {_fmt(end)} 1 {_fmt(end)} 0 {_fmt(dt)}")
+        # timetypeprint, hdbackup, storages, solver, capdiagonalization
+        L.append("1\n0\n11 11")
+        L.append(f"20 {ni} {_fmt(res)} {iv}")
+        L.append(f"{precond}\n0")
     L.append(f"{mesh.nn}")
     for i, (x, y, z) in enumerate(mesh.coords):
         L.append(f"{i + 1} {_fmt(x)} {_fmt(y)} {_fmt(z)} 1 0")
@@ -355,13 +360,14 @@ def write_trfel_deck(mesh: Mesh, path: str, dt: float, nsteps: int, alpha: float
     # one load case: prescribed values, no sources / element loads / nodal values / climatic conditions
     L.append("1")
     L.append(f"{len(values)}")
-    for v in values:
-        L.append(f"{_fmt(v)} 0 {_fmt(v)}")
+    for v in values:  # pvalt::read: initial value, then (nonstationary) a constant time function
+        L.append(f"{_fmt(v)} {_fmt(v)}" if stationary else f"{_fmt(v)} 0 {_fmt(v)}")
     L.append("0\n0\n0\n0\n0\n0")  # nqs neb nnv ncc ncc2 nmultfunc
     L.append("0")  # boundary fluxes: neb
-    for i in range(mesh.nn):  # initial values
-        L.append(f"{i + 1} 0.0")
-    L.append("0\n0\n0")  # textout outgr_format numdiag
+    if not stationary:
+        for i in range(mesh.nn):  # initial values (lhsrhst::initcond)
+            L.append(f"{i + 1} 0.0")
+    L.append("0\n0" if stationary else "0\n0\n0")  # textout outgr_format [numdiag]
     with open(path, "w") as fh:
         fh.write("\n".join(L) + "\n")
 

@@ -155,3 +155,17 @@ def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True):
         return xs, out
     finally:
         K.close()
+
+
+def solve_stationary_problem(mesh, ni=100000, res=1e-20, zero=1e-30, mode="fp64", rnode=None):
+    """solve_stationary_problem (TRFEL/SRC/spsolvert.cpp:13) on the GPU:
+    conductivity matrix assembled on the device, the lifting of the
+    prescribed values as right-hand side, Jacobi-PCG."""
+    K = conductivity_matrix(mesh)
+    try:
+        if rnode is None:
+            rnode = mesh.meta["prescribed"][:, 0]
+        rhs = trfel_lift(K, rnode)
+        return K.pcg(rhs, ni=ni, res=res, zero=zero, crit="scr", prec=1, mode=mode)
+    finally:
+        K.close()

@@ -102,6 +102,15 @@ def main(big=False):
                         C_adr=d3["C_adr"], C_ci=d3["C_ci"], C_a=d3["C_a"], T1=d1["T"], V1=d1["V"], T3=d3["T"],
                         V3=d3["V"], ani3=d3["meta"]["ani"], dt=10.0)
 
+    # TRFEL stationary conduction on the same kind of cube (solve_stationary_problem)
+    cube_s = decks.heat_cube(4, seed=3)
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "st.in")
+        decks.write_trfel_deck(cube_s, deck, stationary=True)
+        ds = O.run_trfel_dump(deck, td)
+    np.savez_compressed(os.path.join(HERE, "trfel_stationary.npz"), K_a=ds["K_a"], T=ds["T"], ani=ds["meta"]["ani"],
+                        ares=ds["meta"]["ares"])
+
     for (nx, ny, nz), key in (((100, 20, 20), "cantilever_100x20x20"),) + (
             (((200, 40, 40), "cantilever_200x40x40"),) if big else ()):
         d = run(decks.cantilever_hex(nx, ny, nz), key)

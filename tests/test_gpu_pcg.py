@@ -121,7 +121,8 @@ def test_linear_statics_end_to_end(oracle, gpu_lib):
     assert np.linalg.norm(X[0] - xo) / np.linalg.norm(xo) <= 1e-8
 
 
-@pytest.mark.parametrize("fmt,variant", [(0, 4), (0, 8), (0, 16), (0, 32), (3, 8), (3, 16), (3, 32)])
+@pytest.mark.parametrize("fmt,variant", [(0, 4), (0, 8), (0, 16), (0, 32), (3, 8), (3, 16), (3, 32), (3, 132),
+                                         (3, 232), (3, 116), (3, 216), (3, 108), (3, 208)])
 def test_every_spmv_kernel_fp64(oracle, gpu_lib, fmt, variant):
     m, adr, ci, a, f = _system(oracle, nx=12, ny=3, nz=3)
     b = np.random.default_rng(7).standard_normal(adr.size - 1)
@@ -132,7 +133,8 @@ def test_every_spmv_kernel_fp64(oracle, gpu_lib, fmt, variant):
     assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("fmt,variant", [(0, 4), (0, 8), (0, 16), (0, 32), (3, 8), (3, 16), (3, 32)])
+@pytest.mark.parametrize("fmt,variant", [(0, 4), (0, 8), (0, 16), (0, 32), (3, 8), (3, 16), (3, 32), (3, 132),
+                                         (3, 232), (3, 116), (3, 216), (3, 108), (3, 208)])
 def test_every_spmv_kernel_fp32_scaled(oracle, gpu_lib, fmt, variant):
     import ctypes
     import torch

@@ -48,3 +48,14 @@ def test_transient_mixed_form(oracle, gpu_lib):
     d_o, _, _ = oracle.trfel_steps(m, 2, 10.0, res=1e-24, iv=1)
     d, _, _, info = mefel.linear_nonstat_solv_dform(m, 2, 10.0, res=1e-20, iv=1, mode="mixed")
     assert np.linalg.norm(d - d_o) / np.linalg.norm(d_o) <= 1e-7
+
+
+def test_stationary_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    from ssf_b200 import _lib as L
+    m = _cube(6, seed=8)
+    xo, st, ani_o, _ = oracle.trfel_stationary(m)
+    assert st == 0
+    x, r = mefel.solve_stationary_problem(m)
+    assert r.status == L.OK and abs(r.ani - ani_o) <= 2
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8

@@ -125,3 +125,14 @@ def test_trfel_cube_matrices_and_steps(oracle):
     T3, V3, its = oracle.trfel_steps(m, 3, float(g["dt"]), iv=1)
     assert np.array_equal(T3, g["T3"]) and np.array_equal(V3, g["V3"])
     assert its[-1][1] == int(g["ani3"])
+
+
+def test_trfel_stationary(oracle):
+    """solve_stationary_problem (TRFEL/SRC/spsolvert.cpp:13): bit-exact."""
+    g = load("trfel_stationary.npz")
+    m = decks.heat_cube(4, seed=3)
+    _, _, ka = oracle.assemble(m, sym=True, kind="hex8t_k")
+    assert np.array_equal(ka, g["K_a"])
+    x, st, ani, ares = oracle.trfel_stationary(m)
+    assert st == 0 and ani == int(g["ani"]) and ares == float(g["ares"])
+    assert np.array_equal(x, g["T"])
