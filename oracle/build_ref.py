@@ -17,7 +17,11 @@ lists; their build system is not run) and writes every output under
 * ``libsifelref.so``                   -- GEFEL compiled position-independent
   plus ``oracle/ref_solver_capi.cpp``: a C entry point into the reference's
   own ``symcomprow::cg_prec`` / ``comprow::cg_prec`` for timing the CPU
-  baseline on exactly the arrays the GPU path receives.
+  baseline on exactly the arrays the GPU path receives;
+* ``mefel_dump_gpu``                   -- the MEFEL harness and SIFEL's objects
+  linked with the drop-in binding ``ssf_b200/integration/sifel_gpu_shim.cpp``
+  (``-Wl,--wrap`` of ``symcomprow::cg_prec``): SIFEL's own front end on a deck,
+  with the solve on the GPU.  Run only by the drop-in test.
 
 Only one compile-environment shim is needed: ``GEFEL/cc.cpp`` includes
 ``umfpack.h`` unconditionally although every use sits under ``INC_CHMD``;
@@ -159,6 +163,26 @@ def build(ref: str, jobs: int) -> None:
     gef_objs = [o for m in GEFEL_PARTS for o in objs[m]]
     run([CXX, "-shared", "-o", os.path.join(OUT, "libsifelref.so"), harness_objs["capi"],
          *gef_objs, "-lm", "-ldl"])
+    build_dropin(ref, harness_objs["mefel"], libmef, libgef, syslibs)
+
+
+WRAP = "_ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver"
+
+
+def build_dropin(ref, harness_obj, libmef, libgef, syslibs):
+    """mefel_dump_gpu: the same harness and SIFEL objects, linked with the
+    drop-in binding (ssf_b200/integration/sifel_gpu_shim.cpp) so that
+    symcomprow::cg_prec runs on the GPU through libsifelgpu.so."""
+    root = os.path.dirname(HERE)
+    lib_dir = os.path.join(root, "ssf_b200")
+    if not os.path.exists(os.path.join(lib_dir, "libsifelgpu.so")):
+        return
+    shim = os.path.join(root, "ssf_b200", "integration", "sifel_gpu_shim.cpp")
+    shim_obj = os.path.join(OUT, "obj", "sifel_gpu_shim.o")
+    run([CXX, *CXXFLAGS, f"-I{os.path.join(ref, 'GEFEL')}", f"-I{os.path.join(ref, 'GEFEL', 'SPARSE')}",
+         f"-I{os.path.join(root, 'include')}", f"-I{os.path.join(HERE, 'ref_compat')}", "-c", shim, "-o", shim_obj])
+    run([CXX, "-o", os.path.join(OUT, "mefel_dump_gpu"), harness_obj, shim_obj, libmef, libgef,
+         f"-Wl,--wrap={WRAP}", f"-L{lib_dir}", "-lsifelgpu", "-Wl,-rpath,$ORIGIN/../../ssf_b200", *syslibs])
 
 
 def main() -> None:

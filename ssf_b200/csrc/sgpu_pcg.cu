@@ -22,11 +22,13 @@
 // residual f - K x is recomputed with the FP64 matrix and replaces the
 // iterated one.  Those FP64 steps (x update, residual, their norms) are the
 // only ones whose stability needs FP64.
+#include <algorithm>
 #include <cfloat>
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
 #include <mutex>
+#include <string>
 #include <unordered_map>
 #include <vector>
 
@@ -745,11 +747,32 @@ int spmv_plan(sgpu_matrix m, int precision, double *bytes, int *format, int *var
 
 // Times every applicable SpMV variant on the handle's matrix (a few
 // repetitions each, CUDA events on the handle's stream) and keeps the fastest.
+namespace {
+// plans already tuned in this process, by matrix shape: a new handle of the
+// same shape (the drop-in entry points make one per call) reuses the choice
+std::mutex g_plan_mu;
+std::unordered_map<std::string, SpmvPlan> g_plans;
+
+std::string plan_key(sgpu_matrix m, int precision) {
+  return std::to_string(precision) + ":" + std::to_string(m->n) + ":" + std::to_string(m->csr.nnz) + ":" +
+         std::to_string(m->bsr.valid ? m->bsr.nblk : -1);
+}
+}  // namespace
+
 int spmv_autotune(sgpu_matrix m, int precision) {
   SGPU_TRY(ensure_work(m, precision == 32));
   SGPU_TRY(ensure_bsr3(m));
   if (precision == 32) SGPU_TRY(ensure_fp32(m));
   cudaStream_t s = m->stream;
+  const std::string key = plan_key(m, precision);
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plans.find(key);
+    if (it != g_plans.end() && !getenv(precision == 64 ? "SGPU_SPMV64" : "SGPU_SPMV32")) {
+      (precision == 64 ? m->plan64 : m->plan32) = it->second;
+      return SGPU_OK;
+    }
+  }
   struct Cand { int format, variant; };
   std::vector<Cand> cands = {{0, 4}, {0, 8}, {0, 16}, {0, 32}};
   if (m->bsr.valid)
@@ -758,25 +781,33 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   const int n = (int)m->n;
   k_fill<<<grid_for_vectors(), TPB, 0, s>>>(n, m->w.t.p, 1.0);
   count_launches(1);
-  float best = FLT_MAX;
-  Cand pick = cands[0];
-  const int reps = 5;
-  for (const Cand &c : cands) {
-    float ms = 0.f;
-    for (int rep = 0; rep < reps + 1; rep++) {
-      if (rep == 1) SGPU_CUDA(cudaEventRecord(m->ev0, s));
-      // with the dot-product epilogue of the iteration's SpMV
-      if (precision == 64)
-        SGPU_TRY(launch_spmv64<EpiDot>(m, c.format, c.variant, m->w.t.p, m->w.p.p, s, 4));
-      else
-        SGPU_TRY(launch_spmv32<EpiDot>(m, c.format, c.variant, reinterpret_cast<const float *>(m->w.t.p),
-                                       m->w.q32.p, s, 4));
+  // two rounds over the candidates, each timed over `reps` launches after one
+  // warm launch; a candidate's time is its better round
+  const int reps = 6;
+  std::vector<float> t(cands.size(), FLT_MAX);
+  for (int round = 0; round < 2; round++) {
+    for (size_t ci = 0; ci < cands.size(); ci++) {
+      const Cand &c = cands[ci];
+      float ms = 0.f;
+      for (int rep = 0; rep < reps + 1; rep++) {
+        if (rep == 1) SGPU_CUDA(cudaEventRecord(m->ev0, s));
+        // with the dot-product epilogue of the iteration's SpMV
+        if (precision == 64)
+          SGPU_TRY(launch_spmv64<EpiDot>(m, c.format, c.variant, m->w.t.p, m->w.p.p, s, 4));
+        else
+          SGPU_TRY(launch_spmv32<EpiDot>(m, c.format, c.variant, reinterpret_cast<const float *>(m->w.t.p),
+                                         m->w.q32.p, s, 4));
+      }
+      SGPU_CUDA(cudaEventRecord(m->ev1, s));
+      SGPU_CUDA(cudaEventSynchronize(m->ev1));
+      SGPU_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+      t[ci] = std::min(t[ci], ms);
     }
-    SGPU_CUDA(cudaEventRecord(m->ev1, s));
-    SGPU_CUDA(cudaEventSynchronize(m->ev1));
-    SGPU_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
-    if (ms < best) { best = ms; pick = c; }
   }
+  size_t bi = 0;
+  for (size_t ci = 1; ci < cands.size(); ci++)
+    if (t[ci] < t[bi]) bi = ci;
+  const Cand pick = cands[bi];
   SpmvPlan &p = precision == 64 ? m->plan64 : m->plan32;
   p.format = pick.format;
   p.variant = pick.variant;
@@ -790,6 +821,9 @@ int spmv_autotune(sgpu_matrix m, int precision) {
       for (const Cand &c : cands)
         if (c.format == f && c.variant == v) { p.format = f; p.variant = v; }
     }
+  } else {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plans[key] = p;
   }
   return SGPU_OK;
 }

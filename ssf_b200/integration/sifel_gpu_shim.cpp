@@ -1,0 +1,50 @@
+// The binding a SIFEL maintainer adds to send GEFEL's Jacobi-PCG to the GPU.
+//
+// It replaces symcomprow::cg_prec (GEFEL/scr.cpp:1093) at link time:
+// linking SIFEL's unchanged objects with
+//   -Wl,--wrap=_ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver
+// makes every call to cg_prec from gmatrix::solve_system (GEFEL/gmatrix.cpp:
+// 1225-1227) land here; the diagonal (Jacobi) case, tprec == 1, goes to
+// sgpu_scr_cg_prec with the storage object's own arrays, every other case to
+// the original routine.  SIFEL_GPU=off keeps the CPU routine, SIFEL_GPU=mixed
+// selects the mixed-precision form.  Decks in SIFEL's input format run
+// unchanged.
+#include <cstdlib>
+#include <cstring>
+
+#include "iotools.h"
+#include "scr.h"
+#include "sifelgpu.h"
+
+extern "C" {
+
+void __real__ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver(symcomprow *self, double *x, double *y, long ni,
+                                                             double res, long &ani, double &ares, double zero,
+                                                             long iv, long tprec, double par, ISolver *sdirect);
+
+void __wrap__ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver(symcomprow *self, double *x, double *y, long ni,
+                                                             double res, long &ani, double &ares, double zero,
+                                                             long iv, long tprec, double par, ISolver *sdirect) {
+  const char *mode_env = getenv("SIFEL_GPU");
+  if (tprec != 1 || (mode_env && !strcmp(mode_env, "off"))) {
+    __real__ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver(self, x, y, ni, res, ani, ares, zero, iv, tprec, par,
+                                                            sdirect);
+    return;
+  }
+  const int mode = (mode_env && !strcmp(mode_env, "mixed")) ? SGPU_MIXED : SGPU_FP64;
+  int64_t a_ni = ani;
+  double a_res = ares;
+  const int st = sgpu_scr_cg_prec(self->n, self->adr, self->ci, self->a, x, y, ni, res, &a_ni, &a_res, zero, iv,
+                                  mode, NULL);
+  ani = (long)a_ni;
+  ares = a_res;
+  // the reference's own messages for the same outcomes (scr.cpp:1117-1151)
+  if (st == SGPU_ZERO_RHS)
+    print_err("right hand side vector has zero norm", __FILE__, __LINE__, __func__);
+  else if (st == SGPU_BREAKDOWN)
+    print_err("denominator in alpha expression is equal to zero", __FILE__, __LINE__, __func__);
+  else if (st != SGPU_OK && st != SGPU_NOT_CONVERGED)
+    print_err("GPU PCG failed: %s", __FILE__, __LINE__, __func__, sgpu_last_error());
+}
+
+}  // extern "C"

@@ -1,0 +1,55 @@
+"""SIFEL's own front end with the GPU solver linked in (the drop-in binding
+of INTEGRATION.md): a deck in SIFEL's input format runs unchanged through the
+compiled reference pipeline; only symcomprow::cg_prec is replaced at link
+time by the C-ABI call.  Compared with the all-CPU reference run."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from ssf_b200 import decks
+
+pytestmark = pytest.mark.gpu
+
+REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+
+def _run(exe, deck, env_extra=None):
+    from oracle import oracle as O
+    td = tempfile.mkdtemp()
+    env = dict(os.environ, **(env_extra or {}))
+    with open(os.path.join(td, "run.log"), "w") as log:
+        subprocess.run([os.path.join(REF, exe), deck, "."], cwd=td, stdout=log, stderr=subprocess.STDOUT,
+                       check=True, env=env, timeout=300)
+    return O.read_dump(td)
+
+
+@pytest.fixture(scope="module")
+def bins(gpu_lib):
+    for exe in ("mefel_dump", "mefel_dump_gpu"):
+        if not os.path.exists(os.path.join(REF, exe)):
+            pytest.fail(f"{exe} not built (python oracle/build_ref.py)")
+    return REF
+
+
+@pytest.mark.parametrize("case", ["cantilever", "plate"])
+def test_unchanged_deck_runs_with_gpu_solver(bins, case):
+    if case == "cantilever":
+        m = decks.cantilever_hex(20, 4, 4)
+    else:
+        m = decks.plate_quad(30, 12, E=3e10, nu=0.22, traction=1e6)
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "deck.in")
+        decks.write_mefel_deck(m, deck)
+        cpu = _run("mefel_dump", deck)
+        gpu = _run("mefel_dump_gpu", deck)
+        off = _run("mefel_dump_gpu", deck, {"SIFEL_GPU": "off"})
+    # the front end produced the same system
+    assert np.array_equal(cpu["K_a"], gpu["K_a"]) and np.array_equal(cpu["f"], gpu["f"])
+    u_c, u_g = cpu["u"], gpu["u"]
+    assert np.linalg.norm(u_g - u_c) / np.linalg.norm(u_c) <= 1e-8
+    assert abs(gpu["meta"]["ani_0"] - cpu["meta"]["ani_0"]) <= 2
+    # with the GPU switched off the binding calls the reference routine itself
+    assert np.array_equal(off["u"], u_c) and off["meta"]["ani_0"] == cpu["meta"]["ani_0"]
