@@ -311,10 +311,11 @@ def run_ours(args, ws, rank):
         ach = b / (ms * 1e-3) / 1e9
         return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": traffic_from_profiles(f"{kern}:{args.workload}"),
-                "kernel": kern, "bytes_per_launch": b, "ms_per_launch": round(ms, 5),
+                "kernel": kern, "variant": var_of[prec], "bytes_per_launch": b, "ms_per_launch": round(ms, 5),
                 "peak_source": (f"{peak_kind} hbm_gbs, MEASURED_PEAKS.json" if peak_kind == "measured"
                                 else "fallback 6650 GB/s")}
 
+    var_of = {64: var64, 32: var32}
     rec64 = spmv_record(64, ms64, b64, fmt64)
     rec64["csr_fp64_equiv_gbs"] = round(csr64_bytes / (ms64 * 1e-3) / 1e9, 1)
     rec32 = spmv_record(32, ms32, b32, fmt32)

@@ -9,6 +9,7 @@
 // the original routine.  SIFEL_GPU=off keeps the CPU routine, SIFEL_GPU=mixed
 // selects the mixed-precision form.  Decks in SIFEL's input format run
 // unchanged.
+#include <cerrno>
 #include <cstdlib>
 #include <cstring>
 
@@ -34,8 +35,13 @@ void __wrap__ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver(symcomprow *self, d
   const int mode = (mode_env && !strcmp(mode_env, "mixed")) ? SGPU_MIXED : SGPU_FP64;
   int64_t a_ni = ani;
   double a_res = ares;
+  // SIFEL checks errno after the solve (check_math_err, GEFEL/mathem.cpp:1725)
+  // and aborts on any value; the CUDA runtime may leave one behind (e.g. from
+  // probing files while loading the driver), so errno is kept as it was
+  const int saved_errno = errno;
   const int st = sgpu_scr_cg_prec(self->n, self->adr, self->ci, self->a, x, y, ni, res, &a_ni, &a_res, zero, iv,
                                   mode, NULL);
+  errno = saved_errno;
   ani = (long)a_ni;
   ares = a_res;
   // the reference's own messages for the same outcomes (scr.cpp:1117-1151)
