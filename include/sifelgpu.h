@@ -74,7 +74,21 @@ typedef struct {
   int32_t fallback;         /* MIXED: 1 if the FP32 iteration stagnated and the
                                solve was finished in FP64 from its iterate */
   int32_t tile_rows;        /* batched solves: rows per work segment picked by the tuner */
+  double precond_setup_ms;  /* SGPU_PREC_AGG: hierarchy set-up of this call (0 when reused) */
+  int32_t precond_levels;   /* SGPU_PREC_AGG: levels of the hierarchy, the dense one included */
+  int32_t precond_coarse_n; /* SGPU_PREC_AGG: equations of the dense coarsest level */
 } sgpu_solve_info;
+
+/* Preconditioners (the `prec` argument of the sgpu_matrix_pcg* calls).  The
+ * values follow GEFEL's precondtype (GEFEL/galias.h:103). */
+typedef enum {
+  SGPU_PREC_NONE = 0,   /* noprecond */
+  SGPU_PREC_JACOBI = 1, /* diagprec: h = r / diag (scr.cpp:897-904) */
+  SGPU_PREC_AGG = 101   /* boss: aggregation multilevel preconditioner (see
+                           sgpu_matrix_set_nullspace); the iteration becomes a
+                           flexible CG in FP64 whose preconditioner is one
+                           V-cycle, in FP32 for SGPU_MIXED, FP64 for SGPU_FP64 */
+} sgpu_precond;
 
 /* ------------------------------------------------------------------------ */
 /* Drop-in solver entry points (host arrays)                                */
@@ -149,8 +163,8 @@ SGPU_API int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *byt
  * tuning studies; BAD_INPUT if the format is not available for the matrix. */
 SGPU_API int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32_t variant);
 
-/* Jacobi-PCG on a device-resident matrix, host vectors.  crit selects the
- * reference routine whose criterion is kept. */
+/* PCG on a device-resident matrix, host vectors.  crit selects the reference
+ * routine whose criterion is kept; prec is an sgpu_precond value. */
 SGPU_API int sgpu_matrix_pcg(sgpu_matrix m, double *x, const double *f, int64_t ni, double res,
                     double zero, int64_t iv, int32_t crit, int32_t prec, int32_t mode,
                     int64_t *ani, double *ares, sgpu_solve_info *info);
@@ -158,6 +172,16 @@ SGPU_API int sgpu_matrix_pcg(sgpu_matrix m, double *x, const double *f, int64_t 
 SGPU_API int sgpu_matrix_pcg_d(sgpu_matrix m, double *x_d, const double *f_d, int64_t ni, double res,
                       double zero, int64_t iv, int32_t crit, int32_t prec, int32_t mode,
                       int64_t *ani, double *ares, sgpu_solve_info *info);
+
+/* Near-null space of the matrix for the aggregation preconditioner
+ * (SGPU_PREC_AGG), the role the rigid-body modes play in GEFEL's BOSS
+ * aggregator (aggregator::gener_rbm_1/2, GEFEL/aggregator.cpp:638-700): B is
+ * k (<= 6) host vectors of n entries, column after column -- the 6 rigid-body
+ * motions for 3D elasticity, 3 for plane problems, 1 (constants) for
+ * conduction.  Without this call the preconditioner uses one constant vector
+ * per equation of a node (translations only).  Setting it discards a built
+ * hierarchy; new values (sgpu_matrix_update_values) do too. */
+SGPU_API int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B);
 
 /* All load cases at once (solve_linear_statics, MEFEL/SRC/lssolver.cpp:78-80,
  * solves them one after the other): nrhs (<= 128) independent Jacobi-PCG

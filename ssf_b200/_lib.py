@@ -35,6 +35,9 @@ class SolveInfo(C.Structure):
         ("spmv_variant", C.c_int32),
         ("fallback", C.c_int32),
         ("tile_rows", C.c_int32),
+        ("precond_setup_ms", C.c_double),
+        ("precond_levels", C.c_int32),
+        ("precond_coarse_n", C.c_int32),
     ]
 
     def as_dict(self):
@@ -105,6 +108,7 @@ SIGNATURES = {
     "sgpu_matrix_mxv32_d": ([_vp, _vp, _vp], C.c_int),
     "sgpu_matrix_spmv_plan": ([_vp, _i32, C.POINTER(_dbl), C.POINTER(_i32), C.POINTER(_i32)], C.c_int),
     "sgpu_matrix_set_spmv": ([_vp, _i32, _i32, _i32], C.c_int),
+    "sgpu_matrix_set_nullspace": ([_vp, _i32, _pD], C.c_int),
     "sgpu_csr_pcg_noalloc_d": ([_i32, _vp, _vp, _vp, _vp, _vp, _i64, _dbl, _dbl, _i64, _vp, C.POINTER(_i64),
                                 C.POINTER(_dbl), C.POINTER(_i64)], C.c_int),
     "sgpu_assembly_lift": ([_vp, _pD, _pD], C.c_int),

@@ -1,0 +1,1966 @@
+// Aggregation multilevel preconditioner (SGPU_PREC_AGG) and the flexible CG
+// around it.
+//
+// GEFEL's own aggregation preconditioner is the BOSS aggregator
+// (GEFEL/aggregator.cpp; precondtype boss = 101, GEFEL/galias.h:103, set up by
+// precond::initiation, GEFEL/precond.cpp:136-139): node aggregates
+// (aggregator::prepare_tlnagr, aggregator.cpp:220), a tentative prolongator
+// made of the rigid-body modes restricted to each aggregate
+// (gener_rbm_1/gener_rbm_2, aggregator.cpp:638-700), the coarse matrix
+// P^T A P (coarse_matrix, aggregator.cpp:708) and, as the preconditioner
+// itself, a symmetric multiplicative Schwarz sweep over the aggregates with
+// exact local solves (aggregator::boss, aggregator.cpp:1275; the coarse
+// correction of that routine is commented out).  The sweep is sequential over
+// the aggregates and runs one global SpMV per aggregate, so it has no useful
+// GPU form.  This file keeps the ingredients -- aggregates, a near-null-space
+// tentative prolongator, the Galerkin coarse matrix -- and applies them as a
+// multilevel V-cycle:
+//
+// set-up, on the device in FP64, once per matrix values:
+//   * aggregation: a distance-2 maximal independent set of the node graph
+//     (Luby-style rounds over packed (state, hash, index) keys) gives the
+//     roots; a root takes its neighbours, every other node joins an
+//     aggregated neighbour;
+//   * tentative prolongator: per aggregate, a thin QR (modified Gram-Schmidt,
+//     two passes) of the near-null-space rows: Q (b x k per node) and R (the
+//     coarse near-null space);
+//   * Galerkin product A_c = Q^T A Q: every stored block (i, j) adds
+//     Q_i^T A_ij Q_j to the coarse block (agg i, agg j); the blocks are radix
+//     sorted by that key and each run is summed by one warp in a fixed order,
+//     so the coarse matrices are deterministic;
+//   * smoother bound: power iteration on D^-1 A for each level;
+//   * coarsest level: dense inverse, Gauss-Jordan in one CTA.
+// application (FP32 for SGPU_MIXED, FP64 for SGPU_FP64): one V-cycle with
+// Chebyshev smoothing of degree `deg` on [lmax/ratio, 1.1 lmax] of D^-1 A,
+// the SpMV and the Chebyshev update fused in one kernel; level 0 is the
+// Jacobi-scaled matrix S K S (unit diagonal) the mixed Jacobi form uses too.
+//
+// The outer iteration is CG in FP64 on K with the Polak-Ribiere beta
+// (flexible CG: the FP32 preconditioner is not exactly the same linear map at
+// every call); the residual, the solution update, alpha and beta are FP64.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "sgpu_internal.cuh"
+
+namespace sgpu {
+
+// sgpu_pcg.cu
+int pcg_prepare(sgpu_matrix m, bool mixed);
+int spmv64_flex(sgpu_matrix m, const double *x, double *y, cudaStream_t s);
+PcgState *pcg_state(sgpu_matrix m);
+
+namespace {
+
+constexpr int TPB = 256;
+
+// ---------------------------------------------------------------------------
+// deterministic reductions (one partial per block, the last block sums them)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+  __shared__ double sh[NV][TPB / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) v[q] = warp_sum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) sh[q][wid] = v[q];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) v[q] = warp_sum(lane < (int)(blockDim.x >> 5) ? sh[q][lane] : 0.0);
+  }
+}
+
+template <int NV>
+__device__ __forceinline__ bool reduce_grid(double (&v)[NV], double *partials, unsigned *ticket,
+                                            double (&tot)[NV]) {
+  __shared__ bool am_last;
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) partials[(size_t)q * gridDim.x + blockIdx.x] = v[q];
+    __threadfence();
+    am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double s[NV];
+#pragma unroll
+  for (int q = 0; q < NV; q++) s[q] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) s[q] += __ldcg(partials + (size_t)q * gridDim.x + b);
+  }
+  block_sum<NV>(s);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) tot[q] = s[q];
+    *ticket = 0u;
+  }
+  return threadIdx.x == 0;
+}
+
+// Sums the row contributions of an operator with NV > 0 over the grid and lets
+// the last block finish.
+template <class Op>
+__device__ __forceinline__ void op_reduce(double (&acc)[Op::NV > 0 ? Op::NV : 1], PcgState *st,
+                                          double *partials, unsigned *ticket) {
+  if constexpr (Op::NV > 0) {
+    double tot[Op::NV];
+    if (reduce_grid<Op::NV>(acc, partials, ticket, tot)) Op::finish(st, tot);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// row operators: what a level SpMV does with y_i = (A v)_i
+// ---------------------------------------------------------------------------
+template <typename T>
+struct OpResid {  // res = b - A x
+  static constexpr int NV = 0;
+  const T *b;
+  T *res;
+  __device__ void row(int i, T y, double *) const { res[i] = b[i] - y; }
+  __device__ static void finish(PcgState *, const double *) {}
+};
+
+template <typename T>
+struct OpPower {  // y = D^-1 A v / |v| and |y|^2 (power iteration of the set-up)
+  static constexpr int NV = 1;
+  T *out;
+  const T *dinv;
+  const double *vv;  // |v|^2, written by the previous step's last block
+  __device__ void row(int i, T y, double *acc) const {
+    const T v = (T)rsqrt(*vv) * (dinv ? dinv[i] : T(1)) * y;
+    out[i] = v;
+    acc[0] += (double)v * (double)v;
+  }
+  __device__ static void finish(PcgState *st, const double *tot) { st->last_dot = tot[0]; }
+};
+
+// Chebyshev smoothing step fused with its SpMV.
+//   FIRST (SpMV of x_in): r = D^-1 (b - A x_in); d = c2 r; x = x_in + d
+//   else  (SpMV of d_in): r = r - D^-1 A d_in;   d = c1 d_in + c2 r; x += d
+// The last step of a smoothing pass writes x only.  OUTER (level 0, last
+// step of the V-cycle) also forms z = S x in FP64 and the two dot products of
+// the flexible CG, r.z and q.z, whose last block sets rho and beta.
+template <typename T, bool FIRST, bool OUTER>
+struct OpCheb {
+  static constexpr int NV = OUTER ? 2 : 0;
+  const T *b;
+  const T *x_in;
+  T *x;
+  T *r;
+  const T *d_in;
+  T *d_out;
+  const T *dinv;
+  T c1, c2;
+  int last;
+  // outer coupling (level 0): z = S x is formed on the fly for r.z and q.z
+  // (k_fcg_dir forms it again from x)
+  const double *dscale, *r64, *q64;
+  double *unused;
+  __device__ void row(int i, T y, double *acc) const {
+    const T di_ = dinv ? dinv[i] : T(1);
+    T ri, di, xi;
+    if (FIRST) {
+      ri = di_ * (b[i] - y);
+      di = c2 * ri;
+      xi = x_in[i] + di;
+    } else {
+      ri = r[i] - di_ * y;
+      di = c1 * d_in[i] + c2 * ri;
+      xi = x[i] + di;
+    }
+    x[i] = xi;
+    if (!last) {
+      r[i] = ri;
+      d_out[i] = di;
+    }
+    if constexpr (OUTER) {
+      const double z = dscale[i] * (double)xi;
+      acc[0] += z * r64[i];
+      acc[1] += z * q64[i];
+    }
+  }
+  __device__ static void finish(PcgState *st, const double *tot) {
+    const double rz = tot[0], zq = tot[1];
+    if (!(rz > 0.0) || !isfinite(zq)) {  // the preconditioner is SPD: r.z <= 0 is a breakdown
+      if (st->status == 0) st->status = SGPU_BREAKDOWN;
+      st->done = 1;
+      return;
+    }
+    // Polak-Ribiere: beta = z_new.(r_new - r_old) / (r_old.z_old), r_new - r_old = -alpha q
+    st->beta = st->it > st->it_last_update ? -st->alpha * zq / st->rho : 0.0;
+    st->rho_prev = st->rho;
+    st->rho = rz;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// level SpMV kernels: y = A v with a row operator.  Every kernel returns at
+// once when the solve has stopped (graph chunks past convergence are empty).
+// ---------------------------------------------------------------------------
+
+// level 0 in 3x3 block rows, values component-major per block row (as the
+// handle keeps them): LPR lanes per block row
+template <typename T, int LPR, class Op>
+__global__ void __launch_bounds__(TPB, 6) k_lv_bsr3(int nb, const int *__restrict__ browptr,
+                                                   const int *__restrict__ bcol, const T *__restrict__ bval,
+                                                   const T *__restrict__ v, Op op, PcgState *st,
+                                                   double *partials, unsigned *ticket) {
+  if (st->done) return;
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, g = lane / LPR, sub = lane % LPR;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc[Op::NV > 0 ? Op::NV : 1] = {};
+  for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
+    const int br = base + g;
+    int s = 0, nbr = 0;
+    if (br < nb) { s = __ldg(browptr + br); nbr = __ldg(browptr + br + 1) - s; }
+    const T *bv = bval + 9ll * s;
+    T y0 = 0, y1 = 0, y2 = 0;
+    int j = sub;
+    for (; j + LPR < nbr; j += 2 * LPR) {
+      const int j2 = j + LPR;
+      const int c = __ldcs(bcol + s + j), c2 = __ldcs(bcol + s + j2);
+      T a[9], w[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) { a[q] = __ldcs(bv + q * nbr + j); w[q] = __ldcs(bv + q * nbr + j2); }
+      const T x0 = __ldg(v + 3 * c), x1 = __ldg(v + 3 * c + 1), x2 = __ldg(v + 3 * c + 2);
+      const T z0 = __ldg(v + 3 * c2), z1 = __ldg(v + 3 * c2 + 1), z2 = __ldg(v + 3 * c2 + 2);
+      y0 += a[0] * x0 + a[1] * x1 + a[2] * x2 + w[0] * z0 + w[1] * z1 + w[2] * z2;
+      y1 += a[3] * x0 + a[4] * x1 + a[5] * x2 + w[3] * z0 + w[4] * z1 + w[5] * z2;
+      y2 += a[6] * x0 + a[7] * x1 + a[8] * x2 + w[6] * z0 + w[7] * z1 + w[8] * z2;
+    }
+    if (j < nbr) {
+      const int c = __ldcs(bcol + s + j);
+      T a[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) a[q] = __ldcs(bv + q * nbr + j);
+      const T x0 = __ldg(v + 3 * c), x1 = __ldg(v + 3 * c + 1), x2 = __ldg(v + 3 * c + 2);
+      y0 += a[0] * x0 + a[1] * x1 + a[2] * x2;
+      y1 += a[3] * x0 + a[4] * x1 + a[5] * x2;
+      y2 += a[6] * x0 + a[7] * x1 + a[8] * x2;
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      y0 += __shfl_xor_sync(0xffffffffu, y0, o, LPR);
+      y1 += __shfl_xor_sync(0xffffffffu, y1, o, LPR);
+      y2 += __shfl_xor_sync(0xffffffffu, y2, o, LPR);
+    }
+    if (sub < 3 && br < nb) op.row(3 * br + sub, sub == 0 ? y0 : (sub == 1 ? y1 : y2), acc);
+  }
+  op_reduce<Op>(acc, st, partials, ticket);
+}
+
+// level 0 in scalar CSR: L lanes per row
+template <typename T, int L, class Op>
+__global__ void __launch_bounds__(TPB) k_lv_csr(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                const T *__restrict__ val, const T *__restrict__ v, Op op,
+                                                PcgState *st, double *partials, unsigned *ticket) {
+  if (st->done) return;
+  constexpr int GPW = 32 / L;
+  const int lane = threadIdx.x & 31, g = lane / L, sub = lane % L;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc[Op::NV > 0 ? Op::NV : 1] = {};
+  for (int base = warp * GPW; base < n; base += nwarps * GPW) {
+    const int i = base + g;
+    int b = 0, e = 0;
+    if (i < n) { b = __ldg(rowptr + i); e = __ldg(rowptr + i + 1); }
+    T s = 0;
+    for (int k = b + sub; k < e; k += L) s += __ldcs(val + k) * __ldg(v + __ldcs(col + k));
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, L);
+    if (sub == 0 && i < n) op.row(i, s, acc);
+  }
+  op_reduce<Op>(acc, st, partials, ticket);
+}
+
+// coarse levels: B x B blocks stored row-major, one warp per block row
+template <typename T, int B, class Op>
+__global__ void __launch_bounds__(TPB) k_lv_bsrb(int nb, const int *__restrict__ browptr,
+                                                 const int *__restrict__ bcol, const T *__restrict__ bval,
+                                                 const T *__restrict__ v, Op op, PcgState *st, double *partials,
+                                                 unsigned *ticket) {
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc[Op::NV > 0 ? Op::NV : 1] = {};
+  for (int br = warp; br < nb; br += nwarps) {
+    const int s = __ldg(browptr + br), e = __ldg(browptr + br + 1);
+    T y[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) y[c] = 0;
+    for (int k = s + lane; k < e; k += 32) {
+      const int c = __ldg(bcol + k);
+      const T *a = bval + (size_t)k * B * B;
+      T xv[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) xv[q] = __ldg(v + B * c + q);
+#pragma unroll
+      for (int r = 0; r < B; r++) {
+#pragma unroll
+        for (int q = 0; q < B; q++) y[r] += __ldg(a + r * B + q) * xv[q];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < B; r++) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) y[r] += __shfl_xor_sync(0xffffffffu, y[r], o);
+    }
+    if (lane < B) {
+      T yv = y[0];
+#pragma unroll
+      for (int r = 1; r < B; r++)
+        if (lane == r) yv = y[r];
+      op.row(B * br + lane, yv, acc);
+    }
+  }
+  op_reduce<Op>(acc, st, partials, ticket);
+}
+
+// ---------------------------------------------------------------------------
+// transfer kernels
+// ---------------------------------------------------------------------------
+
+// b_c = Q^T res over each aggregate (one warp per aggregate).  With START the
+// coarse level's smoothing starts here from x = 0: r = D^-1 b, d = x = c2 r.
+template <typename T, int B, int K, bool START>
+__global__ void __launch_bounds__(TPB) k_restrict(int na, const int *__restrict__ aggptr,
+                                                  const int *__restrict__ aggnodes, const T *__restrict__ Q,
+                                                  const T *__restrict__ res, T *__restrict__ bc, T *__restrict__ rc,
+                                                  T *__restrict__ dc, T *__restrict__ xc, const T *__restrict__ dinvc,
+                                                  T c2, const PcgState *st) {
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int G = warp; G < na; G += nwarps) {
+    const int s = __ldg(aggptr + G), e = __ldg(aggptr + G + 1);
+    T acc[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) acc[q] = 0;
+    for (int t = s + lane; t < e; t += 32) {
+      const int i = __ldg(aggnodes + t);
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        const T rv = res[B * i + c];
+        const T *qr = Q + ((size_t)B * i + c) * K;
+#pragma unroll
+        for (int q = 0; q < K; q++) acc[q] += __ldg(qr + q) * rv;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    }
+    if (lane < K) {
+      T v = acc[0];
+#pragma unroll
+      for (int q = 1; q < K; q++)
+        if (lane == q) v = acc[q];
+      const int p = K * G + lane;
+      bc[p] = v;
+      if (START) {
+        const T ri = dinvc[p] * v;
+        rc[p] = ri;
+        dc[p] = c2 * ri;
+        xc[p] = c2 * ri;
+      }
+    }
+  }
+}
+
+// x += alpha Q x_c (one thread per equation)
+template <typename T, int B, int K>
+__global__ void __launch_bounds__(TPB) k_prolong(int n, const int *__restrict__ agg, const T *__restrict__ Q,
+                                                 const T *__restrict__ xc, T *__restrict__ x, T alpha,
+                                                 const PcgState *st) {
+  if (st->done) return;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int G = __ldg(agg + p / B);
+    const T *qr = Q + (size_t)p * K;
+    T s = 0;
+#pragma unroll
+    for (int q = 0; q < K; q++) s += __ldg(qr + q) * __ldg(xc + K * G + q);
+    x[p] += alpha * s;
+  }
+}
+
+// x_c = M^-1 b_c with the dense inverse of the coarsest level (warp per row)
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_dense_mv(int nc, const T *__restrict__ M, const T *__restrict__ b,
+                                                  T *__restrict__ x, const PcgState *st) {
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < nc; i += nwarps) {
+    const T *row = M + (size_t)i * nc;
+    T s = 0;
+    for (int j = lane; j < nc; j += 32) s += __ldg(row + j) * __ldg(b + j);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// flexible CG kernels (FP64) and the start of the level-0 smoothing
+// ---------------------------------------------------------------------------
+
+// r = f - K x0 (q holds K x0); f.f and r.r; level-0 right-hand side S r and
+// the first Chebyshev step from zero (unit diagonal: r0 = b0, d0 = x0 = c2 b0)
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_fcg_init(int n, const double *__restrict__ f, const double *__restrict__ q,
+                                                  double *__restrict__ r, const double *__restrict__ dscale,
+                                                  T *__restrict__ b0, T *__restrict__ r0, T *__restrict__ d0,
+                                                  T *__restrict__ x0, T c2, PcgState *st, double *partials,
+                                                  unsigned *ticket) {
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double fi = f[i], ri = fi - q[i];
+    r[i] = ri;
+    v[0] += fi * fi;
+    v[1] += ri * ri;
+    const T bi = (T)(dscale[i] * ri);
+    b0[i] = bi;
+    r0[i] = bi;
+    d0[i] = c2 * bi;
+    x0[i] = c2 * bi;
+  }
+  double t[2];
+  if (reduce_grid<2>(v, partials, ticket, t)) {
+    st->nory = t[0];
+    st->ff = t[0];
+    st->rr = t[1];
+    st->it_last_update = st->it;  // the next V-cycle starts the recurrence: beta = 0
+    st->beta = 0.0;
+    const bool conv = st->crit == SGPU_CRIT_SCR_PREC ? t[1] < st->res * t[0] : t[1] < st->tol2 * t[0];
+    if (t[0] < st->zero) {  // zero right-hand side: x = 0 is the solution
+      st->status = SGPU_ZERO_RHS;
+      st->done = 1;
+    } else if (conv) {
+      st->ani = st->it;
+      st->ares = t[1] / t[0];
+      st->ani_set = 1;
+      st->done = 1;
+    }
+  }
+}
+
+// x += alpha p; r -= alpha q; r.r and the stopping test; then the level-0
+// right-hand side of the next V-cycle and its first Chebyshev step
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_fcg_update(int n, double *__restrict__ x, double *__restrict__ r,
+                                                    const double *__restrict__ p, const double *__restrict__ q,
+                                                    const double *__restrict__ dscale, T *__restrict__ b0,
+                                                    T *__restrict__ r0, T *__restrict__ d0, T *__restrict__ x0, T c2,
+                                                    PcgState *st, double *partials, unsigned *ticket) {
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    const double ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    v[0] += ri * ri;
+    const T bi = (T)(dscale[i] * ri);
+    b0[i] = bi;
+    r0[i] = bi;
+    d0[i] = c2 * bi;
+    x0[i] = c2 * bi;
+  }
+  double t[1];
+  if (reduce_grid<1>(v, partials, ticket, t)) {
+    st->it += 1;
+    st->rr = t[0];
+    const double ff = st->nory;
+    bool conv;
+    if (st->crit == SGPU_CRIT_SCR_PREC) conv = t[0] < st->res * ff;       // (r.r)/(f.f) < res
+    else conv = t[0] < st->tol2 * ff;                                      // sqrt((r.r)/(f.f)) < res
+    if (conv) {
+      st->ani = st->it;
+      st->ares = t[0] / ff;
+      st->ani_set = 1;
+      st->done = 1;
+    } else if (st->it >= st->ni) {
+      st->status = SGPU_NOT_CONVERGED;
+      st->done = 1;
+    }
+  }
+}
+
+// p = z + beta p with z = S x0 (x0: the V-cycle's level-0 result)
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_fcg_dir(int n, double *__restrict__ p, const T *__restrict__ x0,
+                                                 const double *__restrict__ dscale, const PcgState *st) {
+  if (st->done) return;
+  const double beta = st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = dscale[i] * (double)x0[i] + beta * p[i];
+}
+
+// r = f - q (restart of the recurrence on the true residual); r.r
+__global__ void __launch_bounds__(TPB) k_fcg_true(int n, const double *__restrict__ f, const double *__restrict__ q,
+                                                  PcgState *st, double *partials, unsigned *ticket) {
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = f[i] - q[i];
+    v[0] += ri * ri;
+  }
+  double t[1];
+  if (reduce_grid<1>(v, partials, ticket, t)) {
+    st->true_rr = t[0];
+    st->true_rel = st->nory > 0 ? sqrt(t[0] / st->nory) : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// set-up kernels
+// ---------------------------------------------------------------------------
+
+// FP64 values of a level for the set-up.  layout 1: the handle's BSR3
+// (component-major per block row, unscaled), 2: the handle's CSR (unscaled),
+// 0: an owned coarse level (row-major B x B blocks, already scaled).
+struct LevelView {
+  int layout;
+  const int *browptr, *bcol;
+  const double *val;
+  const double *dscale;
+  template <int B>
+  __device__ __forceinline__ double get(int i, int e, int c) const {
+    if (layout == 1) {
+      const int s = browptr[i], nbr = browptr[i + 1] - s;
+      const int j = bcol[e];
+      return val[9ll * s + (int64_t)c * nbr + (e - s)] * dscale[3 * i + c / 3] * dscale[3 * j + c % 3];
+    }
+    if (layout == 2) return val[e] * dscale[i] * dscale[bcol[e]];
+    return val[(size_t)e * B * B + c];
+  }
+};
+
+__global__ void k_block_rows(int nb, const int *__restrict__ browptr, int *__restrict__ rowid) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    for (int e = browptr[i]; e < browptr[i + 1]; e++) rowid[e] = i;
+}
+
+// level-0 scaled FP64 copy for the FP64 V-cycle (same layout as the source);
+// one warp per (block) row, lanes over its entries
+__global__ void k_scale_level0(int nb, int layout, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                               const double *__restrict__ val, const double *__restrict__ dscale,
+                               double *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < nb; i += nwarps) {
+    const int s = browptr[i], e = browptr[i + 1];
+    if (layout == 2) {
+      const double si = dscale[i];
+      for (int k = s + lane; k < e; k += 32) out[k] = val[k] * si * dscale[bcol[k]];
+    } else {
+      const int nbr = e - s;
+      for (int j = lane; j < nbr; j += 32) {
+        const int c = bcol[s + j];
+        for (int comp = 0; comp < 9; comp++) {
+          const int64_t pos = 9ll * s + (int64_t)comp * nbr + j;
+          out[pos] = val[pos] * dscale[3 * i + comp / 3] * dscale[3 * c + comp % 3];
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {  // integer hash (xorshift-multiply)
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// MIS-2 keys: state in the top 2 bits (0 out, 1 undecided, 2 in), then a
+// hash of the index, then the index (ties impossible)
+__device__ __forceinline__ uint64_t mis_key(uint32_t state, uint32_t i) {
+  return ((uint64_t)state << 62) | ((uint64_t)(mix32(i * 2654435761u + 12345u) >> 2) << 32) | i;
+}
+
+// cand == nullptr: every node is a candidate
+__global__ void k_mis_init(int nb, const int *__restrict__ cand, uint64_t *__restrict__ t) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    t[i] = mis_key(cand == nullptr || cand[i] ? 1 : 0, i);
+}
+
+// max of the keys over the closed neighbourhood; with `agg`, only over the
+// subgraph of the nodes not yet aggregated (agg < 0)
+__global__ void k_mis_max(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                          const int *__restrict__ agg, const uint64_t *__restrict__ in, uint64_t *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    uint64_t m = in[i];
+    for (int e = browptr[i]; e < browptr[i + 1]; e++) {
+      const int j = bcol[e];
+      if (agg == nullptr || agg[j] < 0) m = max(m, in[j]);
+    }
+    out[i] = m;
+  }
+}
+
+// second-phase candidates: unaggregated nodes with at least `min_free`
+// unaggregated neighbours
+__global__ void k_mis_cand(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                           const int *__restrict__ agg, int min_free, int *__restrict__ cand) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    int c = 0;
+    if (agg[i] < 0)
+      for (int e = browptr[i]; e < browptr[i + 1]; e++) c += (bcol[e] != i && agg[bcol[e]] < 0);
+    cand[i] = (agg[i] < 0 && c >= min_free) ? 1 : 0;
+  }
+}
+
+__global__ void k_mis_decide(int nb, uint64_t *__restrict__ t, const uint64_t *__restrict__ m2,
+                             int *__restrict__ undecided) {
+  int cnt = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    const uint64_t ti = t[i];
+    if ((ti >> 62) != 1) continue;
+    const uint64_t mi = m2[i];
+    if (mi == ti) t[i] = mis_key(2, i);
+    else if ((mi >> 62) == 2) t[i] = ti & ~(3ull << 62);
+    else cnt++;
+  }
+  if (cnt) atomicAdd(undecided, cnt);
+}
+
+__global__ void k_root_flags(int nb, const uint64_t *__restrict__ t, int *__restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    flag[i] = (t[i] >> 62) == 2 ? 1 : 0;
+}
+
+// an unaggregated root starts aggregate base + rootid; an unaggregated node
+// next to a root joins it (the roots are >= 3 apart: at most one is adjacent)
+__global__ void k_attach_roots(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                               const uint64_t *__restrict__ t, const int *__restrict__ rootid, int base,
+                               int *__restrict__ agg) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    if (agg[i] >= 0) continue;
+    int a = -1;
+    if ((t[i] >> 62) == 2) {
+      a = base + rootid[i];
+    } else {
+      for (int e = browptr[i]; e < browptr[i + 1]; e++) {
+        const int j = bcol[e];
+        if ((t[j] >> 62) == 2) { a = base + rootid[j]; break; }
+      }
+    }
+    agg[i] = a;
+  }
+}
+
+__global__ void k_attach2(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                          const int *__restrict__ agg1, int *__restrict__ agg, int *__restrict__ lost) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    int a = agg1[i];
+    if (a < 0) {
+      for (int e = browptr[i]; e < browptr[i + 1]; e++) {
+        const int j = bcol[e];
+        if (agg1[j] >= 0) { a = agg1[j]; break; }
+      }
+      if (a < 0) atomicAdd(lost, 1);
+    }
+    agg[i] = a;
+  }
+}
+
+__global__ void k_iota(int n, int *__restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+// aggptr from the nodes sorted by aggregate
+__global__ void k_agg_ptr(int nb, int na, const int *__restrict__ sorted_agg, int *__restrict__ aggptr) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    const int a = sorted_agg[t];
+    if (t == 0 || sorted_agg[t - 1] != a) aggptr[a] = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) aggptr[na] = nb;
+}
+
+// level-0 near-null space, Jacobi-scaled and equation-major: B0[p][q] = B[p + q n] / S_p
+// (k0 = 0: one constant per equation of a node, translations)
+__global__ void k_nullspace0(int n, int b, int k0, const double *__restrict__ B, const double *__restrict__ dscale,
+                             double *__restrict__ out, int K) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const double sp = 1.0 / dscale[p];
+    for (int q = 0; q < K; q++)
+      out[(size_t)p * K + q] = (k0 > 0 ? B[p + (size_t)q * n] : (p % b == q ? 1.0 : 0.0)) * sp;
+  }
+}
+
+// Thin QR of the near-null-space rows of each aggregate (one warp per
+// aggregate): modified Gram-Schmidt with a second orthogonalisation pass; a
+// column that (numerically) depends on the previous ones becomes zero.
+// Q (per equation K values) replaces the rows; R is the coarse near-null space.
+template <int B, int K>
+__global__ void __launch_bounds__(TPB) k_tentative(int na, const int *__restrict__ aggptr,
+                                                   const int *__restrict__ aggnodes, const double *__restrict__ Bl,
+                                                   double *__restrict__ Q, double *__restrict__ Bnext) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int G = warp; G < na; G += nwarps) {
+    const int s = __ldg(aggptr + G), e = __ldg(aggptr + G + 1);
+    const int rows = (e - s) * B;
+    auto eq = [&](int r) { return B * __ldg(aggnodes + s + r / B) + r % B; };
+    for (int r = lane; r < rows; r += 32) {
+      const int p = eq(r);
+#pragma unroll
+      for (int q = 0; q < K; q++) Q[(size_t)p * K + q] = Bl[(size_t)p * K + q];
+    }
+    __syncwarp();
+    double R[K][K];
+#pragma unroll
+    for (int a = 0; a < K; a++)
+#pragma unroll
+      for (int c = 0; c < K; c++) R[a][c] = 0.0;
+    bool live[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      double o2 = 0.0;
+      for (int r = lane; r < rows; r += 32) { const double v = Q[(size_t)eq(r) * K + q]; o2 += v * v; }
+      o2 = warp_sum(o2);
+      for (int pass = 0; pass < 2; pass++) {
+#pragma unroll
+        for (int pp = 0; pp < q; pp++) {
+          if (!live[pp]) continue;
+          double dt = 0.0;
+          for (int r = lane; r < rows; r += 32) {
+            const size_t p = (size_t)eq(r) * K;
+            dt += Q[p + pp] * Q[p + q];
+          }
+          dt = warp_sum(dt);
+          R[pp][q] += dt;
+          for (int r = lane; r < rows; r += 32) {
+            const size_t p = (size_t)eq(r) * K;
+            Q[p + q] -= dt * Q[p + pp];
+          }
+          __syncwarp();
+        }
+      }
+      double n2 = 0.0;
+      for (int r = lane; r < rows; r += 32) { const double v = Q[(size_t)eq(r) * K + q]; n2 += v * v; }
+      n2 = warp_sum(n2);
+      const double nrm = sqrt(n2);
+      live[q] = nrm > 1e-10 * sqrt(o2) && nrm > 0.0;
+      R[q][q] = live[q] ? nrm : 0.0;
+      const double inv = live[q] ? 1.0 / nrm : 0.0;
+      for (int r = lane; r < rows; r += 32) Q[(size_t)eq(r) * K + q] *= inv;
+      __syncwarp();
+    }
+    if (lane < K) {
+#pragma unroll
+      for (int a = 0; a < K; a++)
+        if (lane == a) {
+#pragma unroll
+          for (int c = 0; c < K; c++) Bnext[((size_t)G * K + a) * K + c] = live[a] ? R[a][c] : 0.0;
+        }
+    }
+  }
+}
+
+__global__ void k_gal_keys(int64_t nblk, const int *__restrict__ rowid, const int *__restrict__ bcol,
+                           const int *__restrict__ agg, uint64_t *__restrict__ keys, int *__restrict__ idx) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nblk; e += (int64_t)gridDim.x * blockDim.x) {
+    keys[e] = ((uint64_t)(uint32_t)agg[rowid[e]] << 32) | (uint32_t)agg[bcol[e]];
+    idx[e] = (int)e;
+  }
+}
+
+// coarse pattern from the sorted unique keys: block r is (G, H) = key >> 32, key
+__global__ void k_gal_pattern(int nruns, int na, const uint64_t *__restrict__ ukeys, int *__restrict__ browptr,
+                              int *__restrict__ bcol) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nruns; r += gridDim.x * blockDim.x) {
+    const uint64_t k = ukeys[r];
+    const int G = (int)(k >> 32);
+    bcol[r] = (int)(k & 0xffffffffu);
+    if (r == 0 || (int)(ukeys[r - 1] >> 32) != G) browptr[G] = r;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) browptr[na] = nruns;
+}
+
+// A_c(G,H) = sum over the run of Q_i^T A_ij Q_j (one warp per run)
+template <int B, int K>
+__global__ void __launch_bounds__(128) k_galerkin(int nruns, const int *__restrict__ runoff,
+                                                  const int *__restrict__ eidx, const int *__restrict__ rowid,
+                                                  LevelView A, const double *__restrict__ Q, double *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = warp; r < nruns; r += nwarps) {
+    double acc[K * K];
+#pragma unroll
+    for (int t = 0; t < K * K; t++) acc[t] = 0.0;
+    for (int t = runoff[r] + lane; t < runoff[r + 1]; t += 32) {
+      const int e = eidx[t];
+      const int i = rowid[e], j = A.bcol[e];
+      double a[B * B];
+#pragma unroll
+      for (int c = 0; c < B * B; c++) a[c] = A.get<B>(i, e, c);
+      const double *Qi = Q + (size_t)i * B * K, *Qj = Q + (size_t)j * B * K;
+#pragma unroll
+      for (int q2 = 0; q2 < K; q2++) {
+        double tcol[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) {
+          double s = 0.0;
+#pragma unroll
+          for (int c2 = 0; c2 < B; c2++) s += a[c * B + c2] * Qj[c2 * K + q2];
+          tcol[c] = s;
+        }
+#pragma unroll
+        for (int q1 = 0; q1 < K; q1++) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < B; c++) s += Qi[c * K + q1] * tcol[c];
+          acc[q1 * K + q2] += s;
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < K * K; t++) acc[t] = warp_sum(acc[t]);
+#pragma unroll
+    for (int t = 0; t < K * K; t++)
+      if ((t & 31) == lane) out[(size_t)r * K * K + t] = acc[t];
+  }
+}
+
+// 1/diag of a coarse level (0 for a zero diagonal: an equation that a
+// dependent near-null-space column left empty stays 0)
+__global__ void k_coarse_dinv(int na, int K, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                              const double *__restrict__ val, double *__restrict__ dinv64, float *__restrict__ dinv32) {
+  for (int G = blockIdx.x * blockDim.x + threadIdx.x; G < na; G += gridDim.x * blockDim.x) {
+    int rd = -1;
+    for (int e = browptr[G]; e < browptr[G + 1]; e++)
+      if (bcol[e] == G) { rd = e; break; }
+    for (int q = 0; q < K; q++) {
+      const double d = rd >= 0 ? val[(size_t)rd * K * K + q * K + q] : 0.0;
+      const double iv = d > 0.0 ? 1.0 / d : 0.0;
+      dinv64[G * K + q] = iv;
+      dinv32[G * K + q] = (float)iv;
+    }
+  }
+}
+
+__global__ void k_dense_fill(int nb, int K, int nc, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                             const double *__restrict__ val, double *__restrict__ M) {
+  for (int G = blockIdx.x * blockDim.x + threadIdx.x; G < nb; G += gridDim.x * blockDim.x)
+    for (int e = browptr[G]; e < browptr[G + 1]; e++) {
+      const int H = bcol[e];
+      for (int a = 0; a < K; a++)
+        for (int c = 0; c < K; c++) M[(size_t)(G * K + a) * nc + H * K + c] = val[(size_t)e * K * K + a * K + c];
+    }
+}
+
+// Inverse of an SPD matrix by Gauss-Jordan without pivoting, one launch per
+// pivot k, out of place (in -> out) so that no element is read after it has
+// been overwritten:
+//   out[k][k] = 1/p, out[k][j] = a[k][j]/p, out[i][k] = -a[i][k]/p,
+//   out[i][j] = a[i][j] - a[i][k] a[k][j]/p      (p = a[k][k])
+__global__ void k_gj_step(int n, int k, const double *__restrict__ a, double *__restrict__ out) {
+  const double p = 1.0 / a[(size_t)k * n + k];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n * n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t / n), j = (int)(t - (int64_t)i * n);
+    double v;
+    if (i == k) v = (j == k) ? p : a[t] * p;
+    else if (j == k) v = -a[t] * p;
+    else v = a[t] - a[(size_t)i * n + k] * a[(size_t)k * n + j] * p;
+    out[t] = v;
+  }
+}
+
+// an equation with a zero diagonal (a near-null-space column dropped by the
+// QR leaves a zero row and column) gets the identity
+__global__ void k_unit_empty_diag(int n, double *__restrict__ a) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    if (!(a[(size_t)p * n + p] > 0.0)) a[(size_t)p * n + p] = 1.0;
+}
+
+__global__ void k_to32(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+template <typename T>
+__global__ void k_rand_vec(int n, T *__restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i] = (T)((double)(mix32(i + 777u) >> 8) * (2.0 / 16777216.0) - 1.0);
+}
+
+int grid_for(int64_t work, int per_block = TPB) {
+  int64_t g = (work + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > 8 * kNumSMs) g = 8 * kNumSMs;
+  return (int)g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+template <typename T>
+struct LevelVecs {
+  DevBuf<T> b, x, x2, r, d, d2, res;
+  int alloc(size_t n) {
+    SGPU_TRY(b.alloc(n));
+    SGPU_TRY(x.alloc(n));
+    SGPU_TRY(x2.alloc(n));
+    SGPU_TRY(r.alloc(n));
+    SGPU_TRY(d.alloc(n));
+    SGPU_TRY(d2.alloc(n));
+    SGPU_TRY(res.alloc(n));
+    return SGPU_OK;
+  }
+};
+
+struct AmgLevel {
+  int nb = 0, b = 0, n = 0;
+  int64_t nblk = 0;
+  int layout = 0;  // 0 owned row-major blocks, 1 handle BSR3, 2 handle CSR
+  const int *browptr = nullptr, *bcol = nullptr;
+  DevBuf<int> own_browptr, own_bcol;
+  DevBuf<double> val64;  // owned coarse values (FP64), or the level-0 scaled FP64 copy
+  DevBuf<float> val32;   // owned coarse values (FP32)
+  DevBuf<double> dinv64;
+  DevBuf<float> dinv32;
+  bool unit_diag = false;
+  double lmax64 = 0.0, lmax32 = 0.0;
+  // transfer to the next level
+  int na = 0, k = 0;
+  DevBuf<int> agg, aggptr, aggnodes;
+  DevBuf<double> Q64;
+  DevBuf<float> Q32;
+  LevelVecs<double> v64;
+  LevelVecs<float> v32;
+};
+
+struct Amg {
+  int k0 = 0;             // near-null-space vectors given (0: translations)
+  DevBuf<double> B0;      // n x k0 as given
+  bool built = false;     // hierarchy (FP64 set-up) current
+  bool have32 = false;    // FP32 copies current
+  bool have64 = false;    // FP64 level-0 scaled copy current
+  std::vector<AmgLevel *> lv;
+  int nc = 0;             // coarsest (dense) equations
+  DevBuf<double> M64;
+  DevBuf<float> M32;
+  DevBuf<double> cb64, cx64;
+  DevBuf<float> cb32, cx32;
+  // options: Chebyshev degree, coarse-correction weight, smoothing interval
+  // [lmax/ratio, 1.1 lmax], largest dense coarsest level, coarse visits per
+  // level (1: V-cycle, 2: W-cycle), power-iteration steps
+  int deg = 1;
+  double ratio = 30.0, alpha = 1.5;
+  int coarse_max = 768;
+  int gamma = 2;       // visits of level 1 per level-0 cycle
+  int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
+  int power_its = 40;
+  ~Amg() { clear(); }
+  void clear() {
+    for (AmgLevel *l : lv) delete l;
+    lv.clear();
+    built = have32 = have64 = false;
+  }
+};
+
+void amg_free(Amg *a) { delete a; }
+
+void amg_values_changed(sgpu_matrix m) {
+  if (m->amg) m->amg->clear();
+}
+
+int amg_set_nullspace(sgpu_matrix m, int k, const double *B_host) {
+  if (!m->amg) m->amg = new Amg();
+  Amg &A = *m->amg;
+  A.clear();
+  A.k0 = k;
+  SGPU_TRY(A.B0.alloc((size_t)m->n * k));
+  SGPU_CUDA(cudaMemcpyAsync(A.B0.p, B_host, (size_t)m->n * k * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+  SGPU_CUDA(cudaStreamSynchronize(m->stream));
+  return SGPU_OK;
+}
+
+namespace {
+
+// Set-up temporaries: stream-ordered allocations from the device's memory
+// pool (the pool keeps freed memory, so repeated set-ups do not pay for
+// cudaMalloc / cudaFree and their device synchronisation).
+void keep_pool_memory() {
+  static bool done = false;
+  if (done) return;
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done = true;
+}
+
+template <class T>
+struct TmpBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  explicit TmpBuf(cudaStream_t st) : s(st) {}
+  TmpBuf(const TmpBuf &) = delete;
+  TmpBuf &operator=(const TmpBuf &) = delete;
+  ~TmpBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    if (count <= n && p) return SGPU_OK;
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), s);
+    if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    n = count;
+    return SGPU_OK;
+  }
+};
+
+struct CubTmp {
+  TmpBuf<unsigned char> buf;
+  explicit CubTmp(cudaStream_t s) : buf(s) {}
+  int ensure(size_t bytes) { return buf.alloc(bytes); }
+};
+
+int read_int(const int *d, cudaStream_t s, int *out) {
+  SGPU_CUDA(cudaMemcpyAsync(out, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  return SGPU_OK;
+}
+
+// Distance-2 maximal independent set over the candidate nodes (all nodes, or
+// with `agg` the candidates among the unaggregated ones, on their subgraph):
+// on return the roots have state 2 in t.
+int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t, cudaStream_t s) {
+  const int nb = L.nb, g = grid_for(nb);
+  TmpBuf<uint64_t> m1(s), m2(s);
+  TmpBuf<int> cnt(s);
+  SGPU_TRY(m1.alloc(nb));
+  SGPU_TRY(m2.alloc(nb));
+  SGPU_TRY(cnt.alloc(1));
+  k_mis_init<<<g, TPB, 0, s>>>(nb, cand, t.p);
+  count_launches(1);
+  int undecided = nb, rounds = 0;
+  while (undecided > 0) {
+    if (++rounds > 200) return fail(SGPU_CUDA_ERROR, "aggregation: independent-set rounds did not finish");
+    SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), s));
+    // two rounds per check of the undecided count
+    for (int k = 0; k < 2; k++) {
+      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p);
+      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, m2.p);
+      k_mis_decide<<<g, TPB, 0, s>>>(nb, t.p, m2.p, cnt.p);
+      count_launches(3);
+    }
+    SGPU_CUDA(cudaGetLastError());
+    SGPU_TRY(read_int(cnt.p, s, &undecided));
+  }
+  return SGPU_OK;
+}
+
+// numbers the roots of t after `base` and attaches their unaggregated
+// neighbours; returns the number of new aggregates
+int take_roots(const AmgLevel &L, const TmpBuf<uint64_t> &t, int base, int *agg, cudaStream_t s, CubTmp &tmp,
+               int *count) {
+  const int nb = L.nb, g = grid_for(nb);
+  TmpBuf<int> flag(s), rootid(s);
+  SGPU_TRY(flag.alloc(nb));
+  SGPU_TRY(rootid.alloc(nb));
+  k_root_flags<<<g, TPB, 0, s>>>(nb, t.p, flag.p);
+  count_launches(1);
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag.p, rootid.p, nb, s);
+  SGPU_TRY(tmp.ensure(bytes));
+  SGPU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.buf.p, bytes, flag.p, rootid.p, nb, s));
+  int last_id = 0, last_flag = 0;
+  SGPU_TRY(read_int(rootid.p + nb - 1, s, &last_id));
+  SGPU_TRY(read_int(flag.p + nb - 1, s, &last_flag));
+  *count = last_id + last_flag;
+  k_attach_roots<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, t.p, rootid.p, base, agg);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// Aggregation of a level's node graph -> L.agg, L.aggptr, L.aggnodes, L.na.
+//   phase 1: MIS-2 roots over all nodes; a root takes its neighbours;
+//   phase 2: MIS-2 roots among the left-over nodes that still have at least
+//            4 left-over neighbours, on the left-over subgraph; same rule;
+//   phase 3: every node still left joins an aggregated neighbour.
+// Phase 2 keeps the aggregates near the size of a node's neighbourhood (a
+// random MIS-2 alone leaves many distance-2 nodes, which then swell the
+// aggregates and weaken the coarse levels).
+int aggregate(AmgLevel &L, cudaStream_t s, CubTmp &tmp) {
+  const int nb = L.nb, g = grid_for(nb);
+  TmpBuf<uint64_t> t(s);
+  TmpBuf<int> agg1(s), cand(s), cnt(s);
+  SGPU_TRY(t.alloc(nb));
+  SGPU_TRY(agg1.alloc(nb));
+  SGPU_TRY(cand.alloc(nb));
+  SGPU_TRY(cnt.alloc(1));
+  SGPU_CUDA(cudaMemsetAsync(agg1.p, 0xff, (size_t)nb * sizeof(int), s));  // -1: unaggregated
+  SGPU_TRY(mis2(L, nullptr, nullptr, t, s));
+  int na1 = 0, na2 = 0;
+  SGPU_TRY(take_roots(L, t, 0, agg1.p, s, tmp, &na1));
+  k_mis_cand<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg1.p, 4, cand.p);
+  count_launches(1);
+  SGPU_TRY(mis2(L, cand.p, agg1.p, t, s));
+  SGPU_TRY(take_roots(L, t, na1, agg1.p, s, tmp, &na2));
+  L.na = na1 + na2;
+  SGPU_TRY(L.agg.alloc(nb));
+  SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), s));
+  k_attach2<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg1.p, L.agg.p, cnt.p);
+  count_launches(1);
+  int lost = 0;
+  SGPU_TRY(read_int(cnt.p, s, &lost));
+  if (lost) return fail(SGPU_CUDA_ERROR, "aggregation left " + std::to_string(lost) + " nodes unassigned");
+  // node lists per aggregate
+  TmpBuf<int> keys_out(s), ids(s);
+  SGPU_TRY(keys_out.alloc(nb));
+  SGPU_TRY(ids.alloc(nb));
+  SGPU_TRY(L.aggnodes.alloc(nb));
+  SGPU_TRY(L.aggptr.alloc((size_t)L.na + 1));
+  k_iota<<<g, TPB, 0, s>>>(nb, ids.p);
+  count_launches(1);
+  int end_bit = 1;
+  while ((1ll << end_bit) <= L.na) end_bit++;
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, L.agg.p, keys_out.p, ids.p, L.aggnodes.p, nb, 0, end_bit, s);
+  SGPU_TRY(tmp.ensure(bytes));
+  SGPU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.buf.p, bytes, L.agg.p, keys_out.p, ids.p, L.aggnodes.p, nb, 0,
+                                            end_bit, s));
+  k_agg_ptr<<<g, TPB, 0, s>>>(nb, L.na, keys_out.p, L.aggptr.p);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+template <int B, int K>
+void launch_tentative(AmgLevel &L, const double *Bl, double *Bnext, cudaStream_t s) {
+  k_tentative<B, K><<<grid_for((int64_t)L.na * 32), TPB, 0, s>>>(L.na, L.aggptr.p, L.aggnodes.p, Bl, L.Q64.p, Bnext);
+}
+
+template <int B, int K>
+void launch_galerkin(int nruns, const int *runoff, const int *eidx, const int *rowid, const LevelView &A,
+                     const double *Q, double *out, cudaStream_t s) {
+  k_galerkin<B, K><<<grid_for((int64_t)nruns * 32, 128), 128, 0, s>>>(nruns, runoff, eidx, rowid, A, Q, out);
+}
+
+bool bk_supported(int B, int K) {
+  return (B == 3 && K == 6) || (B == 6 && K == 6) || (B == 1 && K == 1) || (B == 1 && K == 3) ||
+         (B == 3 && K == 3) || (B == 1 && K == 6);
+}
+
+int tentative(AmgLevel &L, int K, const double *Bl, double *Bnext, cudaStream_t s) {
+  SGPU_TRY(L.Q64.alloc((size_t)L.n * K));
+  const int B = L.b;
+  if (B == 3 && K == 6) launch_tentative<3, 6>(L, Bl, Bnext, s);
+  else if (B == 6 && K == 6) launch_tentative<6, 6>(L, Bl, Bnext, s);
+  else if (B == 1 && K == 1) launch_tentative<1, 1>(L, Bl, Bnext, s);
+  else if (B == 1 && K == 3) launch_tentative<1, 3>(L, Bl, Bnext, s);
+  else if (B == 3 && K == 3) launch_tentative<3, 3>(L, Bl, Bnext, s);
+  else if (B == 1 && K == 6) launch_tentative<1, 6>(L, Bl, Bnext, s);
+  else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// Galerkin product of level L into a new coarse level C (owned, block size K)
+int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_t s, CubTmp &tmp) {
+  const int64_t nblk = L.nblk;
+  if (nblk >= (int64_t)INT32_MAX) return fail(SGPU_BAD_INPUT, "too many blocks for the aggregation set-up");
+  const int nbk = (int)nblk;
+  TmpBuf<int> rowid(s), idx(s), sidx(s), counts(s), runoff(s), nruns_d(s);
+  TmpBuf<uint64_t> keys(s), skeys(s), ukeys(s);
+  SGPU_TRY(rowid.alloc(nblk));
+  SGPU_TRY(idx.alloc(nblk));
+  SGPU_TRY(sidx.alloc(nblk));
+  SGPU_TRY(keys.alloc(nblk));
+  SGPU_TRY(skeys.alloc(nblk));
+  k_block_rows<<<grid_for(L.nb), TPB, 0, s>>>(L.nb, L.browptr, rowid.p);
+  k_gal_keys<<<grid_for(nblk), TPB, 0, s>>>(nblk, rowid.p, L.bcol, L.agg.p, keys.p, idx.p);
+  count_launches(2);
+  int abits = 1;
+  while ((1ll << abits) <= L.na) abits++;
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, skeys.p, idx.p, sidx.p, nbk, 0, 32 + abits, s);
+  SGPU_TRY(tmp.ensure(bytes));
+  SGPU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.buf.p, bytes, keys.p, skeys.p, idx.p, sidx.p, nbk, 0, 32 + abits, s));
+  keys.release();
+  idx.release();
+  SGPU_TRY(ukeys.alloc(nblk));
+  SGPU_TRY(counts.alloc(nblk + 1));
+  SGPU_TRY(nruns_d.alloc(1));
+  bytes = 0;
+  cub::DeviceRunLengthEncode::Encode(nullptr, bytes, skeys.p, ukeys.p, counts.p, nruns_d.p, nbk, s);
+  SGPU_TRY(tmp.ensure(bytes));
+  SGPU_CUDA(cub::DeviceRunLengthEncode::Encode(tmp.buf.p, bytes, skeys.p, ukeys.p, counts.p, nruns_d.p, nbk, s));
+  int nruns = 0;
+  SGPU_TRY(read_int(nruns_d.p, s, &nruns));
+  SGPU_TRY(runoff.alloc((size_t)nruns + 1));
+  SGPU_CUDA(cudaMemsetAsync(counts.p + nruns, 0, sizeof(int), s));
+  bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, counts.p, runoff.p, nruns + 1, s);
+  SGPU_TRY(tmp.ensure(bytes));
+  SGPU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.buf.p, bytes, counts.p, runoff.p, nruns + 1, s));
+  // coarse level
+  C.nb = L.na;
+  C.b = K;
+  C.n = L.na * K;
+  C.nblk = nruns;
+  C.layout = 0;
+  SGPU_TRY(C.own_browptr.alloc((size_t)C.nb + 1));
+  SGPU_TRY(C.own_bcol.alloc(nruns));
+  SGPU_TRY(C.val64.alloc((size_t)nruns * K * K));
+  C.browptr = C.own_browptr.p;
+  C.bcol = C.own_bcol.p;
+  k_gal_pattern<<<grid_for(nruns), TPB, 0, s>>>(nruns, C.nb, ukeys.p, C.own_browptr.p, C.own_bcol.p);
+  count_launches(1);
+  const int B = L.b;
+  if (B == 3 && K == 6) launch_galerkin<3, 6>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
+  else if (B == 6 && K == 6) launch_galerkin<6, 6>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
+  else if (B == 1 && K == 1) launch_galerkin<1, 1>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
+  else if (B == 1 && K == 3) launch_galerkin<1, 3>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
+  else if (B == 3 && K == 3) launch_galerkin<3, 3>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
+  else if (B == 1 && K == 6) launch_galerkin<1, 6>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
+  else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
+  count_launches(1);
+  SGPU_TRY(C.dinv64.alloc(C.n));
+  SGPU_TRY(C.dinv32.alloc(C.n));
+  k_coarse_dinv<<<grid_for(C.nb), TPB, 0, s>>>(C.nb, K, C.browptr, C.bcol, C.val64.p, C.dinv64.p, C.dinv32.p);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// ----- level SpMV dispatch --------------------------------------------------
+
+template <typename T>
+const T *level_vals(const sgpu_matrix m, const AmgLevel &L);
+template <>
+const float *level_vals<float>(const sgpu_matrix m, const AmgLevel &L) {
+  if (L.layout == 1) return m->bsr.bval32s.p;
+  if (L.layout == 2) return m->csr.val32s.p;
+  return L.val32.p;
+}
+template <>
+const double *level_vals<double>(const sgpu_matrix m, const AmgLevel &L) {
+  return L.val64.p;  // level 0: the scaled FP64 copy; coarse: owned values
+}
+
+template <typename T>
+const T *level_dinv(const AmgLevel &L);
+template <>
+const float *level_dinv<float>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dinv32.p; }
+template <>
+const double *level_dinv<double>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dinv64.p; }
+
+// resident blocks of a kernel, queried once and cached (no query inside a capture)
+template <class K>
+int resident_grid(K kern, int64_t warps_needed) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> cache;
+  int nb = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find((const void *)kern);
+    if (it != cache.end()) {
+      nb = it->second;
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TPB, 0);
+      cache[(const void *)kern] = nb;
+    }
+  }
+  int64_t g = (int64_t)kNumSMs * (nb > 0 ? nb : 4);
+  const int64_t need = (warps_needed * 32 + TPB - 1) / TPB;
+  if (g > need) g = need;
+  if (g > 8192) g = 8192;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// the level-0 lanes per row follow the tuned SpMV of the same precision
+int level0_lanes(const sgpu_matrix m, bool fp32) {
+  const SpmvPlan &p = fp32 ? m->plan32 : m->plan64;
+  int v = p.variant % 100;
+  if (v != 4 && v != 8 && v != 16 && v != 32) v = 8;
+  return v;
+}
+
+template <typename T, class Op>
+int launch_level(sgpu_matrix m, const AmgLevel &L, const T *v, const Op &op, cudaStream_t s, int slot) {
+  PcgState *st = pcg_state(m);
+  double *part = m->w.partials.p;
+  unsigned *tk = m->w.counters.p + slot;
+  const T *val = level_vals<T>(m, L);
+  if (L.layout == 1) {
+    const int lanes = level0_lanes(m, sizeof(T) == 4);
+    if (lanes == 32) {
+      auto k = k_lv_bsr3<T, 32, Op>;
+      k<<<resident_grid(k, L.nb), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    } else if (lanes == 16) {
+      auto k = k_lv_bsr3<T, 16, Op>;
+      k<<<resident_grid(k, (L.nb + 1) / 2), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    } else {
+      auto k = k_lv_bsr3<T, 8, Op>;
+      k<<<resident_grid(k, (L.nb + 3) / 4), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    }
+  } else if (L.layout == 2) {
+    const int lanes = level0_lanes(m, sizeof(T) == 4);
+    if (lanes == 32) {
+      auto k = k_lv_csr<T, 32, Op>;
+      k<<<resident_grid(k, L.nb), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    } else if (lanes == 16) {
+      auto k = k_lv_csr<T, 16, Op>;
+      k<<<resident_grid(k, (L.nb + 1) / 2), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    } else if (lanes == 4) {
+      auto k = k_lv_csr<T, 4, Op>;
+      k<<<resident_grid(k, (L.nb + 7) / 8), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    } else {
+      auto k = k_lv_csr<T, 8, Op>;
+      k<<<resident_grid(k, (L.nb + 3) / 4), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    }
+  } else {
+    switch (L.b) {
+      case 1: { auto k = k_lv_bsrb<T, 1, Op>;
+        k<<<resident_grid(k, L.nb), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk); break; }
+      case 3: { auto k = k_lv_bsrb<T, 3, Op>;
+        k<<<resident_grid(k, L.nb), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk); break; }
+      case 6: { auto k = k_lv_bsrb<T, 6, Op>;
+        k<<<resident_grid(k, L.nb), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk); break; }
+      default:
+        return fail(SGPU_BAD_INPUT, "unsupported coarse block size");
+    }
+  }
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// lmax of D^-1 A by power iteration; every step divides by the previous
+// step's norm on the device, so the host reads once at the end
+template <typename T>
+int power_lmax(sgpu_matrix m, const AmgLevel &L, cudaStream_t s, int its, double *lmax) {
+  TmpBuf<T> v(s), y(s);
+  SGPU_TRY(v.alloc(L.n));
+  SGPU_TRY(y.alloc(L.n));
+  k_rand_vec<T><<<grid_for(L.n), TPB, 0, s>>>(L.n, v.p);
+  count_launches(1);
+  PcgState *st = pcg_state(m);
+  const double v2 = (double)L.n / 3.0;  // E|v|^2 for v uniform in [-1, 1]
+  SGPU_CUDA(cudaMemcpyAsync(&st->last_dot, &v2, sizeof(double), cudaMemcpyHostToDevice, s));
+  for (int it = 0; it < its; it++) {
+    OpPower<T> op{y.p, level_dinv<T>(L), &st->last_dot};
+    SGPU_TRY(launch_level<T>(m, L, v.p, op, s, 5));
+    std::swap(v.p, y.p);
+  }
+  double yy = 0.0;
+  SGPU_CUDA(cudaMemcpyAsync(&yy, &st->last_dot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  if (!(yy > 0.0) || !std::isfinite(yy)) return fail(SGPU_BAD_INPUT, "smoother bound: power iteration failed");
+  *lmax = sqrt(yy);
+  return SGPU_OK;
+}
+
+const char *env_or(const char *name) { return getenv(name); }
+
+// Host-side phase timer of the set-up (SGPU_AMG_VERBOSE only: it synchronises).
+struct PhaseClock {
+  bool on;
+  cudaStream_t s;
+  std::chrono::steady_clock::time_point t0;
+  explicit PhaseClock(cudaStream_t st) : on(getenv("SGPU_AMG_VERBOSE") != nullptr), s(st) {
+    if (on) { cudaStreamSynchronize(s); t0 = std::chrono::steady_clock::now(); }
+  }
+  void mark(const char *what) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "amg set-up %-28s %8.3f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
+
+// Builds the hierarchy (FP64 set-up).
+int amg_build(sgpu_matrix m) {
+  Amg &A = *m->amg;
+  cudaStream_t s = m->stream;
+  A.clear();
+  if (const char *o = env_or("SGPU_AMG")) {  // "deg,alpha,ratio,coarse_max,gamma,power,gamma_deep" (tuning)
+    int deg = A.deg, cmax = A.coarse_max, gam = A.gamma, pw = A.power_its, gd = A.gamma_deep;
+    double al = A.alpha, ra = A.ratio;
+    if (sscanf(o, "%d,%lf,%lf,%d,%d,%d,%d", &deg, &al, &ra, &cmax, &gam, &pw, &gd) >= 1) {
+      A.gamma_deep = std::max(1, std::min(gd, 2));
+      A.deg = std::max(1, std::min(deg, 6));
+      A.alpha = al;
+      A.ratio = ra;
+      A.coarse_max = std::max(16, std::min(cmax, 4096));
+      A.gamma = std::max(1, std::min(gam, 2));
+      A.power_its = std::max(4, std::min(pw, 400));
+    }
+  }
+  SGPU_TRY(ensure_bsr3(m));
+  SGPU_TRY(ensure_fp32(m));  // scaled FP32 level 0 and S = diag^-1/2
+  const int n = (int)m->n;
+  keep_pool_memory();
+  CubTmp tmp(s);
+  PhaseClock clk(s);
+  // level 0
+  AmgLevel *L0 = new AmgLevel();
+  A.lv.push_back(L0);
+  if (m->bsr.valid) {
+    L0->layout = 1;
+    L0->b = 3;
+    L0->nb = m->bsr.nb;
+    L0->browptr = m->bsr.browptr.p;
+    L0->bcol = m->bsr.bcol.p;
+    L0->nblk = m->bsr.nblk;
+  } else {
+    L0->layout = 2;
+    L0->b = 1;
+    L0->nb = n;
+    L0->browptr = m->csr.rowptr.p;
+    L0->bcol = m->csr.col.p;
+    L0->nblk = m->csr.nnz;
+  }
+  L0->n = n;
+  L0->unit_diag = true;
+  const int K = A.k0 > 0 ? A.k0 : L0->b;
+  DevBuf<double> Bcur, Bnext;
+  SGPU_TRY(Bcur.alloc((size_t)n * K));
+  k_nullspace0<<<grid_for(n), TPB, 0, s>>>(n, L0->b, A.k0, A.B0.p, m->csr.dscale.p, Bcur.p, K);
+  count_launches(1);
+  // coarsen
+  for (int level = 0; level < 12; level++) {
+    AmgLevel &L = *A.lv.back();
+    if (!bk_supported(L.b, K)) return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
+    SGPU_TRY(aggregate(L, s, tmp));
+    clk.mark("aggregation");
+    L.k = K;
+    SGPU_TRY(Bnext.alloc((size_t)L.na * K * K));
+    SGPU_TRY(tentative(L, K, Bcur.p, Bnext.p, s));
+    clk.mark("tentative prolongator");
+    AmgLevel *C = new AmgLevel();
+    A.lv.push_back(C);
+    LevelView view{L.layout, L.browptr, L.bcol,
+                   L.layout == 1 ? m->bsr.bval.p : (L.layout == 2 ? m->csr.val.p : L.val64.p), m->csr.dscale.p};
+    SGPU_TRY(galerkin(L, view, *C, K, s, tmp));
+    clk.mark("galerkin product");
+    std::swap(Bcur.p, Bnext.p);
+    std::swap(Bcur.n, Bnext.n);
+    // stop when the next level is small enough for the dense solve, or when
+    // aggregation no longer reduces the size
+    if (C->n <= A.coarse_max || C->nb * 10 > L.nb * 8) break;
+  }
+  AmgLevel *Cl = A.lv.back();
+  if (Cl->n > 4096) return fail(SGPU_BAD_INPUT, "aggregation did not reach a small coarsest level");
+  // coarsest: dense inverse
+  A.nc = Cl->n;
+  SGPU_TRY(A.M64.alloc((size_t)A.nc * A.nc));
+  SGPU_CUDA(cudaMemsetAsync(A.M64.p, 0, (size_t)A.nc * A.nc * sizeof(double), s));
+  k_dense_fill<<<grid_for(Cl->nb), TPB, 0, s>>>(Cl->nb, Cl->b, A.nc, Cl->browptr, Cl->bcol, Cl->val64.p, A.M64.p);
+  k_unit_empty_diag<<<grid_for(A.nc), TPB, 0, s>>>(A.nc, A.M64.p);
+  {
+    TmpBuf<double> other(s);
+    SGPU_TRY(other.alloc((size_t)A.nc * A.nc));
+    double *src = A.M64.p, *dst = other.p;
+    const int g = grid_for((int64_t)A.nc * A.nc);
+    for (int k = 0; k < A.nc; k++) {
+      k_gj_step<<<g, TPB, 0, s>>>(A.nc, k, src, dst);
+      std::swap(src, dst);
+    }
+    if (src != A.M64.p)
+      SGPU_CUDA(cudaMemcpyAsync(A.M64.p, src, (size_t)A.nc * A.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    count_launches(2 + A.nc);
+  }
+  SGPU_CUDA(cudaGetLastError());
+  clk.mark("dense coarsest inverse");
+  // the dense level is not a smoothing level
+  A.lv.pop_back();
+  delete Cl;
+  A.built = true;
+  if (getenv("SGPU_AMG_VERBOSE")) {
+    for (size_t l = 0; l < A.lv.size(); l++) {
+      const AmgLevel &L = *A.lv[l];
+      fprintf(stderr, "amg level %zu: n %d nb %d b %d blocks %lld -> aggregates %d (k %d)\n", l, L.n, L.nb, L.b,
+              (long long)L.nblk, L.na, L.k);
+    }
+    fprintf(stderr, "amg coarsest: %d equations\n", A.nc);
+  }
+  return SGPU_OK;
+}
+
+int amg_prepare_precision(sgpu_matrix m, bool fp32) {
+  Amg &A = *m->amg;
+  cudaStream_t s = m->stream;
+  PhaseClock clk(s);
+  if (fp32 && !A.have32) {
+    for (size_t l = 0; l < A.lv.size(); l++) {
+      AmgLevel &L = *A.lv[l];
+      SGPU_TRY(L.v32.alloc(L.n));
+      SGPU_TRY(L.Q32.alloc((size_t)L.n * L.k));
+      k_to32<<<grid_for((int64_t)L.n * L.k), TPB, 0, s>>>((int64_t)L.n * L.k, L.Q64.p, L.Q32.p);
+      count_launches(1);
+      if (L.layout == 0) {
+        SGPU_TRY(L.val32.alloc((size_t)L.nblk * L.b * L.b));
+        k_to32<<<grid_for((int64_t)L.nblk * L.b * L.b), TPB, 0, s>>>((int64_t)L.nblk * L.b * L.b, L.val64.p,
+                                                                     L.val32.p);
+        count_launches(1);
+      }
+      clk.mark("fp32 copies");
+      SGPU_TRY(power_lmax<float>(m, L, s, A.power_its, &L.lmax32));
+      clk.mark("power iteration");
+      if (getenv("SGPU_AMG_VERBOSE")) fprintf(stderr, "amg level %zu: lmax (fp32) %.6g\n", l, L.lmax32);
+    }
+    SGPU_TRY(A.M32.alloc((size_t)A.nc * A.nc));
+    k_to32<<<grid_for((int64_t)A.nc * A.nc), TPB, 0, s>>>((int64_t)A.nc * A.nc, A.M64.p, A.M32.p);
+    count_launches(1);
+    SGPU_TRY(A.cb32.alloc(A.nc));
+    SGPU_TRY(A.cx32.alloc(A.nc));
+    SGPU_CUDA(cudaGetLastError());
+    A.have32 = true;
+  }
+  if (!fp32 && !A.have64) {
+    for (size_t l = 0; l < A.lv.size(); l++) {
+      AmgLevel &L = *A.lv[l];
+      SGPU_TRY(L.v64.alloc(L.n));
+      if (L.layout != 0) {
+        SGPU_TRY(L.val64.alloc(L.layout == 1 ? (size_t)L.nblk * 9 : (size_t)L.nblk));
+        k_scale_level0<<<grid_for((int64_t)L.nb * 32), TPB, 0, s>>>(L.nb, L.layout, L.browptr, L.bcol,
+                                                      L.layout == 1 ? m->bsr.bval.p : m->csr.val.p,
+                                                      m->csr.dscale.p, L.val64.p);
+        count_launches(1);
+      }
+      clk.mark("fp64 scaled level 0");
+      SGPU_TRY(power_lmax<double>(m, L, s, A.power_its, &L.lmax64));
+      clk.mark("power iteration");
+      if (getenv("SGPU_AMG_VERBOSE")) fprintf(stderr, "amg level %zu: lmax (fp64) %.6g\n", l, L.lmax64);
+    }
+    SGPU_TRY(A.cb64.alloc(A.nc));
+    SGPU_TRY(A.cx64.alloc(A.nc));
+    SGPU_CUDA(cudaGetLastError());
+    A.have64 = true;
+  }
+  return SGPU_OK;
+}
+
+// ----- the V-cycle ------------------------------------------------------------
+
+struct Cheb {
+  double c2_first;             // 1/theta
+  double c1[8], c2[8];         // steps 1..deg-1
+};
+
+Cheb cheb_coeffs(double lmax, double ratio, int deg) {
+  Cheb c{};
+  const double a = lmax / ratio, b = 1.1 * lmax;
+  const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+  c.c2_first = 1.0 / theta;
+  double rho = 1.0 / sigma;
+  for (int k = 1; k < deg && k < 8; k++) {
+    const double rn = 1.0 / (2.0 * sigma - rho);
+    c.c1[k] = rn * rho;
+    c.c2[k] = 2.0 * rn / delta;
+    rho = rn;
+  }
+  return c;
+}
+
+template <typename T>
+LevelVecs<T> &vecs(AmgLevel &L);
+template <>
+LevelVecs<float> &vecs<float>(AmgLevel &L) { return L.v32; }
+template <>
+LevelVecs<double> &vecs<double>(AmgLevel &L) { return L.v64; }
+template <typename T>
+const T *qmat(const AmgLevel &L);
+template <>
+const float *qmat<float>(const AmgLevel &L) { return L.Q32.p; }
+template <>
+const double *qmat<double>(const AmgLevel &L) { return L.Q64.p; }
+
+template <typename T, int B, int K>
+void launch_restrict(const AmgLevel &L, const T *res, T *bc, T *rc, T *dc, T *xc, const T *dinvc, T c2, bool start,
+                     const PcgState *st, cudaStream_t s) {
+  const int g = grid_for((int64_t)L.na * 32);
+  if (start)
+    k_restrict<T, B, K, true><<<g, TPB, 0, s>>>(L.na, L.aggptr.p, L.aggnodes.p, qmat<T>(L), res, bc, rc, dc, xc,
+                                                 dinvc, c2, st);
+  else
+    k_restrict<T, B, K, false><<<g, TPB, 0, s>>>(L.na, L.aggptr.p, L.aggnodes.p, qmat<T>(L), res, bc, rc, dc, xc,
+                                                  dinvc, c2, st);
+}
+
+template <typename T>
+int restrict_level(const AmgLevel &L, const T *res, T *bc, T *rc, T *dc, T *xc, const T *dinvc, T c2, bool start,
+                   const PcgState *st, cudaStream_t s) {
+  const int B = L.b, K = L.k;
+  if (B == 3 && K == 6) launch_restrict<T, 3, 6>(L, res, bc, rc, dc, xc, dinvc, c2, start, st, s);
+  else if (B == 6 && K == 6) launch_restrict<T, 6, 6>(L, res, bc, rc, dc, xc, dinvc, c2, start, st, s);
+  else if (B == 1 && K == 1) launch_restrict<T, 1, 1>(L, res, bc, rc, dc, xc, dinvc, c2, start, st, s);
+  else if (B == 1 && K == 3) launch_restrict<T, 1, 3>(L, res, bc, rc, dc, xc, dinvc, c2, start, st, s);
+  else if (B == 3 && K == 3) launch_restrict<T, 3, 3>(L, res, bc, rc, dc, xc, dinvc, c2, start, st, s);
+  else if (B == 1 && K == 6) launch_restrict<T, 1, 6>(L, res, bc, rc, dc, xc, dinvc, c2, start, st, s);
+  else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+template <typename T>
+int prolong_level(const AmgLevel &L, const T *xc, T *x, T alpha, const PcgState *st, cudaStream_t s) {
+  const int B = L.b, K = L.k, g = grid_for(L.n);
+  if (B == 3 && K == 6) k_prolong<T, 3, 6><<<g, TPB, 0, s>>>(L.n, L.agg.p, qmat<T>(L), xc, x, alpha, st);
+  else if (B == 6 && K == 6) k_prolong<T, 6, 6><<<g, TPB, 0, s>>>(L.n, L.agg.p, qmat<T>(L), xc, x, alpha, st);
+  else if (B == 1 && K == 1) k_prolong<T, 1, 1><<<g, TPB, 0, s>>>(L.n, L.agg.p, qmat<T>(L), xc, x, alpha, st);
+  else if (B == 1 && K == 3) k_prolong<T, 1, 3><<<g, TPB, 0, s>>>(L.n, L.agg.p, qmat<T>(L), xc, x, alpha, st);
+  else if (B == 3 && K == 3) k_prolong<T, 3, 3><<<g, TPB, 0, s>>>(L.n, L.agg.p, qmat<T>(L), xc, x, alpha, st);
+  else if (B == 1 && K == 6) k_prolong<T, 1, 6><<<g, TPB, 0, s>>>(L.n, L.agg.p, qmat<T>(L), xc, x, alpha, st);
+  else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// One smoothing pass after the first step (the first step from x = 0 is
+// fused into whatever produced b).  `x` is the current iterate, `din` the
+// current direction; on return x holds the smoothed iterate.
+template <typename T>
+int cheb_steps(sgpu_matrix m, AmgLevel &L, const Cheb &c, int deg, T *x, T **din, T **dout, bool outer,
+               cudaStream_t s) {
+  LevelVecs<T> &V = vecs<T>(L);
+  Work &w = m->w;
+  for (int k = 1; k < deg; k++) {
+    const bool last = (k == deg - 1);
+    if (outer && last) {
+      OpCheb<T, false, true> op{V.b.p, nullptr, x, V.r.p, *din, *dout, level_dinv<T>(L), (T)c.c1[k], (T)c.c2[k], 1,
+                                m->csr.dscale.p, w.r.p, w.p.p, w.h.p};
+      SGPU_TRY(launch_level<T>(m, L, *din, op, s, 6));
+    } else {
+      OpCheb<T, false, false> op{V.b.p, nullptr, x, V.r.p, *din, *dout, level_dinv<T>(L), (T)c.c1[k], (T)c.c2[k],
+                                 last ? 1 : 0, nullptr, nullptr, nullptr, nullptr};
+      SGPU_TRY(launch_level<T>(m, L, *din, op, s, 0));
+    }
+    std::swap(*din, *dout);
+  }
+  return SGPU_OK;
+}
+
+// One cycle on level l (l = number of smoothing levels: the dense coarsest).
+// With zero_init the first smoothing step from x = 0 was fused into whatever
+// produced b (k_fcg_update / k_fcg_init for level 0, the restriction for the
+// coarser levels); otherwise the cycle starts from xcur[l].  Each level
+// visits the next one `gamma` times (1: V-cycle, 2: W-cycle).  The level-0
+// post-smoothing's last step forms z = S x with r.z and q.z (OpCheb OUTER).
+template <typename T>
+int cycle(sgpu_matrix m, int l, bool zero_init, const std::vector<Cheb> &ch, std::vector<T *> &xcur, cudaStream_t s) {
+  Amg &A = *m->amg;
+  const int nl = (int)A.lv.size();
+  const int deg = A.deg;
+  PcgState *st = pcg_state(m);
+  Work &w = m->w;
+  if (l == nl) {
+    const T *M = sizeof(T) == 4 ? (const T *)A.M32.p : (const T *)A.M64.p;
+    T *cb = sizeof(T) == 4 ? (T *)A.cb32.p : (T *)A.cb64.p;
+    T *cx = sizeof(T) == 4 ? (T *)A.cx32.p : (T *)A.cx64.p;
+    k_dense_mv<T><<<grid_for((int64_t)A.nc * 32), TPB, 0, s>>>(A.nc, M, cb, cx, st);
+    count_launches(1);
+    xcur[l] = cx;
+    return SGPU_OK;
+  }
+  AmgLevel &L = *A.lv[l];
+  LevelVecs<T> &V = vecs<T>(L);
+  T *xp;
+  // pre-smoothing
+  if (zero_init) {
+    xp = V.x.p;
+  } else {
+    T *from = xcur[l], *to = (from == V.x.p) ? V.x2.p : V.x.p;
+    OpCheb<T, true, false> op{V.b.p, from, to, V.r.p, nullptr, V.d.p, level_dinv<T>(L), (T)0, (T)ch[l].c2_first,
+                              deg == 1 ? 1 : 0, nullptr, nullptr, nullptr, nullptr};
+    SGPU_TRY(launch_level<T>(m, L, from, op, s, 0));
+    xp = to;
+  }
+  {
+    T *din = V.d.p, *dout = V.d2.p;
+    SGPU_TRY(cheb_steps<T>(m, L, ch[l], deg, xp, &din, &dout, false, s));
+  }
+  // residual and restriction
+  {
+    OpResid<T> op{V.b.p, V.res.p};
+    SGPU_TRY(launch_level<T>(m, L, xp, op, s, 0));
+  }
+  if (l + 1 < nl) {
+    AmgLevel &C = *A.lv[l + 1];
+    LevelVecs<T> &W = vecs<T>(C);
+    SGPU_TRY(restrict_level<T>(L, V.res.p, W.b.p, W.r.p, W.d.p, W.x.p, level_dinv<T>(C), (T)ch[l + 1].c2_first, true,
+                               st, s));
+  } else {
+    T *cb = sizeof(T) == 4 ? (T *)A.cb32.p : (T *)A.cb64.p;
+    SGPU_TRY(restrict_level<T>(L, V.res.p, cb, nullptr, nullptr, nullptr, nullptr, (T)0, false, st, s));
+  }
+  // coarse correction
+  const int visits = (l + 1 < nl) ? (l == 0 ? A.gamma : A.gamma_deep) : 1;
+  for (int v = 0; v < visits; v++) SGPU_TRY(cycle<T>(m, l + 1, v == 0, ch, xcur, s));
+  SGPU_TRY(prolong_level<T>(L, xcur[l + 1], xp, (T)A.alpha, st, s));
+  // post-smoothing: first step from x (SpMV of x, result in the other buffer)
+  const bool outer = (l == 0);
+  T *to = (xp == V.x.p) ? V.x2.p : V.x.p;
+  if (outer && deg == 1) {
+    OpCheb<T, true, true> op{V.b.p, xp, to, V.r.p, nullptr, V.d.p, level_dinv<T>(L), (T)0, (T)ch[l].c2_first, 1,
+                             m->csr.dscale.p, w.r.p, w.p.p, w.h.p};
+    SGPU_TRY(launch_level<T>(m, L, xp, op, s, 6));
+  } else {
+    OpCheb<T, true, false> op{V.b.p, xp, to, V.r.p, nullptr, V.d.p, level_dinv<T>(L), (T)0, (T)ch[l].c2_first,
+                              deg == 1 ? 1 : 0, nullptr, nullptr, nullptr, nullptr};
+    SGPU_TRY(launch_level<T>(m, L, xp, op, s, 0));
+  }
+  {
+    T *din = V.d.p, *dout = V.d2.p;
+    SGPU_TRY(cheb_steps<T>(m, L, ch[l], deg, to, &din, &dout, outer, s));
+  }
+  xcur[l] = to;
+  return SGPU_OK;
+}
+
+// One preconditioner application followed by p = S x0 + beta p.
+template <typename T>
+int vcycle_dir(sgpu_matrix m, cudaStream_t s) {
+  Amg &A = *m->amg;
+  const int nl = (int)A.lv.size();
+  std::vector<Cheb> ch(nl);
+  for (int l = 0; l < nl; l++)
+    ch[l] = cheb_coeffs(sizeof(T) == 4 ? A.lv[l]->lmax32 : A.lv[l]->lmax64, A.ratio, A.deg);
+  std::vector<T *> xcur(nl + 1, nullptr);
+  SGPU_TRY(cycle<T>(m, 0, true, ch, xcur, s));
+  k_fcg_dir<T><<<grid_for(m->n), TPB, 0, s>>>((int)m->n, m->w.d.p, xcur[0], m->csr.dscale.p, pcg_state(m));
+  count_launches(1);
+  return SGPU_OK;
+}
+
+template <typename T>
+int fcg_update(sgpu_matrix m, cudaStream_t s) {
+  Amg &A = *m->amg;
+  AmgLevel &L0 = *A.lv[0];
+  LevelVecs<T> &V = vecs<T>(L0);
+  Work &w = m->w;
+  const double l0 = sizeof(T) == 4 ? L0.lmax32 : L0.lmax64;
+  const T c2 = (T)cheb_coeffs(l0, A.ratio, A.deg).c2_first;
+  k_fcg_update<T><<<grid_for(m->n), TPB, 0, s>>>((int)m->n, w.x.p, w.r.p, w.d.p, w.p.p, m->csr.dscale.p, V.b.p,
+                                                  V.r.p, V.d.p, V.x.p, c2, pcg_state(m), w.partials.p,
+                                                  w.counters.p + 2);
+  count_launches(1);
+  return SGPU_OK;
+}
+
+template <typename T>
+int fcg_init(sgpu_matrix m, cudaStream_t s) {
+  Amg &A = *m->amg;
+  AmgLevel &L0 = *A.lv[0];
+  LevelVecs<T> &V = vecs<T>(L0);
+  Work &w = m->w;
+  const double l0 = sizeof(T) == 4 ? L0.lmax32 : L0.lmax64;
+  const T c2 = (T)cheb_coeffs(l0, A.ratio, A.deg).c2_first;
+  k_fcg_init<T><<<grid_for(m->n), TPB, 0, s>>>((int)m->n, w.f.p, w.p.p, w.r.p, m->csr.dscale.p, V.b.p, V.r.p, V.d.p,
+                                                V.x.p, c2, pcg_state(m), w.partials.p, w.counters.p + 2);
+  count_launches(1);
+  return SGPU_OK;
+}
+
+int read_st(sgpu_matrix m, PcgState *h) {
+  SGPU_CUDA(cudaMemcpyAsync(h, pcg_state(m), sizeof(PcgState), cudaMemcpyDeviceToHost, m->stream));
+  SGPU_CUDA(cudaStreamSynchronize(m->stream));
+  return SGPU_OK;
+}
+
+int write_st(sgpu_matrix m, const PcgState *h) {
+  SGPU_CUDA(cudaMemcpyAsync(pcg_state(m), h, sizeof(PcgState), cudaMemcpyHostToDevice, m->stream));
+  SGPU_CUDA(cudaStreamSynchronize(m->stream));
+  return SGPU_OK;
+}
+
+template <typename T>
+int capture_chunk(sgpu_matrix m, int iters, cudaGraphExec_t *exec, int64_t *nodes) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int64_t before = sgpu_kernel_launches();
+  cudaGraph_t g;
+  SGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  int rc = SGPU_OK;
+  for (int it = 0; it < iters && rc == SGPU_OK; it++) {
+    rc = spmv64_flex(m, w.d.p, w.p.p, s);
+    if (rc == SGPU_OK) rc = fcg_update<T>(m, s);
+    if (rc == SGPU_OK) rc = vcycle_dir<T>(m, s);
+  }
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc != SGPU_OK) return rc;
+  if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  *nodes = sgpu_kernel_launches() - before;
+  count_launches(-*nodes);  // captured launches run (and are counted) at each replay
+  return SGPU_OK;
+}
+
+// r = f - K x with a fresh V-cycle and p = z: (re)start of the recurrence
+template <typename T>
+int fcg_start(sgpu_matrix m, cudaStream_t s) {
+  Work &w = m->w;
+  SGPU_TRY(spmv64(m, w.x.p, w.p.p, s));
+  SGPU_TRY(fcg_init<T>(m, s));
+  return vcycle_dir<T>(m, s);
+}
+
+template <typename T>
+int fcg_solve(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, PcgState *hs) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  const int n = (int)m->n;
+  PcgState init{};
+  init.ni = ni;
+  init.res = res;
+  init.zero = zero;
+  init.tol2 = res * res;
+  init.crit = crit;
+  init.prec = SGPU_PREC_AGG;
+  SGPU_TRY(write_st(m, &init));
+  if (iv == 0) SGPU_CUDA(cudaMemsetAsync(w.x.p, 0, (size_t)n * sizeof(double), s));
+  SGPU_TRY(fcg_start<T>(m, s));
+  SGPU_TRY(read_st(m, hs));
+  if (hs->done) return SGPU_OK;
+  const int chunk = 8;
+  cudaGraphExec_t exec = nullptr;
+  int64_t nodes = 0;
+  SGPU_TRY(capture_chunk<T>(m, chunk, &exec, &nodes));
+  int rc = SGPU_OK;
+  int restarts = 0;
+  for (;;) {
+    cudaError_t e = cudaGraphLaunch(exec, s);
+    if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
+    count_launches(nodes);
+    rc = read_st(m, hs);
+    if (rc != SGPU_OK) break;
+    if (!hs->done) continue;
+    // converged on the recurrence: with SGPU_CRIT_TRUE the true residual must
+    // agree, else the recurrence restarts from it
+    if (crit != SGPU_CRIT_TRUE || hs->status != 0 || restarts >= 4) break;
+    rc = spmv64(m, w.x.p, w.p.p, s);
+    if (rc != SGPU_OK) break;
+    k_fcg_true<<<grid_for(n), TPB, 0, s>>>(n, w.f.p, w.p.p, pcg_state(m), w.partials.p, w.counters.p + 3);
+    count_launches(1);
+    rc = read_st(m, hs);
+    if (rc != SGPU_OK || hs->true_rel < res) break;
+    restarts++;
+    PcgState t = *hs;
+    t.done = 0;
+    t.ani_set = 0;
+    rc = write_st(m, &t);
+    if (rc == SGPU_OK) rc = fcg_start<T>(m, s);
+    if (rc != SGPU_OK) break;
+  }
+  cudaGraphExecDestroy(exec);
+  return rc;
+}
+
+}  // namespace
+
+int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int mode, int64_t *ani,
+                double *ares, sgpu_solve_info *info) {
+  cudaStream_t s = m->stream;
+  if (!m->csr.diag_positive)
+    return fail(SGPU_BAD_INPUT, "the aggregation preconditioner needs a positive diagonal (Jacobi scaling)");
+  SGPU_TRY(pcg_prepare(m, false));
+  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
+  const bool fp32 = (mode == SGPU_MIXED);
+  if (fp32 && !m->plan32.tuned) SGPU_TRY(spmv_autotune(m, 32));
+  if (!m->amg) m->amg = new Amg();
+  Amg &A = *m->amg;
+  SGPU_CUDA(cudaEventRecord(m->ev0, s));
+  {
+    PcgState zero_st{};
+    SGPU_TRY(write_st(m, &zero_st));  // set-up kernels run with a live state
+  }
+  if (!A.built) SGPU_TRY(amg_build(m));
+  SGPU_TRY(amg_prepare_precision(m, fp32));
+  SGPU_CUDA(cudaEventRecord(m->ev1, s));
+  SGPU_CUDA(cudaEventSynchronize(m->ev1));
+  float setup_ms = 0.f;
+  SGPU_CUDA(cudaEventElapsedTime(&setup_ms, m->ev0, m->ev1));
+  PcgState hs{};
+  SGPU_CUDA(cudaEventRecord(m->ev0, s));
+  int rc = fp32 ? fcg_solve<float>(m, ni, res, zero, iv, crit, &hs) : fcg_solve<double>(m, ni, res, zero, iv, crit, &hs);
+  SGPU_CUDA(cudaEventRecord(m->ev1, s));
+  if (rc != SGPU_OK) return rc;
+  SGPU_CUDA(cudaEventSynchronize(m->ev1));
+  float solve_ms = 0.f;
+  SGPU_CUDA(cudaEventElapsedTime(&solve_ms, m->ev0, m->ev1));
+  // true FP64 residual of the returned x
+  Work &w = m->w;
+  SGPU_TRY(spmv64(m, w.x.p, w.p.p, s));
+  k_fcg_true<<<grid_for(m->n), TPB, 0, s>>>((int)m->n, w.f.p, w.p.p, pcg_state(m), w.partials.p, w.counters.p + 3);
+  count_launches(1);
+  PcgState fin{};
+  SGPU_TRY(read_st(m, &fin));
+  if (hs.ani_set && hs.status == 0) {
+    if (ani) *ani = hs.ani;
+    if (ares) *ares = hs.ares;
+  }
+  if (info) {
+    info->iterations = hs.it;
+    info->refinements = 0;
+    info->rh_over_ff = hs.rho / (hs.nory > 0 ? hs.nory : 1.0);
+    info->crit_value = crit == SGPU_CRIT_SCR_PREC ? hs.rr / (hs.nory > 0 ? hs.nory : 1.0)
+                                                  : sqrt(hs.rr / (hs.nory > 0 ? hs.nory : 1.0));
+    info->true_relres = fin.true_rel;
+    info->solve_ms = solve_ms;
+    info->precond_setup_ms = setup_ms;
+    info->precond_levels = (int32_t)A.lv.size() + 1;
+    info->precond_coarse_n = A.nc;
+    info->spmv_format = m->plan64.format;
+    info->spmv_variant = m->plan64.variant;
+    info->spmv_bytes = 0.0;
+  }
+  return hs.status;
+}
+
+}  // namespace sgpu

@@ -234,6 +234,13 @@ int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32
   return SGPU_OK;
 }
 
+int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B) {
+  if (!m) return fail(SGPU_BAD_INPUT, "null handle");
+  if (k != 1 && k != 3 && k != 6) return fail(SGPU_BAD_INPUT, "the near-null space has 1, 3 or 6 vectors");
+  if (!B) return fail(SGPU_BAD_INPUT, "null near-null space");
+  return amg_set_nullspace(m, k, B);
+}
+
 int sgpu_matrix_pcg(sgpu_matrix m, double *x, const double *f, int64_t ni, double res, double zero, int64_t iv,
                     int32_t crit, int32_t prec, int32_t mode, int64_t *ani, double *ares, sgpu_solve_info *info) {
   if (!m) return fail(SGPU_BAD_INPUT, "null handle");

@@ -86,7 +86,7 @@ struct Bsr3 {
   int nb = 0;          // block rows
   int64_t nblk = 0;    // stored 3x3 blocks
   DevBuf<int> browptr, bcol;
-  DevBuf<double> bval;   // nblk * 9, row-major inside a block
+  DevBuf<double> bval;   // nblk * 9, component-major per block row: bval[9*s + comp*nbr + j]
   DevBuf<float> bval32s; // scaled FP32 copy
   DevBuf<int64_t> csr2bsr;  // CSR entry -> position in bval (for value updates)
   bool valid = false;
@@ -98,6 +98,29 @@ struct SpmvPlan {
   int format = 0;   // 0 CSR, 3 BSR3
   int variant = 0;  // kernel variant id
   bool tuned = false;
+};
+
+// ---------------------------------------------------------------------------
+// device-side solver state (one per handle, in Work::scal)
+// ---------------------------------------------------------------------------
+struct PcgState {
+  // configuration
+  int64_t ni;
+  double res, zero, tol2, delta2;
+  int crit, prec;
+  // FP64 iteration scalars
+  double nory, nom, denom, alpha, beta, rr;
+  // mixed iteration scalars
+  double ff, rho, rho_prev, rr_ref, kappa2, true_rr, true_rel;
+  double sigma;  // scale of the FP32 residual: the first one has unit norm
+  int64_t it, it_last_update, refinements;
+  // outputs in the reference's conventions
+  int64_t ani;
+  double ares;
+  int ani_set;
+  // control
+  int done, pause, status;
+  double last_dot;
 };
 
 // Per-handle scratch vectors of the iteration.
@@ -113,6 +136,10 @@ struct Work {
 
 struct sgpu_assembly_s;  // element data kept by sgpu_assemble (sgpu_assemble.cu)
 void sgpu_free_assembly(sgpu_assembly_s *a);
+namespace sgpu {
+struct Amg;  // aggregation multilevel preconditioner (sgpu_amg.cu)
+void amg_free(Amg *a);
+}  // namespace sgpu
 
 struct sgpu_matrix_s {
   int64_t n = 0;
@@ -129,8 +156,10 @@ struct sgpu_matrix_s {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool values_dirty32 = true;
   sgpu_assembly_s *asm_data = nullptr;
+  sgpu::Amg *amg = nullptr;  // built on first use of SGPU_PREC_AGG
   ~sgpu_matrix_s() {
     if (asm_data) sgpu_free_assembly(asm_data);
+    if (amg) sgpu::amg_free(amg);
   }
 };
 
@@ -148,4 +177,9 @@ int spmv64(sgpu_matrix m, const double *x, double *y, cudaStream_t s);
 int spmv_autotune(sgpu_matrix m, int precision);
 int spmv32(sgpu_matrix m, const float *x, float *y, cudaStream_t s);
 int spmv_plan(sgpu_matrix m, int precision, double *bytes, int *format, int *variant);
+// sgpu_amg.cu
+void amg_values_changed(sgpu_matrix m);
+int amg_set_nullspace(sgpu_matrix m, int k, const double *B_host);
+int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int mode,
+                int64_t *ani, double *ares, sgpu_solve_info *info);
 }  // namespace sgpu

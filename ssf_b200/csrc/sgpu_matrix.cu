@@ -358,6 +358,7 @@ int finish_values(sgpu_matrix m) {
   // still run); Jacobi and the scaled FP32 form refuse it later
   c.diag_positive = (e == 0);
   m->values_dirty32 = true;
+  amg_values_changed(m);
   return SGPU_OK;
 }
 

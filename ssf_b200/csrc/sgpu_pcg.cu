@@ -36,29 +36,6 @@
 
 namespace sgpu {
 
-// ---------------------------------------------------------------------------
-// device-side solver state
-// ---------------------------------------------------------------------------
-struct PcgState {
-  // configuration
-  int64_t ni;
-  double res, zero, tol2, delta2;
-  int crit, prec;
-  // FP64 iteration scalars
-  double nory, nom, denom, alpha, beta, rr;
-  // mixed iteration scalars
-  double ff, rho, rho_prev, rr_ref, kappa2, true_rr, true_rel;
-  double sigma;  // scale of the FP32 residual: the first one has unit norm
-  int64_t it, it_last_update, refinements;
-  // outputs in the reference's conventions
-  int64_t ani;
-  double ares;
-  int ani_set;
-  // control
-  int done, pause, status;
-  double last_dot;
-};
-
 namespace {
 
 constexpr int TPB = 256;
@@ -164,6 +141,27 @@ struct EpiAlpha32 {  // mixed: alpha = rho / (p.q)
     st->denom = pq;
     if (!(pq > 0.0)) {  // S K S is SPD: a non-positive (or NaN) p.q is a breakdown
       st->status = SGPU_BREAKDOWN;
+      st->done = 1;
+      return;
+    }
+    st->alpha = st->rho / pq;
+  }
+};
+
+struct EpiAlphaFlex {  // flexible CG around a multilevel preconditioner: alpha = (r.z) / (p.q)
+  static constexpr bool kDot = true;
+  static constexpr bool kGate = true;
+  __device__ static void finish(PcgState *st, double pq) {
+    st->denom = pq;
+    // K is SPD: a non-positive (or NaN) p.q is a breakdown.  (No absolute
+    // threshold: unlike the reference routines, this iteration has no
+    // counterpart whose exits it must reproduce, and an absolute 1e-30 stops
+    // problems of small physical scale early.)
+    if (!(pq > 0.0)) {
+      st->ani = st->it;
+      st->ares = st->rho;
+      st->ani_set = 1;
+      if (st->status == 0) st->status = SGPU_BREAKDOWN;
       st->done = 1;
       return;
     }
@@ -721,6 +719,13 @@ int spmv64(sgpu_matrix m, const double *x, double *y, cudaStream_t s) {
   return launch_spmv64<EpiNone>(m, m->plan64.format, m->plan64.variant, x, y, s, 0);
 }
 
+// The flexible CG of the multilevel preconditioner (sgpu_amg.cu): q = K p with
+// alpha = (r.z)/(p.q) in the epilogue, skipped once the solve has stopped.
+int spmv64_flex(sgpu_matrix m, const double *x, double *y, cudaStream_t s) {
+  return launch_spmv64<EpiAlphaFlex>(m, m->plan64.format, m->plan64.variant, x, y, s, 1);
+}
+PcgState *pcg_state(sgpu_matrix m) { return state_of(m); }
+
 int spmv32(sgpu_matrix m, const float *x, float *y, cudaStream_t s) {
   SGPU_TRY(ensure_work(m, true));
   if (!m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "scaled operator needs a positive diagonal");
@@ -1075,6 +1080,8 @@ int solve_mixed(sgpu_matrix m, int64_t ni, double tol, double zero, int64_t iv, 
 // Runs one solve on the handle: w.f holds f, w.x holds x0 (iv = 1) and gets x.
 int pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int prec, int mode,
             int64_t *ani, double *ares, sgpu_solve_info *info) {
+  if (prec == SGPU_PREC_AGG) return amg_pcg_run(m, ni, res, zero, iv, crit, mode, ani, ares, info);
+  if (prec != SGPU_PREC_NONE && prec != SGPU_PREC_JACOBI) return fail(SGPU_BAD_INPUT, "unknown preconditioner");
   cudaStream_t s = m->stream;
   PcgState hs{};
   if (prec && !m->csr.diag_positive) return fail(SGPU_BAD_INPUT, "Jacobi preconditioner needs a positive diagonal");

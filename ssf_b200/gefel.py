@@ -122,6 +122,9 @@ class comprow(_Storage):
         return Result(st, ani.value if got else None, ares.value if got else None, info.as_dict())
 
 
+PREC = {"none": 0, "jacobi": 1, "agg": 101}
+
+
 class DeviceMatrix:
     """A matrix held in HBM (handle of the C ABI), created from GEFEL storage."""
 
@@ -189,8 +192,21 @@ class DeviceMatrix:
                                              C.byref(negm)))
         return adr, ci, a
 
+    def set_nullspace(self, B):
+        """Near-null space (n x k, k = 1, 3 or 6) for the aggregation
+        preconditioner, e.g. :func:`ssf_b200.mefel.rigid_body_modes`."""
+        B = np.asarray(B, dtype=np.float64)
+        if B.ndim == 1:
+            B = B[:, None]
+        cols = np.ascontiguousarray(B.T)  # column after column
+        L.check(L.lib().sgpu_matrix_set_nullspace(self.h, cols.shape[0], cols.ravel()))
+
     def pcg(self, f, x=None, ni=100000, res=1e-20, zero=1e-30, crit="scr", prec=1, mode="fp64") -> tuple:
+        """PCG with the criterion of the reference routine ``crit``; ``prec``
+        0 / "none", 1 / "jacobi" or 101 / "agg" (aggregation multilevel
+        preconditioner, flexible CG)."""
         crit_id = {"scr": L.CRIT_SCR_PREC, "cr": L.CRIT_CR_PREC, "true": L.CRIT_TRUE}[crit]
+        prec = PREC.get(prec, prec)
         iv = 0 if x is None else 1
         xx = np.zeros(self.n) if x is None else _f64(x).copy()
         ani, ares = C.c_int64(-1), C.c_double(float("nan"))

@@ -61,6 +61,41 @@ def capacity_matrix(mesh, rho=None) -> DeviceMatrix:
     return _assemble(mesh, "hex8t_c", rho)
 
 
+def rigid_body_modes(mesh) -> np.ndarray:
+    """Near-null space of the mesh's operator in equation order (n x k): the
+    6 rigid-body motions of a 3D elastic body, the 3 of a plane one, or the
+    constant of a conduction problem -- the vectors GEFEL's BOSS aggregator
+    builds per aggregate (aggregator::gener_rbm_1/2, GEFEL/aggregator.cpp:638-700),
+    here for the whole mesh at once (each aggregate's QR restricts them).
+    Coordinates are centred so the rotations are well scaled."""
+    cn = mesh.code_numbers()
+    n = int(cn.max())
+    ndofn = cn.shape[1]
+    xyz = np.asarray(mesh.coords, dtype=np.float64)
+    xyz = xyz - xyz.mean(axis=0)
+    if ndofn == 1:
+        B = np.zeros((n, 1))
+        c = cn[:, 0]
+        B[c[c > 0] - 1, 0] = 1.0
+        return B
+    if ndofn == 2:
+        B = np.zeros((n, 3))
+        x, y = xyz[:, 0], xyz[:, 1]
+        rows = [(1.0, 0.0, -y), (0.0, 1.0, x)]
+    else:
+        B = np.zeros((n, 6))
+        x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+        o = np.zeros_like(x)
+        # translations, then rotations about z, x, y
+        rows = [(1.0, 0.0, 0.0, -y, o, z), (0.0, 1.0, 0.0, x, -z, o), (0.0, 0.0, 1.0, o, y, -x)]
+    for comp in range(ndofn):
+        c = cn[:, comp]
+        keep = c > 0
+        for q, v in enumerate(rows[comp]):
+            B[c[keep] - 1, q] = v[keep] if np.ndim(v) else v
+    return B
+
+
 def mefel_right_hand_side(mesh, lc: int = 0) -> np.ndarray:
     """Nodal forces of load case ``lc`` in equation order."""
     cn = mesh.code_numbers().reshape(-1)

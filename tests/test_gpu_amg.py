@@ -1,0 +1,109 @@
+"""The aggregation multilevel preconditioner (SGPU_PREC_AGG) and the flexible
+CG around it.  The preconditioner changes the iteration, not the system: every
+solve must reach the solution of the reference's own Jacobi-PCG on the same
+inputs (the oracle, solved to a tighter residual) within the tolerance the
+FP64 drop-in meets (1e-8 relative in the solution), in far fewer iterations.
+"""
+import numpy as np
+import pytest
+
+from ssf_b200 import decks, gefel, mefel
+from ssf_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_system(oracle, m, kind=None):
+    adr, ci, a = oracle.assemble(m, sym=True, kind=kind) if kind else oracle.assemble(m, sym=True)
+    return adr, ci, a
+
+
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+@pytest.mark.parametrize("dims,res", [((20, 4, 4), 1e-20), ((40, 8, 8), 1e-22)])
+def test_cantilever_matches_oracle(oracle, gpu_lib, mode, dims, res):
+    m = decks.cantilever_hex(*dims)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, st, ani_jacobi, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    assert st == 0
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x, r = dm.pcg(f, res=res, prec="agg", mode=mode)
+    assert r.status == L.OK
+    assert r.ani == r.info["iterations"]
+    assert r.info["true_relres"] < 3.0 * np.sqrt(res)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+    # the point of the preconditioner: a small fraction of the Jacobi iterations
+    assert r.info["iterations"] * 3 < ani_jacobi
+    assert r.info["precond_levels"] >= 2 and 0 < r.info["precond_coarse_n"] <= 4096
+
+
+def test_plane_stress_plate(oracle, gpu_lib):
+    m = decks.plate_quad(48, 24, E=3e10, nu=0.22)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, st, ani_jacobi, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))  # 3 plane rigid-body modes, scalar CSR level 0
+        x, r = dm.pcg(f, res=1e-22, prec="agg", mode="mixed")
+    assert r.status == L.OK
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+    assert r.info["iterations"] * 4 < ani_jacobi
+
+
+def test_heterogeneous_conduction(oracle, gpu_lib):
+    # lognormal conductivity, scalar problem (near-null space: constants)
+    m = decks.heat_cube(14, sigma=1.0)
+    with mefel.conductivity_matrix(m) as K:
+        adr, ci, a = K.download(symmetric=1)
+    n = adr.size - 1
+    f = np.random.default_rng(7).standard_normal(n)
+    xo, st, ani_jacobi, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(np.ones(n))
+        for mode in ("mixed", "fp64"):
+            x, r = dm.pcg(f, res=1e-22, prec="agg", mode=mode)
+            assert r.status == L.OK
+            assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+            assert r.info["iterations"] * 3 < ani_jacobi
+
+
+def test_translations_only_and_true_criterion(oracle, gpu_lib):
+    # no near-null space given: one constant per node component
+    m = decks.cantilever_hex(30, 6, 6)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        x, r = dm.pcg(f, res=1e-11, crit="true", prec="agg", mode="mixed")
+    assert r.status == L.OK
+    assert r.info["true_relres"] < 1e-11
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_deterministic_and_values_update(oracle, gpu_lib):
+    m = decks.cantilever_hex(24, 6, 6)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x1, r1 = dm.pcg(f, res=1e-20, prec="agg", mode="mixed")
+        x2, r2 = dm.pcg(f, res=1e-20, prec="agg", mode="mixed")
+        assert np.array_equal(x1, x2) and r1.info["iterations"] == r2.info["iterations"]
+        assert r1.info["precond_setup_ms"] > 0.0 and r2.info["precond_setup_ms"] >= 0.0
+        # new values on the same pattern rebuild the hierarchy: 2 K -> x / 2
+        dm.update_values(2.0 * a)
+        x3, r3 = dm.pcg(f, res=1e-20, prec="agg", mode="mixed")
+        assert r3.status == L.OK
+        assert np.linalg.norm(2.0 * x3 - x1) / np.linalg.norm(x1) <= 1e-8
+        # zero right-hand side
+        x0, r0 = dm.pcg(np.zeros_like(f), res=1e-20, prec="agg", mode="mixed")
+        assert r0.status == L.ZERO_RHS and not np.any(x0)
+
+
+def test_bad_nullspace_rejected(oracle, gpu_lib):
+    m = decks.cantilever_hex(4, 2, 2)
+    adr, ci, a = _oracle_system(oracle, m)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        with pytest.raises(L.SgpuError):
+            dm.set_nullspace(np.ones((adr.size - 1, 2)))
