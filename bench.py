@@ -5,24 +5,33 @@ Workload (one "step" = one full solve): the 3D linear-elastic cantilever
 78.8M CSR entries), E = 210 GPa, nu = 0.3, clamped at x = 0, 1 MPa traction
 in -z on the x = 1 face, 2x2x2 Gauss points.  The mesh is generated; the
 stiffness matrix is assembled on the GPU (untimed set-up), then each step
-solves K u = f from u = 0 to ||f - K u|| / ||f|| < 1e-10 (true FP64
-residual) with the faster of the two GPU forms, picked on one untimed solve:
-the FP64 Jacobi-PCG (the reference's iteration) and the mixed form (FP32
-inner PCG on the Jacobi-scaled matrix with FP64 reliable updates, falling
-back to FP64 when the FP32 iteration stagnates).
+solves K u = f from u = 0 to relative residual 1e-10.  Four GPU forms:
+
+  fp64       the reference's iteration (Jacobi-PCG, symcomprow::cg_prec, its
+             criterion (r.r)/(f.f) < 1e-20), all FP64 -- the drop-in;
+  mixed      FP32 inner Jacobi-PCG on the scaled matrix with FP64 reliable
+             updates (falls back to FP64 when the FP32 iteration stagnates);
+  agg_mixed  FP64 flexible CG, preconditioned by one FP32 W-cycle of the
+             aggregation multilevel preconditioner (GEFEL's precondtype
+             boss = 101); every step rebuilds the hierarchy, so set-up is in
+             the timed region;
+  agg_fp64   the same with an FP64 W-cycle (isolates what FP32 buys).
 
 Reported (one JSON line on rank 0):
-  value         solve time (ms) of the faster form, CUDA events on the
+  value         time per step (ms) of the fastest form, CUDA events on the
                 solve's stream, matrix and vectors resident in HBM; max over
-                ranks; both forms' times, iterations and residuals beside it
-  e2e           the drop-in C-ABI call sgpu_scr_cg_prec with host (pinned)
-                SCR arrays: upload, device format build, solve, download
-  roofline      the SpMV of the timed form (its dominant kernel)
+                ranks; every form's time, iterations and residuals beside it
+  e2e           the same form through the C ABI with host (pinned) arrays:
+                sgpu_scr_cg_prec (drop-in for symcomprow::cg_prec) for the
+                Jacobi forms, sgpu_matrix_create + sgpu_matrix_set_nullspace +
+                sgpu_matrix_pcg for the aggregation forms
+  roofline      the dominant kernel of the timed form (its FP64 SpMV)
   cpu_baseline  SIFEL's own symcomprow::cg_prec (compiled reference) on a
                 bounded sample of iterations of the same system, scaled to
                 the full solve
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--forms all|fp64|mixed|agg_mixed|agg_fp64|jacobi]
 
 With N > 1 (torchrun) every rank solves its own replica (the single system
 has no independent parts to shard without a per-iteration exchange).
@@ -54,7 +63,7 @@ WORKLOADS = {
 }
 # the other benchmark configurations, one JSON line each when asked for
 EXTRA = ("cantilever_100x20x20_64rhs", "heat_cube_128_50steps", "plates_512")
-METRIC = "solve time to relative residual 1e-10 (fastest GPU form; mixed-refined and FP64 PCG both reported)"
+METRIC = "solve time to relative residual 1e-10 (fastest GPU form; mixed and FP64 forms all reported)"
 TOL = 1.0e-10
 # Iterations SIFEL's own Jacobi-PCG (symcomprow::cg_prec, SCR storage,
 # (r.r)/(f.f) < 1e-20) takes on each workload, from full runs of the compiled
@@ -196,6 +205,19 @@ def cpu_reference_time(adr, ci, a, f, workload, sample_iters=20, repeats=1):
 # the GPU arm
 # ----------------------------------------------------------------------------
 
+FORMS = {
+    # name: (preconditioner, arithmetic)
+    "fp64": (1, 0),
+    "mixed": (1, 1),
+    "agg_mixed": (101, 1),
+    "agg_fp64": (101, 0),
+}
+FORM_SETS = {"all": ["fp64", "mixed", "agg_mixed", "agg_fp64"], "jacobi": ["fp64", "mixed"],
+             "fp64": ["fp64"], "mixed": ["mixed"], "agg_mixed": ["agg_mixed"], "agg_fp64": ["agg_fp64"]}
+DTYPE = {"fp64": "f64", "mixed": "f32 inner PCG / f64 refinement",
+         "agg_mixed": "f64 iteration / f32 multilevel preconditioner", "agg_fp64": "f64"}
+
+
 def run_ours(args, ws, rank):
     import torch
     from ssf_b200 import mefel
@@ -203,34 +225,44 @@ def run_ours(args, ws, rank):
     nx, ny, nz = WORKLOADS[args.workload]
     mesh = decks.cantilever_hex(nx, ny, nz)
     f_host = mefel.mefel_right_hand_side(mesh)
+    rbm = mefel.rigid_body_modes(mesh)
+    rbm_cols = np.ascontiguousarray(rbm.T)
     K = mefel.stiffness_matrix(mesh)
     n = K.n
     nnz = K.nnz()
     log(f"[rank {rank}] assembled n={n} nnz={nnz} {K.assembly}")
     stream = torch.cuda.Stream()
     L.check(L.lib().sgpu_matrix_set_stream(K.h, C.c_void_p(stream.cuda_stream)))
+    K.set_nullspace(rbm)
     f_d = torch.from_numpy(f_host).to(dev)
     x_d = torch.zeros(n, dtype=torch.float64, device=dev)
     lib = L.lib()
 
-    def solve(mode):
+    def crit_args(form):
+        # Jacobi FP64: the reference's criterion, (r.r)/(f.f) < 1e-20 on the
+        # recurrence residual; aggregation forms: the same criterion on the
+        # flexible CG's FP64 recurrence; Jacobi mixed: the FP64 residual of
+        # every reliable update < 1e-10.  True residuals are reported.
+        if form == "mixed":
+            return TOL, L.CRIT_TRUE
+        return TOL * TOL, L.CRIT_SCR_PREC
+
+    def solve(form):
+        prec, mode = FORMS[form]
+        if prec == L.PREC_AGG:
+            L.check(lib.sgpu_matrix_precond_clear(K.h))  # set-up inside the step
         info = L.SolveInfo()
         ani, ares = C.c_int64(-1), C.c_double(0.0)
-        # FP64: the reference's criterion, (r.r)/(f.f) < 1e-20 on the recurrence
-        # residual; mixed: the FP64 residual of every reliable update < 1e-10
-        # (true relative residuals of both are reported)
-        fp64 = mode == L.FP64
+        res, crit = crit_args(form)
         st = lib.sgpu_matrix_pcg_d(K.h, C.c_void_p(x_d.data_ptr()), C.c_void_p(f_d.data_ptr()), 200000,
-                                   TOL * TOL if fp64 else TOL, 1e-30, 0,
-                                   L.CRIT_SCR_PREC if fp64 else L.CRIT_TRUE, 1, mode,
-                                   C.byref(ani), C.byref(ares), C.byref(info))
+                                   res, 1e-30, 0, crit, prec, mode, C.byref(ani), C.byref(ares), C.byref(info))
         L.check(st)
         return info
 
-    def timed(mode, steps, warmup):
+    def timed(form, steps, warmup):
         with torch.cuda.stream(stream):
             for _ in range(warmup):
-                solve(mode)
+                solve(form)
             torch.cuda.synchronize()
             barrier(ws)
             torch.cuda.synchronize()
@@ -240,7 +272,7 @@ def run_ours(args, ws, rank):
             infos = []
             e0.record(stream)
             for _ in range(steps):
-                infos.append(solve(mode))
+                infos.append(solve(form))
             e1.record(stream)
             torch.cuda.synchronize()
             barrier(ws)
@@ -248,37 +280,50 @@ def run_ours(args, ws, rank):
         ms = e0.elapsed_time(e1) / steps
         return dist_max(ms, ws), infos, launches
 
-    # pick the faster form on untimed solves (the second of two, so set-up and
-    # autotuning are out of it), then time it
-    forms = {"fp64": [L.FP64], "mixed": [L.MIXED], "both": [L.FP64, L.MIXED]}[args.forms]
+    forms = FORM_SETS[args.forms]
+    # pick the fastest form on untimed solves (the second of two, so module
+    # loading and autotuning are out of it), then time it
     probe = {}
-    for mode in forms:
+    for form in forms:
         for _ in range(2 if len(forms) > 1 else 0):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             with torch.cuda.stream(stream):
-                solve(mode)
+                solve(form)
             torch.cuda.synchronize()
-            probe[mode] = dist_max(time.perf_counter() - t0, ws)  # same choice on every rank
+            probe[form] = dist_max(time.perf_counter() - t0, ws)  # same choice on every rank
     best = min(probe, key=probe.get) if probe else forms[0]
-    other = L.MIXED if best == L.FP64 else L.FP64
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
     ms_best, inf_best, launches = timed(best, args.steps, args.warmup)
     clk = clocks.stop()
-    if len(forms) > 1:
-        ms_other, inf_other, _ = timed(other, max(2, args.steps // 2), 1)
-    else:
-        ms_other, inf_other = float("nan"), [L.SolveInfo()]
-    if best == L.MIXED:
-        ms_mixed, inf_mixed, ms_fp64, inf_fp64 = ms_best, inf_best, ms_other, inf_other
-    else:
-        ms_mixed, inf_mixed, ms_fp64, inf_fp64 = ms_other, inf_other, ms_best, inf_best
-    im, i64 = inf_mixed[-1], inf_fp64[-1]
-    log(f"[rank {rank}] mixed {ms_mixed:.2f} ms {im.as_dict()}")
-    log(f"[rank {rank}] fp64  {ms_fp64:.2f} ms {i64.as_dict()}")
+    results = {best: (ms_best, inf_best[-1])}
+    for form in forms:
+        if form != best:
+            ms_o, inf_o, _ = timed(form, max(2, args.steps // 2), 1)
+            results[form] = (ms_o, inf_o[-1])
+    forms_out = {}
+    for form, (ms, inf) in results.items():
+        d = {"ms_per_step": round(ms, 3), "iterations": inf.iterations, "true_relres": inf.true_relres,
+             "dtype": DTYPE[form]}
+        if FORMS[form][0] == L.PREC_AGG:
+            d.update({"precond_setup_ms": round(inf.precond_setup_ms, 3), "solve_ms": round(inf.solve_ms, 3),
+                      "levels": inf.precond_levels, "coarsest_equations": inf.precond_coarse_n})
+        if form == "mixed":
+            d.update({"refinements": inf.refinements, "fell_back_to_fp64": bool(inf.fallback)})
+        if form == "fp64":
+            d["reference_iterations"] = reference_iterations(args.workload)
+        forms_out[form] = d
+        log(f"[rank {rank}] {form:9s} {ms:9.3f} ms {inf.as_dict()}")
+    if "fp64" in results:
+        for form in results:
+            forms_out[form]["speedup_vs_fp64"] = round(results["fp64"][0] / results[form][0], 3)
+    if "agg_fp64" in results and "agg_mixed" in results:
+        forms_out["agg_mixed"]["speedup_vs_agg_fp64"] = round(results["agg_fp64"][0] / results["agg_mixed"][0], 3)
 
-    # roofline of the dominant kernel: the FP32 SpMV of the mixed iteration
+    # roofline of the dominant kernel: the FP64 SpMV (the iteration's SpMV for
+    # the FP64 forms, the outer flexible CG's SpMV of the aggregation forms);
+    # the FP32 SpMV beside it
     def spmv_time(prec, reps=50):
         """Average launch time of the tuned SpMV kernel alone (CUDA events)."""
         bytes_, fmt, var = C.c_double(), C.c_int32(), C.c_int32()
@@ -305,6 +350,7 @@ def run_ours(args, ws, rank):
     ms64, b64, fmt64, var64 = spmv_time(64)
     csr64_bytes = nnz * 12.0 + (n + 1) * 4.0 + 2.0 * n * 8.0
     fmt_name = {0: "csr", 3: "bsr3"}
+    var_of = {64: var64, 32: var32}
 
     def spmv_record(prec, ms, b, fmt):
         kern = f"spmv_fp{prec}_{fmt_name[fmt]}"
@@ -315,35 +361,44 @@ def run_ours(args, ws, rank):
                 "peak_source": (f"{peak_kind} hbm_gbs, MEASURED_PEAKS.json" if peak_kind == "measured"
                                 else "fallback 6650 GB/s")}
 
-    var_of = {64: var64, 32: var32}
     rec64 = spmv_record(64, ms64, b64, fmt64)
     rec64["csr_fp64_equiv_gbs"] = round(csr64_bytes / (ms64 * 1e-3) / 1e9, 1)
     rec32 = spmv_record(32, ms32, b32, fmt32)
-    # the dominant kernel of the timed form is its SpMV
-    roofline = rec32 if best == L.MIXED else rec64
-    spmv_other = rec64 if best == L.MIXED else rec32
+    roofline = rec32 if best == "mixed" else rec64
+    spmv_other = rec64 if best == "mixed" else rec32
 
     if args.no_e2e:
         K.close()
-        print(json.dumps({"profile_run": True, "value": round(ms_best, 3), "form": args.forms}), flush=True)
+        print(json.dumps({"profile_run": True, "value": round(ms_best, 3), "form": best}), flush=True)
         return
-    # e2e: the drop-in call with host (pinned) SCR arrays
+    # e2e: the same form through the C ABI with host (pinned) arrays
     adr_h, ci_h, a_h = K.download(symmetric=1)
     K.close()
     pin = lambda arr: torch.from_numpy(arr).pin_memory().numpy()  # noqa: E731
     adr_p, ci_p, a_p, f_p = pin(adr_h), pin(ci_h), pin(a_h), pin(f_host)
+    rbm_p = pin(rbm_cols.ravel())
     x_p = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
+    prec_b, mode_b = FORMS[best]
+    res_b, crit_b = crit_args(best)
     e2e_ms = []
     for rep in range(2):
         info = L.SolveInfo()
         ani, ares = C.c_int64(-1), C.c_double(0.0)
         t0 = time.perf_counter()
-        st = lib.sgpu_scr_cg_prec(n, adr_p, ci_p, a_p, x_p, f_p, 200000, TOL * TOL, C.byref(ani), C.byref(ares),
-                                  1e-30, 0, best, C.byref(info))
+        if prec_b == L.PREC_AGG:
+            h = C.c_void_p()
+            L.check(lib.sgpu_matrix_create(n, adr_p, ci_p, a_p, 1, C.byref(h)))
+            L.check(lib.sgpu_matrix_set_nullspace(h, rbm_cols.shape[0], rbm_p))
+            st = lib.sgpu_matrix_pcg(h, x_p, f_p, 200000, res_b, 1e-30, 0, crit_b, prec_b, mode_b,
+                                     C.byref(ani), C.byref(ares), C.byref(info))
+            lib.sgpu_matrix_destroy(h)
+        else:
+            st = lib.sgpu_scr_cg_prec(n, adr_p, ci_p, a_p, x_p, f_p, 200000, TOL * TOL, C.byref(ani), C.byref(ares),
+                                      1e-30, 0, mode_b, C.byref(info))
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         L.check(st)
     e2e_v = dist_max(min(e2e_ms), ws)
-    h2d = adr_h.nbytes + ci_h.nbytes + a_h.nbytes + f_host.nbytes
+    h2d = adr_h.nbytes + ci_h.nbytes + a_h.nbytes + f_host.nbytes + (rbm_cols.nbytes if prec_b == L.PREC_AGG else 0)
     d2h = x_p.nbytes
 
     cpu = None
@@ -363,24 +418,22 @@ def run_ours(args, ws, rank):
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": round(ms_best, 3),
-        "form": "mixed" if best == L.MIXED else "fp64",
+        "form": best,
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 inner / f64 refinement" if best == L.MIXED else "f64",
+        "dtype": DTYPE[best],
         "data": "synthetic (generated mesh, GPU-assembled stiffness)",
         "config": {"workload": args.workload, "n_equations": n, "nnz_full": nnz, "tolerance": TOL,
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (matrix >= 0.6 GB vs 126 MB)"},
-        "mixed": {"solve_ms": round(ms_mixed, 3), "iterations": im.iterations, "refinements": im.refinements,
-                  "true_relres": im.true_relres, "fell_back_to_fp64": bool(im.fallback),
-                  "speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3) if ms_mixed == ms_mixed else None},
-        "fp64": {"solve_ms": round(ms_fp64, 3), "iterations": i64.iterations, "true_relres": i64.true_relres,
-                 "reference_iterations": reference_iterations(args.workload)},
+        "forms": forms_out,
         "spmv_other": spmv_other,
         "roofline": roofline,
         "e2e": {"value": round(e2e_v, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "path": "sgpu_scr_cg_prec, the drop-in for symcomprow::cg_prec (host SCR arrays)"},
+                "path": ("sgpu_matrix_create + sgpu_matrix_set_nullspace + sgpu_matrix_pcg (host arrays)"
+                         if prec_b == L.PREC_AGG else
+                         "sgpu_scr_cg_prec, the drop-in for symcomprow::cg_prec (host SCR arrays)")},
         "gpu_launches": int(launches),
         "clocks": clk,
         "cpu_baseline": cpu,
@@ -617,7 +670,7 @@ def main():
     ap.add_argument("--workload", default="cantilever_200x40x40", choices=sorted(WORKLOADS) + list(EXTRA))
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--forms", default="both", choices=["both", "fp64", "mixed"],
+    ap.add_argument("--forms", default="all", choices=sorted(FORM_SETS),
                     help="GPU forms to run (profiling runs time one form only)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the e2e and CPU legs (profiling runs)")
     args = ap.parse_args()

@@ -182,6 +182,9 @@ SGPU_API int sgpu_matrix_pcg_d(sgpu_matrix m, double *x_d, const double *f_d, in
  * per equation of a node (translations only).  Setting it discards a built
  * hierarchy; new values (sgpu_matrix_update_values) do too. */
 SGPU_API int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B);
+/* Discards the hierarchy of SGPU_PREC_AGG (the next such solve builds it
+ * again); the near-null space is kept.  For timing set-up with the solve. */
+SGPU_API int sgpu_matrix_precond_clear(sgpu_matrix m);
 
 /* All load cases at once (solve_linear_statics, MEFEL/SRC/lssolver.cpp:78-80,
  * solves them one after the other): nrhs (<= 128) independent Jacobi-PCG

@@ -19,6 +19,7 @@ OK, NOT_CONVERGED, BREAKDOWN, BAD_INPUT, CUDA_ERROR, ZERO_RHS = range(6)
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "BAD_INPUT", 4: "CUDA_ERROR", 5: "ZERO_RHS"}
 CRIT_SCR_PREC, CRIT_CR_PREC, CRIT_TRUE = 0, 1, 2
 FP64, MIXED = 0, 1
+PREC_NONE, PREC_JACOBI, PREC_AGG = 0, 1, 101
 
 
 class SolveInfo(C.Structure):
@@ -109,6 +110,7 @@ SIGNATURES = {
     "sgpu_matrix_spmv_plan": ([_vp, _i32, C.POINTER(_dbl), C.POINTER(_i32), C.POINTER(_i32)], C.c_int),
     "sgpu_matrix_set_spmv": ([_vp, _i32, _i32, _i32], C.c_int),
     "sgpu_matrix_set_nullspace": ([_vp, _i32, _pD], C.c_int),
+    "sgpu_matrix_precond_clear": ([_vp], C.c_int),
     "sgpu_csr_pcg_noalloc_d": ([_i32, _vp, _vp, _vp, _vp, _vp, _i64, _dbl, _dbl, _i64, _vp, C.POINTER(_i64),
                                 C.POINTER(_dbl), C.POINTER(_i64)], C.c_int),
     "sgpu_assembly_lift": ([_vp, _pD, _pD], C.c_int),

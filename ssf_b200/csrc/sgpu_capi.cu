@@ -241,6 +241,12 @@ int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B) {
   return amg_set_nullspace(m, k, B);
 }
 
+int sgpu_matrix_precond_clear(sgpu_matrix m) {
+  if (!m) return fail(SGPU_BAD_INPUT, "null handle");
+  amg_values_changed(m);
+  return SGPU_OK;
+}
+
 int sgpu_matrix_pcg(sgpu_matrix m, double *x, const double *f, int64_t ni, double res, double zero, int64_t iv,
                     int32_t crit, int32_t prec, int32_t mode, int64_t *ani, double *ares, sgpu_solve_info *info) {
   if (!m) return fail(SGPU_BAD_INPUT, "null handle");

@@ -201,6 +201,10 @@ class DeviceMatrix:
         cols = np.ascontiguousarray(B.T)  # column after column
         L.check(L.lib().sgpu_matrix_set_nullspace(self.h, cols.shape[0], cols.ravel()))
 
+    def precond_clear(self):
+        """Discard the aggregation hierarchy (rebuilt by the next solve)."""
+        L.check(L.lib().sgpu_matrix_precond_clear(self.h))
+
     def pcg(self, f, x=None, ni=100000, res=1e-20, zero=1e-30, crit="scr", prec=1, mode="fp64") -> tuple:
         """PCG with the criterion of the reference routine ``crit``; ``prec``
         0 / "none", 1 / "jacobi" or 101 / "agg" (aggregation multilevel
