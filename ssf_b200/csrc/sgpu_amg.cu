@@ -122,11 +122,11 @@ __device__ __forceinline__ bool reduce_grid(double (&v)[NV], double *partials, u
 // Sums the row contributions of an operator with NV > 0 over the grid and lets
 // the last block finish.
 template <class Op>
-__device__ __forceinline__ void op_reduce(double (&acc)[Op::NV > 0 ? Op::NV : 1], PcgState *st,
+__device__ __forceinline__ void op_reduce(const Op &op, double (&acc)[Op::NV > 0 ? Op::NV : 1], PcgState *st,
                                           double *partials, unsigned *ticket) {
   if constexpr (Op::NV > 0) {
     double tot[Op::NV];
-    if (reduce_grid<Op::NV>(acc, partials, ticket, tot)) Op::finish(st, tot);
+    if (reduce_grid<Op::NV>(acc, partials, ticket, tot)) op.finish(st, tot);
   }
 }
 
@@ -142,18 +142,23 @@ struct OpResid {  // res = b - A x
   __device__ static void finish(PcgState *, const double *) {}
 };
 
+// Lanczos step on M = D^-1/2 A D^-1/2 (the SpMV input is u = D^-1/2 w_j,
+// unnormalised; v_j = w_j / beta_j): y = M v_j and alpha_j = y . v_j
 template <typename T>
-struct OpPower {  // y = D^-1 A v / |v| and |y|^2 (power iteration of the set-up)
+struct OpLanczos {
   static constexpr int NV = 1;
-  T *out;
-  const T *dinv;
-  const double *vv;  // |v|^2, written by the previous step's last block
-  __device__ void row(int i, T y, double *acc) const {
-    const T v = (T)rsqrt(*vv) * (dinv ? dinv[i] : T(1)) * y;
-    out[i] = v;
-    acc[0] += (double)v * (double)v;
+  const T *dsq;
+  const T *wj;
+  const double *beta_j;
+  T *y;
+  double *alpha_out;
+  __device__ void row(int i, T ay, double *acc) const {
+    const double ib = 1.0 / *beta_j;
+    const double yi = (dsq ? (double)dsq[i] : 1.0) * (double)ay * ib;
+    y[i] = (T)yi;
+    acc[0] += yi * (double)wj[i] * ib;
   }
-  __device__ static void finish(PcgState *st, const double *tot) { st->last_dot = tot[0]; }
+  __device__ void finish(PcgState *, const double *tot) const { *alpha_out = tot[0]; }
 };
 
 // Chebyshev smoothing step fused with its SpMV.
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(TPB, 6) k_lv_bsr3(int nb, const int *__restric
     }
     if (sub < 3 && br < nb) op.row(3 * br + sub, sub == 0 ? y0 : (sub == 1 ? y1 : y2), acc);
   }
-  op_reduce<Op>(acc, st, partials, ticket);
+  op_reduce<Op>(op, acc, st, partials, ticket);
 }
 
 // level 0 in scalar CSR: L lanes per row
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(TPB) k_lv_csr(int n, const int *__restrict__ r
     for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, L);
     if (sub == 0 && i < n) op.row(i, s, acc);
   }
-  op_reduce<Op>(acc, st, partials, ticket);
+  op_reduce<Op>(op, acc, st, partials, ticket);
 }
 
 // coarse levels: B x B blocks stored row-major, one warp per block row
@@ -338,7 +343,7 @@ __global__ void __launch_bounds__(TPB) k_lv_bsrb(int nb, const int *__restrict__
       op.row(B * br + lane, yv, acc);
     }
   }
-  op_reduce<Op>(acc, st, partials, ticket);
+  op_reduce<Op>(op, acc, st, partials, ticket);
 }
 
 // ---------------------------------------------------------------------------
@@ -908,6 +913,45 @@ __global__ void k_unit_empty_diag(int n, double *__restrict__ a) {
     if (!(a[(size_t)p * n + p] > 0.0)) a[(size_t)p * n + p] = 1.0;
 }
 
+// w_{j+1} = y - alpha_j v_j - beta_j v_{j-1} (v = w / beta), u = D^-1/2 w_{j+1},
+// beta_{j+1} = |w_{j+1}|.  ab holds alpha_0..alpha_63 then beta_0..beta_64.
+// The first call (wj == nullptr) takes y as the start vector.
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_lanczos_w(int n, const T *__restrict__ y, const T *__restrict__ wj,
+                                                   const T *__restrict__ wprev, const T *__restrict__ dsq,
+                                                   const double *__restrict__ ab, int j, T *__restrict__ wnext,
+                                                   T *__restrict__ u, double *partials, unsigned *ticket,
+                                                   double *beta_out) {
+  double a = 0.0, bj = 1.0, bp = 1.0;
+  if (wj) {
+    a = ab[j];
+    bj = ab[64 + j];
+    if (wprev) bp = ab[64 + j - 1];
+  }
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double w = (double)y[i];
+    if (wj) {
+      w -= a * (double)wj[i] / bj;
+      if (wprev) w -= bj * (double)wprev[i] / bp;
+    }
+    wnext[i] = (T)w;
+    u[i] = (T)((dsq ? (double)dsq[i] : 1.0) * w);
+    v[0] += w * w;
+  }
+  double t[1];
+  if (reduce_grid<1>(v, partials, ticket, t)) *beta_out = sqrt(t[0]);
+}
+
+__global__ void k_sqrt_vec(int n, const double *__restrict__ dinv, float *__restrict__ d32,
+                           double *__restrict__ d64) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = sqrt(dinv[i]);
+    d32[i] = (float)v;
+    d64[i] = v;
+  }
+}
+
 __global__ void k_to32(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
@@ -957,6 +1001,8 @@ struct AmgLevel {
   DevBuf<float> val32;   // owned coarse values (FP32)
   DevBuf<double> dinv64;
   DevBuf<float> dinv32;
+  DevBuf<double> dsq64;  // sqrt(dinv): the symmetric scaling of the Lanczos operator
+  DevBuf<float> dsq32;
   bool unit_diag = false;
   double lmax64 = 0.0, lmax32 = 0.0;
   // transfer to the next level
@@ -982,18 +1028,29 @@ struct Amg {
   DevBuf<float> cb32, cx32;
   // options: Chebyshev degree, coarse-correction weight, smoothing interval
   // [lmax/ratio, 1.1 lmax], largest dense coarsest level, coarse visits per
-  // level (1: V-cycle, 2: W-cycle), power-iteration steps
+  // level (1: V-cycle, 2: W-cycle), Lanczos steps of the lmax estimate
   int deg = 1;
-  double ratio = 30.0, alpha = 1.5;
+  double ratio = 30.0, alpha = 1.7;
   int coarse_max = 768;
   int gamma = 2;       // visits of level 1 per level-0 cycle
   int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
-  int power_its = 40;
-  ~Amg() { clear(); }
+  int lanczos_steps = 14;
+  // level objects by depth, kept when a hierarchy is discarded so that a
+  // rebuild of the same matrix reuses their device buffers
+  std::vector<AmgLevel *> pool;
+  ~Amg() {
+    for (AmgLevel *l : pool) delete l;
+  }
   void clear() {
-    for (AmgLevel *l : lv) delete l;
     lv.clear();
     built = have32 = have64 = false;
+  }
+  AmgLevel *take_level(size_t depth) {
+    while (pool.size() <= depth) pool.push_back(new AmgLevel());
+    AmgLevel *l = pool[depth];
+    l->unit_diag = false;
+    l->browptr = l->bcol = nullptr;
+    return l;
   }
 };
 
@@ -1268,7 +1325,10 @@ int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_
   SGPU_TRY(C.dinv64.alloc(C.n));
   SGPU_TRY(C.dinv32.alloc(C.n));
   k_coarse_dinv<<<grid_for(C.nb), TPB, 0, s>>>(C.nb, K, C.browptr, C.bcol, C.val64.p, C.dinv64.p, C.dinv32.p);
-  count_launches(1);
+  SGPU_TRY(C.dsq64.alloc(C.n));
+  SGPU_TRY(C.dsq32.alloc(C.n));
+  k_sqrt_vec<<<grid_for(C.n), TPB, 0, s>>>(C.n, C.dinv64.p, C.dsq32.p, C.dsq64.p);
+  count_launches(2);
   SGPU_CUDA(cudaGetLastError());
   return SGPU_OK;
 }
@@ -1376,28 +1436,79 @@ int launch_level(sgpu_matrix m, const AmgLevel &L, const T *v, const Op &op, cud
   return SGPU_OK;
 }
 
-// lmax of D^-1 A by power iteration; every step divides by the previous
-// step's norm on the device, so the host reads once at the end
 template <typename T>
-int power_lmax(sgpu_matrix m, const AmgLevel &L, cudaStream_t s, int its, double *lmax) {
-  TmpBuf<T> v(s), y(s);
-  SGPU_TRY(v.alloc(L.n));
-  SGPU_TRY(y.alloc(L.n));
-  k_rand_vec<T><<<grid_for(L.n), TPB, 0, s>>>(L.n, v.p);
-  count_launches(1);
-  PcgState *st = pcg_state(m);
-  const double v2 = (double)L.n / 3.0;  // E|v|^2 for v uniform in [-1, 1]
-  SGPU_CUDA(cudaMemcpyAsync(&st->last_dot, &v2, sizeof(double), cudaMemcpyHostToDevice, s));
-  for (int it = 0; it < its; it++) {
-    OpPower<T> op{y.p, level_dinv<T>(L), &st->last_dot};
-    SGPU_TRY(launch_level<T>(m, L, v.p, op, s, 5));
-    std::swap(v.p, y.p);
+const T *level_dsq(const AmgLevel &L);
+template <>
+const float *level_dsq<float>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dsq32.p; }
+template <>
+const double *level_dsq<double>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dsq64.p; }
+
+// largest eigenvalue of the symmetric tridiagonal matrix (a on the diagonal,
+// b[1..k-1] below it) by bisection on Sturm counts
+double tridiag_lmax(const std::vector<double> &a, const std::vector<double> &b) {
+  const int k = (int)a.size();
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < k; i++) {
+    const double r = (i > 0 ? fabs(b[i]) : 0.0) + (i + 1 < k ? fabs(b[i + 1]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
   }
-  double yy = 0.0;
-  SGPU_CUDA(cudaMemcpyAsync(&yy, &st->last_dot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  auto below = [&](double x) {  // number of eigenvalues < x
+    int c = 0;
+    double q = a[0] - x;
+    if (q < 0) c++;
+    for (int i = 1; i < k; i++) {
+      if (q == 0.0) q = 1e-300;
+      q = a[i] - x - b[i] * b[i] / q;
+      if (q < 0) c++;
+    }
+    return c;
+  };
+  for (int it = 0; it < 200 && hi - lo > 1e-12 * std::max(1.0, fabs(hi)); it++) {
+    const double mid = 0.5 * (lo + hi);
+    if (below(mid) >= k) hi = mid;  // every eigenvalue is below mid
+    else lo = mid;
+  }
+  return hi;
+}
+
+// lmax of D^-1 A (= that of the symmetric D^-1/2 A D^-1/2) by `steps`
+// Lanczos steps; the host reads the coefficients once at the end
+template <typename T>
+int lanczos_lmax(sgpu_matrix m, const AmgLevel &L, cudaStream_t s, int steps, double *lmax) {
+  steps = std::max(2, std::min(steps, 63));
+  TmpBuf<T> w0(s), w1(s), w2(s), u(s), y(s);
+  TmpBuf<double> ab(s);
+  SGPU_TRY(w0.alloc(L.n));
+  SGPU_TRY(w1.alloc(L.n));
+  SGPU_TRY(w2.alloc(L.n));
+  SGPU_TRY(u.alloc(L.n));
+  SGPU_TRY(y.alloc(L.n));
+  SGPU_TRY(ab.alloc(129));
+  T *w[3] = {w0.p, w1.p, w2.p};
+  const T *dsq = level_dsq<T>(L);
+  Work &wk = m->w;
+  const int g = grid_for(L.n);
+  k_rand_vec<T><<<g, TPB, 0, s>>>(L.n, y.p);
+  k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y.p, nullptr, nullptr, dsq, ab.p, 0, w[0], u.p, wk.partials.p,
+                                   wk.counters.p + 7, ab.p + 64);
+  count_launches(2);
+  for (int j = 0; j < steps; j++) {
+    OpLanczos<T> op{dsq, w[j % 3], ab.p + 64 + j, y.p, ab.p + j};
+    SGPU_TRY(launch_level<T>(m, L, u.p, op, s, 5));
+    k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y.p, w[j % 3], j > 0 ? w[(j + 2) % 3] : nullptr, dsq, ab.p, j,
+                                     w[(j + 1) % 3], u.p, wk.partials.p, wk.counters.p + 7, ab.p + 64 + j + 1);
+    count_launches(1);
+  }
+  std::vector<double> h(129);
+  SGPU_CUDA(cudaMemcpyAsync(h.data(), ab.p, 129 * sizeof(double), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
-  if (!(yy > 0.0) || !std::isfinite(yy)) return fail(SGPU_BAD_INPUT, "smoother bound: power iteration failed");
-  *lmax = sqrt(yy);
+  std::vector<double> a(h.begin(), h.begin() + steps), b(steps, 0.0);
+  for (int j = 1; j < steps; j++) b[j] = h[64 + j];
+  for (int j = 0; j < steps; j++)
+    if (!std::isfinite(a[j]) || !std::isfinite(b[j])) return fail(SGPU_BAD_INPUT, "smoother bound: Lanczos failed");
+  *lmax = tridiag_lmax(a, b);
+  if (!(*lmax > 0.0)) return fail(SGPU_BAD_INPUT, "smoother bound: non-positive estimate");
   return SGPU_OK;
 }
 
@@ -1425,8 +1536,8 @@ int amg_build(sgpu_matrix m) {
   Amg &A = *m->amg;
   cudaStream_t s = m->stream;
   A.clear();
-  if (const char *o = env_or("SGPU_AMG")) {  // "deg,alpha,ratio,coarse_max,gamma,power,gamma_deep" (tuning)
-    int deg = A.deg, cmax = A.coarse_max, gam = A.gamma, pw = A.power_its, gd = A.gamma_deep;
+  if (const char *o = env_or("SGPU_AMG")) {  // "deg,alpha,ratio,coarse_max,gamma,lanczos,gamma_deep" (tuning)
+    int deg = A.deg, cmax = A.coarse_max, gam = A.gamma, pw = A.lanczos_steps, gd = A.gamma_deep;
     double al = A.alpha, ra = A.ratio;
     if (sscanf(o, "%d,%lf,%lf,%d,%d,%d,%d", &deg, &al, &ra, &cmax, &gam, &pw, &gd) >= 1) {
       A.gamma_deep = std::max(1, std::min(gd, 2));
@@ -1435,7 +1546,7 @@ int amg_build(sgpu_matrix m) {
       A.ratio = ra;
       A.coarse_max = std::max(16, std::min(cmax, 4096));
       A.gamma = std::max(1, std::min(gam, 2));
-      A.power_its = std::max(4, std::min(pw, 400));
+      A.lanczos_steps = std::max(4, std::min(pw, 63));
     }
   }
   SGPU_TRY(ensure_bsr3(m));
@@ -1445,7 +1556,7 @@ int amg_build(sgpu_matrix m) {
   CubTmp tmp(s);
   PhaseClock clk(s);
   // level 0
-  AmgLevel *L0 = new AmgLevel();
+  AmgLevel *L0 = A.take_level(0);
   A.lv.push_back(L0);
   if (m->bsr.valid) {
     L0->layout = 1;
@@ -1479,7 +1590,7 @@ int amg_build(sgpu_matrix m) {
     SGPU_TRY(Bnext.alloc((size_t)L.na * K * K));
     SGPU_TRY(tentative(L, K, Bcur.p, Bnext.p, s));
     clk.mark("tentative prolongator");
-    AmgLevel *C = new AmgLevel();
+    AmgLevel *C = A.take_level(A.lv.size());
     A.lv.push_back(C);
     LevelView view{L.layout, L.browptr, L.bcol,
                    L.layout == 1 ? m->bsr.bval.p : (L.layout == 2 ? m->csr.val.p : L.val64.p), m->csr.dscale.p};
@@ -1515,8 +1626,7 @@ int amg_build(sgpu_matrix m) {
   SGPU_CUDA(cudaGetLastError());
   clk.mark("dense coarsest inverse");
   // the dense level is not a smoothing level
-  A.lv.pop_back();
-  delete Cl;
+  A.lv.pop_back();  // (its object stays in the pool)
   A.built = true;
   if (getenv("SGPU_AMG_VERBOSE")) {
     for (size_t l = 0; l < A.lv.size(); l++) {
@@ -1547,8 +1657,8 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
         count_launches(1);
       }
       clk.mark("fp32 copies");
-      SGPU_TRY(power_lmax<float>(m, L, s, A.power_its, &L.lmax32));
-      clk.mark("power iteration");
+      SGPU_TRY(lanczos_lmax<float>(m, L, s, A.lanczos_steps, &L.lmax32));
+      clk.mark("Lanczos bound");
       if (getenv("SGPU_AMG_VERBOSE")) fprintf(stderr, "amg level %zu: lmax (fp32) %.6g\n", l, L.lmax32);
     }
     SGPU_TRY(A.M32.alloc((size_t)A.nc * A.nc));
@@ -1571,8 +1681,8 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
         count_launches(1);
       }
       clk.mark("fp64 scaled level 0");
-      SGPU_TRY(power_lmax<double>(m, L, s, A.power_its, &L.lmax64));
-      clk.mark("power iteration");
+      SGPU_TRY(lanczos_lmax<double>(m, L, s, A.lanczos_steps, &L.lmax64));
+      clk.mark("Lanczos bound");
       if (getenv("SGPU_AMG_VERBOSE")) fprintf(stderr, "amg level %zu: lmax (fp64) %.6g\n", l, L.lmax64);
     }
     SGPU_TRY(A.cb64.alloc(A.nc));
@@ -1734,14 +1844,16 @@ int cycle(sgpu_matrix m, int l, bool zero_init, const std::vector<Cheb> &ch, std
     LevelVecs<T> &W = vecs<T>(C);
     SGPU_TRY(restrict_level<T>(L, V.res.p, W.b.p, W.r.p, W.d.p, W.x.p, level_dinv<T>(C), (T)ch[l + 1].c2_first, true,
                                st, s));
+    // coarse correction
+    const int visits = l == 0 ? A.gamma : A.gamma_deep;
+    for (int v = 0; v < visits; v++) SGPU_TRY(cycle<T>(m, l + 1, v == 0, ch, xcur, s));
+    SGPU_TRY(prolong_level<T>(L, xcur[l + 1], xp, (T)A.alpha, st, s));
   } else {
     T *cb = sizeof(T) == 4 ? (T *)A.cb32.p : (T *)A.cb64.p;
     SGPU_TRY(restrict_level<T>(L, V.res.p, cb, nullptr, nullptr, nullptr, nullptr, (T)0, false, st, s));
+    SGPU_TRY(cycle<T>(m, l + 1, true, ch, xcur, s));
+    SGPU_TRY(prolong_level<T>(L, xcur[l + 1], xp, (T)A.alpha, st, s));
   }
-  // coarse correction
-  const int visits = (l + 1 < nl) ? (l == 0 ? A.gamma : A.gamma_deep) : 1;
-  for (int v = 0; v < visits; v++) SGPU_TRY(cycle<T>(m, l + 1, v == 0, ch, xcur, s));
-  SGPU_TRY(prolong_level<T>(L, xcur[l + 1], xp, (T)A.alpha, st, s));
   // post-smoothing: first step from x (SpMV of x, result in the other buffer)
   const bool outer = (l == 0);
   T *to = (xp == V.x.p) ? V.x2.p : V.x.p;
@@ -1871,7 +1983,9 @@ int fcg_solve(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, in
   const int chunk = 8;
   cudaGraphExec_t exec = nullptr;
   int64_t nodes = 0;
+  PhaseClock clk(s);
   SGPU_TRY(capture_chunk<T>(m, chunk, &exec, &nodes));
+  clk.mark("graph capture + instantiate");
   int rc = SGPU_OK;
   int restarts = 0;
   for (;;) {
