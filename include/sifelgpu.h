@@ -279,16 +279,18 @@ SGPU_API int sgpu_matrix_combine(sgpu_matrix K, sgpu_matrix C, double a, double 
 /* nsteps steps of the d-form generalized trapezoid of
  * linear_nonstat_solv_dform (TRFEL/SRC/npsolvert.cpp:1071-1272) with a fixed
  * dt and alpha: dd = d + (1-alpha) dt v; A = alpha dt K + C; f = alpha dt rhs
- * + C dd; A d = f by Jacobi-PCG with the reference's criterion (ni, res,
- * zero, iv as for sgpu_scr_cg_prec; x starts from the previous d when
- * iv = 1); v = (d - dd)/dt/alpha.  rhs[n] is the step's right-hand side
+ * + C dd; A d = f by PCG with the reference's criterion (ni, res, zero, iv as
+ * for sgpu_scr_cg_prec; x starts from the previous d when iv = 1); v = (d -
+ * dd)/dt/alpha.  prec: SGPU_PREC_JACOBI (the reference's) or SGPU_PREC_AGG
+ * (the hierarchy is built on the first step and kept for all of them).  rhs[n] is the step's right-hand side
  * (constant: the lifting of time-constant prescribed values), d and v (host,
  * n) are read and overwritten; step_iterations (may be NULL) gets the
  * iterations of every step.  Everything between the first and the last copy
  * stays on the device. */
 SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v,
                                   double dt, double alpha, int64_t nsteps, int64_t ni, double res, double zero,
-                                  int64_t iv, int32_t mode, int64_t *step_iterations, sgpu_solve_info *info);
+                                  int64_t iv, int32_t prec, int32_t mode, int64_t *step_iterations,
+                                  sgpu_solve_info *info);
 
 /* ------------------------------------------------------------------------ */
 /* Solving without allocating device memory                                 */

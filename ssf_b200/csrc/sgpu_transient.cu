@@ -122,10 +122,11 @@ SGPU_API int sgpu_matrix_combine(sgpu_matrix K, sgpu_matrix C, double a, double 
 
 SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v, double dt,
                                   double alpha, int64_t nsteps, int64_t ni, double res, double zero, int64_t iv,
-                                  int32_t mode, int64_t *step_iterations, sgpu_solve_info *info) {
+                                  int32_t prec, int32_t mode, int64_t *step_iterations, sgpu_solve_info *info) {
   if (!K || !C || !rhs || !d || !v) return fail(SGPU_BAD_INPUT, "null argument");
   if (!(dt > 0.0) || !(alpha > 0.0) || alpha > 1.0) return fail(SGPU_BAD_INPUT, "need dt > 0 and 0 < alpha <= 1");
   if (nsteps < 0) return fail(SGPU_BAD_INPUT, "negative step count");
+  if (prec != SGPU_PREC_JACOBI && prec != SGPU_PREC_AGG) return fail(SGPU_BAD_INPUT, "prec: Jacobi or aggregation");
   if (info) memset(info, 0, sizeof(*info));
   sgpu_matrix A = nullptr;
   // A = alpha dt K + C (scalgm then addgm, GEFEL/gmatrix.cpp:1848/1791)
@@ -155,7 +156,8 @@ SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rh
   cudaMemcpyAsync(rhs_d.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s);
   const int vb = blocks_for(n);
   int64_t total_its = 0;
-  double total_ms = 0.0, last_true = 0.0;
+  double total_ms = 0.0, last_true = 0.0, setup_ms = 0.0;
+  int32_t levels = 0, coarse_n = 0;
   for (int64_t step = 0; step < nsteps; step++) {
     k_predict<<<vb, TPB, 0, s>>>((int)n, d_d.p, v_d.p, (1.0 - alpha) * dt, dd_d.p);
     count_launches(1);
@@ -168,13 +170,16 @@ SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rh
     memset(&si, 0, sizeof(si));
     int64_t ani = -1;
     double ares = 0.0;
-    st = pcg_run(A, ni, res, zero, iv, SGPU_CRIT_SCR_PREC, 1, mode, &ani, &ares, &si);
+    st = pcg_run(A, ni, res, zero, iv, SGPU_CRIT_SCR_PREC, prec, mode, &ani, &ares, &si);
     if (st == SGPU_BAD_INPUT || st == SGPU_CUDA_ERROR) break;
     if (st != SGPU_OK && status == SGPU_OK) status = st;
     st = SGPU_OK;
     if (step_iterations) step_iterations[step] = si.iterations;
     total_its += si.iterations;
-    total_ms += si.solve_ms;
+    total_ms += si.solve_ms + si.precond_setup_ms;
+    setup_ms += si.precond_setup_ms;
+    levels = si.precond_levels;
+    coarse_n = si.precond_coarse_n;
     last_true = si.true_relres;
     cudaMemcpyAsync(d_d.p, work_x(A), n * sizeof(double), cudaMemcpyDeviceToDevice, s);
     k_velocity<<<vb, TPB, 0, s>>>((int)n, d_d.p, dd_d.p, dt, alpha, v_d.p);
@@ -189,6 +194,9 @@ SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rh
     info->iterations = total_its;
     info->solve_ms = total_ms;
     info->true_relres = last_true;
+    info->precond_setup_ms = setup_ms;
+    info->precond_levels = levels;
+    info->precond_coarse_n = coarse_n;
   }
   cleanup(SGPU_OK);
   return status;

@@ -140,10 +140,12 @@ def trfel_lift(K: DeviceMatrix, rnode) -> np.ndarray:
 
 
 def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1,
-                              mode="fp64", rnode=None, d0=None, v0=None):
+                              mode="fp64", rnode=None, d0=None, v0=None, prec="jacobi"):
     """The d-form generalized trapezoid (TRFEL/SRC/npsolvert.cpp:1071) on the
-    GPU: K and C assembled once, `nsteps` steps with everything on the device.
-    Returns (d, v, per-step iterations, solve info)."""
+    GPU: K and C assembled once, `nsteps` steps with everything on the device;
+    ``prec`` "jacobi" (the reference's) or "agg" (aggregation multilevel, its
+    hierarchy built once for all steps).  Returns (d, v, per-step iterations,
+    solve info)."""
     K = conductivity_matrix(mesh)
     Cm = capacity_matrix(mesh)
     try:
@@ -155,8 +157,9 @@ def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20,
         its = np.zeros(max(nsteps, 1), dtype=np.int64)
         info = L.SolveInfo()
         m = {"fp64": L.FP64, "mixed": L.MIXED}[mode]
+        p = {"jacobi": L.PREC_JACOBI, "agg": L.PREC_AGG}[prec]
         st = L.lib().sgpu_transient_dform(K.h, Cm.h, rhs, d, v, float(dt), float(alpha), int(nsteps), int(ni),
-                                          float(res), float(zero), int(iv), m, its.ctypes.data, C.byref(info))
+                                          float(res), float(zero), int(iv), p, m, its.ctypes.data, C.byref(info))
         L.check(st, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN))
         return d, v, its[:nsteps], info.as_dict()
     finally:

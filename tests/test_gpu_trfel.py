@@ -50,6 +50,19 @@ def test_transient_mixed_form(oracle, gpu_lib):
     assert np.linalg.norm(d - d_o) / np.linalg.norm(d_o) <= 1e-7
 
 
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+def test_transient_aggregation_preconditioner(oracle, gpu_lib, mode):
+    # the aggregation hierarchy is built on the first step and reused by the
+    # others; the steps still reach the oracle's states
+    from ssf_b200 import mefel
+    m = _cube(12, seed=9)
+    d_o, v_o, _ = oracle.trfel_steps(m, 3, 10.0, res=1e-26, iv=1)
+    d, v, its, info = mefel.linear_nonstat_solv_dform(m, 3, 10.0, res=1e-22, iv=1, mode=mode, prec="agg")
+    assert np.linalg.norm(d - d_o) / np.linalg.norm(d_o) <= 1e-8
+    assert np.linalg.norm(v - v_o) / np.linalg.norm(v_o) <= 1e-6
+    assert info["precond_levels"] >= 2 and info["precond_setup_ms"] > 0.0
+
+
 def test_stationary_matches_oracle(oracle, gpu_lib):
     from ssf_b200 import mefel
     from ssf_b200 import _lib as L
