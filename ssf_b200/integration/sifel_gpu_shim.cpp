@@ -7,8 +7,11 @@
 // 1225-1227) land here; the diagonal (Jacobi) case, tprec == 1, goes to
 // sgpu_scr_cg_prec with the storage object's own arrays, every other case to
 // the original routine.  SIFEL_GPU=off keeps the CPU routine, SIFEL_GPU=mixed
-// selects the mixed-precision form.  Decks in SIFEL's input format run
-// unchanged.
+// selects the mixed-precision form, SIFEL_GPU=agg (agg64) the flexible CG with
+// the aggregation multilevel preconditioner in FP32 (FP64) -- GEFEL's own
+// precondtype boss = 101 -- on the same criterion; only the storage object is
+// at hand here, so its near-null space is the translations (one constant per
+// node component).  Decks in SIFEL's input format run unchanged.
 #include <cerrno>
 #include <cstdlib>
 #include <cstring>
@@ -32,15 +35,24 @@ void __wrap__ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver(symcomprow *self, d
                                                             sdirect);
     return;
   }
-  const int mode = (mode_env && !strcmp(mode_env, "mixed")) ? SGPU_MIXED : SGPU_FP64;
+  const bool agg = mode_env && (!strcmp(mode_env, "agg") || !strcmp(mode_env, "agg64"));
+  const int mode = (mode_env && (!strcmp(mode_env, "mixed") || !strcmp(mode_env, "agg"))) ? SGPU_MIXED : SGPU_FP64;
   int64_t a_ni = ani;
   double a_res = ares;
   // SIFEL checks errno after the solve (check_math_err, GEFEL/mathem.cpp:1725)
   // and aborts on any value; the CUDA runtime may leave one behind (e.g. from
   // probing files while loading the driver), so errno is kept as it was
   const int saved_errno = errno;
-  const int st = sgpu_scr_cg_prec(self->n, self->adr, self->ci, self->a, x, y, ni, res, &a_ni, &a_res, zero, iv,
-                                  mode, NULL);
+  int st;
+  if (agg) {
+    sgpu_matrix m = NULL;
+    st = sgpu_matrix_create(self->n, self->adr, self->ci, self->a, 1, &m);
+    if (st == SGPU_OK)
+      st = sgpu_matrix_pcg(m, x, y, ni, res, zero, iv, SGPU_CRIT_SCR_PREC, SGPU_PREC_AGG, mode, &a_ni, &a_res, NULL);
+    if (m) sgpu_matrix_destroy(m);
+  } else {
+    st = sgpu_scr_cg_prec(self->n, self->adr, self->ci, self->a, x, y, ni, res, &a_ni, &a_res, zero, iv, mode, NULL);
+  }
   errno = saved_errno;
   ani = (long)a_ni;
   ares = a_res;

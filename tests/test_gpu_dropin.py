@@ -53,3 +53,19 @@ def test_unchanged_deck_runs_with_gpu_solver(bins, case):
     assert abs(gpu["meta"]["ani_0"] - cpu["meta"]["ani_0"]) <= 2
     # with the GPU switched off the binding calls the reference routine itself
     assert np.array_equal(off["u"], u_c) and off["meta"]["ani_0"] == cpu["meta"]["ani_0"]
+
+
+@pytest.mark.parametrize("env", ["agg", "agg64"])
+def test_unchanged_deck_with_aggregation_preconditioner(bins, env):
+    # SIFEL_GPU=agg: the flexible CG with the aggregation preconditioner, a
+    # different iteration from the reference's, so both runs solve to a
+    # tighter threshold (1e-24 on (r.r)/(f.f)) and the solutions are compared
+    m = decks.cantilever_hex(30, 6, 6)
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "deck.in")
+        decks.write_mefel_deck(m, deck, res=1e-24)
+        cpu = _run("mefel_dump", deck)
+        gpu = _run("mefel_dump_gpu", deck, {"SIFEL_GPU": env})
+    u_c, u_g = cpu["u"], gpu["u"]
+    assert np.linalg.norm(u_g - u_c) / np.linalg.norm(u_c) <= 1e-8
+    assert 0 < gpu["meta"]["ani_0"] < cpu["meta"]["ani_0"] / 3
