@@ -57,9 +57,10 @@ def test_unchanged_deck_runs_with_gpu_solver(bins, case):
 
 @pytest.mark.parametrize("env", ["agg", "agg64"])
 def test_unchanged_deck_with_aggregation_preconditioner(bins, env):
-    # SIFEL_GPU=agg: the flexible CG with the aggregation preconditioner, a
-    # different iteration from the reference's, so both runs solve to a
-    # tighter threshold (1e-24 on (r.r)/(f.f)) and the solutions are compared
+    # SIFEL_GPU=agg: the flexible CG with the aggregation preconditioner (its
+    # near-null space from MEFEL's topology), a different iteration from the
+    # reference's, so both runs solve to a tighter threshold (1e-24 on
+    # (r.r)/(f.f)) and the solutions are compared
     m = decks.cantilever_hex(30, 6, 6)
     with tempfile.TemporaryDirectory() as td:
         deck = os.path.join(td, "deck.in")
