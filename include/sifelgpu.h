@@ -198,6 +198,17 @@ SGPU_API int sgpu_matrix_pcg_multi(sgpu_matrix m, int32_t nrhs, double *X, const
                                    double res, double zero, int64_t iv, int64_t *ani, double *ares,
                                    int32_t *status, sgpu_solve_info *info);
 
+/* All load cases with the aggregation preconditioner: nrhs (<= 128) flexible
+ * CGs (FP64, each with the criterion of symcomprow::cg_prec on its own
+ * column) sharing one hierarchy (built on first use, as for SGPU_PREC_AGG)
+ * and advanced together, so every kernel of the cycle treats all columns --
+ * each level's matrix is read once per sweep for all of them.  mode:
+ * SGPU_MIXED (FP32 cycle) or SGPU_FP64.  Arguments as sgpu_matrix_pcg_multi;
+ * info->iterations is the largest column count. */
+SGPU_API int sgpu_matrix_pcg_multi_agg(sgpu_matrix m, int32_t nrhs, double *X, const double *F, int64_t ni,
+                                       double res, double zero, int64_t iv, int32_t mode, int64_t *ani,
+                                       double *ares, int32_t *status, sgpu_solve_info *info);
+
 /* Many independent systems of uneven size (the diagonal blocks of m, in
  * order; sys_rows[k] equations each, summing to n) solved together: every
  * system its own Jacobi-PCG with the criterion of symcomprow::cg_prec, all

@@ -50,7 +50,7 @@
 #include <unordered_map>
 #include <vector>
 
-#include "sgpu_internal.cuh"
+#include "sgpu_amg.cuh"
 
 namespace sgpu {
 
@@ -976,84 +976,6 @@ int grid_for(int64_t work, int per_block = TPB) {
 // host side
 // ---------------------------------------------------------------------------
 
-template <typename T>
-struct LevelVecs {
-  DevBuf<T> b, x, x2, r, d, d2, res;
-  int alloc(size_t n) {
-    SGPU_TRY(b.alloc(n));
-    SGPU_TRY(x.alloc(n));
-    SGPU_TRY(x2.alloc(n));
-    SGPU_TRY(r.alloc(n));
-    SGPU_TRY(d.alloc(n));
-    SGPU_TRY(d2.alloc(n));
-    SGPU_TRY(res.alloc(n));
-    return SGPU_OK;
-  }
-};
-
-struct AmgLevel {
-  int nb = 0, b = 0, n = 0;
-  int64_t nblk = 0;
-  int layout = 0;  // 0 owned row-major blocks, 1 handle BSR3, 2 handle CSR
-  const int *browptr = nullptr, *bcol = nullptr;
-  DevBuf<int> own_browptr, own_bcol;
-  DevBuf<double> val64;  // owned coarse values (FP64), or the level-0 scaled FP64 copy
-  DevBuf<float> val32;   // owned coarse values (FP32)
-  DevBuf<double> dinv64;
-  DevBuf<float> dinv32;
-  DevBuf<double> dsq64;  // sqrt(dinv): the symmetric scaling of the Lanczos operator
-  DevBuf<float> dsq32;
-  bool unit_diag = false;
-  double lmax64 = 0.0, lmax32 = 0.0;
-  // transfer to the next level
-  int na = 0, k = 0;
-  DevBuf<int> agg, aggptr, aggnodes;
-  DevBuf<double> Q64;
-  DevBuf<float> Q32;
-  LevelVecs<double> v64;
-  LevelVecs<float> v32;
-};
-
-struct Amg {
-  int k0 = 0;             // near-null-space vectors given (0: translations)
-  DevBuf<double> B0;      // n x k0 as given
-  bool built = false;     // hierarchy (FP64 set-up) current
-  bool have32 = false;    // FP32 copies current
-  bool have64 = false;    // FP64 level-0 scaled copy current
-  std::vector<AmgLevel *> lv;
-  int nc = 0;             // coarsest (dense) equations
-  DevBuf<double> M64;
-  DevBuf<float> M32;
-  DevBuf<double> cb64, cx64;
-  DevBuf<float> cb32, cx32;
-  // options: Chebyshev degree, coarse-correction weight, smoothing interval
-  // [lmax/ratio, 1.1 lmax], largest dense coarsest level, coarse visits per
-  // level (1: V-cycle, 2: W-cycle), Lanczos steps of the lmax estimate
-  int deg = 1;
-  double ratio = 30.0, alpha = 1.7;
-  int coarse_max = 768;
-  int gamma = 2;       // visits of level 1 per level-0 cycle
-  int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
-  int lanczos_steps = 14;
-  // level objects by depth, kept when a hierarchy is discarded so that a
-  // rebuild of the same matrix reuses their device buffers
-  std::vector<AmgLevel *> pool;
-  ~Amg() {
-    for (AmgLevel *l : pool) delete l;
-  }
-  void clear() {
-    lv.clear();
-    built = have32 = have64 = false;
-  }
-  AmgLevel *take_level(size_t depth) {
-    while (pool.size() <= depth) pool.push_back(new AmgLevel());
-    AmgLevel *l = pool[depth];
-    l->unit_diag = false;
-    l->browptr = l->bcol = nullptr;
-    return l;
-  }
-};
-
 void amg_free(Amg *a) { delete a; }
 
 void amg_values_changed(sgpu_matrix m) {
@@ -1335,26 +1257,6 @@ int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_
 
 // ----- level SpMV dispatch --------------------------------------------------
 
-template <typename T>
-const T *level_vals(const sgpu_matrix m, const AmgLevel &L);
-template <>
-const float *level_vals<float>(const sgpu_matrix m, const AmgLevel &L) {
-  if (L.layout == 1) return m->bsr.bval32s.p;
-  if (L.layout == 2) return m->csr.val32s.p;
-  return L.val32.p;
-}
-template <>
-const double *level_vals<double>(const sgpu_matrix m, const AmgLevel &L) {
-  return L.val64.p;  // level 0: the scaled FP64 copy; coarse: owned values
-}
-
-template <typename T>
-const T *level_dinv(const AmgLevel &L);
-template <>
-const float *level_dinv<float>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dinv32.p; }
-template <>
-const double *level_dinv<double>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dinv64.p; }
-
 // resident blocks of a kernel, queried once and cached (no query inside a capture)
 template <class K>
 int resident_grid(K kern, int64_t warps_needed) {
@@ -1435,6 +1337,7 @@ int launch_level(sgpu_matrix m, const AmgLevel &L, const T *v, const Op &op, cud
   SGPU_CUDA(cudaGetLastError());
   return SGPU_OK;
 }
+
 
 template <typename T>
 const T *level_dsq(const AmgLevel &L);
@@ -1694,26 +1597,6 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
 }
 
 // ----- the V-cycle ------------------------------------------------------------
-
-struct Cheb {
-  double c2_first;             // 1/theta
-  double c1[8], c2[8];         // steps 1..deg-1
-};
-
-Cheb cheb_coeffs(double lmax, double ratio, int deg) {
-  Cheb c{};
-  const double a = lmax / ratio, b = 1.1 * lmax;
-  const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
-  c.c2_first = 1.0 / theta;
-  double rho = 1.0 / sigma;
-  for (int k = 1; k < deg && k < 8; k++) {
-    const double rn = 1.0 / (2.0 * sigma - rho);
-    c.c1[k] = rn * rho;
-    c.c2[k] = 2.0 * rn / delta;
-    rho = rn;
-  }
-  return c;
-}
 
 template <typename T>
 LevelVecs<T> &vecs(AmgLevel &L);
@@ -2018,15 +1901,8 @@ int fcg_solve(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, in
 
 }  // namespace
 
-int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int mode, int64_t *ani,
-                double *ares, sgpu_solve_info *info) {
+int amg_ensure(sgpu_matrix m, bool fp32, float *setup_ms) {
   cudaStream_t s = m->stream;
-  if (!m->csr.diag_positive)
-    return fail(SGPU_BAD_INPUT, "the aggregation preconditioner needs a positive diagonal (Jacobi scaling)");
-  SGPU_TRY(pcg_prepare(m, false));
-  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
-  const bool fp32 = (mode == SGPU_MIXED);
-  if (fp32 && !m->plan32.tuned) SGPU_TRY(spmv_autotune(m, 32));
   if (!m->amg) m->amg = new Amg();
   Amg &A = *m->amg;
   SGPU_CUDA(cudaEventRecord(m->ev0, s));
@@ -2038,8 +1914,23 @@ int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, 
   SGPU_TRY(amg_prepare_precision(m, fp32));
   SGPU_CUDA(cudaEventRecord(m->ev1, s));
   SGPU_CUDA(cudaEventSynchronize(m->ev1));
+  *setup_ms = 0.f;
+  SGPU_CUDA(cudaEventElapsedTime(setup_ms, m->ev0, m->ev1));
+  return SGPU_OK;
+}
+
+int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int mode, int64_t *ani,
+                double *ares, sgpu_solve_info *info) {
+  cudaStream_t s = m->stream;
+  if (!m->csr.diag_positive)
+    return fail(SGPU_BAD_INPUT, "the aggregation preconditioner needs a positive diagonal (Jacobi scaling)");
+  SGPU_TRY(pcg_prepare(m, false));
+  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
+  const bool fp32 = (mode == SGPU_MIXED);
+  if (fp32 && !m->plan32.tuned) SGPU_TRY(spmv_autotune(m, 32));
   float setup_ms = 0.f;
-  SGPU_CUDA(cudaEventElapsedTime(&setup_ms, m->ev0, m->ev1));
+  SGPU_TRY(amg_ensure(m, fp32, &setup_ms));
+  Amg &A = *m->amg;
   PcgState hs{};
   SGPU_CUDA(cudaEventRecord(m->ev0, s));
   int rc = fp32 ? fcg_solve<float>(m, ni, res, zero, iv, crit, &hs) : fcg_solve<double>(m, ni, res, zero, iv, crit, &hs);

@@ -1,0 +1,137 @@
+// Aggregation multilevel preconditioner: the hierarchy shared by the
+// single-vector solve (sgpu_amg.cu) and the many-load-case solve
+// (sgpu_amg_multi.cu).
+#pragma once
+
+#include <vector>
+
+#include "sgpu_internal.cuh"
+
+namespace sgpu {
+
+template <typename T>
+struct LevelVecs {
+  DevBuf<T> b, x, x2, r, d, d2, res;
+  int alloc(size_t n) {
+    SGPU_TRY(b.alloc(n));
+    SGPU_TRY(x.alloc(n));
+    SGPU_TRY(x2.alloc(n));
+    SGPU_TRY(r.alloc(n));
+    SGPU_TRY(d.alloc(n));
+    SGPU_TRY(d2.alloc(n));
+    SGPU_TRY(res.alloc(n));
+    return SGPU_OK;
+  }
+};
+
+struct AmgLevel {
+  int nb = 0, b = 0, n = 0;
+  int64_t nblk = 0;
+  int layout = 0;  // 0 owned row-major blocks, 1 handle BSR3, 2 handle CSR
+  const int *browptr = nullptr, *bcol = nullptr;
+  DevBuf<int> own_browptr, own_bcol;
+  DevBuf<double> val64;  // owned coarse values (FP64), or the level-0 scaled FP64 copy
+  DevBuf<float> val32;   // owned coarse values (FP32)
+  DevBuf<double> dinv64;
+  DevBuf<float> dinv32;
+  DevBuf<double> dsq64;  // sqrt(dinv): the symmetric scaling of the Lanczos operator
+  DevBuf<float> dsq32;
+  bool unit_diag = false;
+  double lmax64 = 0.0, lmax32 = 0.0;
+  // transfer to the next level
+  int na = 0, k = 0;
+  DevBuf<int> agg, aggptr, aggnodes;
+  DevBuf<double> Q64;
+  DevBuf<float> Q32;
+  LevelVecs<double> v64;
+  LevelVecs<float> v32;
+};
+
+struct Amg {
+  int k0 = 0;             // near-null-space vectors given (0: translations)
+  DevBuf<double> B0;      // n x k0 as given
+  bool built = false;     // hierarchy (FP64 set-up) current
+  bool have32 = false;    // FP32 copies current
+  bool have64 = false;    // FP64 level-0 scaled copy current
+  std::vector<AmgLevel *> lv;
+  int nc = 0;             // coarsest (dense) equations
+  DevBuf<double> M64;
+  DevBuf<float> M32;
+  DevBuf<double> cb64, cx64;
+  DevBuf<float> cb32, cx32;
+  // options: Chebyshev degree, coarse-correction weight, smoothing interval
+  // [lmax/ratio, 1.1 lmax], largest dense coarsest level, coarse visits per
+  // level (1: V-cycle, 2: W-cycle), Lanczos steps of the lmax estimate
+  int deg = 1;
+  double ratio = 30.0, alpha = 1.7;
+  int coarse_max = 768;
+  int gamma = 2;       // visits of level 1 per level-0 cycle
+  int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
+  int lanczos_steps = 14;
+  // level objects by depth, kept when a hierarchy is discarded so that a
+  // rebuild of the same matrix reuses their device buffers
+  std::vector<AmgLevel *> pool;
+  ~Amg() {
+    for (AmgLevel *l : pool) delete l;
+  }
+  void clear() {
+    lv.clear();
+    built = have32 = have64 = false;
+  }
+  AmgLevel *take_level(size_t depth) {
+    while (pool.size() <= depth) pool.push_back(new AmgLevel());
+    AmgLevel *l = pool[depth];
+    l->unit_diag = false;
+    l->browptr = l->bcol = nullptr;
+    return l;
+  }
+};
+
+
+// Chebyshev smoothing on [lmax/ratio, 1.1 lmax] of D^-1 A: the first step's
+// 1/theta and the recurrence coefficients of steps 1..deg-1
+struct Cheb {
+  double c2_first;             // 1/theta
+  double c1[8], c2[8];         // steps 1..deg-1
+};
+
+inline Cheb cheb_coeffs(double lmax, double ratio, int deg) {
+  Cheb c{};
+  const double a = lmax / ratio, b = 1.1 * lmax;
+  const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+  c.c2_first = 1.0 / theta;
+  double rho = 1.0 / sigma;
+  for (int k = 1; k < deg && k < 8; k++) {
+    const double rn = 1.0 / (2.0 * sigma - rho);
+    c.c1[k] = rn * rho;
+    c.c2[k] = 2.0 * rn / delta;
+    rho = rn;
+  }
+  return c;
+}
+
+template <typename T>
+const T *level_vals(const sgpu_matrix m, const AmgLevel &L);
+template <>
+inline const float *level_vals<float>(const sgpu_matrix m, const AmgLevel &L) {
+  if (L.layout == 1) return m->bsr.bval32s.p;
+  if (L.layout == 2) return m->csr.val32s.p;
+  return L.val32.p;
+}
+template <>
+inline const double *level_vals<double>(const sgpu_matrix m, const AmgLevel &L) {
+  return L.val64.p;  // level 0: the scaled FP64 copy; coarse: owned values
+}
+
+template <typename T>
+const T *level_dinv(const AmgLevel &L);
+template <>
+inline const float *level_dinv<float>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dinv32.p; }
+template <>
+inline const double *level_dinv<double>(const AmgLevel &L) { return L.unit_diag ? nullptr : L.dinv64.p; }
+
+// Builds the hierarchy if the handle has none (set-up in FP64) and the copies
+// of the requested cycle precision; set-up device time into *setup_ms.
+int amg_ensure(sgpu_matrix m, bool fp32, float *setup_ms);
+
+}  // namespace sgpu

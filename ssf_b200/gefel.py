@@ -222,24 +222,46 @@ class DeviceMatrix:
         return xx, Result(st, ani.value if got else None, ares.value if got else None, info.as_dict())
 
 
-def pcg_multi(dm: "DeviceMatrix", F, ni=100000, res=1e-20, zero=1e-30, X0=None):
-    """Every column of F (n x R, or R column blocks) solved together by the
-    batched Jacobi-PCG (one SpMM per iteration).  Returns X (n x R) and a
-    list of per-column Results."""
+def pcg_multi(dm: "DeviceMatrix", F, ni=100000, res=1e-20, zero=1e-30, X0=None, prec="jacobi", mode="fp64"):
+    """Every column of F (n x R) solved together: prec "jacobi" is the batched
+    Jacobi-PCG (one SpMM per iteration, FP64), "agg" the batched flexible CG
+    with the aggregation cycle (FP32 for mode "mixed").  Returns X (n x R)
+    and a list of per-column Results."""
     F = np.asarray(F, dtype=np.float64)
-    R = F.shape[1]
     Fc = np.ascontiguousarray(F.T)  # R column blocks of n
-    Xc = np.zeros_like(Fc) if X0 is None else np.ascontiguousarray(np.asarray(X0, dtype=np.float64).T)
+    X0c = None if X0 is None else np.ascontiguousarray(np.asarray(X0, dtype=np.float64).T)
+    Xc, out = pcg_multi_blocks(dm, Fc, ni, res, zero, X0c, prec, mode)
+    return Xc.T.copy(), out
+
+
+def pcg_multi_blocks(dm: "DeviceMatrix", Fc, ni=100000, res=1e-20, zero=1e-30, X0c=None, prec="jacobi",
+                     mode="fp64", Xc=None):
+    """pcg_multi on the reference's own layout (lhsrhs.cpp:72-74): Fc holds R
+    column blocks of n (an R x n C array), as does the returned Xc (written
+    into ``Xc`` when given, e.g. pinned host memory)."""
+    R = Fc.shape[0]
+    if Xc is None:
+        Xc = np.zeros_like(Fc) if X0c is None else np.array(X0c, dtype=np.float64)
+    elif X0c is not None:
+        Xc[...] = X0c
+    else:
+        Xc[...] = 0.0
+    X0 = X0c
     ani = np.full(R, -1, dtype=np.int64)
     ares = np.full(R, np.nan)
     st = np.zeros(R, dtype=np.int32)
     info = L.SolveInfo()
-    rc = L.lib().sgpu_matrix_pcg_multi(dm.h, R, Xc, Fc, int(ni), float(res), float(zero), 0 if X0 is None else 1,
-                                       ani.ctypes.data, ares.ctypes.data, st.ctypes.data, C.byref(info))
+    if PREC.get(prec, prec) == L.PREC_AGG:
+        rc = L.lib().sgpu_matrix_pcg_multi_agg(dm.h, R, Xc, Fc, int(ni), float(res), float(zero),
+                                               0 if X0 is None else 1, _mode(mode), ani.ctypes.data,
+                                               ares.ctypes.data, st.ctypes.data, C.byref(info))
+    else:
+        rc = L.lib().sgpu_matrix_pcg_multi(dm.h, R, Xc, Fc, int(ni), float(res), float(zero), 0 if X0 is None else 1,
+                                           ani.ctypes.data, ares.ctypes.data, st.ctypes.data, C.byref(info))
     L.check(rc, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN, L.ZERO_RHS))
     out = [Result(int(st[c]), int(ani[c]) if ani[c] >= 0 else None, float(ares[c]) if ani[c] >= 0 else None,
                   info.as_dict()) for c in range(R)]
-    return Xc.T.copy(), out
+    return Xc, out
 
 
 class gmatrix:

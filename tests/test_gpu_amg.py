@@ -107,3 +107,23 @@ def test_bad_nullspace_rejected(oracle, gpu_lib):
     with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
         with pytest.raises(L.SgpuError):
             dm.set_nullspace(np.ones((adr.size - 1, 2)))
+
+
+@pytest.mark.parametrize("mode,nrhs", [("mixed", 5), ("fp64", 40), ("mixed", 70)])
+def test_batched_load_cases(oracle, gpu_lib, mode, nrhs):
+    # every load case its own flexible CG, all sharing one hierarchy and every
+    # kernel: each column must reach the oracle's solution of its own system
+    m = decks.cantilever_top_loads(decks.cantilever_hex(24, 6, 6), nrhs, seed=3)
+    adr, ci, a = _oracle_system(oracle, m)
+    F = np.stack([oracle.load_vector(m, lc) for lc in range(nrhs)], axis=1)
+    F[:, 1] = 0.0  # a zero load case stops at once with its own status
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        X, res = gefel.pcg_multi(dm, F, res=1e-22, prec="agg", mode=mode)
+    assert res[1].status == L.ZERO_RHS and not np.any(X[:, 1])
+    for c in range(nrhs):
+        if c == 1:
+            continue
+        xo, st, _, _ = oracle.scr_cg_prec(adr, ci, a, F[:, c], ni=200000, res=1e-26)
+        assert res[c].status == L.OK and res[c].ani is not None
+        assert np.linalg.norm(X[:, c] - xo) / np.linalg.norm(xo) <= 1e-8, c
