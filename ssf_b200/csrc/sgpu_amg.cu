@@ -227,8 +227,10 @@ struct OpCheb {
 
 // level 0 in 3x3 block rows, values component-major per block row (as the
 // handle keeps them): LPR lanes per block row
+// (6 resident blocks per SM for FP32 -- 40 registers; 4 for FP64, whose
+// operators with the outer coupling need more registers)
 template <typename T, int LPR, class Op>
-__global__ void __launch_bounds__(TPB, 6) k_lv_bsr3(int nb, const int *__restrict__ browptr,
+__global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? 4 : 6) k_lv_bsr3(int nb, const int *__restrict__ browptr,
                                                    const int *__restrict__ bcol, const T *__restrict__ bval,
                                                    const T *__restrict__ v, Op op, PcgState *st,
                                                    double *partials, unsigned *ticket) {
@@ -302,6 +304,28 @@ __global__ void __launch_bounds__(TPB) k_lv_csr(int n, const int *__restrict__ r
   op_reduce<Op>(op, acc, st, partials, ticket);
 }
 
+// Loads a B x B row-major block (16-byte aligned: the value array is from
+// cudaMalloc and every block is B*B*sizeof(T) bytes, a multiple of 16 for
+// B = 6) with 16-byte loads; other sizes element by element.
+template <typename T, int B>
+__device__ __forceinline__ void load_block(const T *__restrict__ a, T (&v)[B * B]) {
+  constexpr int NB = B * B * (int)sizeof(T);
+  if constexpr (NB % 16 == 0) {
+    constexpr int PER = 16 / (int)sizeof(T);
+    const float4 *a4 = reinterpret_cast<const float4 *>(a);
+#pragma unroll
+    for (int t = 0; t < NB / 16; t++) {
+      const float4 w = __ldg(a4 + t);
+      const T *wt = reinterpret_cast<const T *>(&w);
+#pragma unroll
+      for (int u = 0; u < PER; u++) v[t * PER + u] = wt[u];
+    }
+  } else {
+#pragma unroll
+    for (int t = 0; t < B * B; t++) v[t] = __ldg(a + t);
+  }
+}
+
 // coarse levels: B x B blocks stored row-major, one warp per block row
 template <typename T, int B, class Op>
 __global__ void __launch_bounds__(TPB) k_lv_bsrb(int nb, const int *__restrict__ browptr,
@@ -320,14 +344,15 @@ __global__ void __launch_bounds__(TPB) k_lv_bsrb(int nb, const int *__restrict__
     for (int c = 0; c < B; c++) y[c] = 0;
     for (int k = s + lane; k < e; k += 32) {
       const int c = __ldg(bcol + k);
-      const T *a = bval + (size_t)k * B * B;
+      T a[B * B];
+      load_block<T, B>(bval + (size_t)k * B * B, a);
       T xv[B];
 #pragma unroll
       for (int q = 0; q < B; q++) xv[q] = __ldg(v + B * c + q);
 #pragma unroll
       for (int r = 0; r < B; r++) {
 #pragma unroll
-        for (int q = 0; q < B; q++) y[r] += __ldg(a + r * B + q) * xv[q];
+        for (int q = 0; q < B; q++) y[r] += a[r * B + q] * xv[q];
       }
     }
 #pragma unroll
@@ -1479,7 +1504,7 @@ int amg_build(sgpu_matrix m) {
   L0->n = n;
   L0->unit_diag = true;
   const int K = A.k0 > 0 ? A.k0 : L0->b;
-  DevBuf<double> Bcur, Bnext;
+  TmpBuf<double> Bcur(s), Bnext(s);
   SGPU_TRY(Bcur.alloc((size_t)n * K));
   k_nullspace0<<<grid_for(n), TPB, 0, s>>>(n, L0->b, A.k0, A.B0.p, m->csr.dscale.p, Bcur.p, K);
   count_launches(1);

@@ -304,6 +304,28 @@ __global__ void __launch_bounds__(TPB) k_mspmm_csr(int n, const int *__restrict_
   op_finish<Op, CPL>(op, acc, partials, ticket, cols, R, ms);
 }
 
+// Loads a B x B row-major block (16-byte aligned: the value array is from
+// cudaMalloc and every block is B*B*sizeof(T) bytes, a multiple of 16 for
+// B = 6) with 16-byte loads; other sizes element by element.
+template <typename T, int B>
+__device__ __forceinline__ void load_block(const T *__restrict__ a, T (&v)[B * B]) {
+  constexpr int NB = B * B * (int)sizeof(T);
+  if constexpr (NB % 16 == 0) {
+    constexpr int PER = 16 / (int)sizeof(T);
+    const float4 *a4 = reinterpret_cast<const float4 *>(a);
+#pragma unroll
+    for (int t = 0; t < NB / 16; t++) {
+      const float4 w = __ldg(a4 + t);
+      const T *wt = reinterpret_cast<const T *>(&w);
+#pragma unroll
+      for (int u = 0; u < PER; u++) v[t * PER + u] = wt[u];
+    }
+  } else {
+#pragma unroll
+    for (int t = 0; t < B * B; t++) v[t] = __ldg(a + t);
+  }
+}
+
 // B x B row-major blocks (coarse levels).  A coarse level has few block rows,
 // so each is split over SPLIT warps of a CTA (each takes every SPLIT-th
 // block); the partial sums meet in shared memory and the first warp of the
@@ -331,7 +353,8 @@ __global__ void __launch_bounds__(TPB) k_mspmm_bsrb(int nb, const int *__restric
 #pragma unroll 2
       for (int k = __ldg(browptr + br) + sub; k < __ldg(browptr + br + 1); k += SPLIT) {
         const int col = __ldg(bcol + k);
-        const T *a = bval + (size_t)k * B * B;
+        T a[B * B];
+        load_block<T, B>(bval + (size_t)k * B * B, a);
         const T *x0 = X + (size_t)(B * col) * RP + lane;
 #pragma unroll
         for (int c = 0; c < CPL; c++) {
@@ -342,7 +365,7 @@ __global__ void __launch_bounds__(TPB) k_mspmm_bsrb(int nb, const int *__restric
           for (int r = 0; r < B; r++) {
             T s = 0;
 #pragma unroll
-            for (int q = 0; q < B; q++) s += __ldg(a + r * B + q) * xv[q];
+            for (int q = 0; q < B; q++) s += a[r * B + q] * xv[q];
             y[r][c] += s;
           }
         }
