@@ -224,6 +224,19 @@ SGPU_API int sgpu_matrix_pcg_batch(sgpu_matrix m, int32_t nsys, const int64_t *s
                                    int64_t *ani, double *ares, int32_t *status, int64_t *iterations,
                                    sgpu_solve_info *info);
 
+/* The same uneven batch with the aggregation preconditioner: every system its
+ * own FP64 flexible CG (scalars, the criterion of symcomprow::cg_prec and
+ * ani/ares per system) while the hierarchy of the whole block-diagonal
+ * matrix -- whose aggregates never cross systems -- is shared, so every
+ * cycle kernel runs once for all systems; per-system sums are formed from
+ * per-row products in row order.  mode: SGPU_MIXED (FP32 cycle) or
+ * SGPU_FP64.  The near-null space comes from sgpu_matrix_set_nullspace on m
+ * (e.g. every plate's rigid-body modes).  x starts from 0. */
+SGPU_API int sgpu_matrix_pcg_batch_agg(sgpu_matrix m, int32_t nsys, const int64_t *sys_rows, double *x,
+                                       const double *f, int64_t ni, double res, double zero, int32_t mode,
+                                       int64_t *ani, double *ares, int32_t *status, int64_t *iterations,
+                                       sgpu_solve_info *info);
+
 /* ------------------------------------------------------------------------ */
 /* Assembly on the GPU                                                      */
 /* ------------------------------------------------------------------------ */

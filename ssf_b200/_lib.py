@@ -121,6 +121,8 @@ SIGNATURES = {
                               C.c_int),
     "sgpu_matrix_pcg_multi_agg": ([_vp, _i32, _pD, _pD, _i64, _dbl, _dbl, _i64, _i32, _vp, _vp, _vp,
                                    C.POINTER(SolveInfo)], C.c_int),
+    "sgpu_matrix_pcg_batch_agg": ([_vp, _i32, _pL, _pD, _pD, _i64, _dbl, _dbl, _i32, _vp, _vp, _vp, _vp,
+                                   C.POINTER(SolveInfo)], C.c_int),
     "sgpu_matrix_pcg_batch": ([_vp, _i32, _pL, _pD, _pD, _i64, _dbl, _dbl, _i32, _vp, _vp, _vp, _vp,
                                C.POINTER(SolveInfo)], C.c_int),
     "sgpu_assemble": ([C.POINTER(Mesh), C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),

@@ -220,6 +220,43 @@ struct OpCheb {
   }
 };
 
+// The same last step for many independent systems solved together: the
+// products z_i r_i and z_i q_i are written per row and summed per system
+// afterwards (k_bseg_*), since every system has its own scalars.
+template <typename T, bool FIRST>
+struct OpChebRows {
+  static constexpr int NV = 0;
+  const T *b, *x_in;
+  T *x;
+  const T *r, *d_in, *dinv;
+  T c1, c2;
+  const double *dscale, *r64, *q64;
+  double *zr, *zq;
+  __device__ void row(int i, T y, double *) const {
+    const T di_ = dinv ? dinv[i] : T(1);
+    T xi;
+    if (FIRST) xi = x_in[i] + c2 * (di_ * (b[i] - y));
+    else xi = x[i] + c1 * d_in[i] + c2 * (r[i] - di_ * y);
+    x[i] = xi;
+    const double z = dscale[i] * (double)xi;
+    zr[i] = z * r64[i];
+    zq[i] = z * q64[i];
+  }
+  __device__ static void finish(PcgState *, const double *) {}
+};
+
+// q = K p with the products p_i q_i (batched systems)
+struct OpStorePQ {
+  static constexpr int NV = 0;
+  const double *p;
+  double *q, *prod;
+  __device__ void row(int i, double y, double *) const {
+    q[i] = y;
+    prod[i] = p[i] * y;
+  }
+  __device__ static void finish(PcgState *, const double *) {}
+};
+
 // ---------------------------------------------------------------------------
 // level SpMV kernels: y = A v with a row operator.  Every kernel returns at
 // once when the solve has stopped (graph chunks past convergence are empty).
@@ -567,6 +604,191 @@ __global__ void __launch_bounds__(TPB) k_fcg_true(int n, const double *__restric
     st->true_rr = t[0];
     st->true_rel = st->nory > 0 ? sqrt(t[0] / st->nory) : 0.0;
   }
+}
+
+// ---------------------------------------------------------------------------
+// many independent systems (diagonal blocks of one matrix), each with its own
+// flexible CG scalars: rows carry products, one warp per system sums them in
+// row order (deterministic), then updates that system's state
+// ---------------------------------------------------------------------------
+struct BSys {
+  double ff, rr, rho, alpha, beta, ares;
+  long long it, it_restart, ani;
+  int done, status;
+};
+
+__device__ __forceinline__ double seg_sum(const double *__restrict__ v, long long r0, long long r1) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (long long i = r0 + lane; i < r1; i += 32) s += v[i];
+  return warp_sum(s);
+}
+
+// start of every system's recurrence: f.f and r.r
+__global__ void k_bseg_init(int nsys, const long long *__restrict__ sysptr, const double *__restrict__ pff,
+                            const double *__restrict__ prr, BSys *sys, double res) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int k = warp; k < nsys; k += nw) {
+    const double ff = seg_sum(pff, sysptr[k], sysptr[k + 1]);
+    const double rr = seg_sum(prr, sysptr[k], sysptr[k + 1]);
+    if (lane == 0) {
+      BSys &b = sys[k];
+      b.it_restart = b.it;
+      b.beta = 0.0;
+      if (b.done) continue;
+      b.ff = ff;
+      b.rr = rr;
+      if (ff < 1e-300) {
+        b.done = 1;
+        b.status = SGPU_ZERO_RHS;
+      } else if (rr < res * ff) {
+        b.done = 1;
+        b.ani = b.it;
+        b.ares = rr / ff;
+      }
+    }
+  }
+}
+
+__global__ void k_bseg_alpha(int nsys, const long long *__restrict__ sysptr, const double *__restrict__ ppq,
+                             BSys *sys) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int k = warp; k < nsys; k += nw) {
+    if (sys[k].done) {
+      if (lane == 0) sys[k].alpha = 0.0;
+      continue;
+    }
+    const double pq = seg_sum(ppq, sysptr[k], sysptr[k + 1]);
+    if (lane == 0) {
+      BSys &b = sys[k];
+      if (!(pq > 0.0)) {
+        b.done = 1;
+        b.status = SGPU_BREAKDOWN;
+        b.alpha = 0.0;
+      } else {
+        b.alpha = b.rho / pq;
+      }
+    }
+  }
+}
+
+__global__ void k_bseg_rr(int nsys, const long long *__restrict__ sysptr, const double *__restrict__ prr, BSys *sys,
+                          long long ni, double res) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int k = warp; k < nsys; k += nw) {
+    if (sys[k].done) continue;
+    const double rr = seg_sum(prr, sysptr[k], sysptr[k + 1]);
+    if (lane == 0) {
+      BSys &b = sys[k];
+      b.it += 1;
+      b.rr = rr;
+      if (rr < res * b.ff) {  // (r.r)/(f.f) < res per system, symcomprow::cg_prec's test
+        b.done = 1;
+        b.ani = b.it;
+        b.ares = rr / b.ff;
+      } else if (b.it >= ni) {
+        b.done = 1;
+        b.status = SGPU_NOT_CONVERGED;
+      }
+    }
+  }
+}
+
+__global__ void k_bseg_beta(int nsys, const long long *__restrict__ sysptr, const double *__restrict__ pzr,
+                            const double *__restrict__ pzq, BSys *sys) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int k = warp; k < nsys; k += nw) {
+    if (sys[k].done) continue;
+    const double rz = seg_sum(pzr, sysptr[k], sysptr[k + 1]);
+    const double zq = seg_sum(pzq, sysptr[k], sysptr[k + 1]);
+    if (lane == 0) {
+      BSys &b = sys[k];
+      if (!(rz > 0.0) || !isfinite(zq)) {
+        b.done = 1;
+        b.status = SGPU_BREAKDOWN;
+      } else {
+        b.beta = b.it > b.it_restart ? -b.alpha * zq / b.rho : 0.0;
+        b.rho = rz;
+      }
+    }
+  }
+}
+
+// the solve stops (every kernel returns at once) when no system is active
+__global__ void k_bcount(int nsys, const BSys *sys, PcgState *st) {
+  __shared__ int act;
+  if (threadIdx.x == 0) act = 0;
+  __syncthreads();
+  int c = 0;
+  for (int k = threadIdx.x; k < nsys; k += blockDim.x) c += sys[k].done ? 0 : 1;
+  if (c) atomicAdd(&act, c);
+  __syncthreads();
+  if (threadIdx.x == 0 && act == 0) st->done = 1;
+}
+
+// r = f - q (q = K x0), the products f_i^2 and r_i^2, level-0 right-hand side
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_b_init_rows(int n, const double *__restrict__ f, const double *__restrict__ q,
+                                                     double *__restrict__ r, const double *__restrict__ dscale,
+                                                     T *__restrict__ b0, T *__restrict__ r0, T *__restrict__ d0,
+                                                     T *__restrict__ x0, T c2, double *__restrict__ pff,
+                                                     double *__restrict__ prr) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double fi = f[i], ri = fi - q[i];
+    r[i] = ri;
+    pff[i] = fi * fi;
+    prr[i] = ri * ri;
+    const T bi = (T)(dscale[i] * ri);
+    b0[i] = bi;
+    r0[i] = bi;
+    d0[i] = c2 * bi;
+    x0[i] = c2 * bi;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_b_update(int n, const int *__restrict__ rowsys, const BSys *sys,
+                                                  double *__restrict__ x, double *__restrict__ r,
+                                                  const double *__restrict__ p, const double *__restrict__ q,
+                                                  const double *__restrict__ dscale, T *__restrict__ b0,
+                                                  T *__restrict__ r0, T *__restrict__ d0, T *__restrict__ x0, T c2,
+                                                  double *__restrict__ prr, const PcgState *st) {
+  if (st->done) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double al = sys[rowsys[i]].alpha;
+    x[i] += al * p[i];
+    const double ri = r[i] - al * q[i];
+    r[i] = ri;
+    prr[i] = ri * ri;
+    const T bi = (T)(dscale[i] * ri);
+    b0[i] = bi;
+    r0[i] = bi;
+    d0[i] = c2 * bi;
+    x0[i] = c2 * bi;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_b_dir(int n, const int *__restrict__ rowsys, const BSys *sys,
+                                               double *__restrict__ p, const T *__restrict__ x0,
+                                               const double *__restrict__ dscale, const PcgState *st) {
+  if (st->done) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const BSys &b = sys[rowsys[i]];
+    if (b.done) continue;
+    p[i] = dscale[i] * (double)x0[i] + b.beta * p[i];
+  }
+}
+
+__global__ void k_b_rowsys(int nsys, const long long *__restrict__ sysptr, int *__restrict__ rowsys) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int k = warp; k < nsys; k += nw)
+    for (long long i = sysptr[k] + lane; i < sysptr[k + 1]; i += 32) rowsys[i] = k;
 }
 
 // ---------------------------------------------------------------------------
@@ -1689,7 +1911,11 @@ int cheb_steps(sgpu_matrix m, AmgLevel &L, const Cheb &c, int deg, T *x, T **din
   Work &w = m->w;
   for (int k = 1; k < deg; k++) {
     const bool last = (k == deg - 1);
-    if (outer && last) {
+    if (outer && last && m->amg->batch_zr) {
+      OpChebRows<T, false> op{V.b.p, nullptr, x, V.r.p, *din, level_dinv<T>(L), (T)c.c1[k], (T)c.c2[k],
+                              m->csr.dscale.p, w.r.p, w.p.p, m->amg->batch_zr, m->amg->batch_zq};
+      SGPU_TRY(launch_level<T>(m, L, *din, op, s, 0));
+    } else if (outer && last) {
       OpCheb<T, false, true> op{V.b.p, nullptr, x, V.r.p, *din, *dout, level_dinv<T>(L), (T)c.c1[k], (T)c.c2[k], 1,
                                 m->csr.dscale.p, w.r.p, w.p.p, w.h.p};
       SGPU_TRY(launch_level<T>(m, L, *din, op, s, 6));
@@ -1765,7 +1991,11 @@ int cycle(sgpu_matrix m, int l, bool zero_init, const std::vector<Cheb> &ch, std
   // post-smoothing: first step from x (SpMV of x, result in the other buffer)
   const bool outer = (l == 0);
   T *to = (xp == V.x.p) ? V.x2.p : V.x.p;
-  if (outer && deg == 1) {
+  if (outer && deg == 1 && A.batch_zr) {
+    OpChebRows<T, true> op{V.b.p, xp, to, nullptr, nullptr, level_dinv<T>(L), (T)0, (T)ch[l].c2_first,
+                           m->csr.dscale.p, w.r.p, w.p.p, A.batch_zr, A.batch_zq};
+    SGPU_TRY(launch_level<T>(m, L, xp, op, s, 0));
+  } else if (outer && deg == 1) {
     OpCheb<T, true, true> op{V.b.p, xp, to, V.r.p, nullptr, V.d.p, level_dinv<T>(L), (T)0, (T)ch[l].c2_first, 1,
                              m->csr.dscale.p, w.r.p, w.p.p, w.h.p};
     SGPU_TRY(launch_level<T>(m, L, xp, op, s, 6));
@@ -1991,6 +2221,191 @@ int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, 
     info->spmv_bytes = 0.0;
   }
   return hs.status;
+}
+
+
+// ---------------------------------------------------------------------------
+// many independent systems with the aggregation preconditioner
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+int batch_cycle_dir(sgpu_matrix m, const int *rowsys, const BSys *sys, cudaStream_t s) {
+  Amg &A = *m->amg;
+  const int nl = (int)A.lv.size();
+  std::vector<Cheb> ch(nl);
+  for (int l = 0; l < nl; l++)
+    ch[l] = cheb_coeffs(sizeof(T) == 4 ? A.lv[l]->lmax32 : A.lv[l]->lmax64, A.ratio, A.deg);
+  std::vector<T *> xcur(nl + 1, nullptr);
+  SGPU_TRY(cycle<T>(m, 0, true, ch, xcur, s));
+  k_b_dir<T><<<grid_for(m->n), TPB, 0, s>>>((int)m->n, rowsys, sys, m->w.d.p, xcur[0], m->csr.dscale.p, pcg_state(m));
+  count_launches(1);
+  return SGPU_OK;
+}
+
+// the outer FP64 product q = K p with the products p_i q_i
+int batch_spmv64(sgpu_matrix m, const double *p, double *q, double *prod, cudaStream_t s) {
+  PcgState *st = pcg_state(m);
+  OpStorePQ op{p, q, prod};
+  if (m->bsr.valid) {
+    auto k = k_lv_bsr3<double, 32, OpStorePQ>;
+    k<<<resident_grid(k, m->bsr.nb), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval.p, p, op,
+                                                  st, m->w.partials.p, m->w.counters.p);
+  } else {
+    auto k = k_lv_csr<double, 8, OpStorePQ>;
+    k<<<resident_grid(k, (m->n + 3) / 4), TPB, 0, s>>>((int)m->n, m->csr.rowptr.p, m->csr.col.p, m->csr.val.p, p, op,
+                                                        st, m->w.partials.p, m->w.counters.p);
+  }
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+template <typename T>
+int batch_solve(sgpu_matrix m, int nsys, const long long *sysptr, const int *rowsys, BSys *sys, double *pff,
+                double *prr, double *ppq, int64_t ni, double res, PcgState *hs) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  Amg &A = *m->amg;
+  const int n = (int)m->n;
+  const int g = grid_for(n);
+  const int gs = grid_for((int64_t)nsys * 32);
+  AmgLevel &L0 = *A.lv[0];
+  LevelVecs<T> &V = vecs<T>(L0);
+  const T c2 = (T)cheb_coeffs(sizeof(T) == 4 ? L0.lmax32 : L0.lmax64, A.ratio, A.deg).c2_first;
+  PcgState init{};
+  SGPU_TRY(write_st(m, &init));
+  // start: x = 0, r = f
+  SGPU_CUDA(cudaMemsetAsync(w.x.p, 0, (size_t)n * sizeof(double), s));
+  SGPU_CUDA(cudaMemsetAsync(w.p.p, 0, (size_t)n * sizeof(double), s));
+  SGPU_CUDA(cudaMemsetAsync(w.d.p, 0, (size_t)n * sizeof(double), s));
+  k_b_init_rows<T><<<g, TPB, 0, s>>>(n, w.f.p, w.p.p, w.r.p, m->csr.dscale.p, V.b.p, V.r.p, V.d.p, V.x.p, c2, pff,
+                                     prr);
+  k_bseg_init<<<gs, TPB, 0, s>>>(nsys, sysptr, pff, prr, sys, res);
+  k_bcount<<<1, TPB, 0, s>>>(nsys, sys, pcg_state(m));
+  count_launches(3);
+  SGPU_TRY(batch_cycle_dir<T>(m, rowsys, sys, s));
+  k_bseg_beta<<<gs, TPB, 0, s>>>(nsys, sysptr, A.batch_zr, A.batch_zq, sys);
+  count_launches(1);
+  // (k_b_dir ran before the first beta: p = S x0, beta = 0 at a start)
+  cudaGraph_t graph;
+  cudaGraphExec_t exec = nullptr;
+  const int64_t before = sgpu_kernel_launches();
+  SGPU_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  int rc = SGPU_OK;
+  for (int it = 0; it < 8 && rc == SGPU_OK; it++) {
+    rc = batch_spmv64(m, w.d.p, w.p.p, ppq, s);
+    if (rc != SGPU_OK) break;
+    k_bseg_alpha<<<gs, TPB, 0, s>>>(nsys, sysptr, ppq, sys);
+    k_b_update<T><<<g, TPB, 0, s>>>(n, rowsys, sys, w.x.p, w.r.p, w.d.p, w.p.p, m->csr.dscale.p, V.b.p, V.r.p, V.d.p,
+                                    V.x.p, c2, prr, pcg_state(m));
+    k_bseg_rr<<<gs, TPB, 0, s>>>(nsys, sysptr, prr, sys, (long long)ni, res);
+    k_bcount<<<1, TPB, 0, s>>>(nsys, sys, pcg_state(m));
+    count_launches(4);
+    // the new residual's preconditioned direction: cycle, beta, then p
+    Amg &Ar = *m->amg;
+    const int nl = (int)Ar.lv.size();
+    std::vector<Cheb> ch(nl);
+    for (int l = 0; l < nl; l++)
+      ch[l] = cheb_coeffs(sizeof(T) == 4 ? Ar.lv[l]->lmax32 : Ar.lv[l]->lmax64, Ar.ratio, Ar.deg);
+    std::vector<T *> xcur(nl + 1, nullptr);
+    rc = cycle<T>(m, 0, true, ch, xcur, s);
+    if (rc != SGPU_OK) break;
+    k_bseg_beta<<<gs, TPB, 0, s>>>(nsys, sysptr, A.batch_zr, A.batch_zq, sys);
+    k_b_dir<T><<<g, TPB, 0, s>>>(n, rowsys, sys, w.d.p, xcur[0], m->csr.dscale.p, pcg_state(m));
+    count_launches(2);
+  }
+  cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (rc != SGPU_OK) return rc;
+  if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  const int64_t nodes = sgpu_kernel_launches() - before;
+  count_launches(-nodes);
+  for (int64_t it = 0;; it += 8) {
+    SGPU_TRY(read_st(m, hs));
+    if (hs->done || it > ni + 8) break;
+    e = cudaGraphLaunch(exec, s);
+    if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
+    count_launches(nodes);
+  }
+  cudaGraphExecDestroy(exec);
+  return rc;
+}
+
+}  // namespace
+
+int amg_batch_run(sgpu_matrix m, int nsys, const int64_t *sys_rows, double *x, const double *f, int64_t ni,
+                  double res, int mode, int64_t *ani, double *ares, int32_t *status, int64_t *iterations,
+                  sgpu_solve_info *info) {
+  cudaStream_t s = m->stream;
+  const int64_t n = m->n;
+  std::vector<long long> ptr(nsys + 1, 0);
+  for (int k = 0; k < nsys; k++) {
+    if (sys_rows[k] <= 0) return fail(SGPU_BAD_INPUT, "every system needs at least one equation");
+    ptr[k + 1] = ptr[k] + sys_rows[k];
+  }
+  if (ptr[nsys] != n) return fail(SGPU_BAD_INPUT, "system sizes do not add up to the matrix size");
+  if (!m->csr.diag_positive)
+    return fail(SGPU_BAD_INPUT, "the aggregation preconditioner needs a positive diagonal (Jacobi scaling)");
+  SGPU_TRY(pcg_prepare(m, false));
+  if (!m->plan64.tuned) SGPU_TRY(spmv_autotune(m, 64));
+  const bool fp32 = (mode == SGPU_MIXED);
+  if (fp32 && !m->plan32.tuned) SGPU_TRY(spmv_autotune(m, 32));
+  float setup_ms = 0.f;
+  SGPU_TRY(amg_ensure(m, fp32, &setup_ms));
+  Amg &A = *m->amg;
+  TmpBuf<long long> sysptr(s);
+  TmpBuf<int> rowsys(s);
+  TmpBuf<BSys> sys(s);
+  TmpBuf<double> pff(s), prr(s), ppq(s), pzr(s), pzq(s);
+  SGPU_TRY(sysptr.alloc(nsys + 1));
+  SGPU_TRY(rowsys.alloc(n));
+  SGPU_TRY(sys.alloc(nsys));
+  for (TmpBuf<double> *b : {&pff, &prr, &ppq, &pzr, &pzq}) SGPU_TRY(b->alloc(n));
+  SGPU_CUDA(cudaMemcpyAsync(sysptr.p, ptr.data(), (nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
+  std::vector<BSys> hsys(nsys);
+  for (auto &b : hsys) { memset(&b, 0, sizeof(b)); b.ani = -1; }
+  SGPU_CUDA(cudaMemcpyAsync(sys.p, hsys.data(), nsys * sizeof(BSys), cudaMemcpyHostToDevice, s));
+  SGPU_CUDA(cudaMemcpyAsync(m->w.f.p, f, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_b_rowsys<<<grid_for((int64_t)nsys * 32), TPB, 0, s>>>(nsys, sysptr.p, rowsys.p);
+  count_launches(1);
+  A.batch_zr = pzr.p;
+  A.batch_zq = pzq.p;
+  SGPU_CUDA(cudaEventRecord(m->ev0, s));
+  PcgState hs{};
+  int rc = fp32 ? batch_solve<float>(m, nsys, sysptr.p, rowsys.p, sys.p, pff.p, prr.p, ppq.p, ni, res, &hs)
+                : batch_solve<double>(m, nsys, sysptr.p, rowsys.p, sys.p, pff.p, prr.p, ppq.p, ni, res, &hs);
+  A.batch_zr = A.batch_zq = nullptr;
+  SGPU_CUDA(cudaEventRecord(m->ev1, s));
+  if (rc != SGPU_OK) return rc;
+  SGPU_CUDA(cudaMemcpyAsync(x, m->w.x.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaMemcpyAsync(hsys.data(), sys.p, nsys * sizeof(BSys), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  float solve_ms = 0.f;
+  SGPU_CUDA(cudaEventElapsedTime(&solve_ms, m->ev0, m->ev1));
+  int first_bad = SGPU_OK;
+  long long maxit = 0;
+  for (int k = 0; k < nsys; k++) {
+    const BSys &b = hsys[k];
+    if (status) status[k] = b.status;
+    if (iterations) iterations[k] = b.it;
+    if (b.status == SGPU_OK && b.done && b.ani >= 0) {
+      if (ani) ani[k] = b.ani;
+      if (ares) ares[k] = b.ares;
+    }
+    if (b.status != SGPU_OK && first_bad == SGPU_OK) first_bad = b.status;
+    maxit = std::max(maxit, b.it);
+  }
+  if (info) {
+    info->iterations = maxit;
+    info->solve_ms = solve_ms;
+    info->precond_setup_ms = setup_ms;
+    info->precond_levels = (int32_t)A.lv.size() + 1;
+    info->precond_coarse_n = A.nc;
+  }
+  return first_bad;
 }
 
 }  // namespace sgpu

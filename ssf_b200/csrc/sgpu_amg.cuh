@@ -68,6 +68,9 @@ struct Amg {
   int gamma = 2;       // visits of level 1 per level-0 cycle
   int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
   int lanczos_steps = 14;
+  // batched independent systems (sgpu_matrix_pcg_batch_agg): the level-0 last
+  // smoothing step writes the per-row products z r and z q here
+  double *batch_zr = nullptr, *batch_zq = nullptr;
   // level objects by depth, kept when a hierarchy is discarded so that a
   // rebuild of the same matrix reuses their device buffers
   std::vector<AmgLevel *> pool;

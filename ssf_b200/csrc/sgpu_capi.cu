@@ -241,6 +241,16 @@ int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B) {
   return amg_set_nullspace(m, k, B);
 }
 
+int sgpu_matrix_pcg_batch_agg(sgpu_matrix m, int32_t nsys, const int64_t *sys_rows, double *x, const double *f,
+                              int64_t ni, double res, double zero, int32_t mode, int64_t *ani, double *ares,
+                              int32_t *status, int64_t *iterations, sgpu_solve_info *info) {
+  (void)zero;
+  if (!m || !sys_rows || !x || !f) return fail(SGPU_BAD_INPUT, "null argument");
+  if (nsys < 1) return fail(SGPU_BAD_INPUT, "nsys must be positive");
+  if (info) memset(info, 0, sizeof(*info));
+  return amg_batch_run(m, nsys, sys_rows, x, f, ni, res, mode, ani, ares, status, iterations, info);
+}
+
 int sgpu_matrix_precond_clear(sgpu_matrix m) {
   if (!m) return fail(SGPU_BAD_INPUT, "null handle");
   amg_values_changed(m);

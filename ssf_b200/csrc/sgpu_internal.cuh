@@ -182,4 +182,7 @@ void amg_values_changed(sgpu_matrix m);
 int amg_set_nullspace(sgpu_matrix m, int k, const double *B_host);
 int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int mode,
                 int64_t *ani, double *ares, sgpu_solve_info *info);
+int amg_batch_run(sgpu_matrix m, int nsys, const int64_t *sys_rows, double *x, const double *f, int64_t ni,
+                  double res, int mode, int64_t *ani, double *ares, int32_t *status, int64_t *iterations,
+                  sgpu_solve_info *info);
 }  // namespace sgpu

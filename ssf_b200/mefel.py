@@ -167,10 +167,13 @@ def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20,
         Cm.close()
 
 
-def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True):
+def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True, prec="jacobi", mode="fp64"):
     """Many independent meshes (e.g. the uneven plate batch) assembled in one
-    call and solved by the batched PCG in one launch sequence.  Returns the
-    list of solutions, per-system (status, ani, ares, iterations) and info."""
+    call and solved together: prec "jacobi" is the batched Jacobi-PCG (FP64,
+    segment work units), "agg" the batched flexible CGs with the aggregation
+    cycle of the whole block-diagonal matrix (FP32 cycle for mode "mixed").
+    Returns the list of solutions, per-system (status, ani, ares, iterations)
+    and info."""
     from .decks import merge_meshes
     merged, rows = merge_meshes(meshes)
     K = stiffness_matrix(merged)
@@ -183,9 +186,15 @@ def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True):
         st = np.zeros(nsys, dtype=np.int32)
         its = np.zeros(nsys, dtype=np.int64)
         info = L.SolveInfo()
-        rc = L.lib().sgpu_matrix_pcg_batch(K.h, nsys, rows, x, f, int(ni), float(res), float(zero), int(tune),
-                                           ani.ctypes.data, ares.ctypes.data, st.ctypes.data, its.ctypes.data,
-                                           C.byref(info))
+        if prec == "agg":
+            K.set_nullspace(rigid_body_modes(merged))
+            rc = L.lib().sgpu_matrix_pcg_batch_agg(K.h, nsys, rows, x, f, int(ni), float(res), float(zero),
+                                                   {"fp64": L.FP64, "mixed": L.MIXED}[mode], ani.ctypes.data,
+                                                   ares.ctypes.data, st.ctypes.data, its.ctypes.data, C.byref(info))
+        else:
+            rc = L.lib().sgpu_matrix_pcg_batch(K.h, nsys, rows, x, f, int(ni), float(res), float(zero), int(tune),
+                                               ani.ctypes.data, ares.ctypes.data, st.ctypes.data, its.ctypes.data,
+                                               C.byref(info))
         L.check(rc, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN, L.ZERO_RHS))
         offs = np.concatenate([[0], np.cumsum(rows)])
         xs = [x[offs[k]:offs[k + 1]] for k in range(nsys)]

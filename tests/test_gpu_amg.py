@@ -127,3 +127,19 @@ def test_batched_load_cases(oracle, gpu_lib, mode, nrhs):
         xo, st, _, _ = oracle.scr_cg_prec(adr, ci, a, F[:, c], ni=200000, res=1e-26)
         assert res[c].status == L.OK and res[c].ani is not None
         assert np.linalg.norm(X[:, c] - xo) / np.linalg.norm(xo) <= 1e-8, c
+
+
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+def test_uneven_batch(oracle, gpu_lib, mode):
+    # independent plates of uneven size in one block-diagonal matrix: every
+    # plate its own flexible CG, one shared hierarchy; each plate must reach
+    # the oracle's solution of its own system
+    plates = decks.plate_batch(12, seed=5, lo=8, hi=40)
+    xs, o = mefel.solve_batch(plates, res=1e-22, zero=1e-300, prec="agg", mode=mode)
+    assert (o["status"] == 0).all()
+    for k, p in enumerate(plates):
+        adr, ci, a = oracle.assemble(p, sym=True)
+        f = oracle.load_vector(p)
+        xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26, zero=1e-300)
+        assert np.linalg.norm(xs[k] - xo) / np.linalg.norm(xo) <= 1e-8, k
+        assert o["iterations"][k] < ani_o
