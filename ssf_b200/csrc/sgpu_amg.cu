@@ -1686,10 +1686,12 @@ int amg_build(sgpu_matrix m) {
   Amg &A = *m->amg;
   cudaStream_t s = m->stream;
   A.clear();
-  if (const char *o = env_or("SGPU_AMG")) {  // "deg,alpha,ratio,coarse_max,gamma,lanczos,gamma_deep" (tuning)
-    int deg = A.deg, cmax = A.coarse_max, gam = A.gamma, pw = A.lanczos_steps, gd = A.gamma_deep;
+  // "deg,alpha,ratio,coarse_max,gamma,lanczos,gamma_deep,dense_max" (tuning runs)
+  if (const char *o = env_or("SGPU_AMG")) {
+    int deg = A.deg, cmax = A.coarse_max, gam = A.gamma, pw = A.lanczos_steps, gd = A.gamma_deep, dm = A.dense_max;
     double al = A.alpha, ra = A.ratio;
-    if (sscanf(o, "%d,%lf,%lf,%d,%d,%d,%d", &deg, &al, &ra, &cmax, &gam, &pw, &gd) >= 1) {
+    if (sscanf(o, "%d,%lf,%lf,%d,%d,%d,%d,%d", &deg, &al, &ra, &cmax, &gam, &pw, &gd, &dm) >= 1) {
+      A.dense_max = std::max(0, std::min(dm, 4096));
       A.gamma_deep = std::max(1, std::min(gd, 2));
       A.deg = std::max(1, std::min(deg, 6));
       A.alpha = al;
@@ -1753,7 +1755,18 @@ int amg_build(sgpu_matrix m) {
     if (C->n <= A.coarse_max || C->nb * 10 > L.nb * 8) break;
   }
   AmgLevel *Cl = A.lv.back();
-  if (Cl->n > 4096) return fail(SGPU_BAD_INPUT, "aggregation did not reach a small coarsest level");
+  if (Cl->n > A.dense_max) {
+    // The coarsening stalled above the dense limit (many small independent
+    // components, e.g. a batch of systems, each down to one or a few
+    // aggregates): the last level stays a smoothing level and its "solve" is
+    // `bottom_deg` Chebyshev steps, which the flexible outer CG tolerates.
+    Cl->na = 0;
+    Cl->k = 0;
+    A.nc = 0;
+    A.built = true;
+    clk.mark("bottom level (smoothed, no dense inverse)");
+    return SGPU_OK;
+  }
   // coarsest: dense inverse
   A.nc = Cl->n;
   SGPU_TRY(A.M64.alloc((size_t)A.nc * A.nc));
@@ -1797,9 +1810,11 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
     for (size_t l = 0; l < A.lv.size(); l++) {
       AmgLevel &L = *A.lv[l];
       SGPU_TRY(L.v32.alloc(L.n));
-      SGPU_TRY(L.Q32.alloc((size_t)L.n * L.k));
-      k_to32<<<grid_for((int64_t)L.n * L.k), TPB, 0, s>>>((int64_t)L.n * L.k, L.Q64.p, L.Q32.p);
-      count_launches(1);
+      if (L.k > 0) {
+        SGPU_TRY(L.Q32.alloc((size_t)L.n * L.k));
+        k_to32<<<grid_for((int64_t)L.n * L.k), TPB, 0, s>>>((int64_t)L.n * L.k, L.Q64.p, L.Q32.p);
+        count_launches(1);
+      }
       if (L.layout == 0) {
         SGPU_TRY(L.val32.alloc((size_t)L.nblk * L.b * L.b));
         k_to32<<<grid_for((int64_t)L.nblk * L.b * L.b), TPB, 0, s>>>((int64_t)L.nblk * L.b * L.b, L.val64.p,
@@ -1811,11 +1826,13 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
       clk.mark("Lanczos bound");
       if (getenv("SGPU_AMG_VERBOSE")) fprintf(stderr, "amg level %zu: lmax (fp32) %.6g\n", l, L.lmax32);
     }
-    SGPU_TRY(A.M32.alloc((size_t)A.nc * A.nc));
-    k_to32<<<grid_for((int64_t)A.nc * A.nc), TPB, 0, s>>>((int64_t)A.nc * A.nc, A.M64.p, A.M32.p);
-    count_launches(1);
-    SGPU_TRY(A.cb32.alloc(A.nc));
-    SGPU_TRY(A.cx32.alloc(A.nc));
+    if (A.nc > 0) {
+      SGPU_TRY(A.M32.alloc((size_t)A.nc * A.nc));
+      k_to32<<<grid_for((int64_t)A.nc * A.nc), TPB, 0, s>>>((int64_t)A.nc * A.nc, A.M64.p, A.M32.p);
+      count_launches(1);
+      SGPU_TRY(A.cb32.alloc(A.nc));
+      SGPU_TRY(A.cx32.alloc(A.nc));
+    }
     SGPU_CUDA(cudaGetLastError());
     A.have32 = true;
   }
@@ -1953,6 +1970,22 @@ int cycle(sgpu_matrix m, int l, bool zero_init, const std::vector<Cheb> &ch, std
   }
   AmgLevel &L = *A.lv[l];
   LevelVecs<T> &V = vecs<T>(L);
+  if (l == nl - 1 && A.nc == 0) {
+    // bottom level without a dense inverse: bottom_deg Chebyshev steps
+    const Cheb cb = cheb_coeffs(sizeof(T) == 4 ? L.lmax32 : L.lmax64, A.ratio, A.bottom_deg);
+    T *xp = V.x.p;
+    if (!zero_init) {
+      T *from = xcur[l], *to = (from == V.x.p) ? V.x2.p : V.x.p;
+      OpCheb<T, true, false> op{V.b.p, from, to, V.r.p, nullptr, V.d.p, level_dinv<T>(L), (T)0, (T)cb.c2_first, 0,
+                                nullptr, nullptr, nullptr, nullptr};
+      SGPU_TRY(launch_level<T>(m, L, from, op, s, 0));
+      xp = to;
+    }
+    T *din = V.d.p, *dout = V.d2.p;
+    SGPU_TRY(cheb_steps<T>(m, L, cb, A.bottom_deg, xp, &din, &dout, false, s));
+    xcur[l] = xp;
+    return SGPU_OK;
+  }
   T *xp;
   // pre-smoothing
   if (zero_init) {

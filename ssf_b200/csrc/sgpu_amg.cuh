@@ -65,6 +65,8 @@ struct Amg {
   int deg = 1;
   double ratio = 30.0, alpha = 1.7;
   int coarse_max = 768;
+  int dense_max = 1024;  // larger coarsest levels are smoothed, not inverted
+  int bottom_deg = 8;    // Chebyshev steps of such a bottom level
   int gamma = 2;       // visits of level 1 per level-0 cycle
   int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
   int lanczos_steps = 14;

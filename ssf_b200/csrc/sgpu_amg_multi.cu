@@ -844,6 +844,27 @@ struct Multi {
     }
     const AmgLevel &L = *A->lv[l];
     MVecs<T> &V = lv[l];
+    if (l == nl - 1 && A->nc == 0) {  // bottom level without a dense inverse (as the single solve)
+      const Cheb cb = cheb_coeffs(sizeof(T) == 4 ? L.lmax32 : L.lmax64, A->ratio, A->bottom_deg);
+      T *xp = V.x;
+      if (!zero_init) {
+        T *from = xcur[l], *to = (from == V.x) ? V.x2 : V.x;
+        MOpCheb<T, true, false> op{V.b, from, to, V.r, nullptr, V.d, level_dinv<T>(L), (T)0, (T)cb.c2_first, 0, RP,
+                                   nullptr, nullptr, nullptr};
+        SGPU_TRY(level_product(l, from, op, 0));
+        xp = to;
+      }
+      T *din = V.d, *dout = V.d2;
+      for (int k = 1; k < A->bottom_deg; k++) {
+        const bool last = (k == A->bottom_deg - 1);
+        MOpCheb<T, false, false> op{V.b, nullptr, xp, V.r, din, dout, level_dinv<T>(L), (T)cb.c1[k], (T)cb.c2[k],
+                                    last ? 1 : 0, RP, nullptr, nullptr, nullptr};
+        SGPU_TRY(level_product(l, din, op, 0));
+        std::swap(din, dout);
+      }
+      xcur[l] = xp;
+      return SGPU_OK;
+    }
     T *xp;
     if (zero_init) {
       xp = V.x;
@@ -968,8 +989,8 @@ int run_multi(sgpu_matrix m, int R, double *Xh, const double *Fh, int64_t ni, do
       return SGPU_CUDA_ERROR;
     }
   }
-  M.cb = vec((size_t)A.nc * RP);
-  M.cx = vec((size_t)A.nc * RP);
+  M.cb = vec((size_t)std::max(A.nc, 1) * RP);
+  M.cx = vec((size_t)std::max(A.nc, 1) * RP);
   if (!M.cb || !M.cx) {
     cleanup();
     return SGPU_CUDA_ERROR;

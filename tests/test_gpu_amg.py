@@ -143,3 +143,22 @@ def test_uneven_batch(oracle, gpu_lib, mode):
         xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26, zero=1e-300)
         assert np.linalg.norm(xs[k] - xo) / np.linalg.norm(xo) <= 1e-8, k
         assert o["iterations"][k] < ani_o
+
+
+def test_smoothed_bottom_level(oracle, gpu_lib, monkeypatch):
+    # a coarsest level above the dense limit is smoothed instead of inverted
+    # (the tuning switch SGPU_AMG sets the limit to 0 here); the solve still
+    # reaches the oracle's solution, single and batched
+    monkeypatch.setenv("SGPU_AMG", "1,1.7,30,768,2,14,2,0")
+    m = decks.cantilever_hex(24, 6, 6)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x, r = dm.pcg(f, res=1e-22, prec="agg", mode="mixed")
+        assert r.status == L.OK and r.info["precond_coarse_n"] == 0
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+        X, res = gefel.pcg_multi(dm, np.stack([f, 2.0 * f], axis=1), res=1e-22, prec="agg", mode="mixed")
+        assert all(rr.status == L.OK for rr in res)
+        assert np.linalg.norm(X[:, 1] - 2.0 * xo) / np.linalg.norm(2.0 * xo) <= 1e-8
