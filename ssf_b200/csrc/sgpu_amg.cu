@@ -1135,21 +1135,121 @@ __global__ void k_dense_fill(int nb, int K, int nc, const int *__restrict__ brow
     }
 }
 
-// Inverse of an SPD matrix by Gauss-Jordan without pivoting, one launch per
-// pivot k, out of place (in -> out) so that no element is read after it has
-// been overwritten:
-//   out[k][k] = 1/p, out[k][j] = a[k][j]/p, out[i][k] = -a[i][k]/p,
-//   out[i][j] = a[i][j] - a[i][k] a[k][j]/p      (p = a[k][k])
-__global__ void k_gj_step(int n, int k, const double *__restrict__ a, double *__restrict__ out) {
-  const double p = 1.0 / a[(size_t)k * n + k];
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n * n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t / n), j = (int)(t - (int64_t)i * n);
-    double v;
-    if (i == k) v = (j == k) ? p : a[t] * p;
-    else if (j == k) v = -a[t] * p;
-    else v = a[t] - a[(size_t)i * n + k] * a[(size_t)k * n + j] * p;
-    out[t] = v;
+// Blocked Gauss-Jordan inverse (pivot blocks of 32, no pivoting: the matrix
+// is SPD, so every diagonal block of the successive Schur complements is):
+// for the block K of rows/columns [k0, k0 + bs):
+//   P = A[K,K]^-1                                   (k_bgj_diag, one CTA)
+//   A[K,j] = P A[K,j]              for j not in K   (k_bgj_rowpanel)
+//   A[i,j] -= A[i,K] A[K,j]        for i, j not in K (k_bgj_update, tiled)
+//   A[i,K] = -A[i,K] P, A[K,K] = P for i not in K   (k_bgj_colpanel)
+constexpr int GJB = 32;
+
+__global__ void __launch_bounds__(GJB *GJB) k_bgj_diag(int n, int k0, int bs, const double *__restrict__ A,
+                                                       double *__restrict__ P) {
+  __shared__ double d[GJB][GJB + 1];
+  __shared__ double col[GJB];
+  const int r = threadIdx.x / GJB, c = threadIdx.x % GJB;
+  d[r][c] = (r < bs && c < bs) ? A[(size_t)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+  __syncthreads();
+  for (int k = 0; k < GJB; k++) {
+    const double piv = 1.0 / d[k][k];
+    if (c == 0) col[r] = d[r][k];
+    __syncthreads();
+    double v = d[r][c];
+    if (r == k) v = (c == k) ? piv : v * piv;
+    else v = (c == k) ? -col[r] * piv : v - col[r] * d[k][c] * piv;
+    __syncthreads();
+    d[r][c] = v;
+    __syncthreads();
+  }
+  P[r * GJB + c] = d[r][c];
+}
+
+__global__ void __launch_bounds__(TPB) k_bgj_rowpanel(int n, int k0, int bs, const double *__restrict__ P,
+                                                      double *__restrict__ A) {
+  __shared__ double ps[GJB][GJB];
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) ps[t / GJB][t % GJB] = P[t];
+  __syncthreads();
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    if (j >= k0 && j < k0 + bs) continue;
+    double v[GJB];
+#pragma unroll
+    for (int k = 0; k < GJB; k++) v[k] = k < bs ? A[(size_t)(k0 + k) * n + j] : 0.0;
+    for (int r = 0; r < bs; r++) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < GJB; k++) s += ps[r][k] * v[k];
+      A[(size_t)(k0 + r) * n + j] = s;
+    }
+  }
+}
+
+// A[i,j] -= A[i,K] A[K,j] on 64 x 64 tiles (rows and columns of K skipped)
+__global__ void __launch_bounds__(TPB) k_bgj_update(int n, int k0, int bs, double *__restrict__ A) {
+  constexpr int TI = 64, TJ = 64;
+  __shared__ double ak[TI][GJB + 1];  // A[i, K]
+  __shared__ double kb[GJB][TJ];      // A[K, j]
+  const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+  for (int t = threadIdx.x; t < TI * GJB; t += blockDim.x) {
+    const int r = t / GJB, k = t % GJB, i = i0 + r;
+    ak[r][k] = (i < n && k < bs) ? A[(size_t)i * n + k0 + k] : 0.0;
+  }
+  for (int t = threadIdx.x; t < GJB * TJ; t += blockDim.x) {
+    const int k = t / TJ, c = t % TJ, j = j0 + c;
+    kb[k][c] = (j < n && k < bs) ? A[(size_t)(k0 + k) * n + j] : 0.0;
+  }
+  __syncthreads();
+  // 256 threads, 16 elements each: thread (ty, tx) owns rows ty + 16 a, column tx + ... 
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+#pragma unroll 8
+  for (int k = 0; k < GJB; k++) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) av[a] = ak[ty + 16 * a][k];
+#pragma unroll
+    for (int b = 0; b < 4; b++) bv[b] = kb[k][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int i = i0 + ty + 16 * a;
+    if (i >= n || (i >= k0 && i < k0 + bs)) continue;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int j = j0 + tx + 16 * b;
+      if (j >= n || (j >= k0 && j < k0 + bs)) continue;
+      A[(size_t)i * n + j] -= acc[a][b];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TPB) k_bgj_colpanel(int n, int k0, int bs, const double *__restrict__ P,
+                                                      double *__restrict__ A) {
+  __shared__ double ps[GJB][GJB];
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) ps[t / GJB][t % GJB] = P[t];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i >= k0 && i < k0 + bs) {
+      for (int c = 0; c < bs; c++) A[(size_t)i * n + k0 + c] = ps[i - k0][c];
+      continue;
+    }
+    double v[GJB];
+#pragma unroll
+    for (int k = 0; k < GJB; k++) v[k] = k < bs ? A[(size_t)i * n + k0 + k] : 0.0;
+    for (int c = 0; c < bs; c++) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < GJB; k++) s += v[k] * ps[k][c];
+      A[(size_t)i * n + k0 + c] = -s;
+    }
   }
 }
 
@@ -1223,6 +1323,8 @@ int grid_for(int64_t work, int per_block = TPB) {
 // host side
 // ---------------------------------------------------------------------------
 
+thread_local cudaStream_t amg_stream = nullptr;
+
 void amg_free(Amg *a) { delete a; }
 
 void amg_values_changed(sgpu_matrix m) {
@@ -1230,6 +1332,7 @@ void amg_values_changed(sgpu_matrix m) {
 }
 
 int amg_set_nullspace(sgpu_matrix m, int k, const double *B_host) {
+  amg_stream = m->stream;
   if (!m->amg) m->amg = new Amg();
   Amg &A = *m->amg;
   A.clear();
@@ -1774,17 +1877,18 @@ int amg_build(sgpu_matrix m) {
   k_dense_fill<<<grid_for(Cl->nb), TPB, 0, s>>>(Cl->nb, Cl->b, A.nc, Cl->browptr, Cl->bcol, Cl->val64.p, A.M64.p);
   k_unit_empty_diag<<<grid_for(A.nc), TPB, 0, s>>>(A.nc, A.M64.p);
   {
-    TmpBuf<double> other(s);
-    SGPU_TRY(other.alloc((size_t)A.nc * A.nc));
-    double *src = A.M64.p, *dst = other.p;
-    const int g = grid_for((int64_t)A.nc * A.nc);
-    for (int k = 0; k < A.nc; k++) {
-      k_gj_step<<<g, TPB, 0, s>>>(A.nc, k, src, dst);
-      std::swap(src, dst);
+    TmpBuf<double> P(s);
+    SGPU_TRY(P.alloc(GJB * GJB));
+    const int nc = A.nc;
+    const dim3 tiles((nc + 63) / 64, (nc + 63) / 64);
+    for (int k0 = 0; k0 < nc; k0 += GJB) {
+      const int bs = std::min(GJB, nc - k0);
+      k_bgj_diag<<<1, GJB * GJB, 0, s>>>(nc, k0, bs, A.M64.p, P.p);
+      k_bgj_rowpanel<<<grid_for(nc), TPB, 0, s>>>(nc, k0, bs, P.p, A.M64.p);
+      k_bgj_update<<<tiles, TPB, 0, s>>>(nc, k0, bs, A.M64.p);
+      k_bgj_colpanel<<<grid_for(nc), TPB, 0, s>>>(nc, k0, bs, P.p, A.M64.p);
     }
-    if (src != A.M64.p)
-      SGPU_CUDA(cudaMemcpyAsync(A.M64.p, src, (size_t)A.nc * A.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    count_launches(2 + A.nc);
+    count_launches(2 + 4 * ((nc + GJB - 1) / GJB));
   }
   SGPU_CUDA(cudaGetLastError());
   clk.mark("dense coarsest inverse");
@@ -2191,6 +2295,7 @@ int fcg_solve(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, in
 
 int amg_ensure(sgpu_matrix m, bool fp32, float *setup_ms) {
   cudaStream_t s = m->stream;
+  amg_stream = s;
   if (!m->amg) m->amg = new Amg();
   Amg &A = *m->amg;
   SGPU_CUDA(cudaEventRecord(m->ev0, s));

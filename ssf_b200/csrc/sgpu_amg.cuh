@@ -9,9 +9,43 @@
 
 namespace sgpu {
 
+// Device buffers of the hierarchy come from the device's stream-ordered
+// memory pool (the pool keeps freed memory, so building a hierarchy for a new
+// handle -- a batch solved handle after handle -- does not pay for cudaMalloc
+// and cudaFree and their device synchronisation).  The stream is the handle's,
+// set by the AMG entry points (amg_stream) before any allocation; a buffer is
+// freed on the stream it was allocated on, after the work queued there.
+extern thread_local cudaStream_t amg_stream;
+
+template <class T>
+struct PBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  PBuf() = default;
+  PBuf(const PBuf &) = delete;
+  PBuf &operator=(const PBuf &) = delete;
+  ~PBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    if (count <= n && p) return SGPU_OK;
+    release();
+    if (count == 0) count = 1;
+    s = amg_stream;
+    cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), s);
+    if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    n = count;
+    return SGPU_OK;
+  }
+};
+
 template <typename T>
 struct LevelVecs {
-  DevBuf<T> b, x, x2, r, d, d2, res;
+  PBuf<T> b, x, x2, r, d, d2, res;
   int alloc(size_t n) {
     SGPU_TRY(b.alloc(n));
     SGPU_TRY(x.alloc(n));
@@ -29,43 +63,43 @@ struct AmgLevel {
   int64_t nblk = 0;
   int layout = 0;  // 0 owned row-major blocks, 1 handle BSR3, 2 handle CSR
   const int *browptr = nullptr, *bcol = nullptr;
-  DevBuf<int> own_browptr, own_bcol;
-  DevBuf<double> val64;  // owned coarse values (FP64), or the level-0 scaled FP64 copy
-  DevBuf<float> val32;   // owned coarse values (FP32)
-  DevBuf<double> dinv64;
-  DevBuf<float> dinv32;
-  DevBuf<double> dsq64;  // sqrt(dinv): the symmetric scaling of the Lanczos operator
-  DevBuf<float> dsq32;
+  PBuf<int> own_browptr, own_bcol;
+  PBuf<double> val64;  // owned coarse values (FP64), or the level-0 scaled FP64 copy
+  PBuf<float> val32;   // owned coarse values (FP32)
+  PBuf<double> dinv64;
+  PBuf<float> dinv32;
+  PBuf<double> dsq64;  // sqrt(dinv): the symmetric scaling of the Lanczos operator
+  PBuf<float> dsq32;
   bool unit_diag = false;
   double lmax64 = 0.0, lmax32 = 0.0;
   // transfer to the next level
   int na = 0, k = 0;
-  DevBuf<int> agg, aggptr, aggnodes;
-  DevBuf<double> Q64;
-  DevBuf<float> Q32;
+  PBuf<int> agg, aggptr, aggnodes;
+  PBuf<double> Q64;
+  PBuf<float> Q32;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };
 
 struct Amg {
   int k0 = 0;             // near-null-space vectors given (0: translations)
-  DevBuf<double> B0;      // n x k0 as given
+  PBuf<double> B0;      // n x k0 as given
   bool built = false;     // hierarchy (FP64 set-up) current
   bool have32 = false;    // FP32 copies current
   bool have64 = false;    // FP64 level-0 scaled copy current
   std::vector<AmgLevel *> lv;
   int nc = 0;             // coarsest (dense) equations
-  DevBuf<double> M64;
-  DevBuf<float> M32;
-  DevBuf<double> cb64, cx64;
-  DevBuf<float> cb32, cx32;
+  PBuf<double> M64;
+  PBuf<float> M32;
+  PBuf<double> cb64, cx64;
+  PBuf<float> cb32, cx32;
   // options: Chebyshev degree, coarse-correction weight, smoothing interval
   // [lmax/ratio, 1.1 lmax], largest dense coarsest level, coarse visits per
   // level (1: V-cycle, 2: W-cycle), Lanczos steps of the lmax estimate
   int deg = 1;
   double ratio = 30.0, alpha = 1.7;
   int coarse_max = 768;
-  int dense_max = 1024;  // larger coarsest levels are smoothed, not inverted
+  int dense_max = 4096;  // larger coarsest levels are smoothed, not inverted
   int bottom_deg = 8;    // Chebyshev steps of such a bottom level
   int gamma = 2;       // visits of level 1 per level-0 cycle
   int gamma_deep = 2;  // visits of level l+1 per level-l cycle, l >= 1
