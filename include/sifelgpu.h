@@ -315,6 +315,14 @@ SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rh
                                   double dt, double alpha, int64_t nsteps, int64_t ni, double res, double zero,
                                   int64_t iv, int32_t prec, int32_t mode, int64_t *step_iterations,
                                   sgpu_solve_info *info);
+/* The v-form of the same trapezoid, nonstat_solv_vform_comp / one_step_linear
+ * (TRFEL/SRC/npsolvert.cpp:62, 367-480; nonstatsolver trapezoidv): dd = d +
+ * (1-alpha) dt v; f = rhs - K dd; A v = f (x starts from the previous v when
+ * iv = 1); d = dd + alpha dt v.  Arguments as sgpu_transient_dform. */
+SGPU_API int sgpu_transient_vform(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v,
+                                  double dt, double alpha, int64_t nsteps, int64_t ni, double res, double zero,
+                                  int64_t iv, int32_t prec, int32_t mode, int64_t *step_iterations,
+                                  sgpu_solve_info *info);
 
 /* ------------------------------------------------------------------------ */
 /* Solving without allocating device memory                                 */

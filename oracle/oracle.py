@@ -57,9 +57,10 @@ def lib():
         for f in (L.or_scr_cg_prec, L.or_cr_cg_prec):
             f.argtypes = [_L, _pL, _pL, _pD, _pD, _pD, _L, _D, _D, _L, C.POINTER(_L), C.POINTER(_D)]
             f.restype = C.c_int
-        L.or_trfel_step.argtypes = [_L, _pL, _pL, _pD, _pD, _pD, _pD, _pD, _pD, _D, _D, _L, _D, _D,
-                                    _L, C.POINTER(_L), C.POINTER(_D)]
-        L.or_trfel_step.restype = C.c_int
+        for f in (L.or_trfel_step, L.or_trfel_step_v):
+            f.argtypes = [_L, _pL, _pL, _pD, _pD, _pD, _pD, _pD, _pD, _D, _D, _L, _D, _D,
+                          _L, C.POINTER(_L), C.POINTER(_D)]
+            f.restype = C.c_int
         L.or_trfel_lift.argtypes = [_L, _pD, _pL, _pL, _pD, _pD, _pD]
         _lib = L
     return _lib
@@ -192,10 +193,11 @@ def trfel_lift(mesh, rnode):
     return rhs
 
 
-def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1, rnode=None):
-    """nsteps of linear_nonstat_solv_dform (TRFEL/SRC/npsolvert.cpp:1146-1230)
-    with K and C assembled once (their values do not change for linear
-    materials) and the lifting of time-constant prescribed values."""
+def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1, rnode=None, form="d"):
+    """nsteps of linear_nonstat_solv_dform (TRFEL/SRC/npsolvert.cpp:1146-1230,
+    form "d") or of the v-form's one_step_linear (npsolvert.cpp:367-480,
+    form "v") with K and C assembled once (their values do not change for
+    linear materials) and the lifting of time-constant prescribed values."""
     adr, ci, ka = assemble(mesh, sym=True, kind="hex8t_k")
     _, _, ca = assemble(mesh, sym=True, kind="hex8t_c")
     n = adr.size - 1
@@ -208,7 +210,8 @@ def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, i
     its = []
     for _ in range(nsteps):
         ani, ares = _L(-1), _D(0.0)
-        st = lib().or_trfel_step(n, adr, ci, ka, ca, work, rhs, d, v, dt, alpha, ni, res, zero, iv,
+        step = lib().or_trfel_step if form == "d" else lib().or_trfel_step_v
+        st = step(n, adr, ci, ka, ca, work, rhs, d, v, dt, alpha, ni, res, zero, iv,
                                  C.byref(ani), C.byref(ares))
         its.append((st, ani.value))
     return d, v, its

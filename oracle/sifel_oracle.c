@@ -621,6 +621,30 @@ int or_trfel_step(long n, const long *adr, const long *ci, const double *ka, con
   return st;
 }
 
+/* One linear step of the v-form generalized trapezoid, one_step_linear of
+ * nonstat_solv_vform_comp (TRFEL/SRC/npsolvert.cpp:367-480): predictor
+ * dd = d + (1-alpha) dt v; p = K dd (Kmat->gmxv before K is overwritten);
+ * A = alpha dt K + C (scalgm, addgm); f = rhs - p; A v = f (x from the
+ * previous v when iv = 1); d = dd + alpha dt v.  solution_correction is the
+ * identity for isotropic conduction. */
+int or_trfel_step_v(long n, const long *adr, const long *ci, const double *ka, const double *ca,
+                    double *work_a, const double *rhs, double *d, double *v, double dt,
+                    double alpha, long ni, double res, double zero, long iv, long *ani,
+                    double *ares) {
+  long negm = adr[n];
+  double *dd = (double *)malloc(n * sizeof(double)), *p = (double *)malloc(n * sizeof(double));
+  double *f = (double *)malloc(n * sizeof(double));
+  for (long j = 0; j < n; j++) dd[j] = d[j] + (1.0 - alpha) * dt * v[j];
+  or_scr_mxv(n, adr, ci, ka, dd, p);
+  for (long k = 0; k < negm; k++) work_a[k] = ka[k] * (dt * alpha);
+  for (long k = 0; k < negm; k++) work_a[k] += 1.0 * ca[k];
+  for (long j = 0; j < n; j++) f[j] = rhs[j] - p[j];
+  int st = or_scr_cg_prec(n, adr, ci, work_a, v, f, ni, res, zero, iv, ani, ares);
+  for (long j = 0; j < n; j++) d[j] = dd[j] + alpha * dt * v[j];
+  free(f); free(p); free(dd);
+  return st;
+}
+
 /* Dirichlet lifting of assemble_init (TRFEL/SRC/globmatt.cpp:1635-1760) for
  * linear hexahedra with isotropic conduction: r_e = nodal values given by
  * prescvalues() (globmatt.cpp:1057: prescribed values on prescribed DOFs,

@@ -117,6 +117,8 @@ SIGNATURES = {
     "sgpu_matrix_combine": ([_vp, _vp, _dbl, _dbl, C.POINTER(_vp)], C.c_int),
     "sgpu_transient_dform": ([_vp, _vp, _pD, _pD, _pD, _dbl, _dbl, _i64, _i64, _dbl, _dbl, _i64, _i32, _i32, _vp,
                               C.POINTER(SolveInfo)], C.c_int),
+    "sgpu_transient_vform": ([_vp, _vp, _pD, _pD, _pD, _dbl, _dbl, _i64, _i64, _dbl, _dbl, _i64, _i32, _i32, _vp,
+                              C.POINTER(SolveInfo)], C.c_int),
     "sgpu_matrix_pcg_multi": ([_vp, _i32, _pD, _pD, _i64, _dbl, _dbl, _i64, _vp, _vp, _vp, C.POINTER(SolveInfo)],
                               C.c_int),
     "sgpu_matrix_pcg_multi_agg": ([_vp, _i32, _pD, _pD, _i64, _dbl, _dbl, _i64, _i32, _vp, _vp, _vp,

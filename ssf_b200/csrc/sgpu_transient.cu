@@ -8,6 +8,10 @@
 //   f  = alpha dt rhs + p                              rhs = trfel_right_hand_side
 //   A d = f                                            ssle->solve_system (x starts from d)
 //   v  = (d - dd) / dt / alpha
+// The v-form of nonstat_solv_vform_comp (npsolvert.cpp:62, one_step_linear
+// at 367-480) solves for the rates instead:
+//   dd = d + (1 - alpha) dt v;  p = K dd;  f = rhs - p;  A v = f (x starts
+//   from v);  d = dd + alpha dt v
 // The reference re-integrates K and C every step (npsolvert.cpp:1160,1170);
 // for linear materials and a fixed time step their values do not change, so
 // here A is formed once on the device and every step is two vector kernels,
@@ -55,6 +59,17 @@ __global__ void k_rhs(int n, const double *__restrict__ rhs, const double *__res
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) f[i] = rhs[i] * c + p[i];
 }
 
+// v-form: f = rhs - p
+__global__ void k_rhs_v(int n, const double *__restrict__ rhs, const double *__restrict__ p, double *__restrict__ f) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) f[i] = rhs[i] - p[i];
+}
+
+// v-form: d = dd + alpha dt v
+__global__ void k_value(int n, const double *__restrict__ dd, const double *__restrict__ v, double c,
+                        double *__restrict__ d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = dd[i] + c * v[i];
+}
+
 // v = (d - dd) / dt / alpha
 __global__ void k_velocity(int n, const double *__restrict__ d, const double *__restrict__ dd, double dt,
                            double alpha, double *__restrict__ v) {
@@ -64,6 +79,106 @@ __global__ void k_velocity(int n, const double *__restrict__ d, const double *__
 
 bool same_pattern(sgpu_matrix a, sgpu_matrix b) {
   return a->n == b->n && a->csr.nnz == b->csr.nnz && a->src_negm == b->src_negm;
+}
+
+}  // namespace
+
+namespace {
+int transient(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v, double dt, double alpha,
+              int64_t nsteps, int64_t ni, double res, double zero, int64_t iv, int32_t prec, int32_t mode,
+              int64_t *step_iterations, sgpu_solve_info *info, bool vform) {
+  if (!K || !C || !rhs || !d || !v) return fail(SGPU_BAD_INPUT, "null argument");
+  if (!(dt > 0.0) || !(alpha > 0.0) || alpha > 1.0) return fail(SGPU_BAD_INPUT, "need dt > 0 and 0 < alpha <= 1");
+  if (nsteps < 0) return fail(SGPU_BAD_INPUT, "negative step count");
+  if (prec != SGPU_PREC_JACOBI && prec != SGPU_PREC_AGG) return fail(SGPU_BAD_INPUT, "prec: Jacobi or aggregation");
+  if (info) memset(info, 0, sizeof(*info));
+  sgpu_matrix A = nullptr;
+  // A = alpha dt K + C (scalgm then addgm, GEFEL/gmatrix.cpp:1848/1791)
+  SGPU_TRY(sgpu_matrix_combine(K, C, dt * alpha, 1.0, &A));
+  const int64_t n = K->n;
+  int status = SGPU_OK;
+  DevBuf<double> d_d, v_d, dd_d, rhs_d;
+  auto cleanup = [&](int st) {
+    cudaStream_t s = A->own_stream;
+    cudaEvent_t e0 = A->ev0, e1 = A->ev1;
+    cudaStreamSynchronize(A->stream);
+    delete A;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+    return st;
+  };
+  int st;
+  if ((st = d_d.alloc(n)) || (st = v_d.alloc(n)) || (st = dd_d.alloc(n)) || (st = rhs_d.alloc(n)) ||
+      (st = pcg_prepare(A, mode == SGPU_MIXED)) || (st = pcg_prepare(C, false)))
+    return cleanup(st);
+  cudaStream_t s = A->stream;
+  cudaStream_t c_stream_saved = C->stream, k_stream_saved = K->stream;
+  C->stream = s;  // C's (d-form) or K's (v-form) products run on A's stream for ordering
+  K->stream = s;
+  cudaMemcpyAsync(d_d.p, d, n * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(v_d.p, v, n * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(rhs_d.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s);
+  const int vb = blocks_for(n);
+  int64_t total_its = 0;
+  double total_ms = 0.0, last_true = 0.0, setup_ms = 0.0;
+  int32_t levels = 0, coarse_n = 0;
+  for (int64_t step = 0; step < nsteps; step++) {
+    k_predict<<<vb, TPB, 0, s>>>((int)n, d_d.p, v_d.p, (1.0 - alpha) * dt, dd_d.p);
+    count_launches(1);
+    if (vform) {
+      st = spmv64(K, dd_d.p, A->w.p.p, s);  // p = K dd  (A's p buffer as scratch)
+      if (st != SGPU_OK) break;
+      k_rhs_v<<<vb, TPB, 0, s>>>((int)n, rhs_d.p, A->w.p.p, work_f(A));
+      count_launches(1);
+      cudaMemcpyAsync(work_x(A), v_d.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    } else {
+      st = spmv64(C, dd_d.p, A->w.p.p, s);  // p = C dd
+      if (st != SGPU_OK) break;
+      k_rhs<<<vb, TPB, 0, s>>>((int)n, rhs_d.p, A->w.p.p, alpha * dt, work_f(A));
+      count_launches(1);
+      cudaMemcpyAsync(work_x(A), d_d.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    }
+    sgpu_solve_info si;
+    memset(&si, 0, sizeof(si));
+    int64_t ani = -1;
+    double ares = 0.0;
+    st = pcg_run(A, ni, res, zero, iv, SGPU_CRIT_SCR_PREC, prec, mode, &ani, &ares, &si);
+    if (st == SGPU_BAD_INPUT || st == SGPU_CUDA_ERROR) break;
+    if (st != SGPU_OK && status == SGPU_OK) status = st;
+    st = SGPU_OK;
+    if (step_iterations) step_iterations[step] = si.iterations;
+    total_its += si.iterations;
+    total_ms += si.solve_ms + si.precond_setup_ms;
+    setup_ms += si.precond_setup_ms;
+    levels = si.precond_levels;
+    coarse_n = si.precond_coarse_n;
+    last_true = si.true_relres;
+    if (vform) {
+      cudaMemcpyAsync(v_d.p, work_x(A), n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      k_value<<<vb, TPB, 0, s>>>((int)n, dd_d.p, v_d.p, alpha * dt, d_d.p);
+    } else {
+      cudaMemcpyAsync(d_d.p, work_x(A), n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      k_velocity<<<vb, TPB, 0, s>>>((int)n, d_d.p, dd_d.p, dt, alpha, v_d.p);
+    }
+    count_launches(1);
+  }
+  C->stream = c_stream_saved;
+  K->stream = k_stream_saved;
+  if (st != SGPU_OK) return cleanup(st);
+  cudaMemcpyAsync(d, d_d.p, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(v, v_d.p, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return cleanup(fail(SGPU_CUDA_ERROR, "transient copy-back failed"));
+  if (info) {
+    info->iterations = total_its;
+    info->solve_ms = total_ms;
+    info->true_relres = last_true;
+    info->precond_setup_ms = setup_ms;
+    info->precond_levels = levels;
+    info->precond_coarse_n = coarse_n;
+  }
+  cleanup(SGPU_OK);
+  return status;
 }
 
 }  // namespace
@@ -123,83 +238,13 @@ SGPU_API int sgpu_matrix_combine(sgpu_matrix K, sgpu_matrix C, double a, double 
 SGPU_API int sgpu_transient_dform(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v, double dt,
                                   double alpha, int64_t nsteps, int64_t ni, double res, double zero, int64_t iv,
                                   int32_t prec, int32_t mode, int64_t *step_iterations, sgpu_solve_info *info) {
-  if (!K || !C || !rhs || !d || !v) return fail(SGPU_BAD_INPUT, "null argument");
-  if (!(dt > 0.0) || !(alpha > 0.0) || alpha > 1.0) return fail(SGPU_BAD_INPUT, "need dt > 0 and 0 < alpha <= 1");
-  if (nsteps < 0) return fail(SGPU_BAD_INPUT, "negative step count");
-  if (prec != SGPU_PREC_JACOBI && prec != SGPU_PREC_AGG) return fail(SGPU_BAD_INPUT, "prec: Jacobi or aggregation");
-  if (info) memset(info, 0, sizeof(*info));
-  sgpu_matrix A = nullptr;
-  // A = alpha dt K + C (scalgm then addgm, GEFEL/gmatrix.cpp:1848/1791)
-  SGPU_TRY(sgpu_matrix_combine(K, C, dt * alpha, 1.0, &A));
-  const int64_t n = K->n;
-  int status = SGPU_OK;
-  DevBuf<double> d_d, v_d, dd_d, rhs_d;
-  auto cleanup = [&](int st) {
-    cudaStream_t s = A->own_stream;
-    cudaEvent_t e0 = A->ev0, e1 = A->ev1;
-    cudaStreamSynchronize(A->stream);
-    delete A;
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    if (s) cudaStreamDestroy(s);
-    return st;
-  };
-  int st;
-  if ((st = d_d.alloc(n)) || (st = v_d.alloc(n)) || (st = dd_d.alloc(n)) || (st = rhs_d.alloc(n)) ||
-      (st = pcg_prepare(A, mode == SGPU_MIXED)) || (st = pcg_prepare(C, false)))
-    return cleanup(st);
-  cudaStream_t s = A->stream;
-  cudaStream_t c_stream_saved = C->stream;
-  C->stream = s;  // C's products run on A's stream for ordering
-  cudaMemcpyAsync(d_d.p, d, n * sizeof(double), cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(v_d.p, v, n * sizeof(double), cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(rhs_d.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s);
-  const int vb = blocks_for(n);
-  int64_t total_its = 0;
-  double total_ms = 0.0, last_true = 0.0, setup_ms = 0.0;
-  int32_t levels = 0, coarse_n = 0;
-  for (int64_t step = 0; step < nsteps; step++) {
-    k_predict<<<vb, TPB, 0, s>>>((int)n, d_d.p, v_d.p, (1.0 - alpha) * dt, dd_d.p);
-    count_launches(1);
-    st = spmv64(C, dd_d.p, A->w.p.p, s);  // p = C dd  (A's p buffer as scratch)
-    if (st != SGPU_OK) break;
-    k_rhs<<<vb, TPB, 0, s>>>((int)n, rhs_d.p, A->w.p.p, alpha * dt, work_f(A));
-    count_launches(1);
-    cudaMemcpyAsync(work_x(A), d_d.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
-    sgpu_solve_info si;
-    memset(&si, 0, sizeof(si));
-    int64_t ani = -1;
-    double ares = 0.0;
-    st = pcg_run(A, ni, res, zero, iv, SGPU_CRIT_SCR_PREC, prec, mode, &ani, &ares, &si);
-    if (st == SGPU_BAD_INPUT || st == SGPU_CUDA_ERROR) break;
-    if (st != SGPU_OK && status == SGPU_OK) status = st;
-    st = SGPU_OK;
-    if (step_iterations) step_iterations[step] = si.iterations;
-    total_its += si.iterations;
-    total_ms += si.solve_ms + si.precond_setup_ms;
-    setup_ms += si.precond_setup_ms;
-    levels = si.precond_levels;
-    coarse_n = si.precond_coarse_n;
-    last_true = si.true_relres;
-    cudaMemcpyAsync(d_d.p, work_x(A), n * sizeof(double), cudaMemcpyDeviceToDevice, s);
-    k_velocity<<<vb, TPB, 0, s>>>((int)n, d_d.p, dd_d.p, dt, alpha, v_d.p);
-    count_launches(1);
-  }
-  C->stream = c_stream_saved;
-  if (st != SGPU_OK) return cleanup(st);
-  cudaMemcpyAsync(d, d_d.p, n * sizeof(double), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(v, v_d.p, n * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return cleanup(fail(SGPU_CUDA_ERROR, "transient copy-back failed"));
-  if (info) {
-    info->iterations = total_its;
-    info->solve_ms = total_ms;
-    info->true_relres = last_true;
-    info->precond_setup_ms = setup_ms;
-    info->precond_levels = levels;
-    info->precond_coarse_n = coarse_n;
-  }
-  cleanup(SGPU_OK);
-  return status;
+  return transient(K, C, rhs, d, v, dt, alpha, nsteps, ni, res, zero, iv, prec, mode, step_iterations, info, false);
+}
+
+SGPU_API int sgpu_transient_vform(sgpu_matrix K, sgpu_matrix C, const double *rhs, double *d, double *v, double dt,
+                                  double alpha, int64_t nsteps, int64_t ni, double res, double zero, int64_t iv,
+                                  int32_t prec, int32_t mode, int64_t *step_iterations, sgpu_solve_info *info) {
+  return transient(K, C, rhs, d, v, dt, alpha, nsteps, ni, res, zero, iv, prec, mode, step_iterations, info, true);
 }
 
 }  // extern "C"

@@ -302,7 +302,8 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
 
 def write_trfel_deck(mesh: Mesh, path: str, dt: float = 1.0, nsteps: int = 1, alpha: float = 1.0, ni: int = 20000,
                      res: float = 1.0e-20, iv: int = 1, precond: int = 1, rho: float = 1.0,
-                     title: str = "sifel-b200 synthetic transport deck", stationary: bool = False) -> None:
+                     title: str = "sifel-b200 synthetic transport deck", stationary: bool = False,
+                     form: str = "d") -> None:
     """Write a linear nonstationary heat-conduction TRFEL deck (positional).
 
     Token order as read by probdesct::read (TRFEL/SRC/probdesct.cpp:177-560;
@@ -327,8 +328,9 @@ def write_trfel_deck(mesh: Mesh, path: str, dt: float = 1.0, nsteps: int = 1, al
         L.append(f"20 {ni} {_fmt(res)} {iv}")
         L.append(f"{precond}")
     else:
-        # nonstatsolver trapezoidd(1) alpha; timecontr fixed(0) start end, one important time, constant dt
-        L.append(f"1 {_fmt(alpha)}")
+        # nonstatsolver trapezoidd(1) / trapezoidv(2) alpha; timecontr fixed(0) start end, one
+        # important time, constant dt
+        L.append(f"{1 if form == 'd' else 2} {_fmt(alpha)}")
         L.append(f"0 0.0 {_fmt(end)} 1 {_fmt(end)} 0 {_fmt(dt)}")
         # timetypeprint, hdbackup, storages, solver, capdiagonalization
         L.append("1\n0\n11 11")

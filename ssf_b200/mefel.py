@@ -140,11 +140,12 @@ def trfel_lift(K: DeviceMatrix, rnode) -> np.ndarray:
 
 
 def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1,
-                              mode="fp64", rnode=None, d0=None, v0=None, prec="jacobi"):
+                              mode="fp64", rnode=None, d0=None, v0=None, prec="jacobi", form="d"):
     """The d-form generalized trapezoid (TRFEL/SRC/npsolvert.cpp:1071) on the
     GPU: K and C assembled once, `nsteps` steps with everything on the device;
     ``prec`` "jacobi" (the reference's) or "agg" (aggregation multilevel, its
-    hierarchy built once for all steps).  Returns (d, v, per-step iterations,
+    hierarchy built once for all steps); ``form`` "v" runs the v-form of
+    nonstat_solv_vform_comp (npsolvert.cpp:62, trapezoidv) instead.  Returns (d, v, per-step iterations,
     solve info)."""
     K = conductivity_matrix(mesh)
     Cm = capacity_matrix(mesh)
@@ -158,13 +159,20 @@ def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20,
         info = L.SolveInfo()
         m = {"fp64": L.FP64, "mixed": L.MIXED}[mode]
         p = {"jacobi": L.PREC_JACOBI, "agg": L.PREC_AGG}[prec]
-        st = L.lib().sgpu_transient_dform(K.h, Cm.h, rhs, d, v, float(dt), float(alpha), int(nsteps), int(ni),
-                                          float(res), float(zero), int(iv), p, m, its.ctypes.data, C.byref(info))
+        fn = L.lib().sgpu_transient_dform if form == "d" else L.lib().sgpu_transient_vform
+        st = fn(K.h, Cm.h, rhs, d, v, float(dt), float(alpha), int(nsteps), int(ni), float(res), float(zero),
+                int(iv), p, m, its.ctypes.data, C.byref(info))
         L.check(st, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN))
         return d, v, its[:nsteps], info.as_dict()
     finally:
         K.close()
         Cm.close()
+
+
+def nonstat_solv_vform_comp(mesh, nsteps, dt, alpha=1.0, **kw):
+    """The v-form generalized trapezoid (TRFEL/SRC/npsolvert.cpp:62,
+    one_step_linear at 367-480) on the GPU."""
+    return linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=alpha, form="v", **kw)
 
 
 def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True, prec="jacobi", mode="fp64"):

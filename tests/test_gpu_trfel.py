@@ -50,6 +50,20 @@ def test_transient_mixed_form(oracle, gpu_lib):
     assert np.linalg.norm(d - d_o) / np.linalg.norm(d_o) <= 1e-7
 
 
+@pytest.mark.parametrize("alpha", [1.0, 0.5])
+def test_vform_steps_match_oracle(oracle, gpu_lib, alpha):
+    # trapezoidv: nonstat_solv_vform_comp (npsolvert.cpp:62) solves for the rates
+    from ssf_b200 import mefel
+    m = _cube()
+    d_o, v_o, its_o = oracle.trfel_steps(m, 3, 10.0, alpha=alpha, res=1e-24, iv=1, form="v")
+    assert all(st == 0 for st, _ in its_o)
+    d, v, its, info = mefel.nonstat_solv_vform_comp(m, 3, 10.0, alpha=alpha, res=1e-24, iv=1)
+    assert np.linalg.norm(d - d_o) / np.linalg.norm(d_o) <= 1e-8
+    assert np.linalg.norm(v - v_o) / np.linalg.norm(v_o) <= 1e-8
+    for (st, a_o), a in zip(its_o, its):
+        assert abs(int(a) - (a_o + 1)) <= 2
+
+
 @pytest.mark.parametrize("mode", ["mixed", "fp64"])
 def test_transient_aggregation_preconditioner(oracle, gpu_lib, mode):
     # the aggregation hierarchy is built on the first step and reused by the

@@ -45,11 +45,14 @@ def test_reference_solver_library_matches_oracle(ref):
     assert ani_r == ani_o and ares_r == ares_o and np.array_equal(x_r, x_o)
 
 
-def test_trfel_random_cube_bit_exact(ref):
+@pytest.mark.parametrize("form", ["d", "v"])
+def test_trfel_random_cube_bit_exact(ref, form):
+    # trapezoidd (linear_nonstat_solv_dform) and trapezoidv
+    # (nonstat_solv_vform_comp) decks through the compiled reference
     m = decks.heat_cube(3, seed=77)
     with tempfile.TemporaryDirectory() as td:
         deck = os.path.join(td, "c.in")
-        decks.write_trfel_deck(m, deck, dt=25.0, nsteps=2, alpha=0.5)
+        decks.write_trfel_deck(m, deck, dt=25.0, nsteps=2, alpha=0.5, form=form)
         d = ref.run_trfel_dump(deck, td)
-    T, V, its = ref.trfel_steps(m, 2, 25.0, alpha=0.5, iv=1)
+    T, V, its = ref.trfel_steps(m, 2, 25.0, alpha=0.5, iv=1, form=form)
     assert np.array_equal(T, d["T"]) and np.array_equal(V, d["V"])
