@@ -246,21 +246,25 @@ typedef enum {
   SGPU_ELEM_HEX8 = 0,    /* linhex, 3D elasticity, 2x2x2 Gauss (MEFEL/SRC/linhex.cpp:583) */
   SGPU_ELEM_QUAD4 = 1,   /* planeelemlq, plane stress, 2x2 Gauss (MEFEL/SRC/plelemlq.cpp:611) */
   SGPU_ELEM_HEX8T_K = 2, /* linhext conductivity (TRFEL/SRC/linhext.cpp:774) */
-  SGPU_ELEM_HEX8T_C = 3  /* linhext capacity (TRFEL/SRC/linhext.cpp:979) */
+  SGPU_ELEM_HEX8T_C = 3, /* linhext capacity (TRFEL/SRC/linhext.cpp:979) */
+  SGPU_ELEM_TET4 = 4,    /* lintet, 3D elasticity, 1 point (MEFEL/SRC/lintet.cpp:290) */
+  SGPU_ELEM_TRI3 = 5     /* planeelemlt, plane stress, 1 point (MEFEL/SRC/plelemlt.cpp:234) */
 } sgpu_elem_kind;
 
 /* A mesh in SIFEL's terms.  Node order inside an element follows SIFEL
- * (GEFEL/basefun.cpp:2299 for hexahedra, :609 for quadrilaterals). */
+ * (GEFEL/basefun.cpp:2299 for hexahedra, :609 for quadrilaterals); a
+ * tetrahedron must have det3d > 0 (GEFEL/matrix.cpp:3629), else
+ * sgpu_assemble fails with SGPU_BAD_INPUT as the reference aborts. */
 typedef struct {
   int32_t kind;          /* sgpu_elem_kind */
-  int32_t ndofn;         /* DOFs per node: 3 (hex8), 2 (quad4), 1 (hex8t) */
+  int32_t ndofn;         /* DOFs per node: 3 (hex8, tet4), 2 (quad4, tri3), 1 (hex8t) */
   int64_t nn;            /* nodes */
-  const double *coords;  /* nn x 3 (z ignored for quad4) */
+  const double *coords;  /* nn x 3 (z ignored for quad4, tri3) */
   int64_t ne;            /* elements */
   const int64_t *elems;  /* ne x nne, 0-based node ids */
   const int64_t *cn;     /* nn x ndofn code numbers (1-based, <= 0: no equation) */
   const double *emat;    /* ne x 2: (E, nu) for elasticity, (k, c) for hex8t */
-  const double *thick;   /* ne thicknesses (quad4), else NULL */
+  const double *thick;   /* ne thicknesses (quad4, tri3), else NULL */
   const double *rho;     /* ne densities (capacity), NULL = 1 */
 } sgpu_mesh;
 

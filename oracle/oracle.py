@@ -52,6 +52,10 @@ def lib():
         L.or_pattern.restype = _L
         L.or_assemble.argtypes = [C.c_int, C.c_int, _L, _pD, _pL, _pL, _pD, C.c_void_p, C.c_void_p,
                                   _pL, _pL, _pD]
+        L.or_assemble.restype = _L
+        L.or_tet4_ke.argtypes = [_pD, _D, _D, _pD]
+        L.or_tri3_ke.argtypes = [_pD, _D, _D, _pD, _pD]
+        L.or_tet4_ke.restype = C.c_int
         L.or_scr_mxv.argtypes = [_L, _pL, _pL, _pD, _pD, _pD]
         L.or_cr_mxv.argtypes = [_L, _pL, _pL, _pD, _pD, _pD]
         for f in (L.or_scr_cg_prec, L.or_cr_cg_prec):
@@ -84,6 +88,20 @@ def hex8_ke(xyz, E, nu):
     return ke.reshape(24, 24)
 
 
+def tet4_ke(xyz, E, nu):
+    ke = np.zeros(144)
+    if lib().or_tet4_ke(_f64(xyz).reshape(-1), float(E), float(nu), ke) != 0:
+        raise ValueError("negative volume (wrong node numbering)")
+    return ke.reshape(12, 12)
+
+
+def tri3_ke(xy, E, nu, t):
+    ke = np.zeros(36)
+    tt = _f64(np.broadcast_to(np.asarray(t, dtype=np.float64), (3,)))
+    lib().or_tri3_ke(_f64(xy).reshape(-1), float(E), float(nu), tt, ke)
+    return ke.reshape(6, 6)
+
+
 def quad4_ke(xy, E, nu, t):
     ke = np.zeros(64)
     tt = _f64(np.broadcast_to(np.asarray(t, dtype=np.float64), (4,)))
@@ -103,7 +121,7 @@ def hex8t_kc(xyz, k, c, rho=1.0):
 # mesh-level assembly
 # ----------------------------------------------------------------------------
 
-KIND = {"hex8": 0, "quad4": 1, "hex8t_k": 2, "hex8t_c": 3}
+KIND = {"hex8": 0, "quad4": 1, "hex8t_k": 2, "hex8t_c": 3, "tet4": 4, "tri3": 5}
 
 
 def element_code_numbers(mesh):
@@ -131,9 +149,11 @@ def assemble(mesh, sym=True, kind=None, rho=None):
     emat = _f64(mesh.mats[mesh.emat])
     thick = _f64(mesh.thick) if mesh.thick is not None else None
     rr = _f64(rho) if rho is not None else None
-    lib().or_assemble(k, int(sym), mesh.ne, _f64(mesh.coords), _i64(mesh.elems), cne, emat,
-                      thick.ctypes.data if thick is not None else None,
-                      rr.ctypes.data if rr is not None else None, adr, ci, a)
+    st = lib().or_assemble(k, int(sym), mesh.ne, _f64(mesh.coords), _i64(mesh.elems), cne, emat,
+                           thick.ctypes.data if thick is not None else None,
+                           rr.ctypes.data if rr is not None else None, adr, ci, a)
+    if st != 0:
+        raise ValueError(f"element {-st} has a negative volume (wrong node numbering)")
     return adr, ci, a
 
 

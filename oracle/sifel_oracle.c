@@ -205,6 +205,58 @@ void or_hex8_ke(const double *xyz, double e, double nu, double *ke) {
   }
 }
 
+/* det3d, GEFEL/matrix.cpp:3629-3660 (the active branch): six times the signed
+ * volume of the tetrahedron, (p0-p3) . ((p1-p3) x (p2-p3)). */
+static double det3d(const double *x, const double *y, const double *z) {
+  double a0 = x[0] - x[3], a1 = y[0] - y[3], a2 = z[0] - z[3];
+  double b0 = x[1] - x[3], b1 = y[1] - y[3], b2 = z[1] - z[3];
+  double c0 = x[2] - x[3], c1 = y[2] - y[3], c2 = z[2] - z[3];
+  return a0 * b1 * c2 + b0 * c1 * a2 + c0 * a1 * b2 - c0 * b1 * a2 - c1 * b2 * a0 - c2 * b0 * a1;
+}
+
+/* lintet::stiffness_matrix, MEFEL/SRC/lintet.cpp:290-315: one integration
+ * point; geom_matrix (lintet.cpp:213-240) takes the Cartesian gradients of the
+ * natural derivatives dx/dy/dz_bf_lin_tet (GEFEL/basefun.cpp:1974-2000)
+ * through derivatives_3d (GEFEL/difcalc.cpp:487-565, 4-node case) at
+ * (0.25, 0.25, 0.25); the weight is det3d/6, and a negative det3d (wrong node
+ * numbering) is an error.  xyz: 4 x (x,y,z).  Returns 0, or -1 on a negative
+ * volume (ke untouched then). */
+int or_tet4_ke(const double *xyz, double e, double nu, double *ke) {
+  static const double NX[4] = {1.0, 0.0, 0.0, -1.0}, NY[4] = {0.0, 1.0, 0.0, -1.0},
+                      NZ[4] = {0.0, 0.0, 1.0, -1.0};
+  double x[4], y[4], z[4], dx[4], dy[4], dz[4], gm[6 * 12], d[36];
+  for (int i = 0; i < 4; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
+  double det = det3d(x, y, z);
+  if (det < 0.0) return -1;
+  double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0, jac;
+  for (int i = 0; i < 4; i++) {
+    d1 += NX[i] * x[i]; d2 += NY[i] * x[i]; d3 += NZ[i] * x[i];
+    d4 += NX[i] * y[i]; d5 += NY[i] * y[i]; d6 += NZ[i] * y[i];
+    d7 += NX[i] * z[i]; d8 += NY[i] * z[i]; d9 += NZ[i] * z[i];
+  }
+  jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+  for (int i = 0; i < 4; i++) {
+    double ddx = NX[i], ddy = NY[i], ddz = NZ[i];
+    dx[i] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
+    dy[i] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
+    dz[i] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+  }
+  memset(gm, 0, sizeof(gm));
+  for (int a = 0; a < 4; a++) {
+    int jj = 3 * a, kk = 3 * a + 1, ll = 3 * a + 2;
+    gm[0 * 12 + jj] = dx[a];
+    gm[1 * 12 + kk] = dy[a];
+    gm[2 * 12 + ll] = dz[a];
+    gm[3 * 12 + kk] = dz[a]; gm[3 * 12 + ll] = dy[a];
+    gm[4 * 12 + jj] = dz[a]; gm[4 * 12 + ll] = dx[a];
+    gm[5 * 12 + jj] = dy[a]; gm[5 * 12 + kk] = dx[a];
+  }
+  matstiff_spacestr(e, nu, d);
+  memset(ke, 0, 144 * sizeof(double));
+  bdbjac(ke, gm, d, gm, det / 6.0, 6, 12);
+  return 0;
+}
+
 /* planeelemlq::gl_stiffness_matrix, MEFEL/SRC/plelemlq.cpp:611-690 with
  * geom_matrix (294-320); thickness interpolated from nodal values t[4]
  * (planeelemlq::approx, plelemlq.cpp:127). xy: 4 x (x,y). */
@@ -261,6 +313,35 @@ static void bdbj(double *k, const double *b, const double *d, double jac, int m,
       ii++; mm += n;
     }
   }
+}
+
+/* planeelemlt::stiffness_matrix, MEFEL/SRC/plelemlt.cpp:234-272: the
+ * constant-strain triangle.  det = twice the signed area; B from the
+ * area-coordinate coefficients plsb/plsc (GEFEL/basefun.cpp:394-416)
+ * (planeelemlt::geom_matrix, plelemlt.cpp:166-192); plane-stress D; the
+ * thickness interpolated at (1/3, 1/3) from nodal values t[3] through area
+ * coordinates (planeelemlt::approx_nat, :119-131, scprd order); weight
+ * thick*det/2 and the symmetric product bdbj.  No sign check: a clockwise
+ * triangle gives the negative matrix, as in the reference.  xy: 3 x (x,y). */
+void or_tri3_ke(const double *xy, double e, double nu, const double *t, double *ke) {
+  double x[3], y[3], b[3], c[3], gm[3 * 6], d[9], ac[3];
+  for (int i = 0; i < 3; i++) { x[i] = xy[2 * i]; y[i] = xy[2 * i + 1]; }
+  double det = (x[1] - x[0]) * (y[2] - y[0]) - (x[2] - x[0]) * (y[1] - y[0]);
+  b[0] = (y[1] - y[2]) / det; b[1] = (y[2] - y[0]) / det; b[2] = (y[0] - y[1]) / det;
+  c[0] = (x[2] - x[1]) / det; c[1] = (x[0] - x[2]) / det; c[2] = (x[1] - x[0]) / det;
+  memset(gm, 0, sizeof(gm));
+  gm[0 * 6 + 0] = b[0]; gm[0 * 6 + 2] = b[1]; gm[0 * 6 + 4] = b[2];
+  gm[1 * 6 + 1] = c[0]; gm[1 * 6 + 3] = c[1]; gm[1 * 6 + 5] = c[2];
+  gm[2 * 6 + 0] = c[0]; gm[2 * 6 + 1] = b[0]; gm[2 * 6 + 2] = c[1];
+  gm[2 * 6 + 3] = b[1]; gm[2 * 6 + 4] = c[2]; gm[2 * 6 + 5] = b[2];
+  matstiff_plstress(e, nu, d);
+  double xi = 1.0 / 3.0, eta = 1.0 / 3.0;
+  ac[0] = xi; ac[1] = eta; ac[2] = 1.0 - ac[0] - ac[1];
+  double thick = 0.0;
+  for (int i = 0; i < 3; i++) thick += ac[i] * t[i];
+  double jac = thick * det / 2.0;
+  memset(ke, 0, 36 * sizeof(double));
+  bdbj(ke, gm, d, jac, 3, 6);
 }
 
 /* nnj, GEFEL/matrix.cpp:3149-3174 (single row N) */
@@ -439,18 +520,27 @@ void or_cr_localize(long *adr, long *ci, double *a, const double *b, const long 
 /* ------------------------------------------------------------------------ */
 
 /* kind 0 = hex8 elasticity, 1 = quad4 plane stress, 2 = hex8 conduction,
- * 3 = hex8 capacity.  coords: nn x 3; elems: ne x nne; cn: ne x ndofe;
- * mats: per element material row (E,nu) or (k,c); thick: per element (quad4)
- * or NULL; rho: per element density (capacity) or NULL (then 1). */
-void or_assemble(int kind, int sym, long ne, const double *coords, const long *elems,
+ * 3 = hex8 capacity, 4 = tet4 elasticity, 5 = tri3 plane stress.  coords: nn x 3; elems: ne x nne;
+ * cn: ne x ndofe; mats: per element material row (E,nu) or (k,c); thick: per
+ * element (quad4) or NULL; rho: per element density (capacity) or NULL
+ * (then 1).  Returns 0, or -(e+1) for the first element e of negative volume
+ * (tet4; the reference aborts there). */
+long or_assemble(int kind, int sym, long ne, const double *coords, const long *elems,
                  const long *cn, const double *emat, const double *thick, const double *rho,
                  long *adr, long *ci, double *a) {
-  long nne = (kind == 1) ? 4 : 8;
-  long ndofe = (kind == 0) ? 24 : (kind == 1 ? 8 : 8);
+  long nne = (kind == 5) ? 3 : ((kind == 1 || kind == 4) ? 4 : 8);
+  long ndofe = (kind == 0) ? 24 : (kind == 4 ? 12 : (kind == 5 ? 6 : 8));
   double xyz[24], xy[8], t[4], r[8], ke[576];
   for (long e = 0; e < ne; e++) {
     const long *nd = elems + e * nne;
-    if (kind == 1) {
+    if (kind == 5) {
+      for (int i = 0; i < 3; i++) { xy[2 * i] = coords[3 * nd[i]]; xy[2 * i + 1] = coords[3 * nd[i] + 1]; t[i] = thick[e]; }
+      or_tri3_ke(xy, emat[2 * e], emat[2 * e + 1], t, ke);
+    } else if (kind == 4) {
+      for (int i = 0; i < 4; i++)
+        for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
+      if (or_tet4_ke(xyz, emat[2 * e], emat[2 * e + 1], ke) != 0) return -(e + 1);
+    } else if (kind == 1) {
       for (int i = 0; i < 4; i++) { xy[2 * i] = coords[3 * nd[i]]; xy[2 * i + 1] = coords[3 * nd[i] + 1]; t[i] = thick[e]; }
       or_quad4_ke(xy, emat[2 * e], emat[2 * e + 1], t, ke);
     } else {
@@ -467,6 +557,7 @@ void or_assemble(int kind, int sym, long ne, const double *coords, const long *e
     if (sym) or_scr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
     else or_cr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
   }
+  return 0;
 }
 
 /* ------------------------------------------------------------------------ */

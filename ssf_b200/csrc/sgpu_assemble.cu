@@ -255,6 +255,99 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
   }
 }
 
+// tet4 elasticity (lintet::stiffness_matrix, MEFEL/SRC/lintet.cpp:290-315):
+// the linear tetrahedron's gradients are constant, so one integration point
+// with weight det3d/6 (GEFEL/matrix.cpp:3629) gives block (a,b) =
+// det/6 B_a^T D B_b, B rows [xx, yy, zz, yz, xz, xy] as for the hexahedron
+// (lintet::geom_matrix, :213-240).  The gradients follow derivatives_3d
+// (GEFEL/difcalc.cpp:487-565) with the natural derivatives
+// (1,0,0,-1), (0,1,0,-1), (0,0,1,-1) of dx/dy/dz_bf_lin_tet.  A negative
+// det3d sets err bit 8 (the reference aborts on wrong node numbering).
+// Half a warp per element, lane (a,b) of the 4 x 4 node blocks; lanes 0..11
+// of a half load the 12 coordinates.
+__global__ void __launch_bounds__(TPB) k_tet4_elastic(int ne_c, const int *__restrict__ elist,
+                                                      const double *__restrict__ coords,
+                                                      const int64_t *__restrict__ elems,
+                                                      const int *__restrict__ cne, const double *__restrict__ emat,
+                                                      const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                      double *__restrict__ val, unsigned *err) {
+  const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+  const int warp = (int)((blockIdx.x * (unsigned)TPB + threadIdx.x) >> 5);
+  const int nwarps = gridDim.x * WPB;
+  // every lane runs the same trips (the shuffles need the whole warp)
+  for (int t0 = 2 * warp; t0 < ne_c; t0 += 2 * nwarps) {
+    const int t = t0 + half;
+    const bool live = t < ne_c;
+    const int e = live ? elist[t] : 0;
+    double cv = 0.0;
+    if (live && hl < 12) cv = coords[3 * elems[(int64_t)e * 4 + hl / 3] + hl % 3];
+    double x[4], y[4], z[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cv, 16 * half + 3 * a);
+      y[a] = __shfl_sync(0xffffffffu, cv, 16 * half + 3 * a + 1);
+      z[a] = __shfl_sync(0xffffffffu, cv, 16 * half + 3 * a + 2);
+    }
+    if (!live) continue;
+    // det3d: (p0-p3) . ((p1-p3) x (p2-p3)); the Jacobian columns are the
+    // same differences (d1..d9 of derivatives_3d)
+    const double d1 = x[0] - x[3], d2 = x[1] - x[3], d3 = x[2] - x[3];
+    const double d4 = y[0] - y[3], d5 = y[1] - y[3], d6 = y[2] - y[3];
+    const double d7 = z[0] - z[3], d8 = z[1] - z[3], d9 = z[2] - z[3];
+    const double det = d1 * d5 * d9 + d2 * d6 * d7 + d3 * d4 * d8 - d3 * d5 * d7 - d6 * d8 * d1 - d9 * d2 * d4;
+    if (det < 0.0) {
+      if (hl == 0) atomicOr(err, 8u);
+      continue;
+    }
+    const double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+    // rows of the inverse Jacobian: gradient of node a = natural (nx,ny,nz) . rows
+    const double r00 = (d5 * d9 - d8 * d6) / jac, r01 = (d7 * d6 - d9 * d4) / jac, r02 = (d4 * d8 - d7 * d5) / jac;
+    const double r10 = (d8 * d3 - d9 * d2) / jac, r11 = (d1 * d9 - d7 * d3) / jac, r12 = (d7 * d2 - d8 * d1) / jac;
+    const double r20 = (d2 * d6 - d5 * d3) / jac, r21 = (d4 * d3 - d6 * d1) / jac, r22 = (d1 * d5 - d4 * d2) / jac;
+    const int a = hl >> 2, b = hl & 3;
+    // node 3 has natural derivatives (-1,-1,-1); nodes 0..2 pick one column
+    double ax, ay, az, bx, by, bz;
+    if (a < 3) {
+      ax = a == 0 ? r00 : (a == 1 ? r01 : r02);
+      ay = a == 0 ? r10 : (a == 1 ? r11 : r12);
+      az = a == 0 ? r20 : (a == 1 ? r21 : r22);
+    } else {
+      ax = -(r00 + r01 + r02); ay = -(r10 + r11 + r12); az = -(r20 + r21 + r22);
+    }
+    if (b < 3) {
+      bx = b == 0 ? r00 : (b == 1 ? r01 : r02);
+      by = b == 0 ? r10 : (b == 1 ? r11 : r12);
+      bz = b == 0 ? r20 : (b == 1 ? r21 : r22);
+    } else {
+      bx = -(r00 + r01 + r02); by = -(r10 + r11 + r12); bz = -(r20 + r21 + r22);
+    }
+    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+    const double G = E / 2.0 / (1.0 + nu);
+    const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
+    const double c0 = s * (1 - nu), c1 = s * nu;
+    const double w = det / 6.0;
+    const double db[6][3] = {{c0 * bx, c1 * by, c1 * bz}, {c1 * bx, c0 * by, c1 * bz}, {c1 * bx, c1 * by, c0 * bz},
+                             {0.0, G * bz, G * by},        {G * bz, 0.0, G * bx},        {G * by, G * bx, 0.0}};
+    double k[3][3];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      k[0][j] = w * (ax * db[0][j] + az * db[4][j] + ay * db[5][j]);
+      k[1][j] = w * (ay * db[1][j] + az * db[3][j] + ax * db[5][j]);
+      k[2][j] = w * (az * db[2][j] + ay * db[3][j] + ax * db[4][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int r = __ldg(cne + (int64_t)e * 12 + 3 * a + i);
+      if (r < 0) continue;
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const int c = __ldg(cne + (int64_t)e * 12 + 3 * b + j);
+        if (c >= 0) csr_add(rowptr, col, val, r, c, k[i][j], err);
+      }
+    }
+  }
+}
+
 // quad4 plane stress (planeelemlq::gl_stiffness_matrix, MEFEL/SRC/plelemlq.cpp:611-690):
 // B rows [xx, yy, xy] (geom_matrix, :294-320), D plane stress
 // (elastisomat::matstiff_plstress, MEFEL/SRC/elastisomat.cpp:255), thickness
@@ -339,6 +432,64 @@ __global__ void __launch_bounds__(TPB) k_quad4_elastic(int ne_c, const int *__re
       }
     }
     __syncwarp();
+  }
+}
+
+// tri3 plane stress, the constant-strain triangle (planeelemlt::stiffness_matrix,
+// MEFEL/SRC/plelemlt.cpp:234-272): det = twice the signed area, B from the
+// area-coordinate coefficients b_i = (y_j - y_k)/det, c_i = (x_k - x_j)/det
+// (plsb/plsc, GEFEL/basefun.cpp:394-416; geom_matrix, plelemlt.cpp:166-192),
+// weight thick*det/2 with the thickness interpolated at (1/3, 1/3) through
+// area coordinates (approx_nat, :119-131).  No sign check, as in the
+// reference.  One thread per element: 3 x 3 node blocks of 2 x 2.
+__global__ void __launch_bounds__(TPB) k_tri3_elastic(int ne_c, const int *__restrict__ elist,
+                                                      const double *__restrict__ coords,
+                                                      const int64_t *__restrict__ elems,
+                                                      const int *__restrict__ cne, const double *__restrict__ emat,
+                                                      const double *__restrict__ thick,
+                                                      const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                      double *__restrict__ val, unsigned *err) {
+  for (int t = blockIdx.x * TPB + threadIdx.x; t < ne_c; t += gridDim.x * TPB) {
+    const int e = elist[t];
+    double x[3], y[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int64_t nd = elems[(int64_t)e * 3 + a];
+      x[a] = coords[3 * nd];
+      y[a] = coords[3 * nd + 1];
+    }
+    const double det = (x[1] - x[0]) * (y[2] - y[0]) - (x[2] - x[0]) * (y[1] - y[0]);
+    const double b[3] = {(y[1] - y[2]) / det, (y[2] - y[0]) / det, (y[0] - y[1]) / det};
+    const double c[3] = {(x[2] - x[1]) / det, (x[0] - x[2]) / det, (x[1] - x[0]) / det};
+    const double t_e = thick[e];
+    const double third = 1.0 / 3.0;
+    const double th = third * t_e + third * t_e + (1.0 - third - third) * t_e;
+    const double w = th * det / 2.0;
+    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+    const double cc = E / (1.0 - nu * nu), d01 = cc * nu, g3 = E / 2.0 / (1.0 + nu);
+    int code[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) code[q] = __ldg(cne + (int64_t)e * 6 + q);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        // B_a^T D B_b with B_n = [[b_n, 0], [0, c_n], [c_n, b_n]]
+        const double k00 = w * (b[a] * cc * b[bb] + c[a] * g3 * c[bb]);
+        const double k01 = w * (b[a] * d01 * c[bb] + c[a] * g3 * b[bb]);
+        const double k10 = w * (c[a] * d01 * b[bb] + b[a] * g3 * c[bb]);
+        const double k11 = w * (c[a] * cc * c[bb] + b[a] * g3 * b[bb]);
+        const int r0 = code[2 * a], r1 = code[2 * a + 1], c0 = code[2 * bb], c1 = code[2 * bb + 1];
+        if (r0 >= 0) {
+          if (c0 >= 0) csr_add(rowptr, col, val, r0, c0, k00, err);
+          if (c1 >= 0) csr_add(rowptr, col, val, r0, c1, k01, err);
+        }
+        if (r1 >= 0) {
+          if (c0 >= 0) csr_add(rowptr, col, val, r1, c0, k10, err);
+          if (c1 >= 0) csr_add(rowptr, col, val, r1, c1, k11, err);
+        }
+      }
+    }
   }
 }
 
@@ -518,6 +669,18 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
         k_quad4_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,
                                              c.rowptr.p, c.col.p, c.val.p, err.p);
         break;
+      case 4: {
+        const int g4 = std::min((cnt + 2 * WPB - 1) / (2 * WPB), kNumSMs * 16);
+        k_tet4_elastic<<<g4, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, c.rowptr.p,
+                                          c.col.p, c.val.p, err.p);
+        break;
+      }
+      case 5: {
+        const int g5 = std::min((cnt + TPB - 1) / TPB, kNumSMs * 16);
+        k_tri3_elastic<<<g5, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,
+                                          c.rowptr.p, c.col.p, c.val.p, err.p);
+        break;
+      }
       case 2:
         k_hex8_scalar<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, nullptr,
                                                   c.rowptr.p, c.col.p, c.val.p, err.p);
@@ -534,6 +697,7 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
   SGPU_CUDA(cudaEventRecord(m->ev1, s));
   unsigned e = 0;
   SGPU_TRY(read_err(err.p, s, &e));
+  if (e & 8u) return fail(SGPU_BAD_INPUT, "tetrahedron of negative volume (wrong node numbering)");
   if (e) return fail(SGPU_BAD_INPUT, "element scatter found no CSR entry (bits " + std::to_string(e) + ")");
   float ms = 0.f;
   SGPU_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
@@ -560,6 +724,8 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   switch (kind) {
     case SGPU_ELEM_HEX8: nne = 8; ndofn = 3; break;
     case SGPU_ELEM_QUAD4: nne = 4; ndofn = 2; break;
+    case SGPU_ELEM_TET4: nne = 4; ndofn = 3; break;
+    case SGPU_ELEM_TRI3: nne = 3; ndofn = 2; break;
     case SGPU_ELEM_HEX8T_K:
     case SGPU_ELEM_HEX8T_C: nne = 8; ndofn = 1; break;
     default: return fail(SGPU_BAD_INPUT, "unknown element kind");
@@ -567,7 +733,8 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   if (mesh->ndofn != ndofn) return fail(SGPU_BAD_INPUT, "ndofn does not match the element kind");
   if (mesh->nn <= 0 || mesh->ne <= 0 || !mesh->coords || !mesh->elems || !mesh->cn || !mesh->emat)
     return fail(SGPU_BAD_INPUT, "empty mesh");
-  if (kind == SGPU_ELEM_QUAD4 && !mesh->thick) return fail(SGPU_BAD_INPUT, "quad4 needs thicknesses");
+  if ((kind == SGPU_ELEM_QUAD4 || kind == SGPU_ELEM_TRI3) && !mesh->thick)
+    return fail(SGPU_BAD_INPUT, "plane elements need thicknesses");
   if (mesh->ne > (1LL << 31) - 1) return fail(SGPU_BAD_INPUT, "too many elements");
   const int64_t nn = mesh->nn, ne = mesh->ne;
   const int ndofe = nne * ndofn;

@@ -10,7 +10,11 @@ The benchmark problems of this project are generated, never downloaded:
 * ``plate_quad``       -- 2D plane-stress plate of 4-node quads, left edge
   clamped, unit traction x thickness on the right edge;
 * ``heat_cube``        -- unit cube of linear hexahedra for transient
-  conduction with one conductivity per element.
+  conduction with one conductivity per element;
+* ``cantilever_tet``   -- the cantilever of ``cantilever_hex`` meshed with
+  linear tetrahedra (six per grid cell);
+* ``plate_tri``        -- the plate of ``plate_quad`` meshed with
+  constant-strain triangles (two per quad).
 
 ``write_mefel_deck`` writes a deck in SIFEL's positional (``-kwd`` absent)
 MEFEL input format, token order as read by ``probdesc::read``
@@ -188,6 +192,19 @@ def plate_quad(nx, ny, Lx=None, Ly=None, E=1.0e10, nu=0.25, t=0.01, traction=1.0
     )
 
 
+def plate_tri(nx, ny, Lx=None, Ly=None, E=1.0e10, nu=0.25, t=0.01, traction=1.0) -> Mesh:
+    """The plate of ``plate_quad`` meshed with constant-strain triangles
+    (planeelemlt, 3 nodes): every quad cut along its n0-n2 diagonal into
+    (n0, n1, n2) and (n0, n2, n3), both counter-clockwise (positive area, the
+    orientation the element's formulas assume); same supports and loads."""
+    q = plate_quad(nx, ny, Lx, Ly, E, nu, t, traction)
+    e = q.elems
+    tris = np.stack([e[:, [0, 1, 2]], e[:, [0, 2, 3]]], axis=1).reshape(-1, 3)
+    return Mesh(kind="tri3", coords=q.coords, elems=tris.astype(np.int64), dofflag=q.dofflag,
+                emat=np.zeros(tris.shape[0], dtype=np.int64), mats=q.mats, loads=q.loads,
+                thick=np.full(tris.shape[0], t), meta=q.meta)
+
+
 def plate_batch(count=512, seed=0, lo=16, hi=128):
     """The uneven batch: ``count`` plates with side counts uniform in
     [lo, hi], E uniform in [1e9, 1e11], nu uniform in [0.2, 0.35]."""
@@ -228,6 +245,61 @@ def heat_cube(n=8, L=1.0, sigma=1.0, mu=0.0, seed=1234, rhoc=2.0e6, T_left=1.0) 
 # deck writers
 # ----------------------------------------------------------------------------
 
+def det3d(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    """Six times the signed volume of every tetrahedron, with the reference's
+    formula and sign (det3d, GEFEL/matrix.cpp:3629): (p0-p3).((p1-p3)x(p2-p3))."""
+    p = coords[tets]
+    a, b, c = p[:, 0] - p[:, 3], p[:, 1] - p[:, 3], p[:, 2] - p[:, 3]
+    return np.einsum("ij,ij->i", a, np.cross(b, c))
+
+
+def cantilever_tet(nx=20, ny=4, nz=4, L=1.0, B=0.2, H=0.2, E=210e9, nu=0.3,
+                   traction=1.0e6) -> Mesh:
+    """Clamped cantilever of linear tetrahedra (lintet, 4 nodes).
+
+    Every cell of the nx x ny x nz grid is split into six tetrahedra along its
+    diagonal from the lowest to the highest corner (one per ordering of the
+    three axes, so neighbouring cells split their shared face the same way),
+    nodes ordered so that det3d > 0, the orientation the reference requires
+    (lintet::stiffness_matrix aborts on a negative volume).  The end traction
+    in -z goes to the nodes of the x = L face triangles, a third of each
+    triangle's force per corner.
+    """
+    coords, _, nid = _hex_grid(nx, ny, nz, L, B, H)
+    nn = coords.shape[0]
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    unit = np.eye(3, dtype=np.int64)
+    tets = []
+    for perm in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+        o1 = unit[perm[0]]
+        o2 = o1 + unit[perm[1]]
+        tets.append(np.stack([nid(i, j, k), nid(i + o1[0], j + o1[1], k + o1[2]),
+                              nid(i + o2[0], j + o2[1], k + o2[2]), nid(i + 1, j + 1, k + 1)], axis=1))
+    elems = np.stack(tets, axis=1).reshape(-1, 4).astype(np.int64)
+    neg = det3d(coords, elems) < 0.0
+    elems[neg, 0], elems[neg, 1] = elems[neg, 1].copy(), elems[neg, 0].copy()
+    dofflag = np.ones((nn, 3), dtype=np.int64)
+    dofflag[np.isclose(coords[:, 0], 0.0)] = 0
+    loads = np.zeros((1, nn, 3))
+    onface = np.isclose(coords[:, 0], L)
+    faces = np.concatenate([elems[:, [0, 1, 2]], elems[:, [0, 1, 3]], elems[:, [0, 2, 3]], elems[:, [1, 2, 3]]])
+    faces = faces[onface[faces].all(axis=1)]
+    p = coords[faces]
+    area = 0.5 * np.linalg.norm(np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), axis=1)
+    np.add.at(loads[0, :, 2], faces.ravel(), np.repeat(-traction * area / 3.0, 3))
+    return Mesh(
+        kind="tet4",
+        coords=coords,
+        elems=elems,
+        dofflag=dofflag,
+        emat=np.zeros(elems.shape[0], dtype=np.int64),
+        mats=np.array([[E, nu]]),
+        loads=loads,
+        meta=dict(nx=nx, ny=ny, nz=nz, L=L, B=B, H=H),
+    )
+
+
 def _fmt(v: float) -> str:
     return repr(float(v))
 
@@ -250,7 +322,7 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
     lines.append(f"20 {ni} {_fmt(res)} {iv}")
     lines.append(f"{precond}")
     lines.append(f"{mesh.nn}")
-    is2d = mesh.kind == "quad4"
+    is2d = mesh.kind in ("quad4", "tri3")
     for i, (x, y, z) in enumerate(mesh.coords):
         lines.append(f"{i + 1} {_fmt(x)} {_fmt(y)} {_fmt(z)} {nd} 0 0")
     con = np.where((mesh.dofflag != 1).any(axis=1))[0]
@@ -262,12 +334,16 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
         ns = " ".join(str(int(v) + 1) for v in nodes)
         m = int(mesh.emat[e]) + 1
         if is2d:
-            # type planeelementlq (23), strastrestate planestress (10),
-            # cne 0, crst csplanestr (10) instance e+1... one thickness set
-            lines.append(f"{e + 1} 23 10 {ns} 0 10 {int(mesh.meta.get('tset', [0] * mesh.ne)[e]) + 1 if 'tset' in mesh.meta else 1} 1 1 {m}")
+            # type planeelementlq (23) or planeelementlt (20), strastrestate
+            # planestress (10), cne 0, crst csplanestr (10) with the
+            # element's thickness set, one material
+            et = 20 if mesh.kind == "tri3" else 23
+            lines.append(f"{e + 1} {et} 10 {ns} 0 10 {int(mesh.meta.get('tset', [0] * mesh.ne)[e]) + 1 if 'tset' in mesh.meta else 1} 1 1 {m}")
         else:
-            # type linearhex (102), cne 0, crst 0, one material elisomat (1)
-            lines.append(f"{e + 1} 102 {ns} 0 0 1 1 {m}")
+            # type lineartet (100) or linearhex (102), cne 0, crst 0, one
+            # material elisomat (1)
+            et = 100 if mesh.kind == "tet4" else 102
+            lines.append(f"{e + 1} {et} {ns} 0 0 1 1 {m}")
     # materials: one type (elisomat = 1), mats.shape[0] instances "id e nu"
     lines.append("1")
     lines.append(f"1 {mesh.mats.shape[0]}")

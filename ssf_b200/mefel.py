@@ -21,7 +21,8 @@ import numpy as np
 from . import _lib as L
 from .gefel import DeviceMatrix, Result
 
-KIND = {"hex8": L.ELEM_HEX8, "quad4": L.ELEM_QUAD4, "hex8t_k": L.ELEM_HEX8T_K, "hex8t_c": L.ELEM_HEX8T_C}
+KIND = {"hex8": L.ELEM_HEX8, "quad4": L.ELEM_QUAD4, "hex8t_k": L.ELEM_HEX8T_K, "hex8t_c": L.ELEM_HEX8T_C,
+        "tet4": L.ELEM_TET4, "tri3": L.ELEM_TRI3}
 
 
 def _c(a, dt):
@@ -49,7 +50,7 @@ def _assemble(mesh, kind: str, rho=None):
 
 
 def stiffness_matrix(mesh) -> DeviceMatrix:
-    """Global stiffness matrix of a hex8 / quad4 mesh, assembled on the GPU."""
+    """Global stiffness matrix of a hex8 / tet4 / quad4 / tri3 mesh, assembled on the GPU."""
     return _assemble(mesh, mesh.kind)
 
 

@@ -14,13 +14,19 @@ oracle/ref_harness_mefel.cpp / ref_harness_trfel.cpp:
                       (the reference's comprow::cg_prec path): K, f, u
   trfel_cube.npz      4^3 heat cube, lognormal k, T = 1 on x = 0, implicit
                       Euler: K, C and T after 1 and 3 steps
+  tet4_cantilever.npz 5x2x2 distorted cantilever of linear tetrahedra (lintet,
+                      element type 100), 2 materials, SCR + Jacobi-PCG:
+                      coordinates, elements, K, f, u, ani, ares
+  tri3_plate.npz      6x4 distorted plane-stress plate of constant-strain
+                      triangles (planeelemlt, type 20), 2 materials: K, f, u
   reference_iterations.json
                       iteration counts and solve times of full reference runs
                       on the benchmark cantilevers (used by bench.py to scale
                       its bounded CPU sample to a full solve)
 
-Usage: python tests/golden/make_golden.py [--big]   (--big adds the 1.01M-DOF
-run, about 2-3 minutes of CPU)
+Usage: python tests/golden/make_golden.py [--big] [--elements]   (--big adds
+the 1.01M-DOF run, about 2-3 minutes of CPU; --elements writes only the
+tet4 and tri3 fixtures)
 """
 from __future__ import annotations
 
@@ -46,9 +52,39 @@ def run(mesh, tag, **deck_kw):
         return O.run_mefel_dump(deck, td)
 
 
-def main(big=False):
+def tet4_fixture():
+    t = decks.cantilever_tet(5, 2, 2)
+    rng = np.random.default_rng(13)
+    inner = ~np.isclose(t.coords[:, 0], 0.0)
+    t.coords[inner] += rng.uniform(-0.01, 0.01, (int(inner.sum()), 3))
+    t.emat = (np.arange(t.ne) % 2).astype(np.int64)
+    t.mats = np.array([[210e9, 0.3], [70e9, 0.33]])
+    d = run(t, "tet4")
+    np.savez_compressed(os.path.join(HERE, "tet4_cantilever.npz"), coords=t.coords, elems=t.elems, emat=t.emat,
+                        mats=t.mats, dofflag=t.dofflag, loads=t.loads, adr=d["K_adr"], ci=d["K_ci"], a=d["K_a"],
+                        f=d["f"], u=d["u"], ani=d["meta"]["ani_0"], ares=d["meta"]["ares_0"])
+
+
+def tri3_fixture():
+    q = decks.plate_tri(6, 4, E=3.0e10, nu=0.22, t=0.02)
+    rng = np.random.default_rng(14)
+    q.coords[:, :2] += rng.uniform(-0.15, 0.15, (q.nn, 2))
+    q.emat = (np.arange(q.ne) % 2).astype(np.int64)
+    q.mats = np.array([[3.0e10, 0.22], [7.0e10, 0.31]])
+    d = run(q, "tri3")
+    np.savez_compressed(os.path.join(HERE, "tri3_plate.npz"), coords=q.coords, elems=q.elems, emat=q.emat,
+                        mats=q.mats, thick=q.thick, dofflag=q.dofflag, loads=q.loads, adr=d["K_adr"],
+                        ci=d["K_ci"], a=d["K_a"], f=d["f"], u=d["u"], ani=d["meta"]["ani_0"],
+                        ares=d["meta"]["ares_0"])
+
+
+def main(big=False, elements_only=False):
     if not O.ref_available():
         raise SystemExit("build the reference first: python oracle/build_ref.py")
+    tet4_fixture()
+    tri3_fixture()
+    if elements_only:
+        return
     out = {}
 
     m = decks.cantilever_hex(20, 4, 4)
@@ -130,4 +166,4 @@ def main(big=False):
 
 
 if __name__ == "__main__":
-    main(big="--big" in sys.argv)
+    main(big="--big" in sys.argv, elements_only="--elements" in sys.argv)

@@ -1,0 +1,214 @@
+"""Linear tetrahedra (lintet, MEFEL element type 100) and constant-strain
+triangles (planeelemlt, type 20): the oracle pinned to the compiled
+reference's fixtures, the elements' own invariants, the generated meshes, and
+the GPU assembly and solves against the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from ssf_b200 import decks
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _golden_mesh(g, kind="tet4"):
+    return decks.Mesh(kind=kind, coords=g["coords"], elems=g["elems"], dofflag=g["dofflag"], emat=g["emat"],
+                      mats=g["mats"], loads=g["loads"], thick=g["thick"] if "thick" in g else None)
+
+
+def test_tet4_cantilever_golden(oracle):
+    g = np.load(os.path.join(GOLDEN, "tet4_cantilever.npz"))
+    m = _golden_mesh(g)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    assert np.array_equal(adr, g["adr"]) and np.array_equal(ci, g["ci"])
+    assert np.array_equal(a, g["a"])
+    f = oracle.load_vector(m)
+    assert np.array_equal(f, g["f"])
+    x, st, ani, ares = oracle.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == int(g["ani"]) and ares == float(g["ares"])
+    assert np.array_equal(x, g["u"])
+
+
+def test_tet4_element_invariants(oracle):
+    rng = np.random.default_rng(21)
+    xyz = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    xyz = xyz + rng.uniform(-0.1, 0.1, xyz.shape)
+    if decks.det3d(xyz, np.arange(4)[None])[0] < 0:
+        xyz[[0, 1]] = xyz[[1, 0]]
+    ke = oracle.tet4_ke(xyz, 70e9, 0.33)
+    assert np.allclose(ke, ke.T, rtol=0, atol=1e-12 * np.abs(ke).max())
+    # the six rigid-body motions produce no forces
+    for i in range(3):
+        v = np.zeros((4, 3)); v[:, i] = 1.0
+        assert np.abs(ke @ v.ravel()).max() < 1e-9 * np.abs(ke).max()
+    for i, j in ((0, 1), (1, 2), (0, 2)):
+        v = np.zeros((4, 3)); v[:, i] = -xyz[:, j]; v[:, j] = xyz[:, i]
+        assert np.abs(ke @ v.ravel()).max() < 1e-9 * np.abs(ke).max()
+    # 6 independent deformation modes: rank 12 - 6
+    assert np.linalg.matrix_rank(ke, tol=1e-9 * np.abs(ke).max()) == 6
+    # K scales with the length (B ~ 1/h, volume ~ h^3)
+    assert np.allclose(oracle.tet4_ke(2.0 * xyz, 70e9, 0.33), 2.0 * ke, rtol=1e-12, atol=0)
+    # wrong node numbering (negative det3d) is an error, as in the reference
+    with pytest.raises(ValueError):
+        oracle.tet4_ke(xyz[[1, 0, 2, 3]], 70e9, 0.33)
+
+
+def test_tet_mesh_is_conforming():
+    m = decks.cantilever_tet(4, 3, 2, L=1.0, B=0.3, H=0.2)
+    det = decks.det3d(m.coords, m.elems)
+    assert (det > 0).all() and np.isclose(det.sum() / 6.0, 1.0 * 0.3 * 0.2)
+    faces = np.sort(np.concatenate([m.elems[:, [0, 1, 2]], m.elems[:, [0, 1, 3]], m.elems[:, [0, 2, 3]],
+                                    m.elems[:, [1, 2, 3]]]), axis=1)
+    _, counts = np.unique(faces, axis=0, return_counts=True)
+    # every face is shared by two tetrahedra or lies on the boundary: 2 x 2
+    # triangles per boundary cell face
+    nb = 2 * 2 * (4 * 3 + 4 * 2 + 3 * 2)
+    assert counts.max() == 2 and (counts == 1).sum() == nb
+    # consistent nodal forces add up to traction x end area
+    assert np.isclose(m.loads.sum(), -1.0e6 * 0.3 * 0.2)
+
+
+def test_negative_volume_rejected_by_oracle(oracle):
+    m = decks.cantilever_tet(2, 1, 1)
+    m.elems[3, [0, 1]] = m.elems[3, [1, 0]]
+    with pytest.raises(ValueError, match="element 4"):
+        oracle.assemble(m, sym=True)
+
+
+@pytest.mark.gpu
+def test_tet4_assembly_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    m = decks.cantilever_tet(6, 3, 3)
+    rng = np.random.default_rng(6)
+    m.coords = m.coords + rng.uniform(-0.005, 0.005, m.coords.shape)
+    m.emat = np.arange(m.ne) % 3
+    m.mats = np.array([[210e9, 0.3], [70e9, 0.25], [30e9, 0.2]])
+    adr, ci, a = oracle.assemble(m, sym=True)
+    with mefel.stiffness_matrix(m) as K:
+        assert K.assembly["colours"] <= 64
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+    assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+@pytest.mark.gpu
+def test_tet4_golden_on_device(gpu_lib):
+    from ssf_b200 import mefel
+    g = np.load(os.path.join(GOLDEN, "tet4_cantilever.npz"))
+    m = _golden_mesh(g)
+    with mefel.stiffness_matrix(m) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, g["adr"]) and np.array_equal(g_ci, g["ci"])
+    assert np.allclose(g_a, g["a"], rtol=1e-12, atol=1e-12 * np.abs(g["a"]).max())
+
+
+@pytest.mark.gpu
+def test_tet4_negative_volume_rejected_on_device(gpu_lib):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.cantilever_tet(2, 1, 1)
+    m.elems[3, [0, 1]] = m.elems[3, [1, 0]]
+    with pytest.raises(L.SgpuError, match="negative volume"):
+        mefel.stiffness_matrix(m)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,mode", [("jacobi", "fp64"), ("agg", "mixed"), ("agg", "fp64")])
+def test_tet_cantilever_solve_matches_oracle(oracle, gpu_lib, prec, mode):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.cantilever_tet(30, 6, 6)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    f = oracle.load_vector(m)
+    xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with mefel.stiffness_matrix(m) as K:
+        if prec == "agg":
+            K.set_nullspace(mefel.rigid_body_modes(m))
+        x, r = K.pcg(f, res=1e-22, prec=prec, mode=mode)
+    assert r.status == L.OK
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+    if prec == "agg":
+        assert r.info["iterations"] * 3 < ani_o
+
+
+# ---------------------------------------------------------------------------
+# tri3
+# ---------------------------------------------------------------------------
+
+def test_tri3_plate_golden(oracle):
+    g = np.load(os.path.join(GOLDEN, "tri3_plate.npz"))
+    m = _golden_mesh(g, "tri3")
+    adr, ci, a = oracle.assemble(m, sym=True)
+    assert np.array_equal(adr, g["adr"]) and np.array_equal(ci, g["ci"])
+    assert np.array_equal(a, g["a"])
+    f = oracle.load_vector(m)
+    assert np.array_equal(f, g["f"])
+    x, st, ani, ares = oracle.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == int(g["ani"]) and ares == float(g["ares"])
+    assert np.array_equal(x, g["u"])
+
+
+def test_tri3_element_invariants(oracle):
+    xy = np.array([[0.1, 0.0], [1.2, 0.2], [0.3, 0.9]])
+    ke = oracle.tri3_ke(xy, 3e10, 0.22, 0.02)
+    assert np.allclose(ke, ke.T, rtol=0, atol=1e-12 * np.abs(ke).max())
+    for v in (np.tile([1.0, 0.0], 3), np.tile([0.0, 1.0], 3), np.stack([-xy[:, 1], xy[:, 0]], 1).ravel()):
+        assert np.abs(ke @ v).max() < 1e-9 * np.abs(ke).max()
+    assert np.linalg.matrix_rank(ke, tol=1e-9 * np.abs(ke).max()) == 3
+    # K does not change with the size of a plane element (B ~ 1/h, area ~ h^2)
+    assert np.allclose(oracle.tri3_ke(3.0 * xy, 3e10, 0.22, 0.02), ke, rtol=1e-12, atol=0)
+    # a clockwise triangle gives the negative matrix (no orientation check)
+    assert np.allclose(oracle.tri3_ke(xy[[1, 0, 2]], 3e10, 0.22, 0.02)[np.ix_([2, 3, 0, 1, 4, 5], [2, 3, 0, 1, 4, 5])],
+                       -ke, rtol=1e-12, atol=1e-12 * np.abs(ke).max())
+
+
+def test_tri_plate_mesh():
+    m = decks.plate_tri(5, 3, Lx=2.0, Ly=1.0)
+    p = m.coords[m.elems]
+    area2 = (p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1]) - (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 1, 1] - p[:, 0, 1])
+    assert (area2 > 0).all() and np.isclose(area2.sum() / 2.0, 2.0)
+    assert m.ne == 2 * 5 * 3 and np.isclose(m.loads.sum(), 1.0 * 0.01 * 1.0)
+
+
+@pytest.mark.gpu
+def test_tri3_assembly_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import mefel
+    m = decks.plate_tri(9, 6, E=3e10, nu=0.22)
+    rng = np.random.default_rng(8)
+    m.coords[:, :2] += rng.uniform(-0.1, 0.1, (m.nn, 2))
+    m.emat = np.arange(m.ne) % 2
+    m.mats = np.array([[3e10, 0.22], [7e10, 0.31]])
+    m.thick = rng.uniform(0.01, 0.03, m.ne)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    with mefel.stiffness_matrix(m) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+    assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+@pytest.mark.gpu
+def test_tri3_golden_on_device(gpu_lib):
+    from ssf_b200 import mefel
+    g = np.load(os.path.join(GOLDEN, "tri3_plate.npz"))
+    with mefel.stiffness_matrix(_golden_mesh(g, "tri3")) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, g["adr"]) and np.array_equal(g_ci, g["ci"])
+    assert np.allclose(g_a, g["a"], rtol=1e-12, atol=1e-12 * np.abs(g["a"]).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,mode", [("jacobi", "fp64"), ("agg", "mixed")])
+def test_tri_plate_solve_matches_oracle(oracle, gpu_lib, prec, mode):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.plate_tri(60, 30, E=3e10, nu=0.22)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    f = oracle.load_vector(m)
+    xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26, zero=1e-300)
+    with mefel.stiffness_matrix(m) as K:
+        if prec == "agg":
+            K.set_nullspace(mefel.rigid_body_modes(m))
+        x, r = K.pcg(f, res=1e-22, zero=1e-300, prec=prec, mode=mode)
+    assert r.status == L.OK
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8

@@ -35,6 +35,48 @@ def test_random_distorted_cantilever_bit_exact(ref):
     assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
 
 
+def test_random_distorted_tet_cantilever_bit_exact(ref):
+    # lintet (element type 100): one integration point, weight det3d/6
+    m = decks.cantilever_tet(6, 3, 2)
+    rng = np.random.default_rng(43)
+    inner = ~np.isclose(m.coords[:, 0], 0.0)
+    m.coords[inner] += rng.uniform(-0.005, 0.005, (inner.sum(), 3))
+    assert (decks.det3d(m.coords, m.elems) > 0).all()
+    m.emat = rng.integers(0, 3, m.ne)
+    m.mats = np.array([[210e9, 0.3], [70e9, 0.33], [30e9, 0.2]])
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    assert np.array_equal(a, d["K_a"])
+    f = ref.load_vector(m)
+    assert np.array_equal(f, d["f"][: f.size])
+    x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
+
+
+def test_random_distorted_tri_plate_bit_exact(ref):
+    # planeelemlt (element type 20): one point at (1/3, 1/3), weight t det/2
+    m = decks.plate_tri(7, 4, E=3e10, nu=0.22, t=0.02)
+    rng = np.random.default_rng(44)
+    m.coords[:, :2] += rng.uniform(-0.1, 0.1, (m.nn, 2))
+    m.emat = rng.integers(0, 2, m.ne)
+    m.mats = np.array([[3e10, 0.22], [7e10, 0.31]])
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    assert np.array_equal(a, d["K_a"])
+    f = ref.load_vector(m)
+    assert np.array_equal(f, d["f"][: f.size])
+    x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
+
+
 def test_reference_solver_library_matches_oracle(ref):
     """libsifelref.so runs the reference's own symcomprow::cg_prec."""
     m = decks.cantilever_hex(10, 2, 2)
