@@ -266,6 +266,11 @@ typedef struct {
   const double *emat;    /* ne x 2: (E, nu) for elasticity, (k, c) for hex8t */
   const double *thick;   /* ne thicknesses (quad4, tri3), else NULL */
   const double *rho;     /* ne densities (capacity), NULL = 1 */
+  const double *dmat;    /* NULL, or ne x 36: a general material stiffness per
+                            element (6 x 6 row-major, global axes, strain order
+                            xx yy zz yz xz xy) for hex8 / tet4, replacing emat:
+                            elastgmat3d::matstiff (MEFEL/SRC/elastgmat3d.cpp:69)
+                            or elastortomat::matstiff (elastortomat.cpp:100) */
 } sgpu_mesh;
 
 typedef struct {
@@ -285,7 +290,8 @@ typedef struct {
 SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembly_info *info);
 /* Re-integrate the values of a handle made by sgpu_assemble, on the same
  * pattern: new per-element parameters (emat, rho; NULL keeps the old ones) or,
- * for hex8t handles, the other matrix (kind K <-> C). */
+ * for hex8t handles, the other matrix (kind K <-> C).  For a handle built
+ * with dmat, emat is the new ne x 36 array. */
 SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,
                              sgpu_assembly_info *info);
 

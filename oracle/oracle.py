@@ -55,6 +55,9 @@ def lib():
         L.or_assemble.restype = _L
         L.or_tet4_ke.argtypes = [_pD, _D, _D, _pD]
         L.or_tri3_ke.argtypes = [_pD, _D, _D, _pD, _pD]
+        L.or_assemble_d.argtypes = [C.c_int, C.c_int, _L, _pD, _pL, _pL, _pD, _pL, _pL, _pD]
+        L.or_assemble_d.restype = _L
+        L.or_ortho_dmat.argtypes = [_pD, _pD, _pD]
         L.or_tet4_ke.restype = C.c_int
         L.or_scr_mxv.argtypes = [_L, _pL, _pL, _pD, _pD, _pD]
         L.or_cr_mxv.argtypes = [_L, _pL, _pL, _pD, _pD, _pD]
@@ -138,6 +141,25 @@ def pattern(n, cne, sym):
     return adr, ci
 
 
+def material_dmat(mesh):
+    """Per-material 6 x 6 global stiffness (nmat, 36) of a "gen3d" mesh
+    (elastgmat3d::matstiff, symmetric fill of the 21 read entries) or an
+    "ortho" mesh (elastortomat::matstiff with constant transformation
+    functions, through the C restatement of lg_tens4transf)."""
+    out = np.zeros((mesh.mats.shape[0], 36))
+    for k, row in enumerate(np.asarray(mesh.mats, dtype=np.float64)):
+        if mesh.mtype == "gen3d":
+            D = np.zeros((6, 6))
+            D[np.triu_indices(6)] = row[:21]
+            D = np.triu(D) + np.triu(D, 1).T
+            out[k] = D.ravel()
+        else:
+            g = np.zeros(36)
+            lib().or_ortho_dmat(_f64(row[:36]), _f64(row[36:45]), g)
+            out[k] = g
+    return out
+
+
 def assemble(mesh, sym=True, kind=None, rho=None):
     """Global matrix of ``mesh`` in SCR (sym) or CR storage: (adr, ci, a)."""
     kind = kind or mesh.kind
@@ -146,6 +168,14 @@ def assemble(mesh, sym=True, kind=None, rho=None):
     cne = element_code_numbers(mesh)
     adr, ci = pattern(n, cne, sym)
     a = np.zeros(ci.size)
+    if getattr(mesh, "mtype", "iso") != "iso":
+        if kind not in ("hex8", "tet4"):
+            raise ValueError("general materials are defined for the 3D elements")
+        dm = _f64(material_dmat(mesh)[mesh.emat])
+        st = lib().or_assemble_d(k, int(sym), mesh.ne, _f64(mesh.coords), _i64(mesh.elems), cne, dm, adr, ci, a)
+        if st != 0:
+            raise ValueError(f"element {-st} has a negative volume (wrong node numbering)")
+        return adr, ci, a
     emat = _f64(mesh.mats[mesh.emat])
     thick = _f64(mesh.thick) if mesh.thick is not None else None
     rr = _f64(rho) if rho is not None else None

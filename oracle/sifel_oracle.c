@@ -171,8 +171,10 @@ static void matstiff_plstress(double e, double nu, double *d) {
 }
 
 /* linhex::gl_stiffness_matrix, MEFEL/SRC/linhex.cpp:583-630, with
- * linhex::geom_matrix (linhex.cpp:153-186).  xyz: 8 x (x,y,z). */
-void or_hex8_ke(const double *xyz, double e, double nu, double *ke) {
+ * linhex::geom_matrix (linhex.cpp:153-186).  xyz: 8 x (x,y,z).  dm: the
+ * material stiffness (6 x 6, row-major) of every integration point, or NULL
+ * for the isotropic (e, nu) of elastisomat. */
+static void hex8_ke(const double *xyz, double e, double nu, const double *dm, double *ke) {
   double x[8], y[8], z[8], dx[8], dy[8], dz[8], gm[6 * 24], d[36];
   for (int i = 0; i < 8; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
   memset(ke, 0, 576 * sizeof(double));
@@ -196,7 +198,8 @@ void or_hex8_ke(const double *xyz, double e, double nu, double *ke) {
           gm[4 * 24 + jj] = dz[a]; gm[4 * 24 + ll] = dx[a];
           gm[5 * 24 + jj] = dy[a]; gm[5 * 24 + kk] = dx[a];
         }
-        matstiff_spacestr(e, nu, d);
+        if (dm) memcpy(d, dm, sizeof(d));
+        else matstiff_spacestr(e, nu, d);
         jac *= GW2[i] * GW2[j] * GW2[k];
         if (jac < 0.0) jac = fabs(jac);
         bdbjac(ke, gm, d, gm, jac, 6, 24);
@@ -204,6 +207,9 @@ void or_hex8_ke(const double *xyz, double e, double nu, double *ke) {
     }
   }
 }
+
+void or_hex8_ke(const double *xyz, double e, double nu, double *ke) { hex8_ke(xyz, e, nu, NULL, ke); }
+void or_hex8_ke_d(const double *xyz, const double *dm, double *ke) { hex8_ke(xyz, 0.0, 0.0, dm, ke); }
 
 /* det3d, GEFEL/matrix.cpp:3629-3660 (the active branch): six times the signed
  * volume of the tetrahedron, (p0-p3) . ((p1-p3) x (p2-p3)). */
@@ -221,7 +227,7 @@ static double det3d(const double *x, const double *y, const double *z) {
  * (0.25, 0.25, 0.25); the weight is det3d/6, and a negative det3d (wrong node
  * numbering) is an error.  xyz: 4 x (x,y,z).  Returns 0, or -1 on a negative
  * volume (ke untouched then). */
-int or_tet4_ke(const double *xyz, double e, double nu, double *ke) {
+static int tet4_ke(const double *xyz, double e, double nu, const double *dm, double *ke) {
   static const double NX[4] = {1.0, 0.0, 0.0, -1.0}, NY[4] = {0.0, 1.0, 0.0, -1.0},
                       NZ[4] = {0.0, 0.0, 1.0, -1.0};
   double x[4], y[4], z[4], dx[4], dy[4], dz[4], gm[6 * 12], d[36];
@@ -251,10 +257,58 @@ int or_tet4_ke(const double *xyz, double e, double nu, double *ke) {
     gm[4 * 12 + jj] = dz[a]; gm[4 * 12 + ll] = dx[a];
     gm[5 * 12 + jj] = dy[a]; gm[5 * 12 + kk] = dx[a];
   }
-  matstiff_spacestr(e, nu, d);
+  if (dm) memcpy(d, dm, sizeof(d));
+  else matstiff_spacestr(e, nu, d);
   memset(ke, 0, 144 * sizeof(double));
   bdbjac(ke, gm, d, gm, det / 6.0, 6, 12);
   return 0;
+}
+
+int or_tet4_ke(const double *xyz, double e, double nu, double *ke) { return tet4_ke(xyz, e, nu, NULL, ke); }
+int or_tet4_ke_d(const double *xyz, const double *dm, double *ke) { return tet4_ke(xyz, 0.0, 0.0, dm, ke); }
+
+/* elastortomat::matstiff, MEFEL/SRC/elastortomat.cpp:100-115, for a
+ * transformation of constant general functions: lg_tens4transf
+ * (MEFEL/SRC/vecttens.cpp:1561-1622) builds the 6 x 6 strain transformation
+ * t from the 3 x 3 tmat (x_g = T x_l), then g = t^T l t by mtxm and mxm
+ * (GEFEL/matrix.cpp:1362, 1184).  l, g: 6 x 6 row-major; tm: 3 x 3. */
+void or_ortho_dmat(const double *l, const double *tm, double *g) {
+#define TM(i, j) tm[3 * (i) + (j)]
+  double t[36], aux[36];
+  for (int c = 0; c < 3; c++) {
+    /* rows 0..2: the squares of column c */
+    t[6 * c + 0] = TM(0, c) * TM(0, c);
+    t[6 * c + 1] = TM(1, c) * TM(1, c);
+    t[6 * c + 2] = TM(2, c) * TM(2, c);
+    t[6 * c + 3] = TM(1, c) * TM(2, c);
+    t[6 * c + 4] = TM(0, c) * TM(2, c);
+    t[6 * c + 5] = TM(0, c) * TM(1, c);
+  }
+  /* rows 3, 4, 5 pair the columns (2,1), (2,0), (1,0) */
+  static const int P[3][2] = {{2, 1}, {2, 0}, {1, 0}};
+  for (int r = 0; r < 3; r++) {
+    int a = P[r][0], b = P[r][1];
+    double *row = t + 6 * (3 + r);
+    row[0] = 2.0 * TM(0, a) * TM(0, b);
+    row[1] = 2.0 * TM(1, a) * TM(1, b);
+    row[2] = 2.0 * TM(2, a) * TM(2, b);
+    row[3] = TM(1, a) * TM(2, b) + TM(2, a) * TM(1, b);
+    row[4] = TM(0, a) * TM(2, b) + TM(2, a) * TM(0, b);
+    row[5] = TM(0, a) * TM(1, b) + TM(1, a) * TM(0, b);
+  }
+#undef TM
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      double s = 0.0;
+      for (int k = 0; k < 6; k++) s += t[6 * k + i] * l[6 * k + j];
+      aux[6 * i + j] = s;
+    }
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      double s = 0.0;
+      for (int k = 0; k < 6; k++) s += aux[6 * i + k] * t[6 * k + j];
+      g[6 * i + j] = s;
+    }
 }
 
 /* planeelemlq::gl_stiffness_matrix, MEFEL/SRC/plelemlq.cpp:611-690 with
@@ -553,6 +607,29 @@ long or_assemble(int kind, int sym, long ne, const double *coords, const long *e
         if (kind == 2) or_hex8t_kc(xyz, emat[2 * e], emat[2 * e + 1], r, ke, NULL);
         else or_hex8t_kc(xyz, emat[2 * e], emat[2 * e + 1], r, NULL, ke);
       }
+    }
+    if (sym) or_scr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
+    else or_cr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
+  }
+  return 0;
+}
+
+/* or_assemble for the 3D elasticity kinds (0 hex8, 4 tet4) with a general
+ * material stiffness per element: dmat ne x 36 (row-major 6 x 6, global
+ * system), as elastgmat3d::matstiff (MEFEL/SRC/elastgmat3d.cpp:69) or
+ * elastortomat::matstiff give it.  Returns as or_assemble. */
+long or_assemble_d(int kind, int sym, long ne, const double *coords, const long *elems, const long *cn,
+                   const double *dmat, long *adr, long *ci, double *a) {
+  long nne = (kind == 4) ? 4 : 8, ndofe = 3 * nne;
+  double xyz[24], ke[576];
+  for (long e = 0; e < ne; e++) {
+    const long *nd = elems + e * nne;
+    for (int i = 0; i < nne; i++)
+      for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
+    if (kind == 4) {
+      if (or_tet4_ke_d(xyz, dmat + 36 * e, ke) != 0) return -(e + 1);
+    } else {
+      or_hex8_ke_d(xyz, dmat + 36 * e, ke);
     }
     if (sym) or_scr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
     else or_cr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);

@@ -57,6 +57,7 @@ class Mesh(C.Structure):
         ("emat", C.c_void_p),
         ("thick", C.c_void_p),
         ("rho", C.c_void_p),
+        ("dmat", C.c_void_p),
     ]
 
 

@@ -142,7 +142,20 @@ struct HexShared {
   double g[8][8][3];  // [gp][node][x,y,z]
   double w[8];
   double nb[8][8];    // shape functions at the Gauss points (capacity)
+  double D[36];       // general material stiffness of the element (row-major)
 };
+
+// D B_b for a general 6 x 6 D (row-major) and the gradient (bx, by, bz) of
+// node b: B_b columns u = (bx,0,0,0,bz,by), v = (0,by,0,bz,0,bx),
+// w = (0,0,bz,by,bx,0) in the strain order [xx, yy, zz, yz, xz, xy]
+__device__ __forceinline__ void elastic_db(const double *D, double bx, double by, double bz, double db[6][3]) {
+#pragma unroll
+  for (int r = 0; r < 6; r++) {
+    db[r][0] = D[6 * r + 0] * bx + D[6 * r + 4] * bz + D[6 * r + 5] * by;
+    db[r][1] = D[6 * r + 1] * by + D[6 * r + 3] * bz + D[6 * r + 5] * bx;
+    db[r][2] = D[6 * r + 2] * bz + D[6 * r + 3] * by + D[6 * r + 4] * bx;
+  }
+}
 
 // lanes 0..7: Gauss point `lane` (reference loop order xi, eta, zeta)
 __device__ __forceinline__ void hex_gauss_point(int lane, const double *x, const double *y, const double *z,
@@ -188,6 +201,7 @@ __device__ __forceinline__ void csr_add(const int *__restrict__ rowptr, const in
 // sum_gp |J| B_a^T D B_b with B rows [xx, yy, zz, yz, xz, xy]
 // (linhex::geom_matrix, MEFEL/SRC/linhex.cpp:153-186) and isotropic D
 // (elastisomat::matstiff_spacestr, MEFEL/SRC/elastisomat.cpp:395-420)
+template <bool GEN>
 __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__restrict__ elist,
                                                       const double *__restrict__ coords,
                                                       const int64_t *__restrict__ elems,
@@ -212,11 +226,18 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
       z[a] = __shfl_sync(0xffffffffu, cz, a);
     }
     hex_gauss_point(lane, x, y, z, sh, false);
+    if (GEN) {
+      for (int q = lane; q < 36; q += 32) sh.D[q] = emat[36 * (int64_t)e + q];
+    }
     __syncwarp();
-    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
-    const double G = E / 2.0 / (1.0 + nu);
-    const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
-    const double d0 = s * (1 - nu), d1 = s * nu;
+    double d0 = 0.0, d1 = 0.0, G = 0.0;
+    if (!GEN) {
+      const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+      G = E / 2.0 / (1.0 + nu);
+      const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
+      d0 = s * (1 - nu);
+      d1 = s * nu;
+    }
     int code[24];
 #pragma unroll
     for (int q = 0; q < 24; q++) code[q] = __ldg(cne + (int64_t)e * 24 + q);
@@ -230,8 +251,17 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
         const double w = sh.w[gp];
         // D B_b: columns (u, v, w) of node b
         // rows: xx, yy, zz, yz, xz, xy
-        const double db[6][3] = {{d0 * bx, d1 * by, d1 * bz}, {d1 * bx, d0 * by, d1 * bz}, {d1 * bx, d1 * by, d0 * bz},
-                                 {0.0, G * bz, G * by},        {G * bz, 0.0, G * bx},        {G * by, G * bx, 0.0}};
+        double db[6][3];
+        if (GEN) {
+          elastic_db(sh.D, bx, by, bz, db);
+        } else {
+          db[0][0] = d0 * bx; db[0][1] = d1 * by; db[0][2] = d1 * bz;
+          db[1][0] = d1 * bx; db[1][1] = d0 * by; db[1][2] = d1 * bz;
+          db[2][0] = d1 * bx; db[2][1] = d1 * by; db[2][2] = d0 * bz;
+          db[3][0] = 0.0;     db[3][1] = G * bz;  db[3][2] = G * by;
+          db[4][0] = G * bz;  db[4][1] = 0.0;     db[4][2] = G * bx;
+          db[5][0] = G * by;  db[5][1] = G * bx;  db[5][2] = 0.0;
+        }
 #pragma unroll
         for (int j = 0; j < 3; j++) {
           // B_a^T rows: u -> (xx: ax, xz: az, xy: ay); v -> (yy: ay, yz: az, xy: ax); w -> (zz: az, yz: ay, xz: ax)
@@ -265,6 +295,7 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
 // det3d sets err bit 8 (the reference aborts on wrong node numbering).
 // Half a warp per element, lane (a,b) of the 4 x 4 node blocks; lanes 0..11
 // of a half load the 12 coordinates.
+template <bool GEN>
 __global__ void __launch_bounds__(TPB) k_tet4_elastic(int ne_c, const int *__restrict__ elist,
                                                       const double *__restrict__ coords,
                                                       const int64_t *__restrict__ elems,
@@ -321,13 +352,25 @@ __global__ void __launch_bounds__(TPB) k_tet4_elastic(int ne_c, const int *__res
     } else {
       bx = -(r00 + r01 + r02); by = -(r10 + r11 + r12); bz = -(r20 + r21 + r22);
     }
-    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
-    const double G = E / 2.0 / (1.0 + nu);
-    const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
-    const double c0 = s * (1 - nu), c1 = s * nu;
     const double w = det / 6.0;
-    const double db[6][3] = {{c0 * bx, c1 * by, c1 * bz}, {c1 * bx, c0 * by, c1 * bz}, {c1 * bx, c1 * by, c0 * bz},
-                             {0.0, G * bz, G * by},        {G * bz, 0.0, G * bx},        {G * by, G * bx, 0.0}};
+    double db[6][3];
+    if (GEN) {
+      double D[36];
+#pragma unroll
+      for (int q = 0; q < 36; q++) D[q] = __ldg(emat + 36 * (int64_t)e + q);
+      elastic_db(D, bx, by, bz, db);
+    } else {
+      const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+      const double G = E / 2.0 / (1.0 + nu);
+      const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
+      const double c0 = s * (1 - nu), c1 = s * nu;
+      db[0][0] = c0 * bx; db[0][1] = c1 * by; db[0][2] = c1 * bz;
+      db[1][0] = c1 * bx; db[1][1] = c0 * by; db[1][2] = c1 * bz;
+      db[2][0] = c1 * bx; db[2][1] = c1 * by; db[2][2] = c0 * bz;
+      db[3][0] = 0.0;     db[3][1] = G * bz;  db[3][2] = G * by;
+      db[4][0] = G * bz;  db[4][1] = 0.0;     db[4][2] = G * bx;
+      db[5][0] = G * by;  db[5][1] = G * bx;  db[5][2] = 0.0;
+    }
     double k[3][3];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
@@ -639,6 +682,7 @@ int colour_elements(int64_t nn, int64_t ne, int nne, const int64_t *elems, std::
 // re-integrated (new materials, the capacity form) on the same pattern.
 struct AssemblyData {
   int kind = 0, nne = 0, ndofn = 0;
+  bool general = false;  // emat holds a 6 x 6 material stiffness per element
   int64_t nn = 0, ne = 0;
   DevBuf<double> coords, emat, thick, rho;
   DevBuf<int64_t> elems;
@@ -662,8 +706,12 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
     const int *el = ad.elist.p + beg;
     switch (kind) {
       case 0:
-        k_hex8_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, c.rowptr.p,
-                                            c.col.p, c.val.p, err.p);
+        if (ad.general)
+          k_hex8_elastic<true><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                    c.rowptr.p, c.col.p, c.val.p, err.p);
+        else
+          k_hex8_elastic<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                     c.rowptr.p, c.col.p, c.val.p, err.p);
         break;
       case 1:
         k_quad4_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,
@@ -671,8 +719,12 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
         break;
       case 4: {
         const int g4 = std::min((cnt + 2 * WPB - 1) / (2 * WPB), kNumSMs * 16);
-        k_tet4_elastic<<<g4, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, c.rowptr.p,
-                                          c.col.p, c.val.p, err.p);
+        if (ad.general)
+          k_tet4_elastic<true><<<g4, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                  c.rowptr.p, c.col.p, c.val.p, err.p);
+        else
+          k_tet4_elastic<false><<<g4, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                   c.rowptr.p, c.col.p, c.val.p, err.p);
         break;
       }
       case 5: {
@@ -731,8 +783,10 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
     default: return fail(SGPU_BAD_INPUT, "unknown element kind");
   }
   if (mesh->ndofn != ndofn) return fail(SGPU_BAD_INPUT, "ndofn does not match the element kind");
-  if (mesh->nn <= 0 || mesh->ne <= 0 || !mesh->coords || !mesh->elems || !mesh->cn || !mesh->emat)
+  if (mesh->nn <= 0 || mesh->ne <= 0 || !mesh->coords || !mesh->elems || !mesh->cn || (!mesh->emat && !mesh->dmat))
     return fail(SGPU_BAD_INPUT, "empty mesh");
+  if (mesh->dmat && kind != SGPU_ELEM_HEX8 && kind != SGPU_ELEM_TET4)
+    return fail(SGPU_BAD_INPUT, "general material matrices are defined for the 3D elasticity kinds");
   if ((kind == SGPU_ELEM_QUAD4 || kind == SGPU_ELEM_TRI3) && !mesh->thick)
     return fail(SGPU_BAD_INPUT, "plane elements need thicknesses");
   if (mesh->ne > (1LL << 31) - 1) return fail(SGPU_BAD_INPUT, "too many elements");
@@ -782,13 +836,16 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   } while (0)
   BAIL_ON(ad.coords.alloc(nn * 3));
   BAIL_ON(ad.elems.alloc(ne * nne));
-  BAIL_ON(ad.emat.alloc(ne * 2));
+  ad.general = mesh->dmat != nullptr;
+  const int64_t nmatp = ad.general ? 36 : 2;
+  BAIL_ON(ad.emat.alloc(ne * nmatp));
   DevBuf<int64_t> cn_d;
   BAIL_ON(cn_d.alloc(nn * ndofn));
   BAIL_ON(ad.cne.alloc(ne * ndofe));
   cudaMemcpyAsync(ad.coords.p, mesh->coords, nn * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(ad.elems.p, mesh->elems, ne * nne * sizeof(int64_t), cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(ad.emat.p, mesh->emat, ne * 2 * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(ad.emat.p, ad.general ? mesh->dmat : mesh->emat, ne * nmatp * sizeof(double),
+                  cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(cn_d.p, mesh->cn, nn * ndofn * sizeof(int64_t), cudaMemcpyHostToDevice, s);
   if (mesh->thick) {
     BAIL_ON(ad.thick.alloc(ne));
@@ -912,7 +969,9 @@ SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, co
                          (kind == SGPU_ELEM_HEX8T_K || kind == SGPU_ELEM_HEX8T_C);
   if (kind != ad.kind && !scalar_ok) return fail(SGPU_BAD_INPUT, "element kind differs from the pattern's");
   cudaStream_t s = m->stream;
-  if (emat) SGPU_CUDA(cudaMemcpyAsync(ad.emat.p, emat, ad.ne * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (emat)
+    SGPU_CUDA(cudaMemcpyAsync(ad.emat.p, emat, ad.ne * (ad.general ? 36 : 2) * sizeof(double),
+                              cudaMemcpyHostToDevice, s));
   if (rho) {
     SGPU_TRY(ad.rho.alloc(ad.ne));
     SGPU_CUDA(cudaMemcpyAsync(ad.rho.p, rho, ad.ne * sizeof(double), cudaMemcpyHostToDevice, s));

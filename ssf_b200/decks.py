@@ -43,7 +43,11 @@ class Mesh:
     elems    (ne, nne) int64 0-based node ids in SIFEL element node order
     dofflag  (nn, ndofn) int64 constraint codes as in the deck: 1 free, 0 fixed
     emat     (ne,) int64 0-based material instance per element
-    mats     (nmat, k) float64 material parameters ((E, nu) or (k, c))
+    mats     (nmat, k) float64 material parameters: (E, nu) or (k, c) for
+             mtype "iso"; the 21 upper-triangle entries d11..d16, d22..d66 of
+             the 6 x 6 stiffness for "gen3d" (elastgmat3d); the 36 entries
+             of the local stiffness then the 9 of the transformation T
+             (x_global = T x_local), both row-major, for "ortho" (elastortomat)
     thick    (ne,) float64 element thickness (plane stress) or None
     loads    (nlc, nn, ndofn) float64 nodal forces per load case
     """
@@ -57,6 +61,7 @@ class Mesh:
     loads: np.ndarray
     thick: np.ndarray | None = None
     meta: dict = field(default_factory=dict)
+    mtype: str = "iso"
 
     @property
     def nn(self) -> int:
@@ -85,6 +90,34 @@ class Mesh:
     @property
     def ndof(self) -> int:
         return int((self.dofflag == 1).sum())
+
+
+MATTYPE = {"iso": 1, "gen3d": 2, "ortho": 3}
+
+
+def orthotropic_local(E1, E2, E3, nu12, nu13, nu23, G23, G13, G12) -> np.ndarray:
+    """6 x 6 stiffness of an orthotropic material in its own axes, strain
+    order [xx, yy, zz, yz, xz, xy] with engineering shears: the inverse of the
+    compliance (nu_ij E_j = nu_ji E_i)."""
+    S = np.zeros((6, 6))
+    S[0, 0], S[1, 1], S[2, 2] = 1.0 / E1, 1.0 / E2, 1.0 / E3
+    S[0, 1] = S[1, 0] = -nu12 / E1
+    S[0, 2] = S[2, 0] = -nu13 / E1
+    S[1, 2] = S[2, 1] = -nu23 / E2
+    S[3, 3], S[4, 4], S[5, 5] = 1.0 / G23, 1.0 / G13, 1.0 / G12
+    D = np.linalg.inv(S)
+    return 0.5 * (D + D.T)
+
+
+def rotation(angles) -> np.ndarray:
+    """x_global = R x_local for rotations by angles (radians) about x, then y,
+    then z."""
+    ax, ay, az = angles
+    cx, sx, cy, sy, cz, sz = np.cos(ax), np.sin(ax), np.cos(ay), np.sin(ay), np.cos(az), np.sin(az)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return Rz @ Ry @ Rx
 
 
 def _hex_grid(nx, ny, nz, lx, ly, lz):
@@ -343,12 +376,20 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
             # type lineartet (100) or linearhex (102), cne 0, crst 0, one
             # material elisomat (1)
             et = 100 if mesh.kind == "tet4" else 102
-            lines.append(f"{e + 1} {et} {ns} 0 0 1 1 {m}")
-    # materials: one type (elisomat = 1), mats.shape[0] instances "id e nu"
+            lines.append(f"{e + 1} {et} {ns} 0 0 1 {MATTYPE[mesh.mtype]} {m}")
+    # materials: one type, mats.shape[0] instances: "id e nu" (elisomat = 1),
+    # "id d11 .. d16 d22 .. d66" (elgmat3d = 2, elastgmat3d::read), or
+    # "id" + the 36 local stiffness entries + 9 transformation functions,
+    # each "0 value" (funct_type stat, const_val) (elortomat = 3,
+    # elastortomat::read and gfunct::read)
     lines.append("1")
-    lines.append(f"1 {mesh.mats.shape[0]}")
-    for k, (E, nu) in enumerate(mesh.mats):
-        lines.append(f"{k + 1} {_fmt(E)} {_fmt(nu)}")
+    lines.append(f"{MATTYPE[mesh.mtype]} {mesh.mats.shape[0]}")
+    for k, row in enumerate(mesh.mats):
+        if mesh.mtype == "ortho":
+            lines.append(f"{k + 1} " + " ".join(_fmt(v) for v in row[:36]) + " "
+                         + " ".join(f"0 {_fmt(v)}" for v in row[36:45]))
+        else:
+            lines.append(f"{k + 1} " + " ".join(_fmt(v) for v in row))
     # cross sections
     if is2d:
         tvals = mesh.meta.get("tvals", [float(mesh.thick[0])])

@@ -29,17 +29,56 @@ def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
 
 
+def strain_transformation(T) -> np.ndarray:
+    """6 x 6 transformation of strain vectors [xx, yy, zz, yz, xz, xy]
+    (engineering shears) built from the 3 x 3 axes T (x_global = T x_local),
+    as lg_tens4transf (MEFEL/SRC/vecttens.cpp:1561-1615) lays it out."""
+    t = np.zeros((6, 6))
+    for c in range(3):
+        t[c] = [T[0, c] ** 2, T[1, c] ** 2, T[2, c] ** 2, T[1, c] * T[2, c], T[0, c] * T[2, c], T[0, c] * T[1, c]]
+    for r, (a, b) in enumerate(((2, 1), (2, 0), (1, 0))):
+        t[3 + r] = [2.0 * T[0, a] * T[0, b], 2.0 * T[1, a] * T[1, b], 2.0 * T[2, a] * T[2, b],
+                    T[1, a] * T[2, b] + T[2, a] * T[1, b], T[0, a] * T[2, b] + T[2, a] * T[0, b],
+                    T[0, a] * T[1, b] + T[1, a] * T[0, b]]
+    return t
+
+
+def material_matrices(mesh) -> np.ndarray:
+    """Global 6 x 6 material stiffness per material instance, (nmat, 36), of a
+    mesh with general materials: "gen3d" rows are the 21 upper-triangle
+    entries (elastgmat3d::matstiff, MEFEL/SRC/elastgmat3d.cpp:69); "ortho"
+    rows are the local stiffness (36) and the constant axes T (9), turned
+    into the global system as t^T D t (elastortomat::matstiff,
+    MEFEL/SRC/elastortomat.cpp:100-115)."""
+    mats = np.asarray(mesh.mats, dtype=np.float64)
+    out = np.zeros((mats.shape[0], 36))
+    for k, row in enumerate(mats):
+        if mesh.mtype == "gen3d":
+            D = np.zeros((6, 6))
+            D[np.triu_indices(6)] = row[:21]
+            out[k] = (np.triu(D) + np.triu(D, 1).T).ravel()
+        elif mesh.mtype == "ortho":
+            t = strain_transformation(row[36:45].reshape(3, 3))
+            out[k] = (t.T @ row[:36].reshape(6, 6) @ t).ravel()
+        else:
+            raise ValueError(f"material type {mesh.mtype!r} has no general matrix")
+    return out
+
+
 def _assemble(mesh, kind: str, rho=None):
     coords = _c(mesh.coords, np.float64)
     elems = _c(mesh.elems, np.int64)
     cn = _c(mesh.code_numbers(), np.int64)
-    emat = _c(mesh.mats[mesh.emat], np.float64)
+    general = getattr(mesh, "mtype", "iso") != "iso"
+    emat = None if general else _c(mesh.mats[mesh.emat], np.float64)
+    dmat = _c(material_matrices(mesh)[mesh.emat], np.float64) if general else None
     thick = _c(mesh.thick, np.float64) if mesh.thick is not None else None
     rr = _c(rho, np.float64) if rho is not None else None
-    keep = (coords, elems, cn, emat, thick, rr)
+    keep = (coords, elems, cn, emat, dmat, thick, rr)
     m = L.Mesh(KIND[kind], cn.shape[1], coords.shape[0], coords.ctypes.data, elems.shape[0], elems.ctypes.data,
-               cn.ctypes.data, emat.ctypes.data, thick.ctypes.data if thick is not None else None,
-               rr.ctypes.data if rr is not None else None)
+               cn.ctypes.data, emat.ctypes.data if emat is not None else None,
+               thick.ctypes.data if thick is not None else None,
+               rr.ctypes.data if rr is not None else None, dmat.ctypes.data if dmat is not None else None)
     h = C.c_void_p()
     info = L.AssemblyInfo()
     L.check(L.lib().sgpu_assemble(C.byref(m), C.byref(h), C.byref(info)))

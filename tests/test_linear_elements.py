@@ -212,3 +212,60 @@ def test_tri_plate_solve_matches_oracle(oracle, gpu_lib, prec, mode):
         x, r = K.pcg(f, res=1e-22, zero=1e-300, prec=prec, mode=mode)
     assert r.status == L.OK
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+# ---------------------------------------------------------------------------
+# general material matrices (elastgmat3d, elastortomat) on hex8 / tet4
+# ---------------------------------------------------------------------------
+
+def _ortho_mesh(kind, nx=6, ny=3, nz=3):
+    m = decks.cantilever_hex(nx, ny, nz) if kind == "hex8" else decks.cantilever_tet(nx, ny, nz)
+    Dl = decks.orthotropic_local(150e9, 10e9, 9e9, 0.3, 0.28, 0.45, 3.5e9, 5e9, 5.5e9)
+    rows = [np.concatenate([Dl.ravel(), decks.rotation(a).ravel()]) for a in ((0.0, 0.0, 0.0), (0.3, -0.5, 0.9))]
+    m.mtype, m.mats = "ortho", np.array(rows)
+    m.emat = np.arange(m.ne) % 2
+    return m
+
+
+def test_material_matrices_host_mirror(oracle):
+    # the product's host-side transformation against the oracle's restatement
+    from ssf_b200 import mefel
+    m = _ortho_mesh("hex8", 2, 1, 1)
+    a, b = mefel.material_matrices(m), oracle.material_dmat(m)
+    assert np.allclose(a, b, rtol=1e-14, atol=1e-14 * np.abs(b).max())
+    # the identity transformation leaves the local matrix unchanged
+    assert np.array_equal(b[0], m.mats[0, :36])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["hex8", "tet4"])
+@pytest.mark.parametrize("mtype", ["ortho", "gen3d"])
+def test_general_material_assembly_matches_oracle(oracle, gpu_lib, kind, mtype):
+    from ssf_b200 import mefel
+    m = _ortho_mesh(kind)
+    if mtype == "gen3d":
+        D = mefel.material_matrices(m)
+        m.mtype = "gen3d"
+        m.mats = np.array([d.reshape(6, 6)[np.triu_indices(6)] for d in D])
+    rng = np.random.default_rng(9)
+    m.coords = m.coords + rng.uniform(-0.004, 0.004, m.coords.shape)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    with mefel.stiffness_matrix(m) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+    assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+@pytest.mark.gpu
+def test_orthotropic_cantilever_solve_matches_oracle(oracle, gpu_lib):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = _ortho_mesh("hex8", 30, 6, 6)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    f = oracle.load_vector(m)
+    xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with mefel.stiffness_matrix(m) as K:
+        K.set_nullspace(mefel.rigid_body_modes(m))
+        x, r = K.pcg(f, res=1e-22, prec="agg", mode="mixed")
+    assert r.status == L.OK
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8

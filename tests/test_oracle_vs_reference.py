@@ -77,6 +77,45 @@ def test_random_distorted_tri_plate_bit_exact(ref):
     assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
 
 
+def _dump_and_compare(ref, m):
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    assert np.array_equal(a, d["K_a"])
+    f = ref.load_vector(m)
+    x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
+
+
+@pytest.mark.parametrize("kind", ["hex8", "tet4"])
+def test_orthotropic_material_bit_exact(ref, kind):
+    # elastortomat (material type 3): local orthotropic stiffness turned into
+    # the global system by lg_tens4transf with a constant rotation; two
+    # instances with different axes
+    m = decks.cantilever_hex(6, 2, 2) if kind == "hex8" else decks.cantilever_tet(5, 2, 2)
+    rng = np.random.default_rng(45)
+    inner = ~np.isclose(m.coords[:, 0], 0.0)
+    m.coords[inner] += rng.uniform(-0.004, 0.004, (inner.sum(), 3))
+    Dl = decks.orthotropic_local(150e9, 10e9, 9e9, 0.3, 0.28, 0.45, 3.5e9, 5e9, 5.5e9)
+    rows = [np.concatenate([Dl.ravel(), decks.rotation(a).ravel()]) for a in ((0.0, 0.0, 0.0), (0.3, -0.5, 0.9))]
+    m.mtype, m.mats = "ortho", np.array(rows)
+    m.emat = rng.integers(0, 2, m.ne)
+    _dump_and_compare(ref, m)
+
+
+def test_general_anisotropic_material_bit_exact(ref):
+    # elastgmat3d (material type 2): the 21 entries of a symmetric 6 x 6 D
+    m = decks.cantilever_hex(6, 2, 2)
+    Dl = decks.orthotropic_local(150e9, 10e9, 9e9, 0.3, 0.28, 0.45, 3.5e9, 5e9, 5.5e9)
+    m.mtype = "gen3d"
+    m.mats = np.array([Dl[np.triu_indices(6)], (1.5 * Dl)[np.triu_indices(6)]])
+    m.emat = np.arange(m.ne) % 2
+    _dump_and_compare(ref, m)
+
+
 def test_reference_solver_library_matches_oracle(ref):
     """libsifelref.so runs the reference's own symcomprow::cg_prec."""
     m = decks.cantilever_hex(10, 2, 2)
