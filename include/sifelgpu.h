@@ -248,27 +248,31 @@ typedef enum {
   SGPU_ELEM_HEX8T_K = 2, /* linhext conductivity (TRFEL/SRC/linhext.cpp:774) */
   SGPU_ELEM_HEX8T_C = 3, /* linhext capacity (TRFEL/SRC/linhext.cpp:979) */
   SGPU_ELEM_TET4 = 4,    /* lintet, 3D elasticity, 1 point (MEFEL/SRC/lintet.cpp:290) */
-  SGPU_ELEM_TRI3 = 5     /* planeelemlt, plane stress, 1 point (MEFEL/SRC/plelemlt.cpp:234) */
+  SGPU_ELEM_TRI3 = 5,    /* planeelemlt, plane stress, 1 point (MEFEL/SRC/plelemlt.cpp:234) */
+  SGPU_ELEM_HEX20 = 6,   /* quadhex, 3D elasticity, 3x3x3 Gauss (MEFEL/SRC/quadhex.cpp:232) */
+  SGPU_ELEM_QUAD8 = 7    /* planeelemqq, plane stress, 3x3 Gauss (MEFEL/SRC/plelemqq.cpp:215) */
 } sgpu_elem_kind;
 
 /* A mesh in SIFEL's terms.  Node order inside an element follows SIFEL
- * (GEFEL/basefun.cpp:2299 for hexahedra, :609 for quadrilaterals); a
+ * (GEFEL/basefun.cpp:2299 for hexahedra, :609 for quadrilaterals, :2377 and
+ * :708 for their serendipity forms); a quad8 with a negative Jacobian fails
+ * like a tetrahedron of negative volume; a
  * tetrahedron must have det3d > 0 (GEFEL/matrix.cpp:3629), else
  * sgpu_assemble fails with SGPU_BAD_INPUT as the reference aborts. */
 typedef struct {
   int32_t kind;          /* sgpu_elem_kind */
-  int32_t ndofn;         /* DOFs per node: 3 (hex8, tet4), 2 (quad4, tri3), 1 (hex8t) */
+  int32_t ndofn;         /* DOFs per node: 3 (hex8, tet4, hex20), 2 (quad4, tri3, quad8), 1 (hex8t) */
   int64_t nn;            /* nodes */
-  const double *coords;  /* nn x 3 (z ignored for quad4, tri3) */
+  const double *coords;  /* nn x 3 (z ignored for the plane kinds) */
   int64_t ne;            /* elements */
   const int64_t *elems;  /* ne x nne, 0-based node ids */
   const int64_t *cn;     /* nn x ndofn code numbers (1-based, <= 0: no equation) */
   const double *emat;    /* ne x 2: (E, nu) for elasticity, (k, c) for hex8t */
-  const double *thick;   /* ne thicknesses (quad4, tri3), else NULL */
+  const double *thick;   /* ne thicknesses (plane kinds), else NULL */
   const double *rho;     /* ne densities (capacity), NULL = 1 */
   const double *dmat;    /* NULL, or ne x 36: a general material stiffness per
                             element (6 x 6 row-major, global axes, strain order
-                            xx yy zz yz xz xy) for hex8 / tet4, replacing emat:
+                            xx yy zz yz xz xy) for hex8 / tet4 / hex20, replacing emat:
                             elastgmat3d::matstiff (MEFEL/SRC/elastgmat3d.cpp:69)
                             or elastortomat::matstiff (elastortomat.cpp:100) */
 } sgpu_mesh;

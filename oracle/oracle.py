@@ -58,6 +58,9 @@ def lib():
         L.or_assemble_d.argtypes = [C.c_int, C.c_int, _L, _pD, _pL, _pL, _pD, _pL, _pL, _pD]
         L.or_assemble_d.restype = _L
         L.or_ortho_dmat.argtypes = [_pD, _pD, _pD]
+        L.or_hex20_ke.argtypes = [_pD, _D, _D, _pD]
+        L.or_quad8_ke.argtypes = [_pD, _D, _D, _pD, _pD]
+        L.or_quad8_ke.restype = C.c_int
         L.or_tet4_ke.restype = C.c_int
         L.or_scr_mxv.argtypes = [_L, _pL, _pL, _pD, _pD, _pD]
         L.or_cr_mxv.argtypes = [_L, _pL, _pL, _pD, _pD, _pD]
@@ -98,6 +101,20 @@ def tet4_ke(xyz, E, nu):
     return ke.reshape(12, 12)
 
 
+def hex20_ke(xyz, E, nu):
+    ke = np.zeros(3600)
+    lib().or_hex20_ke(_f64(xyz).reshape(-1), float(E), float(nu), ke)
+    return ke.reshape(60, 60)
+
+
+def quad8_ke(xy, E, nu, t):
+    ke = np.zeros(256)
+    tt = _f64(np.broadcast_to(np.asarray(t, dtype=np.float64), (8,)))
+    if lib().or_quad8_ke(_f64(xy).reshape(-1), float(E), float(nu), tt, ke) != 0:
+        raise ValueError("negative Jacobian (wrong node numbering)")
+    return ke.reshape(16, 16)
+
+
 def tri3_ke(xy, E, nu, t):
     ke = np.zeros(36)
     tt = _f64(np.broadcast_to(np.asarray(t, dtype=np.float64), (3,)))
@@ -124,7 +141,7 @@ def hex8t_kc(xyz, k, c, rho=1.0):
 # mesh-level assembly
 # ----------------------------------------------------------------------------
 
-KIND = {"hex8": 0, "quad4": 1, "hex8t_k": 2, "hex8t_c": 3, "tet4": 4, "tri3": 5}
+KIND = {"hex8": 0, "quad4": 1, "hex8t_k": 2, "hex8t_c": 3, "tet4": 4, "tri3": 5, "hex20": 6, "quad8": 7}
 
 
 def element_code_numbers(mesh):
@@ -169,7 +186,7 @@ def assemble(mesh, sym=True, kind=None, rho=None):
     adr, ci = pattern(n, cne, sym)
     a = np.zeros(ci.size)
     if getattr(mesh, "mtype", "iso") != "iso":
-        if kind not in ("hex8", "tet4"):
+        if kind not in ("hex8", "tet4", "hex20"):
             raise ValueError("general materials are defined for the 3D elements")
         dm = _f64(material_dmat(mesh)[mesh.emat])
         st = lib().or_assemble_d(k, int(sym), mesh.ne, _f64(mesh.coords), _i64(mesh.elems), cne, dm, adr, ci, a)

@@ -134,7 +134,7 @@ static double derivatives_2d(double *dx, double *dy, const double *x, const doub
  * (matrix.cpp:1362, 1184), then cmulm and addm (y + d). A, C: m x n; B: m x m */
 static void bdbjac(double *d, const double *a, const double *b, const double *c, double jac,
                    int m, int n) {
-  double x[24 * 6];
+  double x[60 * 6];
   double y;
   for (int i = 0; i < n; i++)
     for (int j = 0; j < m; j++) {
@@ -345,7 +345,7 @@ void or_quad4_ke(const double *xy, double e, double nu, const double *t, double 
 
 /* bdbj, GEFEL/matrix.cpp:3066-3110: symmetric fill of B^T D B jac */
 static void bdbj(double *k, const double *b, const double *d, double jac, int m, int n) {
-  double am[3 * 8];
+  double am[3 * 16];
   int ll = 0;
   for (int i = 0; i < n; i++)
     for (int j = 0; j < m; j++) {
@@ -396,6 +396,168 @@ void or_tri3_ke(const double *xy, double e, double nu, const double *t, double *
   double jac = thick * det / 2.0;
   memset(ke, 0, 36 * sizeof(double));
   bdbj(ke, gm, d, jac, 3, 6);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Quadratic serendipity elements: quadhex (20 nodes), planeelemqq (8)      */
+/* ------------------------------------------------------------------------ */
+
+/* Gauss rule of order 3 with the reference's constants (gauss_points,
+ * GEFEL/intp.cpp:34-43) */
+static const double GP3[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+static const double GW3[3] = {0.5555555555555555, 0.8888888888888888, 0.5555555555555555};
+
+/* natural coordinates of the 20 nodes in SIFEL's order (bf_quad_hex_3d,
+ * GEFEL/basefun.cpp:2377-2403): corners as the linear hexahedron, then the
+ * mid-edge nodes of the zeta = +1 face, the four vertical edges, and the
+ * zeta = -1 face */
+static const double H20[20][3] = {
+    {1, 1, 1},  {-1, 1, 1},  {-1, -1, 1},  {1, -1, 1},  {1, 1, -1},  {-1, 1, -1},  {-1, -1, -1},
+    {1, -1, -1}, {0, 1, 1},  {-1, 0, 1},   {0, -1, 1},  {1, 0, 1},   {1, 1, 0},    {-1, 1, 0},
+    {-1, -1, 0}, {1, -1, 0}, {0, 1, -1},   {-1, 0, -1}, {0, -1, -1}, {1, 0, -1}};
+
+/* derivatives of the 20-node serendipity functions with respect to the
+ * natural coordinates (the functions of dx/dy/dz_bf_quad_hex_3d,
+ * basefun.cpp:2413-2520, written from the corner and mid-edge formulas) */
+static void hex20_dnat(double xi, double eta, double zeta, double *nx, double *ny, double *nz) {
+  for (int a = 0; a < 20; a++) {
+    double p = H20[a][0], q = H20[a][1], r = H20[a][2];
+    double fx = 1.0 + xi * p, fy = 1.0 + eta * q, fz = 1.0 + zeta * r;
+    if (p != 0.0 && q != 0.0 && r != 0.0) {
+      nx[a] = p * fy * fz * (2.0 * xi * p + eta * q + zeta * r - 1.0) / 8.0;
+      ny[a] = q * fx * fz * (xi * p + 2.0 * eta * q + zeta * r - 1.0) / 8.0;
+      nz[a] = r * fx * fy * (xi * p + eta * q + 2.0 * zeta * r - 1.0) / 8.0;
+    } else if (p == 0.0) {
+      nx[a] = -xi * fy * fz / 2.0;
+      ny[a] = q * (1.0 - xi * xi) * fz / 4.0;
+      nz[a] = r * (1.0 - xi * xi) * fy / 4.0;
+    } else if (q == 0.0) {
+      nx[a] = p * (1.0 - eta * eta) * fz / 4.0;
+      ny[a] = -eta * fx * fz / 2.0;
+      nz[a] = r * (1.0 - eta * eta) * fx / 4.0;
+    } else {
+      nx[a] = p * (1.0 - zeta * zeta) * fy / 4.0;
+      ny[a] = q * (1.0 - zeta * zeta) * fx / 4.0;
+      nz[a] = -zeta * fx * fy / 2.0;
+    }
+  }
+}
+
+/* derivatives_3d (GEFEL/difcalc.cpp:487-565) for nn nodes: natural
+ * derivatives in, Cartesian out; returns detJ */
+static double derivatives_3d_n(int nn, double *dx, double *dy, double *dz, const double *x, const double *y,
+                               const double *z) {
+  double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0, jac;
+  for (int i = 0; i < nn; i++) {
+    d1 += dx[i] * x[i]; d2 += dy[i] * x[i]; d3 += dz[i] * x[i];
+    d4 += dx[i] * y[i]; d5 += dy[i] * y[i]; d6 += dz[i] * y[i];
+    d7 += dx[i] * z[i]; d8 += dy[i] * z[i]; d9 += dz[i] * z[i];
+  }
+  jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+  for (int i = 0; i < nn; i++) {
+    double ddx = dx[i], ddy = dy[i], ddz = dz[i];
+    dx[i] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
+    dy[i] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
+    dz[i] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+  }
+  return jac;
+}
+
+/* quadhex::stiffness_matrix, MEFEL/SRC/quadhex.cpp:232-270: 3 x 3 x 3 Gauss
+ * (loop order xi, eta, zeta), geom_matrix (:150-180) as for the linear
+ * hexahedron, weight detJ w_i w_j w_k (no absolute value), bdbjac.
+ * xyz: 20 x (x,y,z); dm: general 6 x 6 D or NULL for (e, nu). */
+static void hex20_ke(const double *xyz, double e, double nu, const double *dm, double *ke) {
+  double x[20], y[20], z[20], dx[20], dy[20], dz[20], gm[6 * 60], d[36];
+  for (int i = 0; i < 20; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
+  memset(ke, 0, 3600 * sizeof(double));
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      for (int k = 0; k < 3; k++) {
+        hex20_dnat(GP3[i], GP3[j], GP3[k], dx, dy, dz);
+        double jac = derivatives_3d_n(20, dx, dy, dz, x, y, z);
+        memset(gm, 0, sizeof(gm));
+        for (int a = 0; a < 20; a++) {
+          int jj = 3 * a, kk = 3 * a + 1, ll = 3 * a + 2;
+          gm[0 * 60 + jj] = dx[a];
+          gm[1 * 60 + kk] = dy[a];
+          gm[2 * 60 + ll] = dz[a];
+          gm[3 * 60 + kk] = dz[a]; gm[3 * 60 + ll] = dy[a];
+          gm[4 * 60 + jj] = dz[a]; gm[4 * 60 + ll] = dx[a];
+          gm[5 * 60 + jj] = dy[a]; gm[5 * 60 + kk] = dx[a];
+        }
+        if (dm) memcpy(d, dm, sizeof(d));
+        else matstiff_spacestr(e, nu, d);
+        jac *= GW3[i] * GW3[j] * GW3[k];
+        bdbjac(ke, gm, d, gm, jac, 6, 60);
+      }
+}
+
+void or_hex20_ke(const double *xyz, double e, double nu, double *ke) { hex20_ke(xyz, e, nu, NULL, ke); }
+
+/* natural coordinates of the 8 nodes (bf_quad_4_2d, GEFEL/basefun.cpp:708-718):
+ * corners as the bilinear quad, then the mid-sides eta = +1, xi = -1,
+ * eta = -1, xi = +1 */
+static const double Q8[8][2] = {{1, 1}, {-1, 1}, {-1, -1}, {1, -1}, {0, 1}, {-1, 0}, {0, -1}, {1, 0}};
+
+static void quad8_n(double xi, double eta, double *n, double *nx, double *ny) {
+  for (int a = 0; a < 8; a++) {
+    double p = Q8[a][0], q = Q8[a][1], fx = 1.0 + xi * p, fy = 1.0 + eta * q;
+    if (p != 0.0 && q != 0.0) {
+      n[a] = 0.25 * fx * fy * (xi * p + eta * q - 1.0);
+      nx[a] = 0.25 * p * fy * (2.0 * xi * p + eta * q);
+      ny[a] = 0.25 * q * fx * (xi * p + 2.0 * eta * q);
+    } else if (p == 0.0) {
+      n[a] = 0.5 * (1.0 - xi * xi) * fy;
+      nx[a] = -xi * fy;
+      ny[a] = 0.5 * q * (1.0 - xi * xi);
+    } else {
+      n[a] = 0.5 * fx * (1.0 - eta * eta);
+      nx[a] = 0.5 * p * (1.0 - eta * eta);
+      ny[a] = -eta * fx;
+    }
+  }
+}
+
+/* planeelemqq::stiffness_matrix, MEFEL/SRC/plelemqq.cpp:215-270: 3 x 3 Gauss,
+ * geom_matrix (:150-170) with derivatives_2d (GEFEL/difcalc.cpp:86-138),
+ * a negative detJ is an error (the reference aborts), thickness
+ * interpolated from nodal values t[8] (planeelemqq::approx, :102-112),
+ * weight detJ t w_i w_j, bdbj.  xy: 8 x (x,y).  Returns 0 or -1. */
+int or_quad8_ke(const double *xy, double e, double nu, const double *t, double *ke) {
+  double x[8], y[8], n[8], dx[8], dy[8], gm[3 * 16], d[9];
+  for (int i = 0; i < 8; i++) { x[i] = xy[2 * i]; y[i] = xy[2 * i + 1]; }
+  memset(ke, 0, 256 * sizeof(double));
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double xi = GP3[i], eta = GP3[j];
+      quad8_n(xi, eta, n, dx, dy);
+      double d1 = 0, d2 = 0, d3 = 0, d4 = 0;
+      for (int a = 0; a < 8; a++) {
+        d1 += dx[a] * x[a]; d2 += dy[a] * x[a];
+        d3 += dx[a] * y[a]; d4 += dy[a] * y[a];
+      }
+      double jac = d1 * d4 - d2 * d3;
+      for (int a = 0; a < 8; a++) {
+        double ddx = dx[a], ddy = dy[a];
+        dx[a] = (ddx * d4 - ddy * d3) / jac;
+        dy[a] = (ddy * d1 - ddx * d2) / jac;
+      }
+      if (jac < 0.0) return -1;
+      memset(gm, 0, sizeof(gm));
+      for (int a = 0; a < 8; a++) {
+        gm[0 * 16 + 2 * a] = dx[a];
+        gm[1 * 16 + 2 * a + 1] = dy[a];
+        gm[2 * 16 + 2 * a] = dy[a];
+        gm[2 * 16 + 2 * a + 1] = dx[a];
+      }
+      matstiff_plstress(e, nu, d);
+      double thick = 0.0;
+      for (int a = 0; a < 8; a++) thick += n[a] * t[a];
+      jac *= thick * GW3[i] * GW3[j];
+      bdbj(ke, gm, d, jac, 3, 16);
+    }
+  return 0;
 }
 
 /* nnj, GEFEL/matrix.cpp:3149-3174 (single row N) */
@@ -574,7 +736,8 @@ void or_cr_localize(long *adr, long *ci, double *a, const double *b, const long 
 /* ------------------------------------------------------------------------ */
 
 /* kind 0 = hex8 elasticity, 1 = quad4 plane stress, 2 = hex8 conduction,
- * 3 = hex8 capacity, 4 = tet4 elasticity, 5 = tri3 plane stress.  coords: nn x 3; elems: ne x nne;
+ * 3 = hex8 capacity, 4 = tet4 elasticity, 5 = tri3 plane stress,
+ * 6 = hex20 elasticity, 7 = quad8 plane stress.  coords: nn x 3; elems: ne x nne;
  * cn: ne x ndofe; mats: per element material row (E,nu) or (k,c); thick: per
  * element (quad4) or NULL; rho: per element density (capacity) or NULL
  * (then 1).  Returns 0, or -(e+1) for the first element e of negative volume
@@ -582,18 +745,26 @@ void or_cr_localize(long *adr, long *ci, double *a, const double *b, const long 
 long or_assemble(int kind, int sym, long ne, const double *coords, const long *elems,
                  const long *cn, const double *emat, const double *thick, const double *rho,
                  long *adr, long *ci, double *a) {
-  long nne = (kind == 5) ? 3 : ((kind == 1 || kind == 4) ? 4 : 8);
-  long ndofe = (kind == 0) ? 24 : (kind == 4 ? 12 : (kind == 5 ? 6 : 8));
-  double xyz[24], xy[8], t[4], r[8], ke[576];
+  static const long NNE[8] = {8, 4, 8, 8, 4, 3, 20, 8}, NDOFN[8] = {3, 2, 1, 1, 3, 2, 3, 2};
+  long nne = NNE[kind], ndofe = NNE[kind] * NDOFN[kind];
+  double xyz[60], xy[16], t[8], r[8];
+  double *ke = (double *)malloc(3600 * sizeof(double));
   for (long e = 0; e < ne; e++) {
     const long *nd = elems + e * nne;
-    if (kind == 5) {
+    if (kind == 6) {
+      for (int i = 0; i < 20; i++)
+        for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
+      or_hex20_ke(xyz, emat[2 * e], emat[2 * e + 1], ke);
+    } else if (kind == 7) {
+      for (int i = 0; i < 8; i++) { xy[2 * i] = coords[3 * nd[i]]; xy[2 * i + 1] = coords[3 * nd[i] + 1]; t[i] = thick[e]; }
+      if (or_quad8_ke(xy, emat[2 * e], emat[2 * e + 1], t, ke) != 0) { free(ke); return -(e + 1); }
+    } else if (kind == 5) {
       for (int i = 0; i < 3; i++) { xy[2 * i] = coords[3 * nd[i]]; xy[2 * i + 1] = coords[3 * nd[i] + 1]; t[i] = thick[e]; }
       or_tri3_ke(xy, emat[2 * e], emat[2 * e + 1], t, ke);
     } else if (kind == 4) {
       for (int i = 0; i < 4; i++)
         for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
-      if (or_tet4_ke(xyz, emat[2 * e], emat[2 * e + 1], ke) != 0) return -(e + 1);
+      if (or_tet4_ke(xyz, emat[2 * e], emat[2 * e + 1], ke) != 0) { free(ke); return -(e + 1); }
     } else if (kind == 1) {
       for (int i = 0; i < 4; i++) { xy[2 * i] = coords[3 * nd[i]]; xy[2 * i + 1] = coords[3 * nd[i] + 1]; t[i] = thick[e]; }
       or_quad4_ke(xy, emat[2 * e], emat[2 * e + 1], t, ke);
@@ -611,29 +782,34 @@ long or_assemble(int kind, int sym, long ne, const double *coords, const long *e
     if (sym) or_scr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
     else or_cr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
   }
+  free(ke);
   return 0;
 }
 
-/* or_assemble for the 3D elasticity kinds (0 hex8, 4 tet4) with a general
+/* or_assemble for the 3D elasticity kinds (0 hex8, 4 tet4, 6 hex20) with a general
  * material stiffness per element: dmat ne x 36 (row-major 6 x 6, global
  * system), as elastgmat3d::matstiff (MEFEL/SRC/elastgmat3d.cpp:69) or
  * elastortomat::matstiff give it.  Returns as or_assemble. */
 long or_assemble_d(int kind, int sym, long ne, const double *coords, const long *elems, const long *cn,
                    const double *dmat, long *adr, long *ci, double *a) {
-  long nne = (kind == 4) ? 4 : 8, ndofe = 3 * nne;
-  double xyz[24], ke[576];
+  long nne = (kind == 4) ? 4 : (kind == 6 ? 20 : 8), ndofe = 3 * nne;
+  double xyz[60];
+  double *ke = (double *)malloc(3600 * sizeof(double));
   for (long e = 0; e < ne; e++) {
     const long *nd = elems + e * nne;
     for (int i = 0; i < nne; i++)
       for (int c = 0; c < 3; c++) xyz[3 * i + c] = coords[3 * nd[i] + c];
     if (kind == 4) {
-      if (or_tet4_ke_d(xyz, dmat + 36 * e, ke) != 0) return -(e + 1);
+      if (or_tet4_ke_d(xyz, dmat + 36 * e, ke) != 0) { free(ke); return -(e + 1); }
+    } else if (kind == 6) {
+      hex20_ke(xyz, 0.0, 0.0, dmat + 36 * e, ke);
     } else {
       or_hex8_ke_d(xyz, dmat + 36 * e, ke);
     }
     if (sym) or_scr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
     else or_cr_localize(adr, ci, a, ke, cn + e * ndofe, ndofe);
   }
+  free(ke);
   return 0;
 }
 

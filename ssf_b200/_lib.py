@@ -75,7 +75,7 @@ class AssemblyInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-ELEM_HEX8, ELEM_QUAD4, ELEM_HEX8T_K, ELEM_HEX8T_C, ELEM_TET4, ELEM_TRI3 = 0, 1, 2, 3, 4, 5
+ELEM_HEX8, ELEM_QUAD4, ELEM_HEX8T_K, ELEM_HEX8T_C, ELEM_TET4, ELEM_TRI3, ELEM_HEX20, ELEM_QUAD8 = range(8)
 
 
 class SgpuError(RuntimeError):

@@ -478,6 +478,272 @@ __global__ void __launch_bounds__(TPB) k_quad4_elastic(int ne_c, const int *__re
   }
 }
 
+// ---------------------------------------------------------------------------
+// quadratic serendipity elements
+// ---------------------------------------------------------------------------
+
+// order-3 Gauss rule with the reference's constants (GEFEL/intp.cpp:34-43)
+__constant__ double c_gp3[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+__constant__ double c_gw3[3] = {0.5555555555555555, 0.8888888888888888, 0.5555555555555555};
+// natural node coordinates in SIFEL's order (bf_quad_hex_3d,
+// GEFEL/basefun.cpp:2377-2403; bf_quad_4_2d, :708-718)
+__constant__ signed char c_h20[20][3] = {
+    {1, 1, 1},  {-1, 1, 1},  {-1, -1, 1},  {1, -1, 1},  {1, 1, -1},  {-1, 1, -1},  {-1, -1, -1},
+    {1, -1, -1}, {0, 1, 1},  {-1, 0, 1},   {0, -1, 1},  {1, 0, 1},   {1, 1, 0},    {-1, 1, 0},
+    {-1, -1, 0}, {1, -1, 0}, {0, 1, -1},   {-1, 0, -1}, {0, -1, -1}, {1, 0, -1}};
+__constant__ signed char c_q8[8][2] = {{1, 1}, {-1, 1}, {-1, -1}, {1, -1}, {0, 1}, {-1, 0}, {0, -1}, {1, 0}};
+
+// dN_a/d(xi, eta, zeta) of the 20-node serendipity hexahedron
+__device__ __forceinline__ void hex20_dnat(int a, double xi, double eta, double zeta, double &nx, double &ny,
+                                           double &nz) {
+  const double p = c_h20[a][0], q = c_h20[a][1], r = c_h20[a][2];
+  const double fx = 1.0 + xi * p, fy = 1.0 + eta * q, fz = 1.0 + zeta * r;
+  if (p != 0.0 && q != 0.0 && r != 0.0) {
+    nx = p * fy * fz * (2.0 * xi * p + eta * q + zeta * r - 1.0) / 8.0;
+    ny = q * fx * fz * (xi * p + 2.0 * eta * q + zeta * r - 1.0) / 8.0;
+    nz = r * fx * fy * (xi * p + eta * q + 2.0 * zeta * r - 1.0) / 8.0;
+  } else if (p == 0.0) {
+    nx = -xi * fy * fz / 2.0;
+    ny = q * (1.0 - xi * xi) * fz / 4.0;
+    nz = r * (1.0 - xi * xi) * fy / 4.0;
+  } else if (q == 0.0) {
+    nx = p * (1.0 - eta * eta) * fz / 4.0;
+    ny = -eta * fx * fz / 2.0;
+    nz = r * (1.0 - eta * eta) * fx / 4.0;
+  } else {
+    nx = p * (1.0 - zeta * zeta) * fy / 4.0;
+    ny = q * (1.0 - zeta * zeta) * fx / 4.0;
+    nz = -zeta * fx * fy / 2.0;
+  }
+}
+
+struct Hex20Shared {
+  double g[27][20][3];  // Cartesian gradients [gp][node][x,y,z]
+  double w[27];         // detJ w_i w_j w_k
+  double D[36];
+  double xyz[20][3];
+};
+constexpr int TPB20 = 128;
+constexpr int WPB20 = TPB20 / 32;
+
+// node pair (a, b), a <= b, number blk of the 210 upper-triangle pairs of a
+// 20-node element in row order
+__device__ __forceinline__ void pair20(int blk, int &a, int &b) {
+  a = 0;
+  while (blk >= 20 - a) {
+    blk -= 20 - a;
+    a++;
+  }
+  b = a + blk;
+}
+
+// hex20 elasticity (quadhex::stiffness_matrix, MEFEL/SRC/quadhex.cpp:232-270):
+// 3 x 3 x 3 Gauss points (lane gp = 9 i + 3 j + k, the reference's loop order),
+// B as for the linear hexahedron (quadhex::geom_matrix, :150-180), weight
+// detJ w_i w_j w_k without an absolute value.  One warp per element, the
+// gradients of all points in shared memory; each lane forms whole 3 x 3
+// blocks (a, b), a <= b, and writes the block and its transpose.
+template <bool GEN>
+__global__ void __launch_bounds__(TPB20) k_hex20_elastic(int ne_c, const int *__restrict__ elist,
+                                                         const double *__restrict__ coords,
+                                                         const int64_t *__restrict__ elems,
+                                                         const int *__restrict__ cne, const double *__restrict__ emat,
+                                                         const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                         double *__restrict__ val, unsigned *err) {
+  extern __shared__ double smem20[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  Hex20Shared &sh = reinterpret_cast<Hex20Shared *>(smem20)[wib];
+  for (int t = blockIdx.x * WPB20 + wib; t < ne_c; t += gridDim.x * WPB20) {
+    const int e = elist[t];
+    if (lane < 20) {
+      const int64_t nd = elems[(int64_t)e * 20 + lane];
+      sh.xyz[lane][0] = coords[3 * nd];
+      sh.xyz[lane][1] = coords[3 * nd + 1];
+      sh.xyz[lane][2] = coords[3 * nd + 2];
+    }
+    if (GEN) {
+      for (int q = lane; q < 36; q += 32) sh.D[q] = emat[36 * (int64_t)e + q];
+    }
+    __syncwarp();
+    if (lane < 27) {
+      const int i = lane / 9, j = (lane / 3) % 3, k = lane % 3;
+      const double xi = c_gp3[i], eta = c_gp3[j], zeta = c_gp3[k];
+      double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0;
+      for (int a = 0; a < 20; a++) {
+        double nx, ny, nz;
+        hex20_dnat(a, xi, eta, zeta, nx, ny, nz);
+        const double x = sh.xyz[a][0], y = sh.xyz[a][1], z = sh.xyz[a][2];
+        d1 += nx * x; d2 += ny * x; d3 += nz * x;
+        d4 += nx * y; d5 += ny * y; d6 += nz * y;
+        d7 += nx * z; d8 += ny * z; d9 += nz * z;
+      }
+      const double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+      for (int a = 0; a < 20; a++) {
+        double ddx, ddy, ddz;
+        hex20_dnat(a, xi, eta, zeta, ddx, ddy, ddz);
+        sh.g[lane][a][0] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
+        sh.g[lane][a][1] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
+        sh.g[lane][a][2] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+      }
+      sh.w[lane] = jac * (c_gw3[i] * c_gw3[j] * c_gw3[k]);
+    }
+    __syncwarp();
+    double d0 = 0.0, d1 = 0.0, G = 0.0;
+    if (!GEN) {
+      const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+      G = E / 2.0 / (1.0 + nu);
+      const double s = E / (1.0 + nu) / (1.0 - 2.0 * nu);
+      d0 = s * (1 - nu);
+      d1 = s * nu;
+    }
+    for (int blk = lane; blk < 210; blk += 32) {
+      int a, b;
+      pair20(blk, a, b);
+      double k[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int gp = 0; gp < 27; gp++) {
+        const double ax = sh.g[gp][a][0], ay = sh.g[gp][a][1], az = sh.g[gp][a][2];
+        const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1], bz = sh.g[gp][b][2];
+        const double w = sh.w[gp];
+        double db[6][3];
+        if (GEN) {
+          elastic_db(sh.D, bx, by, bz, db);
+        } else {
+          db[0][0] = d0 * bx; db[0][1] = d1 * by; db[0][2] = d1 * bz;
+          db[1][0] = d1 * bx; db[1][1] = d0 * by; db[1][2] = d1 * bz;
+          db[2][0] = d1 * bx; db[2][1] = d1 * by; db[2][2] = d0 * bz;
+          db[3][0] = 0.0;     db[3][1] = G * bz;  db[3][2] = G * by;
+          db[4][0] = G * bz;  db[4][1] = 0.0;     db[4][2] = G * bx;
+          db[5][0] = G * by;  db[5][1] = G * bx;  db[5][2] = 0.0;
+        }
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+          k[0][jj] += w * (ax * db[0][jj] + az * db[4][jj] + ay * db[5][jj]);
+          k[1][jj] += w * (ay * db[1][jj] + az * db[3][jj] + ax * db[5][jj]);
+          k[2][jj] += w * (az * db[2][jj] + ay * db[3][jj] + ax * db[4][jj]);
+        }
+      }
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++) {
+        const int r = __ldg(cne + (int64_t)e * 60 + 3 * a + ii);
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+          const int c = __ldg(cne + (int64_t)e * 60 + 3 * b + jj);
+          if (r >= 0 && c >= 0) {
+            csr_add(rowptr, col, val, r, c, k[ii][jj], err);
+            if (a != b) csr_add(rowptr, col, val, c, r, k[ii][jj], err);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+struct Quad8Shared {
+  double g[9][8][2];
+  double w[9];
+};
+
+// quad8 plane stress (planeelemqq::stiffness_matrix, MEFEL/SRC/plelemqq.cpp:215-270):
+// 3 x 3 Gauss (lane gp = 3 i + j), gradients by derivatives_2d, a negative
+// detJ sets err bit 8 (the reference aborts), thickness interpolated from the
+// nodal values (planeelemqq::approx, :102-112), weight detJ t w_i w_j; B rows
+// [xx, yy, xy] (geom_matrix, :150-170), plane-stress D.  One warp per
+// element, lanes cover the 64 node blocks of 2 x 2.
+__global__ void __launch_bounds__(TPB) k_quad8_elastic(int ne_c, const int *__restrict__ elist,
+                                                       const double *__restrict__ coords,
+                                                       const int64_t *__restrict__ elems,
+                                                       const int *__restrict__ cne, const double *__restrict__ emat,
+                                                       const double *__restrict__ thick,
+                                                       const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                       double *__restrict__ val, unsigned *err) {
+  __shared__ Quad8Shared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  Quad8Shared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double cx = 0, cy = 0;
+    if (lane < 8) {
+      const int64_t nd = elems[(int64_t)e * 8 + lane];
+      cx = coords[3 * nd];
+      cy = coords[3 * nd + 1];
+    }
+    double x[8], y[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+    }
+    const double t_e = thick[e];
+    bool bad = false;
+    if (lane < 9) {
+      const double xi = c_gp3[lane / 3], eta = c_gp3[lane % 3];
+      double nx[8], ny[8], th = 0.0, d1 = 0, d2 = 0, d3 = 0, d4 = 0;
+#pragma unroll
+      for (int a = 0; a < 8; a++) {
+        const double p = c_q8[a][0], q = c_q8[a][1], fx = 1.0 + xi * p, fy = 1.0 + eta * q;
+        double n;
+        if (p != 0.0 && q != 0.0) {
+          n = 0.25 * fx * fy * (xi * p + eta * q - 1.0);
+          nx[a] = 0.25 * p * fy * (2.0 * xi * p + eta * q);
+          ny[a] = 0.25 * q * fx * (xi * p + 2.0 * eta * q);
+        } else if (p == 0.0) {
+          n = 0.5 * (1.0 - xi * xi) * fy;
+          nx[a] = -xi * fy;
+          ny[a] = 0.5 * q * (1.0 - xi * xi);
+        } else {
+          n = 0.5 * fx * (1.0 - eta * eta);
+          nx[a] = 0.5 * p * (1.0 - eta * eta);
+          ny[a] = -eta * fx;
+        }
+        th += n * t_e;
+        d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nx[a] * y[a]; d4 += ny[a] * y[a];
+      }
+      const double jac = d1 * d4 - d2 * d3;
+      bad = jac < 0.0;
+#pragma unroll
+      for (int a = 0; a < 8; a++) {
+        sh.g[lane][a][0] = (nx[a] * d4 - ny[a] * d3) / jac;
+        sh.g[lane][a][1] = (ny[a] * d1 - nx[a] * d2) / jac;
+      }
+      sh.w[lane] = jac * (th * c_gw3[lane / 3] * c_gw3[lane % 3]);
+    }
+    if (__any_sync(0xffffffffu, bad)) {
+      if (lane == 0) atomicOr(err, 8u);
+      continue;
+    }
+    __syncwarp();
+    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+    const double c = E / (1.0 - nu * nu), d01 = c * nu, g3 = E / 2.0 / (1.0 + nu);
+    for (int blk = lane; blk < 64; blk += 32) {
+      const int a = blk >> 3, b = blk & 7;
+      double k00 = 0, k01 = 0, k10 = 0, k11 = 0;
+#pragma unroll
+      for (int gp = 0; gp < 9; gp++) {
+        const double ax = sh.g[gp][a][0], ay = sh.g[gp][a][1];
+        const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1];
+        const double w = sh.w[gp];
+        const double db00 = c * bx, db01 = d01 * by, db10 = d01 * bx, db11 = c * by, db20 = g3 * by, db21 = g3 * bx;
+        k00 += w * (ax * db00 + ay * db20);
+        k01 += w * (ax * db01 + ay * db21);
+        k10 += w * (ay * db10 + ax * db20);
+        k11 += w * (ay * db11 + ax * db21);
+      }
+      const int r0 = __ldg(cne + (int64_t)e * 16 + 2 * a), r1 = __ldg(cne + (int64_t)e * 16 + 2 * a + 1);
+      const int c0 = __ldg(cne + (int64_t)e * 16 + 2 * b), c1 = __ldg(cne + (int64_t)e * 16 + 2 * b + 1);
+      if (r0 >= 0) {
+        if (c0 >= 0) csr_add(rowptr, col, val, r0, c0, k00, err);
+        if (c1 >= 0) csr_add(rowptr, col, val, r0, c1, k01, err);
+      }
+      if (r1 >= 0) {
+        if (c0 >= 0) csr_add(rowptr, col, val, r1, c0, k10, err);
+        if (c1 >= 0) csr_add(rowptr, col, val, r1, c1, k11, err);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // tri3 plane stress, the constant-strain triangle (planeelemlt::stiffness_matrix,
 // MEFEL/SRC/plelemlt.cpp:234-272): det = twice the signed area, B from the
 // area-coordinate coefficients b_i = (y_j - y_k)/det, c_i = (x_k - x_j)/det
@@ -727,6 +993,24 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
                                                    c.rowptr.p, c.col.p, c.val.p, err.p);
         break;
       }
+      case 6: {
+        const int g6 = std::min((cnt + WPB20 - 1) / WPB20, kNumSMs * 8);
+        const size_t sm = WPB20 * sizeof(Hex20Shared);
+        if (ad.general) {
+          SGPU_CUDA(cudaFuncSetAttribute(k_hex20_elastic<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+          k_hex20_elastic<true><<<g6, TPB20, sm, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                      c.rowptr.p, c.col.p, c.val.p, err.p);
+        } else {
+          SGPU_CUDA(cudaFuncSetAttribute(k_hex20_elastic<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+          k_hex20_elastic<false><<<g6, TPB20, sm, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                       c.rowptr.p, c.col.p, c.val.p, err.p);
+        }
+        break;
+      }
+      case 7:
+        k_quad8_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,
+                                             c.rowptr.p, c.col.p, c.val.p, err.p);
+        break;
       case 5: {
         const int g5 = std::min((cnt + TPB - 1) / TPB, kNumSMs * 16);
         k_tri3_elastic<<<g5, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,
@@ -749,7 +1033,7 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
   SGPU_CUDA(cudaEventRecord(m->ev1, s));
   unsigned e = 0;
   SGPU_TRY(read_err(err.p, s, &e));
-  if (e & 8u) return fail(SGPU_BAD_INPUT, "tetrahedron of negative volume (wrong node numbering)");
+  if (e & 8u) return fail(SGPU_BAD_INPUT, "element of negative volume or Jacobian (wrong node numbering)");
   if (e) return fail(SGPU_BAD_INPUT, "element scatter found no CSR entry (bits " + std::to_string(e) + ")");
   float ms = 0.f;
   SGPU_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
@@ -778,6 +1062,8 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
     case SGPU_ELEM_QUAD4: nne = 4; ndofn = 2; break;
     case SGPU_ELEM_TET4: nne = 4; ndofn = 3; break;
     case SGPU_ELEM_TRI3: nne = 3; ndofn = 2; break;
+    case SGPU_ELEM_HEX20: nne = 20; ndofn = 3; break;
+    case SGPU_ELEM_QUAD8: nne = 8; ndofn = 2; break;
     case SGPU_ELEM_HEX8T_K:
     case SGPU_ELEM_HEX8T_C: nne = 8; ndofn = 1; break;
     default: return fail(SGPU_BAD_INPUT, "unknown element kind");
@@ -785,9 +1071,9 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   if (mesh->ndofn != ndofn) return fail(SGPU_BAD_INPUT, "ndofn does not match the element kind");
   if (mesh->nn <= 0 || mesh->ne <= 0 || !mesh->coords || !mesh->elems || !mesh->cn || (!mesh->emat && !mesh->dmat))
     return fail(SGPU_BAD_INPUT, "empty mesh");
-  if (mesh->dmat && kind != SGPU_ELEM_HEX8 && kind != SGPU_ELEM_TET4)
+  if (mesh->dmat && kind != SGPU_ELEM_HEX8 && kind != SGPU_ELEM_TET4 && kind != SGPU_ELEM_HEX20)
     return fail(SGPU_BAD_INPUT, "general material matrices are defined for the 3D elasticity kinds");
-  if ((kind == SGPU_ELEM_QUAD4 || kind == SGPU_ELEM_TRI3) && !mesh->thick)
+  if ((kind == SGPU_ELEM_QUAD4 || kind == SGPU_ELEM_TRI3 || kind == SGPU_ELEM_QUAD8) && !mesh->thick)
     return fail(SGPU_BAD_INPUT, "plane elements need thicknesses");
   if (mesh->ne > (1LL << 31) - 1) return fail(SGPU_BAD_INPUT, "too many elements");
   const int64_t nn = mesh->nn, ne = mesh->ne;

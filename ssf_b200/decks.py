@@ -14,7 +14,9 @@ The benchmark problems of this project are generated, never downloaded:
 * ``cantilever_tet``   -- the cantilever of ``cantilever_hex`` meshed with
   linear tetrahedra (six per grid cell);
 * ``plate_tri``        -- the plate of ``plate_quad`` meshed with
-  constant-strain triangles (two per quad).
+  constant-strain triangles (two per quad);
+* ``cantilever_hex20`` / ``plate_quad8`` -- the same problems with the
+  quadratic serendipity elements.
 
 ``write_mefel_deck`` writes a deck in SIFEL's positional (``-kwd`` absent)
 MEFEL input format, token order as read by ``probdesc::read``
@@ -333,6 +335,79 @@ def cantilever_tet(nx=20, ny=4, nz=4, L=1.0, B=0.2, H=0.2, E=210e9, nu=0.3,
     )
 
 
+# natural coordinates of the serendipity nodes in SIFEL's order
+# (bf_quad_hex_3d, GEFEL/basefun.cpp:2377; bf_quad_4_2d, :708)
+HEX20_NODES = np.array([[1, 1, 1], [-1, 1, 1], [-1, -1, 1], [1, -1, 1], [1, 1, -1], [-1, 1, -1], [-1, -1, -1],
+                        [1, -1, -1], [0, 1, 1], [-1, 0, 1], [0, -1, 1], [1, 0, 1], [1, 1, 0], [-1, 1, 0],
+                        [-1, -1, 0], [1, -1, 0], [0, 1, -1], [-1, 0, -1], [0, -1, -1], [1, 0, -1]])
+QUAD8_NODES = np.array([[1, 1], [-1, 1], [-1, -1], [1, -1], [0, 1], [-1, 0], [0, -1], [1, 0]])
+
+
+def cantilever_hex20(nx=10, ny=2, nz=2, L=1.0, B=0.2, H=0.2, E=210e9, nu=0.3, traction=1.0e6) -> Mesh:
+    """The cantilever of ``cantilever_hex`` with 20-node serendipity
+    hexahedra (quadhex, element type 103): grid corners plus one node in the
+    middle of every cell edge.  The end traction in -z goes to the 8 nodes of
+    every face quad as consistent forces: -1/12 of the quad's force at each
+    corner, 1/3 at each mid-side."""
+    mx, my, mz = 2 * nx + 1, 2 * ny + 1, 2 * nz + 1
+    I, J, K = np.meshgrid(np.arange(mx), np.arange(my), np.arange(mz), indexing="ij")
+    keep = ((I % 2) + (J % 2) + (K % 2)) <= 1  # no face or cell centres
+    lid = -np.ones((mx, my, mz), dtype=np.int64)
+    # node numbering x fastest, then y, then z (as the grid of cantilever_hex)
+    order = np.argsort((K * my + J) * mx + I, axis=None, kind="stable")
+    flat_keep = keep.ravel()[order]
+    lid.ravel()[order[flat_keep]] = np.arange(int(flat_keep.sum()))
+    pts = np.stack([I.ravel()[order[flat_keep]], J.ravel()[order[flat_keep]], K.ravel()[order[flat_keep]]], 1)
+    coords = pts * np.array([L / (2 * nx), B / (2 * ny), H / (2 * nz)])
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    elems = np.stack([lid[2 * i + 1 + p, 2 * j + 1 + q, 2 * k + 1 + r] for p, q, r in HEX20_NODES], axis=1)
+    nn = coords.shape[0]
+    dofflag = np.ones((nn, 3), dtype=np.int64)
+    dofflag[np.isclose(coords[:, 0], 0.0)] = 0
+    loads = np.zeros((1, nn, 3))
+    fq = traction * (B / ny) * (H / nz)
+    for kk in range(nz):
+        for jj in range(ny):
+            for dj in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    if dj == 0 and dk == 0:
+                        continue
+                    share = -1.0 / 12.0 if (dj != 0 and dk != 0) else 1.0 / 3.0
+                    loads[0, lid[2 * nx, 2 * jj + 1 + dj, 2 * kk + 1 + dk], 2] -= share * fq
+    return Mesh(kind="hex20", coords=coords, elems=elems.astype(np.int64), dofflag=dofflag,
+                emat=np.zeros(elems.shape[0], dtype=np.int64), mats=np.array([[E, nu]]), loads=loads,
+                meta=dict(nx=nx, ny=ny, nz=nz, L=L, B=B, H=H))
+
+
+def plate_quad8(nx, ny, Lx=None, Ly=None, E=1.0e10, nu=0.25, t=0.01, traction=1.0) -> Mesh:
+    """The plate of ``plate_quad`` with 8-node serendipity quads
+    (planeelemqq, element type 24); the right-edge traction goes to each
+    3-node edge as 1/6, 2/3, 1/6 of its force."""
+    Lx = float(nx) if Lx is None else Lx
+    Ly = float(ny) if Ly is None else Ly
+    mx, my = 2 * nx + 1, 2 * ny + 1
+    J, I = np.meshgrid(np.arange(my), np.arange(mx), indexing="ij")
+    keep = ((I % 2) + (J % 2)) <= 1
+    lid = -np.ones((my, mx), dtype=np.int64)
+    lid[keep] = np.arange(int(keep.sum()))
+    coords = np.stack([I[keep] * (Lx / (2 * nx)), J[keep] * (Ly / (2 * ny)), np.zeros(int(keep.sum()))], axis=1)
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    i, j = i.ravel(), j.ravel()
+    elems = np.stack([lid[2 * j + 1 + q, 2 * i + 1 + p] for p, q in QUAD8_NODES], axis=1)
+    nn = coords.shape[0]
+    dofflag = np.ones((nn, 2), dtype=np.int64)
+    dofflag[np.isclose(coords[:, 0], 0.0)] = 0
+    loads = np.zeros((1, nn, 2))
+    fe = traction * t * (Ly / ny)
+    for jj in range(ny):
+        for dj, share in ((-1, 1.0 / 6.0), (0, 2.0 / 3.0), (1, 1.0 / 6.0)):
+            loads[0, lid[2 * jj + 1 + dj, 2 * nx], 0] += share * fe
+    return Mesh(kind="quad8", coords=coords, elems=elems.astype(np.int64), dofflag=dofflag,
+                emat=np.zeros(elems.shape[0], dtype=np.int64), mats=np.array([[E, nu]]), loads=loads,
+                thick=np.full(elems.shape[0], t), meta=dict(nx=nx, ny=ny, Lx=Lx, Ly=Ly))
+
+
 def _fmt(v: float) -> str:
     return repr(float(v))
 
@@ -355,7 +430,7 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
     lines.append(f"20 {ni} {_fmt(res)} {iv}")
     lines.append(f"{precond}")
     lines.append(f"{mesh.nn}")
-    is2d = mesh.kind in ("quad4", "tri3")
+    is2d = mesh.kind in ("quad4", "tri3", "quad8")
     for i, (x, y, z) in enumerate(mesh.coords):
         lines.append(f"{i + 1} {_fmt(x)} {_fmt(y)} {_fmt(z)} {nd} 0 0")
     con = np.where((mesh.dofflag != 1).any(axis=1))[0]
@@ -367,15 +442,16 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
         ns = " ".join(str(int(v) + 1) for v in nodes)
         m = int(mesh.emat[e]) + 1
         if is2d:
-            # type planeelementlq (23) or planeelementlt (20), strastrestate
+            # type planeelementlt (20), planeelementlq (23) or
+            # planeelementqq (24), strastrestate
             # planestress (10), cne 0, crst csplanestr (10) with the
             # element's thickness set, one material
-            et = 20 if mesh.kind == "tri3" else 23
+            et = {"tri3": 20, "quad4": 23, "quad8": 24}[mesh.kind]
             lines.append(f"{e + 1} {et} 10 {ns} 0 10 {int(mesh.meta.get('tset', [0] * mesh.ne)[e]) + 1 if 'tset' in mesh.meta else 1} 1 1 {m}")
         else:
-            # type lineartet (100) or linearhex (102), cne 0, crst 0, one
-            # material elisomat (1)
-            et = 100 if mesh.kind == "tet4" else 102
+            # type lineartet (100), linearhex (102) or quadrhex (103), cne 0,
+            # crst 0, one material
+            et = {"tet4": 100, "hex8": 102, "hex20": 103}[mesh.kind]
             lines.append(f"{e + 1} {et} {ns} 0 0 1 {MATTYPE[mesh.mtype]} {m}")
     # materials: one type, mats.shape[0] instances: "id e nu" (elisomat = 1),
     # "id d11 .. d16 d22 .. d66" (elgmat3d = 2, elastgmat3d::read), or

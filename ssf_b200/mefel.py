@@ -22,7 +22,7 @@ from . import _lib as L
 from .gefel import DeviceMatrix, Result
 
 KIND = {"hex8": L.ELEM_HEX8, "quad4": L.ELEM_QUAD4, "hex8t_k": L.ELEM_HEX8T_K, "hex8t_c": L.ELEM_HEX8T_C,
-        "tet4": L.ELEM_TET4, "tri3": L.ELEM_TRI3}
+        "tet4": L.ELEM_TET4, "tri3": L.ELEM_TRI3, "hex20": L.ELEM_HEX20, "quad8": L.ELEM_QUAD8}
 
 
 def _c(a, dt):
@@ -89,7 +89,8 @@ def _assemble(mesh, kind: str, rho=None):
 
 
 def stiffness_matrix(mesh) -> DeviceMatrix:
-    """Global stiffness matrix of a hex8 / tet4 / quad4 / tri3 mesh, assembled on the GPU."""
+    """Global stiffness matrix of a hex8 / tet4 / hex20 / quad4 / tri3 / quad8
+    mesh, assembled on the GPU."""
     return _assemble(mesh, mesh.kind)
 
 

@@ -19,6 +19,9 @@ oracle/ref_harness_mefel.cpp / ref_harness_trfel.cpp:
                       coordinates, elements, K, f, u, ani, ares
   tri3_plate.npz      6x4 distorted plane-stress plate of constant-strain
                       triangles (planeelemlt, type 20), 2 materials: K, f, u
+  hex20_cantilever.npz, quad8_plate.npz
+                      the serendipity elements (quadhex, type 103;
+                      planeelemqq, type 24), distorted, 2 materials: K, f, u
   reference_iterations.json
                       iteration counts and solve times of full reference runs
                       on the benchmark cantilevers (used by bench.py to scale
@@ -26,7 +29,7 @@ oracle/ref_harness_mefel.cpp / ref_harness_trfel.cpp:
 
 Usage: python tests/golden/make_golden.py [--big] [--elements]   (--big adds
 the 1.01M-DOF run, about 2-3 minutes of CPU; --elements writes only the
-tet4 and tri3 fixtures)
+tet4, tri3, hex20 and quad8 fixtures)
 """
 from __future__ import annotations
 
@@ -78,11 +81,29 @@ def tri3_fixture():
                         ares=d["meta"]["ares_0"])
 
 
+def serendipity_fixtures():
+    h = decks.cantilever_hex20(4, 2, 2)
+    inner = ~np.isclose(h.coords[:, 0], 0.0)
+    h.coords[inner] += np.random.default_rng(15).uniform(-0.004, 0.004, (int(inner.sum()), 3))
+    q = decks.plate_quad8(5, 4, E=3.0e10, nu=0.22, t=0.02)
+    q.coords[:, :2] += np.random.default_rng(16).uniform(-0.1, 0.1, (q.nn, 2))
+    for m, name in ((h, "hex20_cantilever"), (q, "quad8_plate")):
+        m.emat = (np.arange(m.ne) % 2).astype(np.int64)
+        m.mats = np.array([[m.mats[0, 0], m.mats[0, 1]], [0.5 * m.mats[0, 0], 0.27]])
+        d = run(m, name)
+        extra = {"thick": m.thick} if m.thick is not None else {}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), coords=m.coords, elems=m.elems, emat=m.emat,
+                            mats=m.mats, dofflag=m.dofflag, loads=m.loads, adr=d["K_adr"], ci=d["K_ci"],
+                            a=d["K_a"], f=d["f"], u=d["u"], ani=d["meta"]["ani_0"], ares=d["meta"]["ares_0"],
+                            **extra)
+
+
 def main(big=False, elements_only=False):
     if not O.ref_available():
         raise SystemExit("build the reference first: python oracle/build_ref.py")
     tet4_fixture()
     tri3_fixture()
+    serendipity_fixtures()
     if elements_only:
         return
     out = {}

@@ -1,7 +1,8 @@
-"""Linear tetrahedra (lintet, MEFEL element type 100) and constant-strain
-triangles (planeelemlt, type 20): the oracle pinned to the compiled
-reference's fixtures, the elements' own invariants, the generated meshes, and
-the GPU assembly and solves against the oracle."""
+"""Linear tetrahedra (lintet, MEFEL element type 100), constant-strain
+triangles (planeelemlt, type 20), the serendipity hexahedron and quad
+(quadhex 103, planeelemqq 24) and general material matrices: the oracle
+pinned to the compiled reference's fixtures, the elements' own invariants,
+the generated meshes, and the GPU assembly and solves against the oracle."""
 import os
 
 import numpy as np
@@ -269,3 +270,119 @@ def test_orthotropic_cantilever_solve_matches_oracle(oracle, gpu_lib):
         x, r = K.pcg(f, res=1e-22, prec="agg", mode="mixed")
     assert r.status == L.OK
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+# ---------------------------------------------------------------------------
+# serendipity elements: hex20 (quadhex), quad8 (planeelemqq)
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("name,kind", [("hex20_cantilever", "hex20"), ("quad8_plate", "quad8")])
+def test_serendipity_golden(oracle, name, kind):
+    # the oracle's shape-function derivatives are written differently from
+    # the reference's, so K agrees to rounding, not bit for bit
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    m = _golden_mesh(g, kind)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    assert np.array_equal(adr, g["adr"]) and np.array_equal(ci, g["ci"])
+    assert np.abs(a - g["a"]).max() <= 1e-14 * np.abs(g["a"]).max()
+    f = oracle.load_vector(m)
+    assert np.array_equal(f, g["f"])
+    x, st, ani, ares = oracle.scr_cg_prec(g["adr"], g["ci"], g["a"], f, ni=20000, res=1e-20)
+    assert ani == int(g["ani"]) and np.array_equal(x, g["u"])
+
+
+def test_serendipity_element_invariants(oracle):
+    m = decks.cantilever_hex20(1, 1, 1, L=1.0, B=0.8, H=0.6)
+    xyz = m.coords[m.elems[0]] + np.random.default_rng(22).uniform(-0.03, 0.03, (20, 3))
+    ke = oracle.hex20_ke(xyz, 70e9, 0.33)
+    assert np.allclose(ke, ke.T, rtol=0, atol=1e-12 * np.abs(ke).max())
+    for i in range(3):
+        v = np.zeros((20, 3)); v[:, i] = 1.0
+        assert np.abs(ke @ v.ravel()).max() < 1e-9 * np.abs(ke).max()
+    for i, j in ((0, 1), (1, 2), (0, 2)):
+        v = np.zeros((20, 3)); v[:, i] = -xyz[:, j]; v[:, j] = xyz[:, i]
+        assert np.abs(ke @ v.ravel()).max() < 1e-9 * np.abs(ke).max()
+    assert np.linalg.matrix_rank(ke, tol=1e-9 * np.abs(ke).max()) == 54
+    q = decks.plate_quad8(1, 1, Lx=1.3, Ly=0.9)
+    xy = q.coords[q.elems[0], :2] + np.random.default_rng(23).uniform(-0.05, 0.05, (8, 2))
+    kq = oracle.quad8_ke(xy, 3e10, 0.22, 0.02)
+    assert np.allclose(kq, kq.T, rtol=0, atol=1e-12 * np.abs(kq).max())
+    assert np.linalg.matrix_rank(kq, tol=1e-9 * np.abs(kq).max()) == 13
+    # a reflected quad (negative Jacobian) is an error, as in the reference
+    with pytest.raises(ValueError):
+        oracle.quad8_ke(xy * np.array([-1.0, 1.0]), 3e10, 0.22, 0.02)
+
+
+def test_serendipity_meshes():
+    m = decks.cantilever_hex20(3, 2, 2)
+    assert m.nn == 4 * 3 * 3 + 3 * 3 * 3 + 4 * 2 * 3 + 4 * 3 * 2 and np.isclose(m.loads.sum(), -1.0e6 * 0.04)
+    assert (m.elems >= 0).all() and len(np.unique(m.elems)) == m.nn
+    q = decks.plate_quad8(4, 3)
+    assert q.nn == 5 * 4 + 4 * 4 + 5 * 3 and np.isclose(q.loads.sum(), 1.0 * 0.01 * 3.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,mtype", [("hex20", "iso"), ("hex20", "ortho"), ("quad8", "iso")])
+def test_serendipity_assembly_matches_oracle(oracle, gpu_lib, kind, mtype):
+    from ssf_b200 import mefel
+    rng = np.random.default_rng(10)
+    if kind == "hex20":
+        m = decks.cantilever_hex20(5, 3, 2)
+        m.coords = m.coords + rng.uniform(-0.004, 0.004, m.coords.shape)
+        if mtype == "ortho":
+            o = _ortho_mesh("hex8")
+            m.mtype, m.mats = "ortho", o.mats
+        else:
+            m.mats = np.array([[210e9, 0.3], [70e9, 0.25]])
+    else:
+        m = decks.plate_quad8(7, 5, E=3e10, nu=0.22)
+        m.coords[:, :2] += rng.uniform(-0.1, 0.1, (m.nn, 2))
+        m.mats = np.array([[3e10, 0.22], [7e10, 0.31]])
+        m.thick = rng.uniform(0.01, 0.03, m.ne)
+    m.emat = np.arange(m.ne) % 2
+    adr, ci, a = oracle.assemble(m, sym=True)
+    with mefel.stiffness_matrix(m) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
+    assert np.allclose(g_a, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kind", [("hex20_cantilever", "hex20"), ("quad8_plate", "quad8")])
+def test_serendipity_golden_on_device(gpu_lib, name, kind):
+    from ssf_b200 import mefel
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    with mefel.stiffness_matrix(_golden_mesh(g, kind)) as K:
+        g_adr, g_ci, g_a = K.download(symmetric=1)
+    assert np.array_equal(g_adr, g["adr"]) and np.array_equal(g_ci, g["ci"])
+    assert np.allclose(g_a, g["a"], rtol=1e-12, atol=1e-12 * np.abs(g["a"]).max())
+
+
+@pytest.mark.gpu
+def test_quad8_negative_jacobian_rejected_on_device(gpu_lib):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.plate_quad8(3, 2)
+    e = m.elems[2].copy()
+    m.elems[2] = e[[1, 0, 3, 2, 4, 7, 6, 5]]  # mirrored node order
+    with pytest.raises(L.SgpuError, match="negative"):
+        mefel.stiffness_matrix(m)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["hex20", "quad8"])
+def test_serendipity_solve_matches_oracle(oracle, gpu_lib, kind):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex20(16, 3, 3) if kind == "hex20" else decks.plate_quad8(40, 20, E=3e10, nu=0.22)
+    adr, ci, a = oracle.assemble(m, sym=True)
+    f = oracle.load_vector(m)
+    xo, st, ani_o, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26, zero=1e-300)
+    with mefel.stiffness_matrix(m) as K:
+        x, r = K.pcg(f, res=1e-22, zero=1e-300, prec="jacobi", mode="fp64")
+        assert r.status == L.OK
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+        K.set_nullspace(mefel.rigid_body_modes(m))
+        x, r = K.pcg(f, res=1e-22, zero=1e-300, prec="agg", mode="mixed")
+        assert r.status == L.OK
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8

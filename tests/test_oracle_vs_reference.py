@@ -116,6 +116,37 @@ def test_general_anisotropic_material_bit_exact(ref):
     _dump_and_compare(ref, m)
 
 
+@pytest.mark.parametrize("kind", ["hex20", "quad8"])
+def test_serendipity_elements_match_reference(ref, kind):
+    # quadhex (type 103, 3x3x3 Gauss) and planeelemqq (type 24, 3x3 Gauss):
+    # the oracle writes the serendipity derivatives from the corner and
+    # mid-edge formulas instead of the reference's per-node expressions, so
+    # the pin is to rounding (1e-13 of the largest entry), with the same
+    # pattern, loads and CG iteration count
+    if kind == "hex20":
+        m = decks.cantilever_hex20(5, 2, 2)
+        inner = ~np.isclose(m.coords[:, 0], 0.0)
+        m.coords[inner] += np.random.default_rng(46).uniform(-0.004, 0.004, (inner.sum(), 3))
+    else:
+        m = decks.plate_quad8(6, 4, E=3e10, nu=0.22, t=0.02)
+        m.coords[:, :2] += np.random.default_rng(47).uniform(-0.1, 0.1, (m.nn, 2))
+    m.emat = np.arange(m.ne) % 2
+    m.mats = np.array([[m.mats[0, 0], m.mats[0, 1]], [0.5 * m.mats[0, 0], 0.27]])
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    assert np.abs(a - d["K_a"]).max() <= 1e-13 * np.abs(d["K_a"]).max()
+    f = ref.load_vector(m)
+    assert np.allclose(f, d["f"][: f.size], rtol=1e-15, atol=0)
+    x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20, zero=1e-300)
+    xr, _, _, _ = ref.scr_cg_prec(d["K_adr"], d["K_ci"], d["K_a"], d["f"][: f.size], ni=20000, res=1e-20,
+                                  zero=1e-300)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
 def test_reference_solver_library_matches_oracle(ref):
     """libsifelref.so runs the reference's own symcomprow::cg_prec."""
     m = decks.cantilever_hex(10, 2, 2)
