@@ -62,7 +62,7 @@ WORKLOADS = {
     "cantilever_20x4x4": (20, 4, 4),
 }
 # the other benchmark configurations, one JSON line each when asked for
-EXTRA = ("cantilever_100x20x20_64rhs", "heat_cube_128_50steps", "plates_512")
+EXTRA = ("cantilever_100x20x20_64rhs", "heat_cube_128_50steps", "plates_512", "deck_cantilever_200x40x40")
 METRIC = "solve time to relative residual 1e-10 (fastest GPU form; mixed and FP64 forms all reported)"
 TOL = 1.0e-10
 # Iterations SIFEL's own Jacobi-PCG (symcomprow::cg_prec, SCR storage,
@@ -609,6 +609,72 @@ def run_extra(args, ws, rank):
                                    "sample": "the oracle's K and C integration and one step on this mesh, scaled "
                                              "to 50 steps that each integrate K, C and the lifting again as "
                                              "the reference does"}
+    elif args.workload == "deck_cantilever_200x40x40":
+        # SIFEL's whole linear-statics run from its input file: read the
+        # positional deck, number the DOFs, assemble K, solve, solution back
+        import tempfile
+        mesh = decks.cantilever_hex(200, 40, 40)
+        tdir = tempfile.mkdtemp(prefix="sgpu_deck_")
+        path = os.path.join(tdir, "cantilever_200x40x40.in")
+        decks.write_mefel_deck(mesh, path)  # res 1e-20 on (r.r)/(f.f), SCR, diagonal preconditioner
+        deck_bytes = os.path.getsize(path)
+        state = {}
+        timings = {}
+        clk = None
+        for name, (prec, mode) in {"agg_mixed": ("agg", "mixed"), "jacobi_fp64": (None, "fp64")}.items():
+            def run(prec=prec, mode=mode, name=name):
+                X, res, info = mefel.solve_deck(path, prec=prec, mode=mode)
+                state[name] = (res, info)
+                return X
+            if name == "agg_mixed":
+                clocks.start()
+            ms_f, outs, launches_f = _timed_calls(run, args.steps, args.warmup, ws)
+            if name == "agg_mixed":
+                clk = clocks.stop()
+            timings[name] = (ms_f, launches_f)
+        best = min(timings, key=lambda k: timings[k][0])
+        ms, launches = timings[best]
+        forms_out = {}
+        for name, (ms_f, _) in timings.items():
+            res, info = state[name]
+            forms_out[name] = {"ms_per_step": round(ms_f, 3), "parse_ms": round(info["parse_ms"], 3),
+                               "pattern_ms": round(info["assembly"]["pattern_ms"], 3),
+                               "integrate_ms": round(info["assembly"]["integrate_ms"], 3),
+                               "precond_setup_ms": round(res[0].info.get("precond_setup_ms", 0.0), 3),
+                               "device_solve_ms": round(res[0].info["solve_ms"], 3),
+                               "iterations": int(res[0].info["iterations"]),
+                               "true_relres": res[0].info["true_relres"],
+                               "converged": all(r.status == L.OK for r in res)}
+        out.update({"metric": "SIFEL linear-statics run from its input deck to relative residual 1e-10: read the "
+                              "34 MB positional deck, DOF numbering, assembly, solve, solution on the host "
+                              "(fastest form, wall clock)",
+                    "value": round(ms, 3), "ms_per_step": round(ms, 3), "form": best,
+                    "dtype": {"jacobi_fp64": "f64", "agg_mixed": "f64 iteration / f32 multilevel preconditioner"}[best],
+                    "scaling": "weak",
+                    "config": {"workload": args.workload, "n_equations": int(mesh.ndof), "deck_bytes": deck_bytes,
+                               "parallelism": "single GPU" if ws == 1 else f"{ws} independent replicas",
+                               "host_threads": os.cpu_count()},
+                    "forms": forms_out, "gpu_launches": int(launches), "clocks": clk})
+        if rank == 0 and ws == 1 and not args.no_cpu and O.ref_available():
+            # the reference's own front end on the same file: mefel_init and
+            # stiffness_matrix timed live by the harness, the solve by a
+            # 20-iteration sample of its cg_prec scaled to its full count
+            with tempfile.TemporaryDirectory() as od:
+                subprocess.run([os.path.join(ROOT, "oracle", "_ref", "mefel_dump"), path, od, "nosolve"],
+                               check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                dd = O.read_dump(od)
+            meta, adr, ci, a, f = dd["meta"], dd["K_adr"], dd["K_ci"], dd["K_a"], dd["f"]
+            ms_solve, cinfo = cpu_reference_time(adr, ci, a, f, "cantilever_200x40x40",
+                                                 sample_iters=args.cpu_sample_iters)
+            del dd, adr, ci, a
+            t_front = (float(meta["t_init"]) + float(meta["t_stiffness"]) + float(meta["t_rhs"])) * 1e3
+            out["cpu_baseline"] = {"value": round(t_front + ms_solve, 1), "unit": "ms", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": f"SIFEL's mefel_init + stiffness_matrix + right-hand side on this deck "
+                                             f"timed live ({t_front:.0f} ms), plus " + cinfo["sample"],
+                                   "front_end_ms": round(t_front, 1), "solve_ms": round(ms_solve, 1)}
+        os.remove(path)
+        os.rmdir(tdir)
     else:  # plates_512
         from ssf_b200 import shard
         all_plates = decks.plate_batch(512, seed=0)

@@ -182,6 +182,12 @@ SGPU_API int sgpu_matrix_pcg_d(sgpu_matrix m, double *x_d, const double *f_d, in
  * per equation of a node (translations only).  Setting it discards a built
  * hierarchy; new values (sgpu_matrix_update_values) do too. */
 SGPU_API int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B);
+/* The same near-null space built on the device from the mesh: the rigid-body
+ * motions of the centred node coordinates (coords nn x 3) in the equations
+ * the code numbers give (cn nn x ndofn, 1-based, <= 0 none): 6 vectors for
+ * ndofn 3, 3 for ndofn 2, the constant for ndofn 1.  No n x k host array. */
+SGPU_API int sgpu_matrix_set_rigid_body_modes(sgpu_matrix m, int64_t nn, int32_t ndofn, const double *coords,
+                                              const int64_t *cn);
 /* Discards the hierarchy of SGPU_PREC_AGG (the next such solve builds it
  * again); the near-null space is kept.  For timing set-up with the solve. */
 SGPU_API int sgpu_matrix_precond_clear(sgpu_matrix m);
@@ -361,6 +367,54 @@ SGPU_API int sgpu_csr_pcg_noalloc_d(int32_t n, const int32_t *rowptr_d, const in
                                     const double *val_d, const double *f_d, double *x_d, int64_t ni,
                                     double res, double zero, int64_t iv, void *stream, int64_t *ani,
                                     double *ares, int64_t *iterations);
+
+/* ------------------------------------------------------------------------ */
+/* Deck input (host)                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* A MEFEL linear-statics deck in SIFEL's positional format, read by all host
+ * threads.  Replaces the reading part of mefel_init (MEFEL/SRC/mefelinit.cpp:47:
+ * probdesc::read, mechtop::read, mechmat::read, mechcrsec::read,
+ * mechbclc::read) and gtopology::gencodnum (GEFEL/gtopology.cpp:1619) for the
+ * decks of the hot path: linear statics, one element type of the
+ * sgpu_elem_kind list, one material type (elisomat, elgmat3d, elortomat with
+ * constant axes), constraint codes 0/1, nodal loads.  Other decks fail with
+ * SGPU_BAD_INPUT naming the record or token. */
+typedef struct sgpu_deck_s *sgpu_deck;
+
+typedef struct {
+  int32_t kind;            /* sgpu_elem_kind */
+  int32_t ndofn, nne;      /* DOFs per node, nodes per element */
+  int32_t mtype;           /* material type: 1 elisomat, 2 elgmat3d, 3 elortomat */
+  int64_t nn, ne, n;       /* nodes, elements, equations */
+  int32_t nmat, nmatp;     /* material instances, parameters per instance (2, 21, 45) */
+  int32_t nlc;             /* load cases */
+  int32_t storage;         /* 10 compressed_rows, 11 symm_comp_rows */
+  int32_t precond;         /* 0 none, 1 diagonal */
+  int32_t iv;              /* initial-vector flag of the solver line */
+  int64_t ni;              /* iteration limit */
+  double res;              /* required residual */
+  double parse_ms;         /* wall time of sgpu_deck_read_mefel */
+  const double *coords;    /* nn x 3 */
+  const int64_t *elems;    /* ne x nne, 0-based */
+  const int64_t *dofflag;  /* nn x ndofn: 1 free, 0 fixed */
+  const int64_t *cn;       /* nn x ndofn code numbers (1-based, 0 fixed) */
+  const int64_t *emat_id;  /* ne material instances (0-based) */
+  const double *mats;      /* nmat x nmatp as read */
+  const double *thick;     /* ne (plane kinds) or NULL */
+  const double *loads;     /* nlc x nn x ndofn nodal forces */
+} sgpu_deck_view;
+
+/* threads <= 0: all hardware threads (at most 64). */
+SGPU_API int sgpu_deck_read_mefel(const char *path, int32_t threads, sgpu_deck *out);
+/* Arrays of the deck (owned by it, valid until sgpu_deck_free). */
+SGPU_API int sgpu_deck_get(sgpu_deck d, sgpu_deck_view *view);
+/* The deck as an sgpu_assemble input (pointers into the deck). */
+SGPU_API int sgpu_deck_mesh(sgpu_deck d, sgpu_mesh *mesh);
+/* Nodal loads of load case lc in equation order, f[n]
+ * (mefel_right_hand_side, MEFEL/SRC/globmat.cpp:2369, for nodal forces). */
+SGPU_API int sgpu_deck_rhs(sgpu_deck d, int32_t lc, double *f);
+SGPU_API void sgpu_deck_free(sgpu_deck d);
 
 /* ------------------------------------------------------------------------ */
 /* Library state                                                            */

@@ -78,6 +78,18 @@ class AssemblyInfo(C.Structure):
 ELEM_HEX8, ELEM_QUAD4, ELEM_HEX8T_K, ELEM_HEX8T_C, ELEM_TET4, ELEM_TRI3, ELEM_HEX20, ELEM_QUAD8 = range(8)
 
 
+class DeckView(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("ndofn", C.c_int32), ("nne", C.c_int32), ("mtype", C.c_int32),
+        ("nn", C.c_int64), ("ne", C.c_int64), ("n", C.c_int64),
+        ("nmat", C.c_int32), ("nmatp", C.c_int32), ("nlc", C.c_int32), ("storage", C.c_int32),
+        ("precond", C.c_int32), ("iv", C.c_int32), ("ni", C.c_int64), ("res", C.c_double),
+        ("parse_ms", C.c_double),
+        ("coords", C.c_void_p), ("elems", C.c_void_p), ("dofflag", C.c_void_p), ("cn", C.c_void_p),
+        ("emat_id", C.c_void_p), ("mats", C.c_void_p), ("thick", C.c_void_p), ("loads", C.c_void_p),
+    ]
+
+
 class SgpuError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
@@ -112,6 +124,7 @@ SIGNATURES = {
     "sgpu_matrix_set_spmv": ([_vp, _i32, _i32, _i32], C.c_int),
     "sgpu_matrix_set_nullspace": ([_vp, _i32, _pD], C.c_int),
     "sgpu_matrix_precond_clear": ([_vp], C.c_int),
+    "sgpu_matrix_set_rigid_body_modes": ([_vp, _i64, _i32, _vp, _vp], C.c_int),
     "sgpu_csr_pcg_noalloc_d": ([_i32, _vp, _vp, _vp, _vp, _vp, _i64, _dbl, _dbl, _i64, _vp, C.POINTER(_i64),
                                 C.POINTER(_dbl), C.POINTER(_i64)], C.c_int),
     "sgpu_assembly_lift": ([_vp, _pD, _pD], C.c_int),
@@ -130,6 +143,11 @@ SIGNATURES = {
                                C.POINTER(SolveInfo)], C.c_int),
     "sgpu_assemble": ([C.POINTER(Mesh), C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_reassemble": ([_vp, _i32, _vp, _vp, C.POINTER(AssemblyInfo)], C.c_int),
+    "sgpu_deck_read_mefel": ([C.c_char_p, _i32, C.POINTER(_vp)], C.c_int),
+    "sgpu_deck_get": ([_vp, C.POINTER(DeckView)], C.c_int),
+    "sgpu_deck_mesh": ([_vp, C.POINTER(Mesh)], C.c_int),
+    "sgpu_deck_rhs": ([_vp, _i32, _pD], C.c_int),
+    "sgpu_deck_free": ([_vp], None),
     "sgpu_last_error": ([], C.c_char_p),
     "sgpu_version": ([], C.c_char_p),
     "sgpu_kernel_launches": ([], C.c_int64),

@@ -1331,6 +1331,68 @@ void amg_values_changed(sgpu_matrix m) {
   if (m->amg) m->amg->clear();
 }
 
+namespace {
+// the rigid-body motions of node i in its equations, B column after column
+// (B[eq + q n], the layout of sgpu_matrix_set_nullspace): the translations,
+// then the rotations about z, x, y of the centred coordinates (the vectors
+// aggregator::gener_rbm_1/2, GEFEL/aggregator.cpp:638-700, builds per
+// aggregate); plane problems: 2 translations and the rotation; scalar
+// problems: the constant
+__global__ void k_rigid_body_modes(int64_t nn, int ndofn, int k, const double *__restrict__ xyz,
+                                   const int64_t *__restrict__ cn, double cx, double cy, double cz,
+                                   double *__restrict__ B, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const double x = xyz[3 * i] - cx, y = xyz[3 * i + 1] - cy, z = xyz[3 * i + 2] - cz;
+  for (int c = 0; c < ndofn; c++) {
+    const int64_t eq = cn[i * ndofn + c];
+    if (eq <= 0 || eq > n) continue;
+    double *b = B + (eq - 1);
+    if (ndofn == 1) {
+      b[0] = 1.0;
+    } else if (ndofn == 2) {
+      b[0] = c == 0 ? 1.0 : 0.0;
+      b[n] = c == 1 ? 1.0 : 0.0;
+      b[2 * n] = c == 0 ? -y : x;
+    } else {
+      b[0] = c == 0 ? 1.0 : 0.0;
+      b[n] = c == 1 ? 1.0 : 0.0;
+      b[2 * n] = c == 2 ? 1.0 : 0.0;
+      b[3 * n] = c == 0 ? -y : (c == 1 ? x : 0.0);  // about z
+      b[4 * n] = c == 1 ? -z : (c == 2 ? y : 0.0);  // about x
+      b[5 * n] = c == 0 ? z : (c == 2 ? -x : 0.0);  // about y
+    }
+  }
+}
+}  // namespace
+
+int amg_set_rigid_body_modes(sgpu_matrix m, int64_t nn, int ndofn, const double *coords_h, const int64_t *cn_h) {
+  amg_stream = m->stream;
+  if (!m->amg) m->amg = new Amg();
+  Amg &A = *m->amg;
+  A.clear();
+  const int k = ndofn == 1 ? 1 : (ndofn == 2 ? 3 : 6);
+  A.k0 = k;
+  double c[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = 0; i < nn; i++)
+    for (int q = 0; q < 3; q++) c[q] += coords_h[3 * i + q];
+  for (int q = 0; q < 3; q++) c[q] /= (double)nn;
+  SGPU_TRY(A.B0.alloc((size_t)m->n * k));
+  PBuf<double> xyz;
+  PBuf<int64_t> cn;
+  SGPU_TRY(xyz.alloc((size_t)nn * 3));
+  SGPU_TRY(cn.alloc((size_t)nn * ndofn));
+  SGPU_CUDA(cudaMemcpyAsync(xyz.p, coords_h, (size_t)nn * 3 * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+  SGPU_CUDA(cudaMemcpyAsync(cn.p, cn_h, (size_t)nn * ndofn * sizeof(int64_t), cudaMemcpyHostToDevice, m->stream));
+  SGPU_CUDA(cudaMemsetAsync(A.B0.p, 0, (size_t)m->n * k * sizeof(double), m->stream));
+  k_rigid_body_modes<<<(unsigned)((nn + 255) / 256), 256, 0, m->stream>>>(nn, ndofn, k, xyz.p, cn.p, c[0], c[1],
+                                                                           c[2], A.B0.p, m->n);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  SGPU_CUDA(cudaStreamSynchronize(m->stream));
+  return SGPU_OK;
+}
+
 int amg_set_nullspace(sgpu_matrix m, int k, const double *B_host) {
   amg_stream = m->stream;
   if (!m->amg) m->amg = new Amg();

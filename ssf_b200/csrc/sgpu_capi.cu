@@ -241,6 +241,14 @@ int sgpu_matrix_set_nullspace(sgpu_matrix m, int32_t k, const double *B) {
   return amg_set_nullspace(m, k, B);
 }
 
+int sgpu_matrix_set_rigid_body_modes(sgpu_matrix m, int64_t nn, int32_t ndofn, const double *coords,
+                                     const int64_t *cn) {
+  if (!m) return fail(SGPU_BAD_INPUT, "null handle");
+  if (!coords || !cn || nn <= 0) return fail(SGPU_BAD_INPUT, "empty node arrays");
+  if (ndofn < 1 || ndofn > 3) return fail(SGPU_BAD_INPUT, "ndofn must be 1, 2 or 3");
+  return amg_set_rigid_body_modes(m, nn, ndofn, coords, cn);
+}
+
 int sgpu_matrix_pcg_batch_agg(sgpu_matrix m, int32_t nsys, const int64_t *sys_rows, double *x, const double *f,
                               int64_t ni, double res, double zero, int32_t mode, int64_t *ani, double *ares,
                               int32_t *status, int64_t *iterations, sgpu_solve_info *info) {

@@ -180,6 +180,7 @@ int spmv_plan(sgpu_matrix m, int precision, double *bytes, int *format, int *var
 // sgpu_amg.cu
 void amg_values_changed(sgpu_matrix m);
 int amg_set_nullspace(sgpu_matrix m, int k, const double *B_host);
+int amg_set_rigid_body_modes(sgpu_matrix m, int64_t nn, int ndofn, const double *coords_h, const int64_t *cn_h);
 int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int crit, int mode,
                 int64_t *ani, double *ares, sgpu_solve_info *info);
 int amg_batch_run(sgpu_matrix m, int nsys, const int64_t *sys_rows, double *x, const double *f, int64_t ni,

@@ -201,6 +201,14 @@ class DeviceMatrix:
         cols = np.ascontiguousarray(B.T)  # column after column
         L.check(L.lib().sgpu_matrix_set_nullspace(self.h, cols.shape[0], cols.ravel()))
 
+    def set_rigid_body_modes(self, coords, cn):
+        """The rigid-body near-null space built on the device from node
+        coordinates (nn x 3) and code numbers (nn x ndofn)."""
+        xyz = np.ascontiguousarray(coords, dtype=np.float64)
+        c = np.ascontiguousarray(cn, dtype=np.int64)
+        L.check(L.lib().sgpu_matrix_set_rigid_body_modes(self.h, xyz.shape[0], c.shape[1], xyz.ctypes.data,
+                                                         c.ctypes.data))
+
     def precond_clear(self):
         """Discard the aggregation hierarchy (rebuilt by the next solve)."""
         L.check(L.lib().sgpu_matrix_precond_clear(self.h))

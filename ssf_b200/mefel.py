@@ -172,6 +172,103 @@ def solve_linear_statics(mesh, ni=100000, res=1e-20, mode="fp64", batched=None):
     return np.stack(out), results
 
 
+class Deck:
+    """A MEFEL linear-statics deck read by the library's parallel reader
+    (``sgpu_deck_read_mefel``: the reading part of mefel_init,
+    MEFEL/SRC/mefelinit.cpp:47, and gtopology::gencodnum)."""
+
+    def __init__(self, path: str, threads: int = 0):
+        self.h = C.c_void_p()
+        L.check(L.lib().sgpu_deck_read_mefel(str(path).encode(), int(threads), C.byref(self.h)))
+        v = L.DeckView()
+        L.check(L.lib().sgpu_deck_get(self.h, C.byref(v)))
+        self.view = v
+        self.info = {k: getattr(v, k) for k in ("kind", "ndofn", "nne", "mtype", "nn", "ne", "n", "nmat", "nlc",
+                                                "storage", "precond", "iv", "ni", "res", "parse_ms")}
+
+    def _arr(self, ptr, shape, dt):
+        n = int(np.prod(shape))
+        ctype = C.c_double if dt == np.float64 else C.c_int64
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,)).reshape(shape).copy()
+
+    def mesh(self):
+        """The deck as a :class:`ssf_b200.decks.Mesh` (copies)."""
+        from .decks import Mesh
+        v = self.view
+        kinds = {L.ELEM_HEX8: "hex8", L.ELEM_QUAD4: "quad4", L.ELEM_TET4: "tet4", L.ELEM_TRI3: "tri3",
+                 L.ELEM_HEX20: "hex20", L.ELEM_QUAD8: "quad8"}
+        return Mesh(kind=kinds[v.kind], coords=self._arr(v.coords, (v.nn, 3), np.float64),
+                    elems=self._arr(v.elems, (v.ne, v.nne), np.int64),
+                    dofflag=self._arr(v.dofflag, (v.nn, v.ndofn), np.int64),
+                    emat=self._arr(v.emat_id, (v.ne,), np.int64),
+                    mats=self._arr(v.mats, (v.nmat, v.nmatp), np.float64),
+                    loads=self._arr(v.loads, (v.nlc, v.nn, v.ndofn), np.float64),
+                    thick=self._arr(v.thick, (v.ne,), np.float64) if v.thick else None,
+                    mtype={1: "iso", 2: "gen3d", 3: "ortho"}[v.mtype])
+
+    def stiffness_matrix(self) -> DeviceMatrix:
+        """sgpu_assemble straight from the deck's arrays."""
+        m = L.Mesh()
+        L.check(L.lib().sgpu_deck_mesh(self.h, C.byref(m)))
+        h = C.c_void_p()
+        info = L.AssemblyInfo()
+        L.check(L.lib().sgpu_assemble(C.byref(m), C.byref(h), C.byref(info)))
+        dm = DeviceMatrix.from_handle(h, info.n, 1)
+        dm.assembly = info.as_dict()
+        return dm
+
+    def rhs(self, lc: int = 0) -> np.ndarray:
+        f = np.zeros(self.view.n)
+        L.check(L.lib().sgpu_deck_rhs(self.h, int(lc), f))
+        return f
+
+    def close(self):
+        if self.h:
+            L.lib().sgpu_deck_free(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_deck(path: str, prec=None, mode="fp64", threads: int = 0, nullspace: bool = True):
+    """What SIFEL's ``mefel deck.in`` does for linear statics, on the GPU:
+    read the deck, assemble K, solve every load case with the deck's solver
+    line (ni, res, diagonal or no preconditioner, the storage's criterion).
+    ``prec`` "agg" swaps in the aggregation preconditioner (with the rigid-body
+    modes when ``nullspace``).  Returns (X (nlc x n), results, info)."""
+    import time
+    t0 = time.perf_counter()
+    with Deck(path, threads) as d:
+        info = dict(d.info)
+        K = d.stiffness_matrix()
+        try:
+            info["assembly"] = K.assembly
+            crit = "scr" if d.info["storage"] == 11 else "cr"
+            p = prec if prec is not None else d.info["precond"]
+            if p == "agg" and nullspace:
+                v = d.view
+                L.check(L.lib().sgpu_matrix_set_rigid_body_modes(K.h, v.nn, v.ndofn, v.coords, v.cn))
+            out, results = [], []
+            for lc in range(d.info["nlc"]):
+                x, r = K.pcg(d.rhs(lc), ni=d.info["ni"], res=d.info["res"], crit=crit, prec=p, mode=mode)
+                out.append(x)
+                results.append(r)
+        finally:
+            K.close()
+    info["wall_s"] = time.perf_counter() - t0
+    return np.stack(out), results, info
+
+
 def trfel_lift(K: DeviceMatrix, rnode) -> np.ndarray:
     """Right-hand side of TRFEL's assemble_init for time-constant prescribed
     values: -sum_e K_e r_e at the free DOFs (TRFEL/SRC/globmatt.cpp:1635)."""

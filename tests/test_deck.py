@@ -1,0 +1,165 @@
+"""The library's parallel reader of MEFEL positional decks (sgpu_deck_read_mefel):
+decks written by ssf_b200.decks come back array for array, the reader agrees
+with the reference's own reading (the compiled reference assembles the same
+K from the same file), unsupported decks fail naming the record, and on the
+GPU a deck runs end to end to the oracle's solution.  The reader is host
+code: the CPU tests call no GPU work."""
+import os
+
+import numpy as np
+import pytest
+
+from ssf_b200 import decks
+
+KINDS = {
+    "hex8": lambda: decks.cantilever_hex(5, 2, 2),
+    "tet4": lambda: decks.cantilever_tet(3, 2, 2),
+    "hex20": lambda: decks.cantilever_hex20(3, 2, 2),
+    "quad4": lambda: decks.plate_quad(4, 3),
+    "tri3": lambda: decks.plate_tri(4, 3),
+    "quad8": lambda: decks.plate_quad8(4, 3),
+}
+
+
+def _ortho(m):
+    Dl = decks.orthotropic_local(150e9, 10e9, 9e9, 0.3, 0.28, 0.45, 3.5e9, 5e9, 5.5e9)
+    m.mtype = "ortho"
+    m.mats = np.array([np.concatenate([Dl.ravel(), decks.rotation(a).ravel()]) for a in ((0, 0, 0), (0.3, -0.5, 0.9))])
+    m.emat = np.arange(m.ne) % 2
+    return m
+
+
+def _variants():
+    for k, make in KINDS.items():
+        yield k, make
+    yield "hex8_ortho", lambda: _ortho(decks.cantilever_hex(4, 2, 2))
+    yield "tet4_gen3d", lambda: _gen3d(decks.cantilever_tet(3, 2, 2))
+    yield "hex8_loadcases", lambda: decks.cantilever_top_loads(decks.cantilever_hex(6, 2, 2), 7, seed=2)
+    yield "quad4_tsets", lambda: _tsets(decks.plate_quad(5, 4))
+
+
+def _gen3d(m):
+    Dl = decks.orthotropic_local(150e9, 10e9, 9e9, 0.3, 0.28, 0.45, 3.5e9, 5e9, 5.5e9)
+    m.mtype = "gen3d"
+    m.mats = np.array([Dl[np.triu_indices(6)]])
+    return m
+
+
+def _tsets(m):
+    m.meta["tvals"] = [0.01, 0.03]
+    m.meta["tset"] = list(np.arange(m.ne) % 2)
+    m.thick = np.array([0.01, 0.03])[np.arange(m.ne) % 2]
+    m.mats = np.array([[1e10, 0.25], [3e10, 0.2]])
+    m.emat = (np.arange(m.ne) // 3) % 2
+    return m
+
+
+@pytest.mark.parametrize("name,make", list(_variants()))
+def test_round_trip(tmp_path, name, make):
+    from ssf_b200 import mefel
+    m = make()
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    with mefel.Deck(p, threads=3) as d:
+        r = d.mesh()
+        assert d.info["n"] == m.ndof and d.info["nlc"] == m.loads.shape[0]
+        for lc in range(m.loads.shape[0]):
+            assert np.array_equal(d.rhs(lc), mefel.mefel_right_hand_side(m, lc))
+    assert r.kind == m.kind and r.mtype == m.mtype
+    for k in ("coords", "elems", "dofflag", "emat", "loads"):
+        assert np.array_equal(getattr(r, k), getattr(m, k)), k
+    assert np.array_equal(r.mats, np.asarray(m.mats, dtype=np.float64))
+    if m.thick is not None:
+        assert np.array_equal(r.thick, m.thick)
+    assert np.array_equal(r.code_numbers(), m.code_numbers())
+
+
+def test_records_in_any_order(tmp_path):
+    # node and element records may come in any id order, as the reference
+    # indexes them by id
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex(4, 2, 2)
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    lines = open(p).read().split("\n")
+    i0 = 10  # first node record
+    nodes = lines[i0:i0 + m.nn]
+    rng = np.random.default_rng(1)
+    lines[i0:i0 + m.nn] = [nodes[k] for k in rng.permutation(m.nn)]
+    ncon = int(lines[i0 + m.nn])
+    e0 = i0 + m.nn + 1 + ncon + 1
+    el = lines[e0:e0 + m.ne]
+    lines[e0:e0 + m.ne] = [el[k] for k in rng.permutation(m.ne)]
+    open(p, "w").write("\n".join(lines))
+    with mefel.Deck(p) as d:
+        r = d.mesh()
+    assert np.array_equal(r.coords, m.coords) and np.array_equal(r.elems, m.elems)
+
+
+@pytest.mark.parametrize("edit,match", [
+    (lambda L: L.__setitem__(2, "2"), "problemtype"),
+    (lambda L: L.__setitem__(10, L[10].replace(" 3 0 0", " 3 1 0")), "node record 1"),
+    (lambda L: L.__setitem__(11, L[10]), "node record"),
+    (lambda L: L.__setitem__(-1, "oops"), "integer expected"),
+    (lambda L: L.append("7"), "unexpected token"),
+])
+def test_unsupported_or_broken_decks_fail(tmp_path, edit, match):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex(3, 2, 2)
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    lines = open(p).read().rstrip("\n").split("\n")
+    edit(lines)
+    open(p, "w").write("\n".join(lines) + "\n")
+    with pytest.raises(L.SgpuError, match=match):
+        mefel.Deck(p)
+
+
+def test_missing_file_fails(tmp_path):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    with pytest.raises(L.SgpuError, match="cannot open"):
+        mefel.Deck(str(tmp_path / "absent.in"))
+
+
+@pytest.mark.parametrize("name", ["hex8", "tet4", "quad8", "hex8_ortho"])
+def test_reader_agrees_with_the_reference_reading(oracle, tmp_path, name):
+    # the compiled reference reads the same file: its K is the oracle's K of
+    # the mesh this reader returns, bit for bit
+    from ssf_b200 import mefel
+    if not oracle.ref_available():
+        pytest.skip("compiled reference (oracle/_ref) not built")
+    m = dict(_variants())[name]()
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    d = oracle.run_mefel_dump(p, str(tmp_path), solve=False)
+    with mefel.Deck(p) as dk:
+        r = dk.mesh()
+        f = dk.rhs(0)
+    adr, ci, a = oracle.assemble(r, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    if name == "quad8":
+        assert np.abs(a - d["K_a"]).max() <= 1e-14 * np.abs(d["K_a"]).max()
+    else:
+        assert np.array_equal(a, d["K_a"])
+    assert np.array_equal(f, d["f"][: f.size])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,prec", [("hex8", None), ("tet4", None), ("hex8_ortho", "agg"),
+                                       ("hex8_loadcases", None)])
+def test_deck_end_to_end(oracle, gpu_lib, tmp_path, name, prec):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = dict(_variants())[name]()
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p, res=1e-22)
+    X, results, info = mefel.solve_deck(p, prec=prec, mode="fp64")
+    adr, ci, a = oracle.assemble(m, sym=True)
+    for lc in range(m.loads.shape[0]):
+        f = oracle.load_vector(m, lc)
+        xo, st, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+        assert results[lc].status == L.OK
+        assert np.linalg.norm(X[lc] - xo) / np.linalg.norm(xo) <= 1e-8
+    assert info["n"] == m.ndof and info["parse_ms"] > 0.0

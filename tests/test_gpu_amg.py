@@ -162,3 +162,22 @@ def test_smoothed_bottom_level(oracle, gpu_lib, monkeypatch):
         X, res = gefel.pcg_multi(dm, np.stack([f, 2.0 * f], axis=1), res=1e-22, prec="agg", mode="mixed")
         assert all(rr.status == L.OK for rr in res)
         assert np.linalg.norm(X[:, 1] - 2.0 * xo) / np.linalg.norm(2.0 * xo) <= 1e-8
+
+
+@pytest.mark.parametrize("which", ["hex", "plate"])
+def test_rigid_body_modes_built_on_device(oracle, gpu_lib, which):
+    # sgpu_matrix_set_rigid_body_modes (coordinates and code numbers in, the
+    # vectors formed on the device) preconditions like the host-built modes
+    m = decks.cantilever_hex(24, 6, 6) if which == "hex" else decks.plate_quad(48, 24, E=3e10, nu=0.22)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x1, r1 = dm.pcg(f, res=1e-22, prec="agg", mode="mixed")
+        dm.set_rigid_body_modes(m.coords, m.code_numbers())
+        x2, r2 = dm.pcg(f, res=1e-22, prec="agg", mode="mixed")
+    assert r1.status == L.OK and r2.status == L.OK
+    assert abs(r1.info["iterations"] - r2.info["iterations"]) <= 1
+    for x in (x1, x2):
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
