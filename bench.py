@@ -62,7 +62,8 @@ WORKLOADS = {
     "cantilever_20x4x4": (20, 4, 4),
 }
 # the other benchmark configurations, one JSON line each when asked for
-EXTRA = ("cantilever_100x20x20_64rhs", "heat_cube_128_50steps", "plates_512", "deck_cantilever_200x40x40")
+EXTRA = ("cantilever_100x20x20_64rhs", "heat_cube_128_50steps", "plates_512", "deck_cantilever_200x40x40",
+         "deck_heat_cube_128_50steps")
 METRIC = "solve time to relative residual 1e-10 (fastest GPU form; mixed and FP64 forms all reported)"
 TOL = 1.0e-10
 # Iterations SIFEL's own Jacobi-PCG (symcomprow::cg_prec, SCR storage,
@@ -675,6 +676,76 @@ def run_extra(args, ws, rank):
                                    "front_end_ms": round(t_front, 1), "solve_ms": round(ms_solve, 1)}
         import shutil
         shutil.rmtree(tdir, ignore_errors=True)  # the deck and the reference's log beside it
+    elif args.workload == "deck_heat_cube_128_50steps":
+        # SIFEL's whole transient heat run from its input file: read the
+        # 370 MB TRFEL deck (2.1M element and material records), assemble K
+        # and C, lift, 50 implicit-Euler steps, temperatures on the host
+        import shutil
+        import tempfile
+        mesh = decks.heat_cube(128, seed=1234)
+        tdir = tempfile.mkdtemp(prefix="sgpu_deck_")
+        path = os.path.join(tdir, "heat_cube_128.in")
+        decks.write_trfel_deck(mesh, path, dt=10.0, nsteps=50)
+        deck_bytes = os.path.getsize(path)
+        state = {}
+        timings = {}
+        clk = None
+        for name, (prec, mode) in {"jacobi_fp64": ("jacobi", "fp64"), "agg_mixed": ("agg", "mixed")}.items():
+            def run(prec=prec, mode=mode, name=name):
+                d, v, its, info = mefel.solve_trfel_deck(path, prec=prec, mode=mode)
+                state[name] = (its, info)
+                return d
+            if name == "jacobi_fp64":
+                clocks.start()
+            ms_f, outs, launches_f = _timed_calls(run, args.steps, args.warmup, ws)
+            if name == "jacobi_fp64":
+                clk = clocks.stop()
+            timings[name] = (ms_f, launches_f)
+        best = min(timings, key=lambda k: timings[k][0])
+        ms, launches = timings[best]
+        forms_out = {}
+        for name, (ms_f, _) in timings.items():
+            its, info = state[name]
+            forms_out[name] = {"ms_per_step": round(ms_f, 3), "parse_ms": round(info["parse_ms"], 3),
+                               "pattern_ms": round(info["assembly"]["pattern_ms"], 3),
+                               "integrate_ms": round(info["assembly"]["integrate_ms"], 3),
+                               "device_solve_ms": round(info["solve"]["solve_ms"], 3),
+                               "iterations_total": int(its.sum()), "steps": int(info["nsteps"])}
+        out.update({"metric": "SIFEL transient heat run from its input deck: read the 370 MB TRFEL deck, "
+                              "assemble K and C, lift, 50 implicit-Euler steps each to (r.r)/(f.f) < 1e-20, "
+                              "temperatures on the host (fastest form, wall clock)",
+                    "value": round(ms, 3), "ms_per_step": round(ms, 3), "form": best,
+                    "dtype": {"jacobi_fp64": "f64", "agg_mixed": "f64 iteration / f32 multilevel preconditioner"}[best],
+                    "scaling": "weak",
+                    "config": {"workload": args.workload, "n_equations": int(mesh.ndof), "elements": int(mesh.ne),
+                               "deck_bytes": deck_bytes, "dt_s": 10.0, "steps": 50,
+                               "parallelism": "single GPU" if ws == 1 else f"{ws} independent replicas",
+                               "host_threads": os.cpu_count()},
+                    "forms": forms_out, "gpu_launches": int(launches), "clocks": clk})
+        shutil.rmtree(tdir, ignore_errors=True)
+        if rank == 0 and ws == 1 and not args.no_cpu and O.ref_available():
+            # the reference's trfel_init + K + C on a 64^3 deck of the same
+            # kind (1/8 of the elements), timed live and scaled by elements;
+            # its 50 steps from the oracle's one-step sample as in the
+            # heat_cube_128_50steps line
+            small = decks.heat_cube(64, seed=1234)
+            with tempfile.TemporaryDirectory() as od:
+                sp = os.path.join(od, "h64.in")
+                decks.write_trfel_deck(small, sp, dt=10.0, nsteps=1)
+                subprocess.run([os.path.join(ROOT, "oracle", "_ref", "trfel_dump"), sp, od, "nosolve"],
+                               check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                meta = O.read_dump(od)["meta"]
+            scale = mesh.ne / small.ne
+            t_front = (float(meta["t_init"]) + float(meta["t_conductivity"]) + float(meta["t_capacity"])) * 1e3 * scale
+            t0 = time.perf_counter()
+            O.trfel_steps(small, 1, 10.0, iv=1, ni=100000)
+            t_step = (time.perf_counter() - t0) * 1e3 * scale * 2.0  # one step; iterations grow ~2x at 128^3
+            out["cpu_baseline"] = {"value": round(t_front + 50 * t_step, 1), "unit": "ms", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": "SIFEL's trfel_init + conductivity and capacity matrices on a 64^3 deck "
+                                             "timed live and scaled by elements (8x), plus 50 steps from one "
+                                             "oracle step on 64^3 scaled by elements and 2x iterations",
+                                   "front_end_ms": round(t_front, 1)}
     else:  # plates_512
         from ssf_b200 import shard
         all_plates = decks.plate_batch(512, seed=0)

@@ -402,17 +402,33 @@ typedef struct {
   const int64_t *emat_id;  /* ne material instances (0-based) */
   const double *mats;      /* nmat x nmatp as read */
   const double *thick;     /* ne (plane kinds) or NULL */
-  const double *loads;     /* nlc x nn x ndofn nodal forces */
+  const double *loads;     /* nlc x nn x ndofn nodal forces (MEFEL) */
+  /* TRFEL decks (sgpu_deck_read_trfel) */
+  int32_t problem;         /* 1 linear statics (MEFEL), 50 stationary, 60 nonstationary (TRFEL) */
+  int32_t tform;           /* nonstationary solver: 1 trapezoidd (d-form), 2 trapezoidv (v-form) */
+  double alpha, t0, t1, dt;/* trapezoid parameter, start and end time, constant time step */
+  const double *rnode;     /* nn nodal values of the lifting: prescribed values on prescribed
+                              nodes, initial values on free ones (prescvalues) */
+  const double *rho;       /* ne densities of the elements' cross sections */
 } sgpu_deck_view;
 
 /* threads <= 0: all hardware threads (at most 64). */
 SGPU_API int sgpu_deck_read_mefel(const char *path, int32_t threads, sgpu_deck *out);
+/* A TRFEL linear heat-conduction deck (the reading part of trfel_init,
+ * TRFEL/SRC/trfelinit.cpp:24): stationary (50) or nonstationary (60, d- or
+ * v-form trapezoid with a fixed time step), linear hexahedra (linhext, 225),
+ * isotropic materials (isotransmat "c k", one instance per element allowed),
+ * crsec3dt densities, constant prescribed values, initial values.
+ * sgpu_deck_mesh gives the conduction kind (set kind SGPU_ELEM_HEX8T_C for the
+ * capacity matrix); the right-hand side is sgpu_assembly_lift of view.rnode. */
+SGPU_API int sgpu_deck_read_trfel(const char *path, int32_t threads, sgpu_deck *out);
 /* Arrays of the deck (owned by it, valid until sgpu_deck_free). */
 SGPU_API int sgpu_deck_get(sgpu_deck d, sgpu_deck_view *view);
 /* The deck as an sgpu_assemble input (pointers into the deck). */
 SGPU_API int sgpu_deck_mesh(sgpu_deck d, sgpu_mesh *mesh);
 /* Nodal loads of load case lc in equation order, f[n]
- * (mefel_right_hand_side, MEFEL/SRC/globmat.cpp:2369, for nodal forces). */
+ * (mefel_right_hand_side, MEFEL/SRC/globmat.cpp:2369, for nodal forces);
+ * MEFEL decks only. */
 SGPU_API int sgpu_deck_rhs(sgpu_deck d, int32_t lc, double *f);
 SGPU_API void sgpu_deck_free(sgpu_deck d);
 

@@ -87,6 +87,8 @@ class DeckView(C.Structure):
         ("parse_ms", C.c_double),
         ("coords", C.c_void_p), ("elems", C.c_void_p), ("dofflag", C.c_void_p), ("cn", C.c_void_p),
         ("emat_id", C.c_void_p), ("mats", C.c_void_p), ("thick", C.c_void_p), ("loads", C.c_void_p),
+        ("problem", C.c_int32), ("tform", C.c_int32), ("alpha", C.c_double), ("t0", C.c_double),
+        ("t1", C.c_double), ("dt", C.c_double), ("rnode", C.c_void_p), ("rho", C.c_void_p),
     ]
 
 
@@ -144,6 +146,7 @@ SIGNATURES = {
     "sgpu_assemble": ([C.POINTER(Mesh), C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_reassemble": ([_vp, _i32, _vp, _vp, C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_deck_read_mefel": ([C.c_char_p, _i32, C.POINTER(_vp)], C.c_int),
+    "sgpu_deck_read_trfel": ([C.c_char_p, _i32, C.POINTER(_vp)], C.c_int),
     "sgpu_deck_get": ([_vp, C.POINTER(DeckView)], C.c_int),
     "sgpu_deck_mesh": ([_vp, C.POINTER(Mesh)], C.c_int),
     "sgpu_deck_rhs": ([_vp, _i32, _pD], C.c_int),

@@ -36,10 +36,15 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <unistd.h>
 
 #include "sgpu_internal.cuh"
 
@@ -66,9 +71,44 @@ void parallel_for(int64_t n, int threads, F &&f) {
 
 }  // namespace
 
+// an array whose resize leaves the memory uninitialised (the file buffer and
+// the token table are hundreds of MB on large decks: a zero fill on one
+// thread would cost more than reading and tokenising them on all)
+template <class T>
+struct RawArray {
+  std::unique_ptr<T[]> p;
+  size_t n = 0;
+  void resize(size_t count) {
+    p.reset(count ? new T[count] : nullptr);
+    n = count;
+  }
+  void clear() {
+    p.reset();
+    n = 0;
+  }
+  T *data() { return p.get(); }
+  const T *data() const { return p.get(); }
+  size_t size() const { return n; }
+  T &operator[](size_t i) { return p[i]; }
+  const T &operator[](size_t i) const { return p[i]; }
+};
+
+// phase times on stderr when SGPU_DECK_TIMING is set
+struct PhaseClock {
+  bool on = std::getenv("SGPU_DECK_TIMING") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char *what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "deck: %-12s %8.1f ms\n", what, std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
+
 struct DeckData {
-  std::vector<char> buf;
-  std::vector<int64_t> tok;  // start offset of every token after the title line
+  PhaseClock clk;
+  RawArray<char> buf;
+  RawArray<int64_t> tok;  // start offset of every token after the title line
   int threads = 1;
   // header
   int32_t storage = 0, solver = 0, iv = 0, precond = 0;
@@ -81,6 +121,11 @@ struct DeckData {
   std::vector<double> coords, mats, thick, loads, emat2, dmat;
   std::vector<int64_t> elems, dofflag, cn, emat_id;
   double parse_ms = 0.0;
+  // TRFEL
+  int32_t problem = 1;  // 1 linear statics (MEFEL); 50 stationary, 60 nonstationary (TRFEL)
+  int32_t tform = 0;    // nonstationary solver: 1 trapezoidd, 2 trapezoidv
+  double alpha = 0.0, t0 = 0.0, t1 = 0.0, dt = 0.0;
+  std::vector<double> rnode, rho;  // nodal values of the lifting; per-element density
 
   // token access ------------------------------------------------------------
   const char *at(int64_t t) const { return buf.data() + tok[(size_t)t]; }
@@ -231,11 +276,12 @@ int64_t parallel_records(const DeckData &d, int64_t base, int64_t count, int64_t
   return v == INT64_MAX ? -1 : v;
 }
 
-int parse(DeckData &d) {
+int parse_mefel(DeckData &d) {
   // the title is the first line (probdesc::read reads it whole)
   size_t start = 0;
   while (start < d.buf.size() && d.buf[start] != '\n') start++;
   SGPU_TRY(tokenize(d, start));
+  d.clk.mark("tokenize");
   Cursor c{d};
   // --- problem description (probdesc::read, positional) ---
   c.i();                                // mespr
@@ -475,6 +521,260 @@ int parse(DeckData &d) {
   return SGPU_OK;
 }
 
+// TRFEL linear heat conduction with linear hexahedra (linhext, element type
+// 225), as trfel_init (TRFEL/SRC/trfelinit.cpp:24) reads it: probdesct::read
+// (TRFEL/SRC/probdesct.cpp:177-560, timecontr::read GEFEL/timecontr.cpp:70),
+// transtop::read (transtop.cpp:93), elementt::read (elementt.cpp:72),
+// transmat::read (isotrmat "c k", isotrmat.cpp:444), transcrsec::read
+// (transcrsec.cpp:33, one crsec3dt density), transbclc::read / loadcaset::read
+// (loadcaset.cpp:133, pvalt::read pvalt.cpp:24) and lhsrhst::initcond
+// (lhsrhst.cpp:157).  Every element may carry its own material instance (the
+// heterogeneous cube has one per element), so the material records are
+// converted by all threads too.
+int parse_trfel(DeckData &d) {
+  size_t start = 0;
+  while (start < d.buf.size() && d.buf[start] != '\n') start++;
+  SGPU_TRY(tokenize(d, start));
+  d.clk.mark("tokenize");
+  Cursor c{d};
+  c.i();  // mesprt
+  d.problem = (int32_t)c.i();
+  if (d.problem != 50 && d.problem != 60 && c.err.empty())
+    c.err = "problem type " + std::to_string(d.problem) + " is not supported";
+  c.expect(1, "transmatter (one medium)");
+  c.expect(1, "medium (heat)");
+  c.f();  // scale
+  for (int k = 0; k < 11; k++) c.expect(0, "optional computation flag");
+  if (d.problem == 50) {
+    d.storage = (int32_t)c.i();
+  } else {
+    d.tform = (int32_t)c.i();
+    if (d.tform != 1 && d.tform != 2 && c.err.empty()) c.err = "nonstationary solver " + std::to_string(d.tform) + " is not supported";
+    d.alpha = c.f();
+    c.expect(0, "time control type (fixed)");
+    d.t0 = c.f();
+    d.t1 = c.f();
+    const int64_t nit = c.i();
+    if (nit < 0 && c.err.empty()) c.err = "generated important times are not supported";
+    for (int64_t k = 0; k < nit; k++) c.f();
+    c.expect(0, "time step function (constant)");
+    d.dt = c.f();
+    c.i();  // timetypeprint
+    c.expect(0, "hdbackup");
+    d.storage = (int32_t)c.i();
+    c.expect(d.storage, "capacity storage (as the conductivity's)");
+  }
+  if (d.storage != 11 && d.storage != 10 && c.err.empty()) c.err = "storage " + std::to_string(d.storage) + " is not supported";
+  d.solver = (int32_t)c.i();
+  if (d.solver != 20 && c.err.empty()) c.err = "linear solver " + std::to_string(d.solver) + " is not supported";
+  d.ni = c.i();
+  d.res = c.f();
+  d.iv = (int32_t)c.i();
+  d.precond = (int32_t)c.i();
+  if (d.problem == 60) c.expect(0, "capacity diagonalization");
+  if (!c.err.empty()) return fail(SGPU_BAD_INPUT, "deck: " + c.err);
+
+  // nodes: "id x y z ndofn crst" with one DOF and no cross section
+  d.ndofn = 1;
+  d.nn = c.i();
+  if (!c.err.empty() || d.nn <= 0) return fail(SGPU_BAD_INPUT, "deck: bad node count");
+  d.coords.assign((size_t)d.nn * 3, 0.0);
+  std::vector<std::atomic<uint8_t>> seen((size_t)d.nn);
+  for (auto &q : seen) q.store(0, std::memory_order_relaxed);
+  int64_t bad = parallel_records(d, c.t, d.nn, 6, [&](int64_t, int64_t t, bool &ok) {
+    int64_t id = 0, nd = 0, crst = 0;
+    ok = d.geti(t, id) && id >= 1 && id <= d.nn && d.geti(t + 4, nd) && nd == 1 && d.geti(t + 5, crst) && crst == 0;
+    if (!ok) return;
+    double *x = &d.coords[(size_t)(id - 1) * 3];
+    ok = d.getd(t + 1, x[0]) && d.getd(t + 2, x[1]) && d.getd(t + 3, x[2]) && seen[(size_t)(id - 1)].exchange(1) == 0;
+  });
+  if (bad >= 0) return fail(SGPU_BAD_INPUT, "deck: node record " + std::to_string(bad + 1) + " is not 'id x y z 1 0'");
+  c.t += d.nn * 6;
+  d.clk.mark("nodes");
+
+  // constraints: "id code", code < 0 the prescribed value -code, 1 free
+  d.dofflag.assign((size_t)d.nn, 1);
+  std::vector<int64_t> pv_of((size_t)d.nn, 0);
+  const int64_t ncn = c.i();
+  if (!c.err.empty() || ncn < 0 || ncn > d.nn) return fail(SGPU_BAD_INPUT, "deck: bad constraint count");
+  bad = parallel_records(d, c.t, ncn, 2, [&](int64_t, int64_t t, bool &ok) {
+    int64_t id = 0, code = 0;
+    ok = d.geti(t, id) && id >= 1 && id <= d.nn && d.geti(t + 1, code) && (code < 0 || code == 1);
+    if (ok && code < 0) {
+      d.dofflag[(size_t)(id - 1)] = 0;
+      pv_of[(size_t)(id - 1)] = -code;
+    }
+  });
+  if (bad >= 0)
+    return fail(SGPU_BAD_INPUT, "deck: constraint record " + std::to_string(bad + 1) +
+                                    " is not 'id code' with a prescribed-value index (< 0) or 1");
+  c.t += ncn * 2;
+
+  // elements: "id 225 n1..n8 cne crst idcs tm idm"
+  d.kind = SGPU_ELEM_HEX8T_K;
+  d.nne = 8;
+  d.ne = c.i();
+  if (!c.err.empty() || d.ne <= 0 || d.ne > (1LL << 31) - 1) return fail(SGPU_BAD_INPUT, "deck: bad element count");
+  d.elems.assign((size_t)d.ne * 8, 0);
+  d.emat_id.assign((size_t)d.ne, 0);
+  std::vector<int64_t> cs_of((size_t)d.ne, 0);
+  std::vector<std::atomic<uint8_t>> eseen((size_t)d.ne);
+  for (auto &q : eseen) q.store(0, std::memory_order_relaxed);
+  bad = parallel_records(d, c.t, d.ne, 15, [&](int64_t, int64_t t, bool &ok) {
+    int64_t id = 0, type = 0, v = 0;
+    ok = d.geti(t, id) && id >= 1 && id <= d.ne && d.geti(t + 1, type) && type == 225;
+    if (!ok) return;
+    const size_t e = (size_t)(id - 1);
+    for (int a = 0; ok && a < 8; a++) {
+      ok = d.geti(t + 2 + a, v) && v >= 1 && v <= d.nn;
+      if (ok) d.elems[e * 8 + a] = v - 1;
+    }
+    ok = ok && d.geti(t + 10, v) && v == 0 && d.geti(t + 11, v) && v == 3 && d.geti(t + 12, v) && v >= 1;
+    if (ok) cs_of[e] = v - 1;
+    ok = ok && d.geti(t + 13, v) && v == 100 && d.geti(t + 14, v) && v >= 1;
+    if (ok) d.emat_id[e] = v - 1;
+    ok = ok && eseen[e].exchange(1) == 0;
+  });
+  if (bad >= 0)
+    return fail(SGPU_BAD_INPUT, "deck: element record " + std::to_string(bad + 1) +
+                                    " is not 'id 225 n1..n8 0 3 cs 100 mat' or repeats an id");
+  c.t += d.ne * 15;
+  d.clk.mark("elements");
+
+  // materials: one type isotransmat (100), instances "id c k"
+  c.expect(1, "number of material types");
+  c.expect(100, "material type (isotransmat)");
+  d.nmat = (int32_t)c.i();
+  if (!c.err.empty() || d.nmat <= 0) return fail(SGPU_BAD_INPUT, "deck: " + (c.err.empty() ? std::string("no materials") : c.err));
+  d.mtype = 100;
+  d.nmatp = 2;
+  d.mats.assign((size_t)d.nmat * 2, 0.0);  // (k, c) per instance
+  std::vector<std::atomic<uint8_t>> mseen((size_t)d.nmat);
+  for (auto &q : mseen) q.store(0, std::memory_order_relaxed);
+  bad = parallel_records(d, c.t, d.nmat, 3, [&](int64_t, int64_t t, bool &ok) {
+    int64_t id = 0;
+    double cc = 0.0, kk = 0.0;
+    ok = d.geti(t, id) && id >= 1 && id <= d.nmat && d.getd(t + 1, cc) && d.getd(t + 2, kk) &&
+         mseen[(size_t)(id - 1)].exchange(1) == 0;
+    if (ok) {
+      d.mats[(size_t)(id - 1) * 2] = kk;
+      d.mats[(size_t)(id - 1) * 2 + 1] = cc;
+    }
+  });
+  if (bad >= 0) return fail(SGPU_BAD_INPUT, "deck: material record " + std::to_string(bad + 1) + " is not 'id c k'");
+  c.t += (int64_t)d.nmat * 3;
+  d.clk.mark("materials");
+
+  // cross sections: one type crsec3dt (3), instances "id rho"
+  c.expect(1, "number of cross-section types");
+  c.expect(3, "cross-section type (crsec3dt)");
+  const int64_t ncs = c.i();
+  std::vector<double> rho_cs((size_t)std::max<int64_t>(ncs, 0), 0.0);
+  for (int64_t k = 0; k < ncs && c.err.empty(); k++) {
+    const int64_t id = c.i();
+    if (id < 1 || id > ncs) c.err = "cross section out of range";
+    else rho_cs[(size_t)(id - 1)] = c.f();
+  }
+  if (!c.err.empty()) return fail(SGPU_BAD_INPUT, "deck: " + c.err);
+
+  // one load case: prescribed values, nothing else
+  c.expect(1, "number of load cases");
+  const int64_t npv = c.i();
+  std::vector<double> pv((size_t)std::max<int64_t>(npv, 0), 0.0);
+  for (int64_t k = 0; k < npv && c.err.empty(); k++) {
+    c.f();  // initial prescribed value
+    if (d.problem == 60) c.expect(0, "prescribed-value function (constant)");
+    pv[(size_t)k] = c.f();
+  }
+  for (int k = 0; k < 6; k++) c.expect(0, "sources / element loads / nodal values / climatic conditions / functions");
+  c.expect(0, "boundary fluxes");
+  if (!c.err.empty()) return fail(SGPU_BAD_INPUT, "deck: " + c.err);
+  // initial values (nonstationary): "id value" for every node
+  std::vector<double> init((size_t)d.nn, 0.0);
+  if (d.problem == 60) {
+    bad = parallel_records(d, c.t, d.nn, 2, [&](int64_t, int64_t t, bool &ok) {
+      int64_t id = 0;
+      double v = 0.0;
+      ok = d.geti(t, id) && id >= 1 && id <= d.nn && d.getd(t + 1, v);
+      if (ok) init[(size_t)(id - 1)] = v;
+    });
+    if (bad >= 0) return fail(SGPU_BAD_INPUT, "deck: initial-value record " + std::to_string(bad + 1));
+    c.t += d.nn * 2;
+  }
+  d.clk.mark("initial");
+  c.expect(0, "text output");
+  c.expect(0, "graphic output");
+  if (d.problem == 60) c.expect(0, "diagnostics");
+  if (c.err.empty() && c.t != (int64_t)d.tok.size()) c.err = "unexpected token " + std::to_string(c.t) + " after the deck";
+  if (!c.err.empty()) return fail(SGPU_BAD_INPUT, "deck: " + c.err);
+
+  // validate indices, then: code numbers, per-element (k, c) rows and
+  // density, the nodal values of the lifting (prescribed values on
+  // prescribed nodes, initial values on free ones: prescvalues,
+  // TRFEL/SRC/globmatt.cpp:1057)
+  for (int64_t e = 0; e < d.ne; e++)
+    if (d.emat_id[(size_t)e] >= d.nmat || cs_of[(size_t)e] >= ncs)
+      return fail(SGPU_BAD_INPUT, "deck: element " + std::to_string(e + 1) + " names a missing material or cross section");
+  d.rnode.assign((size_t)d.nn, 0.0);
+  for (int64_t i = 0; i < d.nn; i++) {
+    const int64_t k = pv_of[(size_t)i];
+    if (k > npv) return fail(SGPU_BAD_INPUT, "deck: prescribed-value index out of range");
+    d.rnode[(size_t)i] = k > 0 ? pv[(size_t)(k - 1)] : init[(size_t)i];
+  }
+  d.cn.assign((size_t)d.nn, 0);
+  int64_t next = 0;
+  for (int64_t i = 0; i < d.nn; i++)
+    if (d.dofflag[(size_t)i] == 1) d.cn[(size_t)i] = ++next;
+  d.n = next;
+  if (d.n == 0) return fail(SGPU_BAD_INPUT, "deck: no free DOFs");
+  d.emat2.resize((size_t)d.ne * 2);
+  d.rho.resize((size_t)d.ne);
+  parallel_for(d.ne, d.threads, [&](int64_t b, int64_t e) {
+    for (int64_t k = b; k < e; k++) {
+      const double *row = &d.mats[(size_t)d.emat_id[(size_t)k] * 2];
+      d.emat2[(size_t)k * 2] = row[0];
+      d.emat2[(size_t)k * 2 + 1] = row[1];
+      d.rho[(size_t)k] = rho_cs[(size_t)cs_of[(size_t)k]];
+    }
+  });
+  d.nlc = 1;
+  return SGPU_OK;
+}
+
+// reads the file with all threads (pread of one chunk each)
+int read_file(const char *path, DeckData &d) {
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(SGPU_BAD_INPUT, std::string("cannot open deck ") + path);
+  std::fseek(f, 0, SEEK_END);
+  const long size = std::ftell(f);
+  std::fclose(f);
+  if (size <= 0) return fail(SGPU_BAD_INPUT, std::string("empty deck ") + path);
+  d.buf.resize((size_t)size);
+  const int fd = ::open(path, O_RDONLY);
+  if (fd < 0) return fail(SGPU_BAD_INPUT, std::string("cannot open deck ") + path);
+  std::atomic<bool> ok{true};
+  const int parts = std::max(1, std::min(d.threads, (int)(size / (1 << 22)) + 1));
+  std::vector<std::thread> pool;
+  for (int p = 0; p < parts; p++)
+    pool.emplace_back([&, p] {
+      size_t b = (size_t)size * p / parts, e = (size_t)size * (p + 1) / parts;
+      while (b < e) {
+        const ssize_t got = ::pread(fd, d.buf.data() + b, e - b, (off_t)b);
+        if (got <= 0) {
+          ok = false;
+          return;
+        }
+        b += (size_t)got;
+      }
+    });
+  for (auto &th : pool) th.join();
+  ::close(fd);
+  if (!ok) return fail(SGPU_BAD_INPUT, std::string("cannot read deck ") + path);
+  return SGPU_OK;
+}
+
+int read_deck(const char *path, int32_t threads, bool trfel, sgpu_deck_s **out);
+
 }  // namespace
 }  // namespace sgpu
 
@@ -484,42 +784,40 @@ struct sgpu_deck_s {
   DeckData d;
 };
 
-extern "C" {
-
-SGPU_API int sgpu_deck_read_mefel(const char *path, int32_t threads, sgpu_deck *out) {
+namespace sgpu {
+namespace {
+int read_deck(const char *path, int32_t threads, bool trfel, sgpu_deck_s **out) {
   if (!path || !out) return fail(SGPU_BAD_INPUT, "null argument");
   *out = nullptr;
   const auto t0 = std::chrono::steady_clock::now();
   auto *h = new sgpu_deck_s();
   DeckData &d = h->d;
   d.threads = threads > 0 ? threads : (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
-  FILE *f = std::fopen(path, "rb");
-  if (!f) {
-    delete h;
-    return fail(SGPU_BAD_INPUT, std::string("cannot open deck ") + path);
-  }
-  std::fseek(f, 0, SEEK_END);
-  const long size = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
-  d.buf.resize(size > 0 ? (size_t)size : 0);
-  const size_t got = size > 0 ? std::fread(d.buf.data(), 1, (size_t)size, f) : 0;
-  std::fclose(f);
-  if (size <= 0 || got != (size_t)size) {
-    delete h;
-    return fail(SGPU_BAD_INPUT, std::string("cannot read deck ") + path);
-  }
-  const int st = parse(d);
+  int st = read_file(path, d);
+  d.clk.mark("read");
+  if (st == SGPU_OK) st = trfel ? parse_trfel(d) : parse_mefel(d);
+  d.clk.mark("sections");
   if (st != SGPU_OK) {
     delete h;
     return st;
   }
   d.tok.clear();
-  d.tok.shrink_to_fit();
   d.buf.clear();
-  d.buf.shrink_to_fit();
   d.parse_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   *out = h;
   return SGPU_OK;
+}
+}  // namespace
+}  // namespace sgpu
+
+extern "C" {
+
+SGPU_API int sgpu_deck_read_mefel(const char *path, int32_t threads, sgpu_deck *out) {
+  return sgpu::read_deck(path, threads, false, out);
+}
+
+SGPU_API int sgpu_deck_read_trfel(const char *path, int32_t threads, sgpu_deck *out) {
+  return sgpu::read_deck(path, threads, true, out);
 }
 
 SGPU_API int sgpu_deck_get(sgpu_deck h, sgpu_deck_view *v) {
@@ -542,6 +840,14 @@ SGPU_API int sgpu_deck_get(sgpu_deck h, sgpu_deck_view *v) {
   v->ni = d.ni;
   v->res = d.res;
   v->parse_ms = d.parse_ms;
+  v->problem = d.problem;
+  v->tform = d.tform;
+  v->alpha = d.alpha;
+  v->t0 = d.t0;
+  v->t1 = d.t1;
+  v->dt = d.dt;
+  v->rnode = d.rnode.empty() ? nullptr : d.rnode.data();
+  v->rho = d.rho.empty() ? nullptr : d.rho.data();
   v->coords = d.coords.data();
   v->elems = d.elems.data();
   v->dofflag = d.dofflag.data();
@@ -566,7 +872,7 @@ SGPU_API int sgpu_deck_mesh(sgpu_deck h, sgpu_mesh *mesh) {
   mesh->cn = d.cn.data();
   mesh->emat = d.emat2.empty() ? nullptr : d.emat2.data();
   mesh->thick = d.thick.empty() ? nullptr : d.thick.data();
-  mesh->rho = nullptr;
+  mesh->rho = d.rho.empty() ? nullptr : d.rho.data();
   mesh->dmat = d.dmat.empty() ? nullptr : d.dmat.data();
   return SGPU_OK;
 }
@@ -574,6 +880,8 @@ SGPU_API int sgpu_deck_mesh(sgpu_deck h, sgpu_mesh *mesh) {
 SGPU_API int sgpu_deck_rhs(sgpu_deck h, int32_t lc, double *f) {
   if (!h || !f) return fail(SGPU_BAD_INPUT, "null argument");
   const DeckData &d = h->d;
+  if (d.problem != 1)
+    return fail(SGPU_BAD_INPUT, "a TRFEL deck's right-hand side is the lifting of rnode (sgpu_assembly_lift)");
   if (lc < 0 || lc >= d.nlc) return fail(SGPU_BAD_INPUT, "load case out of range");
   std::memset(f, 0, (size_t)d.n * sizeof(double));
   const double *L = &d.loads[(size_t)lc * d.nn * d.ndofn];

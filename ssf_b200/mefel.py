@@ -177,14 +177,17 @@ class Deck:
     (``sgpu_deck_read_mefel``: the reading part of mefel_init,
     MEFEL/SRC/mefelinit.cpp:47, and gtopology::gencodnum)."""
 
-    def __init__(self, path: str, threads: int = 0):
+    def __init__(self, path: str, threads: int = 0, front: str = "mefel"):
         self.h = C.c_void_p()
-        L.check(L.lib().sgpu_deck_read_mefel(str(path).encode(), int(threads), C.byref(self.h)))
+        read = {"mefel": L.lib().sgpu_deck_read_mefel, "trfel": L.lib().sgpu_deck_read_trfel}[front]
+        L.check(read(str(path).encode(), int(threads), C.byref(self.h)))
         v = L.DeckView()
         L.check(L.lib().sgpu_deck_get(self.h, C.byref(v)))
         self.view = v
+        self.front = front
         self.info = {k: getattr(v, k) for k in ("kind", "ndofn", "nne", "mtype", "nn", "ne", "n", "nmat", "nlc",
-                                                "storage", "precond", "iv", "ni", "res", "parse_ms")}
+                                                "storage", "precond", "iv", "ni", "res", "parse_ms", "problem",
+                                                "tform", "alpha", "t0", "t1", "dt")}
 
     def _arr(self, ptr, shape, dt):
         n = int(np.prod(shape))
@@ -195,6 +198,15 @@ class Deck:
         """The deck as a :class:`ssf_b200.decks.Mesh` (copies)."""
         from .decks import Mesh
         v = self.view
+        if self.front == "trfel":
+            rnode = self._arr(v.rnode, (v.nn,), np.float64)
+            dofflag = self._arr(v.dofflag, (v.nn, 1), np.int64)
+            presc = np.where(dofflag[:, 0] == 1, 0.0, rnode)[:, None]
+            return Mesh(kind="hex8t", coords=self._arr(v.coords, (v.nn, 3), np.float64),
+                        elems=self._arr(v.elems, (v.ne, 8), np.int64), dofflag=dofflag,
+                        emat=self._arr(v.emat_id, (v.ne,), np.int64),
+                        mats=self._arr(v.mats, (v.nmat, 2), np.float64), loads=np.zeros((1, v.nn, 1)),
+                        meta=dict(prescribed=presc, rnode=rnode, rho=self._arr(v.rho, (v.ne,), np.float64)))
         kinds = {L.ELEM_HEX8: "hex8", L.ELEM_QUAD4: "quad4", L.ELEM_TET4: "tet4", L.ELEM_TRI3: "tri3",
                  L.ELEM_HEX20: "hex20", L.ELEM_QUAD8: "quad8"}
         return Mesh(kind=kinds[v.kind], coords=self._arr(v.coords, (v.nn, 3), np.float64),
@@ -206,10 +218,13 @@ class Deck:
                     thick=self._arr(v.thick, (v.ne,), np.float64) if v.thick else None,
                     mtype={1: "iso", 2: "gen3d", 3: "ortho"}[v.mtype])
 
-    def stiffness_matrix(self) -> DeviceMatrix:
-        """sgpu_assemble straight from the deck's arrays."""
+    def stiffness_matrix(self, kind=None) -> DeviceMatrix:
+        """sgpu_assemble straight from the deck's arrays (TRFEL decks: the
+        conductivity matrix, or the capacity matrix for kind "hex8t_c")."""
         m = L.Mesh()
         L.check(L.lib().sgpu_deck_mesh(self.h, C.byref(m)))
+        if kind is not None:
+            m.kind = KIND[kind]
         h = C.c_void_p()
         info = L.AssemblyInfo()
         L.check(L.lib().sgpu_assemble(C.byref(m), C.byref(h), C.byref(info)))
@@ -267,6 +282,52 @@ def solve_deck(path: str, prec=None, mode="fp64", threads: int = 0, nullspace: b
             K.close()
     info["wall_s"] = time.perf_counter() - t0
     return np.stack(out), results, info
+
+
+def solve_trfel_deck(path: str, prec="jacobi", mode="fp64", threads: int = 0, zero: float = 1e-30):
+    """What SIFEL's ``trfel deck.in`` does for linear heat conduction, on the
+    GPU: read the deck, assemble K (and C), lift the prescribed values, then
+    the stationary solve (solve_stationary_problem, TRFEL/SRC/spsolvert.cpp:13)
+    or every time step of the d- or v-form trapezoid the deck names
+    (npsolvert.cpp:1071 / :62).  Returns (d, v, per-step iterations, info)."""
+    import time
+    t0 = time.perf_counter()
+    with Deck(path, threads, front="trfel") as dk:
+        info = dict(dk.info)
+        v = dk.view
+        K = dk.stiffness_matrix()
+        Cm = None
+        try:
+            rnode = np.ctypeslib.as_array(C.cast(v.rnode, C.POINTER(C.c_double)), shape=(v.nn,))
+            rhs = np.zeros(K.n)
+            L.check(L.lib().sgpu_assembly_lift(K.h, np.ascontiguousarray(rnode), rhs))
+            info["assembly"] = K.assembly
+            if v.problem == 50:
+                x, r = K.pcg(rhs, ni=v.ni, res=v.res, zero=zero, crit="scr" if v.storage == 11 else "cr",
+                             prec=prec, mode=mode)
+                info["wall_s"] = time.perf_counter() - t0
+                return x, None, np.array([r.info["iterations"]]), dict(info, solve=r.info)
+            Cm = dk.stiffness_matrix("hex8t_c")
+            cn = np.ctypeslib.as_array(C.cast(v.cn, C.POINTER(C.c_int64)), shape=(v.nn,))
+            free = cn > 0
+            d = np.zeros(K.n)
+            d[cn[free] - 1] = rnode[free]  # initial values (lhsrhst::initcond)
+            vel = np.zeros(K.n)
+            nsteps = int(round((v.t1 - v.t0) / v.dt))
+            its = np.zeros(max(nsteps, 1), dtype=np.int64)
+            sinfo = L.SolveInfo()
+            fn = L.lib().sgpu_transient_dform if v.tform == 1 else L.lib().sgpu_transient_vform
+            st = fn(K.h, Cm.h, rhs, d, vel, float(v.dt), float(v.alpha), nsteps, int(v.ni), float(v.res),
+                    float(zero), int(v.iv), {"jacobi": L.PREC_JACOBI, "agg": L.PREC_AGG}[prec],
+                    {"fp64": L.FP64, "mixed": L.MIXED}[mode], its.ctypes.data, C.byref(sinfo))
+            L.check(st, (L.OK, L.NOT_CONVERGED, L.BREAKDOWN))
+            info["nsteps"] = nsteps
+            info["wall_s"] = time.perf_counter() - t0
+            return d, vel, its[:nsteps], dict(info, solve=sinfo.as_dict())
+        finally:
+            K.close()
+            if Cm is not None:
+                Cm.close()
 
 
 def trfel_lift(K: DeviceMatrix, rnode) -> np.ndarray:

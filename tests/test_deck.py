@@ -163,3 +163,69 @@ def test_deck_end_to_end(oracle, gpu_lib, tmp_path, name, prec):
         assert results[lc].status == L.OK
         assert np.linalg.norm(X[lc] - xo) / np.linalg.norm(xo) <= 1e-8
     assert info["n"] == m.ndof and info["parse_ms"] > 0.0
+
+
+# ---------------------------------------------------------------------------
+# TRFEL decks
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("stationary,form", [(False, "d"), (False, "v"), (True, "d")])
+def test_trfel_round_trip(tmp_path, stationary, form):
+    from ssf_b200 import mefel
+    m = decks.heat_cube(5, seed=3)
+    p = str(tmp_path / "t.in")
+    decks.write_trfel_deck(m, p, dt=10.0, nsteps=3, alpha=0.5, stationary=stationary, form=form)
+    with mefel.Deck(p, front="trfel", threads=3) as d:
+        r = d.mesh()
+        info = d.info
+    assert info["problem"] == (50 if stationary else 60)
+    if not stationary:
+        assert info["tform"] == {"d": 1, "v": 2}[form] and info["alpha"] == 0.5
+        assert info["dt"] == 10.0 and round((info["t1"] - info["t0"]) / info["dt"]) == 3
+    assert np.array_equal(r.coords, m.coords) and np.array_equal(r.elems, m.elems)
+    assert np.array_equal(r.dofflag, m.dofflag)
+    assert np.array_equal(r.mats[r.emat], m.mats[m.emat])
+    assert np.array_equal(r.meta["prescribed"], m.meta["prescribed"])
+    assert np.array_equal(r.meta["rho"], np.ones(m.ne))
+
+
+def test_trfel_reader_agrees_with_the_reference_reading(oracle, tmp_path):
+    from ssf_b200 import mefel
+    if not oracle.ref_available():
+        pytest.skip("compiled reference (oracle/_ref) not built")
+    m = decks.heat_cube(4, seed=11)
+    p = str(tmp_path / "t.in")
+    decks.write_trfel_deck(m, p, dt=25.0, nsteps=2, alpha=0.5)
+    d = oracle.run_trfel_dump(p, str(tmp_path))
+    with mefel.Deck(p, front="trfel") as dk:
+        r = dk.mesh()
+    _, _, ka = oracle.assemble(r, sym=True, kind="hex8t_k")
+    _, _, ca = oracle.assemble(r, sym=True, kind="hex8t_c", rho=r.meta["rho"])
+    assert np.array_equal(ka, d["K_a"]) and np.array_equal(ca, d["C_a"])
+    T, V, _ = oracle.trfel_steps(r, 2, 25.0, alpha=0.5, iv=1, rnode=r.meta["rnode"])
+    assert np.array_equal(T, d["T"]) and np.array_equal(V, d["V"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,prec", [("d", "jacobi"), ("v", "jacobi"), ("d", "agg")])
+def test_trfel_deck_end_to_end(oracle, gpu_lib, tmp_path, form, prec):
+    from ssf_b200 import mefel
+    m = decks.heat_cube(12, seed=5)
+    p = str(tmp_path / "t.in")
+    decks.write_trfel_deck(m, p, dt=10.0, nsteps=4, alpha=1.0, res=1e-24, form=form)
+    d, v, its, info = mefel.solve_trfel_deck(p, prec=prec, mode="fp64")
+    To, Vo, _ = oracle.trfel_steps(m, 4, 10.0, alpha=1.0, res=1e-26, form=form)
+    assert info["nsteps"] == 4 and (its > 0).all()
+    assert np.linalg.norm(d - To) / np.linalg.norm(To) <= 1e-8
+    assert np.linalg.norm(v - Vo) / np.linalg.norm(Vo) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_trfel_stationary_deck_end_to_end(oracle, gpu_lib, tmp_path):
+    from ssf_b200 import mefel
+    m = decks.heat_cube(10, seed=6)
+    p = str(tmp_path / "s.in")
+    decks.write_trfel_deck(m, p, stationary=True, res=1e-24)
+    x, _, its, info = mefel.solve_trfel_deck(p)
+    xo, st, _, _ = oracle.trfel_stationary(m, res=1e-26)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
