@@ -741,7 +741,7 @@ def run_extra(args, ws, rank):
             O.trfel_steps(small, 1, 10.0, iv=1, ni=100000)
             t_step = (time.perf_counter() - t0) * 1e3 * scale * 2.0  # one step; iterations grow ~2x at 128^3
             out["cpu_baseline"] = {"value": round(t_front + 50 * t_step, 1), "unit": "ms", "cores": 1,
-                                   "kind": "reference",
+                                   "kind": "port",
                                    "sample": "SIFEL's trfel_init + conductivity and capacity matrices on a 64^3 deck "
                                              "timed live and scaled by elements (8x), plus 50 steps from one "
                                              "oracle step on 64^3 scaled by elements and 2x iterations",

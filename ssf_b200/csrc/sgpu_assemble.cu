@@ -26,6 +26,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -91,6 +93,137 @@ __global__ void k_keys_to_scr(int64_t m, int64_t n, const unsigned long long *__
     ci[s] = (int64_t)(k & 0xffffffffull);
     if (s == 0 || (keys[s - 1] >> 32) != (unsigned long long)r) adr[r] = s;
     if (s == m - 1) adr[n] = m;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pattern from the node adjacency (no global sort of element pairs)
+// ---------------------------------------------------------------------------
+
+constexpr int kAdjCap = 512;  // candidate lower neighbours of one node (valence x nodes per element)
+
+// node -> element incidence: counts, then the element ids of every node
+__global__ void k_inc_count(int64_t m, const int64_t *__restrict__ elems, int *__restrict__ cnt) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(cnt + elems[t], 1);
+}
+__global__ void k_inc_fill(int64_t m, int nne, const int64_t *__restrict__ elems, const int *__restrict__ iptr,
+                           int *__restrict__ cursor, int *__restrict__ inc) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t node = elems[t];
+    inc[iptr[node] + atomicAdd(cursor + node, 1)] = (int)(t / nne);
+  }
+}
+
+// one warp per node i: the sorted distinct nodes j <= i that share an element
+// with i (bitonic sort of the candidates in shared memory).  FILL = false
+// counts them into ucnt[i]; FILL = true writes them at nptr[i].  A node with
+// more than kAdjCap candidates sets err bit 16 (the caller falls back).
+template <bool FILL>
+__global__ void __launch_bounds__(TPB) k_node_adj(int64_t nn, int nne, const int64_t *__restrict__ elems,
+                                                  const int *__restrict__ iptr, const int *__restrict__ inc,
+                                                  int *__restrict__ ucnt, const int64_t *__restrict__ nptr,
+                                                  int *__restrict__ nadj, unsigned *err) {
+  __shared__ int buf[WPB][kAdjCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int *sb = buf[wib];
+  for (int64_t i = blockIdx.x * (int64_t)WPB + wib; i < nn; i += (int64_t)gridDim.x * WPB) {
+    const int b = iptr[i], e = iptr[i + 1];
+    const int ncand = (e - b) * nne;
+    if (ncand > kAdjCap) {
+      if (lane == 0) atomicOr(err, 16u);
+      continue;
+    }
+    int P = 32;
+    while (P < ncand) P <<= 1;
+    for (int q = lane; q < P; q += 32) {
+      int v = INT_MAX;
+      if (q < ncand) {
+        const int64_t j = elems[(int64_t)inc[b + q / nne] * nne + q % nne];
+        if (j <= i) v = (int)j;
+      }
+      sb[q] = v;
+    }
+    __syncwarp();
+    for (int k = 2; k <= P; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int q = lane; q < P; q += 32) {
+          const int x = q ^ j;
+          if (x > q) {
+            const int a = sb[q], c = sb[x];
+            if ((a > c) == ((q & k) == 0)) {
+              sb[q] = c;
+              sb[x] = a;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    int total = 0;
+    for (int q0 = 0; q0 < P; q0 += 32) {
+      const int q = q0 + lane;
+      const bool keep = q < P && sb[q] != INT_MAX && (q == 0 || sb[q] != sb[q - 1]);
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (FILL && keep) nadj[nptr[i] + total + __popc(bal & ((1u << lane) - 1u))] = sb[q];
+      total += __popc(bal);
+    }
+    if (!FILL && lane == 0) ucnt[i] = total;
+    __syncwarp();
+  }
+}
+
+// SCR row lengths from the node adjacency, for code numbers that grow with
+// (node, component): row (i, c) holds the free components of every lower
+// neighbour j < i and the free components d <= c of i itself
+__global__ void k_scr_rowlen(int64_t nn, int ndofn, const int64_t *__restrict__ cn, const int64_t *__restrict__ nptr,
+                             const int *__restrict__ nadj, int64_t *__restrict__ rowlen, int64_t n, unsigned *err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t base = 0;
+    bool self = false;
+    for (int64_t q = nptr[i]; q < nptr[i + 1]; q++) {
+      const int j = nadj[q];
+      if (j == i) {
+        self = true;
+        continue;
+      }
+      for (int d = 0; d < ndofn; d++) base += cn[(int64_t)j * ndofn + d] > 0;
+    }
+    int own = 0;
+    for (int c = 0; c < ndofn; c++) {
+      const int64_t r = cn[i * ndofn + c];
+      if (r <= 0) continue;
+      own++;
+      if (r > n) {
+        atomicOr(err, 1u);
+        continue;
+      }
+      if (!self) atomicOr(err, 2u);  // an equation no element touches
+      rowlen[r - 1] = base + own;
+    }
+  }
+}
+
+__global__ void k_scr_fill(int64_t nn, int ndofn, const int64_t *__restrict__ cn, const int64_t *__restrict__ nptr,
+                           const int *__restrict__ nadj, const int64_t *__restrict__ adr, int64_t *__restrict__ ci,
+                           int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int c = 0; c < ndofn; c++) {
+      const int64_t r = cn[i * ndofn + c];
+      if (r <= 0 || r > n) continue;
+      int64_t w = adr[r - 1];
+      for (int64_t q = nptr[i]; q < nptr[i + 1]; q++) {
+        const int j = nadj[q];
+        if (j == i) continue;
+        for (int d = 0; d < ndofn; d++) {
+          const int64_t cc = cn[(int64_t)j * ndofn + d];
+          if (cc > 0) ci[w++] = cc - 1;
+        }
+      }
+      for (int d = 0; d <= c; d++) {
+        const int64_t cc = cn[i * ndofn + d];
+        if (cc > 0) ci[w++] = cc - 1;
+      }
+    }
   }
 }
 
@@ -942,6 +1075,106 @@ int colour_elements(int64_t nn, int64_t ne, int nne, const int64_t *elems, std::
   return SGPU_OK;
 }
 
+// stream-ordered temporaries of the pattern build (the device pool keeps the
+// memory between calls, so no cudaMalloc / cudaFree synchronisation)
+template <class T>
+struct AsyncBuf {
+  T *p = nullptr;
+  cudaStream_t s = nullptr;
+  explicit AsyncBuf(cudaStream_t st) : s(st) {}
+  AsyncBuf(const AsyncBuf &) = delete;
+  AsyncBuf &operator=(const AsyncBuf &) = delete;
+  ~AsyncBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+  int alloc(size_t count) {
+    static bool pool_kept = false;
+    if (!pool_kept) {
+      int dev = 0;
+      cudaMemPool_t pool;
+      if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      pool_kept = true;
+    }
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), s);
+    if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    return SGPU_OK;
+  }
+};
+
+// exclusive scan of `len` (n entries) into out (n+1 entries, out[n] = total)
+template <class In, class Out>
+int scan_into(const In *len, Out *out, int64_t n, cudaStream_t s) {
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, len, out, (int)n + 1, s);
+  AsyncBuf<unsigned char> t(s);
+  SGPU_TRY(t.alloc(tmp));
+  cub::DeviceScan::ExclusiveSum(t.p, tmp, len, out, (int)n + 1, s);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// The SCR pattern from the node adjacency when the code numbers grow with
+// (node, component) (gencodnum's numbering): node -> element incidence,
+// per-node sorted lower neighbours, row lengths, scan, fill.  Returns
+// SGPU_OK, or 1 when a node has too many candidate neighbours (the caller
+// uses the element-pair sort instead).  Writes m->src_adr / src_ci / src_negm.
+int pattern_adjacency(sgpu_matrix m, const int64_t *elems_d, const int64_t *cn_d, int64_t nn, int64_t ne, int nne,
+                      int ndofn, int64_t n, unsigned *err_d, cudaStream_t s) {
+  const int64_t m_inc = ne * nne;
+  if (m_inc > (1LL << 31) - 1) return 1;
+  AsyncBuf<int> cnt(s), iptr(s), cursor(s), inc(s), ucnt(s), nadj(s);
+  AsyncBuf<int64_t> nptr(s), rowlen(s);
+  SGPU_TRY(cnt.alloc(nn + 1));
+  SGPU_TRY(iptr.alloc(nn + 1));
+  SGPU_TRY(cursor.alloc(nn));
+  SGPU_TRY(inc.alloc(m_inc));
+  SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, (nn + 1) * sizeof(int), s));
+  SGPU_CUDA(cudaMemsetAsync(cursor.p, 0, nn * sizeof(int), s));
+  k_inc_count<<<blocks_for(m_inc), TPB, 0, s>>>(m_inc, elems_d, cnt.p);
+  count_launches(1);
+  SGPU_TRY(scan_into(cnt.p, iptr.p, nn, s));
+  k_inc_fill<<<blocks_for(m_inc), TPB, 0, s>>>(m_inc, nne, elems_d, iptr.p, cursor.p, inc.p);
+  SGPU_TRY(ucnt.alloc(nn + 1));
+  SGPU_CUDA(cudaMemsetAsync(ucnt.p, 0, (nn + 1) * sizeof(int), s));
+  const int gadj = (int)std::min<int64_t>((nn + WPB - 1) / WPB, (int64_t)kNumSMs * 32);
+  k_node_adj<false><<<gadj, TPB, 0, s>>>(nn, nne, elems_d, iptr.p, inc.p, ucnt.p, nullptr, nullptr, err_d);
+  count_launches(2);
+  unsigned e = 0;
+  SGPU_TRY(read_err(err_d, s, &e));
+  if (e & 16u) {
+    SGPU_CUDA(cudaMemsetAsync(err_d, 0, sizeof(unsigned), s));
+    return 1;
+  }
+  SGPU_TRY(nptr.alloc(nn + 1));
+  SGPU_TRY(scan_into(ucnt.p, nptr.p, nn, s));
+  int64_t nadj_total = 0;
+  SGPU_CUDA(cudaMemcpyAsync(&nadj_total, nptr.p + nn, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  SGPU_TRY(nadj.alloc((size_t)nadj_total));
+  k_node_adj<true><<<gadj, TPB, 0, s>>>(nn, nne, elems_d, iptr.p, inc.p, nullptr, nptr.p, nadj.p, err_d);
+  SGPU_TRY(rowlen.alloc(n + 1));
+  SGPU_CUDA(cudaMemsetAsync(rowlen.p, 0, (n + 1) * sizeof(int64_t), s));
+  k_scr_rowlen<<<blocks_for(nn), TPB, 0, s>>>(nn, ndofn, cn_d, nptr.p, nadj.p, rowlen.p, n, err_d);
+  count_launches(2);
+  SGPU_TRY(m->src_adr.alloc(n + 1));
+  SGPU_TRY(scan_into(rowlen.p, m->src_adr.p, n, s));
+  int64_t negm = 0;
+  SGPU_CUDA(cudaMemcpyAsync(&negm, m->src_adr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SGPU_TRY(read_err(err_d, s, &e));
+  if (e) return fail(SGPU_BAD_INPUT, "code numbers: element node out of range or unused equation");
+  m->src_negm = negm;
+  SGPU_TRY(m->src_ci.alloc(negm));
+  k_scr_fill<<<blocks_for(nn), TPB, 0, s>>>(nn, ndofn, cn_d, nptr.p, nadj.p, m->src_adr.p, m->src_ci.p, n);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
 }  // namespace
 
 // Assembly state kept with the matrix handle so that values can be
@@ -1147,8 +1380,26 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   k_elem_codes<<<blocks_for(ne * ndofe), TPB, 0, s>>>(ne, nne, ndofn, ad.elems.p, cn_d.p, ad.cne.p, err.p, nn);
   count_launches(1);
 
-  // pattern: lower-triangle pairs -> sort -> unique -> SCR
+  // pattern: from the node adjacency when the code numbers grow with (node,
+  // component), else (or for a node of very high valence) lower-triangle
+  // element pairs -> sort -> unique -> SCR
+  bool monotone = true;
   {
+    int64_t last = 0;
+    for (int64_t q = 0; q < nn * ndofn && monotone; q++) {
+      const int64_t c = mesh->cn[q];
+      if (c > 0) {
+        monotone = c == last + 1;  // gencodnum's consecutive numbering
+        last = c;
+      }
+    }
+  }
+  int adj_st = 1;
+  if (monotone && !std::getenv("SGPU_PATTERN_SORT")) {
+    adj_st = pattern_adjacency(m, ad.elems.p, cn_d.p, nn, ne, nne, ndofn, n, err.p, s);
+    if (adj_st != SGPU_OK && adj_st != 1) BAIL_ON(adj_st);
+  }
+  if (adj_st != SGPU_OK) {
     const int64_t npairs = ne * (int64_t)ndofe * ndofe;
     if (npairs > (1LL << 31) - 1) return bail(fail(SGPU_BAD_INPUT, "mesh too large for one pattern sort"));
     DevBuf<unsigned long long> keys, skeys;

@@ -386,3 +386,24 @@ def test_serendipity_solve_matches_oracle(oracle, gpu_lib, kind):
         x, r = K.pcg(f, res=1e-22, zero=1e-300, prec="agg", mode="mixed")
         assert r.status == L.OK
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["hex8", "tet4", "hex20", "quad4", "tri3", "quad8", "hex8t"])
+def test_pattern_paths_agree(gpu_lib, monkeypatch, kind):
+    # the node-adjacency pattern and the element-pair sort give the same SCR
+    # arrays (and therefore the same matrix), constrained DOFs included
+    from ssf_b200 import mefel
+    make = {"hex8": lambda: decks.cantilever_hex(7, 3, 2), "tet4": lambda: decks.cantilever_tet(5, 2, 2),
+            "hex20": lambda: decks.cantilever_hex20(4, 2, 2), "quad4": lambda: decks.plate_quad(9, 5),
+            "tri3": lambda: decks.plate_tri(9, 5), "quad8": lambda: decks.plate_quad8(6, 4),
+            "hex8t": lambda: decks.heat_cube(6, seed=2)}[kind]
+    m = make()
+    fn = mefel.conductivity_matrix if kind == "hex8t" else mefel.stiffness_matrix
+    with fn(m) as K:
+        a1 = K.download(symmetric=1)
+    monkeypatch.setenv("SGPU_PATTERN_SORT", "1")
+    with fn(m) as K:
+        a2 = K.download(symmetric=1)
+    for u, v in zip(a1, a2):
+        assert np.array_equal(u, v)
