@@ -23,7 +23,7 @@ Reported (one JSON line on rank 0):
                 ranks; every form's time, iterations and residuals beside it
   e2e           the same form through the C ABI with host (pinned) arrays:
                 sgpu_scr_cg_prec (drop-in for symcomprow::cg_prec) for the
-                Jacobi forms, sgpu_matrix_create + sgpu_matrix_set_nullspace +
+                Jacobi forms, sgpu_matrix_create + sgpu_matrix_set_rigid_body_modes +
                 sgpu_matrix_pcg for the aggregation forms
   roofline      the dominant kernel of the timed form (its FP64 SpMV)
   cpu_baseline  SIFEL's own symcomprow::cg_prec (compiled reference) on a
@@ -377,7 +377,9 @@ def run_ours(args, ws, rank):
     K.close()
     pin = lambda arr: torch.from_numpy(arr).pin_memory().numpy()  # noqa: E731
     adr_p, ci_p, a_p, f_p = pin(adr_h), pin(ci_h), pin(a_h), pin(f_host)
-    rbm_p = pin(rbm_cols.ravel())
+    # the near-null space from the nodes, formed on the device (as the SIFEL binding does from Gtm)
+    xyz_p = pin(np.ascontiguousarray(mesh.coords, dtype=np.float64))
+    cn_p = pin(np.ascontiguousarray(mesh.code_numbers(), dtype=np.int64))
     x_p = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
     prec_b, mode_b = FORMS[best]
     res_b, crit_b = crit_args(best)
@@ -389,7 +391,8 @@ def run_ours(args, ws, rank):
         if prec_b == L.PREC_AGG:
             h = C.c_void_p()
             L.check(lib.sgpu_matrix_create(n, adr_p, ci_p, a_p, 1, C.byref(h)))
-            L.check(lib.sgpu_matrix_set_nullspace(h, rbm_cols.shape[0], rbm_p))
+            L.check(lib.sgpu_matrix_set_rigid_body_modes(h, xyz_p.shape[0], cn_p.shape[1], xyz_p.ctypes.data,
+                                                         cn_p.ctypes.data))
             st = lib.sgpu_matrix_pcg(h, x_p, f_p, 200000, res_b, 1e-30, 0, crit_b, prec_b, mode_b,
                                      C.byref(ani), C.byref(ares), C.byref(info))
             lib.sgpu_matrix_destroy(h)
@@ -399,7 +402,8 @@ def run_ours(args, ws, rank):
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         L.check(st)
     e2e_v = dist_max(min(e2e_ms), ws)
-    h2d = adr_h.nbytes + ci_h.nbytes + a_h.nbytes + f_host.nbytes + (rbm_cols.nbytes if prec_b == L.PREC_AGG else 0)
+    h2d = adr_h.nbytes + ci_h.nbytes + a_h.nbytes + f_host.nbytes + \
+        (xyz_p.nbytes + cn_p.nbytes if prec_b == L.PREC_AGG else 0)
     d2h = x_p.nbytes
 
     cpu = None
@@ -432,7 +436,7 @@ def run_ours(args, ws, rank):
         "spmv_other": spmv_other,
         "roofline": roofline,
         "e2e": {"value": round(e2e_v, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "path": ("sgpu_matrix_create + sgpu_matrix_set_nullspace + sgpu_matrix_pcg (host arrays)"
+                "path": ("sgpu_matrix_create + sgpu_matrix_set_rigid_body_modes + sgpu_matrix_pcg (host arrays)"
                          if prec_b == L.PREC_AGG else
                          "sgpu_scr_cg_prec, the drop-in for symcomprow::cg_prec (host SCR arrays)")},
         "gpu_launches": int(launches),

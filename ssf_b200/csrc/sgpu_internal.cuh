@@ -38,26 +38,38 @@ constexpr int kNumSMs = 148;
 // ---------------------------------------------------------------------------
 // device buffers
 // ---------------------------------------------------------------------------
+// A process-wide cache of device blocks behind DevBuf (sgpu_alloc.cu): a
+// released block waits for the device to be idle -- the ordering cudaFree
+// gave -- and is kept for the next request of a similar size, so that a
+// handle built and destroyed per solve does not pay cudaMalloc / cudaFree
+// each time.  *bytes is rounded up to the block actually handed out.
+cudaError_t devmem_get(void **p, size_t *bytes);
+void devmem_put(void *p, size_t bytes);
+
 template <class T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  size_t bytes = 0;
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) devmem_put(p, bytes);
     p = nullptr;
     n = 0;
+    bytes = 0;
   }
   int alloc(size_t count) {
     if (count <= n && p) return SGPU_OK;
     release();
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+    size_t b = count * sizeof(T);
+    cudaError_t e = devmem_get((void **)&p, &b);
     if (e != cudaSuccess) return fail(SGPU_CUDA_ERROR, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     n = count;
+    bytes = b;
     return SGPU_OK;
   }
 };

@@ -29,42 +29,25 @@
 // MEFEL's global topology (MEFEL/SRC/global.h:132); absent from TRFEL programs
 extern gtopology *Gtm __attribute__((weak));
 
-// Rigid-body modes of Gtm's nodes in equation order (n x k, column after
-// column); k = 0 when there is no usable topology.
-static int rigid_body_modes(long n, std::vector<double> &B) {
+// Node coordinates (nn x 3) and code numbers (nn x ndofn) of Gtm's nodes,
+// from which sgpu_matrix_set_rigid_body_modes forms the rigid-body modes on
+// the device; returns ndofn, 0 when there is no usable topology.
+static int node_arrays(std::vector<double> &xyz, std::vector<int64_t> &cn) {
   if (&Gtm == nullptr || Gtm == nullptr || Gtm->nn <= 0 || Gtm->gnodes == nullptr) return 0;
   const long nn = Gtm->nn;
   const long ndofn = Gtm->gnodes[0].ndofn;
-  if (ndofn != 2 && ndofn != 3) return 0;
-  double cx = 0, cy = 0, cz = 0;
-  for (long i = 0; i < nn; i++) {
-    if (Gtm->gnodes[i].ndofn != ndofn) return 0;
-    cx += Gtm->gnodes[i].x;
-    cy += Gtm->gnodes[i].y;
-    cz += Gtm->gnodes[i].z;
-  }
-  cx /= nn;
-  cy /= nn;
-  cz /= nn;
-  const int k = ndofn == 3 ? 6 : 3;
-  B.assign((size_t)n * k, 0.0);
+  if (ndofn < 1 || ndofn > 3) return 0;
+  xyz.resize((size_t)nn * 3);
+  cn.resize((size_t)nn * ndofn);
   for (long i = 0; i < nn; i++) {
     const gnode &g = Gtm->gnodes[i];
-    const double x = g.x - cx, y = g.y - cy, z = g.z - cz;
-    for (long c = 0; c < ndofn; c++) {
-      const long e = g.cn[c];
-      if (e <= 0 || e > n) continue;
-      double *row = &B[e - 1];
-      if (ndofn == 3) {  // translations, then rotations about z, x, y
-        const double r[3][6] = {{1, 0, 0, -y, 0, z}, {0, 1, 0, x, -z, 0}, {0, 0, 1, 0, y, -x}};
-        for (int q = 0; q < 6; q++) row[(size_t)q * n] = r[c][q];
-      } else {
-        const double r[2][3] = {{1, 0, -y}, {0, 1, x}};
-        for (int q = 0; q < 3; q++) row[(size_t)q * n] = r[c][q];
-      }
-    }
+    if (g.ndofn != ndofn || g.cn == nullptr) return 0;
+    xyz[3 * i] = g.x;
+    xyz[3 * i + 1] = g.y;
+    xyz[3 * i + 2] = g.z;
+    for (long c = 0; c < ndofn; c++) cn[(size_t)i * ndofn + c] = g.cn[c];
   }
-  return k;
+  return (int)ndofn;
 }
 
 extern "C" {
@@ -94,9 +77,10 @@ void __wrap__ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver(symcomprow *self, d
   if (agg) {
     sgpu_matrix m = NULL;
     st = sgpu_matrix_create(self->n, self->adr, self->ci, self->a, 1, &m);
-    std::vector<double> B;
-    const int k = st == SGPU_OK ? rigid_body_modes(self->n, B) : 0;
-    if (k > 0) st = sgpu_matrix_set_nullspace(m, k, B.data());
+    std::vector<double> xyz;
+    std::vector<int64_t> cn;
+    const int ndofn = st == SGPU_OK ? node_arrays(xyz, cn) : 0;
+    if (ndofn > 0) st = sgpu_matrix_set_rigid_body_modes(m, (int64_t)(xyz.size() / 3), ndofn, xyz.data(), cn.data());
     if (st == SGPU_OK)
       st = sgpu_matrix_pcg(m, x, y, ni, res, zero, iv, SGPU_CRIT_SCR_PREC, SGPU_PREC_AGG, mode, &a_ni, &a_res, NULL);
     if (m) sgpu_matrix_destroy(m);

@@ -394,7 +394,7 @@ def solve_batch(meshes, ni=200000, res=1e-20, zero=1e-30, tune=True, prec="jacob
         its = np.zeros(nsys, dtype=np.int64)
         info = L.SolveInfo()
         if prec == "agg":
-            K.set_nullspace(rigid_body_modes(merged))
+            K.set_rigid_body_modes(merged.coords, merged.code_numbers())
             rc = L.lib().sgpu_matrix_pcg_batch_agg(K.h, nsys, rows, x, f, int(ni), float(res), float(zero),
                                                    {"fp64": L.FP64, "mixed": L.MIXED}[mode], ani.ctypes.data,
                                                    ares.ctypes.data, st.ctypes.data, its.ctypes.data, C.byref(info))
