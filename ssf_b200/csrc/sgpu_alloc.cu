@@ -9,7 +9,10 @@
 //
 // Ordering: cudaFree waits for the device's outstanding work, and code that
 // releases a buffer may rely on that; devmem_put keeps the guarantee with a
-// cudaDeviceSynchronize before the block becomes reusable.
+// cudaDeviceSynchronize before the block becomes reusable.  Contents: memory
+// fresh from cudaMalloc reads as zeros in practice and device flags and
+// counters of this library start from that, so a reused block is cleared
+// (and the clear finished) before it is handed out.
 #include <map>
 #include <mutex>
 
@@ -69,7 +72,9 @@ cudaError_t devmem_get(void **p, size_t *bytes) {
       *bytes = it->first;
       g_cached -= it->first;
       g_free.erase(it);
-      return cudaSuccess;
+      cudaError_t z = cudaMemset(*p, 0, *bytes);
+      if (z == cudaSuccess) z = cudaDeviceSynchronize();
+      return z;
     }
   }
   e = cudaMalloc(p, want);
