@@ -282,27 +282,17 @@ def run_ours(args, ws, rank):
         return dist_max(ms, ws), infos, launches
 
     forms = FORM_SETS[args.forms]
-    # pick the fastest form on untimed solves (the second of two, so module
-    # loading and autotuning are out of it), then time it
-    probe = {}
-    for form in forms:
-        for _ in range(2 if len(forms) > 1 else 0):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            with torch.cuda.stream(stream):
-                solve(form)
-            torch.cuda.synchronize()
-            probe[form] = dist_max(time.perf_counter() - t0, ws)  # same choice on every rank
-    best = min(probe, key=probe.get) if probe else forms[0]
+    # every form timed the same way (warm-up, K steps, CUDA events, clocks
+    # sampled during its timed region); the fastest is the line's value
     clocks = Clocks(torch.cuda.current_device())
-    clocks.start()
-    ms_best, inf_best, launches = timed(best, args.steps, args.warmup)
-    clk = clocks.stop()
-    results = {best: (ms_best, inf_best[-1])}
+    timed_all = {}
     for form in forms:
-        if form != best:
-            ms_o, inf_o, _ = timed(form, max(2, args.steps // 2), 1)
-            results[form] = (ms_o, inf_o[-1])
+        clocks.start()
+        ms_f, inf_f, launches_f = timed(form, args.steps, args.warmup)
+        timed_all[form] = (ms_f, inf_f, launches_f, clocks.stop())
+    best = min(timed_all, key=lambda k: timed_all[k][0])
+    ms_best, inf_best, launches, clk = timed_all[best]
+    results = {form: (v[0], v[1][-1]) for form, v in timed_all.items()}
     forms_out = {}
     for form, (ms, inf) in results.items():
         d = {"ms_per_step": round(ms, 3), "iterations": inf.iterations, "true_relres": inf.true_relres,
