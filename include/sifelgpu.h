@@ -305,6 +305,16 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
 SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,
                              sgpu_assembly_info *info);
 
+/* A second matrix of the same mesh on the pattern of a handle made by
+ * sgpu_assemble, in a new handle: the pattern, the element colouring and the
+ * element data are copied on the device, only the values are integrated
+ * (kind: the handle's own, or for hex8t handles the other of K and C; emat /
+ * rho replace the element parameters when not NULL).  TRFEL's conductivity
+ * and capacity matrices (TRFEL/SRC/globmatt.cpp:19/92) share one pattern this
+ * way instead of building it twice. */
+SGPU_API int sgpu_assemble_copy(sgpu_matrix src, int32_t kind, const double *emat, const double *rho,
+                                sgpu_matrix *out, sgpu_assembly_info *info);
+
 /* Dirichlet lifting of TRFEL's assemble_init (TRFEL/SRC/globmatt.cpp:1635):
  * for a hex8 conduction handle made by sgpu_assemble, add -K_e r_e of every
  * element into rhs[n] (host, accumulated) at its free DOFs, where rnode[nn]

@@ -145,6 +145,7 @@ SIGNATURES = {
                                C.POINTER(SolveInfo)], C.c_int),
     "sgpu_assemble": ([C.POINTER(Mesh), C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_reassemble": ([_vp, _i32, _vp, _vp, C.POINTER(AssemblyInfo)], C.c_int),
+    "sgpu_assemble_copy": ([_vp, _i32, _vp, _vp, C.POINTER(_vp), C.POINTER(AssemblyInfo)], C.c_int),
     "sgpu_deck_read_mefel": ([C.c_char_p, _i32, C.POINTER(_vp)], C.c_int),
     "sgpu_deck_read_trfel": ([C.c_char_p, _i32, C.POINTER(_vp)], C.c_int),
     "sgpu_deck_get": ([_vp, C.POINTER(DeckView)], C.c_int),

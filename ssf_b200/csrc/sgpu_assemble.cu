@@ -1498,6 +1498,92 @@ SGPU_API int sgpu_assembly_lift(sgpu_matrix m, const double *rnode, double *rhs)
   return SGPU_OK;
 }
 
+SGPU_API int sgpu_assemble_copy(sgpu_matrix src, int32_t kind, const double *emat, const double *rho,
+                                sgpu_matrix *out, sgpu_assembly_info *info) {
+  if (!src || !src->asm_data || !out) return fail(SGPU_BAD_INPUT, "handle was not created by sgpu_assemble");
+  *out = nullptr;
+  const AssemblyData &sa = src->asm_data->d;
+  const bool scalar_ok = (sa.kind == SGPU_ELEM_HEX8T_K || sa.kind == SGPU_ELEM_HEX8T_C) &&
+                         (kind == SGPU_ELEM_HEX8T_K || kind == SGPU_ELEM_HEX8T_C);
+  if (kind != sa.kind && !scalar_ok) return fail(SGPU_BAD_INPUT, "element kind differs from the pattern's");
+  SGPU_CUDA(cudaStreamSynchronize(src->stream));
+  sgpu_matrix m = new sgpu_matrix_s();
+  auto bail = [&](int st) {
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    cudaStream_t s = m->own_stream;
+    cudaEvent_t a = m->ev0, b = m->ev1;
+    delete m;
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (s) cudaStreamDestroy(s);
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&m->ev0) != cudaSuccess || cudaEventCreate(&m->ev1) != cudaSuccess)
+    return bail(fail(SGPU_CUDA_ERROR, "stream/event creation failed"));
+  m->stream = m->own_stream;
+  cudaStream_t s = m->stream;
+  m->n = src->n;
+  m->src_sym = src->src_sym;
+  m->src_negm = src->src_negm;
+  m->asm_data = new sgpu_assembly_s();
+  AssemblyData &ad = m->asm_data->d;
+  ad.kind = kind; ad.nne = sa.nne; ad.ndofn = sa.ndofn; ad.nn = sa.nn; ad.ne = sa.ne;
+  ad.general = sa.general;
+  ad.offsets = sa.offsets;
+  Csr &c = m->csr;
+  c.n = src->csr.n;
+  c.nnz = src->csr.nnz;
+  int st = SGPU_OK;
+#define DUP(dst, from)                                                                        \
+  if (st == SGPU_OK && (from).p) {                                                            \
+    st = (dst).alloc((from).n);                                                               \
+    if (st == SGPU_OK &&                                                                      \
+        cudaMemcpyAsync((dst).p, (from).p, (from).n * sizeof(*(from).p), cudaMemcpyDeviceToDevice, s) != cudaSuccess) \
+      st = fail(SGPU_CUDA_ERROR, "device copy of the pattern failed");                        \
+  }
+  DUP(m->src_adr, src->src_adr);
+  DUP(m->src_ci, src->src_ci);
+  DUP(m->map_lo, src->map_lo);
+  DUP(m->map_up, src->map_up);
+  DUP(c.rowptr, src->csr.rowptr);
+  DUP(c.col, src->csr.col);
+  DUP(ad.coords, sa.coords);
+  DUP(ad.elems, sa.elems);
+  DUP(ad.cne, sa.cne);
+  DUP(ad.elist, sa.elist);
+  DUP(ad.emat, sa.emat);
+  DUP(ad.thick, sa.thick);
+  DUP(ad.rho, sa.rho);
+#undef DUP
+  if (st != SGPU_OK) return bail(st);
+  if (c.val.alloc(c.nnz) != SGPU_OK || c.diag.alloc(c.n) != SGPU_OK) return bail(SGPU_CUDA_ERROR);
+  m->bsr.valid = false;
+  m->bsr.nb = -1;  // examined on first use
+  if (emat && cudaMemcpyAsync(ad.emat.p, emat, ad.ne * (ad.general ? 36 : 2) * sizeof(double),
+                              cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return bail(fail(SGPU_CUDA_ERROR, "copy of emat failed"));
+  if (rho) {
+    if (ad.rho.alloc(ad.ne) != SGPU_OK) return bail(SGPU_CUDA_ERROR);
+    if (cudaMemcpyAsync(ad.rho.p, rho, ad.ne * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return bail(fail(SGPU_CUDA_ERROR, "copy of rho failed"));
+  }
+  float ms = 0.f;
+  st = assemble_values(m, ad, kind, &ms);
+  if (st == SGPU_OK) st = finish_values(m);
+  if (st != SGPU_OK) return bail(st);
+  if (info) {
+    memset(info, 0, sizeof(*info));
+    info->n = m->n;
+    info->negm_scr = m->src_negm;
+    info->nnz_full = c.nnz;
+    info->colours = (int32_t)ad.offsets.size() - 1;
+    info->integrate_ms = ms;
+  }
+  *out = m;
+  return SGPU_OK;
+}
+
 SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, const double *rho,
                              sgpu_assembly_info *info) {
   if (!m || !m->asm_data) return fail(SGPU_BAD_INPUT, "handle was not created by sgpu_assemble");

@@ -102,6 +102,21 @@ def capacity_matrix(mesh, rho=None) -> DeviceMatrix:
     return _assemble(mesh, "hex8t_c", rho)
 
 
+def assemble_copy(K: DeviceMatrix, kind: str, emat=None, rho=None) -> DeviceMatrix:
+    """Another matrix of K's mesh on K's pattern (``sgpu_assemble_copy``):
+    e.g. the capacity matrix of a conduction handle, without a second
+    pattern build and colouring."""
+    em = None if emat is None else _c(emat, np.float64)
+    rr = None if rho is None else _c(rho, np.float64)
+    h = C.c_void_p()
+    info = L.AssemblyInfo()
+    L.check(L.lib().sgpu_assemble_copy(K.h, KIND[kind], em.ctypes.data if em is not None else None,
+                                       rr.ctypes.data if rr is not None else None, C.byref(h), C.byref(info)))
+    dm = DeviceMatrix.from_handle(h, info.n, 1)
+    dm.assembly = info.as_dict()
+    return dm
+
+
 def rigid_body_modes(mesh) -> np.ndarray:
     """Near-null space of the mesh's operator in equation order (n x k): the
     6 rigid-body motions of a 3D elastic body, the 3 of a plane one, or the
@@ -307,7 +322,7 @@ def solve_trfel_deck(path: str, prec="jacobi", mode="fp64", threads: int = 0, ze
                              prec=prec, mode=mode)
                 info["wall_s"] = time.perf_counter() - t0
                 return x, None, np.array([r.info["iterations"]]), dict(info, solve=r.info)
-            Cm = dk.stiffness_matrix("hex8t_c")
+            Cm = assemble_copy(K, "hex8t_c")
             cn = np.ctypeslib.as_array(C.cast(v.cn, C.POINTER(C.c_int64)), shape=(v.nn,))
             free = cn > 0
             d = np.zeros(K.n)
@@ -347,7 +362,7 @@ def linear_nonstat_solv_dform(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20,
     nonstat_solv_vform_comp (npsolvert.cpp:62, trapezoidv) instead.  Returns (d, v, per-step iterations,
     solve info)."""
     K = conductivity_matrix(mesh)
-    Cm = capacity_matrix(mesh)
+    Cm = assemble_copy(K, "hex8t_c")
     try:
         if rnode is None:
             rnode = mesh.meta["prescribed"][:, 0]

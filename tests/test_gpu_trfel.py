@@ -86,3 +86,26 @@ def test_stationary_matches_oracle(oracle, gpu_lib):
     x, r = mefel.solve_stationary_problem(m)
     assert r.status == L.OK and abs(r.ani - ani_o) <= 2
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_capacity_on_the_conductivity_pattern(oracle, gpu_lib):
+    # sgpu_assemble_copy: C integrated on K's pattern equals C assembled on
+    # its own, and the oracle's C; new element parameters are taken
+    from ssf_b200 import mefel
+    m = decks.heat_cube(6, seed=8)
+    rho = np.random.default_rng(3).uniform(0.5, 2.0, m.ne)
+    _, _, ca = oracle.assemble(m, sym=True, kind="hex8t_c", rho=rho)
+    with mefel.conductivity_matrix(m) as K:
+        with mefel.assemble_copy(K, "hex8t_c", rho=rho) as Cc, mefel.capacity_matrix(m, rho=rho) as Cs:
+            a1, a2 = Cc.download(symmetric=1), Cs.download(symmetric=1)
+        for u, v in zip(a1[:2], a2[:2]):
+            assert np.array_equal(u, v)
+        assert np.array_equal(a1[2], a2[2])
+        assert np.allclose(a1[2], ca, rtol=1e-12, atol=1e-12 * np.abs(ca).max())
+        # K itself is untouched, and a copy with new conductivities follows them
+        _, _, ka = oracle.assemble(m, sym=True, kind="hex8t_k")
+        assert np.allclose(K.download(symmetric=1)[2], ka, rtol=1e-12, atol=1e-12 * np.abs(ka).max())
+        mats2 = m.mats[m.emat].copy()
+        mats2[:, 0] *= 3.0
+        with mefel.assemble_copy(K, "hex8t_k", emat=mats2) as K3:
+            assert np.allclose(K3.download(symmetric=1)[2], 3.0 * ka, rtol=1e-12, atol=1e-12 * np.abs(ka).max())
