@@ -45,6 +45,9 @@
 
 #include <fcntl.h>
 #include <unistd.h>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include "sgpu_internal.cuh"
 
@@ -213,6 +216,52 @@ void ortho_global(const double *l, const double *tm, double *g) {
     }
 }
 
+// Bit i of the result is set where byte p[i] is blank (space, \t \n \v \f \r),
+// for the 64 bytes at p.
+inline uint64_t blank_mask64(const char *p) {
+#if defined(__SSE2__)
+  const __m128i sp = _mm_set1_epi8(' '), nine = _mm_set1_epi8(9), four = _mm_set1_epi8(4);
+  uint64_t m = 0;
+  for (int k = 0; k < 4; k++) {
+    const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i *>(p + 16 * k));
+    const __m128i x = _mm_sub_epi8(c, nine);  // 9..13 -> 0..4 (unsigned)
+    const __m128i ctl = _mm_cmpeq_epi8(_mm_min_epu8(x, four), x);
+    const __m128i b = _mm_or_si128(_mm_cmpeq_epi8(c, sp), ctl);
+    m |= (uint64_t)(uint32_t)_mm_movemask_epi8(b) << (16 * k);
+  }
+  return m;
+#else
+  uint64_t m = 0;
+  for (int k = 0; k < 64; k++) m |= (uint64_t)blank(p[k]) << k;
+  return m;
+#endif
+}
+
+// Token starts of buf[b, e): where a non-blank follows a blank (or `start`,
+// which counts as preceded by a blank).  F(q) is called for every start q in
+// increasing order.  64 bytes per step: the blank mask of the block, shifted
+// by one with the carry of the previous block, against the non-blank mask.
+template <class F>
+void for_token_starts(const DeckData &d, size_t start, size_t b, size_t e, F &&f) {
+  const char *buf = d.buf.data();
+  uint64_t carry = (b == start) ? 1u : (uint64_t)blank(buf[b - 1]);
+  size_t q = b;
+  for (; q + 64 <= e; q += 64) {
+    const uint64_t B = blank_mask64(buf + q);
+    uint64_t st = ~B & ((B << 1) | carry);
+    carry = B >> 63;
+    while (st) {
+      f(q + (size_t)__builtin_ctzll(st));
+      st &= st - 1;
+    }
+  }
+  for (; q < e; q++) {
+    const bool bl = blank(buf[q]);
+    if (!bl && carry) f(q);
+    carry = bl;
+  }
+}
+
 int tokenize(DeckData &d, size_t start) {
   const int T = d.threads;
   const size_t N = d.buf.size();
@@ -223,7 +272,6 @@ int tokenize(DeckData &d, size_t start) {
     b = start + span * (size_t)p / (size_t)parts;
     e = start + span * (size_t)(p + 1) / (size_t)parts;
   };
-  auto is_start = [&](size_t q) { return !blank(d.buf[q]) && (q == start || blank(d.buf[q - 1])); };
   {
     std::vector<std::thread> pool;
     for (int p = 0; p < parts; p++)
@@ -231,7 +279,7 @@ int tokenize(DeckData &d, size_t start) {
         size_t b, e;
         bounds(p, b, e);
         int64_t c = 0;
-        for (size_t q = b; q < e; q++) c += is_start(q);
+        for_token_starts(d, start, b, e, [&c](size_t) { c++; });
         counts[p + 1] = c;
       });
     for (auto &th : pool) th.join();
@@ -244,9 +292,8 @@ int tokenize(DeckData &d, size_t start) {
       pool.emplace_back([&, p] {
         size_t b, e;
         bounds(p, b, e);
-        int64_t w = counts[p];
-        for (size_t q = b; q < e; q++)
-          if (is_start(q)) d.tok[(size_t)w++] = (int64_t)q;
+        int64_t *w = d.tok.data() + counts[p];
+        for_token_starts(d, start, b, e, [&w](size_t q) { *w++ = (int64_t)q; });
       });
     for (auto &th : pool) th.join();
   }
