@@ -330,6 +330,46 @@ __device__ __forceinline__ void csr_add(const int *__restrict__ rowptr, const in
   else atomicOr(err, 4u);
 }
 
+// adds the 3 x 3 block k at rows r[0..2], columns c[0..2] (< 0: no
+// equation).  When both triples are one node's consecutive equations, the
+// three rows of a node hold the same column list in the full CSR, so one
+// search finds the block's first entry and the other eight sit at fixed
+// offsets -- each checked before it is used; otherwise nine searches.
+__device__ __forceinline__ void block3_add(const int *__restrict__ rowptr, const int *__restrict__ col,
+                                           double *__restrict__ val, const int r[3], const int c[3],
+                                           const double k[3][3], unsigned *err) {
+  if (r[0] >= 0 && r[1] == r[0] + 1 && r[2] == r[0] + 2 && c[0] >= 0 && c[1] == c[0] + 1 && c[2] == c[0] + 2) {
+    const int b0 = __ldg(rowptr + r[0]), e0 = __ldg(rowptr + r[0] + 1);
+    const int p = find_col(col, b0, e0, c[0]);
+    if (p >= 0 && p + 2 < e0) {
+      const int off = p - b0;
+      int q[3];
+      bool ok = true;
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int bi = __ldg(rowptr + r[i]), ei = __ldg(rowptr + r[i] + 1);
+        q[i] = bi + off;
+        ok = ok && q[i] + 2 < ei && __ldg(col + q[i]) == c[0] && __ldg(col + q[i] + 1) == c[1] &&
+             __ldg(col + q[i] + 2) == c[2];
+      }
+      if (ok) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) val[q[i] + j] += k[i][j];
+        return;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    if (r[i] < 0) continue;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      if (c[j] >= 0) csr_add(rowptr, col, val, r[i], c[j], k[i][j], err);
+  }
+}
+
 // hex8 elasticity (linhex::gl_stiffness_matrix): block (a,b) of
 // sum_gp |J| B_a^T D B_b with B rows [xx, yy, zz, yz, xz, xy]
 // (linhex::geom_matrix, MEFEL/SRC/linhex.cpp:153-186) and isotropic D
@@ -403,16 +443,9 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
           k[2][j] += w * (az * db[2][j] + ay * db[3][j] + ax * db[4][j]);
         }
       }
-#pragma unroll
-      for (int i = 0; i < 3; i++) {
-        const int r = code[3 * a + i];
-        if (r < 0) continue;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-          const int c = code[3 * b + j];
-          if (c >= 0) csr_add(rowptr, col, val, r, c, k[i][j], err);
-        }
-      }
+      const int rr[3] = {code[3 * a], code[3 * a + 1], code[3 * a + 2]};
+      const int cc[3] = {code[3 * b], code[3 * b + 1], code[3 * b + 2]};
+      block3_add(rowptr, col, val, rr, cc, k, err);
     }
     __syncwarp();
   }
@@ -511,16 +544,13 @@ __global__ void __launch_bounds__(TPB) k_tet4_elastic(int ne_c, const int *__res
       k[1][j] = w * (ay * db[1][j] + az * db[3][j] + ax * db[5][j]);
       k[2][j] = w * (az * db[2][j] + ay * db[3][j] + ax * db[4][j]);
     }
+    int rr[3], cc[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      const int r = __ldg(cne + (int64_t)e * 12 + 3 * a + i);
-      if (r < 0) continue;
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        const int c = __ldg(cne + (int64_t)e * 12 + 3 * b + j);
-        if (c >= 0) csr_add(rowptr, col, val, r, c, k[i][j], err);
-      }
+      rr[i] = __ldg(cne + (int64_t)e * 12 + 3 * a + i);
+      cc[i] = __ldg(cne + (int64_t)e * 12 + 3 * b + i);
     }
+    block3_add(rowptr, col, val, rr, cc, k, err);
   }
 }
 
@@ -755,17 +785,20 @@ __global__ void __launch_bounds__(TPB20) k_hex20_elastic(int ne_c, const int *__
           k[2][jj] += w * (az * db[2][jj] + ay * db[3][jj] + ax * db[4][jj]);
         }
       }
+      int rr[3], cc[3];
 #pragma unroll
       for (int ii = 0; ii < 3; ii++) {
-        const int r = __ldg(cne + (int64_t)e * 60 + 3 * a + ii);
+        rr[ii] = __ldg(cne + (int64_t)e * 60 + 3 * a + ii);
+        cc[ii] = __ldg(cne + (int64_t)e * 60 + 3 * b + ii);
+      }
+      block3_add(rowptr, col, val, rr, cc, k, err);
+      if (a != b) {
+        double kt[3][3];
 #pragma unroll
-        for (int jj = 0; jj < 3; jj++) {
-          const int c = __ldg(cne + (int64_t)e * 60 + 3 * b + jj);
-          if (r >= 0 && c >= 0) {
-            csr_add(rowptr, col, val, r, c, k[ii][jj], err);
-            if (a != b) csr_add(rowptr, col, val, c, r, k[ii][jj], err);
-          }
-        }
+        for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+          for (int jj = 0; jj < 3; jj++) kt[ii][jj] = k[jj][ii];
+        block3_add(rowptr, col, val, cc, rr, kt, err);
       }
     }
     __syncwarp();
