@@ -108,6 +108,27 @@ struct PhaseClock {
   }
 };
 
+// allocator whose value-less construct leaves trivial elements uninitialised:
+// vectors that the parallel record loops fill entry by entry (one record per
+// id, every id present) need no zero fill first
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U> &) {}
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    if constexpr (sizeof...(A) == 0) ::new ((void *)p) U;
+    else ::new ((void *)p) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using FillVec = std::vector<T, NoInitAlloc<T>>;
+
 struct DeckData {
   PhaseClock clk;
   RawArray<char> buf;
@@ -121,8 +142,10 @@ struct DeckData {
   int32_t kind = -1, ndofn = 0, nne = 0, mtype = 0, nmatp = 0;
   int64_t nn = 0, ne = 0, n = 0;
   int32_t nmat = 0, nlc = 0;
-  std::vector<double> coords, mats, thick, loads, emat2, dmat;
-  std::vector<int64_t> elems, dofflag, cn, emat_id;
+  FillVec<double> coords;
+  FillVec<int64_t> elems, emat_id;
+  std::vector<double> mats, thick, loads, emat2, dmat;
+  std::vector<int64_t> dofflag, cn;
   double parse_ms = 0.0;
   // TRFEL
   int32_t problem = 1;  // 1 linear statics (MEFEL); 50 stationary, 60 nonstationary (TRFEL)
@@ -353,7 +376,7 @@ int parse_mefel(DeckData &d) {
   int64_t nd0 = 0;
   if (!d.geti(c.t + 4, nd0) || nd0 < 1 || nd0 > 3) return fail(SGPU_BAD_INPUT, "deck: bad DOF count of the first node");
   d.ndofn = (int32_t)nd0;
-  d.coords.assign((size_t)d.nn * 3, 0.0);
+  d.coords.resize((size_t)d.nn * 3);  // every node record writes its row
   std::vector<std::atomic<uint8_t>> seen((size_t)d.nn);
   for (auto &s : seen) s.store(0, std::memory_order_relaxed);
   int64_t bad = parallel_records(d, c.t, d.nn, 7, [&](int64_t, int64_t t, bool &ok) {
@@ -405,8 +428,8 @@ int parse_mefel(DeckData &d) {
   // the material type of the first element fixes the deck's one type
   int64_t mt0 = 0;
   d.geti(c.t + stride - 2, mt0);
-  d.elems.assign((size_t)d.ne * d.nne, 0);
-  d.emat_id.assign((size_t)d.ne, 0);
+  d.elems.resize((size_t)d.ne * d.nne);  // every element record writes its row
+  d.emat_id.resize((size_t)d.ne);
   std::vector<int64_t> tset;
   if (et->plane) tset.assign((size_t)d.ne, 0);
   std::vector<std::atomic<uint8_t>> eseen((size_t)d.ne);
@@ -625,7 +648,7 @@ int parse_trfel(DeckData &d) {
   d.ndofn = 1;
   d.nn = c.i();
   if (!c.err.empty() || d.nn <= 0) return fail(SGPU_BAD_INPUT, "deck: bad node count");
-  d.coords.assign((size_t)d.nn * 3, 0.0);
+  d.coords.resize((size_t)d.nn * 3);  // every node record writes its row
   std::vector<std::atomic<uint8_t>> seen((size_t)d.nn);
   for (auto &q : seen) q.store(0, std::memory_order_relaxed);
   int64_t bad = parallel_records(d, c.t, d.nn, 6, [&](int64_t, int64_t t, bool &ok) {
@@ -662,9 +685,9 @@ int parse_trfel(DeckData &d) {
   d.nne = 8;
   d.ne = c.i();
   if (!c.err.empty() || d.ne <= 0 || d.ne > (1LL << 31) - 1) return fail(SGPU_BAD_INPUT, "deck: bad element count");
-  d.elems.assign((size_t)d.ne * 8, 0);
-  d.emat_id.assign((size_t)d.ne, 0);
-  std::vector<int64_t> cs_of((size_t)d.ne, 0);
+  d.elems.resize((size_t)d.ne * 8);  // every element record writes its row
+  d.emat_id.resize((size_t)d.ne);
+  FillVec<int64_t> cs_of((size_t)d.ne);
   std::vector<std::atomic<uint8_t>> eseen((size_t)d.ne);
   for (auto &q : eseen) q.store(0, std::memory_order_relaxed);
   bad = parallel_records(d, c.t, d.ne, 15, [&](int64_t, int64_t t, bool &ok) {
