@@ -260,13 +260,14 @@ def trfel_lift(mesh, rnode):
     return rhs
 
 
-def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1, rnode=None, form="d"):
+def trfel_steps(mesh, nsteps, dt, alpha=1.0, ni=100000, res=1e-20, zero=1e-30, iv=1, rnode=None, form="d",
+                rho=None):
     """nsteps of linear_nonstat_solv_dform (TRFEL/SRC/npsolvert.cpp:1146-1230,
     form "d") or of the v-form's one_step_linear (npsolvert.cpp:367-480,
     form "v") with K and C assembled once (their values do not change for
     linear materials) and the lifting of time-constant prescribed values."""
     adr, ci, ka = assemble(mesh, sym=True, kind="hex8t_k")
-    _, _, ca = assemble(mesh, sym=True, kind="hex8t_c")
+    _, _, ca = assemble(mesh, sym=True, kind="hex8t_c", rho=rho)
     n = adr.size - 1
     if rnode is None:
         rnode = mesh.meta["prescribed"][:, 0]

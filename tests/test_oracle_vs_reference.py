@@ -168,3 +168,29 @@ def test_trfel_random_cube_bit_exact(ref, form):
         d = ref.run_trfel_dump(deck, td)
     T, V, its = ref.trfel_steps(m, 2, 25.0, alpha=0.5, iv=1, form=form)
     assert np.array_equal(T, d["T"]) and np.array_equal(V, d["V"])
+
+
+def test_trfel_density_and_distortion_bit_exact(ref):
+    # a cross-section density other than 1 (crsec3dt) scales the capacity
+    # matrix; distorted nodes exercise the Jacobians; several prescribed
+    # values; the deck reader's view of the same file gives the same matrices
+    from ssf_b200 import mefel
+    m = decks.heat_cube(4, seed=21, T_left=3.5)
+    rng = np.random.default_rng(5)
+    inner = ~np.isclose(m.coords[:, 0], 0.0)
+    m.coords[inner] += rng.uniform(-0.02, 0.02, (inner.sum(), 3))
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "c.in")
+        decks.write_trfel_deck(m, deck, dt=15.0, nsteps=3, alpha=0.75, rho=2.5)
+        d = ref.run_trfel_dump(deck, td)
+        with mefel.Deck(deck, front="trfel") as dk:
+            r = dk.mesh()
+    rho = np.full(m.ne, 2.5)
+    assert np.array_equal(r.meta["rho"], rho)
+    _, _, ka = ref.assemble(m, sym=True, kind="hex8t_k")
+    _, _, ca = ref.assemble(m, sym=True, kind="hex8t_c", rho=rho)
+    assert np.array_equal(ka, d["K_a"]) and np.array_equal(ca, d["C_a"])
+    _, _, ca_r = ref.assemble(r, sym=True, kind="hex8t_c", rho=r.meta["rho"])
+    assert np.array_equal(ca_r, d["C_a"])
+    T, V, _ = ref.trfel_steps(m, 3, 15.0, alpha=0.75, iv=1, rho=rho)
+    assert np.array_equal(T, d["T"]) and np.array_equal(V, d["V"])
