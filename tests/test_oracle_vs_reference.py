@@ -194,3 +194,24 @@ def test_trfel_density_and_distortion_bit_exact(ref):
     assert np.array_equal(ca_r, d["C_a"])
     T, V, _ = ref.trfel_steps(m, 3, 15.0, alpha=0.75, iv=1, rho=rho)
     assert np.array_equal(T, d["T"]) and np.array_equal(V, d["V"])
+
+
+@pytest.mark.parametrize("kind", ["tet4", "tri3", "hex20"])
+def test_cr_storage_of_the_added_elements(ref, kind):
+    # compressed_rows (storage 10) + no preconditioner, the reference's CR
+    # path: the full-row storage and the CG on it
+    m = {"tet4": lambda: decks.cantilever_tet(4, 2, 2), "tri3": lambda: decks.plate_tri(6, 3, E=3e10, nu=0.22),
+         "hex20": lambda: decks.cantilever_hex20(3, 2, 2)}[kind]()
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck, storage=10, precond=0, res=1e-10)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=False)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    if kind == "hex20":
+        assert np.abs(a - d["K_a"]).max() <= 1e-14 * np.abs(d["K_a"]).max()
+        return
+    assert np.array_equal(a, d["K_a"])
+    f = ref.load_vector(m)
+    x, st, ani, ares = ref.cr_cg_prec(adr, ci, a, f, ni=20000, res=1e-10, zero=1e-300)
+    assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
