@@ -153,13 +153,14 @@ SGPU_API int sgpu_matrix_set_stream(sgpu_matrix m, void *stream);
  * iteration, device pointers, autotuned format/kernel. */
 SGPU_API int sgpu_matrix_mxv32_d(sgpu_matrix m, const float *x_d, float *y_d);
 /* Algorithmic bytes of one SpMV (precision 64 or 32) in the tuned format,
- * the format id (0 CSR, 3 BSR3) and the kernel variant; tunes if needed. */
+ * the format id (0 CSR, 2 sliced ELL, 3 BSR3) and the kernel variant; tunes
+ * if needed. */
 SGPU_API int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *bytes, int32_t *format,
                                    int32_t *variant);
 
-/* Override the autotuner: use SpMV `format` (0 CSR, 3 BSR3) and `variant`
- * (lanes per row: 4/8/16/32 for CSR, 8/16/32 for BSR3) for `precision`
- * (64 or 32).  For tests and
+/* Override the autotuner: use SpMV `format` (0 CSR, 2 sliced ELL, 3 BSR3) and
+ * `variant` (lanes per row: 4/8/16/32 for CSR, 8/16/32 for BSR3; 32 for the
+ * sliced ELL, FP64 only) for `precision` (64 or 32).  For tests and
  * tuning studies; BAD_INPUT if the format is not available for the matrix. */
 SGPU_API int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32_t variant);
 

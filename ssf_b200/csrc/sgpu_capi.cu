@@ -214,7 +214,10 @@ int sgpu_matrix_spmv_plan(sgpu_matrix m, int32_t precision, double *bytes, int32
 int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32_t variant) {
   if (!m) return fail(SGPU_BAD_INPUT, "null handle");
   if (precision != 64 && precision != 32) return fail(SGPU_BAD_INPUT, "precision must be 64 or 32");
-  if (format != 0 && format != 3) return fail(SGPU_BAD_INPUT, "format must be 0 (CSR) or 3 (BSR3)");
+  if (format != 0 && format != 2 && format != 3)
+    return fail(SGPU_BAD_INPUT, "format must be 0 (CSR), 2 (sliced ELL, FP64) or 3 (BSR3)");
+  if (format == 2 && (precision != 64 || variant != 32))
+    return fail(SGPU_BAD_INPUT, "sliced ELL is FP64 with variant 32 (a thread per row)");
   if ((format == 0 && variant != 4 && variant != 8 && variant != 16 && variant != 32) ||
       (format == 3 && variant != 8 && variant != 16 && variant != 32 && variant != 132 && variant != 232 &&
        variant != 116 && variant != 216 && variant != 108 && variant != 208))
@@ -227,6 +230,10 @@ int sgpu_matrix_set_spmv(sgpu_matrix m, int32_t precision, int32_t format, int32
   }
   SGPU_TRY(ensure_bsr3(m));
   if (format == 3 && !m->bsr.valid) return fail(SGPU_BAD_INPUT, "matrix has no 3x3 block-row form");
+  if (format == 2) {
+    SGPU_TRY(ensure_sell(m));
+    if (!m->sell.valid) return fail(SGPU_BAD_INPUT, "rows too uneven for the sliced ELL form");
+  }
   SpmvPlan &p = precision == 64 ? m->plan64 : m->plan32;
   p.format = format;
   p.variant = variant;

@@ -106,8 +106,23 @@ struct Bsr3 {
 };
 
 // SpMV kernel choice for one format/precision, picked by the autotuner.
+// Sliced ELL (slices of 32 rows, each padded to its longest row, stored
+// column by column: entry k of row 32 q + l at sptr[q] + 32 k + l), FP64 only.
+// Thread per row, every load of a warp one contiguous segment; padding
+// entries have value 0 and the row's own column.
+struct Sell {
+  bool examined = false;  // ensure_sell has looked at the pattern
+  bool valid = false;     // built (padding within the limit)
+  int nslices = 0;
+  int64_t nent = 0;       // stored entries, padding included
+  DevBuf<int64_t> sptr;   // nslices + 1
+  DevBuf<int> scol;
+  DevBuf<double> sval;
+  DevBuf<int> csr2sell;   // CSR entry -> position in sval
+};
+
 struct SpmvPlan {
-  int format = 0;   // 0 CSR, 3 BSR3
+  int format = 0;   // 0 CSR, 2 sliced ELL (FP64), 3 BSR3
   int variant = 0;  // kernel variant id
   bool tuned = false;
 };
@@ -161,6 +176,7 @@ struct sgpu_matrix_s {
   sgpu::DevBuf<int> map_lo, map_up;       // source entry -> CSR positions
   sgpu::Csr csr;
   sgpu::Bsr3 bsr;
+  sgpu::Sell sell;
   sgpu::SpmvPlan plan64, plan32;
   sgpu::Work w;
   cudaStream_t stream = nullptr;      // stream all work of the handle runs on
@@ -182,6 +198,7 @@ int matrix_set_values_device(sgpu_matrix m, const double *a_d);
 int ensure_fp32(sgpu_matrix m);
 int finish_values(sgpu_matrix m);  // diag, derived formats after val changed
 int ensure_bsr3(sgpu_matrix m);
+int ensure_sell(sgpu_matrix m);
 // sgpu_spmv.cu
 // y = A x (FP64). If dot_out != nullptr also sum_i x_i y_i into a device scalar
 // via the block partials of `w`.

@@ -323,6 +323,8 @@ int matrix_build_from_device_src(sgpu_matrix m) {
   }
   m->bsr.valid = false;
   m->bsr.nb = -1;  // not yet examined
+  m->sell.examined = false;
+  m->sell.valid = false;
   m->plan64 = SpmvPlan{};
   m->plan32 = SpmvPlan{};
   return SGPU_OK;
@@ -336,6 +338,9 @@ int matrix_set_values_device(sgpu_matrix m, const double *a_d) {
   count_launches(1);
   return finish_values(m);
 }
+
+__global__ void k_sell_values(int64_t nnz, const double *__restrict__ val, const int *__restrict__ csr2sell,
+                              double *__restrict__ sval);
 
 // After c.val changed: the diagonal, and the derived formats marked stale.
 int finish_values(sgpu_matrix m) {
@@ -352,6 +357,10 @@ int finish_values(sgpu_matrix m) {
   m->bsr.have32 = false;
   if (m->bsr.valid) {
     k_bsr3_values<<<blocks_for(c.nnz), TPB, 0, s>>>(c.nnz, c.val.p, m->bsr.csr2bsr.p, m->bsr.bval.p);
+    count_launches(1);
+  }
+  if (m->sell.valid) {
+    k_sell_values<<<blocks_for(c.nnz), TPB, 0, s>>>(c.nnz, c.val.p, m->sell.csr2sell.p, m->sell.sval.p);
     count_launches(1);
   }
   // a non-positive diagonal is kept (the FP64 CG without preconditioner can
@@ -378,6 +387,105 @@ int ensure_fp32(sgpu_matrix m) {
     count_launches(1);
     m->bsr.have32 = true;
   }
+  return SGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sliced ELL
+// ---------------------------------------------------------------------------
+__global__ void k_sell_width(int n, int nslices, const int *__restrict__ rowptr, int64_t *__restrict__ width) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nslices; q += gridDim.x * blockDim.x) {
+    int w = 0;
+    for (int l = 0; l < 32; l++) {
+      const int i = 32 * q + l;
+      if (i < n) w = max(w, rowptr[i + 1] - rowptr[i]);
+    }
+    width[q] = 32ll * w;
+  }
+}
+
+__global__ void k_sell_fill(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                            const int64_t *__restrict__ sptr, int *__restrict__ scol, double *__restrict__ sval,
+                            int *__restrict__ csr2sell) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int q = i >> 5, l = i & 31;
+    const int64_t base = sptr[q];
+    const int w = (int)((sptr[q + 1] - base) >> 5);
+    const int b = rowptr[i], len = rowptr[i + 1] - b;
+    for (int k = 0; k < w; k++) {
+      const int64_t pos = base + 32ll * k + l;
+      if (k < len) {
+        scol[pos] = col[b + k];
+        csr2sell[b + k] = (int)pos;
+      } else {
+        scol[pos] = i;
+        sval[pos] = 0.0;
+      }
+    }
+  }
+}
+
+// the lanes past n in the last slice: padding too
+__global__ void k_sell_tail(int n, int nslices, const int64_t *__restrict__ sptr, int *__restrict__ scol,
+                            double *__restrict__ sval) {
+  const int q = nslices - 1;
+  const int w = (int)((sptr[q + 1] - sptr[q]) >> 5);
+  for (int t = threadIdx.x; t < 32 * w; t += blockDim.x) {
+    const int k = t >> 5, l = t & 31;
+    if (32 * q + l >= n) {
+      scol[sptr[q] + 32ll * k + l] = 0;
+      sval[sptr[q] + 32ll * k + l] = 0.0;
+    }
+  }
+}
+
+__global__ void k_sell_values(int64_t nnz, const double *__restrict__ val, const int *__restrict__ csr2sell,
+                              double *__restrict__ sval) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
+    sval[csr2sell[k]] = val[k];
+}
+
+int ensure_sell(sgpu_matrix m) {
+  Sell &e = m->sell;
+  if (e.examined) return SGPU_OK;
+  e.examined = true;
+  e.valid = false;
+  const Csr &c = m->csr;
+  cudaStream_t s = m->stream;
+  const int n = c.n, nslices = (n + 31) / 32;
+  if (n <= 0) return SGPU_OK;
+  DevBuf<int64_t> width;
+  SGPU_TRY(width.alloc((size_t)nslices + 1));
+  SGPU_CUDA(cudaMemsetAsync(width.p + nslices, 0, sizeof(int64_t), s));
+  k_sell_width<<<blocks_for(nslices), TPB, 0, s>>>(n, nslices, c.rowptr.p, width.p);
+  count_launches(1);
+  SGPU_TRY(e.sptr.alloc((size_t)nslices + 1));
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, width.p, e.sptr.p, nslices + 1, s);
+  DevBuf<unsigned char> t;
+  SGPU_TRY(t.alloc(tmp));
+  cub::DeviceScan::ExclusiveSum(t.p, tmp, width.p, e.sptr.p, nslices + 1, s);
+  count_launches(1);
+  int64_t nent = 0;
+  SGPU_CUDA(cudaMemcpyAsync(&nent, e.sptr.p + nslices, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  // worth it only for rows of similar length: at most a quarter of padding
+  if (nent >= (int64_t)INT32_MAX || (double)nent > 1.25 * (double)c.nnz) {
+    e.sptr.release();
+    return SGPU_OK;
+  }
+  e.nslices = nslices;
+  e.nent = nent;
+  SGPU_TRY(e.scol.alloc(nent));
+  SGPU_TRY(e.sval.alloc(nent));
+  SGPU_TRY(e.csr2sell.alloc(c.nnz));
+  k_sell_fill<<<blocks_for(n), TPB, 0, s>>>(n, c.rowptr.p, c.col.p, e.sptr.p, e.scol.p, e.sval.p, e.csr2sell.p);
+  k_sell_tail<<<1, TPB, 0, s>>>(n, nslices, e.sptr.p, e.scol.p, e.sval.p);
+  k_sell_values<<<blocks_for(c.nnz), TPB, 0, s>>>(c.nnz, c.val.p, e.csr2sell.p, e.sval.p);
+  count_launches(3);
+  SGPU_CUDA(cudaGetLastError());
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  e.valid = true;
   return SGPU_OK;
 }
 

@@ -215,6 +215,47 @@ __global__ void __launch_bounds__(TPB) k_spmv_csr(int n, const int *__restrict__
 }
 
 // ---------------------------------------------------------------------------
+// SpMV: sliced ELL, one warp per slice of 32 rows, one thread per row; the
+// warp's loads of entry k are one 256-byte (values) and one 128-byte
+// (columns) segment.  For rows of similar length (scalar 3D stencils), where
+// CSR's lane groups waste part of each transaction.
+// ---------------------------------------------------------------------------
+template <class Epi>
+__global__ void __launch_bounds__(TPB) k_spmv_sell(int n, int nslices, const int64_t *__restrict__ sptr,
+                                                   const int *__restrict__ scol, const double *__restrict__ sval,
+                                                   const double *__restrict__ x, double *__restrict__ y,
+                                                   PcgState *st, double *partials, unsigned *ticket) {
+  if (Epi::kGate && stopped(st)) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc = 0.0;
+  for (int q = warp; q < nslices; q += nwarps) {
+    const int64_t b = __ldg(sptr + q);
+    const int w = (int)((__ldg(sptr + q + 1) - b) >> 5);
+    const double *v = sval + b + lane;
+    const int *c = scol + b + lane;
+    double s0 = 0.0, s1 = 0.0;
+    int k = 0;
+    for (; k + 1 < w; k += 2) {
+      s0 += ld_stream(v + 32 * k) * __ldg(x + ld_stream(c + 32 * k));
+      s1 += ld_stream(v + 32 * (k + 1)) * __ldg(x + ld_stream(c + 32 * (k + 1)));
+    }
+    if (k < w) s0 += ld_stream(v + 32 * k) * __ldg(x + ld_stream(c + 32 * k));
+    const int i = 32 * q + lane;
+    if (i < n) {
+      const double r = s0 + s1;
+      y[i] = r;
+      if (Epi::kDot) acc += __ldg(x + i) * r;
+    }
+  }
+  if (Epi::kDot) {
+    double vv[1] = {acc}, t[1];
+    if (reduce_grid<1>(vv, partials, ticket, t)) Epi::finish(st, t[0]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // SpMV: BSR3, one warp per block row, lanes over the row's 3x3 blocks.
 // Values are stored component-major per block row (see sgpu_matrix.cu) so a
 // warp reading one component of consecutive blocks is fully coalesced.
@@ -649,6 +690,10 @@ int launch_spmv64(sgpu_matrix m, int format, int variant, const double *x, doubl
              : variant == 208 ? k_spmv_bsr3<double, double, double, 8, 8, Epi>
                               : k_spmv_bsr3<double, double, double, 32, 1, Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval.p, x, y, st, part, tk);
+  } else if (format == 2) {
+    const Sell &e = m->sell;
+    auto k = k_spmv_sell<Epi>;
+    k<<<occ_grid(k), TPB, 0, s>>>((int)m->n, e.nslices, e.sptr.p, e.scol.p, e.sval.p, x, y, st, part, tk);
   } else {
     const Csr &c = m->csr;
     switch (variant) {
@@ -707,6 +752,8 @@ double spmv_bytes(sgpu_matrix m, int format, int precision) {
   const double n = (double)m->n;
   if (format == 3)
     return (double)m->bsr.nblk * (9.0 * sv + 4.0) + (m->bsr.nb + 1.0) * 4.0 + 2.0 * n * sv;
+  if (format == 2)  // padding included: it is read
+    return (double)m->sell.nent * (sv + 4.0) + (m->sell.nslices + 1.0) * 8.0 + 2.0 * n * sv;
   return (double)m->csr.nnz * (sv + 4.0) + (n + 1.0) * 4.0 + 2.0 * n * sv;
 }
 
@@ -782,6 +829,10 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   std::vector<Cand> cands = {{0, 4}, {0, 8}, {0, 16}, {0, 32}};
   if (m->bsr.valid)
     for (int v : {32, 16, 8, 132, 232, 116, 216, 108, 208}) cands.push_back({3, v});
+  if (precision == 64) {
+    SGPU_TRY(ensure_sell(m));
+    if (m->sell.valid) cands.push_back({2, 32});
+  }
   // x = 1, y scratch
   const int n = (int)m->n;
   k_fill<<<grid_for_vectors(), TPB, 0, s>>>(n, m->w.t.p, 1.0);

@@ -168,7 +168,8 @@ class DeviceMatrix:
         L.check(L.lib().sgpu_matrix_update_values(self.h, _f64(a)))
 
     def set_spmv(self, precision, fmt, variant=0):
-        """Pin the SpMV kernel (format 0 CSR / 3 BSR3, CSR lanes per row)."""
+        """Pin the SpMV kernel (format 0 CSR / 2 sliced ELL (FP64) / 3 BSR3;
+        lanes per row)."""
         L.check(L.lib().sgpu_matrix_set_spmv(self.h, int(precision), int(fmt), int(variant)))
 
     def spmv_plan(self, precision):
