@@ -690,11 +690,11 @@ int launch_spmv64(sgpu_matrix m, int format, int variant, const double *x, doubl
              : variant == 208 ? k_spmv_bsr3<double, double, double, 8, 8, Epi>
                               : k_spmv_bsr3<double, double, double, 32, 1, Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>(m->bsr.nb, m->bsr.browptr.p, m->bsr.bcol.p, m->bsr.bval.p, x, y, st, part, tk);
-  } else if (format == 2) {
+  } else if (format == 2 && m->sell.valid) {
     const Sell &e = m->sell;
     auto k = k_spmv_sell<Epi>;
     k<<<occ_grid(k), TPB, 0, s>>>((int)m->n, e.nslices, e.sptr.p, e.scol.p, e.sval.p, x, y, st, part, tk);
-  } else {
+  } else {  // CSR (also a sliced-ELL plan on a handle without that form)
     const Csr &c = m->csr;
     switch (variant) {
       case 8: { auto k = k_spmv_csr<double, double, double, 8, Epi>;
@@ -817,11 +817,22 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   if (precision == 32) SGPU_TRY(ensure_fp32(m));
   cudaStream_t s = m->stream;
   const std::string key = plan_key(m, precision);
+  SpmvPlan cached;
+  bool have_cached = false;
   {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     auto it = g_plans.find(key);
     if (it != g_plans.end() && !getenv(precision == 64 ? "SGPU_SPMV64" : "SGPU_SPMV32")) {
-      (precision == 64 ? m->plan64 : m->plan32) = it->second;
+      cached = it->second;
+      have_cached = true;
+    }
+  }
+  if (have_cached) {
+    // a plan tuned on another handle of the same shape: this handle needs the
+    // chosen format's arrays too
+    if (cached.format == 2) SGPU_TRY(ensure_sell(m));
+    if (cached.format != 2 || m->sell.valid) {
+      (precision == 64 ? m->plan64 : m->plan32) = cached;
       return SGPU_OK;
     }
   }
