@@ -215,3 +215,27 @@ def test_cr_storage_of_the_added_elements(ref, kind):
     f = ref.load_vector(m)
     x, st, ani, ares = ref.cr_cg_prec(adr, ci, a, f, ni=20000, res=1e-10, zero=1e-300)
     assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"])
+
+
+def test_thickness_sets_and_load_cases_bit_exact(ref):
+    # plane stress with two cross-section thickness sets, and a cantilever
+    # with three load cases: K, every right-hand side and every solution
+    q = decks.plate_quad(6, 4, E=3e10, nu=0.22)
+    q.meta["tvals"] = [0.01, 0.03]
+    q.meta["tset"] = list(np.arange(q.ne) % 2)
+    q.thick = np.array([0.01, 0.03])[np.arange(q.ne) % 2]
+    c = decks.cantilever_top_loads(decks.cantilever_hex(5, 2, 2), 3, seed=9)
+    for m in (q, c):
+        with tempfile.TemporaryDirectory() as td:
+            deck = os.path.join(td, "d.in")
+            decks.write_mefel_deck(m, deck)
+            d = ref.run_mefel_dump(deck, td)
+        adr, ci, a = ref.assemble(m, sym=True)
+        assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+        assert np.array_equal(a, d["K_a"])
+        n = adr.size - 1
+        for lc in range(m.loads.shape[0]):
+            f = ref.load_vector(m, lc)
+            assert np.array_equal(f, d["f"][lc * n:(lc + 1) * n])
+            x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+            assert ani == d["meta"][f"ani_{lc}"] and np.array_equal(x, d["u"][lc * n:(lc + 1) * n])
