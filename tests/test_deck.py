@@ -229,3 +229,22 @@ def test_trfel_stationary_deck_end_to_end(oracle, gpu_lib, tmp_path):
     x, _, its, info = mefel.solve_trfel_deck(p)
     xo, st, _, _ = oracle.trfel_stationary(m, res=1e-26)
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_crlf_tabs_and_exponents(tmp_path):
+    # the positional format is token based: CR LF line ends, tabs, upper-case
+    # exponents and explicit plus signs read as the reference's xfscanf reads them
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex(3, 2, 2)
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    text = open(p).read()
+    lines = text.rstrip("\n").split("\n")
+    head, rest = lines[:1], lines[1:]
+    rest = [ln.replace(" ", "\t", 1).replace("e-", "E-").replace("e+", "E+") for ln in rest]
+    open(p, "w", newline="").write("\r\n".join(head + rest) + "\r\n")
+    with mefel.Deck(p) as d:
+        r = d.mesh()
+        f = d.rhs(0)
+    assert np.array_equal(r.coords, m.coords) and np.array_equal(r.elems, m.elems)
+    assert np.array_equal(f, mefel.mefel_right_hand_side(m, 0))
