@@ -359,21 +359,39 @@ SGPU_API int sgpu_transient_vform(sgpu_matrix K, sgpu_matrix C, const double *rh
 /* Solving without allocating device memory                                 */
 /* ------------------------------------------------------------------------ */
 
+/* Largest system sgpu_csr_pcg_noalloc_d takes (equations). */
+#define SGPU_NOALLOC_MAX_N 131072
+
 /* No counterpart in the reference: an addition for callers that cannot
  * allocate GPU memory while they solve (an application that owns the whole
  * device memory pool through its own allocator, or one that must not call
- * cudaMalloc/cudaFree because they synchronise the device).  Jacobi-PCG with
- * the criterion of symcomprow::cg_prec on a caller-owned device CSR (full
- * rows, int32 indices, sorted columns, diagonal present): rowptr_d[n+1],
- * col_d/val_d[rowptr_d[n]], f_d[n] read, x_d[n] in/out (start vector when
- * iv = 1), all device pointers, work enqueued on `stream` (NULL = legacy
- * default stream).  The work vectors live in one static device array of the
- * library (about 5 MiB, held by every GPU that loads it until exit), so
- * n <= 131072 (BAD_INPUT beyond).  Nothing is allocated.  Every call uses the
- * same array: calls that overlap on the GPU race and must be serialised.  The
- * first call on each device looks up the array's device address; make it
- * before any stream capture.  *ani/*ares as in sgpu_scr_cg_prec (written only
- * on convergence); *iterations (may be NULL) gets the iterations done. */
+ * cudaMalloc/cudaFree because they synchronise the device).
+ *
+ * Jacobi-preconditioned CG on a caller-owned device CSR: full rows, int32
+ * indices, a positive diagonal entry in every row.  rowptr_d[n+1],
+ * col_d/val_d[rowptr_d[n]], f_d[n] are read, x_d[n] is the start vector when
+ * iv != 0 (else set to 0 first) and gets the solution; all device pointers,
+ * work enqueued on `stream` (NULL = legacy default stream).  The iteration
+ * stops when (r.r)/(f.f) < res for the recurrence residual r, or after ni
+ * iterations (SGPU_NOT_CONVERGED), or when |d.p| < zero for a search
+ * direction d and p = K d (SGPU_BREAKDOWN); on convergence *ani = the index
+ * of the last iteration (counted from 0) and *ares = (r.h)/(f.f) with the
+ * preconditioned residual h = r/diag, otherwise both are left as they were
+ * (a zero right-hand side, (f.f) < zero, returns SGPU_ZERO_RHS after the
+ * first direction fails the |d.p| test, with *ani = 0 and *ares = 0).
+ * *iterations (may be NULL) gets the iterations done.
+ *
+ * The work vectors live in one static device array of the library (about
+ * 5 MiB, held by every GPU that loads it until exit), so n <=
+ * SGPU_NOALLOC_MAX_N (SGPU_BAD_INPUT beyond).  Nothing is allocated.  Every
+ * call uses the same array: calls that overlap on the GPU race and must be
+ * serialised.  The first call on each device looks up the array's device
+ * address.  Each call waits on the host for its own solve (it reads the
+ * iteration state back between chunks of iterations), so it cannot be
+ * recorded into a CUDA graph: a call on a capturing stream returns
+ * SGPU_BAD_INPUT without enqueuing anything.  Malformed rows (rowptr not
+ * within 0..rowptr[n] and non-decreasing, a column outside [0, n), a missing
+ * or non-positive diagonal) give SGPU_BAD_INPUT with x_d untouched. */
 SGPU_API int sgpu_csr_pcg_noalloc_d(int32_t n, const int32_t *rowptr_d, const int32_t *col_d,
                                     const double *val_d, const double *f_d, double *x_d, int64_t ni,
                                     double res, double zero, int64_t iv, void *stream, int64_t *ani,

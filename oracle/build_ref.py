@@ -42,7 +42,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference/SIFEL"
+# where the reference's sources lie; SIFEL_REFERENCE overrides it
+DEFAULT_REF = os.environ.get("SIFEL_REFERENCE", "/root/reference/SIFEL")
 
 CXX = os.environ.get("CXX", "g++")
 # Flags follow the reference's optimized build (Makefile.in: OPTCFLAGS -O3 plus

@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "BAD_INPUT", 4: 
 CRIT_SCR_PREC, CRIT_CR_PREC, CRIT_TRUE = 0, 1, 2
 FP64, MIXED = 0, 1
 PREC_NONE, PREC_JACOBI, PREC_AGG = 0, 1, 101
+NOALLOC_MAX_N = 131072  # SGPU_NOALLOC_MAX_N of include/sifelgpu.h
 
 
 class SolveInfo(C.Structure):

@@ -2333,14 +2333,23 @@ int fcg_solve(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, in
     if (rc != SGPU_OK) break;
     if (!hs->done) continue;
     // converged on the recurrence: with SGPU_CRIT_TRUE the true residual must
-    // agree, else the recurrence restarts from it
-    if (crit != SGPU_CRIT_TRUE || hs->status != 0 || restarts >= 4) break;
+    // agree, else the recurrence restarts from it (at most four times; a
+    // threshold still unmet then is reported as not reached)
+    if (crit != SGPU_CRIT_TRUE || hs->status != 0) break;
     rc = spmv64(m, w.x.p, w.p.p, s);
     if (rc != SGPU_OK) break;
     k_fcg_true<<<grid_for(n), TPB, 0, s>>>(n, w.f.p, w.p.p, pcg_state(m), w.partials.p, w.counters.p + 3);
     count_launches(1);
     rc = read_st(m, hs);
     if (rc != SGPU_OK || hs->true_rel < res) break;
+    if (restarts >= 4 || hs->it >= ni) {
+      PcgState t = *hs;
+      t.status = SGPU_NOT_CONVERGED;
+      t.ani_set = 0;
+      rc = write_st(m, &t);
+      *hs = t;
+      break;
+    }
     restarts++;
     PcgState t = *hs;
     t.done = 0;

@@ -159,13 +159,16 @@ struct DeckData {
   bool geti(int64_t t, int64_t &v) const {
     if (t < 0 || t >= (int64_t)tok.size()) return false;
     const char *p = at(t);
+    // fscanf's %ld takes a leading plus, from_chars does not; a sign after
+    // the plus stays an error
+    if (*p == '+' && p + 1 < end() && p[1] >= '0' && p[1] <= '9') p++;
     auto r = std::from_chars(p, end(), v);
     return r.ec == std::errc() && (r.ptr == end() || blank(*r.ptr));
   }
   bool getd(int64_t t, double &v) const {
     if (t < 0 || t >= (int64_t)tok.size()) return false;
     const char *p = at(t);
-    if (*p == '+') p++;  // from_chars takes no leading plus
+    if (*p == '+' && p + 1 < end() && p[1] != '-' && p[1] != '+') p++;  // as for integers
     auto r = std::from_chars(p, end(), v);
     return r.ec == std::errc() && (r.ptr == end() || blank(*r.ptr));
   }

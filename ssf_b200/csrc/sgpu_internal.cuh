@@ -199,6 +199,7 @@ int ensure_fp32(sgpu_matrix m);
 int finish_values(sgpu_matrix m);  // diag, derived formats after val changed
 int ensure_bsr3(sgpu_matrix m);
 int ensure_sell(sgpu_matrix m);
+void release_sell(sgpu_matrix m);
 // sgpu_spmv.cu
 // y = A x (FP64). If dot_out != nullptr also sum_i x_i y_i into a device scalar
 // via the block partials of `w`.

@@ -23,25 +23,28 @@ inline int blocks_for(int64_t n, int tpb = TPB) {
 }
 
 // -- validation of the source storage --------------------------------------
-// err bits: 1 adr not monotone / adr[0] != 0, 2 column out of range,
-// 4 columns not strictly increasing, 8 SCR row does not end on its diagonal,
-// 16 CR row has no diagonal
-__global__ void k_validate(int64_t n, const int64_t *__restrict__ adr, const int64_t *__restrict__ ci,
+// err bits: 1 adr not monotone / adr[0] != 0 / a row outside [0, negm),
+// 2 column out of range, 4 columns not strictly increasing, 8 SCR row does
+// not end on its diagonal, 16 CR row has no diagonal.  A row whose bounds
+// fail (bit 1) is not read, so every read stays inside the negm entries.
+__global__ void k_validate(int64_t n, int64_t negm, const int64_t *__restrict__ adr, const int64_t *__restrict__ ci,
                            int sym, unsigned *err) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int64_t b = adr[i], e = adr[i + 1];
     unsigned bad = 0;
-    if (e < b || (i == 0 && b != 0)) bad |= 1;
-    bool has_diag = false;
-    for (int64_t k = b; k < e && !(bad & 1); k++) {
-      int64_t c = ci[k];
-      if (c < 0 || c >= n || (sym && c > i)) bad |= 2;
-      if (k > b && ci[k - 1] >= c) bad |= 4;
-      if (c == i) has_diag = true;
+    if (b < 0 || e < b || e > negm || (i == 0 && b != 0)) bad |= 1;
+    if (!(bad & 1)) {
+      bool has_diag = false;
+      for (int64_t k = b; k < e; k++) {
+        int64_t c = ci[k];
+        if (c < 0 || c >= n || (sym && c > i)) bad |= 2;
+        if (k > b && ci[k - 1] >= c) bad |= 4;
+        if (c == i) has_diag = true;
+      }
+      if (sym && (e == b || ci[e - 1] != i)) bad |= 8;
+      if (!sym && !has_diag) bad |= 16;
     }
-    if (sym && (e == b || ci[e - 1] != i)) bad |= 8;
-    if (!sym && !has_diag) bad |= 16;
     if (bad) atomicOr(err, bad);
   }
 }
@@ -246,7 +249,7 @@ int matrix_build_from_device_src(sgpu_matrix m) {
   DevBuf<unsigned> err;
   SGPU_TRY(err.alloc(1));
   SGPU_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
-  k_validate<<<blocks_for(n), TPB, 0, s>>>(n, m->src_adr.p, m->src_ci.p, sym, err.p);
+  k_validate<<<blocks_for(n), TPB, 0, s>>>(n, negm, m->src_adr.p, m->src_ci.p, sym, err.p);
   count_launches(1);
   unsigned e = 0;
   SGPU_TRY(read_err(err.p, s, &e));
@@ -443,6 +446,19 @@ __global__ void k_sell_values(int64_t nnz, const double *__restrict__ val, const
                               double *__restrict__ sval) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
     sval[csr2sell[k]] = val[k];
+}
+
+// Drops the sliced ELL copy; a later ensure_sell builds it again.
+void release_sell(sgpu_matrix m) {
+  Sell &e = m->sell;
+  e.sptr.release();
+  e.scol.release();
+  e.sval.release();
+  e.csr2sell.release();
+  e.valid = false;
+  e.examined = false;
+  e.nslices = 0;
+  e.nent = 0;
 }
 
 int ensure_sell(sgpu_matrix m) {

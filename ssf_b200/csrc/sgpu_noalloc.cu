@@ -25,8 +25,19 @@
 // Set-up: the array's name in host code is only a host-side stand-in, not a
 // device address.  The first call on each device, with that device current,
 // asks the runtime for the array's device address (cudaGetSymbolAddress) and
-// keeps it; later calls reuse it.  Make that first call before any stream
-// capture starts.
+// keeps it; later calls reuse it.
+//
+// Host waits: every call reads the iteration state back after each chunk of
+// iterations (cudaMemcpyAsync + cudaStreamSynchronize), so a call returns
+// only when its solve has finished and cannot be recorded into a CUDA graph;
+// a call made while its stream is capturing is refused with SGPU_BAD_INPUT
+// before anything is enqueued.
+//
+// Input checks (on the device, before any iteration): every row must satisfy
+// 0 <= rowptr[i] <= rowptr[i+1] <= rowptr[n], hold columns in [0, n) and a
+// positive diagonal entry; otherwise the call returns SGPU_BAD_INPUT and
+// leaves x untouched.  The caller's col/val arrays must hold rowptr[n]
+// entries: the checks keep every read inside [0, rowptr[n]).
 //
 // The iteration is the reference's symcomprow::cg_prec with the diagonal
 // preconditioner (GEFEL/scr.cpp:1093-1205): stop on (r.r)/(f.f) < res, and
@@ -42,7 +53,7 @@
 namespace {
 
 constexpr int kTPB = 256;
-constexpr int kMaxN = 131072;         // SGPU_NOALLOC_MAX_N
+constexpr int kMaxN = SGPU_NOALLOC_MAX_N;
 constexpr int kBlocks = 148 * 4;      // grid of every kernel here
 constexpr int kChunk = 16;            // iterations launched between state reads
 
@@ -148,25 +159,43 @@ __device__ bool grid_sum(double (&v)[NV], double *part, unsigned *ticket, double
   return true;
 }
 
-// clears the state and tickets, extracts the diagonal, zeroes x if iv == 0
+// clears the state and the reduction tickets (one thread: nothing else of the
+// call runs before it)
+__global__ void k_na_clear(Scratch s, long long ni, double res, double zero) {
+  NaState z = {};
+  z.ni = ni;
+  z.res = res;
+  z.zero = zero;
+  z.ani = -1;
+  *s.st = z;
+  for (int k = 0; k < 4; k++) s.ticket[k] = 0u;
+}
+
+// checks every row and extracts the diagonal; a malformed row stops the call
+// with SGPU_BAD_INPUT before any product reads the matrix
 __global__ void k_na_setup(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
-                           const double *__restrict__ val, double *__restrict__ x, int iv, Scratch s,
-                           long long ni, double res, double zero) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    NaState z = {};
-    z.ni = ni;
-    z.res = res;
-    z.zero = zero;
-    z.ani = -1;
-    *s.st = z;
-    for (int k = 0; k < 4; k++) s.ticket[k] = 0u;
-  }
+                           const double *__restrict__ val, Scratch s) {
+  const int nnz = rowptr[n];
+  bool bad = false;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = rowptr[i], e = rowptr[i + 1];
     double dv = 0.0;
-    for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
-      if (col[k] == i) { dv = val[k]; break; }
+    if (b < 0 || e < b || e > nnz) {
+      bad = true;
+    } else {
+      bool seen = false;
+      for (int k = b; k < e; k++) {
+        const int c = col[k];
+        if (c < 0 || c >= n) { bad = true; break; }
+        if (c == i && !seen) { dv = val[k]; seen = true; }
+      }
+      if (!(dv > 0.0)) bad = true;  // missing, zero, negative or NaN diagonal
+    }
     s.diag[i] = dv;
-    if (!iv) x[i] = 0.0;
+  }
+  if (bad) {  // every writer stores the same values
+    s.st->status = SGPU_BAD_INPUT;
+    s.st->done = 1;
   }
 }
 
@@ -175,7 +204,7 @@ template <bool DOT>
 __global__ void k_na_spmv(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
                           const double *__restrict__ val, const double *__restrict__ v, double *__restrict__ y,
                           Scratch s) {
-  if (DOT && s.st->done) return;
+  if (s.st->done) return;
   const int lane = threadIdx.x & 31, g = lane >> 4, sub = lane & 15;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   double acc = 0.0;
@@ -201,7 +230,7 @@ __global__ void k_na_spmv(int n, const int *__restrict__ rowptr, const int *__re
         st->ani = st->it;
         st->ares = st->nom;
         st->ani_set = 1;
-        st->status = SGPU_BREAKDOWN;
+        if (st->status == 0) st->status = SGPU_BREAKDOWN;  // a zero right-hand side keeps its status
         st->done = 1;
       } else {
         st->alpha = st->nom / tot[0];
@@ -210,11 +239,19 @@ __global__ void k_na_spmv(int n, const int *__restrict__ rowptr, const int *__re
   }
 }
 
-// r = f - p, h = r/diag, d = h; f.f and r.h
-__global__ void k_na_start(int n, const double *__restrict__ f, Scratch s) {
+// r = f - p (p = A x0 when iv, else x = 0 and r = f), h = r/diag, d = h;
+// f.f and r.h
+__global__ void k_na_start(int n, const double *__restrict__ f, double *__restrict__ x, int iv, Scratch s) {
+  if (s.st->done) return;  // malformed input: x stays as the caller left it
   double v[2] = {0.0, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double ri = f[i] - s.p[i];
+    double ri;
+    if (iv) {
+      ri = f[i] - s.p[i];
+    } else {
+      ri = f[i];
+      x[i] = 0.0;
+    }
     const double hi = ri / s.diag[i];
     s.r[i] = ri;
     s.h[i] = hi;
@@ -290,15 +327,24 @@ extern "C" SGPU_API int sgpu_csr_pcg_noalloc_d(int32_t n, const int32_t *rowptr_
     return sgpu::fail(SGPU_BAD_INPUT, "n = " + std::to_string(n) + " exceeds the no-allocation solver's maximum of " +
                                           std::to_string(kMaxN) + " equations");
   if (!rowptr_d || !col_d || !val_d || !f_d || !x_d) return sgpu::fail(SGPU_BAD_INPUT, "null device pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t ce = cudaStreamIsCapturing(st, &cap);
+  if (ce != cudaSuccess)
+    return sgpu::fail(SGPU_CUDA_ERROR, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+  if (cap != cudaStreamCaptureStatusNone)
+    return sgpu::fail(SGPU_BAD_INPUT,
+                      "the no-allocation solver waits on the host between iterations and cannot run under "
+                      "stream capture");
   unsigned char *base = nullptr;
   int rc = scratch_address(&base);
   if (rc != SGPU_OK) return rc;
   const Scratch s = carve(base);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_na_setup<<<kBlocks, kTPB, 0, st>>>(n, rowptr_d, col_d, val_d, x_d, iv != 0, s, (long long)ni, res, zero);
-  k_na_spmv<false><<<kBlocks, kTPB, 0, st>>>(n, rowptr_d, col_d, val_d, x_d, s.p, s);
-  k_na_start<<<kBlocks, kTPB, 0, st>>>(n, f_d, s);
-  sgpu::count_launches(3);
+  k_na_clear<<<1, 1, 0, st>>>(s, (long long)ni, res, zero);
+  k_na_setup<<<kBlocks, kTPB, 0, st>>>(n, rowptr_d, col_d, val_d, s);
+  if (iv) k_na_spmv<false><<<kBlocks, kTPB, 0, st>>>(n, rowptr_d, col_d, val_d, x_d, s.p, s);
+  k_na_start<<<kBlocks, kTPB, 0, st>>>(n, f_d, x_d, iv != 0, s);
+  sgpu::count_launches(iv ? 4 : 3);
   NaState h = {};
   for (;;) {
     for (int k = 0; k < kChunk; k++) {

@@ -840,7 +840,10 @@ int spmv_autotune(sgpu_matrix m, int precision) {
   std::vector<Cand> cands = {{0, 4}, {0, 8}, {0, 16}, {0, 32}};
   if (m->bsr.valid)
     for (int v : {32, 16, 8, 132, 232, 116, 216, 108, 208}) cands.push_back({3, v});
-  if (precision == 64) {
+  // the sliced ELL is a candidate for scalar matrices only: where the 3x3
+  // block form exists it reads fewer index bytes, and building the sliced
+  // copy would hold another value array for nothing
+  if (precision == 64 && !m->bsr.valid) {
     SGPU_TRY(ensure_sell(m));
     if (m->sell.valid) cands.push_back({2, 32});
   }
@@ -892,6 +895,9 @@ int spmv_autotune(sgpu_matrix m, int precision) {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     g_plans[key] = p;
   }
+  // a sliced ELL copy that lost the comparison is not kept (nor refreshed on
+  // every value update)
+  if (precision == 64 && p.format != 2) release_sell(m);
   return SGPU_OK;
 }
 
@@ -1014,13 +1020,15 @@ int solve_fp64(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, i
       // The true residual of an FP64 iterate cannot fall below the rounding
       // floor of f - K x itself (about 2^-53 ||K|| ||x|| / ||f||).  When
       // replacing the residual stops paying (no halving over three
-      // confirmations), the iterate is as good as FP64 holds: stop there.
+      // confirmations), the iterate is as good as FP64 holds: stop there,
+      // and report that the threshold was not met.
       confirms.push_back(hs->true_rr);
       const size_t k = confirms.size();
       if (k > 3 && confirms[k - 1] > 0.25 * confirms[k - 4]) {
         PcgState t = *hs;
         t.done = 1;
-        t.ares = t.nom / t.nory;
+        t.ani_set = 0;
+        if (t.status == 0) t.status = SGPU_NOT_CONVERGED;
         rc = write_state(m, &t);
         *hs = t;
         break;
@@ -1159,7 +1167,8 @@ int pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, int 
       fallback = 1;
       mixed_its = hs.it;
       mixed_refs = hs.refinements;
-      rc = solve_fp64(m, ni > hs.it ? ni - hs.it : 1, tol * tol, zero, 1, SGPU_CRIT_SCR_PREC, 1, &hs);
+      // to the threshold of the mixed form itself, on the true FP64 residual
+      rc = solve_fp64(m, ni > hs.it ? ni - hs.it : 1, tol, zero, 1, SGPU_CRIT_TRUE, 1, &hs);
       hs.it += mixed_its;
       hs.refinements += mixed_refs;
     }

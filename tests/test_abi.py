@@ -35,3 +35,10 @@ def test_library_exports_every_declared_symbol():
 def test_version_string_without_gpu():
     from ssf_b200 import _lib
     assert b"sm_100a" in _lib.lib().sgpu_version()
+
+
+def test_header_constants_match_the_binding():
+    from ssf_b200 import _lib
+    src = open(os.path.join(ROOT, "include", "sifelgpu.h")).read()
+    m = re.search(r"#define\s+SGPU_NOALLOC_MAX_N\s+(\d+)", src)
+    assert m and int(m.group(1)) == _lib.NOALLOC_MAX_N

@@ -248,3 +248,28 @@ def test_crlf_tabs_and_exponents(tmp_path):
         f = d.rhs(0)
     assert np.array_equal(r.coords, m.coords) and np.array_equal(r.elems, m.elems)
     assert np.array_equal(f, mefel.mefel_right_hand_side(m, 0))
+
+
+def test_integers_with_a_leading_plus(tmp_path):
+    # fscanf's %ld (the reference's integer reading) accepts "+5"; a second
+    # sign does not make a number
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.cantilever_hex(3, 2, 2)
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    lines = open(p).read().rstrip("\n").split("\n")
+    i0 = 10  # first node record: "id x y z ndofn crst transf"
+    lines[i0 - 1] = "+" + lines[i0 - 1].strip()  # the node count
+    tok = lines[i0].split()
+    tok[0], tok[4] = "+" + tok[0], "+" + tok[4]
+    lines[i0] = " ".join(tok)
+    open(p, "w").write("\n".join(lines) + "\n")
+    with mefel.Deck(p) as d:
+        r = d.mesh()
+    assert np.array_equal(r.coords, m.coords) and np.array_equal(r.elems, m.elems)
+    tok[0] = "+-" + tok[0][1:]
+    lines[i0] = " ".join(tok)
+    open(p, "w").write("\n".join(lines) + "\n")
+    with pytest.raises(L.SgpuError, match="node record 1|integer expected"):
+        mefel.Deck(p)

@@ -1,7 +1,7 @@
-"""SIFEL's own front end with the GPU solver linked in (the drop-in binding
-of INTEGRATION.md): a deck in SIFEL's input format runs unchanged through the
-compiled reference pipeline; only symcomprow::cg_prec is replaced at link
-time by the C-ABI call.  Compared with the all-CPU reference run."""
+"""SIFEL's own front end with the GPU solver linked in (the link-time
+drop-in binding, ssf_b200/integration/sifel_gpu_shim.cpp): a deck in SIFEL's
+input format runs unchanged through the compiled reference pipeline; only
+symcomprow::cg_prec is replaced at link time by the C-ABI call.  Compared with the all-CPU reference run."""
 import os
 import subprocess
 import tempfile
