@@ -72,6 +72,9 @@ def lib():
                           _L, C.POINTER(_L), C.POINTER(_D)]
             f.restype = C.c_int
         L.or_trfel_lift.argtypes = [_L, _pD, _pL, _pL, _pD, _pD, _pD]
+        L.or_hex8_surface_nf.argtypes = [_pD, _pL, _pD, _pD]
+        L.or_quad4_edge_nf.argtypes = [_pD, _pL, _pD, _pD]
+        L.or_prescribed_contrib.argtypes = [C.c_int, _pD, _pL, _pD, _pD]
         _lib = L
     return _lib
 
@@ -204,14 +207,60 @@ def assemble(mesh, sym=True, kind=None, rho=None):
     return adr, ci, a
 
 
+def element_load_forces(mesh, eid, flags, values):
+    """Nodal forces of one element load record (loadel::surfaceload /
+    edgeload): linhex::node_forces_surf or planeelemlq::nodeforces."""
+    nd = mesh.elems[eid]
+    if mesh.kind == "hex8":
+        nf = np.zeros(24)
+        lib().or_hex8_surface_nf(_f64(mesh.coords[nd].reshape(-1)), _i64(flags), _f64(values), nf)
+    elif mesh.kind == "quad4":
+        nf = np.zeros(8)
+        lib().or_quad4_edge_nf(_f64(mesh.coords[nd, :2].reshape(-1)), _i64(flags), _f64(values), nf)
+    else:
+        raise ValueError("element loads are restated for hex8 surfaces and quad4 edges")
+    return nf
+
+
+def element_stiffness(mesh, e):
+    """The element matrix stiffness_matrix localises for element e."""
+    nd = mesh.elems[e]
+    E, nu = mesh.mats[mesh.emat[e]][:2]
+    if mesh.kind == "hex8":
+        ke = np.zeros(24 * 24)
+        lib().or_hex8_ke(_f64(mesh.coords[nd].reshape(-1)), E, nu, ke)
+    elif mesh.kind == "quad4":
+        ke = np.zeros(64)
+        lib().or_quad4_ke(_f64(mesh.coords[nd, :2].reshape(-1)), E, nu, _f64(np.full(4, mesh.thick[e])), ke)
+    else:
+        raise ValueError("prescribed displacements are restated for hex8 and quad4")
+    return ke
+
+
 def load_vector(mesh, lc=0):
-    """Nodal loads assembled into equation order (loadcase::assemble for
-    nodal forces, MEFEL/SRC/loadcase.cpp:400)."""
+    """Right-hand side of load case lc in equation order: loadcase::assemble
+    (MEFEL/SRC/loadcase.cpp:400) -- forcecontrib (:546: nodal loads in record
+    order, then the element loads' nodal forces, locglob) and, for elements
+    with prescribed displacements, prdisplcontrib (:615: f -= K_e r_e)."""
     cn = mesh.code_numbers().reshape(-1)
     f = np.zeros(mesh.ndof)
     vals = mesh.loads[lc].reshape(-1)
     m = cn > 0
     np.add.at(f, cn[m] - 1, vals[m])
+    cne = None
+    if mesh.eloads and mesh.eloads[lc]:
+        cne = element_code_numbers(mesh)
+        for eid, flags, values in mesh.eloads[lc]:
+            nf = element_load_forces(mesh, int(eid), flags, values)
+            for j, c in enumerate(cne[int(eid)]):
+                if c > 0:
+                    f[c - 1] += nf[j]
+    if mesh.pd is not None and mesh.pd.shape[1] > 0:
+        cne = element_code_numbers(mesh) if cne is None else cne
+        pd = _f64(mesh.pd[lc])
+        for e in np.nonzero((cne < 0).any(axis=1))[0]:
+            ke = element_stiffness(mesh, int(e))
+            lib().or_prescribed_contrib(cne.shape[1], ke, _i64(cne[e]), pd, f)
     return f
 
 

@@ -1016,3 +1016,160 @@ void or_trfel_lift(long ne, const double *coords, const long *elems, const long 
     }
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Element loads and prescribed displacements of a MEFEL load case          */
+/* ------------------------------------------------------------------------ */
+
+/* nnj with an mm x nn matrix N (GEFEL/matrix.cpp:3149-3174): m += N^T N jac,
+ * symmetric fill, each product summed over the rows of N from 0. */
+static void nnj_rows(double *m, const double *n, double jac, int mm, int nn) {
+  for (int i = 0; i < nn; i++) {
+    int kk = i * nn + i, ll = kk;
+    double s = 0.0;
+    for (int k = 0; k < mm; k++) s += n[k * nn + i] * n[k * nn + i];
+    m[kk] += s * jac;
+    kk++; ll += nn;
+    for (int j = i + 1; j < nn; j++) {
+      s = 0.0;
+      for (int k = 0; k < mm; k++) s += n[k * nn + i] * n[k * nn + j];
+      m[kk] += s * jac; m[ll] += s * jac;
+      kk++; ll += nn;
+    }
+  }
+}
+
+/* Nodal forces of a surface load given in the global system (ls = 1) on the
+ * faces of a linear hexahedron: linhex::node_forces_surf
+ * (MEFEL/SRC/linhex.cpp:2543).  Face s (0..5) lies at xi = 1, eta = 1,
+ * xi = -1, eta = -1, zeta = 1, zeta = -1; its nodes, in the order of the 4 x 3
+ * load values nv[12 s ..] and of jac2d_3d's surface map
+ * (GEFEL/difcalc.cpp:1065-1100), are HEX_FACE[s].  For every loaded face:
+ * am = sum_{i,j} N^T N |J_s| w_i w_j (bf_matrix, linhex.cpp:126; nnj), with
+ * the surface Jacobian of jac2d3d (GEFEL/difcalc.cpp:819-866), then
+ * nf += am av where av holds the face's nodal loads (kept between faces, as
+ * the reference's vector is).  Only ls = 1 is restated. */
+static const int HEX_FACE[6][4] = {{0, 3, 7, 4}, {1, 0, 4, 5}, {2, 1, 5, 6},
+                                   {3, 2, 6, 7}, {0, 1, 2, 3}, {4, 7, 6, 5}};
+
+void or_hex8_surface_nf(const double *xyz, const long *ls, const double *nv, double *nf) {
+  double x[8], y[8], z[8], am[24 * 24], av[24], v[24], n[3 * 24], bf[8];
+  for (int i = 0; i < 8; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
+  memset(av, 0, sizeof(av));
+  for (int s = 0; s < 6; s++) {
+    if (ls[s] <= 0) continue;
+    memset(am, 0, sizeof(am));
+    double lx[4], ly[4], lz[4];
+    for (int q = 0; q < 4; q++) {
+      lx[q] = x[HEX_FACE[s][q]]; ly[q] = y[HEX_FACE[s][q]]; lz[q] = z[HEX_FACE[s][q]];
+    }
+    for (int i = 0; i < 2; i++) {
+      for (int j = 0; j < 2; j++) {
+        const double u = GP2[i], w = GP2[j];
+        double xi, eta, zeta;
+        switch (s) {
+          case 0: xi = 1.0; eta = u; zeta = w; break;
+          case 1: eta = 1.0; xi = u; zeta = w; break;
+          case 2: xi = -1.0; eta = u; zeta = w; break;
+          case 3: eta = -1.0; xi = u; zeta = w; break;
+          case 4: zeta = 1.0; xi = u; eta = w; break;
+          default: zeta = -1.0; xi = u; eta = w; break;
+        }
+        /* jac2d3d with (xi, eta) = (u, w) on the face's bilinear map */
+        double nu4[4], nv4[4];
+        dx_bf_lin_4_2d(nu4, w);
+        dy_bf_lin_4_2d(nv4, u);
+        double dxu = 0.0, dyu = 0.0, dzu = 0.0, dxv = 0.0, dyv = 0.0, dzv = 0.0;
+        for (int q = 0; q < 4; q++) {
+          dxu += nu4[q] * lx[q]; dyu += nu4[q] * ly[q]; dzu += nu4[q] * lz[q];
+          dxv += nv4[q] * lx[q]; dyv += nv4[q] * ly[q]; dzv += nv4[q] * lz[q];
+        }
+        const double g11 = dxu * dxu + dyu * dyu + dzu * dzu;
+        const double g22 = dxv * dxv + dyv * dyv + dzv * dzv;
+        const double g12 = dxu * dxv + dyu * dyv + dzu * dzv;
+        double jac = sqrt(g11 * g22 - g12 * g12);
+        bf_lin_hex_3d(bf, xi, eta, zeta);
+        memset(n, 0, sizeof(n));
+        for (int a = 0; a < 8; a++) {
+          n[0 * 24 + 3 * a] = bf[a];
+          n[1 * 24 + 3 * a + 1] = bf[a];
+          n[2 * 24 + 3 * a + 2] = bf[a];
+        }
+        jac = jac * GW2[i] * GW2[j];
+        nnj_rows(am, n, jac, 3, 24);
+      }
+    }
+    for (int q = 0; q < 4; q++)
+      for (int c = 0; c < 3; c++) av[3 * HEX_FACE[s][q] + c] = nv[12 * s + 3 * q + c];
+    for (int i = 0; i < 24; i++) {
+      double t = 0.0;
+      for (int j = 0; j < 24; j++) t += am[24 * i + j] * av[j];
+      v[i] = t;
+    }
+    for (int i = 0; i < 24; i++) nf[i] = v[i] + nf[i];
+  }
+}
+
+/* Nodal forces of edge loads (le = 1) on a plane-stress bilinear quad:
+ * planeelemlq::nodeforces (MEFEL/SRC/plelemlq.cpp:2433-2514).  Edge e runs
+ * from node e to node e+1 (mod 4) at eta = 1, xi = -1, eta = -1, xi = 1; its
+ * 2 x 2 load values are nv[4 e ..]; am = sum_i N^T N |J_e| w_i with the edge
+ * Jacobian of jac1d2d (GEFEL/difcalc.cpp:730-760), av zeroed per edge. */
+void or_quad4_edge_nf(const double *xy, const long *le, const double *nv, double *nf) {
+  double x[4], y[4], am[64], av[8], v[8], n[2 * 8], bf[4];
+  for (int i = 0; i < 4; i++) { x[i] = xy[2 * i]; y[i] = xy[2 * i + 1]; }
+  for (int e = 0; e < 4; e++) {
+    if (le[e] != 1) continue;
+    memset(am, 0, sizeof(am));
+    const int a0 = e, a1 = (e + 1) & 3;
+    for (int i = 0; i < 2; i++) {
+      const double g = GP2[i];
+      double xi, eta;
+      switch (e) {
+        case 0: eta = 1.0; xi = g; break;
+        case 1: xi = -1.0; eta = g; break;
+        case 2: eta = -1.0; xi = g; break;
+        default: xi = 1.0; eta = g; break;
+      }
+      bf_lin_4_2d(bf, xi, eta);
+      memset(n, 0, sizeof(n));
+      for (int a = 0; a < 4; a++) {
+        n[0 * 8 + 2 * a] = bf[a];
+        n[1 * 8 + 2 * a + 1] = bf[a];
+      }
+      /* jac1d2d: dx_bf_lin_1d = (-0.5, 0.5) on the edge's two nodes */
+      double dx = 0.0, dy = 0.0;
+      dx += -0.5 * x[a0]; dy += -0.5 * y[a0];
+      dx += 0.5 * x[a1]; dy += 0.5 * y[a1];
+      double jac = sqrt(dx * dx + dy * dy);
+      jac *= GW2[i];
+      nnj_rows(am, n, jac, 2, 8);
+    }
+    memset(av, 0, sizeof(av));
+    av[2 * a0] = nv[4 * e]; av[2 * a0 + 1] = nv[4 * e + 1];
+    av[2 * a1] = nv[4 * e + 2]; av[2 * a1 + 1] = nv[4 * e + 3];
+    for (int i = 0; i < 8; i++) {
+      double t = 0.0;
+      for (int j = 0; j < 8; j++) t += am[8 * i + j] * av[j];
+      v[i] = t;
+    }
+    for (int i = 0; i < 8; i++) nf[i] = nf[i] + v[i];
+  }
+}
+
+/* loadcase::prdisplcontrib (MEFEL/SRC/loadcase.cpp:615-664) for one element:
+ * r_e from the prescribed displacements (elprdispl, globmat.cpp:1372: code
+ * number c < 0 takes pd[-c-1], others 0), f = -(K_e r_e), added at the
+ * element's DOFs with code number > 0.  ke: the element's stiffness
+ * (ndofe x ndofe, as assembled). */
+void or_prescribed_contrib(int ndofe, const double *ke, const long *cn, const double *pd, double *rhs) {
+  double r[60], f[60];
+  for (int i = 0; i < ndofe; i++) r[i] = cn[i] < 0 ? pd[-cn[i] - 1] : 0.0;
+  for (int i = 0; i < ndofe; i++) {
+    double s = 0.0;
+    for (int j = 0; j < ndofe; j++) s += ke[i * ndofe + j] * r[j];
+    f[i] = -1.0 * s;
+  }
+  for (int i = 0; i < ndofe; i++)
+    if (cn[i] > 0) rhs[cn[i] - 1] += f[i];
+}

@@ -38,9 +38,11 @@
 // The outer iteration is CG in FP64 on K with the Polak-Ribiere beta
 // (flexible CG: the FP32 preconditioner is not exactly the same linear map at
 // every call); the residual, the solution update, alpha and beta are FP64.
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -130,6 +132,12 @@ __device__ __forceinline__ void op_reduce(const Op &op, double (&acc)[Op::NV > 0
   }
 }
 
+// A product that is never fused into a following add: the kernels that must
+// give the same bits whichever launch form runs them (the separate level
+// kernels and the fused coarse tail) round these products the same way.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // ---------------------------------------------------------------------------
 // row operators: what a level SpMV does with y_i = (A v)_i
 // ---------------------------------------------------------------------------
@@ -188,7 +196,7 @@ struct OpCheb {
     T ri, di, xi;
     if (FIRST) {
       ri = di_ * (b[i] - y);
-      di = c2 * ri;
+      di = mul_rn(c2, ri);
       xi = x_in[i] + di;
     } else {
       ri = r[i] - di_ * y;
@@ -473,7 +481,7 @@ __global__ void __launch_bounds__(TPB) k_prolong(int n, const int *__restrict__ 
     T s = 0;
 #pragma unroll
     for (int q = 0; q < K; q++) s += __ldg(qr + q) * __ldg(xc + K * G + q);
-    x[p] += alpha * s;
+    x[p] = x[p] + mul_rn(alpha, s);
   }
 }
 
@@ -492,6 +500,175 @@ __global__ void __launch_bounds__(TPB) k_dense_mv(int nc, const T *__restrict__ 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) x[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the coarse tail of the cycle in one launch
+//
+// The last smoothed level (a few thousand equations) and the dense coarsest
+// level below it are visited gamma times per visit of the level above, each
+// visit a chain of small dependent steps (smoothing, residual, restriction,
+// dense solve, prolongation, smoothing) that as separate launches cost a
+// launch latency each while doing a microsecond of work.  Here one thread-
+// block cluster runs all the visits of one coarse correction: the cluster's
+// CTAs split every step's rows, and a cluster barrier (release/acquire at
+// cluster scope, no spinning) separates the steps.  Every row is computed
+// with the same loop and summation order as the separate kernels above
+// (k_lv_bsrb, k_restrict, k_dense_mv, k_prolong), so both forms give the same
+// bits.  Vectors written inside the launch are read through L2 (ld.global.cg),
+// never through the non-coherent read-only path.
+// ---------------------------------------------------------------------------
+constexpr int kTailThreads = 512;
+
+template <typename T>
+struct TailArgs {
+  int nb;                                       // block rows of the level
+  const int *browptr, *bcol;
+  const T *val, *dinv;                          // B x B row-major blocks; D^-1 (NULL: unit diagonal)
+  const T *b;                                   // the level's right-hand side
+  T *x, *x2, *res;                              // x holds the first smoothing step (from the restriction)
+  int na;                                       // aggregates of the level = dense rows / K
+  const int *aggptr, *aggnodes, *agg;
+  const T *Q;                                   // n x K tentative prolongator
+  int nc;                                       // dense coarsest equations
+  const T *M;                                   // its inverse, nc x nc row-major
+  T *cb, *cx;
+  T c2, alpha;                                  // first Chebyshev coefficient, coarse-correction weight
+  int visits;
+  const PcgState *st;
+};
+
+// (A v) of block row br, the lanes' partial sums reduced as k_lv_bsrb does;
+// lane r < B returns y_r
+template <typename T, int B>
+__device__ __forceinline__ T tail_bsrb_row(const TailArgs<T> &a, int br, int lane, const T *v) {
+  const int s = __ldg(a.browptr + br), e = __ldg(a.browptr + br + 1);
+  T y[B];
+#pragma unroll
+  for (int c = 0; c < B; c++) y[c] = 0;
+  for (int k = s + lane; k < e; k += 32) {
+    const int c = __ldg(a.bcol + k);
+    T blk[B * B];
+    load_block<T, B>(a.val + (size_t)k * B * B, blk);
+    T xv[B];
+#pragma unroll
+    for (int q = 0; q < B; q++) xv[q] = __ldcg(v + B * c + q);
+#pragma unroll
+    for (int r = 0; r < B; r++) {
+#pragma unroll
+      for (int q = 0; q < B; q++) y[r] += blk[r * B + q] * xv[q];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < B; r++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) y[r] += __shfl_xor_sync(0xffffffffu, y[r], o);
+  }
+  T yv = y[0];
+#pragma unroll
+  for (int r = 1; r < B; r++)
+    if (lane == r) yv = y[r];
+  return yv;
+}
+
+// to = from + c2 D^-1 (b - A from)   (a first Chebyshev step, OpCheb FIRST)
+template <typename T, int B>
+__device__ __forceinline__ void tail_smooth(const TailArgs<T> &a, int gw, int nw, int lane, const T *from, T *to) {
+  for (int br = gw; br < a.nb; br += nw) {
+    const T y = tail_bsrb_row<T, B>(a, br, lane, from);
+    if (lane < B) {
+      const int i = B * br + lane;
+      const T di_ = a.dinv ? __ldg(a.dinv + i) : T(1);
+      const T ri = di_ * (__ldg(a.b + i) - y);
+      const T di = mul_rn(a.c2, ri);
+      to[i] = __ldcg(from + i) + di;
+    }
+  }
+}
+
+template <typename T, int B, int K>
+__global__ void __launch_bounds__(kTailThreads) k_coarse_tail(TailArgs<T> a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  if (a.st->done) return;  // the same for every CTA: nothing writes the state during the launch
+  const int lane = threadIdx.x & 31;
+  const int wpc = kTailThreads / 32;
+  const int gw = (int)cluster.block_rank() * wpc + (threadIdx.x >> 5);
+  const int nw = (int)cluster.num_blocks() * wpc;
+  const int gt = (int)cluster.block_rank() * kTailThreads + threadIdx.x;
+  const int nt = (int)cluster.num_blocks() * kTailThreads;
+  T *xp = a.x;
+  for (int v = 0; v < a.visits; v++) {
+    if (v > 0) {  // pre-smoothing from the previous visit's result
+      T *to = (xp == a.x) ? a.x2 : a.x;
+      tail_smooth<T, B>(a, gw, nw, lane, xp, to);
+      xp = to;
+      cluster.sync();
+    }
+    // residual
+    for (int br = gw; br < a.nb; br += nw) {
+      const T y = tail_bsrb_row<T, B>(a, br, lane, xp);
+      if (lane < B) a.res[B * br + lane] = __ldg(a.b + B * br + lane) - y;
+    }
+    cluster.sync();
+    // restriction to the dense level: cb = Q^T res per aggregate
+    for (int G = gw; G < a.na; G += nw) {
+      const int s = __ldg(a.aggptr + G), e = __ldg(a.aggptr + G + 1);
+      T acc[K];
+#pragma unroll
+      for (int q = 0; q < K; q++) acc[q] = 0;
+      for (int t = s + lane; t < e; t += 32) {
+        const int i = __ldg(a.aggnodes + t);
+#pragma unroll
+        for (int c = 0; c < B; c++) {
+          const T rv = __ldcg(a.res + B * i + c);
+          const T *qr = a.Q + ((size_t)B * i + c) * K;
+#pragma unroll
+          for (int q = 0; q < K; q++) acc[q] += __ldg(qr + q) * rv;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      }
+      if (lane < K) {
+        T vq = acc[0];
+#pragma unroll
+        for (int q = 1; q < K; q++)
+          if (lane == q) vq = acc[q];
+        a.cb[K * G + lane] = vq;
+      }
+    }
+    cluster.sync();
+    // dense coarsest solve: cx = M cb
+    for (int i = gw; i < a.nc; i += nw) {
+      const T *row = a.M + (size_t)i * a.nc;
+      T sum = 0;
+      for (int j = lane; j < a.nc; j += 32) sum += __ldg(row + j) * __ldcg(a.cb + j);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0) a.cx[i] = sum;
+    }
+    cluster.sync();
+    // prolongation: xp += alpha Q cx
+    for (int p = gt; p < B * a.nb; p += nt) {
+      const int G = __ldg(a.agg + p / B);
+      const T *qr = a.Q + (size_t)p * K;
+      T sum = 0;
+#pragma unroll
+      for (int q = 0; q < K; q++) sum += __ldg(qr + q) * __ldcg(a.cx + K * G + q);
+      xp[p] = __ldcg(xp + p) + mul_rn(a.alpha, sum);
+    }
+    cluster.sync();
+    // post-smoothing
+    {
+      T *to = (xp == a.x) ? a.x2 : a.x;
+      tail_smooth<T, B>(a, gw, nw, lane, xp, to);
+      xp = to;
+    }
+    cluster.sync();
   }
 }
 
@@ -2112,6 +2289,85 @@ int cheb_steps(sgpu_matrix m, AmgLevel &L, const Cheb &c, int deg, T *x, T **din
   return SGPU_OK;
 }
 
+// ----- the fused coarse tail (k_coarse_tail) ----------------------------------
+
+constexpr int kTailMaxN = 24576;  // larger last levels keep the full-GPU kernels
+
+// cluster size k_coarse_tail<T, B, K> runs with on this device: 16 CTAs when
+// the device schedules such a cluster, else 8, else 0 (not used).  Asked once
+// per process, on the first cycle (which runs before any graph capture).
+template <typename T, int B, int K>
+int tail_cluster_size() {
+  static std::atomic<int> cached{-1};
+  int c = cached.load();
+  if (c >= 0) return c;
+  auto kern = k_coarse_tail<T, B, K>;
+  c = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) cudaGetLastError();
+  for (int cs : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kTailThreads);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) == cudaSuccess && nclusters >= 1) {
+      c = cs;
+      break;
+    }
+    cudaGetLastError();
+  }
+  cached.store(c);
+  return c;
+}
+
+template <typename T, int B, int K>
+int launch_tail_bk(const TailArgs<T> &a, cudaStream_t s, bool *launched) {
+  *launched = false;
+  const int cs = tail_cluster_size<T, B, K>();
+  if (cs == 0) return SGPU_OK;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(kTailThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  SGPU_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_tail<T, B, K>, a));
+  count_launches(1);
+  *launched = true;
+  return SGPU_OK;
+}
+
+// Runs all `visits` cycles of level C (the last smoothed level, with the
+// dense coarsest below it) in one cluster launch when the block and
+// near-null-space sizes have an instantiation; *launched tells the caller
+// whether it has to run the separate kernels instead.
+template <typename T>
+int launch_tail(const TailArgs<T> &a, int B, int K, cudaStream_t s, bool *launched) {
+  *launched = false;
+  if (B == 6 && K == 6) return launch_tail_bk<T, 6, 6>(a, s, launched);
+  if (B == 3 && K == 3) return launch_tail_bk<T, 3, 3>(a, s, launched);
+  if (B == 1 && K == 1) return launch_tail_bk<T, 1, 1>(a, s, launched);
+  return SGPU_OK;
+}
+
+// SGPU_AMG_TAIL=0 keeps the separate kernels (read at every cycle build, so
+// that a process can compare both forms)
+bool tail_enabled() {
+  const char *e = getenv("SGPU_AMG_TAIL");
+  return !(e && e[0] == '0');
+}
+
 // One cycle on level l (l = number of smoothing levels: the dense coarsest).
 // With zero_init the first smoothing step from x = 0 was fused into whatever
 // produced b (k_fcg_update / k_fcg_init for level 0, the restriction for the
@@ -2179,7 +2435,18 @@ int cycle(sgpu_matrix m, int l, bool zero_init, const std::vector<Cheb> &ch, std
                                st, s));
     // coarse correction
     const int visits = l == 0 ? A.gamma : A.gamma_deep;
-    for (int v = 0; v < visits; v++) SGPU_TRY(cycle<T>(m, l + 1, v == 0, ch, xcur, s));
+    bool fused = false;
+    if (l + 1 == nl - 1 && A.nc > 0 && A.deg == 1 && C.layout == 0 && C.n <= kTailMaxN && tail_enabled()) {
+      TailArgs<T> ta{C.nb, C.browptr, C.bcol, level_vals<T>(m, C), level_dinv<T>(C), W.b.p, W.x.p, W.x2.p,
+                     W.res.p, C.na, C.aggptr.p, C.aggnodes.p, C.agg.p, qmat<T>(C), A.nc,
+                     sizeof(T) == 4 ? (const T *)A.M32.p : (const T *)A.M64.p,
+                     sizeof(T) == 4 ? (T *)A.cb32.p : (T *)A.cb64.p, sizeof(T) == 4 ? (T *)A.cx32.p : (T *)A.cx64.p,
+                     (T)ch[l + 1].c2_first, (T)A.alpha, visits, st};
+      SGPU_TRY(launch_tail<T>(ta, C.b, C.k, s, &fused));
+      if (fused) xcur[l + 1] = W.x2.p;
+    }
+    if (!fused)
+      for (int v = 0; v < visits; v++) SGPU_TRY(cycle<T>(m, l + 1, v == 0, ch, xcur, s));
     SGPU_TRY(prolong_level<T>(L, xcur[l + 1], xp, (T)A.alpha, st, s));
   } else {
     T *cb = sizeof(T) == 4 ? (T *)A.cb32.p : (T *)A.cb64.p;

@@ -451,6 +451,236 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
   }
 }
 
+// ---------------------------------------------------------------------------
+// hex8 isotropic elasticity by rows: one warp per node forms the node's CSR
+// rows from its incident elements in shared memory and writes them once.
+//
+// The colour-ordered scatter above reads and writes every 3 x 3 block once
+// per element that touches it (2.4 times per block on a structured mesh,
+// 24-byte pieces of 32-byte sectors) -- about 3 GB of read-modify-write for
+// the 630 MB value array of a 1M-equation cantilever.  Here each CSR entry is
+// summed in shared memory and stored once, with no colours, no atomics and
+// no zero fill of the value array; the summation order of every entry is
+// fixed (incident elements by ascending id, Gauss points in the reference's
+// order).  The price is that an element's Gauss-point gradients are formed
+// by each of its 8 nodes' warps.
+//
+// For the isotropic D of elastisomat (MEFEL/SRC/elastisomat.cpp:395-420),
+// with lambda = E nu / ((1+nu)(1-2nu)) and mu = E / (2 (1+nu)), block (a,b)
+// of sum_gp |J| B_a^T D B_b (linhex::gl_stiffness_matrix,
+// MEFEL/SRC/linhex.cpp:583-630) is
+//     K_ab = lambda P + mu P^T + mu tr(P) I,   P = sum_gp |J| g_a g_b^T
+// with g the Cartesian gradients of derivatives_3d (GEFEL/difcalc.cpp:487):
+// 24 FMA per block row instead of the full B^T D B product.
+// ---------------------------------------------------------------------------
+constexpr int kRowCap = 96;    // CSR entries of one row held in shared memory
+constexpr int kIncCap = 32;    // elements at one node
+constexpr int kElemBatch = 4;  // elements whose Gauss-point gradients a warp forms at once
+constexpr int kRowWarps = 4;   // warps per block of the row kernel
+
+struct HexRowShared {
+  double g[kElemBatch][8][8][3];  // [element][gp][node][x, y, z]
+  double w[kElemBatch][8];        // |detJ| (weights are 1)
+  double acc[3][kRowCap];         // the node's rows
+  int col[3][kRowCap];            // their column indices
+  int inc[kIncCap];               // incident elements, ascending
+};
+
+// gradients of the 8 shape functions and |detJ| at Gauss point gp (0..7,
+// xi outermost), as hex_gauss_point
+__device__ __forceinline__ void hex_gp_gradients(int gp, const double *x, const double *y, const double *z,
+                                                 double (*g)[3], double *w) {
+  const double xi = c_gp2[(gp >> 2) & 1], eta = c_gp2[(gp >> 1) & 1], zeta = c_gp2[gp & 1];
+  double nx[8], ny[8], nz[8];
+  hex_dnat(xi, eta, zeta, nx, ny, nz);
+  double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0;
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nz[a] * x[a];
+    d4 += nx[a] * y[a]; d5 += ny[a] * y[a]; d6 += nz[a] * y[a];
+    d7 += nx[a] * z[a]; d8 += ny[a] * z[a]; d9 += nz[a] * z[a];
+  }
+  const double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    const double ddx = nx[a], ddy = ny[a], ddz = nz[a];
+    g[a][0] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
+    g[a][1] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
+    g[a][2] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+  }
+  *w = fabs(jac);
+}
+
+// position of column c in the sorted shared row cols[0, len), or -1
+__device__ __forceinline__ int find_col_sh(const int *cols, int len, int c) {
+  int lo = 0, hi = len - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = cols[mid];
+    if (v == c) return mid;
+    if (v < c) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+// err bits: 4 an element entry has no CSR position; 32 a node exceeds
+// kIncCap elements or kRowCap entries per row (the caller falls back to the
+// colour-ordered kernel)
+__global__ void __launch_bounds__(kRowWarps * 32) k_hex8_rows(int64_t nn, const int *__restrict__ iptr,
+                                                              const int *__restrict__ inc,
+                                                              const double *__restrict__ coords,
+                                                              const int64_t *__restrict__ elems,
+                                                              const int *__restrict__ cne,
+                                                              const double *__restrict__ emat,
+                                                              const int *__restrict__ rowptr,
+                                                              const int *__restrict__ col,
+                                                              double *__restrict__ val, unsigned *err) {
+  __shared__ HexRowShared shm[kRowWarps];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexRowShared &sh = shm[wib];
+  for (int64_t node = blockIdx.x * (int64_t)kRowWarps + wib; node < nn; node += (int64_t)gridDim.x * kRowWarps) {
+    const int ib = iptr[node], deg = iptr[node + 1] - ib;
+    if (deg == 0) continue;
+    if (deg > kIncCap) {
+      if (lane == 0) atomicOr(err, 32u);
+      continue;
+    }
+    // incident elements in ascending order (distinct ids: rank sort)
+    const int mine = lane < deg ? inc[ib + lane] : INT_MAX;
+    int rank = 0;
+    for (int k = 0; k < deg; k++) rank += __shfl_sync(0xffffffffu, mine, k) < mine;
+    if (lane < deg) sh.inc[rank] = mine;
+    __syncwarp();
+    // the node's rows: its code numbers in its first element
+    int la0;
+    {
+      const int e0 = sh.inc[0];
+      const bool hit = lane < 8 && elems[(int64_t)e0 * 8 + lane] == node;
+      la0 = __ffs(__ballot_sync(0xffffffffu, hit)) - 1;
+      if (la0 < 0) la0 = 0;  // not reached for a consistent incidence
+    }
+    int r[3], len[3];
+    bool fits = true;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      r[i] = __ldg(cne + (int64_t)sh.inc[0] * 24 + 3 * la0 + i);
+      len[i] = 0;
+      if (r[i] >= 0) {
+        const int rb = __ldg(rowptr + r[i]);
+        len[i] = __ldg(rowptr + r[i] + 1) - rb;
+        if (len[i] > kRowCap) {
+          fits = false;
+        } else {
+          for (int k = lane; k < len[i]; k += 32) {
+            sh.col[i][k] = __ldg(col + rb + k);
+            sh.acc[i][k] = 0.0;
+          }
+        }
+      }
+    }
+    if (!fits) {
+      if (lane == 0) atomicOr(err, 32u);
+      __syncwarp();
+      continue;
+    }
+    if (r[0] < 0 && r[1] < 0 && r[2] < 0) {
+      __syncwarp();
+      continue;  // a fully constrained node has no rows
+    }
+    __syncwarp();
+    for (int q0 = 0; q0 < deg; q0 += kElemBatch) {
+      const int nb = min(kElemBatch, deg - q0);
+      {  // Gauss-point gradients of up to kElemBatch elements: lane = (element, gp)
+        const int el = lane >> 3, gp = lane & 7;
+        if (el < nb) {
+          const int e = sh.inc[q0 + el];
+          double x[8], y[8], z[8];
+#pragma unroll
+          for (int a = 0; a < 8; a++) {
+            const int64_t nd = __ldg(elems + (int64_t)e * 8 + a);
+            x[a] = __ldg(coords + 3 * nd);
+            y[a] = __ldg(coords + 3 * nd + 1);
+            z[a] = __ldg(coords + 3 * nd + 2);
+          }
+          hex_gp_gradients(gp, x, y, z, sh.g[el][gp], &sh.w[el][gp]);
+        }
+      }
+      __syncwarp();
+      for (int q = 0; q < nb; q++) {
+        const int e = sh.inc[q0 + q];
+        const bool hit = lane < 8 && elems[(int64_t)e * 8 + lane] == node;
+        int la = __ffs(__ballot_sync(0xffffffffu, hit)) - 1;
+        if (la < 0) la = 0;
+        const double E = __ldg(emat + 2 * (int64_t)e), nu = __ldg(emat + 2 * (int64_t)e + 1);
+        const double mu = E / 2.0 / (1.0 + nu);
+        const double lam = E / (1.0 + nu) / (1.0 - 2.0 * nu) * nu;
+        // lane (b, i), b = node of the element, i = row component: row i of
+        // P_b = sum_gp |J| g_la g_b^T
+        const int b = lane < 24 ? lane / 3 : 0, i = lane < 24 ? lane - 3 * (lane / 3) : 0;
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+        if (lane < 24) {
+#pragma unroll
+          for (int gp = 0; gp < 8; gp++) {
+            const double wa = sh.w[q][gp] * sh.g[q][gp][la][i];
+            p0 += wa * sh.g[q][gp][b][0];
+            p1 += wa * sh.g[q][gp][b][1];
+            p2 += wa * sh.g[q][gp][b][2];
+          }
+        }
+        // column i of P_b (rows k = 0..2 live in lanes 3b + k) and its trace
+        double pc[3], tr = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const int src = 3 * b + k;
+          const double t0 = __shfl_sync(0xffffffffu, p0, src);
+          const double t1 = __shfl_sync(0xffffffffu, p1, src);
+          const double t2 = __shfl_sync(0xffffffffu, p2, src);
+          pc[k] = i == 0 ? t0 : (i == 1 ? t1 : t2);
+          tr += k == 0 ? t0 : (k == 1 ? t1 : t2);
+        }
+        if (lane < 24 && r[i] >= 0) {
+          const double kr[3] = {lam * p0 + mu * pc[0] + (i == 0 ? mu * tr : 0.0),
+                                lam * p1 + mu * pc[1] + (i == 1 ? mu * tr : 0.0),
+                                lam * p2 + mu * pc[2] + (i == 2 ? mu * tr : 0.0)};
+          const int *cb = cne + (int64_t)e * 24 + 3 * b;
+          const int c0 = __ldg(cb), c1 = __ldg(cb + 1), c2 = __ldg(cb + 2);
+          const int *cols = sh.col[i];
+          double *acc = sh.acc[i];
+          bool done = false;
+          if (c0 >= 0 && c1 == c0 + 1 && c2 == c0 + 2) {  // a fully free node: one search
+            const int p = find_col_sh(cols, len[i], c0);
+            if (p >= 0 && p + 2 < len[i] && cols[p + 1] == c1 && cols[p + 2] == c2) {
+              acc[p] += kr[0];
+              acc[p + 1] += kr[1];
+              acc[p + 2] += kr[2];
+              done = true;
+            }
+          }
+          if (!done) {
+            const int cc[3] = {c0, c1, c2};
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+              if (cc[j] < 0) continue;
+              const int p = find_col_sh(cols, len[i], cc[j]);
+              if (p >= 0) acc[p] += kr[j];
+              else atomicOr(err, 4u);
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // every entry of the node's rows, written once
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      if (r[i] < 0) continue;
+      double *dst = val + __ldg(rowptr + r[i]);
+      for (int k = lane; k < len[i]; k += 32) dst[k] = sh.acc[i][k];
+    }
+    __syncwarp();
+  }
+}
+
 // tet4 elasticity (lintet::stiffness_matrix, MEFEL/SRC/lintet.cpp:290-315):
 // the linear tetrahedron's gradients are constant, so one integration point
 // with weight det3d/6 (GEFEL/matrix.cpp:3629) gives block (a,b) =
@@ -1151,20 +1381,17 @@ int scan_into(const In *len, Out *out, int64_t n, cudaStream_t s) {
   return SGPU_OK;
 }
 
-// The SCR pattern from the node adjacency when the code numbers grow with
-// (node, component) (gencodnum's numbering): node -> element incidence,
-// per-node sorted lower neighbours, row lengths, scan, fill.  Returns
-// SGPU_OK, or 1 when a node has too many candidate neighbours (the caller
-// uses the element-pair sort instead).  Writes m->src_adr / src_ci / src_negm.
-int pattern_adjacency(sgpu_matrix m, const int64_t *elems_d, const int64_t *cn_d, int64_t nn, int64_t ne, int nne,
-                      int ndofn, int64_t n, unsigned *err_d, cudaStream_t s) {
+// node -> element incidence: iptr[nn + 1] and the element ids of every node
+// (in no particular order) in inc[ne * nne].  Returns 1 when the incidence
+// does not fit int32 offsets.
+int build_incidence(const int64_t *elems_d, int64_t nn, int64_t ne, int nne, DevBuf<int> &iptr, DevBuf<int> &inc,
+                    cudaStream_t s) {
   const int64_t m_inc = ne * nne;
   if (m_inc > (1LL << 31) - 1) return 1;
-  AsyncBuf<int> cnt(s), iptr(s), cursor(s), inc(s), ucnt(s), nadj(s);
-  AsyncBuf<int64_t> nptr(s), rowlen(s);
+  AsyncBuf<int> cnt(s), cursor(s);
   SGPU_TRY(cnt.alloc(nn + 1));
-  SGPU_TRY(iptr.alloc(nn + 1));
   SGPU_TRY(cursor.alloc(nn));
+  SGPU_TRY(iptr.alloc(nn + 1));
   SGPU_TRY(inc.alloc(m_inc));
   SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, (nn + 1) * sizeof(int), s));
   SGPU_CUDA(cudaMemsetAsync(cursor.p, 0, nn * sizeof(int), s));
@@ -1172,11 +1399,26 @@ int pattern_adjacency(sgpu_matrix m, const int64_t *elems_d, const int64_t *cn_d
   count_launches(1);
   SGPU_TRY(scan_into(cnt.p, iptr.p, nn, s));
   k_inc_fill<<<blocks_for(m_inc), TPB, 0, s>>>(m_inc, nne, elems_d, iptr.p, cursor.p, inc.p);
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// The SCR pattern from the node adjacency when the code numbers grow with
+// (node, component) (gencodnum's numbering): from the node -> element
+// incidence (build_incidence), per-node sorted lower neighbours, row
+// lengths, scan, fill.  Returns
+// SGPU_OK, or 1 when a node has too many candidate neighbours (the caller
+// uses the element-pair sort instead).  Writes m->src_adr / src_ci / src_negm.
+int pattern_adjacency(sgpu_matrix m, const int64_t *elems_d, const int64_t *cn_d, int64_t nn, int nne, int ndofn,
+                      int64_t n, const int *iptr_d, const int *inc_d, unsigned *err_d, cudaStream_t s) {
+  AsyncBuf<int> ucnt(s), nadj(s);
+  AsyncBuf<int64_t> nptr(s), rowlen(s);
   SGPU_TRY(ucnt.alloc(nn + 1));
   SGPU_CUDA(cudaMemsetAsync(ucnt.p, 0, (nn + 1) * sizeof(int), s));
   const int gadj = (int)std::min<int64_t>((nn + WPB - 1) / WPB, (int64_t)kNumSMs * 32);
-  k_node_adj<false><<<gadj, TPB, 0, s>>>(nn, nne, elems_d, iptr.p, inc.p, ucnt.p, nullptr, nullptr, err_d);
-  count_launches(2);
+  k_node_adj<false><<<gadj, TPB, 0, s>>>(nn, nne, elems_d, iptr_d, inc_d, ucnt.p, nullptr, nullptr, err_d);
+  count_launches(1);
   unsigned e = 0;
   SGPU_TRY(read_err(err_d, s, &e));
   if (e & 16u) {
@@ -1189,7 +1431,7 @@ int pattern_adjacency(sgpu_matrix m, const int64_t *elems_d, const int64_t *cn_d
   SGPU_CUDA(cudaMemcpyAsync(&nadj_total, nptr.p + nn, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
   SGPU_TRY(nadj.alloc((size_t)nadj_total));
-  k_node_adj<true><<<gadj, TPB, 0, s>>>(nn, nne, elems_d, iptr.p, inc.p, nullptr, nptr.p, nadj.p, err_d);
+  k_node_adj<true><<<gadj, TPB, 0, s>>>(nn, nne, elems_d, iptr_d, inc_d, nullptr, nptr.p, nadj.p, err_d);
   SGPU_TRY(rowlen.alloc(n + 1));
   SGPU_CUDA(cudaMemsetAsync(rowlen.p, 0, (n + 1) * sizeof(int64_t), s));
   k_scr_rowlen<<<blocks_for(nn), TPB, 0, s>>>(nn, ndofn, cn_d, nptr.p, nadj.p, rowlen.p, n, err_d);
@@ -1220,6 +1462,11 @@ struct AssemblyData {
   DevBuf<int64_t> elems;
   DevBuf<int> cne, elist;
   std::vector<int> offsets;
+  // node -> element incidence, and whether every equation belongs to one
+  // (node, component) (gencodnum's consecutive numbering): the row kernel's
+  // precondition
+  DevBuf<int> iptr, inc;
+  bool node_rows = false;
 };
 
 int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
@@ -1228,9 +1475,27 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
   DevBuf<unsigned> err;
   SGPU_TRY(err.alloc(1));
   SGPU_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
-  SGPU_CUDA(cudaMemsetAsync(c.val.p, 0, (size_t)c.nnz * sizeof(double), s));
   SGPU_CUDA(cudaEventRecord(m->ev0, s));
-  const int ncol = (int)ad.offsets.size() - 1;
+  // isotropic hex8 elasticity on gencodnum's numbering: rows formed per node
+  // and written once (SGPU_ASSEMBLY_COLOURS=1 keeps the colour-ordered
+  // scatter, for comparisons)
+  bool rows_done = false;
+  if (kind == SGPU_ELEM_HEX8 && !ad.general && ad.node_rows && ad.iptr.p && !std::getenv("SGPU_ASSEMBLY_COLOURS")) {
+    const int grid = (int)std::min<int64_t>((ad.nn + kRowWarps - 1) / kRowWarps, (int64_t)kNumSMs * 64);
+    k_hex8_rows<<<grid, kRowWarps * 32, 0, s>>>(ad.nn, ad.iptr.p, ad.inc.p, ad.coords.p, ad.elems.p, ad.cne.p,
+                                                ad.emat.p, c.rowptr.p, c.col.p, c.val.p, err.p);
+    count_launches(1);
+    SGPU_CUDA(cudaGetLastError());
+    unsigned e = 0;
+    SGPU_TRY(read_err(err.p, s, &e));
+    if (e & 32u) {  // a node beyond the kernel's shared-memory capacity: colour-ordered scatter instead
+      SGPU_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
+    } else {
+      rows_done = true;
+    }
+  }
+  if (!rows_done) SGPU_CUDA(cudaMemsetAsync(c.val.p, 0, (size_t)c.nnz * sizeof(double), s));
+  const int ncol = rows_done ? 0 : (int)ad.offsets.size() - 1;
   for (int col = 0; col < ncol; col++) {
     const int beg = ad.offsets[col], cnt = ad.offsets[col + 1] - beg;
     if (cnt == 0) continue;
@@ -1428,8 +1693,14 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
     }
   }
   int adj_st = 1;
-  if (monotone && !std::getenv("SGPU_PATTERN_SORT")) {
-    adj_st = pattern_adjacency(m, ad.elems.p, cn_d.p, nn, ne, nne, ndofn, n, err.p, s);
+  int inc_st = 1;
+  if (monotone) {
+    inc_st = build_incidence(ad.elems.p, nn, ne, nne, ad.iptr, ad.inc, s);
+    if (inc_st != SGPU_OK && inc_st != 1) BAIL_ON(inc_st);
+    ad.node_rows = inc_st == SGPU_OK;
+  }
+  if (inc_st == SGPU_OK && !std::getenv("SGPU_PATTERN_SORT")) {
+    adj_st = pattern_adjacency(m, ad.elems.p, cn_d.p, nn, nne, ndofn, n, ad.iptr.p, ad.inc.p, err.p, s);
     if (adj_st != SGPU_OK && adj_st != 1) BAIL_ON(adj_st);
   }
   if (adj_st != SGPU_OK) {
@@ -1588,6 +1859,9 @@ SGPU_API int sgpu_assemble_copy(sgpu_matrix src, int32_t kind, const double *ema
   DUP(ad.emat, sa.emat);
   DUP(ad.thick, sa.thick);
   DUP(ad.rho, sa.rho);
+  DUP(ad.iptr, sa.iptr);
+  DUP(ad.inc, sa.inc);
+  ad.node_rows = sa.node_rows;
 #undef DUP
   if (st != SGPU_OK) return bail(st);
   if (c.val.alloc(c.nnz) != SGPU_OK || c.diag.alloc(c.n) != SGPU_OK) return bail(SGPU_CUDA_ERROR);

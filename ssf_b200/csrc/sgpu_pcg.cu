@@ -32,6 +32,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <type_traits>
+
 #include "sgpu_internal.cuh"
 
 namespace sgpu {
@@ -45,6 +47,26 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// Compensated FP32 dot-product accumulation (Dot2 of Ogita, Rump and Oishi,
+// 2005): every product is split exactly into its FP32 rounding and error
+// (TwoProduct with an FMA), every addition into its sum and error (Knuth's
+// TwoSum); the errors are summed apart and added at the end, so an FP32
+// sweep carries its sum to about twice FP32's precision.  The per-thread
+// results are combined in FP64 (exact for a float pair).
+struct Dot2F32 {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add_product(float a, float b) {
+    const float p = __fmul_rn(a, b);
+    const float pe = __fmaf_rn(a, b, -p);  // a b - p, exact
+    const float u = __fadd_rn(s, p);
+    const float bp = __fsub_rn(u, s);
+    const float e = __fadd_rn(__fsub_rn(s, __fsub_rn(u, bp)), __fsub_rn(p, bp));  // s + p - u, exact
+    s = u;
+    c = __fadd_rn(c, __fadd_rn(e, pe));
+  }
+  __device__ __forceinline__ double value() const { return (double)s + (double)c; }
+};
 
 // sum over the block; result valid in thread 0
 template <int NV>
@@ -195,6 +217,7 @@ __global__ void __launch_bounds__(TPB) k_spmv_csr(int n, const int *__restrict__
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double acc = 0.0;
+  Dot2F32 acc32;  // FP32 vectors: x.y in compensated FP32
   for (int base = warp * GPW; base < n; base += nwarps * GPW) {
     const int i = base + g;
     int b = 0, e = 0;
@@ -205,9 +228,11 @@ __global__ void __launch_bounds__(TPB) k_spmv_csr(int n, const int *__restrict__
     s = group_sum<AccT, L>(s);
     if (sub == 0 && i < n) {
       y[i] = (XT)s;
-      if (Epi::kDot) acc += (double)__ldg(x + i) * (double)(XT)s;
+      if constexpr (Epi::kDot && std::is_same<XT, float>::value) acc32.add_product(__ldg(x + i), (float)s);
+      else if (Epi::kDot) acc += (double)__ldg(x + i) * (double)(XT)s;
     }
   }
+  if constexpr (std::is_same<XT, float>::value) acc = acc32.value();
   if (Epi::kDot) {
     double v[1] = {acc}, t[1];
     if (reduce_grid<1>(v, partials, ticket, t)) Epi::finish(st, t[0]);
@@ -274,6 +299,7 @@ __global__ void __launch_bounds__(TPB, MINB) k_spmv_bsr3(int nb, const int *__re
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double acc = 0.0;
+  Dot2F32 acc32;  // FP32 vectors: x.y in compensated FP32
   for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
     const int br = base + g;
     int s = 0, nbr = 0;
@@ -315,9 +341,11 @@ __global__ void __launch_bounds__(TPB, MINB) k_spmv_bsr3(int nb, const int *__re
     if (sub < 3 && br < nb) {
       const AccT yv = sub == 0 ? y0 : (sub == 1 ? y1 : y2);
       y[3 * br + sub] = (XT)yv;
-      if (Epi::kDot) acc += (double)__ldg(x + 3 * br + sub) * (double)(XT)yv;
+      if constexpr (Epi::kDot && std::is_same<XT, float>::value) acc32.add_product(__ldg(x + 3 * br + sub), (float)yv);
+      else if (Epi::kDot) acc += (double)__ldg(x + 3 * br + sub) * (double)(XT)yv;
     }
   }
+  if constexpr (std::is_same<XT, float>::value) acc = acc32.value();
   if (Epi::kDot) {
     double v[1] = {acc}, t[1];
     if (reduce_grid<1>(v, partials, ticket, t)) Epi::finish(st, t[0]);
@@ -574,13 +602,14 @@ __global__ void __launch_bounds__(TPB) k_cg32_update(int n, float *__restrict__ 
                                                      PcgState *st, double *partials, unsigned *ticket) {
   if (stopped(st)) return;
   const float alpha = (float)st->alpha;
-  double v[1] = {0.0};
+  Dot2F32 rr_acc;  // r.r in compensated FP32
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     y32[i] += alpha * p32[i];
     const float ri = r32[i] - alpha * q32[i];
     r32[i] = ri;
-    v[0] += (double)ri * (double)ri;
+    rr_acc.add_product(ri, ri);
   }
+  double v[1] = {rr_acc.value()};
   double t[1];
   if (reduce_grid<1>(v, partials, ticket, t)) {
     const double rr = t[0];

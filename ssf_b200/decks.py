@@ -52,6 +52,14 @@ class Mesh:
              (x_global = T x_local), both row-major, for "ortho" (elastortomat)
     thick    (ne,) float64 element thickness (plane stress) or None
     loads    (nlc, nn, ndofn) float64 nodal forces per load case
+    eloads   None, or per load case a list of element loads (eid, flags,
+             values): a surface load of a hex8 (6 face flags, 1 = loaded in
+             the global system, and 6 x 4 nodes x 3 values) or an edge load
+             of a quad4 (4 edge flags, 4 x 2 nodes x 2 values), in the layout
+             loadel::readsurfaceload / readedgeload read
+             (MEFEL/SRC/loadel.cpp:204-279)
+    pd       None, or (nlc, npd) float64 prescribed displacements: a DOF flag
+             -k in dofflag takes pd[lc, k-1] (elprdispl, MEFEL/SRC/globmat.cpp:1372)
     """
 
     kind: str
@@ -64,6 +72,8 @@ class Mesh:
     thick: np.ndarray | None = None
     meta: dict = field(default_factory=dict)
     mtype: str = "iso"
+    eloads: list | None = None
+    pd: np.ndarray | None = None
 
     @property
     def nn(self) -> int:
@@ -81,12 +91,15 @@ class Mesh:
         """DOF numbering of ``gtopology::gencodnum`` (GEFEL/gtopology.cpp:1619).
 
         Nodes in order, DOFs of a node in order; every free DOF (flag 1) gets
-        the next 1-based number, fixed DOFs get 0.
+        the next 1-based number, fixed DOFs get 0 and DOFs with a prescribed
+        displacement keep their negative flag (-k: the k-th prescribed value).
         """
         flat = self.dofflag.reshape(-1)
         cn = np.zeros_like(flat)
         free = flat == 1
         cn[free] = np.arange(1, int(free.sum()) + 1)
+        neg = flat < 0
+        cn[neg] = flat[neg]
         return cn.reshape(self.dofflag.shape)
 
     @property
@@ -175,6 +188,59 @@ def cantilever_hex(nx=20, ny=4, nz=4, L=1.0, B=0.2, H=0.2, E=210e9, nu=0.3,
         loads=loads,
         meta=dict(nx=nx, ny=ny, nz=nz, L=L, B=B, H=H),
     )
+
+
+def cantilever_surface_traction(mesh: Mesh, traction=(0.0, 0.0, -1.0e6)) -> Mesh:
+    """The cantilever's end traction stated the way a SIFEL deck states a
+    surface load: an element load (surface, global system) on face 1 (xi = 1,
+    the x = L face) of every hexahedron of the last element layer, with the
+    traction vector at the face's 4 nodes; the nodal loads are dropped."""
+    nx = mesh.meta["nx"]
+    ny, nz = mesh.meta["ny"], mesh.meta["nz"]
+    # elements are numbered x fastest: the last layer is i = nx - 1
+    k, j = np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij")
+    last = (nx - 1) + nx * (j.ravel() + ny * k.ravel())
+    rec = []
+    for e in last:
+        vals = np.zeros(72)
+        vals[0:12] = np.tile(np.asarray(traction, dtype=float), 4)
+        rec.append((int(e), [1, 0, 0, 0, 0, 0], vals))
+    out = Mesh(**{**mesh.__dict__})
+    out.loads = np.zeros_like(mesh.loads[:1])
+    out.eloads = [rec]
+    return out
+
+
+def plate_edge_traction(mesh: Mesh, traction=(1.0, 0.0)) -> Mesh:
+    """The plate's right-edge load as element edge loads (edge 4: xi = 1,
+    from node 4 to node 1 of planeelemlq) with the load vector at both edge
+    nodes; the nodal loads are dropped."""
+    nx, ny = mesh.meta["nx"], mesh.meta["ny"]
+    last = (nx - 1) + nx * np.arange(ny)
+    rec = []
+    for e in last:
+        vals = np.zeros(16)
+        vals[12:16] = np.tile(np.asarray(traction, dtype=float), 2)
+        rec.append((int(e), [0, 0, 0, 1], vals))
+    out = Mesh(**{**mesh.__dict__})
+    out.loads = np.zeros_like(mesh.loads[:1])
+    out.eloads = [rec]
+    return out
+
+
+def prescribe(mesh: Mesh, nodes, comp: int, values) -> Mesh:
+    """Prescribed displacements: DOF `comp` of each node in `nodes` takes the
+    matching entry of `values` (one load case); the DOFs get the negative
+    flags -1, -2, ... of a SIFEL deck's constraint records."""
+    out = Mesh(**{**mesh.__dict__})
+    out.dofflag = mesh.dofflag.copy()
+    nodes = np.asarray(nodes, dtype=np.int64)
+    values = np.broadcast_to(np.asarray(values, dtype=float), nodes.shape)
+    base = 0 if mesh.pd is None else mesh.pd.shape[1]
+    out.dofflag[nodes, comp] = -(base + 1 + np.arange(nodes.size))
+    old = np.zeros((mesh.loads.shape[0], 0)) if mesh.pd is None else mesh.pd
+    out.pd = np.concatenate([old, np.tile(values, (mesh.loads.shape[0], 1))], axis=1)
+    return out
 
 
 def cantilever_top_loads(mesh: Mesh, nlc: int, seed: int = 1234, scale: float = 1.0e3) -> Mesh:
@@ -483,8 +549,21 @@ def write_mefel_deck(mesh: Mesh, path: str, storage: int = 11, ni: int = 20000,
         lines.append(f"{ld.size}")
         for i in ld:
             lines.append(f"{i + 1} " + " ".join(_fmt(v) for v in mesh.loads[lc, i]))
-        lines.append("0")  # loaded elements
-        lines.append("0")  # prescribed displacements
+        el = mesh.eloads[lc] if mesh.eloads else []
+        lines.append(f"{len(el)}")  # loaded elements: eid, load type, then per face / edge a flag and its values
+        for eid, flags, values in el:
+            tel = 3 if mesh.kind == "hex8" else 2  # surface (linhex) / edge (planeelemlq) load
+            per = 12 if mesh.kind == "hex8" else 4
+            toks = [str(int(eid) + 1), str(tel)]
+            for k, fl in enumerate(flags):
+                toks.append(str(int(fl)))
+                if fl > 0:
+                    toks += [_fmt(v) for v in values[per * k:per * (k + 1)]]
+            lines.append(" ".join(toks))
+        pdv = mesh.pd[lc] if mesh.pd is not None else np.zeros(0)
+        lines.append(f"{pdv.size}")  # prescribed displacements
+        if pdv.size:
+            lines.append(" ".join(_fmt(v) for v in pdv))
         lines.append("0")  # temperature changes
     lines.append("0")  # eigenstrains
     lines.append("0")  # textout

@@ -181,3 +181,49 @@ def test_rigid_body_modes_built_on_device(oracle, gpu_lib, which):
     assert abs(r1.info["iterations"] - r2.info["iterations"]) <= 1
     for x in (x1, x2):
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def _agg_solve(dm, f, mode, tail):
+    import os
+    old = os.environ.get("SGPU_AMG_TAIL")
+    os.environ["SGPU_AMG_TAIL"] = "1" if tail else "0"
+    try:
+        dm.precond_clear()
+        return dm.pcg(f, res=1e-22, prec="agg", mode=mode)
+    finally:
+        if old is None:
+            os.environ.pop("SGPU_AMG_TAIL", None)
+        else:
+            os.environ["SGPU_AMG_TAIL"] = old
+
+
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+@pytest.mark.parametrize("case", ["cantilever", "plate", "conduction"])
+def test_fused_coarse_tail_gives_the_same_bits(oracle, gpu_lib, mode, case):
+    # the last smoothed level and the dense level below it, run as one
+    # cluster launch per coarse correction, must give exactly the result of
+    # the separate kernels (same rows, same summation order)
+    if case == "cantilever":
+        m = decks.cantilever_hex(60, 12, 12)
+        adr, ci, a = _oracle_system(oracle, m)
+        f = oracle.load_vector(m)
+        B = mefel.rigid_body_modes(m)
+    elif case == "plate":
+        m = decks.plate_quad(96, 48, E=3e10, nu=0.22)
+        adr, ci, a = _oracle_system(oracle, m)
+        f = oracle.load_vector(m)
+        B = mefel.rigid_body_modes(m)
+    else:
+        m = decks.heat_cube(40, sigma=1.0)
+        with mefel.conductivity_matrix(m) as K:
+            adr, ci, a = K.download(symmetric=1)
+        f = np.random.default_rng(9).standard_normal(adr.size - 1)
+        B = np.ones((adr.size - 1, 1))
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(B)
+        x0, r0 = _agg_solve(dm, f, mode, tail=False)
+        x1, r1 = _agg_solve(dm, f, mode, tail=True)
+    assert r0.status == r1.status == L.OK
+    assert r1.info["precond_levels"] >= 3, "the hierarchy has no coarse tail to fuse"
+    assert r0.info["iterations"] == r1.info["iterations"]
+    assert np.array_equal(x0, x1)

@@ -239,3 +239,63 @@ def test_thickness_sets_and_load_cases_bit_exact(ref):
             assert np.array_equal(f, d["f"][lc * n:(lc + 1) * n])
             x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
             assert ani == d["meta"][f"ani_{lc}"] and np.array_equal(x, d["u"][lc * n:(lc + 1) * n])
+
+
+def _run_and_compare(ref, m):
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "d.in")
+        decks.write_mefel_deck(m, deck)
+        d = ref.run_mefel_dump(deck, td)
+    adr, ci, a = ref.assemble(m, sym=True)
+    assert np.array_equal(adr, d["K_adr"]) and np.array_equal(ci, d["K_ci"])
+    assert np.array_equal(a, d["K_a"])
+    f = ref.load_vector(m)
+    assert np.array_equal(f, d["f"][: f.size])
+    x, st, ani, ares = ref.scr_cg_prec(adr, ci, a, f, ni=20000, res=1e-20)
+    assert ani == d["meta"]["ani_0"] and np.array_equal(x, d["u"][: f.size])
+    return f, d
+
+
+def test_surface_traction_as_element_loads_bit_exact(ref):
+    # the 1 MPa end traction of the cantilever as hexahedron surface loads
+    # (linhex::node_forces_surf) on distorted faces; same f and u
+    m = decks.cantilever_surface_traction(decks.cantilever_hex(6, 2, 3))
+    rng = np.random.default_rng(44)
+    inner = ~np.isclose(m.coords[:, 0], 0.0)
+    m.coords = m.coords.copy()
+    m.coords[inner] += rng.uniform(-0.01, 0.01, (inner.sum(), 3))
+    f, _ = _run_and_compare(ref, m)
+    # the consistent forces of a uniform traction on the undistorted face
+    # equal the nodal loads cantilever_hex lumps by hand
+    u = decks.cantilever_hex(6, 2, 3)
+    assert np.allclose(ref.load_vector(decks.cantilever_surface_traction(u)), ref.load_vector(u), rtol=1e-12,
+                       atol=1e-9)
+
+
+def test_edge_load_and_prescribed_displacements_bit_exact(ref):
+    # quad edge loads on every edge kind, a second load case, and prescribed
+    # displacements on part of the clamped edge
+    m = decks.plate_quad(6, 4)
+    rng = np.random.default_rng(45)
+    m.coords = m.coords.copy()
+    m.coords[:, :2] += rng.uniform(-0.1, 0.1, (m.nn, 2))
+    rec = []
+    for e in range(m.ne):
+        flags = [int(v) for v in rng.integers(0, 2, 4)]
+        rec.append((e, flags, rng.standard_normal(16)))
+    m.eloads = [rec[: m.ne // 2], rec[m.ne // 2:]]
+    m.loads = np.concatenate([m.loads, rng.standard_normal((1, m.nn, 2))])
+    left = np.nonzero(np.isclose(decks.plate_quad(6, 4).coords[:, 0], 0.0))[0]
+    m = decks.prescribe(m, left[1:3], 0, [1e-4, -2e-4])
+    m = decks.prescribe(m, left[3:4], 1, [5e-5])
+    m.pd[1] *= -3.0
+    f, d = _run_and_compare(ref, m)
+    assert d["meta"]["nlc"] == 2
+    assert np.array_equal(ref.load_vector(m, 1), d["f"][f.size: 2 * f.size])
+
+
+def test_hex_prescribed_displacements_bit_exact(ref):
+    m = decks.cantilever_hex(5, 2, 2)
+    base = np.nonzero(np.isclose(m.coords[:, 0], 0.0))[0]
+    m = decks.prescribe(m, base[:4], 2, np.linspace(1e-5, 4e-5, 4))
+    _run_and_compare(ref, m)
