@@ -316,13 +316,37 @@ SGPU_API int sgpu_reassemble(sgpu_matrix m, int32_t kind, const double *emat, co
 SGPU_API int sgpu_assemble_copy(sgpu_matrix src, int32_t kind, const double *emat, const double *rho,
                                 sgpu_matrix *out, sgpu_assembly_info *info);
 
-/* Dirichlet lifting of TRFEL's assemble_init (TRFEL/SRC/globmatt.cpp:1635):
- * for a hex8 conduction handle made by sgpu_assemble, add -K_e r_e of every
- * element into rhs[n] (host, accumulated) at its free DOFs, where rnode[nn]
- * holds the nodal values prescvalues() gives (globmatt.cpp:1057): prescribed
- * values on prescribed nodes, initial values on free ones.  Time-constant
- * prescribed values only (the capacity part of the lifting is then zero). */
+/* Dirichlet lifting: add -K_e r_e of every element into rhs[n] (host,
+ * accumulated) at its free DOFs, for a handle made by sgpu_assemble.
+ *  - hex8 conduction handles: TRFEL's assemble_init
+ *    (TRFEL/SRC/globmatt.cpp:1635); rnode[nn] holds the nodal values
+ *    prescvalues() gives (globmatt.cpp:1057): prescribed values on prescribed
+ *    nodes, initial values on free ones.  Time-constant prescribed values
+ *    only (the capacity part of the lifting is then zero).
+ *  - hex8 and quad4 elasticity handles: MEFEL's prescribed displacements,
+ *    loadcase::prdisplcontrib (MEFEL/SRC/loadcase.cpp:615-664) with
+ *    elprdispl (globmat.cpp:1372); rnode[nn * ndofn] holds the prescribed
+ *    displacement of every DOF whose code number is negative (the load
+ *    case's pd[-code-1]) and 0 elsewhere; elements whose values are all zero
+ *    add nothing. */
 SGPU_API int sgpu_assembly_lift(sgpu_matrix m, const double *rnode, double *rhs);
+
+/* Element loads of a load case (loadcase::forcecontrib,
+ * MEFEL/SRC/loadcase.cpp:546-601, after the nodal loads): the consistent
+ * nodal forces of nle element-load records added into f[n] (host) at the
+ * elements' code numbers.  eid[nle] 0-based elements; for a hex8 mesh,
+ * surface loads (loadel type 3): flags nle x 6 (per face, in the order
+ * xi = 1, eta = 1, xi = -1, eta = -1, zeta = 1, zeta = -1: 1 loaded, 0 not)
+ * and values nle x 72 (face s: its 4 nodes x 3 components of the load in
+ * the global system at 12 s; node order as linhex::node_forces_surf,
+ * MEFEL/SRC/linhex.cpp:2543); for a quad4 mesh, edge loads (type 2): flags
+ * nle x 4 (edge e from node e to node e+1; 1 loaded) and values nle x 16
+ * (2 nodes x 2 components at 4 e; planeelemlq::nodeforces,
+ * MEFEL/SRC/plelemlq.cpp:2433).  Loads given in a local system (flag 2) are
+ * SGPU_BAD_INPUT.  Host computation; only mesh->kind, nn, coords, ne, elems
+ * and cn are read. */
+SGPU_API int sgpu_mesh_element_loads(const sgpu_mesh *mesh, int64_t nle, const int64_t *eid, const int32_t *flags,
+                                     const double *values, double *f);
 
 /* ------------------------------------------------------------------------ */
 /* Linear transient conduction                                              */
@@ -407,8 +431,10 @@ SGPU_API int sgpu_csr_pcg_noalloc_d(int32_t n, const int32_t *rowptr_d, const in
  * mechbclc::read) and gtopology::gencodnum (GEFEL/gtopology.cpp:1619) for the
  * decks of the hot path: linear statics, one element type of the
  * sgpu_elem_kind list, one material type (elisomat, elgmat3d, elortomat with
- * constant axes), constraint codes 0/1, nodal loads.  Other decks fail with
- * SGPU_BAD_INPUT naming the record or token. */
+ * constant axes), constraint codes 0 / 1 / -k (prescribed displacement k),
+ * nodal loads, element loads in the global system (linearhex surfaces,
+ * planeelementlq edges) and prescribed displacements.  Other decks fail
+ * with SGPU_BAD_INPUT naming the record or token. */
 typedef struct sgpu_deck_s *sgpu_deck;
 
 typedef struct {
@@ -455,10 +481,16 @@ SGPU_API int sgpu_deck_read_trfel(const char *path, int32_t threads, sgpu_deck *
 SGPU_API int sgpu_deck_get(sgpu_deck d, sgpu_deck_view *view);
 /* The deck as an sgpu_assemble input (pointers into the deck). */
 SGPU_API int sgpu_deck_mesh(sgpu_deck d, sgpu_mesh *mesh);
-/* Nodal loads of load case lc in equation order, f[n]
- * (mefel_right_hand_side, MEFEL/SRC/globmat.cpp:2369, for nodal forces);
- * MEFEL decks only. */
+/* Nodal and element loads of load case lc in equation order, f[n]
+ * (mefel_right_hand_side, MEFEL/SRC/globmat.cpp:2369: loadcase::forcecontrib;
+ * the element loads as sgpu_mesh_element_loads); MEFEL decks only.  The
+ * prescribed displacements' part is sgpu_assembly_lift of
+ * sgpu_deck_prescribed's values. */
 SGPU_API int sgpu_deck_rhs(sgpu_deck d, int32_t lc, double *f);
+/* Prescribed displacements of load case lc as nodal values r[nn * ndofn]
+ * (the load case's pd[-code-1] at every DOF with a negative constraint code,
+ * 0 elsewhere); *count (may be NULL) gets the number of such DOFs. */
+SGPU_API int sgpu_deck_prescribed(sgpu_deck d, int32_t lc, double *r, int64_t *count);
 SGPU_API void sgpu_deck_free(sgpu_deck d);
 
 /* ------------------------------------------------------------------------ */

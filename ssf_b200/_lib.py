@@ -152,6 +152,8 @@ SIGNATURES = {
     "sgpu_deck_get": ([_vp, C.POINTER(DeckView)], C.c_int),
     "sgpu_deck_mesh": ([_vp, C.POINTER(Mesh)], C.c_int),
     "sgpu_deck_rhs": ([_vp, _i32, _pD], C.c_int),
+    "sgpu_deck_prescribed": ([_vp, _i32, _pD, C.POINTER(_i64)], C.c_int),
+    "sgpu_mesh_element_loads": ([C.POINTER(Mesh), _i64, _vp, _vp, _vp, _pD], C.c_int),
     "sgpu_deck_free": ([_vp], None),
     "sgpu_last_error": ([], C.c_char_p),
     "sgpu_version": ([], C.c_char_p),

@@ -1307,6 +1307,193 @@ __global__ void __launch_bounds__(TPB) k_hex8t_lift(int ne_c, const int *__restr
   }
 }
 
+// MEFEL's prescribed displacements (loadcase::prdisplcontrib,
+// MEFEL/SRC/loadcase.cpp:615-664): rhs -= K_e r_e at the element's equations,
+// r_e the element's nodal values of rnode (nn x 3: the prescribed
+// displacement at a prescribed DOF, 0 elsewhere).  One warp per element, as
+// k_hex8_elastic: lane pair (a, b) forms block K_ab and K_ab r_b; the eight
+// lanes of a row node sum their products.  Elements whose r_e is zero add
+// nothing and return at once.  Colour-ordered: no two elements of a launch
+// share a node.
+template <bool GEN>
+__global__ void __launch_bounds__(TPB) k_hex8_lift(int ne_c, const int *__restrict__ elist,
+                                                   const double *__restrict__ coords,
+                                                   const int64_t *__restrict__ elems, const int *__restrict__ cne,
+                                                   const double *__restrict__ emat, const double *__restrict__ rnode,
+                                                   double *__restrict__ rhs) {
+  __shared__ HexShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexShared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double cx = 0, cy = 0, cz = 0, r0 = 0, r1 = 0, r2 = 0;
+    if (lane < 8) {
+      const int64_t nd = elems[(int64_t)e * 8 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1]; cz = coords[3 * nd + 2];
+      r0 = rnode[3 * nd]; r1 = rnode[3 * nd + 1]; r2 = rnode[3 * nd + 2];
+    }
+    if (!__any_sync(0xffffffffu, r0 != 0.0 || r1 != 0.0 || r2 != 0.0)) continue;
+    double x[8], y[8], z[8], r[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+      z[a] = __shfl_sync(0xffffffffu, cz, a);
+      r[a][0] = __shfl_sync(0xffffffffu, r0, a);
+      r[a][1] = __shfl_sync(0xffffffffu, r1, a);
+      r[a][2] = __shfl_sync(0xffffffffu, r2, a);
+    }
+    hex_gauss_point(lane, x, y, z, sh, false);
+    if (GEN) {
+      for (int q = lane; q < 36; q += 32) sh.D[q] = emat[36 * (int64_t)e + q];
+    }
+    __syncwarp();
+    double d0 = 0.0, d1 = 0.0, G = 0.0;
+    if (!GEN) {
+      const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+      G = E / 2.0 / (1.0 + nu);
+      const double sc = E / (1.0 + nu) / (1.0 - 2.0 * nu);
+      d0 = sc * (1 - nu);
+      d1 = sc * nu;
+    }
+    // lanes 0..31: (a, b) = (lane >> 3, lane & 7) and (4 + (lane >> 3), lane & 7)
+    double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int a = 4 * h + (lane >> 3), b = lane & 7;
+      double k[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+      for (int gp = 0; gp < 8; gp++) {
+        const double ax = sh.g[gp][a][0], ay = sh.g[gp][a][1], az = sh.g[gp][a][2];
+        const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1], bz = sh.g[gp][b][2];
+        const double w = sh.w[gp];
+        double db[6][3];
+        if (GEN) {
+          elastic_db(sh.D, bx, by, bz, db);
+        } else {
+          db[0][0] = d0 * bx; db[0][1] = d1 * by; db[0][2] = d1 * bz;
+          db[1][0] = d1 * bx; db[1][1] = d0 * by; db[1][2] = d1 * bz;
+          db[2][0] = d1 * bx; db[2][1] = d1 * by; db[2][2] = d0 * bz;
+          db[3][0] = 0.0;     db[3][1] = G * bz;  db[3][2] = G * by;
+          db[4][0] = G * bz;  db[4][1] = 0.0;     db[4][2] = G * bx;
+          db[5][0] = G * by;  db[5][1] = G * bx;  db[5][2] = 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          k[0][j] += w * (ax * db[0][j] + az * db[4][j] + ay * db[5][j]);
+          k[1][j] += w * (ay * db[1][j] + az * db[3][j] + ax * db[5][j]);
+          k[2][j] += w * (az * db[2][j] + ay * db[3][j] + ax * db[4][j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) f[h][i] = k[i][0] * r[b][0] + k[i][1] * r[b][1] + k[i][2] * r[b][2];
+    }
+    // sum over b: the 8 lanes of one row node
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) f[h][i] += __shfl_xor_sync(0xffffffffu, f[h][i], o);
+    if ((lane & 7) == 0) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int a = 4 * h + (lane >> 3);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          const int row = __ldg(cne + (int64_t)e * 24 + 3 * a + i);
+          if (row >= 0) rhs[row] -= f[h][i];
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// The same for the plane-stress quad (planeelemlq): rnode nn x 2; 16 lanes
+// (a, b) form K_ab r_b, the 4 lanes of a row node sum them.
+__global__ void __launch_bounds__(TPB) k_quad4_lift(int ne_c, const int *__restrict__ elist,
+                                                    const double *__restrict__ coords,
+                                                    const int64_t *__restrict__ elems, const int *__restrict__ cne,
+                                                    const double *__restrict__ emat, const double *__restrict__ thick,
+                                                    const double *__restrict__ rnode, double *__restrict__ rhs) {
+  __shared__ QuadShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  QuadShared &sh = shm[wib];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double x[4], y[4], cx = 0, cy = 0, r0 = 0, r1 = 0;
+    if (lane < 4) {
+      const int64_t nd = elems[(int64_t)e * 4 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1];
+      r0 = rnode[2 * nd]; r1 = rnode[2 * nd + 1];
+    }
+    if (!__any_sync(0xffffffffu, r0 != 0.0 || r1 != 0.0)) continue;
+    double r[4][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      x[a] = __shfl_sync(0xffffffffu, cx, a);
+      y[a] = __shfl_sync(0xffffffffu, cy, a);
+      r[a][0] = __shfl_sync(0xffffffffu, r0, a);
+      r[a][1] = __shfl_sync(0xffffffffu, r1, a);
+    }
+    const double t_e = thick[e];
+    if (lane < 4) {
+      const double xi = c_gp2[(lane >> 1) & 1], eta = c_gp2[lane & 1];
+      const double nx[4] = {0.25 * (1.0 + eta), 0.25 * (-1.0 - eta), 0.25 * (-1.0 + eta), 0.25 * (1.0 - eta)};
+      const double ny[4] = {0.25 * (1.0 + xi), 0.25 * (1.0 - xi), 0.25 * (-1.0 + xi), 0.25 * (-1.0 - xi)};
+      const double n[4] = {0.25 * (1.0 + xi) * (1.0 + eta), 0.25 * (1.0 - xi) * (1.0 + eta),
+                           0.25 * (1.0 - xi) * (1.0 - eta), 0.25 * (1.0 + xi) * (1.0 - eta)};
+      double d1 = 0, d2 = 0, d3 = 0, d4 = 0, th = 0;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nx[a] * y[a]; d4 += ny[a] * y[a];
+        th += n[a] * t_e;
+      }
+      const double jac = d1 * d4 - d2 * d3;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        sh.g[lane][a][0] = (nx[a] * d4 - ny[a] * d3) / jac;
+        sh.g[lane][a][1] = (ny[a] * d1 - nx[a] * d2) / jac;
+      }
+      sh.w[lane] = fabs(jac * th);
+    }
+    __syncwarp();
+    const double E = emat[2 * (int64_t)e], nu = emat[2 * (int64_t)e + 1];
+    const double c = E / (1.0 - nu * nu), d01 = c * nu, g3 = E / 2.0 / (1.0 + nu);
+    double f0 = 0.0, f1 = 0.0;
+    if (lane < 16) {
+      const int a = lane >> 2, b = lane & 3;
+      double k00 = 0, k01 = 0, k10 = 0, k11 = 0;
+#pragma unroll
+      for (int gp = 0; gp < 4; gp++) {
+        const double ax = sh.g[gp][a][0], ay = sh.g[gp][a][1];
+        const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1];
+        const double w = sh.w[gp];
+        const double db00 = c * bx, db01 = d01 * by, db10 = d01 * bx, db11 = c * by, db20 = g3 * by, db21 = g3 * bx;
+        k00 += w * (ax * db00 + ay * db20);
+        k01 += w * (ax * db01 + ay * db21);
+        k10 += w * (ay * db10 + ax * db20);
+        k11 += w * (ay * db11 + ax * db21);
+      }
+      f0 = k00 * r[b][0] + k01 * r[b][1];
+      f1 = k10 * r[b][0] + k11 * r[b][1];
+    }
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+      f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+      f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    }
+    if (lane < 16 && (lane & 3) == 0) {
+      const int a = lane >> 2;
+      const int row0 = __ldg(cne + (int64_t)e * 8 + 2 * a), row1 = __ldg(cne + (int64_t)e * 8 + 2 * a + 1);
+      if (row0 >= 0) rhs[row0] -= f0;
+      if (row1 >= 0) rhs[row1] -= f1;
+    }
+    __syncwarp();
+  }
+}
+
 int read_err(const unsigned *err_d, cudaStream_t s, unsigned *out) {
   SGPU_CUDA(cudaMemcpyAsync(out, err_d, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
@@ -1779,21 +1966,30 @@ SGPU_API int sgpu_assembly_lift(sgpu_matrix m, const double *rnode, double *rhs)
   if (!m || !m->asm_data) return fail(SGPU_BAD_INPUT, "handle was not created by sgpu_assemble");
   if (!rnode || !rhs) return fail(SGPU_BAD_INPUT, "null argument");
   AssemblyData &ad = m->asm_data->d;
-  if (ad.kind != SGPU_ELEM_HEX8T_K && ad.kind != SGPU_ELEM_HEX8T_C)
-    return fail(SGPU_BAD_INPUT, "lifting is defined for the hex8 conduction handles");
+  const bool scalar = ad.kind == SGPU_ELEM_HEX8T_K || ad.kind == SGPU_ELEM_HEX8T_C;
+  if (!scalar && ad.kind != SGPU_ELEM_HEX8 && ad.kind != SGPU_ELEM_QUAD4)
+    return fail(SGPU_BAD_INPUT, "lifting is defined for hex8 conduction, hex8 and quad4 elasticity handles");
   cudaStream_t s = m->stream;
   DevBuf<double> rn, f;
-  SGPU_TRY(rn.alloc(ad.nn));
+  const int64_t nr = ad.nn * ad.ndofn;
+  SGPU_TRY(rn.alloc(nr));
   SGPU_TRY(f.alloc(m->n));
-  SGPU_CUDA(cudaMemcpyAsync(rn.p, rnode, ad.nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  SGPU_CUDA(cudaMemcpyAsync(rn.p, rnode, nr * sizeof(double), cudaMemcpyHostToDevice, s));
   SGPU_CUDA(cudaMemcpyAsync(f.p, rhs, m->n * sizeof(double), cudaMemcpyHostToDevice, s));
   const int ncol = (int)ad.offsets.size() - 1;
   for (int col = 0; col < ncol; col++) {
     const int beg = ad.offsets[col], cnt = ad.offsets[col + 1] - beg;
     if (cnt == 0) continue;
     const int grid = std::min((cnt + WPB - 1) / WPB, kNumSMs * 16);
-    k_hex8t_lift<<<grid, TPB, 0, s>>>(cnt, ad.elist.p + beg, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, rn.p,
-                                      f.p);
+    const int *el = ad.elist.p + beg;
+    if (scalar)
+      k_hex8t_lift<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, rn.p, f.p);
+    else if (ad.kind == SGPU_ELEM_QUAD4)
+      k_quad4_lift<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p, rn.p, f.p);
+    else if (ad.general)
+      k_hex8_lift<true><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, rn.p, f.p);
+    else
+      k_hex8_lift<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, rn.p, f.p);
     count_launches(1);
   }
   SGPU_CUDA(cudaGetLastError());

@@ -23,12 +23,15 @@
 // Supported subset (anything else is SGPU_BAD_INPUT with the token index):
 // problem type linear statics with every optional computation off; storage
 // 10/11, solver cg, precond 0/1; nodes without cross-section or local
-// system; constraint codes 0 (fixed) and 1 (free); one element type per deck
+// system; constraint codes 0 (fixed), 1 (free) and -k (the k-th prescribed
+// displacement of each load case); one element type per deck
 // (lineartet 100, linearhex 102, quadrhex 103 with crst 0; planeelementlt 20,
 // planeelementlq 23, planeelementqq 24 with plane stress and a csplanestr
 // thickness set); one material type per deck (elisomat 1, elgmat3d 2,
-// elortomat 3 with constant transformation functions); nodal loads only;
-// no eigenstrains or output requests.
+// elortomat 3 with constant transformation functions); nodal loads, element
+// loads in the global system (surface loads of linearhex, edge loads of
+// planeelementlq) and prescribed displacements; no temperature changes,
+// eigenstrains or output requests.
 
 #include <algorithm>
 #include <atomic>
@@ -145,6 +148,12 @@ struct DeckData {
   FillVec<double> coords;
   FillVec<int64_t> elems, emat_id;
   std::vector<double> mats, thick, loads, emat2, dmat;
+  // per load case: element-load records (element, flags, values) and the
+  // prescribed displacements
+  std::vector<std::vector<int64_t>> le_eid;
+  std::vector<std::vector<int32_t>> le_flags;
+  std::vector<std::vector<double>> le_vals, pd;
+  int64_t max_pd = 0;  // largest prescribed-displacement index the constraints use
   std::vector<int64_t> dofflag, cn;
   double parse_ms = 0.0;
   // TRFEL
@@ -173,6 +182,11 @@ struct DeckData {
     return r.ec == std::errc() && (r.ptr == end() || blank(*r.ptr));
   }
 };
+
+// sgpu_loads.cu
+int add_element_loads(int kind, const double *coords, const int64_t *elems, const int64_t *cn, int64_t nn,
+                      int64_t ne, int64_t nle, const int64_t *eid, const int32_t *flags, const double *values,
+                      double *f);
 
 namespace {
 
@@ -396,22 +410,29 @@ int parse_mefel(DeckData &d) {
                                     " is not 'id x y z ndofn 0 0' with one DOF count per deck and unique ids");
   c.t += d.nn * 7;
 
-  // --- constraints: "id c1..c_ndofn" with 0 fixed, 1 free ---
+  // --- constraints: "id c1..c_ndofn" with 0 fixed, 1 free, -k prescribed ---
   d.dofflag.assign((size_t)d.nn * d.ndofn, 1);
   const int64_t ncn = c.i();
   if (!c.err.empty() || ncn < 0 || ncn > d.nn) return fail(SGPU_BAD_INPUT, "deck: bad constraint count");
+  std::atomic<int64_t> max_pd{0};
   bad = parallel_records(d, c.t, ncn, 1 + d.ndofn, [&](int64_t, int64_t t, bool &ok) {
     int64_t id = 0;
     ok = d.geti(t, id) && id >= 1 && id <= d.nn;
     for (int q = 0; ok && q < d.ndofn; q++) {
       int64_t v = 0;
-      ok = d.geti(t + 1 + q, v) && (v == 0 || v == 1);
+      ok = d.geti(t + 1 + q, v) && v <= 1 && v > -(1LL << 40);
       if (ok) d.dofflag[(size_t)(id - 1) * d.ndofn + q] = v;
+      if (ok && v < 0) {
+        int64_t cur = max_pd.load();
+        while (-v > cur && !max_pd.compare_exchange_weak(cur, -v)) {
+        }
+      }
     }
   });
   if (bad >= 0)
     return fail(SGPU_BAD_INPUT, "deck: constraint record " + std::to_string(bad + 1) +
-                                    " is not 'id c1..cn' with codes 0 (fixed) or 1 (free)");
+                                    " is not 'id c1..cn' with codes 0 (fixed), 1 (free) or -k (prescribed)");
+  d.max_pd = max_pd.load();
   c.t += ncn * (1 + d.ndofn);
 
   // --- elements: "id type [ssst] n1..nk cne crst [idcs] ntm tm idm" ---
@@ -540,8 +561,48 @@ int parse_mefel(DeckData &d) {
     }
     if (!ok) return fail(SGPU_BAD_INPUT, "deck: bad nodal load record in load case " + std::to_string(lc + 1));
     c.t += nl * (1 + d.ndofn);
-    c.expect(0, "loaded elements");
-    c.expect(0, "prescribed displacements");
+    // loaded elements (loadel::read, MEFEL/SRC/loadel.cpp:96): "eid type"
+    // then, for a surface load (3) of a linear hexahedron, per face a flag
+    // and 4 nodes x 3 values when the flag is 1 or 2; for an edge load (2) of
+    // a plane quad, per edge a flag and 2 nodes x 2 values when positive
+    const int64_t nle = c.i();
+    if (!c.err.empty() || nle < 0 || nle > d.ne)
+      return fail(SGPU_BAD_INPUT, "deck: bad loaded-element count in load case " + std::to_string(lc + 1));
+    d.le_eid.emplace_back();
+    d.le_flags.emplace_back();
+    d.le_vals.emplace_back();
+    const bool hexs = d.kind == SGPU_ELEM_HEX8, quade = d.kind == SGPU_ELEM_QUAD4;
+    const int nfl = hexs ? 6 : 4, per = hexs ? 12 : 4;
+    for (int64_t r = 0; r < nle; r++) {
+      const std::string rec = "deck: loaded element " + std::to_string(r + 1) + " of load case " + std::to_string(lc + 1);
+      const int64_t eid = c.i(), tel = c.i();
+      if (!c.err.empty()) return fail(SGPU_BAD_INPUT, rec + ": " + c.err);
+      if (eid < 1 || eid > d.ne) return fail(SGPU_BAD_INPUT, rec + ": element out of range");
+      if (!((hexs && tel == 3) || (quade && tel == 2)))
+        return fail(SGPU_BAD_INPUT, rec + ": load type " + std::to_string(tel) +
+                                        " is not supported (surface loads of linearhex, edge loads of planeelementlq)");
+      d.le_eid.back().push_back(eid - 1);
+      for (int k = 0; k < nfl; k++) {
+        const int64_t fl = c.i();
+        if (!c.err.empty()) return fail(SGPU_BAD_INPUT, rec + ": " + c.err);
+        if (hexs && fl != 0 && fl != 1)
+          return fail(SGPU_BAD_INPUT, rec + ": surface flag " + std::to_string(fl) +
+                                          " (only 0 and 1, loads in the global system, are supported)");
+        if (fl < 0) return fail(SGPU_BAD_INPUT, rec + ": negative edge flag");
+        d.le_flags.back().push_back((int32_t)fl);
+        for (int q = 0; q < per; q++) d.le_vals.back().push_back(fl > 0 ? c.f() : 0.0);
+        if (!c.err.empty()) return fail(SGPU_BAD_INPUT, rec + ": " + c.err);
+      }
+    }
+    // prescribed displacements (loadcase::read, MEFEL/SRC/loadcase.cpp:135-140)
+    const int64_t npd = c.i();
+    if (!c.err.empty() || npd < 0 || npd > (int64_t)d.nn * d.ndofn)
+      return fail(SGPU_BAD_INPUT, "deck: bad prescribed-displacement count in load case " + std::to_string(lc + 1));
+    if (npd < d.max_pd)
+      return fail(SGPU_BAD_INPUT, "deck: load case " + std::to_string(lc + 1) + " has " + std::to_string(npd) +
+                                      " prescribed displacements, the constraints use " + std::to_string(d.max_pd));
+    d.pd.emplace_back((size_t)npd, 0.0);
+    for (int64_t k = 0; k < npd; k++) d.pd.back()[(size_t)k] = c.f();
     c.expect(0, "temperature changes");
     if (!c.err.empty()) return fail(SGPU_BAD_INPUT, "deck: " + c.err);
   }
@@ -557,8 +618,10 @@ int parse_mefel(DeckData &d) {
   // --- code numbers (gtopology::gencodnum, GEFEL/gtopology.cpp:1619) ---
   d.cn.assign(d.dofflag.size(), 0);
   int64_t next = 0;
-  for (size_t q = 0; q < d.dofflag.size(); q++)
+  for (size_t q = 0; q < d.dofflag.size(); q++) {
     if (d.dofflag[q] == 1) d.cn[q] = ++next;
+    else if (d.dofflag[q] < 0) d.cn[q] = d.dofflag[q];  // gencodnum keeps the prescribed index
+  }
   d.n = next;
   if (d.n == 0) return fail(SGPU_BAD_INPUT, "deck: no free DOFs");
 
@@ -960,6 +1023,30 @@ SGPU_API int sgpu_deck_rhs(sgpu_deck h, int32_t lc, double *f) {
   const double *L = &d.loads[(size_t)lc * d.nn * d.ndofn];
   for (size_t q = 0; q < d.cn.size(); q++)
     if (d.cn[q] > 0) f[d.cn[q] - 1] += L[q];
+  // then the element loads, record by record (loadcase::forcecontrib)
+  if ((size_t)lc < d.le_eid.size() && !d.le_eid[(size_t)lc].empty())
+    return add_element_loads(d.kind, d.coords.data(), d.elems.data(), d.cn.data(), d.nn, d.ne,
+                             (int64_t)d.le_eid[(size_t)lc].size(), d.le_eid[(size_t)lc].data(),
+                             d.le_flags[(size_t)lc].data(), d.le_vals[(size_t)lc].data(), f);
+  return SGPU_OK;
+}
+
+SGPU_API int sgpu_deck_prescribed(sgpu_deck h, int32_t lc, double *r, int64_t *count) {
+  if (!h || !r) return fail(SGPU_BAD_INPUT, "null argument");
+  const DeckData &d = h->d;
+  if (d.problem != 1) return fail(SGPU_BAD_INPUT, "prescribed displacements belong to MEFEL decks");
+  if (lc < 0 || lc >= d.nlc) return fail(SGPU_BAD_INPUT, "load case out of range");
+  int64_t k = 0;
+  const std::vector<double> &pd = d.pd[(size_t)lc];
+  for (size_t q = 0; q < d.dofflag.size(); q++) {
+    const int64_t c = d.dofflag[q];
+    r[q] = 0.0;
+    if (c < 0) {
+      r[q] = pd[(size_t)(-c - 1)];
+      k++;
+    }
+  }
+  if (count) *count = k;
   return SGPU_OK;
 }
 

@@ -152,13 +152,54 @@ def rigid_body_modes(mesh) -> np.ndarray:
     return B
 
 
-def mefel_right_hand_side(mesh, lc: int = 0) -> np.ndarray:
-    """Nodal forces of load case ``lc`` in equation order."""
+def _element_loads_into(mesh, lc: int, f: np.ndarray) -> None:
+    """Adds load case lc's element loads (hex8 surfaces, quad4 edges) into f
+    through the library (sgpu_mesh_element_loads)."""
+    recs = mesh.eloads[lc] if mesh.eloads else []
+    if not recs:
+        return
+    nfl = 6 if mesh.kind == "hex8" else 4
+    eid = _c([r[0] for r in recs], np.int64)
+    flags = _c(np.concatenate([np.asarray(r[1]).reshape(nfl) for r in recs]), np.int32)
+    vals = _c(np.concatenate([np.asarray(r[2], dtype=np.float64).reshape(-1) for r in recs]), np.float64)
+    coords = _c(mesh.coords, np.float64)
+    elems = _c(mesh.elems, np.int64)
+    cn = _c(mesh.code_numbers(), np.int64)
+    m = L.Mesh(KIND[mesh.kind], cn.shape[1], coords.shape[0], coords.ctypes.data, elems.shape[0],
+               elems.ctypes.data, cn.ctypes.data, None, None, None, None)
+    L.check(L.lib().sgpu_mesh_element_loads(C.byref(m), eid.size, eid.ctypes.data, flags.ctypes.data,
+                                            vals.ctypes.data, f))
+
+
+def prescribed_displacements(mesh, lc: int = 0) -> np.ndarray | None:
+    """Nodal prescribed displacements of load case lc (nn x ndofn: the value
+    at a DOF flagged -k, 0 elsewhere), or None when the mesh has none."""
+    neg = mesh.dofflag < 0
+    if not neg.any():
+        return None
+    r = np.zeros(mesh.dofflag.shape)
+    r[neg] = mesh.pd[lc][-mesh.dofflag[neg] - 1]
+    return r
+
+
+def mefel_right_hand_side(mesh, lc: int = 0, K: DeviceMatrix | None = None) -> np.ndarray:
+    """Right-hand side of load case ``lc`` in equation order, as
+    loadcase::assemble (MEFEL/SRC/loadcase.cpp:400) forms it: nodal forces,
+    the element loads' nodal forces (loadcase::forcecontrib, :546), and for
+    prescribed displacements -K_e r_e over the elements that have them
+    (prdisplcontrib, :615) -- formed on the GPU from the assembled handle K,
+    which a mesh with prescribed displacements must pass."""
     cn = mesh.code_numbers().reshape(-1)
     f = np.zeros(mesh.ndof)
     vals = mesh.loads[lc].reshape(-1)
     m = cn > 0
     np.add.at(f, cn[m] - 1, vals[m])
+    _element_loads_into(mesh, lc, f)
+    r = prescribed_displacements(mesh, lc)
+    if r is not None:
+        if K is None:
+            raise ValueError("prescribed displacements need the assembled stiffness matrix (argument K)")
+        L.check(L.lib().sgpu_assembly_lift(K.h, _c(r, np.float64), f))
     return f
 
 
@@ -174,11 +215,11 @@ def solve_linear_statics(mesh, ni=100000, res=1e-20, mode="fp64", batched=None):
     out, results = [], []
     try:
         if batched:
-            F = np.stack([mefel_right_hand_side(mesh, lc) for lc in range(nlc)], axis=1)
+            F = np.stack([mefel_right_hand_side(mesh, lc, K) for lc in range(nlc)], axis=1)
             X, results = pcg_multi(K, F, ni=ni, res=res)
             return X.T.copy(), results
         for lc in range(nlc):
-            f = mefel_right_hand_side(mesh, lc)
+            f = mefel_right_hand_side(mesh, lc, K)
             x, r = K.pcg(f, ni=ni, res=res, crit="scr", prec=1, mode=mode)
             out.append(x)
             results.append(r)
@@ -247,9 +288,20 @@ class Deck:
         dm.assembly = info.as_dict()
         return dm
 
-    def rhs(self, lc: int = 0) -> np.ndarray:
+    def rhs(self, lc: int = 0, K: DeviceMatrix | None = None) -> np.ndarray:
+        """Load case lc's right-hand side: nodal and element loads
+        (sgpu_deck_rhs), then the prescribed displacements' -K_e r_e on the
+        GPU when the deck has any (K: the deck's assembled matrix)."""
         f = np.zeros(self.view.n)
         L.check(L.lib().sgpu_deck_rhs(self.h, int(lc), f))
+        if self.front == "mefel":
+            r = np.zeros(self.view.nn * self.view.ndofn)
+            cnt = C.c_int64(0)
+            L.check(L.lib().sgpu_deck_prescribed(self.h, int(lc), r, C.byref(cnt)))
+            if cnt.value:
+                if K is None:
+                    raise ValueError("the deck prescribes displacements: pass its stiffness matrix K")
+                L.check(L.lib().sgpu_assembly_lift(K.h, r, f))
         return f
 
     def close(self):
@@ -290,7 +342,7 @@ def solve_deck(path: str, prec=None, mode="fp64", threads: int = 0, nullspace: b
                 L.check(L.lib().sgpu_matrix_set_rigid_body_modes(K.h, v.nn, v.ndofn, v.coords, v.cn))
             out, results = [], []
             for lc in range(d.info["nlc"]):
-                x, r = K.pcg(d.rhs(lc), ni=d.info["ni"], res=d.info["res"], crit=crit, prec=p, mode=mode)
+                x, r = K.pcg(d.rhs(lc, K), ni=d.info["ni"], res=d.info["res"], crit=crit, prec=p, mode=mode)
                 out.append(x)
                 results.append(r)
         finally:

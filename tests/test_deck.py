@@ -273,3 +273,81 @@ def test_integers_with_a_leading_plus(tmp_path):
     open(p, "w").write("\n".join(lines) + "\n")
     with pytest.raises(L.SgpuError, match="node record 1|integer expected"):
         mefel.Deck(p)
+
+
+def _loaded_decks():
+    # element loads and prescribed displacements as a SIFEL deck states them
+    hx = decks.cantilever_surface_traction(decks.cantilever_hex(5, 2, 2))
+    hx.coords = hx.coords + np.random.default_rng(3).uniform(-0.004, 0.004, hx.coords.shape)
+    yield "hex8_surface", hx
+    q = decks.plate_quad(5, 4)
+    rng = np.random.default_rng(4)
+    q.eloads = [[(e, [int(v) for v in rng.integers(0, 2, 4)], rng.standard_normal(16)) for e in range(q.ne)]]
+    yield "quad4_edges", q
+    p = decks.prescribe(decks.cantilever_hex(4, 2, 2), [0, 1, 2], 2, [1e-4, 2e-4, 3e-4])
+    yield "hex8_prescribed", p
+
+
+@pytest.mark.parametrize("name,m", list(_loaded_decks()))
+def test_element_loads_and_prescribed_codes_read_back(oracle, tmp_path, name, m):
+    # the reader's right-hand side (nodal + element loads, host code) equals
+    # the oracle's loadcase::assemble bit for bit when nothing is prescribed,
+    # and the prescribed values come back per DOF
+    from ssf_b200 import mefel
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    with mefel.Deck(p, threads=2) as d:
+        r = d.mesh()
+        assert np.array_equal(r.dofflag, m.dofflag)
+        assert np.array_equal(r.code_numbers(), m.code_numbers())
+        f = np.zeros(d.view.n)
+        from ssf_b200 import _lib as L
+        L.check(L.lib().sgpu_deck_rhs(d.h, 0, f))
+        rr = np.zeros(d.view.nn * d.view.ndofn)
+        import ctypes as C
+        cnt = C.c_int64(-1)
+        L.check(L.lib().sgpu_deck_prescribed(d.h, 0, rr, C.byref(cnt)))
+    want = mefel.prescribed_displacements(m, 0)
+    if want is None:
+        assert cnt.value == 0 and not rr.any()
+        assert np.array_equal(f, oracle.load_vector(m, 0))
+    else:
+        assert cnt.value == int((m.dofflag < 0).sum()) and np.array_equal(rr, want.reshape(-1))
+    # the mesh-level entry point adds the same element loads after the nodal
+    # ones (the oracle's order): bit for bit
+    if m.eloads and want is None:
+        m0 = decks.Mesh(**{**m.__dict__})
+        m0.eloads = None
+        g = oracle.load_vector(m0, 0)
+        mefel._element_loads_into(m, 0, g)
+        assert np.array_equal(g, oracle.load_vector(m, 0))
+
+
+@pytest.mark.parametrize("edit,match", [
+    (lambda ln: ln.replace(" 3 1 ", " 3 2 ", 1), "surface flag 2"),
+    (lambda ln: ln.replace(" 3 1 ", " 1 1 ", 1), "load type 1"),
+])
+def test_unsupported_element_loads_fail(tmp_path, edit, match):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.cantilever_surface_traction(decks.cantilever_hex(3, 2, 2))
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    lines = open(p).read().split("\n")
+    first = f"{m.eloads[0][0][0] + 1} 3 1 "  # the first loaded-element record: "eid 3 1 values ..."
+    k = next(i for i, ln in enumerate(lines) if ln.startswith(first))
+    lines[k] = edit(lines[k])
+    open(p, "w").write("\n".join(lines))
+    with pytest.raises(L.SgpuError, match=match):
+        mefel.Deck(p)
+
+
+def test_prescribed_index_beyond_the_load_case_fails(tmp_path):
+    from ssf_b200 import _lib as L
+    from ssf_b200 import mefel
+    m = decks.prescribe(decks.cantilever_hex(3, 2, 2), [0, 1], 2, [1e-4, 2e-4])
+    m.pd = m.pd[:, :1]  # the constraints name value 2, the load case has 1
+    p = str(tmp_path / "d.in")
+    decks.write_mefel_deck(m, p)
+    with pytest.raises(L.SgpuError, match="prescribed displacements"):
+        mefel.Deck(p)
