@@ -18,10 +18,13 @@ lists; their build system is not run) and writes every output under
   plus ``oracle/ref_solver_capi.cpp``: a C entry point into the reference's
   own ``symcomprow::cg_prec`` / ``comprow::cg_prec`` for timing the CPU
   baseline on exactly the arrays the GPU path receives;
-* ``mefel_dump_gpu``                   -- the MEFEL harness and SIFEL's objects
-  linked with the drop-in binding ``ssf_b200/integration/sifel_gpu_shim.cpp``
-  (``-Wl,--wrap`` of ``symcomprow::cg_prec``): SIFEL's own front end on a deck,
-  with the solve on the GPU.  Run only by the drop-in test.
+* ``mefel_dump_gpu`` / ``trfel_dump_gpu`` -- the MEFEL / TRFEL harness and
+  SIFEL's objects linked with the drop-in binding
+  ``ssf_b200/integration/sifel_gpu_shim.cpp`` (``-Wl,--wrap`` of
+  ``symcomprow::cg_prec``) and, for MEFEL, the assembly binding
+  ``ssf_b200/integration/sifel_gpu_assembly.cpp`` (``-Wl,--wrap`` of
+  ``stiffness_matrix``): SIFEL's own front end on a deck, with the assembly
+  and the solves on the GPU.  Run only by the drop-in tests.
 
 Only one compile-environment shim is needed: ``GEFEL/cc.cpp`` includes
 ``umfpack.h`` unconditionally although every use sits under ``INC_CHMD``;
@@ -164,16 +167,20 @@ def build(ref: str, jobs: int) -> None:
     gef_objs = [o for m in GEFEL_PARTS for o in objs[m]]
     run([CXX, "-shared", "-o", os.path.join(OUT, "libsifelref.so"), harness_objs["capi"],
          *gef_objs, "-lm", "-ldl"])
-    build_dropin(ref, harness_objs["mefel"], libmef, libgef, syslibs)
+    build_dropin(ref, harness_objs["mefel"], libmef, libgef, syslibs, harness_objs["trfel"], libtrf)
 
 
 WRAP = "_ZN10symcomprow7cg_precEPdS0_ldRlRddlldP7ISolver"
+WRAP_ASM = "_Z16stiffness_matrixl"  # stiffness_matrix(long), MEFEL/SRC/globmat.cpp:41
 
 
-def build_dropin(ref, harness_obj, libmef, libgef, syslibs):
-    """mefel_dump_gpu: the same harness and SIFEL objects, linked with the
-    drop-in binding (ssf_b200/integration/sifel_gpu_shim.cpp) so that
-    symcomprow::cg_prec runs on the GPU through libsifelgpu.so."""
+def build_dropin(ref, harness_obj, libmef, libgef, syslibs, trfel_obj=None, libtrf=None):
+    """mefel_dump_gpu / trfel_dump_gpu: the same harnesses and SIFEL objects,
+    linked with the drop-in binding (ssf_b200/integration/sifel_gpu_shim.cpp)
+    so that symcomprow::cg_prec -- MEFEL's load-case solves and every TRFEL
+    time step's solve -- runs on the GPU through libsifelgpu.so; the MEFEL
+    program also takes the assembly binding
+    (ssf_b200/integration/sifel_gpu_assembly.cpp: stiffness_matrix on the GPU)."""
     root = os.path.dirname(HERE)
     lib_dir = os.path.join(root, "ssf_b200")
     if not os.path.exists(os.path.join(lib_dir, "libsifelgpu.so")):
@@ -182,8 +189,17 @@ def build_dropin(ref, harness_obj, libmef, libgef, syslibs):
     shim_obj = os.path.join(OUT, "obj", "sifel_gpu_shim.o")
     run([CXX, *CXXFLAGS, f"-I{os.path.join(ref, 'GEFEL')}", f"-I{os.path.join(ref, 'GEFEL', 'SPARSE')}",
          f"-I{os.path.join(root, 'include')}", f"-I{os.path.join(HERE, 'ref_compat')}", "-c", shim, "-o", shim_obj])
-    run([CXX, "-o", os.path.join(OUT, "mefel_dump_gpu"), harness_obj, shim_obj, libmef, libgef,
-         f"-Wl,--wrap={WRAP}", f"-L{lib_dir}", "-lsifelgpu", "-Wl,-rpath,$ORIGIN/../../ssf_b200", *syslibs])
+    asm = os.path.join(root, "ssf_b200", "integration", "sifel_gpu_assembly.cpp")
+    asm_obj = os.path.join(OUT, "obj", "sifel_gpu_assembly.o")
+    inc = [os.path.join(ref, d) for d in MODULES["mefel"][1]] + [os.path.join(ref, MODULES["mefel"][0])]
+    run([CXX, *CXXFLAGS, *[f"-I{d}" for d in inc], f"-I{os.path.join(ref, 'GEFEL', 'SPARSE')}",
+         f"-I{os.path.join(root, 'include')}", f"-I{os.path.join(HERE, 'ref_compat')}", "-c", asm, "-o", asm_obj])
+    run([CXX, "-o", os.path.join(OUT, "mefel_dump_gpu"), harness_obj, shim_obj, asm_obj, libmef, libgef,
+         f"-Wl,--wrap={WRAP}", f"-Wl,--wrap={WRAP_ASM}", f"-L{lib_dir}", "-lsifelgpu",
+         "-Wl,-rpath,$ORIGIN/../../ssf_b200", *syslibs])
+    if trfel_obj is not None:
+        run([CXX, "-o", os.path.join(OUT, "trfel_dump_gpu"), trfel_obj, shim_obj, libtrf, libgef,
+             f"-Wl,--wrap={WRAP}", f"-L{lib_dir}", "-lsifelgpu", "-Wl,-rpath,$ORIGIN/../../ssf_b200", *syslibs])
 
 
 def main() -> None:
