@@ -1046,8 +1046,11 @@ __global__ void k_mis_init(int nb, const int *__restrict__ cand, uint64_t *__res
 
 // max of the keys over the closed neighbourhood; with `agg`, only over the
 // subgraph of the nodes not yet aggregated (agg < 0)
+// (go: the undecided count the previous round left; 0 = nothing to do)
 __global__ void k_mis_max(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
-                          const int *__restrict__ agg, const uint64_t *__restrict__ in, uint64_t *__restrict__ out) {
+                          const int *__restrict__ agg, const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
+                          const int *go) {
+  if (*go == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
     uint64_t m = in[i];
     for (int e = browptr[i]; e < browptr[i + 1]; e++) {
@@ -1070,8 +1073,9 @@ __global__ void k_mis_cand(int nb, const int *__restrict__ browptr, const int *_
   }
 }
 
-__global__ void k_mis_decide(int nb, uint64_t *__restrict__ t, const uint64_t *__restrict__ m2,
+__global__ void k_mis_decide(int nb, uint64_t *__restrict__ t, const uint64_t *__restrict__ m2, const int *go,
                              int *__restrict__ undecided) {
+  if (*go == 0) return;
   int cnt = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
     const uint64_t ti = t[i];
@@ -1641,26 +1645,31 @@ int read_int(const int *d, cudaStream_t s, int *out) {
 // on return the roots have state 2 in t.
 int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t, cudaStream_t s) {
   const int nb = L.nb, g = grid_for(nb);
+  constexpr int kMaxRounds = 200, kGroup = 8;
   TmpBuf<uint64_t> m1(s), m2(s);
   TmpBuf<int> cnt(s);
   SGPU_TRY(m1.alloc(nb));
   SGPU_TRY(m2.alloc(nb));
-  SGPU_TRY(cnt.alloc(1));
+  // cnt[r]: the nodes round r left undecided; cnt[0] a non-zero start.  A
+  // round whose predecessor left none returns at once, so the host enqueues
+  // kGroup rounds and reads the count once per group.
+  SGPU_TRY(cnt.alloc(kMaxRounds + 1));
+  SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, (kMaxRounds + 1) * sizeof(int), s));
+  SGPU_CUDA(cudaMemsetAsync(cnt.p, 0x01, sizeof(int), s));
   k_mis_init<<<g, TPB, 0, s>>>(nb, cand, t.p);
   count_launches(1);
   int undecided = nb, rounds = 0;
   while (undecided > 0) {
-    if (++rounds > 200) return fail(SGPU_CUDA_ERROR, "aggregation: independent-set rounds did not finish");
-    SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), s));
-    // two rounds per check of the undecided count
-    for (int k = 0; k < 2; k++) {
-      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p);
-      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, m2.p);
-      k_mis_decide<<<g, TPB, 0, s>>>(nb, t.p, m2.p, cnt.p);
+    if (rounds + kGroup > kMaxRounds) return fail(SGPU_CUDA_ERROR, "aggregation: independent-set rounds did not finish");
+    for (int k = 0; k < kGroup; k++, rounds++) {
+      const int *go = cnt.p + rounds;
+      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go);
+      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, m2.p, go);
+      k_mis_decide<<<g, TPB, 0, s>>>(nb, t.p, m2.p, go, cnt.p + rounds + 1);
       count_launches(3);
     }
     SGPU_CUDA(cudaGetLastError());
-    SGPU_TRY(read_int(cnt.p, s, &undecided));
+    SGPU_TRY(read_int(cnt.p + rounds, s, &undecided));
   }
   return SGPU_OK;
 }
@@ -1964,6 +1973,33 @@ double tridiag_lmax(const std::vector<double> &a, const std::vector<double> &b) 
   return hi;
 }
 
+// Enqueues `steps` Lanczos steps on M = D^-1/2 A D^-1/2 on stream s; the
+// coefficients land in ab[0..steps) (alpha) and ab[64..] (beta).  w0..w2, u,
+// y: work vectors of L.n.
+template <typename T>
+int lanczos_enqueue(sgpu_matrix m, const AmgLevel &L, cudaStream_t s, int steps, T *w0, T *w1, T *w2, T *u, T *y,
+                    double *ab) {
+  T *w[3] = {w0, w1, w2};
+  const T *dsq = level_dsq<T>(L);
+  Work &wk = m->w;
+  const int g = grid_for(L.n);
+  k_rand_vec<T><<<g, TPB, 0, s>>>(L.n, y);
+  k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y, nullptr, nullptr, dsq, ab, 0, w[0], u, wk.partials.p,
+                                   wk.counters.p + 7, ab + 64);
+  count_launches(2);
+  for (int j = 0; j < steps; j++) {
+    OpLanczos<T> op{dsq, w[j % 3], ab + 64 + j, y, ab + j};
+    SGPU_TRY(launch_level<T>(m, L, u, op, s, 5));
+    k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y, w[j % 3], j > 0 ? w[(j + 2) % 3] : nullptr, dsq, ab, j,
+                                     w[(j + 1) % 3], u, wk.partials.p, wk.counters.p + 7, ab + 64 + j + 1);
+    count_launches(1);
+  }
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+int lanczos_finish(const std::vector<double> &h, int steps, double *lmax);
+
 // lmax of D^-1 A (= that of the symmetric D^-1/2 A D^-1/2) by `steps`
 // Lanczos steps; the host reads the coefficients once at the end
 template <typename T>
@@ -1977,24 +2013,15 @@ int lanczos_lmax(sgpu_matrix m, const AmgLevel &L, cudaStream_t s, int steps, do
   SGPU_TRY(u.alloc(L.n));
   SGPU_TRY(y.alloc(L.n));
   SGPU_TRY(ab.alloc(129));
-  T *w[3] = {w0.p, w1.p, w2.p};
-  const T *dsq = level_dsq<T>(L);
-  Work &wk = m->w;
-  const int g = grid_for(L.n);
-  k_rand_vec<T><<<g, TPB, 0, s>>>(L.n, y.p);
-  k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y.p, nullptr, nullptr, dsq, ab.p, 0, w[0], u.p, wk.partials.p,
-                                   wk.counters.p + 7, ab.p + 64);
-  count_launches(2);
-  for (int j = 0; j < steps; j++) {
-    OpLanczos<T> op{dsq, w[j % 3], ab.p + 64 + j, y.p, ab.p + j};
-    SGPU_TRY(launch_level<T>(m, L, u.p, op, s, 5));
-    k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y.p, w[j % 3], j > 0 ? w[(j + 2) % 3] : nullptr, dsq, ab.p, j,
-                                     w[(j + 1) % 3], u.p, wk.partials.p, wk.counters.p + 7, ab.p + 64 + j + 1);
-    count_launches(1);
-  }
+  SGPU_TRY(lanczos_enqueue<T>(m, L, s, steps, w0.p, w1.p, w2.p, u.p, y.p, ab.p));
   std::vector<double> h(129);
   SGPU_CUDA(cudaMemcpyAsync(h.data(), ab.p, 129 * sizeof(double), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
+  return lanczos_finish(h, steps, lmax);
+}
+
+// the largest eigenvalue of the Lanczos tridiagonal matrix of h
+int lanczos_finish(const std::vector<double> &h, int steps, double *lmax) {
   std::vector<double> a(h.begin(), h.begin() + steps), b(steps, 0.0);
   for (int j = 1; j < steps; j++) b[j] = h[64 + j];
   for (int j = 0; j < steps; j++)
@@ -2069,6 +2096,23 @@ int amg_build(sgpu_matrix m) {
   }
   L0->n = n;
   L0->unit_diag = true;
+  if (A.l0_bound_wanted) {
+    // the FP32 cycle's level-0 smoother bound needs only the scaled FP32
+    // matrix: its Lanczos steps (bandwidth-bound SpMVs) run on a second
+    // stream while the aggregation (latency-bound rounds with host reads)
+    // runs here; amg_prepare_precision collects it.  Neither touches the
+    // other's buffers (the set-up kernels use no reduction partials).
+    if (!A.side) SGPU_CUDA(cudaStreamCreateWithFlags(&A.side, cudaStreamNonBlocking));
+    if (!A.fork) SGPU_CUDA(cudaEventCreateWithFlags(&A.fork, cudaEventDisableTiming));
+    SGPU_TRY(A.lz32.alloc((size_t)5 * n));
+    SGPU_TRY(A.lz_ab.alloc(129));
+    SGPU_CUDA(cudaEventRecord(A.fork, s));
+    SGPU_CUDA(cudaStreamWaitEvent(A.side, A.fork, 0));
+    float *z = A.lz32.p;
+    SGPU_TRY(lanczos_enqueue<float>(m, *L0, A.side, std::max(2, std::min(A.lanczos_steps, 63)), z, z + n, z + 2 * n,
+                                    z + 3 * (size_t)n, z + 4 * (size_t)n, A.lz_ab.p));
+    A.l0_bound_pending = true;
+  }
   const int K = A.k0 > 0 ? A.k0 : L0->b;
   TmpBuf<double> Bcur(s), Bnext(s);
   SGPU_TRY(Bcur.alloc((size_t)n * K));
@@ -2165,7 +2209,15 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
         count_launches(1);
       }
       clk.mark("fp32 copies");
-      SGPU_TRY(lanczos_lmax<float>(m, L, s, A.lanczos_steps, &L.lmax32));
+      if (l == 0 && A.l0_bound_pending) {
+        A.l0_bound_pending = false;
+        std::vector<double> h(129);
+        SGPU_CUDA(cudaMemcpyAsync(h.data(), A.lz_ab.p, 129 * sizeof(double), cudaMemcpyDeviceToHost, A.side));
+        SGPU_CUDA(cudaStreamSynchronize(A.side));
+        SGPU_TRY(lanczos_finish(h, std::max(2, std::min(A.lanczos_steps, 63)), &L.lmax32));
+      } else {
+        SGPU_TRY(lanczos_lmax<float>(m, L, s, A.lanczos_steps, &L.lmax32));
+      }
       clk.mark("Lanczos bound");
       if (getenv("SGPU_AMG_VERBOSE")) fprintf(stderr, "amg level %zu: lmax (fp32) %.6g\n", l, L.lmax32);
     }
@@ -2641,7 +2693,16 @@ int amg_ensure(sgpu_matrix m, bool fp32, float *setup_ms) {
     PcgState zero_st{};
     SGPU_TRY(write_st(m, &zero_st));  // set-up kernels run with a live state
   }
-  if (!A.built) SGPU_TRY(amg_build(m));
+  A.l0_bound_wanted = fp32 && !A.built && !getenv("SGPU_AMG_SERIAL_BOUND");
+  if (!A.built) {
+    const int rc = amg_build(m);
+    if (rc != SGPU_OK) {
+      if (A.side) cudaStreamSynchronize(A.side);
+      A.l0_bound_pending = false;
+      return rc;
+    }
+  }
+  A.l0_bound_wanted = false;
   SGPU_TRY(amg_prepare_precision(m, fp32));
   SGPU_CUDA(cudaEventRecord(m->ev1, s));
   SGPU_CUDA(cudaEventSynchronize(m->ev1));

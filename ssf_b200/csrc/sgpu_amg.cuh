@@ -110,8 +110,22 @@ struct Amg {
   // level objects by depth, kept when a hierarchy is discarded so that a
   // rebuild of the same matrix reuses their device buffers
   std::vector<AmgLevel *> pool;
+  // the level-0 smoother bound of an FP32 cycle, run on a second stream
+  // while the aggregation set-up runs on the handle's (amg_build); its
+  // workspace stays with the handle
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr;
+  bool l0_bound_pending = false;
+  bool l0_bound_wanted = false;
+  DevBuf<float> lz32;    // 5 vectors of n
+  DevBuf<double> lz_ab;  // Lanczos coefficients
   ~Amg() {
     for (AmgLevel *l : pool) delete l;
+    if (side) {
+      cudaStreamSynchronize(side);
+      cudaStreamDestroy(side);
+    }
+    if (fork) cudaEventDestroy(fork);
   }
   void clear() {
     lv.clear();

@@ -1,5 +1,6 @@
-// Many independent systems of uneven size in one launch sequence: batched
-// Jacobi-PCG over a block-diagonal matrix.
+// Many independent systems of uneven size: batched Jacobi-PCG over a
+// block-diagonal matrix, as one persistent launch (the default) or as a
+// graph of segmented launches per iteration.
 //
 // The uneven batch (hundreds of plane-stress plates of different sizes, each
 // its own symcomprow::cg_prec in the reference, GEFEL/scr.cpp:1093) is held
@@ -16,6 +17,7 @@
 // short autotuning run on the batch itself.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -255,6 +257,195 @@ __global__ void __launch_bounds__(TPB) k_bdir(int nsegs, const Seg *__restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// the persistent form: one CTA per system at a time
+//
+// The systems are independent, so a CTA can run a whole system's iteration
+// alone -- SpMV, the two reductions, the updates -- separated by CTA
+// barriers only: no grid-wide step, no launch per iteration, and a converged
+// system costs nothing.  CTAs take systems from a queue (largest first, so
+// the longest solves start early) through one atomic counter; the kernel
+// ends when the queue is empty.  Nothing waits on another CTA.  Each system's
+// sums are formed in a fixed order (thread, then warp, then block), so a
+// solve is repeatable bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int PTPB = 512;
+
+__device__ __forceinline__ void cta_sum2(double &a, double &b, double (*sh)[PTPB / 32]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if (lane == 0) {
+    sh[0][w] = a;
+    sh[1][w] = b;
+  }
+  __syncthreads();
+  double ta = 0.0, tb = 0.0;
+  for (int k = 0; k < PTPB / 32; k++) {  // every thread sums the warp totals in order
+    ta += sh[0][k];
+    tb += sh[1][k];
+  }
+  a = ta;
+  b = tb;
+}
+
+template <int L>
+__global__ void __launch_bounds__(PTPB, 2) k_bpersist(int nsys, const int *__restrict__ order,
+                                                      const long long *__restrict__ sysptr, int *next,
+                                                      const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                      const double *__restrict__ val, const double *__restrict__ diag,
+                                                      const double *__restrict__ f, double *__restrict__ x,
+                                                      double *__restrict__ r, double *__restrict__ h,
+                                                      double *__restrict__ d, double *__restrict__ p, SysState *st,
+                                                      long long ni, double res, double zero) {
+  __shared__ double sh[2][PTPB / 32];
+  __shared__ int q_s;
+  constexpr int GPW = 32 / L;
+  const int lane = threadIdx.x & 31, g = lane / L, sub = lane % L, w = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) q_s = atomicAdd(next, 1);
+    __syncthreads();
+    const int q = q_s;
+    __syncthreads();
+    if (q >= nsys) return;
+    const int k = order[q];
+    const int r0 = (int)sysptr[k], r1 = (int)sysptr[k + 1];
+    // start from x = 0: r = f, h = r/diag, d = h; f.f and r.h
+    double a = 0.0, b = 0.0;
+    for (int i = r0 + threadIdx.x; i < r1; i += PTPB) {
+      const double fi = f[i], hi = fi / diag[i];
+      x[i] = 0.0;
+      r[i] = fi;
+      h[i] = hi;
+      d[i] = hi;
+      a += fi * fi;
+      b += fi * hi;
+    }
+    cta_sum2(a, b, sh);
+    SysState s = {};
+    s.nory = a;
+    s.nom = b;
+    s.ani = -1;
+    if (a < zero) {  // scr.cpp:1117-1120: reported, the iteration goes on
+      s.status = SGPU_ZERO_RHS;
+      s.ares = a;
+      s.ani = 0;
+      s.ani_set = 1;
+    }
+    if (ni <= 0) s.done = 1;
+    while (!s.done) {
+      __syncthreads();  // d complete
+      // p = A d and d.p
+      double dp = 0.0, unused = 0.0;
+      for (int base = r0 + w * GPW; base < r1; base += (PTPB / 32) * GPW) {
+        const int i = base + g;
+        const int ii = i < r1 ? i : r1 - 1;  // every lane shuffles
+        const double y = row_dot<L>(ii, rowptr, col, val, d, sub);
+        if (sub == 0 && i < r1) {
+          p[i] = y;
+          dp += d[i] * y;
+        }
+      }
+      cta_sum2(dp, unused, sh);
+      s.denom = dp;
+      if (fabs(dp) < zero) {  // scr.cpp:1146-1151
+        s.ani = s.it;
+        s.ares = s.nom;
+        s.ani_set = 1;
+        if (s.status == 0) s.status = SGPU_BREAKDOWN;
+        s.done = 1;
+        break;
+      }
+      const double alpha = s.nom / dp;
+      // x += alpha d; r -= alpha p; h = r/diag; r.r and r.h
+      double rr = 0.0, rh = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += PTPB) {
+        x[i] += alpha * d[i];
+        const double ri = r[i] - alpha * p[i], hi = ri / diag[i];
+        r[i] = ri;
+        h[i] = hi;
+        rr += ri * ri;
+        rh += ri * hi;
+      }
+      cta_sum2(rr, rh, sh);
+      s.alpha = alpha;
+      s.rr = rr;
+      s.beta = rh / s.nom;
+      s.nom = rh;
+      const long long it = s.it;
+      s.it = it + 1;
+      if (fabs(rr / s.nory) < res) {  // scr.cpp:1188
+        s.ani = it;
+        s.ares = rh / s.nory;
+        s.ani_set = 1;
+        s.done = 1;
+        break;
+      }
+      if (it + 1 >= ni) {
+        s.done = 1;
+        if (s.status == 0) s.status = SGPU_NOT_CONVERGED;
+        break;
+      }
+      const double beta = s.beta;
+      for (int i = r0 + threadIdx.x; i < r1; i += PTPB) d[i] = beta * d[i] + h[i];
+    }
+    if (threadIdx.x == 0) st[k] = s;
+    __syncthreads();
+  }
+}
+
+// the persistent solve of every system; hs gets the per-system results
+int run_persistent(sgpu_matrix m, const std::vector<int64_t> &rows, int L, double *x, const double *f, double *r,
+                   double *h, double *d, double *p, int64_t ni, double res, double zero, std::vector<SysState> &hs,
+                   int64_t *iters, float *ms) {
+  cudaStream_t s = m->stream;
+  const Csr &c = m->csr;
+  const int nsys = (int)rows.size();
+  std::vector<long long> ptr(nsys + 1, 0);
+  for (int k = 0; k < nsys; k++) ptr[k + 1] = ptr[k] + rows[k];
+  std::vector<int> order(nsys);
+  for (int k = 0; k < nsys; k++) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rows[a] > rows[b]; });
+  DevBuf<long long> ptr_d;
+  DevBuf<int> order_d, next_d;
+  DevBuf<SysState> st;
+  SGPU_TRY(ptr_d.alloc(nsys + 1));
+  SGPU_TRY(order_d.alloc(nsys));
+  SGPU_TRY(next_d.alloc(1));
+  SGPU_TRY(st.alloc(nsys));
+  SGPU_CUDA(cudaMemcpyAsync(ptr_d.p, ptr.data(), (nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
+  SGPU_CUDA(cudaMemcpyAsync(order_d.p, order.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, s));
+  SGPU_CUDA(cudaMemsetAsync(next_d.p, 0, sizeof(int), s));
+  const int grid = std::min(nsys, kNumSMs * 2);
+  SGPU_CUDA(cudaEventRecord(m->ev0, s));
+  switch (L) {
+    case 4:
+      k_bpersist<4><<<grid, PTPB, 0, s>>>(nsys, order_d.p, ptr_d.p, next_d.p, c.rowptr.p, c.col.p, c.val.p, c.diag.p,
+                                          f, x, r, h, d, p, st.p, (long long)ni, res, zero);
+      break;
+    case 16:
+      k_bpersist<16><<<grid, PTPB, 0, s>>>(nsys, order_d.p, ptr_d.p, next_d.p, c.rowptr.p, c.col.p, c.val.p,
+                                           c.diag.p, f, x, r, h, d, p, st.p, (long long)ni, res, zero);
+      break;
+    default:
+      k_bpersist<8><<<grid, PTPB, 0, s>>>(nsys, order_d.p, ptr_d.p, next_d.p, c.rowptr.p, c.col.p, c.val.p, c.diag.p,
+                                          f, x, r, h, d, p, st.p, (long long)ni, res, zero);
+      break;
+  }
+  count_launches(1);
+  SGPU_CUDA(cudaGetLastError());
+  SGPU_CUDA(cudaEventRecord(m->ev1, s));
+  hs.resize(nsys);
+  SGPU_CUDA(cudaMemcpyAsync(hs.data(), st.p, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  if (ms) SGPU_CUDA(cudaEventElapsedTime(ms, m->ev0, m->ev1));
+  int64_t mx = 0;
+  for (const SysState &q : hs) mx = std::max<int64_t>(mx, q.it);
+  if (iters) *iters = mx;
+  return SGPU_OK;
+}
+
 struct Plan {
   int S = 1024, L = 8;
 };
@@ -390,8 +581,12 @@ extern "C" SGPU_API int sgpu_matrix_pcg_batch(sgpu_matrix m, int32_t nsys, const
   SGPU_CUDA(cudaMemcpyAsync(w.f.p, f, n * sizeof(double), cudaMemcpyHostToDevice, s));
   // the plan: segment rows S and lanes per row L; tuned on ~32 iterations of
   // this batch when asked (the iterate is reset for the real solve)
+  // SGPU_BATCH_FORM=graph: the segmented graph-of-launches form below;
+  // otherwise the persistent form (one CTA per system at a time)
+  const char *form = getenv("SGPU_BATCH_FORM");
+  const bool persistent = !(form && !strcmp(form, "graph"));
   Plan best;
-  if (tune) {
+  if (tune && !persistent) {
     float best_ms = 1e30f;
     for (int S : {512, 1024, 2048, 4096})
       for (int L : {4, 8, 16}) {
@@ -405,13 +600,22 @@ extern "C" SGPU_API int sgpu_matrix_pcg_batch(sgpu_matrix m, int32_t nsys, const
         if (ms < best_ms) { best_ms = ms; best = Plan{S, L}; }
       }
   }
-  Batch b;
-  SGPU_TRY(build_segments(rows, best.S, b, s));
-  SGPU_CUDA(cudaMemsetAsync(w.x.p, 0, n * sizeof(double), s));
   std::vector<SysState> hs;
   float ms = 0.f;
   int64_t its = 0;
-  SGPU_TRY(run_batch(m, b, best, w.x.p, w.f.p, w.r.p, w.h.p, w.d.p, w.p.p, ni, res, zero, hs, &its, &ms));
+  if (persistent) {
+    // lanes per row from the rows' mean length
+    const double mean = (double)m->csr.nnz / (double)m->n;
+    best.L = mean > 40 ? 16 : (mean > 12 ? 8 : 4);
+    best.S = 0;
+    SGPU_TRY(run_persistent(m, rows, best.L, w.x.p, w.f.p, w.r.p, w.h.p, w.d.p, w.p.p, ni, res, zero, hs, &its,
+                            &ms));
+  } else {
+    Batch b;
+    SGPU_TRY(build_segments(rows, best.S, b, s));
+    SGPU_CUDA(cudaMemsetAsync(w.x.p, 0, n * sizeof(double), s));
+    SGPU_TRY(run_batch(m, b, best, w.x.p, w.f.p, w.r.p, w.h.p, w.d.p, w.p.p, ni, res, zero, hs, &its, &ms));
+  }
   SGPU_CUDA(cudaMemcpyAsync(x, w.x.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
   int worst = SGPU_OK;

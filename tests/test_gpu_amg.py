@@ -227,3 +227,27 @@ def test_fused_coarse_tail_gives_the_same_bits(oracle, gpu_lib, mode, case):
     assert r1.info["precond_levels"] >= 3, "the hierarchy has no coarse tail to fuse"
     assert r0.info["iterations"] == r1.info["iterations"]
     assert np.array_equal(x0, x1)
+
+
+def test_overlapped_smoother_bound_gives_the_same_bits(oracle, gpu_lib):
+    # the level-0 smoother bound of the FP32 cycle runs on a second stream
+    # beside the aggregation set-up; the same Lanczos steps, so the same
+    # hierarchy and the same solve as the serial set-up
+    import os
+    m = decks.cantilever_hex(40, 8, 8)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    out = []
+    for serial in (True, False):
+        if serial:
+            os.environ["SGPU_AMG_SERIAL_BOUND"] = "1"
+        try:
+            with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+                dm.set_nullspace(mefel.rigid_body_modes(m))
+                out.append(dm.pcg(f, res=1e-22, prec="agg", mode="mixed"))
+        finally:
+            os.environ.pop("SGPU_AMG_SERIAL_BOUND", None)
+    (x0, r0), (x1, r1) = out
+    assert r0.status == r1.status == L.OK
+    assert r0.info["iterations"] == r1.info["iterations"]
+    assert np.array_equal(x0, x1)

@@ -193,6 +193,41 @@ def test_uneven_batch_matches_oracle(oracle, gpu_lib):
         assert np.linalg.norm(xs[k] - xo) / np.linalg.norm(xo) <= 1e-8
 
 
+@pytest.mark.parametrize("form", ["persistent", "graph"])
+def test_uneven_batch_forms_agree(oracle, gpu_lib, form):
+    # the persistent form (one CTA per system, no launch per iteration) and
+    # the segmented graph form are the same iteration per system: the same
+    # statuses, iteration counts within the rounding of the dot products, and
+    # the oracle's solutions; one plate carries a zero load (its own
+    # zero-right-hand-side exit)
+    import os
+    from ssf_b200 import mefel
+    rng = np.random.default_rng(22)
+    plates = [decks.plate_quad(int(a), int(b), E=float(e), nu=float(v), traction=1e6)
+              for a, b, e, v in zip(rng.integers(2, 30, 23), rng.integers(2, 30, 23), rng.uniform(1e9, 1e11, 23),
+                                    rng.uniform(0.2, 0.35, 23))]
+    plates[5].loads = np.zeros_like(plates[5].loads)
+    old = os.environ.get("SGPU_BATCH_FORM")
+    os.environ["SGPU_BATCH_FORM"] = form
+    try:
+        xs, out = mefel.solve_batch(plates, res=1e-20, tune=False)
+    finally:
+        if old is None:
+            os.environ.pop("SGPU_BATCH_FORM", None)
+        else:
+            os.environ["SGPU_BATCH_FORM"] = old
+    for k, p in enumerate(plates):
+        adr, ci, a = oracle.assemble(p, sym=True)
+        f = oracle.load_vector(p)
+        xo, st, ani_o, ares_o = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-20)
+        if k == 5:
+            assert out["status"][k] == L.ZERO_RHS and not xs[k].any() and out["ani"][k] == ani_o == 0
+            continue
+        assert st == 0 and out["status"][k] == L.OK
+        assert abs(int(out["ani"][k]) - ani_o) <= 2
+        assert np.linalg.norm(xs[k] - xo) / np.linalg.norm(xo) <= 1e-8
+
+
 def test_sliced_ell_in_the_solves(oracle, gpu_lib):
     # a scalar conduction matrix (rows of similar length): the sliced ELL
     # SpMV pinned for the FP64 Jacobi-PCG and for the transient steps' combined
