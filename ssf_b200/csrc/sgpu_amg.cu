@@ -274,11 +274,10 @@ struct OpStorePQ {
 // handle keeps them): LPR lanes per block row
 // (6 resident blocks per SM for FP32 -- 40 registers; 4 for FP64, whose
 // operators with the outer coupling need more registers)
-template <typename T, int LPR, class Op>
-__global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? 4 : 6) k_lv_bsr3(int nb, const int *__restrict__ browptr,
-                                                   const int *__restrict__ bcol, const T *__restrict__ bval,
-                                                   const T *__restrict__ v, Op op, PcgState *st,
-                                                   double *partials, unsigned *ticket) {
+template <typename T, int LPR, class Op, int UNR = 2>
+__global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? 4 : (UNR > 2 ? 4 : 6))
+    k_lv_bsr3(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol, const T *__restrict__ bval,
+              const T *__restrict__ v, Op op, PcgState *st, double *partials, unsigned *ticket) {
   if (st->done) return;
   constexpr int RPW = 32 / LPR;
   const int lane = threadIdx.x & 31, g = lane / LPR, sub = lane % LPR;
@@ -292,6 +291,27 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? 4 : 6) k_lv_bsr3(int nb,
     const T *bv = bval + 9ll * s;
     T y0 = 0, y1 = 0, y2 = 0;
     int j = sub;
+    if constexpr (UNR == 4) {
+      // four blocks of the row in flight per lane: twice the loads of the
+      // two-block loop before the first x gather depends on them
+      for (; j + 3 * LPR < nbr; j += 4 * LPR) {
+        int c[4];
+        T a[4][9];
+#pragma unroll
+        for (int u = 0; u < 4; u++) c[u] = __ldcs(bcol + s + j + u * LPR);
+#pragma unroll
+        for (int q = 0; q < 9; q++)
+#pragma unroll
+          for (int u = 0; u < 4; u++) a[u][q] = __ldcs(bv + q * nbr + j + u * LPR);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const T x0 = __ldg(v + 3 * c[u]), x1 = __ldg(v + 3 * c[u] + 1), x2 = __ldg(v + 3 * c[u] + 2);
+          y0 += a[u][0] * x0 + a[u][1] * x1 + a[u][2] * x2;
+          y1 += a[u][3] * x0 + a[u][4] * x1 + a[u][5] * x2;
+          y2 += a[u][6] * x0 + a[u][7] * x1 + a[u][8] * x2;
+        }
+      }
+    }
     for (; j + LPR < nbr; j += 2 * LPR) {
       const int j2 = j + LPR;
       const int c = __ldcs(bcol + s + j), c2 = __ldcs(bcol + s + j2);
@@ -1878,6 +1898,16 @@ int resident_grid(K kern, int64_t warps_needed) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// blocks in flight per lane of the FP32 level-0 products: 2, or 4 with
+// SGPU_LV0_UNROLL=4
+int level0_unroll() {
+  static const int u = [] {
+    const char *e = getenv("SGPU_LV0_UNROLL");
+    return (e && atoi(e) == 4) ? 4 : 2;
+  }();
+  return u;
+}
+
 // the level-0 lanes per row follow the tuned SpMV of the same precision
 int level0_lanes(const sgpu_matrix m, bool fp32) {
   const SpmvPlan &p = fp32 ? m->plan32 : m->plan64;
@@ -1894,7 +1924,10 @@ int launch_level(sgpu_matrix m, const AmgLevel &L, const T *v, const Op &op, cud
   const T *val = level_vals<T>(m, L);
   if (L.layout == 1) {
     const int lanes = level0_lanes(m, sizeof(T) == 4);
-    if (lanes == 32) {
+    if (sizeof(T) == 4 && lanes == 8 && level0_unroll() == 4) {
+      auto k = k_lv_bsr3<T, 8, Op, 4>;
+      k<<<resident_grid(k, (L.nb + 3) / 4), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
+    } else if (lanes == 32) {
       auto k = k_lv_bsr3<T, 32, Op>;
       k<<<resident_grid(k, L.nb), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
     } else if (lanes == 16) {

@@ -19,6 +19,7 @@
 //
 // Link this file into MEFEL programs only (it uses MEFEL's globals); the
 // solver binding sifel_gpu_shim.cpp serves both MEFEL and TRFEL.
+#include <cerrno>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -102,6 +103,10 @@ void __wrap__Z16stiffness_matrixl(long lcid) {
     __real__Z16stiffness_matrixl(lcid);
     return;
   }
+  // SIFEL checks errno after its computations (check_math_err,
+  // GEFEL/mathem.cpp:1725) and aborts on any value; the CUDA runtime may
+  // leave one behind while it starts (probing files), so errno is kept
+  const int saved_errno = errno;
   sgpu_mesh mesh;
   memset(&mesh, 0, sizeof(mesh));
   mesh.kind = SGPU_ELEM_HEX8;
@@ -121,6 +126,7 @@ void __wrap__Z16stiffness_matrixl(long lcid) {
   if (st != SGPU_OK) {
     fprintf(stderr, "\n GPU assembly not used (%s); assembling on the CPU\n", sgpu_last_error());
     if (h) sgpu_matrix_destroy(h);
+    errno = saved_errno;
     __real__Z16stiffness_matrixl(lcid);
     return;
   }
@@ -144,6 +150,7 @@ void __wrap__Z16stiffness_matrixl(long lcid) {
     abort();
   }
   memcpy(scr->adra, scr->adr, (size_t)(Ndofm + 1) * sizeof(long));
+  errno = saved_errno;
   Smat->prepmat(0.0, Mespr);
 }
 

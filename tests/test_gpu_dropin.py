@@ -21,8 +21,11 @@ def _run(exe, deck, env_extra=None):
     td = tempfile.mkdtemp()
     env = dict(os.environ, **(env_extra or {}))
     with open(os.path.join(td, "run.log"), "w") as log:
-        subprocess.run([os.path.join(REF, exe), deck, "."], cwd=td, stdout=log, stderr=subprocess.STDOUT,
-                       check=True, env=env, timeout=300)
+        rc = subprocess.run([os.path.join(REF, exe), deck, "."], cwd=td, stdout=log, stderr=subprocess.STDOUT,
+                            env=env, timeout=300).returncode
+    if rc != 0:
+        tail = open(os.path.join(td, "run.log"), errors="replace").read()[-2000:]
+        raise AssertionError(f"{exe} exited with {rc}; the end of its output:\n{tail}")
     return O.read_dump(td)
 
 

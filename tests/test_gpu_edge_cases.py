@@ -236,8 +236,13 @@ def test_sizes_and_null_arrays_are_refused(gpu_lib):
     st = gpu_lib.sgpu_scr_cg_prec(0, g["adr"], g["ci"], g["a"], x, g["f"], 10, 1e-20, C.byref(ani), C.byref(ares),
                                   1e-30, 0, L.FP64, None)
     assert st == L.BAD_INPUT
-    st = gpu_lib.sgpu_scr_cg_prec(x.size, None, g["ci"], g["a"], x, g["f"], 10, 1e-20, C.byref(ani), C.byref(ares),
-                                  1e-30, 0, L.FP64, None)
+    # a NULL array through a handle of the library without the binding's
+    # array argument types
+    raw = C.CDLL(L.LIB_PATH).sgpu_scr_cg_prec
+    raw.restype = C.c_int
+    vp = lambda arr: arr.ctypes.data_as(C.c_void_p)  # noqa: E731
+    st = raw(C.c_int64(x.size), None, vp(g["ci"]), vp(g["a"]), vp(x), vp(g["f"]), C.c_int64(10), C.c_double(1e-20),
+             C.byref(ani), C.byref(ares), C.c_double(1e-30), C.c_int64(0), C.c_int32(L.FP64), None)
     assert st == L.BAD_INPUT and (ani.value, ares.value) == (SENT_ANI, SENT_ARES)
 
 
@@ -265,10 +270,11 @@ def test_mixed_ok_only_on_the_true_residual(oracle, gpu_lib):
     st, ani, ares, info = _scr(gpu_lib, g["adr"], g["ci"], g["a"], g["f"], x, res=1e-20, mode=L.MIXED)
     assert st == L.OK and info.true_relres < 1e-10 and ani >= 0
     # a threshold below FP64's rounding floor of f - K x cannot be met: the
-    # solve must say so instead of returning OK
+    # solve must say so instead of returning OK (it ends on the iteration's
+    # stall or on the zero-denominator exit, whichever comes first)
     x = np.zeros_like(g["f"])
     st, ani, ares, info = _scr(gpu_lib, g["adr"], g["ci"], g["a"], g["f"], x, res=1e-36, mode=L.MIXED)
-    assert st == L.NOT_CONVERGED, L.STATUS_NAMES.get(st)
+    assert st in (L.NOT_CONVERGED, L.BREAKDOWN), L.STATUS_NAMES.get(st)
     assert (ani, ares) == (SENT_ANI, SENT_ARES)
     assert info.true_relres >= 1e-18
 
