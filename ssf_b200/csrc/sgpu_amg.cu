@@ -1898,12 +1898,13 @@ int resident_grid(K kern, int64_t warps_needed) {
   return (int)(g < 1 ? 1 : g);
 }
 
-// blocks in flight per lane of the FP32 level-0 products: 2, or 4 with
-// SGPU_LV0_UNROLL=4
+// blocks in flight per lane of the FP32 level-0 products with 8 lanes per
+// block row: 4 (the default: 1.6 ms less solve time on the 1.01M-DOF
+// cantilever than 2), or 2 with SGPU_LV0_UNROLL=2
 int level0_unroll() {
   static const int u = [] {
     const char *e = getenv("SGPU_LV0_UNROLL");
-    return (e && atoi(e) == 4) ? 4 : 2;
+    return (e && atoi(e) == 2) ? 2 : 4;
   }();
   return u;
 }
@@ -2446,11 +2447,14 @@ int launch_tail(const TailArgs<T> &a, int B, int K, cudaStream_t s, bool *launch
   return SGPU_OK;
 }
 
-// SGPU_AMG_TAIL=0 keeps the separate kernels (read at every cycle build, so
-// that a process can compare both forms)
+// The fused tail runs with SGPU_AMG_TAIL=1 (read at every cycle build, so
+// that a process can compare both forms).  It is not the default: on the
+// 1.01M-DOF cantilever the 16 SMs of one cluster read the coarse level more
+// slowly than the separate full-GPU kernels pay in launch latency (28.3 ms
+// against 26.1 ms of solve).
 bool tail_enabled() {
   const char *e = getenv("SGPU_AMG_TAIL");
-  return !(e && e[0] == '0');
+  return e && e[0] == '1';
 }
 
 // One cycle on level l (l = number of smoothing levels: the dense coarsest).
