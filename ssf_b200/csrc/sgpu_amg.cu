@@ -345,6 +345,164 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? 4 : (UNR > 2 ? 4 : 6))
   op_reduce<Op>(op, acc, st, partials, ticket);
 }
 
+// ----- level 0 in FP32 BSR3, streamed through shared memory by bulk copies -----
+// A tile is kLvTileRows consecutive block rows.  Its values (component-major
+// per row) and column indices are two contiguous byte ranges, so one bulk
+// copy each (cp.async.bulk, completion on an mbarrier) brings the tile into a
+// stage buffer; kLvStages tiles are in flight per CTA while the oldest is
+// multiplied, whatever the registers and occupancy of the arithmetic.  The
+// copies start at the 16-byte boundary at or below a range's first byte and
+// end at the one at or above its last (the arrays carry 16 bytes of slack).
+// Every wait is bounded by time; one that runs out sets SGPU_CUDA_ERROR in
+// the solver state, waits (bounded) for the copies still in flight and ends
+// the kernel.
+constexpr int kLvTileRows = 32;  // 8 lanes per block row, 256 threads
+constexpr int kLvStages = 3;
+constexpr uint64_t kLvWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// waits for phase `parity` of *bar to complete; false after kLvWaitNs
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_test(bar, parity))
+    if (global_ns() - t0 > kLvWaitNs) return false;
+  return true;
+}
+
+// global -> this CTA's shared memory, completion counted on *bar (both
+// addresses 16-byte aligned, bytes a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+struct LvTile {
+  int vbytes, cbytes;  // a stage's value and column buffers
+  __host__ __device__ static LvTile of(int cap_blocks) {
+    return LvTile{(36 * cap_blocks + 32 + 15) & ~15, (4 * cap_blocks + 32 + 15) & ~15};
+  }
+  __host__ __device__ int stage_bytes() const { return vbytes + cbytes; }
+  __host__ __device__ size_t smem_bytes() const { return (size_t)kLvStages * stage_bytes() + kLvStages * 8; }
+};
+
+template <class Op>
+__global__ void __launch_bounds__(TPB) k_lv_bsr3_tma(int nb, int cap_blocks, const int *__restrict__ browptr,
+                                                     const int *__restrict__ bcol, const float *__restrict__ bval,
+                                                     const float *__restrict__ v, Op op, PcgState *st,
+                                                     double *partials, unsigned *ticket) {
+  static_assert(TPB == kLvTileRows * 8, "one 8-lane group per block row of a tile");
+  if (st->done) return;
+  extern __shared__ __align__(128) unsigned char lv_sm[];
+  const LvTile lt = LvTile::of(cap_blocks);
+  const int sb = lt.stage_bytes();
+  uint64_t *bar = reinterpret_cast<uint64_t *>(lv_sm + (size_t)kLvStages * sb);
+  const int tid = threadIdx.x, g = tid >> 3, sub = tid & 7;
+  const int ntiles = (nb + kLvTileRows - 1) / kLvTileRows;
+  auto issue = [&](int t, int q) {
+    const int r0 = t * kLvTileRows, r1 = min(nb, r0 + kLvTileRows);
+    const int64_t b0 = __ldg(browptr + r0), b1 = __ldg(browptr + r1);
+    const int64_t vs = (36 * b0) & ~15ll, ve = (36 * b1 + 15) & ~15ll;
+    const int64_t cs = (4 * b0) & ~15ll, ce = (4 * b1 + 15) & ~15ll;
+    unsigned char *dst = lv_sm + (size_t)q * sb;
+    mbar_expect_tx(&bar[q], (unsigned)((ve - vs) + (ce - cs)));
+    if (ve > vs) bulk_g2s(dst, reinterpret_cast<const unsigned char *>(bval) + vs, (unsigned)(ve - vs), &bar[q]);
+    if (ce > cs)
+      bulk_g2s(dst + lt.vbytes, reinterpret_cast<const unsigned char *>(bcol) + cs, (unsigned)(ce - cs), &bar[q]);
+  };
+  if (tid == 0) {
+    for (int q = 0; q < kLvStages; q++) mbar_init(&bar[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int q = 0; q < kLvStages; q++) {
+      const int t = blockIdx.x + q * gridDim.x;
+      if (t < ntiles) issue(t, q);
+    }
+  double acc[Op::NV > 0 ? Op::NV : 1] = {};
+  int k = 0;
+  bool failed = false;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+    const int q = k % kLvStages;
+    const unsigned par = (unsigned)(k / kLvStages) & 1u;
+    if (__syncthreads_or(!mbar_wait_bounded(&bar[q], par))) {
+      failed = true;
+      break;
+    }
+    const int r0 = t * kLvTileRows, br = r0 + g;
+    const int b0 = __ldg(browptr + r0);
+    const float *sv = reinterpret_cast<const float *>(lv_sm + (size_t)q * sb) + (((36ll * b0) & 15) >> 2);
+    const int *sc = reinterpret_cast<const int *>(lv_sm + (size_t)q * sb + lt.vbytes) + (((4ll * b0) & 15) >> 2);
+    float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+    if (br < nb) {
+      const int s = __ldg(browptr + br), nbr = __ldg(browptr + br + 1) - s;
+      const float *a = sv + 9 * (s - b0);
+      const int *cc = sc + (s - b0);
+#pragma unroll 4
+      for (int j = sub; j < nbr; j += 8) {
+        const int c = cc[j];
+        const float x0 = __ldg(v + 3 * c), x1 = __ldg(v + 3 * c + 1), x2 = __ldg(v + 3 * c + 2);
+        y0 += a[j] * x0 + a[nbr + j] * x1 + a[2 * nbr + j] * x2;
+        y1 += a[3 * nbr + j] * x0 + a[4 * nbr + j] * x1 + a[5 * nbr + j] * x2;
+        y2 += a[6 * nbr + j] * x0 + a[7 * nbr + j] * x1 + a[8 * nbr + j] * x2;
+      }
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      y0 += __shfl_xor_sync(0xffffffffu, y0, o, 8);
+      y1 += __shfl_xor_sync(0xffffffffu, y1, o, 8);
+      y2 += __shfl_xor_sync(0xffffffffu, y2, o, 8);
+    }
+    if (sub < 3 && br < nb) op.row(3 * br + sub, sub == 0 ? y0 : (sub == 1 ? y1 : y2), acc);
+    __syncthreads();  // stage q is read: the tile kLvStages ahead may overwrite it
+    if (tid == 0 && t + kLvStages * (int)gridDim.x < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(t + kLvStages * gridDim.x, q);
+    }
+  }
+  if (failed && tid == 0) {
+    // the copies issued and not yet seen complete: tiles k .. k + kLvStages - 1
+    for (int d = 0; d < kLvStages; d++) {
+      const int t = blockIdx.x + (k + d) * gridDim.x;
+      if (t >= ntiles) break;
+      mbar_wait_bounded(&bar[(k + d) % kLvStages], (unsigned)((k + d) / kLvStages) & 1u);
+    }
+    atomicCAS(&st->status, 0, (int)SGPU_CUDA_ERROR);
+    st->done = 1;
+  }
+  // the grid reduction runs in any case, so that its ticket returns to zero
+  op_reduce<Op>(op, acc, st, partials, ticket);
+}
+
 // level 0 in scalar CSR: L lanes per row
 template <typename T, int L, class Op>
 __global__ void __launch_bounds__(TPB) k_lv_csr(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
@@ -1309,6 +1467,292 @@ __global__ void __launch_bounds__(128) k_galerkin(int nruns, const int *__restri
   }
 }
 
+// ----- Galerkin product without a global sort -------------------------------
+// One warp per aggregate G builds coarse row G directly: the aggregates H
+// that the rows of G's nodes reach (a hash set in shared memory, then ranked
+// into ascending order) and A_c(G,H) = sum over i in G and the entries (i,j)
+// of row i with agg[j] = H of Q_i^T A_ij Q_j.  The sum runs over G's nodes
+// in aggregate order and each row's entries in column order, so every run
+// gives the same bits.  A coarse row of more than kGalCap blocks makes the
+// count pass raise a flag and the level takes the sort-based path above.
+constexpr int kGalCap = 64;
+constexpr int kGalHash = 128;
+constexpr int kGalWarps = 2;
+
+struct GalTable {
+  int key[kGalHash];  // aggregate H, or -1
+  int pos[kGalHash];  // H's position in the ascending coarse row
+  int list[kGalCap];  // the coarse row's columns, ascending
+};
+
+__device__ __forceinline__ unsigned gal_hash(int h) { return ((unsigned)h * 2654435761u) >> 25; }
+
+// G's coarse columns into T; returns their number, or -1 above kGalCap
+__device__ int gal_table(int G, const int *__restrict__ aggptr, const int *__restrict__ aggnodes,
+                         const int *__restrict__ browptr, const int *__restrict__ bcol, const int *__restrict__ agg,
+                         GalTable &T) {
+  const int lane = threadIdx.x & 31;
+  for (int h = lane; h < kGalHash; h += 32) T.key[h] = -1;
+  __syncwarp();
+  int n = 0;
+  for (int a = aggptr[G]; a < aggptr[G + 1] && n <= kGalCap; a++) {
+    const int i = aggnodes[a];
+    const int re = browptr[i + 1];
+    for (int t0 = browptr[i]; t0 < re && n <= kGalCap; t0 += 32) {
+      const int e = t0 + lane;
+      bool fresh = false;
+      if (e < re) {
+        const int H = agg[bcol[e]];
+        unsigned h = gal_hash(H);
+        // a full table (kGalHash > kGalCap keys) already means overflow
+        for (int p = 0; p < kGalHash; p++) {
+          const int k = atomicCAS(&T.key[h], -1, H);
+          if (k == -1) { fresh = true; break; }
+          if (k == H) break;
+          h = (h + 1) & (kGalHash - 1);
+        }
+      }
+      n += __popc(__ballot_sync(0xffffffffu, fresh));
+      __syncwarp();
+    }
+  }
+  if (n > kGalCap) return -1;
+  for (int h = lane; h < kGalHash; h += 32) {
+    const int k = T.key[h];
+    if (k >= 0) {
+      int r = 0;
+      for (int q = 0; q < kGalHash; q++) {
+        const int o = T.key[q];
+        r += (o >= 0 && o < k);
+      }
+      T.pos[h] = r;
+      T.list[r] = k;
+    }
+  }
+  __syncwarp();
+  return n;
+}
+
+__device__ __forceinline__ int gal_find(const GalTable &T, int H) {
+  unsigned h = gal_hash(H);
+  for (int p = 0; p < kGalHash; p++) {
+    const int k = T.key[h];
+    if (k == H) return T.pos[h];
+    if (k < 0) return -1;
+    h = (h + 1) & (kGalHash - 1);
+  }
+  return -1;
+}
+
+// blocks per coarse row -> cnt[G] and the row's columns, ascending, ->
+// lists[G * kGalCap ...]; *over = 1 when a row exceeds kGalCap
+__global__ void __launch_bounds__(32 * kGalWarps)
+    k_gal_count(int na, const int *__restrict__ aggptr, const int *__restrict__ aggnodes,
+                const int *__restrict__ browptr, const int *__restrict__ bcol, const int *__restrict__ agg,
+                int *__restrict__ cnt, int *__restrict__ lists, int *__restrict__ over) {
+  __shared__ GalTable tab[kGalWarps];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int G = blockIdx.x * kGalWarps + w; G < na; G += gridDim.x * kGalWarps) {
+    const int n = gal_table(G, aggptr, aggnodes, browptr, bcol, agg, tab[w]);
+    if (lane == 0) {
+      cnt[G] = n < 0 ? 0 : n;
+      if (n < 0) atomicOr(over, 1);
+    }
+    for (int t = lane; t < n; t += 32) lists[(size_t)G * kGalCap + t] = tab[w].list[t];
+    __syncwarp();
+  }
+}
+
+// warps per aggregate in k_gal_values
+constexpr int kGalCtaWarps = 4;
+
+template <int K>
+constexpr size_t gal_shared_bytes() {
+  // per CTA: the accumulators [kGalCap][K*K], a staging area per warp with an
+  // odd stride in doubles (32 lanes' stores hit distinct banks), the staged
+  // entries' positions and counts, the table
+  return ((size_t)kGalCap * K * K + (size_t)kGalCtaWarps * 32 * (K * K | 1)) * sizeof(double) +
+         kGalCtaWarps * 33 * sizeof(int) + sizeof(GalTable);
+}
+
+// Coarse row G's values, one CTA per aggregate (columns from the count pass).
+// The CTA's warps take the aggregate's nodes in turn (warp w: nodes w, w + 4,
+// ...), one chunk of up to 32 entries of a row per round: each lane forms the
+// product Q_i^T A_ij Q_j of its entry and stages it.  Then K*K threads, one
+// per value, add the staged products of warps 0..3, rows in entry order, into
+// the accumulators (a run of entries into one block summed first).  The
+// order of every sum is fixed by the data, so every run gives the same bits.
+template <int B, int K>
+__global__ void __launch_bounds__(32 * kGalCtaWarps, 3)
+    k_gal_values(int na, const int *__restrict__ aggptr, const int *__restrict__ aggnodes,
+                 const int *__restrict__ agg, LevelView A, const double *__restrict__ Q,
+                 const int *__restrict__ lists, const int *__restrict__ cbrowptr, int *__restrict__ cbcol,
+                 double *__restrict__ out) {
+  constexpr int KK = K * K, SS = KK | 1, W = kGalCtaWarps, BK = B * K;
+  extern __shared__ double gal_sh[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *acc = gal_sh;                         // [kGalCap][KK]
+  double *stages = acc + kGalCap * KK;          // [W][32][SS]
+  double *stage = stages + w * 32 * SS;         // this warp's
+  int *spos = reinterpret_cast<int *>(stages + W * 32 * SS);  // [W][32]
+  int *srows = spos + W * 32;                                  // [W]
+  GalTable &T = *reinterpret_cast<GalTable *>(srows + W + (W & 1));
+  for (int G = blockIdx.x; G < na; G += gridDim.x) {
+    const int base = cbrowptr[G], n = cbrowptr[G + 1] - base;
+    // the table of the row's columns: key -> position in the ascending list
+    for (int h = threadIdx.x; h < kGalHash; h += blockDim.x) T.key[h] = -1;
+    for (int t = threadIdx.x; t < n * KK; t += blockDim.x) acc[t] = 0.0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const int H = __ldg(lists + (size_t)G * kGalCap + t);
+      T.list[t] = H;
+      unsigned h = gal_hash(H);
+      for (int p = 0; p < kGalHash; p++) {  // n <= kGalCap < kGalHash keys: a free slot exists
+        if (atomicCAS(&T.key[h], -1, H) == -1) {
+          T.pos[h] = t;
+          break;
+        }
+        h = (h + 1) & (kGalHash - 1);
+      }
+    }
+    __syncthreads();
+    const int a_end = aggptr[G];
+    int a = a_end + w;  // this warp's current node
+    const int a_last = aggptr[G + 1];
+    int i = 0, rs = 0, re = 0, t0 = 0;
+    if (a < a_last) {
+      i = __ldg(aggnodes + a);
+      rs = __ldg(A.browptr + i);
+      re = __ldg(A.browptr + i + 1);
+      t0 = rs;
+    }
+    while (__syncthreads_or(a < a_last)) {
+      int p = -1, rows = 0;
+      if (a < a_last) {
+        const int e = t0 + lane;
+        const bool live = e < re;
+        rows = min(32, re - t0);
+        double prod[KK];
+#pragma unroll
+        for (int t = 0; t < KK; t++) prod[t] = 0.0;
+        if (live) {
+          const int j = __ldg(A.bcol + e);
+          p = gal_find(T, __ldg(agg + j));
+          double av[B * B];
+          if (A.layout == 0) {
+#pragma unroll
+            for (int c = 0; c < B * B; c++) av[c] = __ldg(A.val + (size_t)e * B * B + c);
+          } else {
+            double di[B], dj[B];
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+              di[c] = __ldg(A.dscale + (size_t)B * i + c);
+              dj[c] = __ldg(A.dscale + (size_t)B * j + c);
+            }
+            const int nbr = re - rs;
+#pragma unroll
+            for (int c = 0; c < B * B; c++) {
+              // layout 1: the row's blocks component-major; layout 2 (B = 1): CSR
+              const double v = A.layout == 1 ? __ldg(A.val + 9ll * rs + (int64_t)c * nbr + (e - rs))
+                                             : __ldg(A.val + e);
+              av[c] = v * di[c / B] * dj[c % B];
+            }
+          }
+          double qj[BK], qi[BK];
+          if constexpr (BK % 2 == 0) {  // a node's Q rows are 16-byte aligned (BK * 8 bytes each, BK even)
+            const double2 *Qj2 = reinterpret_cast<const double2 *>(Q + (size_t)j * BK);
+            const double2 *Qi2 = reinterpret_cast<const double2 *>(Q + (size_t)i * BK);
+#pragma unroll
+            for (int c = 0; c < BK / 2; c++) {
+              const double2 u = __ldg(Qj2 + c), z = __ldg(Qi2 + c);
+              qj[2 * c] = u.x;
+              qj[2 * c + 1] = u.y;
+              qi[2 * c] = z.x;
+              qi[2 * c + 1] = z.y;
+            }
+          } else {
+#pragma unroll
+            for (int c = 0; c < BK; c++) {
+              qj[c] = __ldg(Q + (size_t)j * BK + c);
+              qi[c] = __ldg(Q + (size_t)i * BK + c);
+            }
+          }
+#pragma unroll
+          for (int q2 = 0; q2 < K; q2++) {
+            double tcol[B];
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+              double sacc = 0.0;
+#pragma unroll
+              for (int c2 = 0; c2 < B; c2++) sacc += av[c * B + c2] * qj[c2 * K + q2];
+              tcol[c] = sacc;
+            }
+#pragma unroll
+            for (int q1 = 0; q1 < K; q1++) {
+              double sacc = 0.0;
+#pragma unroll
+              for (int c = 0; c < B; c++) sacc += qi[c * K + q1] * tcol[c];
+              prod[q1 * K + q2] = sacc;
+            }
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < KK; t++) stage[lane * SS + t] = prod[t];
+        // next chunk of this row, or this warp's next node
+        t0 += 32;
+        if (t0 >= re) {
+          a += W;
+          if (a < a_last) {
+            i = __ldg(aggnodes + a);
+            rs = __ldg(A.browptr + i);
+            re = __ldg(A.browptr + i + 1);
+            t0 = rs;
+          }
+        }
+      }
+      spos[w * 32 + lane] = p;
+      if (lane == 0) srows[w] = rows;
+      __syncthreads();
+      // one thread per value: the staged rows of warps 0..W-1 in order; a
+      // stage's values and positions are loaded before its walk, so that only
+      // the adds at the end of a run wait on shared memory
+      for (int v = threadIdx.x; v < KK; v += blockDim.x) {
+        int cur = -1;
+        double run = 0.0;
+#pragma unroll 1
+        for (int ws = 0; ws < W; ws++) {
+          const int nr = srows[ws];
+          const double *sg = stages + ws * 32 * SS + v;
+          const int *sp = spos + ws * 32;
+          double sv[32];
+          int pq[32];
+#pragma unroll
+          for (int r = 0; r < 32; r++) {
+            sv[r] = r < nr ? sg[r * SS] : 0.0;
+            pq[r] = r < nr ? sp[r] : -1;
+          }
+#pragma unroll
+          for (int r = 0; r < 32; r++) {
+            if (r < nr) {
+              if (pq[r] != cur) {
+                if (cur >= 0) acc[cur * KK + v] += run;
+                run = 0.0;
+                cur = pq[r];
+              }
+              run += sv[r];
+            }
+          }
+        }
+        if (cur >= 0) acc[cur * KK + v] += run;
+      }
+      // (the loop condition's barrier orders these adds before the next staging)
+    }
+    for (int t = threadIdx.x; t < n; t += blockDim.x) cbcol[base + t] = T.list[t];
+    for (int t = threadIdx.x; t < n * KK; t += blockDim.x) out[(size_t)base * KK + t] = acc[t];
+    __syncthreads();
+  }
+}
+
 // 1/diag of a coarse level (0 for a zero diagonal: an equation that a
 // dependent near-null-space column left empty stays 0)
 __global__ void k_coarse_dinv(int na, int K, const int *__restrict__ browptr, const int *__restrict__ bcol,
@@ -1708,10 +2152,11 @@ int take_roots(const AmgLevel &L, const TmpBuf<uint64_t> &t, int base, int *agg,
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag.p, rootid.p, nb, s);
   SGPU_TRY(tmp.ensure(bytes));
   SGPU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.buf.p, bytes, flag.p, rootid.p, nb, s));
-  int last_id = 0, last_flag = 0;
-  SGPU_TRY(read_int(rootid.p + nb - 1, s, &last_id));
-  SGPU_TRY(read_int(flag.p + nb - 1, s, &last_flag));
-  *count = last_id + last_flag;
+  int last[2] = {0, 0};  // the last node's id and root flag, one wait for both
+  SGPU_CUDA(cudaMemcpyAsync(&last[0], rootid.p + nb - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaMemcpyAsync(&last[1], flag.p + nb - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  *count = last[0] + last[1];
   k_attach_roots<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, t.p, rootid.p, base, agg);
   count_launches(1);
   SGPU_CUDA(cudaGetLastError());
@@ -1802,8 +2247,87 @@ int tentative(AmgLevel &L, int K, const double *Bl, double *Bnext, cudaStream_t 
   return SGPU_OK;
 }
 
-// Galerkin product of level L into a new coarse level C (owned, block size K)
-int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_t s, CubTmp &tmp) {
+template <int B, int K>
+int launch_gal_values(const AmgLevel &L, const LevelView &view, const int *lists, AmgLevel &C, cudaStream_t s) {
+  constexpr size_t sm = gal_shared_bytes<K>();
+  SGPU_CUDA(cudaFuncSetAttribute(k_gal_values<B, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int grid = (int)std::min<int64_t>(L.na, 64ll * kNumSMs);
+  k_gal_values<B, K><<<grid, 32 * kGalCtaWarps, sm, s>>>(L.na, L.aggptr.p, L.aggnodes.p, L.agg.p, view, L.Q64.p,
+                                                          lists, C.own_browptr.p, C.own_bcol.p, C.val64.p);
+  count_launches(1);
+  return SGPU_OK;
+}
+
+// 1/diag and its square root for a new coarse level
+int coarse_diagonals(AmgLevel &C, int K, cudaStream_t s) {
+  SGPU_TRY(C.dinv64.alloc(C.n));
+  SGPU_TRY(C.dinv32.alloc(C.n));
+  k_coarse_dinv<<<grid_for(C.nb), TPB, 0, s>>>(C.nb, K, C.browptr, C.bcol, C.val64.p, C.dinv64.p, C.dinv32.p);
+  SGPU_TRY(C.dsq64.alloc(C.n));
+  SGPU_TRY(C.dsq32.alloc(C.n));
+  k_sqrt_vec<<<grid_for(C.n), TPB, 0, s>>>(C.n, C.dinv64.p, C.dsq32.p, C.dsq64.p);
+  count_launches(2);
+  SGPU_CUDA(cudaGetLastError());
+  return SGPU_OK;
+}
+
+// Galerkin product by aggregate rows (k_gal_count, a scan, k_gal_values);
+// *done stays false when a coarse row exceeds kGalCap blocks
+int galerkin_direct(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_t s, CubTmp &tmp,
+                    bool *done) {
+  *done = false;
+  const int na = L.na;
+  TmpBuf<int> cnt(s), lists(s);
+  SGPU_TRY(cnt.alloc((size_t)na + 1));
+  SGPU_TRY(lists.alloc((size_t)na * kGalCap));
+  // cnt[na] is the overflow flag: the exclusive scan's last output leaves it out
+  SGPU_CUDA(cudaMemsetAsync(cnt.p + na, 0, sizeof(int), s));
+  const int grid = (int)std::min<int64_t>(((int64_t)na + kGalWarps - 1) / kGalWarps, 64ll * kNumSMs);
+  k_gal_count<<<grid, 32 * kGalWarps, 0, s>>>(na, L.aggptr.p, L.aggnodes.p, L.browptr, L.bcol, L.agg.p, cnt.p,
+                                               lists.p, cnt.p + na);
+  count_launches(1);
+  SGPU_TRY(C.own_browptr.alloc((size_t)na + 1));
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.p, C.own_browptr.p, na + 1, s);
+  SGPU_TRY(tmp.ensure(bytes));
+  SGPU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.buf.p, bytes, cnt.p, C.own_browptr.p, na + 1, s));
+  int hv[2] = {0, 0};
+  SGPU_CUDA(cudaMemcpyAsync(&hv[0], C.own_browptr.p + na, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaMemcpyAsync(&hv[1], cnt.p + na, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  if (hv[1]) return SGPU_OK;
+  C.nb = na;
+  C.b = K;
+  C.n = na * K;
+  C.nblk = hv[0];
+  C.layout = 0;
+  SGPU_TRY(C.own_bcol.alloc((size_t)hv[0]));
+  SGPU_TRY(C.val64.alloc((size_t)hv[0] * K * K));
+  C.browptr = C.own_browptr.p;
+  C.bcol = C.own_bcol.p;
+  const int B = L.b;
+  if (B == 3 && K == 6) SGPU_TRY((launch_gal_values<3, 6>(L, view, lists.p, C, s)));
+  else if (B == 6 && K == 6) SGPU_TRY((launch_gal_values<6, 6>(L, view, lists.p, C, s)));
+  else if (B == 1 && K == 1) SGPU_TRY((launch_gal_values<1, 1>(L, view, lists.p, C, s)));
+  else if (B == 1 && K == 3) SGPU_TRY((launch_gal_values<1, 3>(L, view, lists.p, C, s)));
+  else if (B == 3 && K == 3) SGPU_TRY((launch_gal_values<3, 3>(L, view, lists.p, C, s)));
+  else if (B == 1 && K == 6) SGPU_TRY((launch_gal_values<1, 6>(L, view, lists.p, C, s)));
+  else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
+  SGPU_CUDA(cudaGetLastError());
+  *done = true;
+  return SGPU_OK;
+}
+
+// Galerkin product of level L into a new coarse level C (owned, block size K):
+// by aggregate rows, or (SGPU_GALERKIN=sort, or a coarse row above kGalCap
+// blocks) by a global sort of the fine blocks' (G, H) keys
+int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_t s, CubTmp &tmp, bool *by_rows) {
+  const char *gm = getenv("SGPU_GALERKIN");
+  *by_rows = false;
+  if (!(gm && !strcmp(gm, "sort"))) {
+    SGPU_TRY(galerkin_direct(L, view, C, K, s, tmp, by_rows));
+    if (*by_rows) return coarse_diagonals(C, K, s);
+  }
   const int64_t nblk = L.nblk;
   if (nblk >= (int64_t)INT32_MAX) return fail(SGPU_BAD_INPUT, "too many blocks for the aggregation set-up");
   const int nbk = (int)nblk;
@@ -1862,15 +2386,7 @@ int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_
   else if (B == 1 && K == 6) launch_galerkin<1, 6>(nruns, runoff.p, sidx.p, rowid.p, view, L.Q64.p, C.val64.p, s);
   else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
   count_launches(1);
-  SGPU_TRY(C.dinv64.alloc(C.n));
-  SGPU_TRY(C.dinv32.alloc(C.n));
-  k_coarse_dinv<<<grid_for(C.nb), TPB, 0, s>>>(C.nb, K, C.browptr, C.bcol, C.val64.p, C.dinv64.p, C.dinv32.p);
-  SGPU_TRY(C.dsq64.alloc(C.n));
-  SGPU_TRY(C.dsq32.alloc(C.n));
-  k_sqrt_vec<<<grid_for(C.n), TPB, 0, s>>>(C.n, C.dinv64.p, C.dsq32.p, C.dsq64.p);
-  count_launches(2);
-  SGPU_CUDA(cudaGetLastError());
-  return SGPU_OK;
+  return coarse_diagonals(C, K, s);
 }
 
 // ----- level SpMV dispatch --------------------------------------------------
@@ -1909,6 +2425,73 @@ int level0_unroll() {
   return u;
 }
 
+// SGPU_LV0_TMA=1: the FP32 level-0 products stream tiles through shared
+// memory (k_lv_bsr3_tma).  Not the default: on the 1.01M-DOF cantilever the
+// solve takes 25.4 ms with it against 24.3 ms with the register kernel (its
+// CTAs wait on each tile's x gathers and row updates between barriers; the
+// register kernel's 32 independent warps per SM hide that latency better).
+// Read at every launch, so a process can compare both.
+bool level0_tma_enabled() {
+  const char *e = getenv("SGPU_LV0_TMA");
+  return e && !strcmp(e, "1");
+}
+
+__global__ void k_tile_blocks(int nb, const int *__restrict__ browptr, int *__restrict__ cap) {
+  const int ntiles = (nb + kLvTileRows - 1) / kLvTileRows;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int r0 = t * kLvTileRows, r1 = min(nb, r0 + kLvTileRows);
+    atomicMax(cap, browptr[r1] - browptr[r0]);
+  }
+}
+
+// the most blocks in a tile of the level-0 BSR3 (once per pattern; set-up
+// only, never inside a capture)
+int level0_tile_plan(sgpu_matrix m, cudaStream_t s) {
+  Bsr3 &b = m->bsr;
+  if (!b.valid || b.tile_cap != 0) return SGPU_OK;
+  TmpBuf<int> cap(s);
+  SGPU_TRY(cap.alloc(1));
+  SGPU_CUDA(cudaMemsetAsync(cap.p, 0, sizeof(int), s));
+  k_tile_blocks<<<grid_for((b.nb + kLvTileRows - 1) / kLvTileRows), TPB, 0, s>>>(b.nb, b.browptr.p, cap.p);
+  count_launches(1);
+  int c = 0;
+  SGPU_TRY(read_int(cap.p, s, &c));
+  // a stage set must fit the shared memory of one CTA
+  b.tile_cap = (c > 0 && LvTile::of(c).smem_bytes() <= 200 * 1024) ? c : -1;
+  return SGPU_OK;
+}
+
+// launches the streamed level-0 kernel; false when it cannot run here (no
+// plan, or its shared-memory attribute not yet set while the stream captures)
+template <class Op>
+bool launch_level0_tma(sgpu_matrix m, const AmgLevel &L, const float *v, const Op &op, cudaStream_t s,
+                       unsigned *ticket) {
+  const int cap = m->bsr.tile_cap;
+  if (cap <= 0 || !level0_tma_enabled()) return false;
+  static int ready = 0, per_sm = 0;  // per instantiation: attribute set, resident CTAs per SM
+  const size_t smem = LvTile::of(cap).smem_bytes();
+  static size_t ready_smem = 0;
+  auto kern = k_lv_bsr3_tma<Op>;
+  if (!ready || ready_smem < smem) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TPB, smem);
+    if (per_sm < 1) return false;
+    ready = 1;
+    ready_smem = smem;
+  }
+  const int ntiles = (L.nb + kLvTileRows - 1) / kLvTileRows;
+  const int grid = std::max(1, std::min(ntiles, kNumSMs * per_sm));
+  kern<<<grid, TPB, smem, s>>>(L.nb, cap, L.browptr, L.bcol, m->bsr.bval32s.p, v, op, pcg_state(m),
+                               m->w.partials.p, ticket);
+  return true;
+}
+
 // the level-0 lanes per row follow the tuned SpMV of the same precision
 int level0_lanes(const sgpu_matrix m, bool fp32) {
   const SpmvPlan &p = fp32 ? m->plan32 : m->plan64;
@@ -1925,7 +2508,10 @@ int launch_level(sgpu_matrix m, const AmgLevel &L, const T *v, const Op &op, cud
   const T *val = level_vals<T>(m, L);
   if (L.layout == 1) {
     const int lanes = level0_lanes(m, sizeof(T) == 4);
-    if (sizeof(T) == 4 && lanes == 8 && level0_unroll() == 4) {
+    bool streamed = false;
+    if constexpr (sizeof(T) == 4) streamed = launch_level0_tma<Op>(m, L, v, op, s, tk);
+    if (streamed) {
+    } else if (sizeof(T) == 4 && lanes == 8 && level0_unroll() == 4) {
       auto k = k_lv_bsr3<T, 8, Op, 4>;
       k<<<resident_grid(k, (L.nb + 3) / 4), TPB, 0, s>>>(L.nb, L.browptr, L.bcol, val, v, op, st, part, tk);
     } else if (lanes == 32) {
@@ -2106,6 +2692,7 @@ int amg_build(sgpu_matrix m) {
   }
   SGPU_TRY(ensure_bsr3(m));
   SGPU_TRY(ensure_fp32(m));  // scaled FP32 level 0 and S = diag^-1/2
+  SGPU_TRY(level0_tile_plan(m, s));
   const int n = (int)m->n;
   keep_pool_memory();
   CubTmp tmp(s);
@@ -2166,8 +2753,9 @@ int amg_build(sgpu_matrix m) {
     A.lv.push_back(C);
     LevelView view{L.layout, L.browptr, L.bcol,
                    L.layout == 1 ? m->bsr.bval.p : (L.layout == 2 ? m->csr.val.p : L.val64.p), m->csr.dscale.p};
-    SGPU_TRY(galerkin(L, view, *C, K, s, tmp));
-    clk.mark("galerkin product");
+    bool by_rows = false;
+    SGPU_TRY(galerkin(L, view, *C, K, s, tmp, &by_rows));
+    clk.mark(by_rows ? "galerkin product (rows)" : "galerkin product (sort)");
     std::swap(Bcur.p, Bnext.p);
     std::swap(Bcur.n, Bnext.n);
     // stop when the next level is small enough for the dense solve, or when
@@ -2647,6 +3235,77 @@ int capture_chunk(sgpu_matrix m, int iters, cudaGraphExec_t *exec, int64_t *node
   return SGPU_OK;
 }
 
+// The loop body's last kernel: run the body again while the iteration has
+// not stopped and the launch's iteration cap is not reached.
+__global__ void k_fcg_continue(cudaGraphConditionalHandle h, PcgState *st, int64_t cap) {
+  const int64_t c = ++st->loops;
+  cudaGraphSetConditional(h, (!st->done && c < cap) ? 1u : 0u);
+}
+
+// The flexible CG's iterations as one graph: a conditional WHILE node whose
+// body is one iteration (FP64 SpMV, update, V-cycle and direction) and
+// k_fcg_continue, which ends the loop when the solver's state says done (the
+// stopping test, a breakdown or ni iterations) or after `cap` iterations of
+// one launch, whichever comes first.  The host waits once per launch.
+// Returns SGPU_OK with *exec == nullptr when the runtime offers no
+// conditional nodes (the caller then uses capture_chunk).
+template <typename T>
+int capture_loop(sgpu_matrix m, int64_t cap, cudaGraphExec_t *exec, int64_t *nodes) {
+  cudaStream_t s = m->stream;
+  Work &w = m->w;
+  *exec = nullptr;
+  cudaGraph_t g = nullptr;
+  SGPU_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return SGPU_OK;
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, nullptr, 0, &cp) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return SGPU_OK;
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  const int64_t before = sgpu_kernel_launches();
+  cudaError_t e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(SGPU_CUDA_ERROR, std::string("cudaStreamBeginCaptureToGraph: ") + cudaGetErrorString(e));
+  }
+  int rc = spmv64_flex(m, w.d.p, w.p.p, s);
+  if (rc == SGPU_OK) rc = fcg_update<T>(m, s);
+  if (rc == SGPU_OK) rc = vcycle_dir<T>(m, s);
+  if (rc == SGPU_OK) {
+    k_fcg_continue<<<1, 1, 0, s>>>(h, pcg_state(m), cap);
+    count_launches(1);
+  }
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(s, &captured);
+  if (rc != SGPU_OK) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  *nodes = sgpu_kernel_launches() - before;  // kernels of one iteration
+  count_launches(-*nodes);
+  if (e != cudaSuccess) {  // a body the runtime does not take: the caller captures chunks
+    cudaGetLastError();
+    *exec = nullptr;
+    if (getenv("SGPU_AMG_VERBOSE"))
+      fprintf(stderr, "amg: no device-side loop graph (%s); chunks of iterations\n", cudaGetErrorString(e));
+  }
+  return SGPU_OK;
+}
+
 // r = f - K x with a fresh V-cycle and p = z: (re)start of the recurrence
 template <typename T>
 int fcg_start(sgpu_matrix m, cudaStream_t s) {
@@ -2677,16 +3336,26 @@ int fcg_solve(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, in
   cudaGraphExec_t exec = nullptr;
   int64_t nodes = 0;
   PhaseClock clk(s);
-  SGPU_TRY(capture_chunk<T>(m, chunk, &exec, &nodes));
-  clk.mark("graph capture + instantiate");
+  // the device-side loop (SGPU_FCG_LOOP=chunk: graphs of `chunk` iterations
+  // and a host test between them)
+  const char *lm = getenv("SGPU_FCG_LOOP");
+  bool loop = !(lm && !strcmp(lm, "chunk"));
+  if (loop) {
+    // at most the remaining iterations (plus one) per launch
+    SGPU_TRY(capture_loop<T>(m, std::max<int64_t>(2, ni - hs->it + 1), &exec, &nodes));
+    loop = exec != nullptr;
+  }
+  if (!loop) SGPU_TRY(capture_chunk<T>(m, chunk, &exec, &nodes));
+  clk.mark(loop ? "graph capture + instantiate (loop)" : "graph capture + instantiate");
   int rc = SGPU_OK;
   int restarts = 0;
   for (;;) {
+    if (loop) SGPU_CUDA(cudaMemsetAsync(&pcg_state(m)->loops, 0, sizeof(int64_t), s));
     cudaError_t e = cudaGraphLaunch(exec, s);
     if (e != cudaSuccess) { rc = fail(SGPU_CUDA_ERROR, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); break; }
-    count_launches(nodes);
     rc = read_st(m, hs);
     if (rc != SGPU_OK) break;
+    count_launches(loop ? nodes * hs->loops : nodes);
     if (!hs->done) continue;
     // converged on the recurrence: with SGPU_CRIT_TRUE the true residual must
     // agree, else the recurrence restarts from it (at most four times; a

@@ -103,6 +103,9 @@ struct Bsr3 {
   DevBuf<int64_t> csr2bsr;  // CSR entry -> position in bval (for value updates)
   bool valid = false;
   bool have32 = false;
+  // most blocks in one tile of 32 block rows (the FP32 level-0 products that
+  // stream tiles through shared memory); 0 not yet known
+  int tile_cap = 0;
 };
 
 // SpMV kernel choice for one format/precision, picked by the autotuner.
@@ -148,6 +151,7 @@ struct PcgState {
   // control
   int done, pause, status;
   double last_dot;
+  int64_t loops;  // iterations run by one launch of a device-side loop graph
 };
 
 // Per-handle scratch vectors of the iteration.

@@ -385,7 +385,7 @@ int ensure_fp32(sgpu_matrix m) {
   count_launches(1);
   c.have32 = true;
   if (m->bsr.valid) {
-    SGPU_TRY(m->bsr.bval32s.alloc(m->bsr.nblk * 9));
+    SGPU_TRY(m->bsr.bval32s.alloc(m->bsr.nblk * 9 + 4));
     k_bsr3_values32<<<blocks_for(c.nnz), TPB, 0, s>>>(c.nnz, c.val32s.p, m->bsr.csr2bsr.p, m->bsr.bval32s.p);
     count_launches(1);
     m->bsr.have32 = true;
@@ -537,7 +537,9 @@ int ensure_bsr3(sgpu_matrix m) {
   SGPU_CUDA(cudaStreamSynchronize(s));
   b.nb = nb;
   b.nblk = nblk;
-  SGPU_TRY(b.bcol.alloc(nblk));
+  // 16 bytes of slack after the columns and the FP32 values: bulk copies of
+  // whole tiles round their end up to a 16-byte boundary
+  SGPU_TRY(b.bcol.alloc((size_t)nblk + 4));
   SGPU_TRY(b.bval.alloc((size_t)nblk * 9));
   SGPU_TRY(b.csr2bsr.alloc(c.nnz));
   k_bsr3_fill<<<blocks_for((int64_t)nb * 32), TPB, 0, s>>>(nb, c.rowptr.p, c.col.p, b.browptr.p, b.bcol.p,
@@ -546,8 +548,9 @@ int ensure_bsr3(sgpu_matrix m) {
   count_launches(2);
   b.valid = true;
   b.have32 = false;
+  b.tile_cap = 0;
   if (c.have32) {
-    SGPU_TRY(b.bval32s.alloc((size_t)nblk * 9));
+    SGPU_TRY(b.bval32s.alloc((size_t)nblk * 9 + 4));
     k_bsr3_values32<<<blocks_for(c.nnz), TPB, 0, s>>>(c.nnz, c.val32s.p, b.csr2bsr.p, b.bval32s.p);
     count_launches(1);
     b.have32 = true;

@@ -251,3 +251,143 @@ def test_overlapped_smoother_bound_gives_the_same_bits(oracle, gpu_lib):
     assert r0.status == r1.status == L.OK
     assert r0.info["iterations"] == r1.info["iterations"]
     assert np.array_equal(x0, x1)
+
+
+def _solve_with_env(dm, f, mode, name, value):
+    import os
+    old = os.environ.get(name)
+    if value is None:
+        os.environ.pop(name, None)
+    else:
+        os.environ[name] = value
+    try:
+        dm.precond_clear()
+        return dm.pcg(f, res=1e-22, prec="agg", mode=mode)
+    finally:
+        if old is None:
+            os.environ.pop(name, None)
+        else:
+            os.environ[name] = old
+
+
+@pytest.mark.parametrize("case", ["cantilever", "plate", "conduction", "dense_graph"])
+def test_galerkin_by_aggregate_rows_matches_the_sort_path(oracle, gpu_lib, case, capfd, monkeypatch):
+    # the coarse operators built one aggregate row per warp and by the
+    # global key sort are the same sums in another order: the hierarchies
+    # agree to rounding, so the solves agree to the solver tolerance.  The
+    # dense graph's coarse rows reach more aggregates than one warp's table
+    # holds, so there the row pass hands the level to the sort path.
+    if case == "cantilever":
+        m = decks.cantilever_hex(48, 10, 10)
+        adr, ci, a = _oracle_system(oracle, m)
+        f = oracle.load_vector(m)
+        B = mefel.rigid_body_modes(m)
+    elif case == "plate":
+        m = decks.plate_quad(48, 24, E=3e10, nu=0.22)
+        adr, ci, a = _oracle_system(oracle, m)
+        f = oracle.load_vector(m)
+        B = mefel.rigid_body_modes(m)
+    elif case == "conduction":
+        m = decks.heat_cube(30, sigma=1.0)
+        with mefel.conductivity_matrix(m) as K:
+            adr, ci, a = K.download(symmetric=1)
+        f = np.random.default_rng(11).standard_normal(adr.size - 1)
+        B = np.ones((adr.size - 1, 1))
+    else:
+        # graph Laplacian plus the identity: a 128 x 128 five-point grid with
+        # 8 random long-range edges per node, so that each small aggregate's
+        # rows reach far more aggregates than a coarse row of the table holds
+        rng = np.random.default_rng(5)
+        side = 128
+        n = side * side
+        idx = np.arange(n).reshape(side, side)
+        e1 = np.concatenate([np.stack([idx[:, :-1].ravel(), idx[:, 1:].ravel()], 1),
+                             np.stack([idx[:-1, :].ravel(), idx[1:, :].ravel()], 1),
+                             np.stack([np.repeat(np.arange(n), 8), rng.integers(0, n, 8 * n)], 1)])
+        e1 = e1[e1[:, 0] != e1[:, 1]]
+        lo, hi = np.minimum(e1[:, 0], e1[:, 1]), np.maximum(e1[:, 0], e1[:, 1])
+        pairs = np.unique(hi * n + lo)
+        r, c = pairs // n, pairs % n  # row r > column c (lower triangle), sorted by row then column
+        w = -rng.uniform(0.5, 1.5, r.size)
+        d = 1.0 + np.bincount(r, -w, n) + np.bincount(c, -w, n)
+        rr = np.concatenate([r, np.arange(n)])
+        cc = np.concatenate([c, np.arange(n)])
+        vv = np.concatenate([w, d])
+        order = np.lexsort((cc, rr))  # the diagonal ends each row
+        ci = cc[order].astype(np.int64)
+        a = vv[order]
+        adr = np.zeros(n + 1, dtype=np.int64)
+        adr[1:] = np.cumsum(np.bincount(rr, minlength=n))
+        f = rng.standard_normal(n)
+        B = np.ones((n, 1))
+    # the reference's solve to a residual below what FP64 reaches (it stops
+    # at its iteration floor, as in the tests above): the solution to compare with
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    monkeypatch.setenv("SGPU_AMG_VERBOSE", "1")  # the set-up names the path of each level
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(B)
+        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_GALERKIN", "sort")
+        log0 = capfd.readouterr().err
+        x1, r1 = _solve_with_env(dm, f, "mixed", "SGPU_GALERKIN", None)
+        log1 = capfd.readouterr().err
+    assert "galerkin product (sort)" in log0 and "galerkin product (rows)" not in log0
+    if case == "dense_graph":
+        assert "galerkin product (sort)" in log1  # the row pass handed the level over
+    else:
+        assert "galerkin product (rows)" in log1 and "galerkin product (sort)" not in log1
+    assert r0.status == r1.status == L.OK
+    assert r0.info["precond_levels"] == r1.info["precond_levels"]
+    assert r0.info["precond_coarse_n"] == r1.info["precond_coarse_n"]
+    assert abs(r0.info["iterations"] - r1.info["iterations"]) <= 1
+    for x in (x0, x1):
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_streamed_level0_products_agree(oracle, gpu_lib):
+    # SGPU_LV0_TMA=1: the FP32 level-0 products stream tiles of 32 block rows
+    # through shared memory with bulk copies; the same sums per row, so the
+    # same solve to rounding
+    m = decks.cantilever_hex(60, 12, 12)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_LV0_TMA", None)
+        x1, r1 = _solve_with_env(dm, f, "mixed", "SGPU_LV0_TMA", "1")
+    assert r0.status == r1.status == L.OK
+    assert abs(r0.info["iterations"] - r1.info["iterations"]) <= 1
+    for x in (x0, x1):
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+def test_device_loop_and_chunked_iterations_agree(oracle, gpu_lib):
+    # the flexible CG's iterations as one graph with a device-side WHILE node
+    # against graphs of 8 iterations with a host test between them: the same
+    # kernels in the same order, so the same bits and iteration count
+    m = decks.cantilever_hex(40, 8, 8)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        for crit in (None, "true"):
+            out = []
+            for loop in (None, "chunk"):
+                import os
+                old = os.environ.get("SGPU_FCG_LOOP")
+                if loop is None:
+                    os.environ.pop("SGPU_FCG_LOOP", None)
+                else:
+                    os.environ["SGPU_FCG_LOOP"] = loop
+                try:
+                    kw = {"crit": crit} if crit else {}
+                    out.append(dm.pcg(f, res=1e-11 if crit else 1e-22, prec="agg", mode="mixed", **kw))
+                finally:
+                    if old is None:
+                        os.environ.pop("SGPU_FCG_LOOP", None)
+                    else:
+                        os.environ["SGPU_FCG_LOOP"] = old
+            (x0, r0), (x1, r1) = out
+            assert r0.status == r1.status == L.OK
+            assert r0.info["iterations"] == r1.info["iterations"]
+            assert np.array_equal(x0, x1)

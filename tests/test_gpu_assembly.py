@@ -1,10 +1,10 @@
 """GPU assembly of the hexahedral stiffness matrix by rows (one warp per node,
-every CSR entry written once) against the oracle's stiffness_matrix
-(MEFEL/SRC/globmat.cpp:41 with linhex::gl_stiffness_matrix and
-symcomprow::localize), and against the colour-ordered element scatter that
-serves the other element kinds: partially constrained nodes (the per-entry
-search), several materials, distorted elements, and a node whose rows do not
-fit the row kernel (the fallback to the colour-ordered scatter)."""
+every CSR entry written once; SGPU_ASSEMBLY_ROWS=1) against the oracle's
+stiffness_matrix (MEFEL/SRC/globmat.cpp:41 with linhex::gl_stiffness_matrix
+and symcomprow::localize), and against the default colour-ordered element
+scatter: partially constrained nodes (the per-entry search), several
+materials, distorted elements, and a node whose rows do not fit the row
+kernel (the fallback to the colour-ordered scatter)."""
 import os
 
 import numpy as np
@@ -17,16 +17,16 @@ pytestmark = pytest.mark.gpu
 
 def _download(m, colours):
     from ssf_b200 import mefel
-    old = os.environ.pop("SGPU_ASSEMBLY_COLOURS", None)
-    if colours:
-        os.environ["SGPU_ASSEMBLY_COLOURS"] = "1"
+    old = os.environ.pop("SGPU_ASSEMBLY_ROWS", None)
+    if not colours:
+        os.environ["SGPU_ASSEMBLY_ROWS"] = "1"
     try:
         with mefel.stiffness_matrix(m) as K:
             return K.download(symmetric=1), K.assembly
     finally:
-        os.environ.pop("SGPU_ASSEMBLY_COLOURS", None)
+        os.environ.pop("SGPU_ASSEMBLY_ROWS", None)
         if old is not None:
-            os.environ["SGPU_ASSEMBLY_COLOURS"] = old
+            os.environ["SGPU_ASSEMBLY_ROWS"] = old
 
 
 def _check(oracle, m):
