@@ -39,6 +39,7 @@
 // (flexible CG: the FP32 preconditioner is not exactly the same linear map at
 // every call); the residual, the solution update, alpha and beta are FP64.
 #include <cooperative_groups.h>
+#include <cuda_fp16.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -343,6 +344,122 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? 4 : (UNR > 2 ? 4 : 6))
     if (sub < 3 && br < nb) op.row(3 * br + sub, sub == 0 ? y0 : (sub == 1 ? y1 : y2), acc);
   }
   op_reduce<Op>(op, acc, st, partials, ticket);
+}
+
+// ----- level 0 of the FP32 cycle with half-precision values -----
+// The scaled level-0 matrix S K S has a unit diagonal and |a_ij| <= 1 (an SPD
+// matrix has a_ij^2 <= a_ii a_jj), so binary16 holds its entries with a
+// relative rounding of 2^-11 and no overflow; entries below 2^-14 lose
+// relative precision (absolutely at most 2^-25 against the unit diagonal).
+// The cycle is a preconditioner of a flexible CG whose residual and update
+// stay FP64, so this rounding changes the preconditioner slightly, never the
+// answer, and halves the bytes of the two level-0 products of every cycle.
+// Arithmetic and the vectors stay FP32.
+//
+// Layout: block row br holds blocks [hptr[br], hptr[br+1]) of the padded
+// arrays, a multiple of four; value (comp, j) of the row at
+// hval[9 hptr[br] + comp len + j].  A lane takes four consecutive blocks: one
+// 16-byte load of their columns and nine 8-byte loads of their components.
+__device__ __forceinline__ float2 h2f(unsigned bits) {
+  __half2 h;
+  memcpy(&h, &bits, sizeof(h));
+  return __half22float2(h);
+}
+
+template <int LPR, int UNR, class Op>
+__global__ void __launch_bounds__(TPB, UNR == 2 ? 4 : 6)
+    k_lv_h16(int nb, const int *__restrict__ hptr, const int *__restrict__ hcol, const uint16_t *__restrict__ hval,
+             const float *__restrict__ v, Op op, PcgState *st, double *partials, unsigned *ticket) {
+  if (st->done) return;
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, g = lane / LPR, sub = lane % LPR;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double acc[Op::NV > 0 ? Op::NV : 1] = {};
+  for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
+    const int br = base + g;
+    int s = 0, len = 0;
+    if (br < nb) { s = __ldg(hptr + br); len = __ldg(hptr + br + 1) - s; }
+    const uint16_t *bv = hval + 9ll * s;
+    float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+    for (int j = 4 * sub; j < len; j += 4 * LPR * UNR) {
+      int4 c[UNR];
+      uint2 a[UNR][9];
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        const int ju = j + 4 * LPR * u;
+        if (ju < len) {
+          c[u] = __ldcs(reinterpret_cast<const int4 *>(hcol + s + ju));
+#pragma unroll
+          for (int q = 0; q < 9; q++) a[u][q] = __ldcs(reinterpret_cast<const uint2 *>(bv + q * len + ju));
+        } else {
+          c[u] = make_int4(0, 0, 0, 0);
+#pragma unroll
+          for (int q = 0; q < 9; q++) a[u][q] = make_uint2(0u, 0u);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        if (j + 4 * LPR * u >= len) continue;
+        const int cols[4] = {c[u].x, c[u].y, c[u].z, c[u].w};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {  // blocks 2h, 2h+1 of the four
+          float2 w[9];
+#pragma unroll
+          for (int q = 0; q < 9; q++) w[q] = h2f(h == 0 ? a[u][q].x : a[u][q].y);
+          const int ca = cols[2 * h], cb = cols[2 * h + 1];
+          const float xa0 = __ldg(v + 3 * ca), xa1 = __ldg(v + 3 * ca + 1), xa2 = __ldg(v + 3 * ca + 2);
+          const float xb0 = __ldg(v + 3 * cb), xb1 = __ldg(v + 3 * cb + 1), xb2 = __ldg(v + 3 * cb + 2);
+          y0 += w[0].x * xa0 + w[1].x * xa1 + w[2].x * xa2 + w[0].y * xb0 + w[1].y * xb1 + w[2].y * xb2;
+          y1 += w[3].x * xa0 + w[4].x * xa1 + w[5].x * xa2 + w[3].y * xb0 + w[4].y * xb1 + w[5].y * xb2;
+          y2 += w[6].x * xa0 + w[7].x * xa1 + w[8].x * xa2 + w[6].y * xb0 + w[7].y * xb1 + w[8].y * xb2;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      y0 += __shfl_xor_sync(0xffffffffu, y0, o, LPR);
+      y1 += __shfl_xor_sync(0xffffffffu, y1, o, LPR);
+      y2 += __shfl_xor_sync(0xffffffffu, y2, o, LPR);
+    }
+    if (sub < 3 && br < nb) op.row(3 * br + sub, sub == 0 ? y0 : (sub == 1 ? y1 : y2), acc);
+  }
+  op_reduce<Op>(op, acc, st, partials, ticket);
+}
+
+// padded row lengths (multiples of four blocks)
+__global__ void k_h16_len(int nb, const int *__restrict__ browptr, int *__restrict__ len) {
+  for (int br = blockIdx.x * blockDim.x + threadIdx.x; br < nb; br += gridDim.x * blockDim.x)
+    len[br] = (browptr[br + 1] - browptr[br] + 3) & ~3;
+}
+
+// padded columns: one warp per block row
+__global__ void k_h16_cols(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                           const int *__restrict__ hptr, int *__restrict__ hcol) {
+  const int lane = threadIdx.x & 31;
+  for (int br = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; br < nb; br += (gridDim.x * blockDim.x) >> 5) {
+    const int s = browptr[br], len = browptr[br + 1] - s;
+    const int hs = hptr[br], hlen = hptr[br + 1] - hs;
+    for (int j = lane; j < hlen; j += 32) hcol[hs + j] = j < len ? bcol[s + j] : br;
+  }
+}
+
+// padded binary16 values from the scaled FP32 values (round to nearest even):
+// one warp per block row, over its (component, block) pairs
+__global__ void k_h16_vals(int nb, const int *__restrict__ browptr, const float *__restrict__ b32,
+                           const int *__restrict__ hptr, uint16_t *__restrict__ hval) {
+  const int lane = threadIdx.x & 31;
+  for (int br = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; br < nb; br += (gridDim.x * blockDim.x) >> 5) {
+    const int s = browptr[br], len = browptr[br + 1] - s;
+    const int hs = hptr[br], hlen = hptr[br + 1] - hs;
+    for (int t = lane; t < 9 * hlen; t += 32) {
+      const int q = t / hlen, j = t - q * hlen;
+      const __half h = __float2half_rn(j < len ? b32[9ll * s + (int64_t)q * len + j] : 0.f);
+      uint16_t bits;
+      memcpy(&bits, &h, sizeof(bits));
+      hval[9ll * hs + t] = bits;
+    }
+  }
 }
 
 // ----- level 0 in FP32 BSR3, streamed through shared memory by bulk copies -----
@@ -2492,6 +2609,96 @@ bool launch_level0_tma(sgpu_matrix m, const AmgLevel &L, const float *v, const O
   return true;
 }
 
+// Half-precision level-0 values for the FP32 cycle: on unless SGPU_LV0_H16=0
+// (read at every use, so a process can compare both forms).
+bool level0_h16_enabled() {
+  const char *e = getenv("SGPU_LV0_H16");
+  return !(e && !strcmp(e, "0"));
+}
+
+// lanes per block row and four-block groups in flight per lane of k_lv_h16:
+// SGPU_LV0_H16_SHAPE = "lanes,groups" (4 or 8 lanes, 1 or 2 groups)
+void level0_h16_shape(int *lanes, int *groups) {
+  *lanes = 8;
+  *groups = 1;
+  if (const char *e = getenv("SGPU_LV0_H16_SHAPE")) {
+    int l = 0, u = 0;
+    if (sscanf(e, "%d,%d", &l, &u) == 2 && (l == 4 || l == 8) && (u == 1 || u == 2)) {
+      *lanes = l;
+      *groups = u;
+    }
+  }
+}
+
+// The padded pattern (once per handle) and the binary16 values (once per
+// FP32 set-up) of level 0; stream-ordered on s, never inside a capture.
+int ensure_level0_h16(sgpu_matrix m, cudaStream_t s) {
+  Amg &A = *m->amg;
+  Bsr3 &b = m->bsr;
+  if (!b.valid || !b.have32 || !level0_h16_enabled()) return SGPU_OK;
+  if (!A.h16_struct) {
+    const int nb = b.nb;
+    TmpBuf<int> len(s);
+    SGPU_TRY(len.alloc((size_t)nb + 1));
+    k_h16_len<<<grid_for(nb), TPB, 0, s>>>(nb, b.browptr.p, len.p);
+    SGPU_CUDA(cudaMemsetAsync(len.p + nb, 0, sizeof(int), s));
+    SGPU_TRY(A.h16ptr.alloc((size_t)nb + 1));
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, len.p, A.h16ptr.p, nb + 1, s);
+    TmpBuf<unsigned char> t(s);
+    SGPU_TRY(t.alloc(tmp));
+    cub::DeviceScan::ExclusiveSum(t.p, tmp, len.p, A.h16ptr.p, nb + 1, s);
+    int total = 0;
+    SGPU_TRY(read_int(A.h16ptr.p + nb, s, &total));
+    A.h16_nblk = total;
+    SGPU_TRY(A.h16col.alloc((size_t)total));
+    SGPU_TRY(A.h16val.alloc((size_t)total * 9));
+    k_h16_cols<<<grid_for((int64_t)nb * 32), TPB, 0, s>>>(nb, b.browptr.p, b.bcol.p, A.h16ptr.p, A.h16col.p);
+    count_launches(2);
+    SGPU_CUDA(cudaGetLastError());
+    A.h16_struct = true;
+  }
+  if (!A.h16_vals) {
+    k_h16_vals<<<grid_for((int64_t)b.nb * 32), TPB, 0, s>>>(b.nb, b.browptr.p, b.bval32s.p, A.h16ptr.p,
+                                                             A.h16val.p);
+    count_launches(1);
+    SGPU_CUDA(cudaGetLastError());
+    A.h16_vals = true;
+  }
+  return SGPU_OK;
+}
+
+// launches the half-precision level-0 product; false when its values are not
+// there (another level-0 form runs)
+template <class Op>
+bool launch_level0_h16(sgpu_matrix m, const AmgLevel &L, const float *v, const Op &op, cudaStream_t s,
+                       unsigned *ticket) {
+  const Amg &A = *m->amg;
+  if (!A.h16_vals || !level0_h16_enabled()) return false;
+  int lanes = 8, groups = 1;
+  level0_h16_shape(&lanes, &groups);
+  PcgState *st = pcg_state(m);
+  double *part = m->w.partials.p;
+  if (lanes == 4 && groups == 2) {
+    auto k = k_lv_h16<4, 2, Op>;
+    k<<<resident_grid(k, (L.nb + 7) / 8), TPB, 0, s>>>(L.nb, A.h16ptr.p, A.h16col.p, A.h16val.p, v, op, st, part,
+                                                     ticket);
+  } else if (lanes == 4) {
+    auto k = k_lv_h16<4, 1, Op>;
+    k<<<resident_grid(k, (L.nb + 7) / 8), TPB, 0, s>>>(L.nb, A.h16ptr.p, A.h16col.p, A.h16val.p, v, op, st, part,
+                                                     ticket);
+  } else if (groups == 2) {
+    auto k = k_lv_h16<8, 2, Op>;
+    k<<<resident_grid(k, (L.nb + 3) / 4), TPB, 0, s>>>(L.nb, A.h16ptr.p, A.h16col.p, A.h16val.p, v, op, st, part,
+                                                     ticket);
+  } else {
+    auto k = k_lv_h16<8, 1, Op>;
+    k<<<resident_grid(k, (L.nb + 3) / 4), TPB, 0, s>>>(L.nb, A.h16ptr.p, A.h16col.p, A.h16val.p, v, op, st, part,
+                                                     ticket);
+  }
+  return true;
+}
+
 // the level-0 lanes per row follow the tuned SpMV of the same precision
 int level0_lanes(const sgpu_matrix m, bool fp32) {
   const SpmvPlan &p = fp32 ? m->plan32 : m->plan64;
@@ -2509,7 +2716,10 @@ int launch_level(sgpu_matrix m, const AmgLevel &L, const T *v, const Op &op, cud
   if (L.layout == 1) {
     const int lanes = level0_lanes(m, sizeof(T) == 4);
     bool streamed = false;
-    if constexpr (sizeof(T) == 4) streamed = launch_level0_tma<Op>(m, L, v, op, s, tk);
+    if constexpr (sizeof(T) == 4) {
+      streamed = launch_level0_h16<Op>(m, L, v, op, s, tk);
+      if (!streamed) streamed = launch_level0_tma<Op>(m, L, v, op, s, tk);
+    }
     if (streamed) {
     } else if (sizeof(T) == 4 && lanes == 8 && level0_unroll() == 4) {
       auto k = k_lv_bsr3<T, 8, Op, 4>;
@@ -2693,6 +2903,7 @@ int amg_build(sgpu_matrix m) {
   SGPU_TRY(ensure_bsr3(m));
   SGPU_TRY(ensure_fp32(m));  // scaled FP32 level 0 and S = diag^-1/2
   SGPU_TRY(level0_tile_plan(m, s));
+  if (A.want_fp32) SGPU_TRY(ensure_level0_h16(m, s));  // before the level-0 bound below reads it
   const int n = (int)m->n;
   keep_pool_memory();
   CubTmp tmp(s);
@@ -2816,6 +3027,7 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
   cudaStream_t s = m->stream;
   PhaseClock clk(s);
   if (fp32 && !A.have32) {
+    SGPU_TRY(ensure_level0_h16(m, s));
     for (size_t l = 0; l < A.lv.size(); l++) {
       AmgLevel &L = *A.lv[l];
       SGPU_TRY(L.v32.alloc(L.n));
@@ -3400,6 +3612,7 @@ int amg_ensure(sgpu_matrix m, bool fp32, float *setup_ms) {
     SGPU_TRY(write_st(m, &zero_st));  // set-up kernels run with a live state
   }
   A.l0_bound_wanted = fp32 && !A.built && !getenv("SGPU_AMG_SERIAL_BOUND");
+  A.want_fp32 = fp32;
   if (!A.built) {
     const int rc = amg_build(m);
     if (rc != SGPU_OK) {

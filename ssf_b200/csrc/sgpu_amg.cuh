@@ -119,6 +119,17 @@ struct Amg {
   bool l0_bound_wanted = false;
   DevBuf<float> lz32;    // 5 vectors of n
   DevBuf<double> lz_ab;  // Lanczos coefficients
+  // Level 0 of the FP32 cycle with half-precision values (3x3 block rows
+  // only): every block row padded to a multiple of four blocks (padding:
+  // value 0, the row's own column), values component-major per padded row,
+  // so that a lane reads one component of four blocks in one 8-byte load.
+  // The padded pattern is kept for the handle's life (the pattern of a handle
+  // never changes); the values are converted at every FP32 set-up.
+  bool want_fp32 = false;  // the set-up under way is for the FP32 cycle
+  bool h16_struct = false, h16_vals = false;
+  int64_t h16_nblk = 0;     // stored blocks, padding included
+  DevBuf<int> h16ptr, h16col;
+  DevBuf<uint16_t> h16val;  // IEEE binary16 bit patterns
   ~Amg() {
     for (AmgLevel *l : pool) delete l;
     if (side) {
@@ -130,6 +141,7 @@ struct Amg {
   void clear() {
     lv.clear();
     built = have32 = have64 = false;
+    h16_vals = false;
   }
   AmgLevel *take_level(size_t depth) {
     while (pool.size() <= depth) pool.push_back(new AmgLevel());

@@ -452,6 +452,246 @@ __global__ void __launch_bounds__(TPB) k_hex8_elastic(int ne_c, const int *__res
 }
 
 // ---------------------------------------------------------------------------
+// hex8 isotropic elasticity, colour-ordered like k_hex8_elastic, with the
+// arithmetic cut down so that the kernel is bound by its scatter:
+//   * every lane works on the Gauss points: lane = gp + 8 q forms the
+//     Jacobian of point gp and the Cartesian gradients of nodes 2q, 2q+1
+//     (one reciprocal of detJ instead of a division per gradient entry);
+//   * for the isotropic D of elastisomat (MEFEL/SRC/elastisomat.cpp:395-420),
+//     with lambda = E nu / ((1+nu)(1-2nu)) and mu = E / (2 (1+nu)), the block
+//     (a,b) of sum_gp |J| B_a^T D B_b (linhex::gl_stiffness_matrix,
+//     MEFEL/SRC/linhex.cpp:583-630) is
+//         K_ab = lambda P + mu P^T + mu tr(P) I,  P = sum_gp |J| g_a g_b^T,
+//     9 FMA per point instead of the full B^T D B product;
+//   * the element matrix is symmetric: the 36 pairs a <= b are formed once
+//     (lanes 0..27 the 28 pairs a < b, lanes 28..31 two diagonal pairs each)
+//     and K_ba = K_ab^T is scattered beside K_ab, so every lane scatters two
+//     blocks.
+// The same sums as the reference's up to rounding (the reciprocal and the
+// regrouped products: relative differences of a few units of 1e-16).
+// ---------------------------------------------------------------------------
+// dN_a/dxi, dN_a/deta, dN_a/dzeta of one node (the expressions of hex_dnat)
+__device__ __forceinline__ void hex_dnat1(int a, double xi, double eta, double zeta, double &nx, double &ny,
+                                          double &nz) {
+  const double sx = ((a + 1) & 2) ? -1.0 : 1.0;  // +, -, -, +, +, -, -, +
+  const double sy = (a & 2) ? -1.0 : 1.0;        // +, +, -, -, +, +, -, -
+  const double sz = (a & 4) ? -1.0 : 1.0;        // +, +, +, +, -, -, -, -
+  nx = sx * (1.0 + sy * eta) * (1.0 + sz * zeta) / 8.0;
+  ny = sy * (1.0 + sx * xi) * (1.0 + sz * zeta) / 8.0;
+  nz = sz * (1.0 + sx * xi) * (1.0 + sy * eta) / 8.0;
+}
+
+constexpr int kIsoRowCap = 96;  // columns of one row held in shared memory
+
+struct HexIsoShared {
+  double g[8][8][3];  // [gp][node][x, y, z]
+  double w[8];        // |detJ| (weights are 1)
+  int rp[24];         // rowptr of the element's equations
+  int rl[8];          // length of node a's rows when its three equations are
+                      // consecutive with rows of one length (<= kIsoRowCap), else -1
+  int cols[8][kIsoRowCap];  // the column list of node a's first row
+};
+
+// 4-byte global -> shared copy that completes asynchronously (cp.async)
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// position of column c in the sorted shared list cols[0, len), or -1
+__device__ __forceinline__ int find_in_shared(const int *cols, int len, int c) {
+  int lo = 0, hi = len - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = cols[mid];
+    if (v == c) return mid;
+    if (v < c) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+// adds block k at the rows of node A (equations rr) and the columns of node B
+// (equations cc).  The three rows of a node whose equations are consecutive
+// hold one column list in the full CSR (every row lists the free equations
+// of the node's neighbours), so with node A's list in shared memory one
+// search there places all nine entries; other blocks take block3_add.
+template <bool ROWCACHE>
+__device__ __forceinline__ void iso_scatter(const HexIsoShared &sh, int A, const int rr[3], const int cc[3],
+                                            const double k[3][3], const int *__restrict__ rowptr,
+                                            const int *__restrict__ col, double *__restrict__ val, unsigned *err) {
+  if (ROWCACHE) {
+    const int len = sh.rl[A];
+    if (len > 0 && cc[0] >= 0 && cc[1] == cc[0] + 1 && cc[2] == cc[0] + 2) {
+      const int p = find_in_shared(sh.cols[A], len, cc[0]);
+      if (p >= 0 && p + 2 < len && sh.cols[A][p + 1] == cc[1] && sh.cols[A][p + 2] == cc[2]) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          double *v = val + sh.rp[3 * A + i] + p;
+          v[0] += k[i][0];
+          v[1] += k[i][1];
+          v[2] += k[i][2];
+        }
+        return;
+      }
+    }
+  }
+  block3_add(rowptr, col, val, rr, cc, k, err);
+}
+
+// the pair (a, b), a < b, of index t in 0..27 (row-major over the upper triangle)
+__device__ __forceinline__ void upper_pair(int t, int &a, int &b) {
+  a = 0;
+  int left = t;
+  while (left >= 7 - a) { left -= 7 - a; a++; }
+  b = a + 1 + left;
+}
+
+__device__ __forceinline__ void hex_iso_block(const HexIsoShared &sh, int a, int b, double lam, double mu,
+                                              double k[3][3]) {
+  double P[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int gp = 0; gp < 8; gp++) {
+    const double w = sh.w[gp];
+    const double ax = w * sh.g[gp][a][0], ay = w * sh.g[gp][a][1], az = w * sh.g[gp][a][2];
+    const double bx = sh.g[gp][b][0], by = sh.g[gp][b][1], bz = sh.g[gp][b][2];
+    P[0][0] += ax * bx; P[0][1] += ax * by; P[0][2] += ax * bz;
+    P[1][0] += ay * bx; P[1][1] += ay * by; P[1][2] += ay * bz;
+    P[2][0] += az * bx; P[2][1] += az * by; P[2][2] += az * bz;
+  }
+  const double tr = mu * (P[0][0] + P[1][1] + P[2][2]);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) k[i][j] = lam * P[i][j] + mu * P[j][i] + (i == j ? tr : 0.0);
+}
+
+template <bool ROWCACHE>
+__global__ void __launch_bounds__(TPB, 3) k_hex8_iso(int ne_c, const int *__restrict__ elist,
+                                                     const double *__restrict__ coords,
+                                                     const int64_t *__restrict__ elems,
+                                                     const int *__restrict__ cne, const double *__restrict__ emat,
+                                                     const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                     double *__restrict__ val, unsigned *err) {
+  __shared__ HexIsoShared shm[WPB];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexIsoShared &sh = shm[wib];
+  const int gp = lane & 7, q = lane >> 3;
+  const double xi = c_gp2[(gp >> 2) & 1], eta = c_gp2[(gp >> 1) & 1], zeta = c_gp2[gp & 1];
+  for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
+    const int e = elist[t];
+    double cx = 0, cy = 0, cz = 0;
+    if (lane < 8) {
+      const int64_t nd = elems[(int64_t)e * 8 + lane];
+      cx = coords[3 * nd]; cy = coords[3 * nd + 1]; cz = coords[3 * nd + 2];
+    }
+    const int code = lane < 24 ? __ldg(cne + (int64_t)e * 24 + lane) : -1;
+    if (ROWCACHE) {
+      // the rows of the element's equations; node a's column list copied
+      // into shared memory while the Gauss points are formed
+      int rpv = -1, rlen = 0;
+      if (code >= 0) {
+        rpv = __ldg(rowptr + code);
+        rlen = __ldg(rowptr + code + 1) - rpv;
+      }
+      const int na = lane & 7;
+      const int c0 = __shfl_sync(0xffffffffu, code, 3 * na), c1 = __shfl_sync(0xffffffffu, code, 3 * na + 1),
+                c2 = __shfl_sync(0xffffffffu, code, 3 * na + 2);
+      const int l0 = __shfl_sync(0xffffffffu, rlen, 3 * na), l1 = __shfl_sync(0xffffffffu, rlen, 3 * na + 1),
+                l2 = __shfl_sync(0xffffffffu, rlen, 3 * na + 2);
+      if (lane < 24) sh.rp[lane] = rpv;
+      if (lane < 8)
+        sh.rl[lane] = (c0 >= 0 && c1 == c0 + 1 && c2 == c0 + 2 && l0 == l1 && l1 == l2 && l0 > 0 &&
+                       l0 <= kIsoRowCap) ? l0 : -1;
+      __syncwarp();
+#pragma unroll
+      for (int a = 0; a < 8; a++) {
+        const int len = sh.rl[a];
+        if (len > 0) {
+          const int *src = col + sh.rp[3 * a];
+          for (int j = lane; j < len; j += 32) cp_async4(&sh.cols[a][j], src + j);
+        }
+      }
+    }
+    // Jacobian of point gp (every lane of the point's four computes it)
+    double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0;
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      const double x = __shfl_sync(0xffffffffu, cx, a), y = __shfl_sync(0xffffffffu, cy, a),
+                   z = __shfl_sync(0xffffffffu, cz, a);
+      double nxa, nya, nza;
+      hex_dnat1(a, xi, eta, zeta, nxa, nya, nza);
+      d1 += nxa * x; d2 += nya * x; d3 += nza * x;
+      d4 += nxa * y; d5 += nya * y; d6 += nza * y;
+      d7 += nxa * z; d8 += nya * z; d9 += nza * z;
+    }
+    const double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+    const double ij = 1.0 / jac;
+    // cofactors of derivatives_3d (GEFEL/difcalc.cpp:487-565), scaled by 1/detJ
+    const double c11 = (d5 * d9 - d8 * d6) * ij, c12 = (d7 * d6 - d9 * d4) * ij, c13 = (d4 * d8 - d7 * d5) * ij;
+    const double c21 = (d8 * d3 - d9 * d2) * ij, c22 = (d1 * d9 - d7 * d3) * ij, c23 = (d7 * d2 - d8 * d1) * ij;
+    const double c31 = (d2 * d6 - d5 * d3) * ij, c32 = (d4 * d3 - d6 * d1) * ij, c33 = (d1 * d5 - d4 * d2) * ij;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int a = 2 * q + h;
+      double ddx, ddy, ddz;
+      hex_dnat1(a, xi, eta, zeta, ddx, ddy, ddz);
+      sh.g[gp][a][0] = ddx * c11 + ddy * c12 + ddz * c13;
+      sh.g[gp][a][1] = ddx * c21 + ddy * c22 + ddz * c23;
+      sh.g[gp][a][2] = ddx * c31 + ddy * c32 + ddz * c33;
+    }
+    if (q == 0) sh.w[gp] = fabs(jac);
+    const double E = __ldg(emat + 2 * (int64_t)e), nu = __ldg(emat + 2 * (int64_t)e + 1);
+    const double mu = E / 2.0 / (1.0 + nu);
+    const double lam = E / (1.0 + nu) / (1.0 - 2.0 * nu) * nu;
+    if (ROWCACHE) cp_async_wait_all();
+    __syncwarp();
+    // first block: lanes < 28 the pair a < b of their index, lanes 28..31
+    // the diagonal pair (2 (lane - 28), same)
+    int a0, b0;
+    if (lane < 28) {
+      upper_pair(lane, a0, b0);
+    } else {
+      a0 = b0 = 2 * (lane - 28);
+    }
+    double k[3][3];
+    hex_iso_block(sh, a0, b0, lam, mu, k);
+    int rr[3], cc[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      rr[i] = __shfl_sync(0xffffffffu, code, 3 * a0 + i);
+      cc[i] = __shfl_sync(0xffffffffu, code, 3 * b0 + i);
+    }
+    iso_scatter<ROWCACHE>(sh, a0, rr, cc, k, rowptr, col, val, err);
+    // second block: the transpose at (b, a), or the next diagonal pair
+    int a1, b1;
+    if (lane < 28) {
+      a1 = b0;
+      b1 = a0;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = i + 1; j < 3; j++) {
+          const double tmp = k[i][j];
+          k[i][j] = k[j][i];
+          k[j][i] = tmp;
+        }
+    } else {
+      a1 = b1 = 2 * (lane - 28) + 1;
+      hex_iso_block(sh, a1, b1, lam, mu, k);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      rr[i] = __shfl_sync(0xffffffffu, code, 3 * a1 + i);
+      cc[i] = __shfl_sync(0xffffffffu, code, 3 * b1 + i);
+    }
+    iso_scatter<ROWCACHE>(sh, a1, rr, cc, k, rowptr, col, val, err);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // hex8 isotropic elasticity by rows: one warp per node forms the node's CSR
 // rows from its incident elements in shared memory and writes them once.
 //
@@ -1656,6 +1896,20 @@ struct AssemblyData {
   bool node_rows = false;
 };
 
+// SGPU_HEX8_FULL=1: isotropic hexahedra through the full B^T D B product of
+// k_hex8_elastic instead of k_hex8_iso (read at every assembly)
+bool hex8_full_product() {
+  const char *e = std::getenv("SGPU_HEX8_FULL");
+  return e && !strcmp(e, "1");
+}
+
+// SGPU_HEX8_ROWCACHE=0: k_hex8_iso searches every block's row in global
+// memory instead of in the shared-memory copy of the element's rows
+bool hex8_row_cache() {
+  const char *e = std::getenv("SGPU_HEX8_ROWCACHE");
+  return !(e && !strcmp(e, "0"));
+}
+
 int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
   cudaStream_t s = m->stream;
   Csr &c = m->csr;
@@ -1697,9 +1951,15 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
         if (ad.general)
           k_hex8_elastic<true><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
                                                     c.rowptr.p, c.col.p, c.val.p, err.p);
-        else
+        else if (hex8_full_product())
           k_hex8_elastic<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
                                                      c.rowptr.p, c.col.p, c.val.p, err.p);
+        else if (hex8_row_cache())
+          k_hex8_iso<true><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, c.rowptr.p,
+                                                c.col.p, c.val.p, err.p);
+        else
+          k_hex8_iso<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                 c.rowptr.p, c.col.p, c.val.p, err.p);
         break;
       case 1:
         k_quad4_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,

@@ -343,10 +343,11 @@ def test_galerkin_by_aggregate_rows_matches_the_sort_path(oracle, gpu_lib, case,
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
 
 
-def test_streamed_level0_products_agree(oracle, gpu_lib):
+def test_streamed_level0_products_agree(oracle, gpu_lib, monkeypatch):
     # SGPU_LV0_TMA=1: the FP32 level-0 products stream tiles of 32 block rows
     # through shared memory with bulk copies; the same sums per row, so the
-    # same solve to rounding
+    # same solve to rounding (both against the FP32-valued level 0)
+    monkeypatch.setenv("SGPU_LV0_H16", "0")
     m = decks.cantilever_hex(60, 12, 12)
     adr, ci, a = _oracle_system(oracle, m)
     f = oracle.load_vector(m)
@@ -391,3 +392,31 @@ def test_device_loop_and_chunked_iterations_agree(oracle, gpu_lib):
             assert r0.status == r1.status == L.OK
             assert r0.info["iterations"] == r1.info["iterations"]
             assert np.array_equal(x0, x1)
+
+
+@pytest.mark.parametrize("shape", [None, "4,1", "4,2", "8,2"])
+def test_half_precision_level0_values(oracle, gpu_lib, shape, monkeypatch):
+    # the FP32 cycle's level 0 with binary16 values (the default for 3x3
+    # block rows) against FP32 values (SGPU_LV0_H16=0): the preconditioner
+    # changes by a rounding of 2^-11, the flexible CG's FP64 residual and
+    # update do not, so both reach the oracle's solution within the FP64
+    # drop-in's 1e-8 in about the same number of iterations; every lane shape
+    # of the half-precision product does too
+    if shape:
+        monkeypatch.setenv("SGPU_LV0_H16_SHAPE", shape)
+    m = decks.cantilever_hex(60, 12, 12)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x16, r16 = _solve_with_env(dm, f, "mixed", "SGPU_LV0_H16", None)
+        x32, r32 = _solve_with_env(dm, f, "mixed", "SGPU_LV0_H16", "0")
+        # a second set-up on the same handle converts the values again
+        x16b, r16b = _solve_with_env(dm, f, "mixed", "SGPU_LV0_H16", None)
+    assert r16.status == r32.status == r16b.status == L.OK
+    assert r16.info["iterations"] <= r32.info["iterations"] + 2
+    assert np.array_equal(x16, x16b)
+    assert not np.array_equal(x16, x32)  # the half-precision product really ran
+    for x in (x16, x32):
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8

@@ -1,5 +1,8 @@
-"""GPU assembly of the hexahedral stiffness matrix by rows (one warp per node,
-every CSR entry written once; SGPU_ASSEMBLY_ROWS=1) against the oracle's
+"""GPU assembly of the hexahedral stiffness matrix in its three forms -- the
+default colour-ordered element scatter on the pairs a <= b with the
+isotropic P-form, the same scatter with the full B^T D B product
+(SGPU_HEX8_FULL=1), and rows (one warp per node, every CSR entry written
+once; SGPU_ASSEMBLY_ROWS=1) -- against the oracle's
 stiffness_matrix (MEFEL/SRC/globmat.cpp:41 with linhex::gl_stiffness_matrix
 and symcomprow::localize), and against the default colour-ordered element
 scatter: partially constrained nodes (the per-entry search), several
@@ -15,31 +18,42 @@ from ssf_b200 import decks
 pytestmark = pytest.mark.gpu
 
 
-def _download(m, colours):
+FORMS = {  # name: (SGPU_ASSEMBLY_ROWS, SGPU_HEX8_FULL)
+    "rows": ("1", None),      # one warp per node, rows written once
+    "iso": (None, None),      # colour-ordered, P-form on the pairs a <= b (default)
+    "full": (None, "1"),      # colour-ordered, full B^T D B product per block
+}
+
+
+def _download(m, form):
     from ssf_b200 import mefel
-    old = os.environ.pop("SGPU_ASSEMBLY_ROWS", None)
-    if not colours:
-        os.environ["SGPU_ASSEMBLY_ROWS"] = "1"
+    names = ("SGPU_ASSEMBLY_ROWS", "SGPU_HEX8_FULL")
+    old = {k: os.environ.pop(k, None) for k in names}
+    for k, v in zip(names, FORMS[form]):
+        if v is not None:
+            os.environ[k] = v
     try:
         with mefel.stiffness_matrix(m) as K:
             return K.download(symmetric=1), K.assembly
     finally:
-        os.environ.pop("SGPU_ASSEMBLY_ROWS", None)
-        if old is not None:
-            os.environ["SGPU_ASSEMBLY_ROWS"] = old
+        for k in names:
+            os.environ.pop(k, None)
+            if old[k] is not None:
+                os.environ[k] = old[k]
 
 
 def _check(oracle, m):
     adr, ci, a = oracle.assemble(m, sym=True)
     tol = 1e-12 * np.abs(a).max()
     out = {}
-    for colours in (False, True):
-        (g_adr, g_ci, g_a), info = _download(m, colours)
+    for form in FORMS:
+        (g_adr, g_ci, g_a), info = _download(m, form)
         assert np.array_equal(g_adr, adr) and np.array_equal(g_ci, ci)
-        assert np.allclose(g_a, a, rtol=1e-12, atol=tol), colours
-        out[colours] = g_a
-    # the two GPU forms differ only in rounding
-    assert np.allclose(out[False], out[True], rtol=1e-13, atol=1e-13 * np.abs(a).max())
+        assert np.allclose(g_a, a, rtol=1e-12, atol=tol), form
+        out[form] = g_a
+    # the GPU forms differ only in rounding
+    for form in ("rows", "full"):
+        assert np.allclose(out[form], out["iso"], rtol=1e-13, atol=1e-13 * np.abs(a).max()), form
     return out
 
 
@@ -94,4 +108,4 @@ def test_rows_match_on_the_cantilever(oracle, gpu_lib):
     m = decks.cantilever_hex(20, 4, 4)
     out = _check(oracle, m)
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c1_cantilever.npz"))
-    assert np.allclose(out[False], g["a"], rtol=1e-12, atol=1e-12 * np.abs(g["a"]).max())
+    assert np.allclose(out["iso"], g["a"], rtol=1e-12, atol=1e-12 * np.abs(g["a"]).max())
