@@ -368,6 +368,15 @@ def run_ours(args, ws, rank):
             barrier(ws)
             launches = L.kernel_launches() - l0
         ms = e0.elapsed_time(e1) / steps
+        if args.profile_step:
+            # one more step, untimed, inside a profiler range (ncu
+            # --profile-from-start off captures exactly its launches)
+            with torch.cuda.stream(stream):
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
+                solve(form)
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
         return dist_max(ms, ws), infos, launches
 
     forms = FORM_SETS[args.forms]
@@ -1017,6 +1026,9 @@ def main():
     ap.add_argument("--forms", default="all", choices=sorted(FORM_SETS),
                     help="GPU forms to run (profiling runs time one form only)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the e2e and CPU legs (profiling runs)")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="after each form's timed steps, one untimed step inside a profiler range "
+                         "(for ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3")

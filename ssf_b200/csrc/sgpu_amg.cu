@@ -452,13 +452,13 @@ __global__ void k_h16_vals(int nb, const int *__restrict__ browptr, const float 
   for (int br = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; br < nb; br += (gridDim.x * blockDim.x) >> 5) {
     const int s = browptr[br], len = browptr[br + 1] - s;
     const int hs = hptr[br], hlen = hptr[br + 1] - hs;
-    for (int t = lane; t < 9 * hlen; t += 32) {
-      const int q = t / hlen, j = t - q * hlen;
-      const __half h = __float2half_rn(j < len ? b32[9ll * s + (int64_t)q * len + j] : 0.f);
-      uint16_t bits;
-      memcpy(&bits, &h, sizeof(bits));
-      hval[9ll * hs + t] = bits;
-    }
+    for (int q = 0; q < 9; q++)
+      for (int j = lane; j < hlen; j += 32) {
+        const __half h = __float2half_rn(j < len ? b32[9ll * s + (int64_t)q * len + j] : 0.f);
+        uint16_t bits;
+        memcpy(&bits, &h, sizeof(bits));
+        hval[9ll * hs + (int64_t)q * hlen + j] = bits;
+      }
   }
 }
 
@@ -1356,6 +1356,55 @@ __global__ void k_mis_max(int nb, const int *__restrict__ browptr, const int *__
   }
 }
 
+// The same maximum with LPR lanes per node (coalesced column reads, the
+// neighbours' keys gathered in parallel, a shuffle maximum).  DECIDE: the
+// second pass of a round, which also makes the round's decision for its
+// nodes (k_mis_decide's rule, with m2 = the maximum it just formed), so a
+// round is two launches.  The keys and their maxima are those of the
+// thread-per-node form, so the independent set is the same.
+template <int LPR, bool DECIDE>
+__global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                            const int *__restrict__ agg, const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
+                            const int *go, uint64_t *__restrict__ t, int *__restrict__ undecided) {
+  if (*go == 0) return;
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, g = lane / LPR, sub = lane % LPR;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  int cnt = 0;
+  for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
+    const int i = base + g;
+    uint64_t m = 0;
+    if (i < nb) {
+      if (sub == 0) m = in[i];
+      const int re = browptr[i + 1];
+      for (int e = browptr[i] + sub; e < re; e += LPR) {
+        const int j = bcol[e];
+        if (agg == nullptr || agg[j] < 0) m = max(m, in[j]);
+      }
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) m = max(m, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)m, o, LPR));
+    if (i < nb && sub == 0) {
+      if (!DECIDE) {
+        out[i] = m;
+      } else {
+        const uint64_t ti = t[i];
+        if ((ti >> 62) == 1) {
+          if (m == ti) t[i] = mis_key(2, i);
+          else if ((m >> 62) == 2) t[i] = ti & ~(3ull << 62);
+          else cnt++;
+        }
+      }
+    }
+  }
+  if (DECIDE) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd(undecided, cnt);
+  }
+}
+
 // second-phase candidates: unaggregated nodes with at least `min_free`
 // unaggregated neighbours
 __global__ void k_mis_cand(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
@@ -1666,7 +1715,7 @@ __device__ __forceinline__ int gal_find(const GalTable &T, int H) {
 __global__ void __launch_bounds__(32 * kGalWarps)
     k_gal_count(int na, const int *__restrict__ aggptr, const int *__restrict__ aggnodes,
                 const int *__restrict__ browptr, const int *__restrict__ bcol, const int *__restrict__ agg,
-                int *__restrict__ cnt, int *__restrict__ lists, int *__restrict__ over) {
+                int *__restrict__ cnt, int *__restrict__ lists, int *__restrict__ over, int *__restrict__ maxn) {
   __shared__ GalTable tab[kGalWarps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int G = blockIdx.x * kGalWarps + w; G < na; G += gridDim.x * kGalWarps) {
@@ -1674,6 +1723,7 @@ __global__ void __launch_bounds__(32 * kGalWarps)
     if (lane == 0) {
       cnt[G] = n < 0 ? 0 : n;
       if (n < 0) atomicOr(over, 1);
+      else atomicMax(maxn, n);
     }
     for (int t = lane; t < n; t += 32) lists[(size_t)G * kGalCap + t] = tab[w].list[t];
     __syncwarp();
@@ -1866,6 +1916,149 @@ __global__ void __launch_bounds__(32 * kGalCtaWarps, 3)
     }
     for (int t = threadIdx.x; t < n; t += blockDim.x) cbcol[base + t] = T.list[t];
     for (int t = threadIdx.x; t < n * KK; t += blockDim.x) out[(size_t)base * KK + t] = acc[t];
+    __syncthreads();
+  }
+}
+
+// Coarse row G's values with warp-private accumulators (the default when no
+// coarse row has more than kGal2Cap blocks).  One CTA per aggregate; warp w
+// takes the aggregate's nodes w, w + 4, ... and a node's row in chunks of 32
+// entries.  Each lane forms T_ij = A_ij Q_j (B x K) for its entry and stages
+// it; the lanes of a chunk whose entries fall into one coarse block (one
+// aggregate H of j) form a group, and the group's lowest lane sums the group
+// in lane order and adds Q_i^T (that sum) into the warp's own accumulator of
+// block (G, H).  The four warps' accumulators are added in warp order at the
+// end.  Every sum has an order fixed by the data (nodes, entries, warps), so
+// every run gives the same bits; no thread walks another's products, which
+// the staging form above does with K*K threads over all 128 lanes' stages.
+constexpr int kGal2Cap = 40;  // blocks per coarse row
+constexpr int kGal2Warps = 4;
+
+template <int B, int K>
+constexpr size_t gal2_shared_bytes() {
+  // [W][kGal2Cap][K*K] accumulators, [W][32][B*K | 1] staging, [W][B*K] the
+  // current node's Q rows, the table
+  return ((size_t)kGal2Warps * kGal2Cap * K * K + (size_t)kGal2Warps * 32 * ((B * K) | 1) +
+          (size_t)kGal2Warps * B * K) * sizeof(double) + sizeof(GalTable);
+}
+
+template <int B, int K>
+__global__ void __launch_bounds__(32 * kGal2Warps)
+    k_gal_values2(int na, const int *__restrict__ aggptr, const int *__restrict__ aggnodes,
+                  const int *__restrict__ agg, LevelView A, const double *__restrict__ Q,
+                  const int *__restrict__ lists, const int *__restrict__ cbrowptr, int *__restrict__ cbcol,
+                  double *__restrict__ out) {
+  constexpr int KK = K * K, BK = B * K, SS = BK | 1, W = kGal2Warps;
+  extern __shared__ double gal2_sh[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *accs = gal2_sh;                                  // [W][kGal2Cap][KK]
+  double *stages = accs + (size_t)W * kGal2Cap * KK;       // [W][32][SS]
+  double *qis = stages + (size_t)W * 32 * SS;              // [W][BK]
+  GalTable &T = *reinterpret_cast<GalTable *>(qis + (size_t)W * BK);
+  double *acc = accs + (size_t)w * kGal2Cap * KK;
+  double *stage = stages + (size_t)w * 32 * SS;
+  double *qi = qis + (size_t)w * BK;
+  for (int G = blockIdx.x; G < na; G += gridDim.x) {
+    const int base = cbrowptr[G], n = cbrowptr[G + 1] - base;
+    for (int h = threadIdx.x; h < kGalHash; h += blockDim.x) T.key[h] = -1;
+    for (int t = threadIdx.x; t < W * n * KK; t += blockDim.x) {
+      const int ww = t / (n * KK);
+      accs[(size_t)ww * kGal2Cap * KK + (t - ww * n * KK)] = 0.0;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const int H = __ldg(lists + (size_t)G * kGalCap + t);
+      T.list[t] = H;
+      unsigned h = gal_hash(H);
+      for (int p = 0; p < kGalHash; p++) {  // n <= kGal2Cap < kGalHash keys: a free slot exists
+        if (atomicCAS(&T.key[h], -1, H) == -1) {
+          T.pos[h] = t;
+          break;
+        }
+        h = (h + 1) & (kGalHash - 1);
+      }
+    }
+    __syncthreads();
+    for (int a = aggptr[G] + w; a < aggptr[G + 1]; a += W) {
+      const int i = __ldg(aggnodes + a);
+      const int rs = __ldg(A.browptr + i), re = __ldg(A.browptr + i + 1);
+      for (int c = lane; c < BK; c += 32) qi[c] = __ldg(Q + (size_t)i * BK + c);
+      double di[B];
+#pragma unroll
+      for (int c = 0; c < B; c++) di[c] = A.layout == 0 ? 1.0 : __ldg(A.dscale + (size_t)B * i + c);
+      __syncwarp();
+      for (int t0 = rs; t0 < re; t0 += 32) {
+        const int e = t0 + lane;
+        const bool live = e < re;
+        int p = -1;
+        if (live) {
+          const int j = __ldg(A.bcol + e);
+          p = gal_find(T, __ldg(agg + j));
+          double av[B * B];
+          if (A.layout == 0) {
+#pragma unroll
+            for (int c = 0; c < B * B; c++) av[c] = __ldg(A.val + (size_t)e * B * B + c);
+          } else {
+            double dj[B];
+#pragma unroll
+            for (int c = 0; c < B; c++) dj[c] = __ldg(A.dscale + (size_t)B * j + c);
+            const int nbr = re - rs;
+#pragma unroll
+            for (int c = 0; c < B * B; c++) {
+              // layout 1: the row's blocks component-major; layout 2 (B = 1): CSR
+              const double v = A.layout == 1 ? __ldg(A.val + 9ll * rs + (int64_t)c * nbr + (e - rs))
+                                             : __ldg(A.val + e);
+              av[c] = v * di[c / B] * dj[c % B];
+            }
+          }
+#pragma unroll
+          for (int q2 = 0; q2 < K; q2++) {
+            double qj[B];
+#pragma unroll
+            for (int c2 = 0; c2 < B; c2++) qj[c2] = __ldg(Q + (size_t)j * BK + c2 * K + q2);
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+              double sacc = 0.0;
+#pragma unroll
+              for (int c2 = 0; c2 < B; c2++) sacc += av[c * B + c2] * qj[c2];
+              stage[lane * SS + c * K + q2] = sacc;
+            }
+          }
+        }
+        __syncwarp();
+        const bool ok = live && p >= 0;
+        const unsigned grp = __match_any_sync(0xffffffffu, ok ? p : -2 - lane);
+        if (ok && __ffs(grp) - 1 == lane) {
+          double sm[BK];
+#pragma unroll
+          for (int x = 0; x < BK; x++) sm[x] = 0.0;
+          for (unsigned mm = grp; mm; mm &= mm - 1) {
+            const double *src = stage + (__ffs(mm) - 1) * SS;
+#pragma unroll
+            for (int x = 0; x < BK; x++) sm[x] += src[x];
+          }
+          double *dst = acc + (size_t)p * KK;
+#pragma unroll
+          for (int q1 = 0; q1 < K; q1++)
+#pragma unroll
+            for (int q2 = 0; q2 < K; q2++) {
+              double v = 0.0;
+#pragma unroll
+              for (int c = 0; c < B; c++) v += qi[c * K + q1] * sm[c * K + q2];
+              dst[q1 * K + q2] += v;
+            }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n * KK; t += blockDim.x) {
+      double v = accs[t];
+#pragma unroll
+      for (int ww = 1; ww < W; ww++) v += accs[(size_t)ww * kGal2Cap * KK + t];
+      out[(size_t)base * KK + t] = v;
+    }
+    for (int t = threadIdx.x; t < n; t += blockDim.x) cbcol[base + t] = T.list[t];
     __syncthreads();
   }
 }
@@ -2226,6 +2419,11 @@ int read_int(const int *d, cudaStream_t s, int *out) {
 // on return the roots have state 2 in t.
 int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t, cudaStream_t s) {
   const int nb = L.nb, g = grid_for(nb);
+  // 8 lanes per node (SGPU_MIS=thread: a thread per node and a separate
+  // decision pass); the same rounds and the same set either way
+  const char *mis_env = getenv("SGPU_MIS");
+  const bool warp_rows = !(mis_env && !strcmp(mis_env, "thread"));
+  const int gw = grid_for((int64_t)nb * 8);
   constexpr int kMaxRounds = 200, kGroup = 8;
   TmpBuf<uint64_t> m1(s), m2(s);
   TmpBuf<int> cnt(s);
@@ -2244,10 +2442,17 @@ int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t
     if (rounds + kGroup > kMaxRounds) return fail(SGPU_CUDA_ERROR, "aggregation: independent-set rounds did not finish");
     for (int k = 0; k < kGroup; k++, rounds++) {
       const int *go = cnt.p + rounds;
-      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go);
-      k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, m2.p, go);
-      k_mis_decide<<<g, TPB, 0, s>>>(nb, t.p, m2.p, go, cnt.p + rounds + 1);
-      count_launches(3);
+      if (warp_rows) {
+        k_mis_max_w<8, false><<<gw, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go, nullptr, nullptr);
+        k_mis_max_w<8, true><<<gw, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, nullptr, go, t.p,
+                                                 cnt.p + rounds + 1);
+        count_launches(2);
+      } else {
+        k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go);
+        k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, m2.p, go);
+        k_mis_decide<<<g, TPB, 0, s>>>(nb, t.p, m2.p, go, cnt.p + rounds + 1);
+        count_launches(3);
+      }
     }
     SGPU_CUDA(cudaGetLastError());
     SGPU_TRY(read_int(cnt.p + rounds, s, &undecided));
@@ -2365,7 +2570,17 @@ int tentative(AmgLevel &L, int K, const double *Bl, double *Bnext, cudaStream_t 
 }
 
 template <int B, int K>
-int launch_gal_values(const AmgLevel &L, const LevelView &view, const int *lists, AmgLevel &C, cudaStream_t s) {
+int launch_gal_values(const AmgLevel &L, const LevelView &view, const int *lists, AmgLevel &C, cudaStream_t s,
+                      bool private_acc) {
+  if (private_acc) {
+    constexpr size_t sm2 = gal2_shared_bytes<B, K>();
+    SGPU_CUDA(cudaFuncSetAttribute(k_gal_values2<B, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    const int grid = (int)std::min<int64_t>(L.na, 64ll * kNumSMs);
+    k_gal_values2<B, K><<<grid, 32 * kGal2Warps, sm2, s>>>(L.na, L.aggptr.p, L.aggnodes.p, L.agg.p, view, L.Q64.p,
+                                                           lists, C.own_browptr.p, C.own_bcol.p, C.val64.p);
+    count_launches(1);
+    return SGPU_OK;
+  }
   constexpr size_t sm = gal_shared_bytes<K>();
   SGPU_CUDA(cudaFuncSetAttribute(k_gal_values<B, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int grid = (int)std::min<int64_t>(L.na, 64ll * kNumSMs);
@@ -2390,29 +2605,38 @@ int coarse_diagonals(AmgLevel &C, int K, cudaStream_t s) {
 
 // Galerkin product by aggregate rows (k_gal_count, a scan, k_gal_values);
 // *done stays false when a coarse row exceeds kGalCap blocks
+// SGPU_GALERKIN=staged: the by-rows Galerkin product through the staging
+// kernel (k_gal_values) even where the warp-private accumulators fit
+bool gal_staged_forced() {
+  const char *g = getenv("SGPU_GALERKIN");
+  return g && !strcmp(g, "staged");
+}
+
 int galerkin_direct(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_t s, CubTmp &tmp,
                     bool *done) {
   *done = false;
   const int na = L.na;
   TmpBuf<int> cnt(s), lists(s);
-  SGPU_TRY(cnt.alloc((size_t)na + 1));
+  SGPU_TRY(cnt.alloc((size_t)na + 2));
   SGPU_TRY(lists.alloc((size_t)na * kGalCap));
-  // cnt[na] is the overflow flag: the exclusive scan's last output leaves it out
-  SGPU_CUDA(cudaMemsetAsync(cnt.p + na, 0, sizeof(int), s));
+  // cnt[na] is the overflow flag (the exclusive scan's last output leaves it
+  // out), cnt[na + 1] the longest coarse row
+  SGPU_CUDA(cudaMemsetAsync(cnt.p + na, 0, 2 * sizeof(int), s));
   const int grid = (int)std::min<int64_t>(((int64_t)na + kGalWarps - 1) / kGalWarps, 64ll * kNumSMs);
   k_gal_count<<<grid, 32 * kGalWarps, 0, s>>>(na, L.aggptr.p, L.aggnodes.p, L.browptr, L.bcol, L.agg.p, cnt.p,
-                                               lists.p, cnt.p + na);
+                                               lists.p, cnt.p + na, cnt.p + na + 1);
   count_launches(1);
   SGPU_TRY(C.own_browptr.alloc((size_t)na + 1));
   size_t bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.p, C.own_browptr.p, na + 1, s);
   SGPU_TRY(tmp.ensure(bytes));
   SGPU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.buf.p, bytes, cnt.p, C.own_browptr.p, na + 1, s));
-  int hv[2] = {0, 0};
+  int hv[3] = {0, 0, 0};
   SGPU_CUDA(cudaMemcpyAsync(&hv[0], C.own_browptr.p + na, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SGPU_CUDA(cudaMemcpyAsync(&hv[1], cnt.p + na, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaMemcpyAsync(&hv[1], cnt.p + na, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   SGPU_CUDA(cudaStreamSynchronize(s));
   if (hv[1]) return SGPU_OK;
+  const bool private_acc = hv[2] <= kGal2Cap && !gal_staged_forced();
   C.nb = na;
   C.b = K;
   C.n = na * K;
@@ -2423,12 +2647,12 @@ int galerkin_direct(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cuda
   C.browptr = C.own_browptr.p;
   C.bcol = C.own_bcol.p;
   const int B = L.b;
-  if (B == 3 && K == 6) SGPU_TRY((launch_gal_values<3, 6>(L, view, lists.p, C, s)));
-  else if (B == 6 && K == 6) SGPU_TRY((launch_gal_values<6, 6>(L, view, lists.p, C, s)));
-  else if (B == 1 && K == 1) SGPU_TRY((launch_gal_values<1, 1>(L, view, lists.p, C, s)));
-  else if (B == 1 && K == 3) SGPU_TRY((launch_gal_values<1, 3>(L, view, lists.p, C, s)));
-  else if (B == 3 && K == 3) SGPU_TRY((launch_gal_values<3, 3>(L, view, lists.p, C, s)));
-  else if (B == 1 && K == 6) SGPU_TRY((launch_gal_values<1, 6>(L, view, lists.p, C, s)));
+  if (B == 3 && K == 6) SGPU_TRY((launch_gal_values<3, 6>(L, view, lists.p, C, s, private_acc)));
+  else if (B == 6 && K == 6) SGPU_TRY((launch_gal_values<6, 6>(L, view, lists.p, C, s, private_acc)));
+  else if (B == 1 && K == 1) SGPU_TRY((launch_gal_values<1, 1>(L, view, lists.p, C, s, private_acc)));
+  else if (B == 1 && K == 3) SGPU_TRY((launch_gal_values<1, 3>(L, view, lists.p, C, s, private_acc)));
+  else if (B == 3 && K == 3) SGPU_TRY((launch_gal_values<3, 3>(L, view, lists.p, C, s, private_acc)));
+  else if (B == 1 && K == 6) SGPU_TRY((launch_gal_values<1, 6>(L, view, lists.p, C, s, private_acc)));
   else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
   SGPU_CUDA(cudaGetLastError());
   *done = true;
@@ -2880,6 +3104,54 @@ struct PhaseClock {
   }
 };
 
+// The FP32 cycle's smoother bounds of the coarse smoothing levels: their
+// values converted here, their Lanczos steps queued on the set-up's second
+// stream after the level-0 bound, so that they run beside the dense coarsest
+// inverse (both are chains of small launches).  amg_prepare_precision reads
+// the coefficients.  The same kernels on the same data as lanczos_lmax, so
+// the same bounds.
+int coarse_bounds_enqueue(sgpu_matrix m, cudaStream_t s) {
+  Amg &A = *m->amg;
+  const AmgLevel *Cl = A.lv.back();
+  const bool dense = Cl->n <= A.dense_max;  // the dense coarsest level is not a smoothing level
+  const size_t last = dense ? A.lv.size() - 1 : A.lv.size();
+  size_t need = 0;
+  int cnt = 0;
+  for (size_t l = 1; l < last; l++) {
+    if (A.lv[l]->layout != 0) continue;
+    need += 5 * (size_t)A.lv[l]->n;
+    cnt++;
+  }
+  A.lzc_levels = 0;
+  if (cnt == 0) return SGPU_OK;
+  SGPU_TRY(A.lzc32.alloc(need));
+  SGPU_TRY(A.lzc_ab.alloc((size_t)129 * cnt));
+  for (size_t l = 1; l < last; l++) {
+    AmgLevel &L = *A.lv[l];
+    if (L.layout != 0) continue;
+    SGPU_TRY(L.val32.alloc((size_t)L.nblk * L.b * L.b));
+    k_to32<<<grid_for((int64_t)L.nblk * L.b * L.b), TPB, 0, s>>>((int64_t)L.nblk * L.b * L.b, L.val64.p, L.val32.p);
+    count_launches(1);
+    L.val32_ready = true;
+  }
+  SGPU_CUDA(cudaEventRecord(A.fork, s));
+  SGPU_CUDA(cudaStreamWaitEvent(A.side, A.fork, 0));
+  const int steps = std::max(2, std::min(A.lanczos_steps, 63));
+  float *z = A.lzc32.p;
+  int slot = 0;
+  for (size_t l = 1; l < last; l++) {
+    AmgLevel &L = *A.lv[l];
+    if (L.layout != 0) continue;
+    const size_t n = (size_t)L.n;
+    SGPU_TRY(lanczos_enqueue<float>(m, L, A.side, steps, z, z + n, z + 2 * n, z + 3 * n, z + 4 * n,
+                                    A.lzc_ab.p + (size_t)129 * slot));
+    L.lz_slot = slot++;
+    z += 5 * n;
+  }
+  A.lzc_levels = slot;
+  return SGPU_OK;
+}
+
 // Builds the hierarchy (FP64 set-up).
 int amg_build(sgpu_matrix m) {
   Amg &A = *m->amg;
@@ -2973,6 +3245,7 @@ int amg_build(sgpu_matrix m) {
     // aggregation no longer reduces the size
     if (C->n <= A.coarse_max || C->nb * 10 > L.nb * 8) break;
   }
+  if (A.l0_bound_pending) SGPU_TRY(coarse_bounds_enqueue(m, s));
   AmgLevel *Cl = A.lv.back();
   if (Cl->n > A.dense_max) {
     // The coarsening stalled above the dense limit (many small independent
@@ -3028,6 +3301,7 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
   PhaseClock clk(s);
   if (fp32 && !A.have32) {
     SGPU_TRY(ensure_level0_h16(m, s));
+    std::vector<double> hc;  // the coarse levels' Lanczos coefficients from the second stream
     for (size_t l = 0; l < A.lv.size(); l++) {
       AmgLevel &L = *A.lv[l];
       SGPU_TRY(L.v32.alloc(L.n));
@@ -3036,7 +3310,7 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
         k_to32<<<grid_for((int64_t)L.n * L.k), TPB, 0, s>>>((int64_t)L.n * L.k, L.Q64.p, L.Q32.p);
         count_launches(1);
       }
-      if (L.layout == 0) {
+      if (L.layout == 0 && !L.val32_ready) {
         SGPU_TRY(L.val32.alloc((size_t)L.nblk * L.b * L.b));
         k_to32<<<grid_for((int64_t)L.nblk * L.b * L.b), TPB, 0, s>>>((int64_t)L.nblk * L.b * L.b, L.val64.p,
                                                                      L.val32.p);
@@ -3047,7 +3321,15 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
         A.l0_bound_pending = false;
         std::vector<double> h(129);
         SGPU_CUDA(cudaMemcpyAsync(h.data(), A.lz_ab.p, 129 * sizeof(double), cudaMemcpyDeviceToHost, A.side));
+        if (A.lzc_levels > 0) {
+          hc.resize((size_t)129 * A.lzc_levels);
+          SGPU_CUDA(cudaMemcpyAsync(hc.data(), A.lzc_ab.p, hc.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                    A.side));
+        }
         SGPU_CUDA(cudaStreamSynchronize(A.side));
+        SGPU_TRY(lanczos_finish(h, std::max(2, std::min(A.lanczos_steps, 63)), &L.lmax32));
+      } else if (L.lz_slot >= 0 && (size_t)(L.lz_slot + 1) * 129 <= hc.size()) {
+        const std::vector<double> h(hc.begin() + (size_t)129 * L.lz_slot, hc.begin() + (size_t)129 * (L.lz_slot + 1));
         SGPU_TRY(lanczos_finish(h, std::max(2, std::min(A.lanczos_steps, 63)), &L.lmax32));
       } else {
         SGPU_TRY(lanczos_lmax<float>(m, L, s, A.lanczos_steps, &L.lmax32));

@@ -79,6 +79,10 @@ struct AmgLevel {
   PBuf<float> Q32;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
+  // FP32 cycle: values converted, and the slot of this level's smoother
+  // bound among the Lanczos runs on the set-up's second stream (-1: none)
+  bool val32_ready = false;
+  int lz_slot = -1;
 };
 
 struct Amg {
@@ -119,6 +123,11 @@ struct Amg {
   bool l0_bound_wanted = false;
   DevBuf<float> lz32;    // 5 vectors of n
   DevBuf<double> lz_ab;  // Lanczos coefficients
+  // the coarse smoothing levels' bounds, run on the second stream beside the
+  // dense coarsest inverse: 5 vectors of each level, 129 coefficients each
+  DevBuf<float> lzc32;
+  DevBuf<double> lzc_ab;
+  int lzc_levels = 0;
   // Level 0 of the FP32 cycle with half-precision values (3x3 block rows
   // only): every block row padded to a multiple of four blocks (padding:
   // value 0, the row's own column), values component-major per padded row,
@@ -148,6 +157,8 @@ struct Amg {
     AmgLevel *l = pool[depth];
     l->unit_diag = false;
     l->browptr = l->bcol = nullptr;
+    l->val32_ready = false;
+    l->lz_slot = -1;
     return l;
   }
 };
