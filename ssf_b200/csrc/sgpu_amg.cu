@@ -1378,9 +1378,22 @@ __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *
     if (i < nb) {
       if (sub == 0) m = in[i];
       const int re = browptr[i + 1];
-      for (int e = browptr[i] + sub; e < re; e += LPR) {
-        const int j = bcol[e];
-        if (agg == nullptr || agg[j] < 0) m = max(m, in[j]);
+      // four neighbours per lane in flight: their columns first, then their
+      // keys (and aggregate marks)
+      for (int e0 = browptr[i] + sub; e0 < re; e0 += 4 * LPR) {
+        int js[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) js[u] = e0 + u * LPR < re ? __ldg(bcol + e0 + u * LPR) : -1;
+        uint64_t kv[4];
+        bool on[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          kv[u] = js[u] >= 0 ? in[js[u]] : 0;
+          on[u] = js[u] >= 0 && (agg == nullptr || __ldg(agg + js[u]) < 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (on[u]) m = max(m, kv[u]);
       }
     }
 #pragma unroll
@@ -1403,6 +1416,70 @@ __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(undecided, cnt);
   }
+}
+
+// The whole independent-set loop of a small graph in one launch: one
+// thread-block cluster runs the rounds of k_mis_max / k_mis_decide (the
+// same keys, maxima and decisions, so the same set), a cluster barrier (a
+// hardware barrier, no spinning) between the passes of a round, and stops
+// after the round that leaves no node undecided or after kMisRounds rounds
+// (*rounds_out: the rounds run; cnt[r + 1]: the nodes round r left
+// undecided, cnt zeroed by the caller).  Small graphs (the coarse levels)
+// otherwise pay a launch per pass and a host read per group of rounds for a
+// microsecond of work each.
+constexpr int kMisRounds = 200;
+constexpr int kMisClusterThreads = 1024;
+
+__global__ void __launch_bounds__(kMisClusterThreads)
+    k_mis2_cluster(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
+                   const int *__restrict__ agg, const int *__restrict__ cand, uint64_t *__restrict__ t,
+                   uint64_t *__restrict__ m1, int *__restrict__ cnt, int *__restrict__ rounds_out) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int nth = (int)(cl.num_blocks() * blockDim.x);
+  const int tid = (int)(cl.block_rank() * blockDim.x + threadIdx.x);
+  __shared__ int bsum;
+  for (int i = tid; i < nb; i += nth) t[i] = mis_key(cand == nullptr || cand[i] ? 1 : 0, i);
+  cl.sync();
+  int r = 0;
+  bool done = false;
+  for (; r < kMisRounds; r++) {
+    for (int i = tid; i < nb; i += nth) {
+      uint64_t m = t[i];
+      for (int e = browptr[i]; e < browptr[i + 1]; e++) {
+        const int j = bcol[e];
+        if (agg == nullptr || agg[j] < 0) m = max(m, t[j]);
+      }
+      m1[i] = m;
+    }
+    cl.sync();
+    if (threadIdx.x == 0) bsum = 0;
+    __syncthreads();
+    int c = 0;
+    for (int i = tid; i < nb; i += nth) {
+      uint64_t m = m1[i];
+      for (int e = browptr[i]; e < browptr[i + 1]; e++) {
+        const int j = bcol[e];
+        if (agg == nullptr || agg[j] < 0) m = max(m, m1[j]);
+      }
+      const uint64_t ti = t[i];
+      if ((ti >> 62) == 1) {
+        if (m == ti) t[i] = mis_key(2, i);
+        else if ((m >> 62) == 2) t[i] = ti & ~(3ull << 62);
+        else c++;
+      }
+    }
+    if (c) atomicAdd(&bsum, c);
+    __syncthreads();
+    if (threadIdx.x == 0 && bsum) atomicAdd(cnt + r + 1, bsum);
+    cl.sync();
+    if (__ldcg(cnt + r + 1) == 0) {
+      r++;
+      done = true;
+      break;
+    }
+  }
+  if (tid == 0) *rounds_out = done ? r : -1;
 }
 
 // second-phase candidates: unaggregated nodes with at least `min_free`
@@ -1933,13 +2010,14 @@ __global__ void __launch_bounds__(32 * kGalCtaWarps, 3)
 // the staging form above does with K*K threads over all 128 lanes' stages.
 constexpr int kGal2Cap = 40;  // blocks per coarse row
 constexpr int kGal2Warps = 4;
+constexpr int kGal2Nodes = 128;  // an aggregate's nodes and rows read ahead into shared memory
 
 template <int B, int K>
 constexpr size_t gal2_shared_bytes() {
   // [W][kGal2Cap][K*K] accumulators, [W][32][B*K | 1] staging, [W][B*K] the
   // current node's Q rows, the table
   return ((size_t)kGal2Warps * kGal2Cap * K * K + (size_t)kGal2Warps * 32 * ((B * K) | 1) +
-          (size_t)kGal2Warps * B * K) * sizeof(double) + sizeof(GalTable);
+          (size_t)kGal2Warps * B * K) * sizeof(double) + sizeof(GalTable) + 3 * kGal2Nodes * sizeof(int);
 }
 
 template <int B, int K>
@@ -1955,11 +2033,19 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
   double *stages = accs + (size_t)W * kGal2Cap * KK;       // [W][32][SS]
   double *qis = stages + (size_t)W * 32 * SS;              // [W][BK]
   GalTable &T = *reinterpret_cast<GalTable *>(qis + (size_t)W * BK);
+  int *pnode = reinterpret_cast<int *>(&T + 1);  // [kGal2Nodes] the aggregate's nodes
+  int *prs = pnode + kGal2Nodes, *pre = prs + kGal2Nodes;  // their rows' ranges
   double *acc = accs + (size_t)w * kGal2Cap * KK;
   double *stage = stages + (size_t)w * 32 * SS;
   double *qi = qis + (size_t)w * BK;
   for (int G = blockIdx.x; G < na; G += gridDim.x) {
     const int base = cbrowptr[G], n = cbrowptr[G + 1] - base;
+    // the aggregate's nodes, then their row ranges, read ahead (two waits
+    // per aggregate instead of two per node)
+    const int a0 = aggptr[G], an = aggptr[G + 1] - a0;
+    const bool ahead = an <= kGal2Nodes;
+    if (ahead)
+      for (int t = threadIdx.x; t < an; t += blockDim.x) pnode[t] = __ldg(aggnodes + a0 + t);
     for (int h = threadIdx.x; h < kGalHash; h += blockDim.x) T.key[h] = -1;
     for (int t = threadIdx.x; t < W * n * KK; t += blockDim.x) {
       const int ww = t / (n * KK);
@@ -1978,10 +2064,16 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
         h = (h + 1) & (kGalHash - 1);
       }
     }
+    if (ahead)
+      for (int t = threadIdx.x; t < an; t += blockDim.x) {
+        const int i = pnode[t];
+        prs[t] = __ldg(A.browptr + i);
+        pre[t] = __ldg(A.browptr + i + 1);
+      }
     __syncthreads();
-    for (int a = aggptr[G] + w; a < aggptr[G + 1]; a += W) {
-      const int i = __ldg(aggnodes + a);
-      const int rs = __ldg(A.browptr + i), re = __ldg(A.browptr + i + 1);
+    for (int k = w; k < an; k += W) {
+      const int i = ahead ? pnode[k] : __ldg(aggnodes + a0 + k);
+      const int rs = ahead ? prs[k] : __ldg(A.browptr + i), re = ahead ? pre[k] : __ldg(A.browptr + i + 1);
       for (int c = lane; c < BK; c += 32) qi[c] = __ldg(Q + (size_t)i * BK + c);
       double di[B];
 #pragma unroll
@@ -2417,8 +2509,73 @@ int read_int(const int *d, cudaStream_t s, int *out) {
 // Distance-2 maximal independent set over the candidate nodes (all nodes, or
 // with `agg` the candidates among the unaggregated ones, on their subgraph):
 // on return the roots have state 2 in t.
+// cluster size for k_mis2_cluster: 16 where the device schedules it, else 8,
+// 0 when neither (the rounds then run as separate launches)
+int mis_cluster_size() {
+  static std::atomic<int> cached{-1};
+  int c = cached.load();
+  if (c >= 0) return c;
+  c = 0;
+  if (cudaFuncSetAttribute(k_mis2_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    cudaGetLastError();
+  for (int cs : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kMisClusterThreads);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_mis2_cluster, &cfg) == cudaSuccess && nclusters >= 1) {
+      c = cs;
+      break;
+    }
+    cudaGetLastError();
+  }
+  cached.store(c);
+  return c;
+}
+
+// graphs of at most this many nodes run their independent-set rounds in one
+// cluster launch (SGPU_MIS=rounds: separate launches at every size)
+constexpr int kMisClusterNodes = 32768;
+
 int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t, cudaStream_t s) {
   const int nb = L.nb, g = grid_for(nb);
+  {
+    const char *me = getenv("SGPU_MIS");
+    const int cs = (nb <= kMisClusterNodes && !(me && !strcmp(me, "rounds"))) ? mis_cluster_size() : 0;
+    if (cs > 0) {
+      TmpBuf<uint64_t> m1(s);
+      TmpBuf<int> cnt(s);
+      SGPU_TRY(m1.alloc(nb));
+      SGPU_TRY(cnt.alloc(kMisRounds + 2));
+      SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, (kMisRounds + 2) * sizeof(int), s));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(kMisClusterThreads);
+      cfg.stream = s;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cs;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int *rounds_d = cnt.p + kMisRounds + 1;
+      SGPU_CUDA(cudaLaunchKernelEx(&cfg, k_mis2_cluster, nb, L.browptr, L.bcol, agg, cand, t.p, m1.p, cnt.p,
+                                   rounds_d));
+      count_launches(1);
+      int rounds = 0;
+      SGPU_TRY(read_int(rounds_d, s, &rounds));
+      if (rounds < 0) return fail(SGPU_CUDA_ERROR, "aggregation: independent-set rounds did not finish");
+      return SGPU_OK;
+    }
+  }
   // 8 lanes per node (SGPU_MIS=thread: a thread per node and a separate
   // decision pass); the same rounds and the same set either way
   const char *mis_env = getenv("SGPU_MIS");
@@ -2732,6 +2889,11 @@ int galerkin(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cudaStream_
 
 // ----- level SpMV dispatch --------------------------------------------------
 
+// grids of the FP32 smoother-bound products are halved (set by
+// lanczos_enqueue): on the set-up's second stream the other half of the GPU
+// stays free for the aggregation rounds that run beside them
+thread_local int g_grid_div = 1;
+
 // resident blocks of a kernel, queried once and cached (no query inside a capture)
 template <class K>
 int resident_grid(K kern, int64_t warps_needed) {
@@ -2748,7 +2910,7 @@ int resident_grid(K kern, int64_t warps_needed) {
       cache[(const void *)kern] = nb;
     }
   }
-  int64_t g = (int64_t)kNumSMs * (nb > 0 ? nb : 4);
+  int64_t g = (int64_t)kNumSMs * (nb > 0 ? nb : 4) / g_grid_div;
   const int64_t need = (warps_needed * 32 + TPB - 1) / TPB;
   if (g > need) g = need;
   if (g > 8192) g = 8192;
@@ -3036,6 +3198,13 @@ int lanczos_enqueue(sgpu_matrix m, const AmgLevel &L, cudaStream_t s, int steps,
   T *w[3] = {w0, w1, w2};
   const T *dsq = level_dsq<T>(L);
   Work &wk = m->w;
+  // FP32 bounds (the ones the set-up runs on its second stream) with half
+  // grids, on either stream, so that the overlapped and the serial set-up
+  // sum every product in the same order; restored on every return
+  struct GridDiv {
+    explicit GridDiv(int d) { g_grid_div = d; }
+    ~GridDiv() { g_grid_div = 1; }
+  } grid_div(sizeof(T) == 4 ? 2 : 1);
   const int g = grid_for(L.n);
   k_rand_vec<T><<<g, TPB, 0, s>>>(L.n, y);
   k_lanczos_w<T><<<g, TPB, 0, s>>>(L.n, y, nullptr, nullptr, dsq, ab, 0, w[0], u, wk.partials.p,

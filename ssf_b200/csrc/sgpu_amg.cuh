@@ -101,7 +101,10 @@ struct Amg {
   // [lmax/ratio, 1.1 lmax], largest dense coarsest level, coarse visits per
   // level (1: V-cycle, 2: W-cycle), Lanczos steps of the lmax estimate
   int deg = 1;
-  double ratio = 30.0, alpha = 1.7;
+  // alpha 1.9: 39 iterations on the 1.01M-DOF cantilever against 41 at 1.7,
+  // 33 against 36 on a 362k-DOF plate, 31 against 32 on a 96^3 lognormal
+  // conduction cube (all FP32 cycle, true residual 1e-10)
+  double ratio = 30.0, alpha = 1.9;
   int coarse_max = 768;
   int dense_max = 4096;  // larger coarsest levels are smoothed, not inverted
   int bottom_deg = 8;    // Chebyshev steps of such a bottom level

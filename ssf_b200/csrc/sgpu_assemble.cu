@@ -567,27 +567,32 @@ __device__ __forceinline__ void hex_iso_block(const HexIsoShared &sh, int a, int
     for (int j = 0; j < 3; j++) k[i][j] = lam * P[i][j] + mu * P[j][i] + (i == j ? tr : 0.0);
 }
 
-template <bool ROWCACHE>
+// STORE: no scatter; the 36 blocks a <= b of element e go to
+// kbuf[324 e + 9 slot + 3 i + j] (slot: the index of (a, b) among the pairs
+// a < b in row-major order, 28 + a for (a, a)), every element in one launch
+// (elist unused), for k_hex8_gather.
+template <bool ROWCACHE, bool STORE>
 __global__ void __launch_bounds__(TPB, 3) k_hex8_iso(int ne_c, const int *__restrict__ elist,
                                                      const double *__restrict__ coords,
                                                      const int64_t *__restrict__ elems,
                                                      const int *__restrict__ cne, const double *__restrict__ emat,
                                                      const int *__restrict__ rowptr, const int *__restrict__ col,
-                                                     double *__restrict__ val, unsigned *err) {
+                                                     double *__restrict__ val, unsigned *err,
+                                                     double *__restrict__ kbuf) {
   __shared__ HexIsoShared shm[WPB];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   HexIsoShared &sh = shm[wib];
   const int gp = lane & 7, q = lane >> 3;
   const double xi = c_gp2[(gp >> 2) & 1], eta = c_gp2[(gp >> 1) & 1], zeta = c_gp2[gp & 1];
   for (int t = blockIdx.x * WPB + wib; t < ne_c; t += gridDim.x * WPB) {
-    const int e = elist[t];
+    const int e = STORE ? t : elist[t];
     double cx = 0, cy = 0, cz = 0;
     if (lane < 8) {
       const int64_t nd = elems[(int64_t)e * 8 + lane];
       cx = coords[3 * nd]; cy = coords[3 * nd + 1]; cz = coords[3 * nd + 2];
     }
-    const int code = lane < 24 ? __ldg(cne + (int64_t)e * 24 + lane) : -1;
-    if (ROWCACHE) {
+    const int code = (lane < 24 && !STORE) ? __ldg(cne + (int64_t)e * 24 + lane) : -1;
+    if (ROWCACHE && !STORE) {
       // the rows of the element's equations; node a's column list copied
       // into shared memory while the Gauss points are formed
       int rpv = -1, rlen = 0;
@@ -645,7 +650,7 @@ __global__ void __launch_bounds__(TPB, 3) k_hex8_iso(int ne_c, const int *__rest
     const double E = __ldg(emat + 2 * (int64_t)e), nu = __ldg(emat + 2 * (int64_t)e + 1);
     const double mu = E / 2.0 / (1.0 + nu);
     const double lam = E / (1.0 + nu) / (1.0 - 2.0 * nu) * nu;
-    if (ROWCACHE) cp_async_wait_all();
+    if (ROWCACHE && !STORE) cp_async_wait_all();
     __syncwarp();
     // first block: lanes < 28 the pair a < b of their index, lanes 28..31
     // the diagonal pair (2 (lane - 28), same)
@@ -657,6 +662,24 @@ __global__ void __launch_bounds__(TPB, 3) k_hex8_iso(int ne_c, const int *__rest
     }
     double k[3][3];
     hex_iso_block(sh, a0, b0, lam, mu, k);
+    if (STORE) {
+      double *dst = kbuf + (size_t)e * 324 + 9 * (lane < 28 ? lane : 28 + a0);
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) dst[3 * i + j] = k[i][j];
+      if (lane >= 28) {
+        const int a1 = 2 * (lane - 28) + 1;
+        hex_iso_block(sh, a1, a1, lam, mu, k);
+        double *d1 = kbuf + (size_t)e * 324 + 9 * (28 + a1);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) d1[3 * i + j] = k[i][j];
+      }
+      __syncwarp();
+      continue;
+    }
     int rr[3], cc[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -718,35 +741,45 @@ constexpr int kIncCap = 32;    // elements at one node
 constexpr int kElemBatch = 4;  // elements whose Gauss-point gradients a warp forms at once
 constexpr int kRowWarps = 4;   // warps per block of the row kernel
 
+constexpr int kGpStride = 25;  // 8 nodes x 3 gradient components, padded: the
+                               // 16 lanes of a half-warp storing their points'
+                               // gradients hit distinct banks
+
 struct HexRowShared {
-  double g[kElemBatch][8][8][3];  // [element][gp][node][x, y, z]
+  double g[kElemBatch][8][kGpStride];  // [element][gp][3 node + x/y/z]
   double w[kElemBatch][8];        // |detJ| (weights are 1)
   double acc[3][kRowCap];         // the node's rows
   int col[3][kRowCap];            // their column indices
   int inc[kIncCap];               // incident elements, ascending
 };
 
-// gradients of the 8 shape functions and |detJ| at Gauss point gp (0..7,
-// xi outermost), as hex_gauss_point
+// gradients of the 8 shape functions (g[3 a + c]) and |detJ| at Gauss point
+// gp (0..7, xi outermost), as hex_gauss_point, with one reciprocal of detJ
+// scaling the cofactors of derivatives_3d (GEFEL/difcalc.cpp:487-565)
 __device__ __forceinline__ void hex_gp_gradients(int gp, const double *x, const double *y, const double *z,
-                                                 double (*g)[3], double *w) {
+                                                 double *g, double *w) {
   const double xi = c_gp2[(gp >> 2) & 1], eta = c_gp2[(gp >> 1) & 1], zeta = c_gp2[gp & 1];
-  double nx[8], ny[8], nz[8];
-  hex_dnat(xi, eta, zeta, nx, ny, nz);
   double d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0, d9 = 0;
 #pragma unroll
   for (int a = 0; a < 8; a++) {
-    d1 += nx[a] * x[a]; d2 += ny[a] * x[a]; d3 += nz[a] * x[a];
-    d4 += nx[a] * y[a]; d5 += ny[a] * y[a]; d6 += nz[a] * y[a];
-    d7 += nx[a] * z[a]; d8 += ny[a] * z[a]; d9 += nz[a] * z[a];
+    double nxa, nya, nza;
+    hex_dnat1(a, xi, eta, zeta, nxa, nya, nza);
+    d1 += nxa * x[a]; d2 += nya * x[a]; d3 += nza * x[a];
+    d4 += nxa * y[a]; d5 += nya * y[a]; d6 += nza * y[a];
+    d7 += nxa * z[a]; d8 += nya * z[a]; d9 += nza * z[a];
   }
   const double jac = d1 * d5 * d9 + d4 * d8 * d3 + d7 * d2 * d6 - d7 * d5 * d3 - d8 * d6 * d1 - d9 * d4 * d2;
+  const double ij = 1.0 / jac;
+  const double c11 = (d5 * d9 - d8 * d6) * ij, c12 = (d7 * d6 - d9 * d4) * ij, c13 = (d4 * d8 - d7 * d5) * ij;
+  const double c21 = (d8 * d3 - d9 * d2) * ij, c22 = (d1 * d9 - d7 * d3) * ij, c23 = (d7 * d2 - d8 * d1) * ij;
+  const double c31 = (d2 * d6 - d5 * d3) * ij, c32 = (d4 * d3 - d6 * d1) * ij, c33 = (d1 * d5 - d4 * d2) * ij;
 #pragma unroll
   for (int a = 0; a < 8; a++) {
-    const double ddx = nx[a], ddy = ny[a], ddz = nz[a];
-    g[a][0] = (ddx * (d5 * d9 - d8 * d6) + ddy * (d7 * d6 - d9 * d4) + ddz * (d4 * d8 - d7 * d5)) / jac;
-    g[a][1] = (ddx * (d8 * d3 - d9 * d2) + ddy * (d1 * d9 - d7 * d3) + ddz * (d7 * d2 - d8 * d1)) / jac;
-    g[a][2] = (ddx * (d2 * d6 - d5 * d3) + ddy * (d4 * d3 - d6 * d1) + ddz * (d1 * d5 - d4 * d2)) / jac;
+    double ddx, ddy, ddz;
+    hex_dnat1(a, xi, eta, zeta, ddx, ddy, ddz);
+    g[3 * a] = ddx * c11 + ddy * c12 + ddz * c13;
+    g[3 * a + 1] = ddx * c21 + ddy * c22 + ddz * c23;
+    g[3 * a + 2] = ddx * c31 + ddy * c32 + ddz * c33;
   }
   *w = fabs(jac);
 }
@@ -861,10 +894,10 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_hex8_rows(int64_t nn, const 
         if (lane < 24) {
 #pragma unroll
           for (int gp = 0; gp < 8; gp++) {
-            const double wa = sh.w[q][gp] * sh.g[q][gp][la][i];
-            p0 += wa * sh.g[q][gp][b][0];
-            p1 += wa * sh.g[q][gp][b][1];
-            p2 += wa * sh.g[q][gp][b][2];
+            const double wa = sh.w[q][gp] * sh.g[q][gp][3 * la + i];
+            p0 += wa * sh.g[q][gp][3 * b];
+            p1 += wa * sh.g[q][gp][3 * b + 1];
+            p2 += wa * sh.g[q][gp][3 * b + 2];
           }
         }
         // column i of P_b (rows k = 0..2 live in lanes 3b + k) and its trace
@@ -916,6 +949,163 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_hex8_rows(int64_t nn, const 
       if (r[i] < 0) continue;
       double *dst = val + __ldg(rowptr + r[i]);
       for (int k = lane; k < len[i]; k += 32) dst[k] = sh.acc[i][k];
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// hex8 isotropic elasticity, write-once: k_hex8_iso<.., STORE> forms the 36
+// blocks a <= b of every element into a buffer (one launch, no colours, no
+// scatter), then one warp per node gathers the blocks of its incident
+// elements into the node's (up to) three CSR rows in shared memory -- the
+// elements by ascending id, so every entry's summation order is fixed -- and
+// writes each entry once.  The colour-ordered scatter reads and writes every
+// 3x3 block once per element that touches it, in 24-byte pieces of 32-byte
+// sectors (about 7 GB of DRAM traffic for the 630 MB value array of the
+// 1.01M-DOF cantilever); here the traffic is the buffer written and read
+// once (324 doubles per element) and the values written once.
+// ---------------------------------------------------------------------------
+constexpr int kGatherBatch = 4;  // incident elements whose blocks a warp loads at once
+
+struct HexGatherShared {
+  double acc[3][kRowCap];  // the node's rows
+  int col[3][kRowCap];     // their column indices
+  int inc[kIncCap];        // incident elements, ascending
+  int la[kIncCap];         // the node's index in each of them
+};
+
+// the slot of pair (a, b), a < b, among the 28 pairs in row-major order
+__device__ __forceinline__ int upper_slot(int a, int b) { return 7 * a - (a * (a - 1)) / 2 + (b - a - 1); }
+
+__global__ void __launch_bounds__(kRowWarps * 32) k_hex8_gather(int64_t nn, const int *__restrict__ iptr,
+                                                                const int *__restrict__ inc,
+                                                                const int64_t *__restrict__ elems,
+                                                                const int *__restrict__ cne,
+                                                                const double *__restrict__ kbuf,
+                                                                const int *__restrict__ rowptr,
+                                                                const int *__restrict__ col,
+                                                                double *__restrict__ val, unsigned *err) {
+  __shared__ HexGatherShared shm[kRowWarps];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  HexGatherShared &sh = shm[wib];
+  // lane (b, i): node b of the element, row component i
+  const int b = lane < 24 ? lane / 3 : 0, i = lane < 24 ? lane - 3 * (lane / 3) : 0;
+  for (int64_t node = blockIdx.x * (int64_t)kRowWarps + wib; node < nn; node += (int64_t)gridDim.x * kRowWarps) {
+    const int ib = iptr[node], deg = iptr[node + 1] - ib;
+    if (deg == 0) continue;
+    if (deg > kIncCap) {
+      if (lane == 0) atomicOr(err, 32u);
+      continue;
+    }
+    // incident elements in ascending order (distinct ids: rank sort), and
+    // the node's index in each
+    const int mine = lane < deg ? inc[ib + lane] : INT_MAX;
+    int rank = 0;
+    for (int k = 0; k < deg; k++) rank += __shfl_sync(0xffffffffu, mine, k) < mine;
+    if (lane < deg) sh.inc[rank] = mine;
+    __syncwarp();
+    for (int t = lane; t < 8 * deg; t += 32) {
+      const int q = t >> 3, a = t & 7;
+      if (elems[(int64_t)sh.inc[q] * 8 + a] == node) sh.la[q] = a;
+    }
+    __syncwarp();
+    // the node's rows: its code numbers in its first element
+    int r[3], len[3];
+    bool fits = true;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      r[c] = __ldg(cne + (int64_t)sh.inc[0] * 24 + 3 * sh.la[0] + c);
+      len[c] = 0;
+      if (r[c] >= 0) {
+        const int rb = __ldg(rowptr + r[c]);
+        len[c] = __ldg(rowptr + r[c] + 1) - rb;
+        if (len[c] > kRowCap) {
+          fits = false;
+        } else {
+          for (int k = lane; k < len[c]; k += 32) {
+            sh.col[c][k] = __ldg(col + rb + k);
+            sh.acc[c][k] = 0.0;
+          }
+        }
+      }
+    }
+    if (!fits) {
+      if (lane == 0) atomicOr(err, 32u);
+      __syncwarp();
+      continue;
+    }
+    if (r[0] < 0 && r[1] < 0 && r[2] < 0) {
+      __syncwarp();
+      continue;  // a fully constrained node has no rows
+    }
+    __syncwarp();
+    for (int q0 = 0; q0 < deg; q0 += kGatherBatch) {
+      // row i of block (la, b) of up to kGatherBatch elements and node b's
+      // code numbers, all loads issued before the first is used
+      double kr[kGatherBatch][3];
+      int cc[kGatherBatch][3];
+#pragma unroll
+      for (int u = 0; u < kGatherBatch; u++) {
+        const int q = q0 + u;
+        kr[u][0] = kr[u][1] = kr[u][2] = 0.0;
+        cc[u][0] = cc[u][1] = cc[u][2] = -1;
+        if (q < deg && lane < 24 && r[i] >= 0) {
+          const int e = sh.inc[q], la = sh.la[q];
+          const double *eb = kbuf + (size_t)e * 324;
+          if (la == b) {
+            const double *blk = eb + 9 * (28 + la);
+#pragma unroll
+            for (int j = 0; j < 3; j++) kr[u][j] = __ldg(blk + 3 * i + j);
+          } else if (la < b) {
+            const double *blk = eb + 9 * upper_slot(la, b);
+#pragma unroll
+            for (int j = 0; j < 3; j++) kr[u][j] = __ldg(blk + 3 * i + j);
+          } else {  // K_{la,b} = K_{b,la}^T
+            const double *blk = eb + 9 * upper_slot(b, la);
+#pragma unroll
+            for (int j = 0; j < 3; j++) kr[u][j] = __ldg(blk + 3 * j + i);
+          }
+#pragma unroll
+          for (int j = 0; j < 3; j++) cc[u][j] = __ldg(cne + (int64_t)e * 24 + 3 * b + j);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kGatherBatch; u++) {
+        // the elements in ascending order: one element's blocks at a time
+        if (q0 + u < deg && lane < 24 && r[i] >= 0) {
+          const int *cols = sh.col[i];
+          double *acc = sh.acc[i];
+          const int c0 = cc[u][0], c1 = cc[u][1], c2 = cc[u][2];
+          bool done = false;
+          if (c0 >= 0 && c1 == c0 + 1 && c2 == c0 + 2) {  // a fully free node: one search
+            const int p = find_col_sh(cols, len[i], c0);
+            if (p >= 0 && p + 2 < len[i] && cols[p + 1] == c1 && cols[p + 2] == c2) {
+              acc[p] += kr[u][0];
+              acc[p + 1] += kr[u][1];
+              acc[p + 2] += kr[u][2];
+              done = true;
+            }
+          }
+          if (!done) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+              if (cc[u][j] < 0) continue;
+              const int p = find_col_sh(cols, len[i], cc[u][j]);
+              if (p >= 0) acc[p] += kr[u][j];
+              else atomicOr(err, 4u);
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // every entry of the node's rows, written once
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (r[c] < 0) continue;
+      double *dst = val + __ldg(rowptr + r[c]);
+      for (int k = lane; k < len[c]; k += 32) dst[k] = sh.acc[c][k];
     }
     __syncwarp();
   }
@@ -1903,6 +2093,13 @@ bool hex8_full_product() {
   return e && !strcmp(e, "1");
 }
 
+// SGPU_HEX8_GATHER=1: isotropic hexahedra through the element buffer and
+// the row gather instead of the colour-ordered scatter (k_hex8_iso)
+bool hex8_gather() {
+  const char *e = std::getenv("SGPU_HEX8_GATHER");
+  return e && !strcmp(e, "1");
+}
+
 // SGPU_HEX8_ROWCACHE=0: k_hex8_iso searches every block's row in global
 // memory instead of in the shared-memory copy of the element's rows
 bool hex8_row_cache() {
@@ -1939,6 +2136,31 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
       rows_done = true;
     }
   }
+  // isotropic hex8 on gencodnum's numbering, SGPU_HEX8_GATHER=1: element
+  // blocks into a buffer, then every node's rows gathered and written once
+  // (k_hex8_gather).  The value array is cleared first: a node without
+  // elements has rows that no warp writes.
+  if (!rows_done && kind == SGPU_ELEM_HEX8 && !ad.general && ad.node_rows && ad.iptr.p && hex8_gather() &&
+      !hex8_full_product()) {
+    AsyncBuf<double> kbuf(s);
+    SGPU_TRY(kbuf.alloc((size_t)ad.ne * 324));
+    SGPU_CUDA(cudaMemsetAsync(c.val.p, 0, (size_t)c.nnz * sizeof(double), s));
+    const int g1 = (int)std::min<int64_t>((ad.ne + WPB - 1) / WPB, (int64_t)kNumSMs * 16);
+    k_hex8_iso<false, true><<<g1, TPB, 0, s>>>((int)ad.ne, nullptr, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                c.rowptr.p, c.col.p, c.val.p, err.p, kbuf.p);
+    const int g2 = (int)std::min<int64_t>((ad.nn + kRowWarps - 1) / kRowWarps, (int64_t)kNumSMs * 64);
+    k_hex8_gather<<<g2, kRowWarps * 32, 0, s>>>(ad.nn, ad.iptr.p, ad.inc.p, ad.elems.p, ad.cne.p, kbuf.p,
+                                                c.rowptr.p, c.col.p, c.val.p, err.p);
+    count_launches(2);
+    SGPU_CUDA(cudaGetLastError());
+    unsigned e = 0;
+    SGPU_TRY(read_err(err.p, s, &e));
+    if (e & 32u) {  // a node beyond the gather's shared-memory capacity: colour-ordered scatter instead
+      SGPU_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
+    } else {
+      rows_done = true;
+    }
+  }
   if (!rows_done) SGPU_CUDA(cudaMemsetAsync(c.val.p, 0, (size_t)c.nnz * sizeof(double), s));
   const int ncol = rows_done ? 0 : (int)ad.offsets.size() - 1;
   for (int col = 0; col < ncol; col++) {
@@ -1955,11 +2177,11 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
           k_hex8_elastic<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
                                                      c.rowptr.p, c.col.p, c.val.p, err.p);
         else if (hex8_row_cache())
-          k_hex8_iso<true><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, c.rowptr.p,
-                                                c.col.p, c.val.p, err.p);
+          k_hex8_iso<true, false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                       c.rowptr.p, c.col.p, c.val.p, err.p, nullptr);
         else
-          k_hex8_iso<false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
-                                                 c.rowptr.p, c.col.p, c.val.p, err.p);
+          k_hex8_iso<false, false><<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p,
+                                                        c.rowptr.p, c.col.p, c.val.p, err.p, nullptr);
         break;
       case 1:
         k_quad4_elastic<<<grid, TPB, 0, s>>>(cnt, el, ad.coords.p, ad.elems.p, ad.cne.p, ad.emat.p, ad.thick.p,

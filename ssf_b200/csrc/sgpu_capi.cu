@@ -66,6 +66,32 @@ void destroy_handle(sgpu_matrix m) {
 }
 
 // upload pattern + values from host GEFEL arrays and build the device forms
+// a second stream and two events for the copy of the values, released when
+// the upload ends (after its last wait)
+struct CopySide {
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t after_pattern_src = nullptr, after_values = nullptr;
+  bool ok = false;
+  CopySide() {
+    ok = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&after_pattern_src, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&after_values, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+  }
+  ~CopySide() {
+    if (s2) {
+      cudaStreamSynchronize(s2);
+      cudaStreamDestroy(s2);
+    }
+    if (after_pattern_src) cudaEventDestroy(after_pattern_src);
+    if (after_values) cudaEventDestroy(after_values);
+  }
+};
+
+// The storage arrays to the device and the device formats built from them.
+// The values travel on a second stream after the pattern arrays, so that
+// their copy (half of the bytes) overlaps the pattern's construction, which
+// needs only adr and ci.
 int upload(sgpu_matrix m, const int64_t *adr, const int64_t *ci, const double *a, double *setup_ms) {
   cudaStream_t s = m->stream;
   const int64_t n = m->n, negm = m->src_negm;
@@ -74,10 +100,19 @@ int upload(sgpu_matrix m, const int64_t *adr, const int64_t *ci, const double *a
   SGPU_TRY(m->src_ci.alloc(negm));
   DevBuf<double> a_d;
   SGPU_TRY(a_d.alloc(negm));
+  CopySide side;
   SGPU_CUDA(cudaMemcpyAsync(m->src_adr.p, adr, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
   SGPU_CUDA(cudaMemcpyAsync(m->src_ci.p, ci, negm * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-  SGPU_CUDA(cudaMemcpyAsync(a_d.p, a, negm * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (side.ok) {
+    SGPU_CUDA(cudaEventRecord(side.after_pattern_src, s));
+    SGPU_CUDA(cudaStreamWaitEvent(side.s2, side.after_pattern_src, 0));
+    SGPU_CUDA(cudaMemcpyAsync(a_d.p, a, negm * sizeof(double), cudaMemcpyHostToDevice, side.s2));
+    SGPU_CUDA(cudaEventRecord(side.after_values, side.s2));
+  } else {
+    SGPU_CUDA(cudaMemcpyAsync(a_d.p, a, negm * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
   SGPU_TRY(matrix_build_from_device_src(m));
+  if (side.ok) SGPU_CUDA(cudaStreamWaitEvent(s, side.after_values, 0));
   SGPU_TRY(matrix_set_values_device(m, a_d.p));
   SGPU_CUDA(cudaEventRecord(m->ev1, s));
   SGPU_CUDA(cudaEventSynchronize(m->ev1));

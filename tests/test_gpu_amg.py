@@ -426,3 +426,25 @@ def test_half_precision_level0_values(oracle, gpu_lib, shape, monkeypatch):
     assert not np.array_equal(x16, x32)  # the half-precision product really ran
     for x in (x16, x32):
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+@pytest.mark.parametrize("case", ["cantilever", "plate"])
+def test_cluster_independent_set_gives_the_same_bits(oracle, gpu_lib, case):
+    # graphs of up to 32768 nodes run all their independent-set rounds in one
+    # thread-block cluster launch; the same keys, maxima and decisions as the
+    # separate launches per pass (SGPU_MIS=rounds), so the same aggregates,
+    # hierarchy and solve to the bit
+    if case == "cantilever":
+        m = decks.cantilever_hex(40, 8, 8)
+    else:
+        m = decks.plate_quad(48, 24, E=3e10, nu=0.22)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", "rounds")
+        x1, r1 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", None)
+    assert r0.status == r1.status == L.OK
+    assert r0.info["iterations"] == r1.info["iterations"]
+    assert r0.info["precond_coarse_n"] == r1.info["precond_coarse_n"]
+    assert np.array_equal(x0, x1)

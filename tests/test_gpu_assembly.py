@@ -1,8 +1,10 @@
-"""GPU assembly of the hexahedral stiffness matrix in its three forms -- the
+"""GPU assembly of the hexahedral stiffness matrix in its four forms -- the
 default colour-ordered element scatter on the pairs a <= b with the
-isotropic P-form, the same scatter with the full B^T D B product
-(SGPU_HEX8_FULL=1), and rows (one warp per node, every CSR entry written
-once; SGPU_ASSEMBLY_ROWS=1) -- against the oracle's
+isotropic P-form, the write-once gather (the 36 blocks a <= b of every
+element into a buffer, then one warp per node sums its rows and writes each
+entry once; SGPU_HEX8_GATHER=1), the same scatter with the full B^T D B product
+(SGPU_HEX8_FULL=1), and rows (one warp per node forming its elements'
+blocks; SGPU_ASSEMBLY_ROWS=1) -- against the oracle's
 stiffness_matrix (MEFEL/SRC/globmat.cpp:41 with linhex::gl_stiffness_matrix
 and symcomprow::localize), and against the default colour-ordered element
 scatter: partially constrained nodes (the per-entry search), several
@@ -18,16 +20,17 @@ from ssf_b200 import decks
 pytestmark = pytest.mark.gpu
 
 
-FORMS = {  # name: (SGPU_ASSEMBLY_ROWS, SGPU_HEX8_FULL)
-    "rows": ("1", None),      # one warp per node, rows written once
-    "iso": (None, None),      # colour-ordered, P-form on the pairs a <= b (default)
-    "full": (None, "1"),      # colour-ordered, full B^T D B product per block
+FORMS = {  # name: (SGPU_ASSEMBLY_ROWS, SGPU_HEX8_FULL, SGPU_HEX8_GATHER)
+    "gather": (None, None, "1"),   # element blocks into a buffer, rows gathered per node
+    "rows": ("1", None, None),     # one warp per node forms its elements' blocks, rows written once
+    "iso": (None, None, None),     # colour-ordered, P-form on the pairs a <= b (default)
+    "full": (None, "1", None),     # colour-ordered, full B^T D B product per block
 }
 
 
 def _download(m, form):
     from ssf_b200 import mefel
-    names = ("SGPU_ASSEMBLY_ROWS", "SGPU_HEX8_FULL")
+    names = ("SGPU_ASSEMBLY_ROWS", "SGPU_HEX8_FULL", "SGPU_HEX8_GATHER")
     old = {k: os.environ.pop(k, None) for k in names}
     for k, v in zip(names, FORMS[form]):
         if v is not None:
@@ -52,8 +55,11 @@ def _check(oracle, m):
         assert np.allclose(g_a, a, rtol=1e-12, atol=tol), form
         out[form] = g_a
     # the GPU forms differ only in rounding
-    for form in ("rows", "full"):
+    for form in ("rows", "full", "gather"):
         assert np.allclose(out[form], out["iso"], rtol=1e-13, atol=1e-13 * np.abs(a).max()), form
+    # the gather sums the same blocks as the colour-ordered scatter, in
+    # ascending element order instead of colour order: rounding apart, equal
+    assert np.allclose(out["gather"], out["iso"], rtol=1e-14, atol=1e-14 * np.abs(a).max())
     return out
 
 
