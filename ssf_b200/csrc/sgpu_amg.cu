@@ -1577,6 +1577,8 @@ __global__ void k_nullspace0(int n, int b, int k0, const double *__restrict__ B,
 // aggregate): modified Gram-Schmidt with a second orthogonalisation pass; a
 // column that (numerically) depends on the previous ones becomes zero.
 // Q (per equation K values) replaces the rows; R is the coarse near-null space.
+constexpr int kTentRows = 4;  // rows per lane of an aggregate QR held in registers (128 rows)
+
 template <int B, int K>
 __global__ void __launch_bounds__(TPB) k_tentative(int na, const int *__restrict__ aggptr,
                                                    const int *__restrict__ aggnodes, const double *__restrict__ Bl,
@@ -1588,6 +1590,71 @@ __global__ void __launch_bounds__(TPB) k_tentative(int na, const int *__restrict
     const int s = __ldg(aggptr + G), e = __ldg(aggptr + G + 1);
     const int rows = (e - s) * B;
     auto eq = [&](int r) { return B * __ldg(aggnodes + s + r / B) + r % B; };
+    if (rows <= 32 * kTentRows) {
+      // the aggregate's rows in registers (lane: rows lane, lane + 32, ...):
+      // the same sweeps, sums and order as below, without the round trips
+      // through memory
+      double v[kTentRows][K];
+      int pr[kTentRows];
+#pragma unroll
+      for (int u = 0; u < kTentRows; u++) {
+        const int r = lane + 32 * u;
+        pr[u] = r < rows ? eq(r) : -1;
+#pragma unroll
+        for (int q = 0; q < K; q++) v[u][q] = pr[u] >= 0 ? Bl[(size_t)pr[u] * K + q] : 0.0;
+      }
+      double R[K][K];
+#pragma unroll
+      for (int a = 0; a < K; a++)
+#pragma unroll
+        for (int c = 0; c < K; c++) R[a][c] = 0.0;
+      bool live[K];
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        double o2 = 0.0;
+#pragma unroll
+        for (int u = 0; u < kTentRows; u++) o2 += v[u][q] * v[u][q];
+        o2 = warp_sum(o2);
+        for (int pass = 0; pass < 2; pass++) {
+#pragma unroll
+          for (int pp = 0; pp < q; pp++) {
+            if (!live[pp]) continue;
+            double dt = 0.0;
+#pragma unroll
+            for (int u = 0; u < kTentRows; u++) dt += v[u][pp] * v[u][q];
+            dt = warp_sum(dt);
+            R[pp][q] += dt;
+#pragma unroll
+            for (int u = 0; u < kTentRows; u++) v[u][q] -= dt * v[u][pp];
+          }
+        }
+        double n2 = 0.0;
+#pragma unroll
+        for (int u = 0; u < kTentRows; u++) n2 += v[u][q] * v[u][q];
+        n2 = warp_sum(n2);
+        const double nrm = sqrt(n2);
+        live[q] = nrm > 1e-10 * sqrt(o2) && nrm > 0.0;
+        R[q][q] = live[q] ? nrm : 0.0;
+        const double inv = live[q] ? 1.0 / nrm : 0.0;
+#pragma unroll
+        for (int u = 0; u < kTentRows; u++) v[u][q] *= inv;
+      }
+#pragma unroll
+      for (int u = 0; u < kTentRows; u++)
+        if (pr[u] >= 0) {
+#pragma unroll
+          for (int q = 0; q < K; q++) Q[(size_t)pr[u] * K + q] = v[u][q];
+        }
+      if (lane < K) {
+#pragma unroll
+        for (int a = 0; a < K; a++)
+          if (lane == a) {
+#pragma unroll
+            for (int c = 0; c < K; c++) Bnext[((size_t)G * K + a) * K + c] = live[a] ? R[a][c] : 0.0;
+          }
+      }
+      continue;
+    }
     for (int r = lane; r < rows; r += 32) {
       const int p = eq(r);
 #pragma unroll
