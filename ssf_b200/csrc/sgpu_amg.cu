@@ -2367,6 +2367,143 @@ __global__ void __launch_bounds__(TPB) k_bgj_colpanel(int n, int k0, int bs, con
   }
 }
 
+// The blocked Gauss-Jordan inverse above in one thread-block-cluster launch:
+// the four steps of every pivot block (diagonal inverse by CTA 0, row panel,
+// rank-32 update of 64 x 64 tiles, column panel) spread over the cluster's
+// CTAs with a cluster barrier (a hardware barrier, no spinning) between them,
+// instead of four launches per pivot block.  The matrix (8 n^2 bytes, L2
+// resident for the coarsest levels here) is read through L2 (ld.global.cg)
+// since the launch itself rewrites it.  Every entry is computed with the
+// expressions and summation order of k_bgj_diag / _rowpanel / _update /
+// _colpanel.
+__global__ void __launch_bounds__(TPB) k_bgj_cluster(int n, double *__restrict__ A, double *__restrict__ Pbuf) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank(), ncta = (int)cl.num_blocks();
+  const int tid = threadIdx.x;
+  constexpr int TI = 64, TJ = 64;
+  __shared__ double ps[GJB][GJB];
+  __shared__ double buf[TI * (GJB + 1) + GJB * TJ];  // update tiles; the diagonal block in CTA 0
+  __shared__ double colv[GJB];
+  double(*ak)[GJB + 1] = reinterpret_cast<double(*)[GJB + 1]>(buf);
+  double(*kb)[TJ] = reinterpret_cast<double(*)[TJ]>(buf + TI * (GJB + 1));
+  double(*d)[GJB + 1] = reinterpret_cast<double(*)[GJB + 1]>(buf);
+  const int ntj = (n + TJ - 1) / TJ, ntiles = ntj * ((n + TI - 1) / TI);
+  for (int k0 = 0; k0 < n; k0 += GJB) {
+    const int bs = min(GJB, n - k0);
+    if (rank == 0) {  // P = A[K,K]^-1, each thread four entries (rows r0, r0 + 8, ...)
+      const int c = tid % GJB, r0 = tid / GJB;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = r0 + 8 * q;
+        d[r][c] = (r < bs && c < bs) ? __ldcg(A + (size_t)(k0 + r) * n + k0 + c) : (r == c ? 1.0 : 0.0);
+      }
+      __syncthreads();
+      for (int k = 0; k < GJB; k++) {
+        const double piv = 1.0 / d[k][k];
+        if (c == 0) {
+#pragma unroll
+          for (int q = 0; q < 4; q++) colv[r0 + 8 * q] = d[r0 + 8 * q][k];
+        }
+        __syncthreads();
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int r = r0 + 8 * q;
+          double x = d[r][c];
+          if (r == k) x = (c == k) ? piv : x * piv;
+          else x = (c == k) ? -colv[r] * piv : x - colv[r] * d[k][c] * piv;
+          v[q] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[r0 + 8 * q][c] = v[q];
+        __syncthreads();
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) Pbuf[(r0 + 8 * q) * GJB + c] = d[r0 + 8 * q][c];
+    }
+    cl.sync();
+    for (int t = tid; t < GJB * GJB; t += blockDim.x) ps[t / GJB][t % GJB] = __ldcg(Pbuf + t);
+    __syncthreads();
+    // row panel: A[K, j] = P A[K, j], j outside K
+    for (int j = rank * blockDim.x + tid; j < n; j += ncta * blockDim.x) {
+      if (j >= k0 && j < k0 + bs) continue;
+      double v[GJB];
+#pragma unroll
+      for (int k = 0; k < GJB; k++) v[k] = k < bs ? __ldcg(A + (size_t)(k0 + k) * n + j) : 0.0;
+      for (int r = 0; r < bs; r++) {
+        double sm = 0.0;
+#pragma unroll
+        for (int k = 0; k < GJB; k++) sm += ps[r][k] * v[k];
+        A[(size_t)(k0 + r) * n + j] = sm;
+      }
+    }
+    cl.sync();
+    // A[i,j] -= A[i,K] A[K,j] on 64 x 64 tiles, rows and columns of K skipped
+    for (int tile = rank; tile < ntiles; tile += ncta) {
+      const int i0 = (tile / ntj) * TI, j0 = (tile % ntj) * TJ;
+      for (int t = tid; t < TI * GJB; t += blockDim.x) {
+        const int r = t / GJB, k = t % GJB, i = i0 + r;
+        ak[r][k] = (i < n && k < bs) ? __ldcg(A + (size_t)i * n + k0 + k) : 0.0;
+      }
+      for (int t = tid; t < GJB * TJ; t += blockDim.x) {
+        const int k = t / TJ, c = t % TJ, j = j0 + c;
+        kb[k][c] = (j < n && k < bs) ? __ldcg(A + (size_t)(k0 + k) * n + j) : 0.0;
+      }
+      __syncthreads();
+      const int tx = tid % 16, ty = tid / 16;
+      double acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+#pragma unroll 8
+      for (int k = 0; k < GJB; k++) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) av[a] = ak[ty + 16 * a][k];
+#pragma unroll
+        for (int b = 0; b < 4; b++) bv[b] = kb[k][tx + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = i0 + ty + 16 * a;
+        if (i >= n || (i >= k0 && i < k0 + bs)) continue;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int j = j0 + tx + 16 * b;
+          if (j >= n || (j >= k0 && j < k0 + bs)) continue;
+          A[(size_t)i * n + j] = __ldcg(A + (size_t)i * n + j) - acc[a][b];
+        }
+      }
+      __syncthreads();
+    }
+    cl.sync();
+    // column panel: A[i, K] = -A[i, K] P outside K, P itself on K
+    for (int i = rank * blockDim.x + tid; i < n; i += ncta * blockDim.x) {
+      if (i >= k0 && i < k0 + bs) {
+        for (int c = 0; c < bs; c++) A[(size_t)i * n + k0 + c] = ps[i - k0][c];
+        continue;
+      }
+      double v[GJB];
+#pragma unroll
+      for (int k = 0; k < GJB; k++) v[k] = k < bs ? __ldcg(A + (size_t)i * n + k0 + k) : 0.0;
+      for (int c = 0; c < bs; c++) {
+        double sm = 0.0;
+#pragma unroll
+        for (int k = 0; k < GJB; k++) sm += v[k] * ps[k][c];
+        A[(size_t)i * n + k0 + c] = -sm;
+      }
+    }
+    cl.sync();
+  }
+}
+
 // an equation with a zero diagonal (a near-null-space column dropped by the
 // QR leaves a zero row and column) gets the identity
 __global__ void k_unit_empty_diag(int n, double *__restrict__ a) {
@@ -2607,15 +2744,18 @@ int mis_cluster_size() {
   return c;
 }
 
-// graphs of at most this many nodes run their independent-set rounds in one
-// cluster launch (SGPU_MIS=rounds: separate launches at every size)
+// with SGPU_MIS=cluster, graphs of at most this many nodes run their
+// independent-set rounds in one cluster launch.  Not the default: on the
+// 1.01M-DOF cantilever the set-up took 0.02-0.07 ms longer with it in every
+// run (the coarse levels' rounds are cheap once the level-0 bound no longer
+// holds the whole GPU)
 constexpr int kMisClusterNodes = 32768;
 
 int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t, cudaStream_t s) {
   const int nb = L.nb, g = grid_for(nb);
   {
     const char *me = getenv("SGPU_MIS");
-    const int cs = (nb <= kMisClusterNodes && !(me && !strcmp(me, "rounds"))) ? mis_cluster_size() : 0;
+    const int cs = (nb <= kMisClusterNodes && me && !strcmp(me, "cluster")) ? mis_cluster_size() : 0;
     if (cs > 0) {
       TmpBuf<uint64_t> m1(s);
       TmpBuf<int> cnt(s);
@@ -3388,6 +3528,42 @@ int coarse_bounds_enqueue(sgpu_matrix m, cudaStream_t s) {
   return SGPU_OK;
 }
 
+// cluster size for k_bgj_cluster (SGPU_GJ=cluster): 16 where the device
+// schedules it, else 8; 0 runs the four launches per pivot block, the
+// default: on the 1.01M-DOF cantilever the cluster launch took 1.34 ms
+// against 0.99 ms, since its 16 CTAs wait for SMs that the smoother bounds
+// on the second stream hold, where the separate launches interleave with them
+int gj_cluster_size() {
+  const char *e = getenv("SGPU_GJ");
+  if (!(e && !strcmp(e, "cluster"))) return 0;
+  static std::atomic<int> cached{-1};
+  int c = cached.load();
+  if (c >= 0) return c;
+  c = 0;
+  if (cudaFuncSetAttribute(k_bgj_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    cudaGetLastError();
+  for (int cs : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(TPB);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_bgj_cluster, &cfg) == cudaSuccess && nclusters >= 1) {
+      c = cs;
+      break;
+    }
+    cudaGetLastError();
+  }
+  cached.store(c);
+  return c;
+}
+
 // Builds the hierarchy (FP64 set-up).
 int amg_build(sgpu_matrix m) {
   Amg &A = *m->amg;
@@ -3501,7 +3677,24 @@ int amg_build(sgpu_matrix m) {
   SGPU_CUDA(cudaMemsetAsync(A.M64.p, 0, (size_t)A.nc * A.nc * sizeof(double), s));
   k_dense_fill<<<grid_for(Cl->nb), TPB, 0, s>>>(Cl->nb, Cl->b, A.nc, Cl->browptr, Cl->bcol, Cl->val64.p, A.M64.p);
   k_unit_empty_diag<<<grid_for(A.nc), TPB, 0, s>>>(A.nc, A.M64.p);
-  {
+  const int gj_cs = gj_cluster_size();
+  if (gj_cs > 0) {
+    TmpBuf<double> P(s);
+    SGPU_TRY(P.alloc(GJB * GJB));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(gj_cs);
+    cfg.blockDim = dim3(TPB);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = gj_cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    SGPU_CUDA(cudaLaunchKernelEx(&cfg, k_bgj_cluster, A.nc, A.M64.p, P.p));
+    count_launches(3);  // with k_dense_fill and k_unit_empty_diag
+  } else {
     TmpBuf<double> P(s);
     SGPU_TRY(P.alloc(GJB * GJB));
     const int nc = A.nc;

@@ -430,10 +430,10 @@ def test_half_precision_level0_values(oracle, gpu_lib, shape, monkeypatch):
 
 @pytest.mark.parametrize("case", ["cantilever", "plate"])
 def test_cluster_independent_set_gives_the_same_bits(oracle, gpu_lib, case):
-    # graphs of up to 32768 nodes run all their independent-set rounds in one
-    # thread-block cluster launch; the same keys, maxima and decisions as the
-    # separate launches per pass (SGPU_MIS=rounds), so the same aggregates,
-    # hierarchy and solve to the bit
+    # with SGPU_MIS=cluster, graphs of up to 32768 nodes run all their
+    # independent-set rounds in one thread-block cluster launch; the same
+    # keys, maxima and decisions as the separate launches per pass, so the
+    # same aggregates, hierarchy and solve to the bit
     if case == "cantilever":
         m = decks.cantilever_hex(40, 8, 8)
     else:
@@ -442,9 +442,34 @@ def test_cluster_independent_set_gives_the_same_bits(oracle, gpu_lib, case):
     f = oracle.load_vector(m)
     with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
         dm.set_nullspace(mefel.rigid_body_modes(m))
-        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", "rounds")
-        x1, r1 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", None)
+        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", None)
+        x1, r1 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", "cluster")
     assert r0.status == r1.status == L.OK
     assert r0.info["iterations"] == r1.info["iterations"]
     assert r0.info["precond_coarse_n"] == r1.info["precond_coarse_n"]
     assert np.array_equal(x0, x1)
+
+
+@pytest.mark.parametrize("case", ["cantilever", "plate"])
+def test_cluster_gauss_jordan_gives_the_same_bits(oracle, gpu_lib, case):
+    # the coarsest level's blocked Gauss-Jordan inverse in one thread-block
+    # cluster launch (SGPU_GJ=cluster) against four launches per pivot block:
+    # the same expressions in the same order, so the same inverse, hierarchy
+    # and solve to the bit
+    if case == "cantilever":
+        m = decks.cantilever_hex(40, 8, 8)
+    else:
+        m = decks.plate_quad(48, 24, E=3e10, nu=0.22)
+    adr, ci, a = _oracle_system(oracle, m)
+    f = oracle.load_vector(m)
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(mefel.rigid_body_modes(m))
+        for mode in ("mixed", "fp64"):
+            x0, r0 = _solve_with_env(dm, f, mode, "SGPU_GJ", None)
+            x1, r1 = _solve_with_env(dm, f, mode, "SGPU_GJ", "cluster")
+            assert r0.status == r1.status == L.OK
+            assert r0.info["precond_coarse_n"] == r1.info["precond_coarse_n"] > 0
+            assert r0.info["iterations"] == r1.info["iterations"]
+            assert np.array_equal(x0, x1)
+            assert np.linalg.norm(x1 - xo) / np.linalg.norm(xo) <= 1e-8
