@@ -2084,7 +2084,8 @@ constexpr size_t gal2_shared_bytes() {
   // [W][kGal2Cap][K*K] accumulators, [W][32][B*K | 1] staging, [W][B*K] the
   // current node's Q rows, the table
   return ((size_t)kGal2Warps * kGal2Cap * K * K + (size_t)kGal2Warps * 32 * ((B * K) | 1) +
-          (size_t)kGal2Warps * B * K) * sizeof(double) + sizeof(GalTable) + 3 * kGal2Nodes * sizeof(int);
+          (size_t)kGal2Warps * B * K) * sizeof(double) + sizeof(GalTable) +
+         (3 * kGal2Nodes + 64 * kGal2Warps) * sizeof(int);
 }
 
 template <int B, int K>
@@ -2102,6 +2103,7 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
   GalTable &T = *reinterpret_cast<GalTable *>(qis + (size_t)W * BK);
   int *pnode = reinterpret_cast<int *>(&T + 1);  // [kGal2Nodes] the aggregate's nodes
   int *prs = pnode + kGal2Nodes, *pre = prs + kGal2Nodes;  // their rows' ranges
+  int *gpos = pre + kGal2Nodes + 64 * w, *gmask = gpos + 32;  // this warp's groups of a chunk
   double *acc = accs + (size_t)w * kGal2Cap * KK;
   double *stage = stages + (size_t)w * 32 * SS;
   double *qi = qis + (size_t)w * BK;
@@ -2187,25 +2189,34 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
         __syncwarp();
         const bool ok = live && p >= 0;
         const unsigned grp = __match_any_sync(0xffffffffu, ok ? p : -2 - lane);
-        if (ok && __ffs(grp) - 1 == lane) {
-          double sm[BK];
+        const bool leader = ok && __ffs(grp) - 1 == lane;
+        const unsigned lmask = __ballot_sync(0xffffffffu, leader);
+        const int ng = __popc(lmask);
+        if (leader) {  // the groups in leader-lane order
+          const int g = __popc(lmask & ((1u << lane) - 1u));
+          gpos[g] = p;
+          gmask[g] = (int)grp;
+        }
+        __syncwarp();
+        // the group sums, work item (group, component) over all lanes: the
+        // members in lane order, the sum stored in the leader's stage row
+        // (only this item reads or writes that column of the group's rows)
+        for (int t = lane; t < ng * BK; t += 32) {
+          const int g = t / BK, x = t - g * BK;
+          const unsigned gm = (unsigned)gmask[g];
+          double sm = 0.0;
+          for (unsigned mm = gm; mm; mm &= mm - 1) sm += stage[(__ffs(mm) - 1) * SS + x];
+          stage[(__ffs(gm) - 1) * SS + x] = sm;
+        }
+        __syncwarp();
+        // Q_i^T (group sum) into the warp's accumulator, work item (group, entry)
+        for (int t = lane; t < ng * KK; t += 32) {
+          const int g = t / KK, v = t - g * KK, q1 = v / K, q2 = v - q1 * K;
+          const double *sg = stage + (__ffs((unsigned)gmask[g]) - 1) * SS;
+          double o = 0.0;
 #pragma unroll
-          for (int x = 0; x < BK; x++) sm[x] = 0.0;
-          for (unsigned mm = grp; mm; mm &= mm - 1) {
-            const double *src = stage + (__ffs(mm) - 1) * SS;
-#pragma unroll
-            for (int x = 0; x < BK; x++) sm[x] += src[x];
-          }
-          double *dst = acc + (size_t)p * KK;
-#pragma unroll
-          for (int q1 = 0; q1 < K; q1++)
-#pragma unroll
-            for (int q2 = 0; q2 < K; q2++) {
-              double v = 0.0;
-#pragma unroll
-              for (int c = 0; c < B; c++) v += qi[c * K + q1] * sm[c * K + q2];
-              dst[q1 * K + q2] += v;
-            }
+          for (int c = 0; c < B; c++) o += qi[c * K + q1] * sg[c * K + q2];
+          acc[(size_t)gpos[g] * KK + v] += o;
         }
         __syncwarp();
       }
