@@ -1517,8 +1517,9 @@ __global__ void k_root_flags(int nb, const uint64_t *__restrict__ t, int *__rest
 // an unaggregated root starts aggregate base + rootid; an unaggregated node
 // next to a root joins it (the roots are >= 3 apart: at most one is adjacent)
 __global__ void k_attach_roots(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
-                               const uint64_t *__restrict__ t, const int *__restrict__ rootid, int base,
-                               int *__restrict__ agg) {
+                               const uint64_t *__restrict__ t, const int *__restrict__ rootid,
+                               const int *__restrict__ base_d, int *__restrict__ agg) {
+  const int base = base_d ? *base_d : 0;  // aggregates numbered by earlier passes
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
     if (agg[i] >= 0) continue;
     int a = -1;
@@ -1532,6 +1533,13 @@ __global__ void k_attach_roots(int nb, const int *__restrict__ browptr, const in
     }
     agg[i] = a;
   }
+}
+
+// *total = (base_d ? *base_d : 0) + the roots of the exclusive scan `rootid`
+// of `flag` (one thread)
+__global__ void k_root_total(int nb, const int *__restrict__ rootid, const int *__restrict__ flag,
+                             const int *__restrict__ base_d, int *__restrict__ total) {
+  *total = (base_d ? *base_d : 0) + rootid[nb - 1] + flag[nb - 1];
 }
 
 __global__ void k_attach2(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
@@ -2799,7 +2807,7 @@ int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t
   const char *mis_env = getenv("SGPU_MIS");
   const bool warp_rows = !(mis_env && !strcmp(mis_env, "thread"));
   const int gw = grid_for((int64_t)nb * 8);
-  constexpr int kMaxRounds = 200, kGroup = 8;
+  constexpr int kMaxRounds = 200, kGroup = 16;  // rounds enqueued per host read of the count
   TmpBuf<uint64_t> m1(s), m2(s);
   TmpBuf<int> cnt(s);
   SGPU_TRY(m1.alloc(nb));
@@ -2837,8 +2845,8 @@ int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t
 
 // numbers the roots of t after `base` and attaches their unaggregated
 // neighbours; returns the number of new aggregates
-int take_roots(const AmgLevel &L, const TmpBuf<uint64_t> &t, int base, int *agg, cudaStream_t s, CubTmp &tmp,
-               int *count) {
+int take_roots(const AmgLevel &L, const TmpBuf<uint64_t> &t, const int *base_d, int *agg, cudaStream_t s,
+               CubTmp &tmp, int *total_d) {
   const int nb = L.nb, g = grid_for(nb);
   TmpBuf<int> flag(s), rootid(s);
   SGPU_TRY(flag.alloc(nb));
@@ -2849,13 +2857,9 @@ int take_roots(const AmgLevel &L, const TmpBuf<uint64_t> &t, int base, int *agg,
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag.p, rootid.p, nb, s);
   SGPU_TRY(tmp.ensure(bytes));
   SGPU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.buf.p, bytes, flag.p, rootid.p, nb, s));
-  int last[2] = {0, 0};  // the last node's id and root flag, one wait for both
-  SGPU_CUDA(cudaMemcpyAsync(&last[0], rootid.p + nb - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SGPU_CUDA(cudaMemcpyAsync(&last[1], flag.p + nb - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SGPU_CUDA(cudaStreamSynchronize(s));
-  *count = last[0] + last[1];
-  k_attach_roots<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, t.p, rootid.p, base, agg);
-  count_launches(1);
+  k_root_total<<<1, 1, 0, s>>>(nb, rootid.p, flag.p, base_d, total_d);
+  k_attach_roots<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, t.p, rootid.p, base_d, agg);
+  count_launches(2);
   SGPU_CUDA(cudaGetLastError());
   return SGPU_OK;
 }
@@ -2875,22 +2879,25 @@ int aggregate(AmgLevel &L, cudaStream_t s, CubTmp &tmp) {
   SGPU_TRY(t.alloc(nb));
   SGPU_TRY(agg1.alloc(nb));
   SGPU_TRY(cand.alloc(nb));
-  SGPU_TRY(cnt.alloc(1));
+  // cnt: aggregates after the first pass, after the second, nodes left over;
+  // the counts stay on the device until the one read after the last pass
+  SGPU_TRY(cnt.alloc(3));
+  SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, 3 * sizeof(int), s));
   SGPU_CUDA(cudaMemsetAsync(agg1.p, 0xff, (size_t)nb * sizeof(int), s));  // -1: unaggregated
   SGPU_TRY(mis2(L, nullptr, nullptr, t, s));
-  int na1 = 0, na2 = 0;
-  SGPU_TRY(take_roots(L, t, 0, agg1.p, s, tmp, &na1));
+  SGPU_TRY(take_roots(L, t, nullptr, agg1.p, s, tmp, cnt.p));
   k_mis_cand<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg1.p, 4, cand.p);
   count_launches(1);
   SGPU_TRY(mis2(L, cand.p, agg1.p, t, s));
-  SGPU_TRY(take_roots(L, t, na1, agg1.p, s, tmp, &na2));
-  L.na = na1 + na2;
+  SGPU_TRY(take_roots(L, t, cnt.p, agg1.p, s, tmp, cnt.p + 1));
   SGPU_TRY(L.agg.alloc(nb));
-  SGPU_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), s));
-  k_attach2<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg1.p, L.agg.p, cnt.p);
+  k_attach2<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg1.p, L.agg.p, cnt.p + 2);
   count_launches(1);
-  int lost = 0;
-  SGPU_TRY(read_int(cnt.p, s, &lost));
+  int hc[2] = {0, 0};
+  SGPU_CUDA(cudaMemcpyAsync(hc, cnt.p + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  SGPU_CUDA(cudaStreamSynchronize(s));
+  L.na = hc[0];
+  const int lost = hc[1];
   if (lost) return fail(SGPU_CUDA_ERROR, "aggregation left " + std::to_string(lost) + " nodes unassigned");
   // node lists per aggregate
   TmpBuf<int> keys_out(s), ids(s);
@@ -4372,13 +4379,19 @@ int amg_pcg_run(sgpu_matrix m, int64_t ni, double res, double zero, int64_t iv, 
   SGPU_CUDA(cudaEventSynchronize(m->ev1));
   float solve_ms = 0.f;
   SGPU_CUDA(cudaEventElapsedTime(&solve_ms, m->ev0, m->ev1));
-  // true FP64 residual of the returned x
-  Work &w = m->w;
-  SGPU_TRY(spmv64(m, w.x.p, w.p.p, s));
-  k_fcg_true<<<grid_for(m->n), TPB, 0, s>>>((int)m->n, w.f.p, w.p.p, pcg_state(m), w.partials.p, w.counters.p + 3);
-  count_launches(1);
+  // true FP64 residual of the returned x: the solve's own last check when it
+  // stopped on the true residual (x has not changed since), else formed here
   PcgState fin{};
-  SGPU_TRY(read_st(m, &fin));
+  if (crit == SGPU_CRIT_TRUE && hs.status == 0 && hs.true_rel > 0.0 && hs.true_rel < res) {
+    fin = hs;
+  } else {
+    Work &w = m->w;
+    SGPU_TRY(spmv64(m, w.x.p, w.p.p, s));
+    k_fcg_true<<<grid_for(m->n), TPB, 0, s>>>((int)m->n, w.f.p, w.p.p, pcg_state(m), w.partials.p,
+                                              w.counters.p + 3);
+    count_launches(1);
+    SGPU_TRY(read_st(m, &fin));
+  }
   if (hs.ani_set && hs.status == 0) {
     if (ani) *ani = hs.ani;
     if (ares) *ares = hs.ares;
