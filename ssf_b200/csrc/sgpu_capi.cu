@@ -112,6 +112,10 @@ int upload(sgpu_matrix m, const int64_t *adr, const int64_t *ci, const double *a
     SGPU_CUDA(cudaMemcpyAsync(a_d.p, a, negm * sizeof(double), cudaMemcpyHostToDevice, s));
   }
   SGPU_TRY(matrix_build_from_device_src(m));
+  // the 3x3 block form's pattern (the tuned FP64 SpMV and the aggregation
+  // cycle use it) while the values are still on their way; its values follow
+  // the CSR values in matrix_set_values_device
+  SGPU_TRY(ensure_bsr3(m));
   if (side.ok) SGPU_CUDA(cudaStreamWaitEvent(s, side.after_values, 0));
   SGPU_TRY(matrix_set_values_device(m, a_d.p));
   SGPU_CUDA(cudaEventRecord(m->ev1, s));
