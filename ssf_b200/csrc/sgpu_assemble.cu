@@ -26,6 +26,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
@@ -2079,6 +2080,7 @@ struct AssemblyData {
   DevBuf<int64_t> elems;
   DevBuf<int> cne, elist;
   std::vector<int> offsets;
+  std::vector<int> order;  // the per-colour element lists on the host (ascending ids per colour)
   // node -> element incidence, and whether every equation belongs to one
   // (node, component) (gencodnum's consecutive numbering): the row kernel's
   // precondition
@@ -2162,9 +2164,26 @@ int assemble_values(sgpu_matrix m, AssemblyData &ad, int kind, float *ms_out) {
     }
   }
   if (!rows_done) SGPU_CUDA(cudaMemsetAsync(c.val.p, 0, (size_t)c.nnz * sizeof(double), s));
+  // SGPU_ASSEMBLY_SLABS=k: k slabs of element ids, all colours of a slab
+  // before the next slab, so that the colours of a slab meet its rows in L2
+  // instead of reading and writing the value array from DRAM once per colour.
+  // Within a launch no two elements share a node (one colour) and launches
+  // run in stream order, so the scatter needs no atomics either way; the order
+  // of each entry's sum is fixed by the slab count.  Not the default: on the
+  // 1.01M-DOF cantilever the colour-major order (one slab) takes 2.03 ms, 4
+  // slabs 2.27 ms, 20 slabs (48 MB of rows each) 2.79 ms, 64 slabs 6.05 ms --
+  // the smaller launches lose more than L2 reuse gains.
   const int ncol = rows_done ? 0 : (int)ad.offsets.size() - 1;
-  for (int col = 0; col < ncol; col++) {
-    const int beg = ad.offsets[col], cnt = ad.offsets[col + 1] - beg;
+  int nslab = 1;
+  if (const char *se = std::getenv("SGPU_ASSEMBLY_SLABS"))
+    nslab = (int)std::max<int64_t>(1, std::min<int64_t>(std::min(256, atoi(se)), ad.ne));
+  for (int pass = 0; pass < ncol * nslab; pass++) {
+    const int sl = pass / ncol, col = pass % ncol;
+    const int *cb = ad.order.data() + ad.offsets[col], *ce = ad.order.data() + ad.offsets[col + 1];
+    const int lo = (int)(sl * ad.ne / nslab), hi = (int)((sl + 1) * ad.ne / nslab);
+    const int beg = (int)(std::lower_bound(cb, ce, lo) - ad.order.data());
+    const int end = (int)(std::lower_bound(cb, ce, hi) - ad.order.data());
+    const int cnt = end - beg;
     if (cnt == 0) continue;
     const int grid = std::min((cnt + WPB - 1) / WPB, kNumSMs * 16);
     const int *el = ad.elist.p + beg;
@@ -2425,11 +2444,10 @@ SGPU_API int sgpu_assemble(const sgpu_mesh *mesh, sgpu_matrix *out, sgpu_assembl
   cudaEventDestroy(t1);
 
   // colouring (host) and the per-colour element lists
-  std::vector<int> order;
-  st = colour_elements(nn, ne, nne, mesh->elems, order, ad.offsets);
+  st = colour_elements(nn, ne, nne, mesh->elems, ad.order, ad.offsets);
   if (st != SGPU_OK) return bail(st);
   if (ad.elist.alloc(ne) != SGPU_OK) return bail(SGPU_CUDA_ERROR);
-  cudaMemcpyAsync(ad.elist.p, order.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(ad.elist.p, ad.order.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s);
   float asm_ms = 0.f;
   st = assemble_values(m, ad, kind, &asm_ms);
   if (st != SGPU_OK) return bail(st);
@@ -2517,6 +2535,7 @@ SGPU_API int sgpu_assemble_copy(sgpu_matrix src, int32_t kind, const double *ema
   ad.kind = kind; ad.nne = sa.nne; ad.ndofn = sa.ndofn; ad.nn = sa.nn; ad.ne = sa.ne;
   ad.general = sa.general;
   ad.offsets = sa.offsets;
+  ad.order = sa.order;
   Csr &c = m->csr;
   c.n = src->csr.n;
   c.nnz = src->csr.nnz;

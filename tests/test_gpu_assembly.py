@@ -20,17 +20,18 @@ from ssf_b200 import decks
 pytestmark = pytest.mark.gpu
 
 
-FORMS = {  # name: (SGPU_ASSEMBLY_ROWS, SGPU_HEX8_FULL, SGPU_HEX8_GATHER)
-    "gather": (None, None, "1"),   # element blocks into a buffer, rows gathered per node
-    "rows": ("1", None, None),     # one warp per node forms its elements' blocks, rows written once
-    "iso": (None, None, None),     # colour-ordered, P-form on the pairs a <= b (default)
-    "full": (None, "1", None),     # colour-ordered, full B^T D B product per block
+FORMS = {  # name: (SGPU_ASSEMBLY_ROWS, SGPU_HEX8_FULL, SGPU_HEX8_GATHER, SGPU_ASSEMBLY_SLABS)
+    "gather": (None, None, "1", None),   # element blocks into a buffer, rows gathered per node
+    "rows": ("1", None, None, None),     # one warp per node forms its elements' blocks, rows written once
+    "iso": (None, None, None, None),     # colour-ordered, P-form on the pairs a <= b (default)
+    "full": (None, "1", None, None),     # colour-ordered, full B^T D B product per block
+    "slabs": (None, None, None, "3"),    # colour-ordered within three slabs of element ids
 }
 
 
 def _download(m, form):
     from ssf_b200 import mefel
-    names = ("SGPU_ASSEMBLY_ROWS", "SGPU_HEX8_FULL", "SGPU_HEX8_GATHER")
+    names = ("SGPU_ASSEMBLY_ROWS", "SGPU_HEX8_FULL", "SGPU_HEX8_GATHER", "SGPU_ASSEMBLY_SLABS")
     old = {k: os.environ.pop(k, None) for k in names}
     for k, v in zip(names, FORMS[form]):
         if v is not None:
@@ -55,7 +56,7 @@ def _check(oracle, m):
         assert np.allclose(g_a, a, rtol=1e-12, atol=tol), form
         out[form] = g_a
     # the GPU forms differ only in rounding
-    for form in ("rows", "full", "gather"):
+    for form in ("rows", "full", "gather", "slabs"):
         assert np.allclose(out[form], out["iso"], rtol=1e-13, atol=1e-13 * np.abs(a).max()), form
     # the gather sums the same blocks as the colour-ordered scatter, in
     # ascending element order instead of colour order: rounding apart, equal
