@@ -1375,7 +1375,16 @@ __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *
   for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
     const int i = base + g;
     uint64_t m = 0;
-    if (i < nb) {
+    // nodes that take no part: an aggregated node (second pass: no node
+    // reads its maximum, it has nothing to decide) and, in the deciding
+    // pass, a node already decided (its maximum feeds nothing else)
+    uint64_t ti = 0;
+    bool on_i = i < nb && (agg == nullptr || __ldg(agg + i) < 0);
+    if (DECIDE && on_i) {
+      ti = t[i];
+      on_i = (ti >> 62) == 1;
+    }
+    if (on_i) {
       if (sub == 0) m = in[i];
       const int re = browptr[i + 1];
       // four neighbours per lane in flight: their columns first, then their
@@ -1398,16 +1407,13 @@ __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *
     }
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) m = max(m, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)m, o, LPR));
-    if (i < nb && sub == 0) {
+    if (on_i && sub == 0) {
       if (!DECIDE) {
         out[i] = m;
-      } else {
-        const uint64_t ti = t[i];
-        if ((ti >> 62) == 1) {
-          if (m == ti) t[i] = mis_key(2, i);
-          else if ((m >> 62) == 2) t[i] = ti & ~(3ull << 62);
-          else cnt++;
-        }
+      } else {  // ti undecided
+        if (m == ti) t[i] = mis_key(2, i);
+        else if ((m >> 62) == 2) t[i] = ti & ~(3ull << 62);
+        else cnt++;
       }
     }
   }
@@ -2087,13 +2093,62 @@ constexpr int kGal2Cap = 40;  // blocks per coarse row
 constexpr int kGal2Warps = 4;
 constexpr int kGal2Nodes = 128;  // an aggregate's nodes and rows read ahead into shared memory
 
+// cap: the longest coarse row of the level (<= kGal2Cap), the accumulators'
+// blocks per warp (fewer blocks, more CTAs per SM)
 template <int B, int K>
-constexpr size_t gal2_shared_bytes() {
-  // [W][kGal2Cap][K*K] accumulators, [W][32][B*K | 1] staging, [W][B*K] the
+constexpr size_t gal2_shared_bytes(int cap) {
+  // [W][cap][K*K] accumulators, [W][32][B*K | 1] staging, [W][B*K] the
   // current node's Q rows, the table
-  return ((size_t)kGal2Warps * kGal2Cap * K * K + (size_t)kGal2Warps * 32 * ((B * K) | 1) +
+  return ((size_t)kGal2Warps * cap * K * K + (size_t)kGal2Warps * 32 * ((B * K) | 1) +
           (size_t)kGal2Warps * B * K) * sizeof(double) + sizeof(GalTable) +
          (3 * kGal2Nodes + 64 * kGal2Warps) * sizeof(int);
+}
+
+// One chunk of the row walk of k_gal_values2: node k of the aggregate (i,
+// its row [rs, re)), entries t0 .. t0 + 31; fresh: the node's first chunk.
+struct GalChunk {
+  int k, i, rs, re, t0;
+  bool fresh;
+};
+
+// The groups of one staged chunk (the lanes whose entries fall into one
+// coarse block): each group's sum in lane order into its leader's stage row,
+// then Q_i^T (that sum) added into the warp's accumulator of the block.
+template <int B, int K>
+__device__ __forceinline__ void gal2_groups(int lane, bool ok, int p, double *stage, int *gpos, int *gmask,
+                                            const double *qi, double *acc) {
+  constexpr int KK = K * K, BK = B * K, SS = BK | 1;
+  const unsigned grp = __match_any_sync(0xffffffffu, ok ? p : -2 - lane);
+  const bool leader = ok && __ffs(grp) - 1 == lane;
+  const unsigned lmask = __ballot_sync(0xffffffffu, leader);
+  const int ng = __popc(lmask);
+  if (leader) {  // the groups in leader-lane order
+    const int g = __popc(lmask & ((1u << lane) - 1u));
+    gpos[g] = p;
+    gmask[g] = (int)grp;
+  }
+  __syncwarp();
+  // the group sums, work item (group, component) over all lanes: the
+  // members in lane order, the sum stored in the leader's stage row (only
+  // this item reads or writes that column of the group's rows)
+  for (int t = lane; t < ng * BK; t += 32) {
+    const int g = t / BK, x = t - g * BK;
+    const unsigned gm = (unsigned)gmask[g];
+    double sm = 0.0;
+    for (unsigned mm = gm; mm; mm &= mm - 1) sm += stage[(__ffs(mm) - 1) * SS + x];
+    stage[(__ffs(gm) - 1) * SS + x] = sm;
+  }
+  __syncwarp();
+  // Q_i^T (group sum) into the warp's accumulator, work item (group, entry)
+  for (int t = lane; t < ng * KK; t += 32) {
+    const int g = t / KK, v = t - g * KK, q1 = v / K, q2 = v - q1 * K;
+    const double *sg = stage + (__ffs((unsigned)gmask[g]) - 1) * SS;
+    double o = 0.0;
+#pragma unroll
+    for (int c = 0; c < B; c++) o += qi[c * K + q1] * sg[c * K + q2];
+    acc[(size_t)gpos[g] * KK + v] += o;
+  }
+  __syncwarp();
 }
 
 template <int B, int K>
@@ -2101,18 +2156,18 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
     k_gal_values2(int na, const int *__restrict__ aggptr, const int *__restrict__ aggnodes,
                   const int *__restrict__ agg, LevelView A, const double *__restrict__ Q,
                   const int *__restrict__ lists, const int *__restrict__ cbrowptr, int *__restrict__ cbcol,
-                  double *__restrict__ out) {
+                  double *__restrict__ out, int cap, bool pipe) {
   constexpr int KK = K * K, BK = B * K, SS = BK | 1, W = kGal2Warps;
   extern __shared__ double gal2_sh[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double *accs = gal2_sh;                                  // [W][kGal2Cap][KK]
-  double *stages = accs + (size_t)W * kGal2Cap * KK;       // [W][32][SS]
+  double *accs = gal2_sh;                            // [W][cap][KK]
+  double *stages = accs + (size_t)W * cap * KK;      // [W][32][SS]
   double *qis = stages + (size_t)W * 32 * SS;              // [W][BK]
   GalTable &T = *reinterpret_cast<GalTable *>(qis + (size_t)W * BK);
   int *pnode = reinterpret_cast<int *>(&T + 1);  // [kGal2Nodes] the aggregate's nodes
   int *prs = pnode + kGal2Nodes, *pre = prs + kGal2Nodes;  // their rows' ranges
   int *gpos = pre + kGal2Nodes + 64 * w, *gmask = gpos + 32;  // this warp's groups of a chunk
-  double *acc = accs + (size_t)w * kGal2Cap * KK;
+  double *acc = accs + (size_t)w * cap * KK;
   double *stage = stages + (size_t)w * 32 * SS;
   double *qi = qis + (size_t)w * BK;
   for (int G = blockIdx.x; G < na; G += gridDim.x) {
@@ -2126,14 +2181,14 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
     for (int h = threadIdx.x; h < kGalHash; h += blockDim.x) T.key[h] = -1;
     for (int t = threadIdx.x; t < W * n * KK; t += blockDim.x) {
       const int ww = t / (n * KK);
-      accs[(size_t)ww * kGal2Cap * KK + (t - ww * n * KK)] = 0.0;
+      accs[(size_t)ww * cap * KK + (t - ww * n * KK)] = 0.0;
     }
     __syncthreads();
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
       const int H = __ldg(lists + (size_t)G * kGalCap + t);
       T.list[t] = H;
       unsigned h = gal_hash(H);
-      for (int p = 0; p < kGalHash; p++) {  // n <= kGal2Cap < kGalHash keys: a free slot exists
+      for (int p = 0; p < kGalHash; p++) {  // n <= cap < kGalHash keys: a free slot exists
         if (atomicCAS(&T.key[h], -1, H) == -1) {
           T.pos[h] = t;
           break;
@@ -2148,92 +2203,164 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
         pre[t] = __ldg(A.browptr + i + 1);
       }
     __syncthreads();
-    for (int k = w; k < an; k += W) {
-      const int i = ahead ? pnode[k] : __ldg(aggnodes + a0 + k);
-      const int rs = ahead ? prs[k] : __ldg(A.browptr + i), re = ahead ? pre[k] : __ldg(A.browptr + i + 1);
-      for (int c = lane; c < BK; c += 32) qi[c] = __ldg(Q + (size_t)i * BK + c);
-      double di[B];
+    // the plain walk: a node's chunks one after another
+    auto walk_plain = [&]() {
+      for (int k = w; k < an; k += W) {
+        const int i = ahead ? pnode[k] : __ldg(aggnodes + a0 + k);
+        const int rs = ahead ? prs[k] : __ldg(A.browptr + i), re = ahead ? pre[k] : __ldg(A.browptr + i + 1);
+        for (int c = lane; c < BK; c += 32) qi[c] = __ldg(Q + (size_t)i * BK + c);
+        double di[B];
 #pragma unroll
-      for (int c = 0; c < B; c++) di[c] = A.layout == 0 ? 1.0 : __ldg(A.dscale + (size_t)B * i + c);
-      __syncwarp();
-      for (int t0 = rs; t0 < re; t0 += 32) {
-        const int e = t0 + lane;
-        const bool live = e < re;
-        int p = -1;
-        if (live) {
-          const int j = __ldg(A.bcol + e);
-          p = gal_find(T, __ldg(agg + j));
-          double av[B * B];
-          if (A.layout == 0) {
+        for (int c = 0; c < B; c++) di[c] = A.layout == 0 ? 1.0 : __ldg(A.dscale + (size_t)B * i + c);
+        __syncwarp();
+        for (int t0 = rs; t0 < re; t0 += 32) {
+          const int e = t0 + lane;
+          const bool live = e < re;
+          int p = -1;
+          if (live) {
+            const int j = __ldg(A.bcol + e);
+            p = gal_find(T, __ldg(agg + j));
+            double av[B * B];
+            if (A.layout == 0) {
 #pragma unroll
-            for (int c = 0; c < B * B; c++) av[c] = __ldg(A.val + (size_t)e * B * B + c);
-          } else {
-            double dj[B];
+              for (int c = 0; c < B * B; c++) av[c] = __ldg(A.val + (size_t)e * B * B + c);
+            } else {
+              double dj[B];
 #pragma unroll
-            for (int c = 0; c < B; c++) dj[c] = __ldg(A.dscale + (size_t)B * j + c);
-            const int nbr = re - rs;
+              for (int c = 0; c < B; c++) dj[c] = __ldg(A.dscale + (size_t)B * j + c);
+              const int nbr = re - rs;
 #pragma unroll
-            for (int c = 0; c < B * B; c++) {
-              // layout 1: the row's blocks component-major; layout 2 (B = 1): CSR
-              const double v = A.layout == 1 ? __ldg(A.val + 9ll * rs + (int64_t)c * nbr + (e - rs))
-                                             : __ldg(A.val + e);
-              av[c] = v * di[c / B] * dj[c % B];
+              for (int c = 0; c < B * B; c++) {
+                // layout 1: the row's blocks component-major; layout 2 (B = 1): CSR
+                const double v = A.layout == 1 ? __ldg(A.val + 9ll * rs + (int64_t)c * nbr + (e - rs))
+                                               : __ldg(A.val + e);
+                av[c] = v * di[c / B] * dj[c % B];
+              }
+            }
+#pragma unroll
+            for (int q2 = 0; q2 < K; q2++) {
+              double qj[B];
+#pragma unroll
+              for (int c2 = 0; c2 < B; c2++) qj[c2] = __ldg(Q + (size_t)j * BK + c2 * K + q2);
+#pragma unroll
+              for (int c = 0; c < B; c++) {
+                double sacc = 0.0;
+#pragma unroll
+                for (int c2 = 0; c2 < B; c2++) sacc += av[c * B + c2] * qj[c2];
+                stage[lane * SS + c * K + q2] = sacc;
+              }
             }
           }
+          __syncwarp();
+          gal2_groups<B, K>(lane, live && p >= 0, p, stage, gpos, gmask, qi, acc);
+        }
+      }
+    };
+    if constexpr (B > 3) {
+      walk_plain();
+    } else if (!pipe) {
+      walk_plain();
+    } else {
+      // The same walk software-pipelined (B <= 3, where one chunk's loads fit
+      // in registers): the chunks in the same order and the same arithmetic,
+      // so the same bits, but the global loads of the next chunk (its values,
+      // the aggregates, scalings and Q rows of its columns) are in flight
+      // while this chunk's groups are summed in shared memory, and the
+      // columns of the chunk after that one a step earlier still.
+      auto node_at = [&](GalChunk &c) {
+        if (c.k >= an) return;
+        c.i = ahead ? pnode[c.k] : __ldg(aggnodes + a0 + c.k);
+        c.rs = ahead ? prs[c.k] : __ldg(A.browptr + c.i);
+        c.re = ahead ? pre[c.k] : __ldg(A.browptr + c.i + 1);
+        c.t0 = c.rs;
+        c.fresh = true;
+      };
+      auto advance = [&](GalChunk &c) {
+        if (c.t0 + 32 < c.re) {
+          c.t0 += 32;
+          c.fresh = false;
+        } else {
+          c.k += W;
+          node_at(c);
+        }
+      };
+      auto column = [&](const GalChunk &c) {
+        const int e = c.t0 + lane;
+        return c.k < an && e < c.re ? __ldg(A.bcol + e) : -1;
+      };
+      // one chunk's loads: its column's aggregate, the values, both
+      // scalings, Q_j, and (first chunk of a node) lane x's entry of Q_i
+      int rH = -1;
+      double rav[B * B], rdi[B], rdj[B], rq[BK], rqi = 0.0;
+      auto fetch = [&](const GalChunk &c, int j) {
+        if (c.k >= an) return;
+        const int e = c.t0 + lane;
+#pragma unroll
+        for (int x = 0; x < B; x++) rdi[x] = A.layout == 0 ? 1.0 : __ldg(A.dscale + (size_t)B * c.i + x);
+        if (c.fresh && lane < BK) rqi = __ldg(Q + (size_t)c.i * BK + lane);
+        if (j >= 0) {
+          rH = __ldg(agg + j);
+          if (A.layout == 0) {
+#pragma unroll
+            for (int x = 0; x < B * B; x++) rav[x] = __ldg(A.val + (size_t)e * B * B + x);
+          } else {
+            const int nbr = c.re - c.rs;
+#pragma unroll
+            for (int x = 0; x < B; x++) rdj[x] = __ldg(A.dscale + (size_t)B * j + x);
+#pragma unroll
+            for (int x = 0; x < B * B; x++)
+              rav[x] = A.layout == 1 ? __ldg(A.val + 9ll * c.rs + (int64_t)x * nbr + (e - c.rs)) : __ldg(A.val + e);
+          }
+#pragma unroll
+          for (int x = 0; x < BK; x++) rq[x] = __ldg(Q + (size_t)j * BK + x);
+        }
+      };
+      GalChunk cur{w, 0, 0, 0, 0, true};
+      node_at(cur);
+      int cj = column(cur);
+      fetch(cur, cj);
+      GalChunk nx = cur;
+      advance(nx);
+      int nj = column(nx);
+      while (cur.k < an) {
+        // this chunk: stage T_ij = A_ij Q_j, the node's Q_i rows on its first chunk
+        const bool live = cj >= 0;
+        int p = -1;
+        if (cur.fresh && lane < BK) qi[lane] = rqi;
+        if (live) {
+          p = gal_find(T, rH);
+          double av[B * B];
+#pragma unroll
+          for (int x = 0; x < B * B; x++) av[x] = A.layout == 0 ? rav[x] : rav[x] * rdi[x / B] * rdj[x % B];
 #pragma unroll
           for (int q2 = 0; q2 < K; q2++) {
-            double qj[B];
-#pragma unroll
-            for (int c2 = 0; c2 < B; c2++) qj[c2] = __ldg(Q + (size_t)j * BK + c2 * K + q2);
 #pragma unroll
             for (int c = 0; c < B; c++) {
               double sacc = 0.0;
 #pragma unroll
-              for (int c2 = 0; c2 < B; c2++) sacc += av[c * B + c2] * qj[c2];
+              for (int c2 = 0; c2 < B; c2++) sacc += av[c * B + c2] * rq[c2 * K + q2];
               stage[lane * SS + c * K + q2] = sacc;
             }
           }
         }
         __syncwarp();
-        const bool ok = live && p >= 0;
-        const unsigned grp = __match_any_sync(0xffffffffu, ok ? p : -2 - lane);
-        const bool leader = ok && __ffs(grp) - 1 == lane;
-        const unsigned lmask = __ballot_sync(0xffffffffu, leader);
-        const int ng = __popc(lmask);
-        if (leader) {  // the groups in leader-lane order
-          const int g = __popc(lmask & ((1u << lane) - 1u));
-          gpos[g] = p;
-          gmask[g] = (int)grp;
-        }
-        __syncwarp();
-        // the group sums, work item (group, component) over all lanes: the
-        // members in lane order, the sum stored in the leader's stage row
-        // (only this item reads or writes that column of the group's rows)
-        for (int t = lane; t < ng * BK; t += 32) {
-          const int g = t / BK, x = t - g * BK;
-          const unsigned gm = (unsigned)gmask[g];
-          double sm = 0.0;
-          for (unsigned mm = gm; mm; mm &= mm - 1) sm += stage[(__ffs(mm) - 1) * SS + x];
-          stage[(__ffs(gm) - 1) * SS + x] = sm;
-        }
-        __syncwarp();
-        // Q_i^T (group sum) into the warp's accumulator, work item (group, entry)
-        for (int t = lane; t < ng * KK; t += 32) {
-          const int g = t / KK, v = t - g * KK, q1 = v / K, q2 = v - q1 * K;
-          const double *sg = stage + (__ffs((unsigned)gmask[g]) - 1) * SS;
-          double o = 0.0;
-#pragma unroll
-          for (int c = 0; c < B; c++) o += qi[c * K + q1] * sg[c * K + q2];
-          acc[(size_t)gpos[g] * KK + v] += o;
-        }
-        __syncwarp();
+        // the next chunk's loads, and the columns of the one after it
+        fetch(nx, nj);
+        GalChunk nn = nx;
+        advance(nn);
+        const int nnj = column(nn);
+        gal2_groups<B, K>(lane, live && p >= 0, p, stage, gpos, gmask, qi, acc);
+        cur = nx;
+        cj = nj;
+        nx = nn;
+        nj = nnj;
       }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < n * KK; t += blockDim.x) {
       double v = accs[t];
 #pragma unroll
-      for (int ww = 1; ww < W; ww++) v += accs[(size_t)ww * kGal2Cap * KK + t];
+      for (int ww = 1; ww < W; ww++) v += accs[(size_t)ww * cap * KK + t];
       out[(size_t)base * KK + t] = v;
     }
     for (int t = threadIdx.x; t < n; t += blockDim.x) cbcol[base + t] = T.list[t];
@@ -2258,14 +2385,18 @@ __global__ void k_coarse_dinv(int na, int K, const int *__restrict__ browptr, co
   }
 }
 
+// the coarsest level's blocks into the dense matrix: a warp per block row,
+// its lanes over the row's values in storage order (coalesced reads)
 __global__ void k_dense_fill(int nb, int K, int nc, const int *__restrict__ browptr, const int *__restrict__ bcol,
                              const double *__restrict__ val, double *__restrict__ M) {
-  for (int G = blockIdx.x * blockDim.x + threadIdx.x; G < nb; G += gridDim.x * blockDim.x)
-    for (int e = browptr[G]; e < browptr[G + 1]; e++) {
-      const int H = bcol[e];
-      for (int a = 0; a < K; a++)
-        for (int c = 0; c < K; c++) M[(size_t)(G * K + a) * nc + H * K + c] = val[(size_t)e * K * K + a * K + c];
+  const int lane = threadIdx.x & 31, KK = K * K;
+  for (int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; G < nb; G += (gridDim.x * blockDim.x) >> 5) {
+    const int rs = browptr[G], cnt = (browptr[G + 1] - rs) * KK;
+    for (int t = lane; t < cnt; t += 32) {
+      const int e = rs + t / KK, v = t % KK, a = v / K, c = v - a * K;
+      M[(size_t)(G * K + a) * nc + bcol[e] * K + c] = val[(size_t)rs * KK + t];
     }
+  }
 }
 
 // Blocked Gauss-Jordan inverse (pivot blocks of 32, no pivoting: the matrix
@@ -2277,49 +2408,53 @@ __global__ void k_dense_fill(int nb, int K, int nc, const int *__restrict__ brow
 //   A[i,K] = -A[i,K] P, A[K,K] = P for i not in K   (k_bgj_colpanel)
 constexpr int GJB = 32;
 
+// one CTA, a thread per entry; every step reads the previous step's matrix
+// and writes the other copy, so a step needs one barrier
 __global__ void __launch_bounds__(GJB *GJB) k_bgj_diag(int n, int k0, int bs, const double *__restrict__ A,
                                                        double *__restrict__ P) {
-  __shared__ double d[GJB][GJB + 1];
-  __shared__ double col[GJB];
+  __shared__ double d[2][GJB][GJB + 1];
   const int r = threadIdx.x / GJB, c = threadIdx.x % GJB;
-  d[r][c] = (r < bs && c < bs) ? A[(size_t)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+  d[0][r][c] = (r < bs && c < bs) ? A[(size_t)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
   __syncthreads();
   for (int k = 0; k < GJB; k++) {
-    const double piv = 1.0 / d[k][k];
-    if (c == 0) col[r] = d[r][k];
-    __syncthreads();
-    double v = d[r][c];
+    const double(*o)[GJB + 1] = d[k & 1];
+    const double piv = 1.0 / o[k][k];
+    const double colr = o[r][k];
+    double v = o[r][c];
     if (r == k) v = (c == k) ? piv : v * piv;
-    else v = (c == k) ? -col[r] * piv : v - col[r] * d[k][c] * piv;
-    __syncthreads();
-    d[r][c] = v;
+    else v = (c == k) ? -colr * piv : v - colr * o[k][c] * piv;
+    d[(k + 1) & 1][r][c] = v;
     __syncthreads();
   }
-  P[r * GJB + c] = d[r][c];
+  P[r * GJB + c] = d[GJB & 1][r][c];
 }
 
+// A[K, j] = P A[K, j] for the columns j outside K: a CTA per 32 columns, the
+// columns' K rows staged first (each CTA reads and writes only its columns)
 __global__ void __launch_bounds__(TPB) k_bgj_rowpanel(int n, int k0, int bs, const double *__restrict__ P,
                                                       double *__restrict__ A) {
-  __shared__ double ps[GJB][GJB];
-  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) ps[t / GJB][t % GJB] = P[t];
+  __shared__ double ps[GJB][GJB + 1];
+  __shared__ double vt[GJB][GJB + 1];  // vt[k][jj] = A[k0 + k, j0 + jj]
+  const int j0 = blockIdx.x * GJB;
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) {
+    const int k = t / GJB, jj = t % GJB, j = j0 + jj;
+    ps[k][jj] = P[t];
+    vt[k][jj] = (k < bs && j < n) ? A[(size_t)(k0 + k) * n + j] : 0.0;
+  }
   __syncthreads();
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    if (j >= k0 && j < k0 + bs) continue;
-    double v[GJB];
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) {
+    const int r = t / GJB, jj = t % GJB, j = j0 + jj;
+    if (r >= bs || j >= n || (j >= k0 && j < k0 + bs)) continue;
+    double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < GJB; k++) v[k] = k < bs ? A[(size_t)(k0 + k) * n + j] : 0.0;
-    for (int r = 0; r < bs; r++) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < GJB; k++) s += ps[r][k] * v[k];
-      A[(size_t)(k0 + r) * n + j] = s;
-    }
+    for (int k = 0; k < GJB; k++) s += ps[r][k] * vt[k][jj];
+    A[(size_t)(k0 + r) * n + j] = s;
   }
 }
 
-// A[i,j] -= A[i,K] A[K,j] on 64 x 64 tiles (rows and columns of K skipped)
+// A[i,j] -= A[i,K] A[K,j] on 32 x 32 tiles (rows and columns of K skipped)
 __global__ void __launch_bounds__(TPB) k_bgj_update(int n, int k0, int bs, double *__restrict__ A) {
-  constexpr int TI = 64, TJ = 64;
+  constexpr int TI = 32, TJ = 32;
   __shared__ double ak[TI][GJB + 1];  // A[i, K]
   __shared__ double kb[GJB][TJ];      // A[K, j]
   const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
@@ -2332,31 +2467,32 @@ __global__ void __launch_bounds__(TPB) k_bgj_update(int n, int k0, int bs, doubl
     kb[k][c] = (j < n && k < bs) ? A[(size_t)(k0 + k) * n + j] : 0.0;
   }
   __syncthreads();
-  // 256 threads, 16 elements each: thread (ty, tx) owns rows ty + 16 a, column tx + ... 
+  // 256 threads, 4 elements each: thread (ty, tx) owns rows ty + 16 a and
+  // columns tx + 16 b (a, b < 2); every element's sum over k in order
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4];
+  double acc[2][2];
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int a = 0; a < 2; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    for (int b = 0; b < 2; b++) acc[a][b] = 0.0;
 #pragma unroll 8
   for (int k = 0; k < GJB; k++) {
-    double av[4], bv[4];
+    double av[2], bv[2];
 #pragma unroll
-    for (int a = 0; a < 4; a++) av[a] = ak[ty + 16 * a][k];
+    for (int a = 0; a < 2; a++) av[a] = ak[ty + 16 * a][k];
 #pragma unroll
-    for (int b = 0; b < 4; b++) bv[b] = kb[k][tx + 16 * b];
+    for (int b = 0; b < 2; b++) bv[b] = kb[k][tx + 16 * b];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int a = 0; a < 2; a++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+      for (int b = 0; b < 2; b++) acc[a][b] += av[a] * bv[b];
   }
 #pragma unroll
-  for (int a = 0; a < 4; a++) {
+  for (int a = 0; a < 2; a++) {
     const int i = i0 + ty + 16 * a;
     if (i >= n || (i >= k0 && i < k0 + bs)) continue;
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
+    for (int b = 0; b < 2; b++) {
       const int j = j0 + tx + 16 * b;
       if (j >= n || (j >= k0 && j < k0 + bs)) continue;
       A[(size_t)i * n + j] -= acc[a][b];
@@ -2364,25 +2500,30 @@ __global__ void __launch_bounds__(TPB) k_bgj_update(int n, int k0, int bs, doubl
   }
 }
 
+// A[i, K] = -A[i, K] P for the rows i outside K, A[K, K] = P: a CTA per 32
+// rows, the rows' K columns staged first
 __global__ void __launch_bounds__(TPB) k_bgj_colpanel(int n, int k0, int bs, const double *__restrict__ P,
                                                       double *__restrict__ A) {
-  __shared__ double ps[GJB][GJB];
-  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) ps[t / GJB][t % GJB] = P[t];
+  __shared__ double ps[GJB][GJB + 1];
+  __shared__ double vt[GJB][GJB + 1];  // vt[ii][k] = A[i0 + ii, k0 + k]
+  const int i0 = blockIdx.x * GJB;
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) {
+    const int ii = t / GJB, k = t % GJB, i = i0 + ii;
+    ps[ii][k] = P[t];
+    vt[ii][k] = (i < n && k < bs) ? A[(size_t)i * n + k0 + k] : 0.0;
+  }
   __syncthreads();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) {
+    const int ii = t / GJB, c = t % GJB, i = i0 + ii;
+    if (i >= n || c >= bs) continue;
     if (i >= k0 && i < k0 + bs) {
-      for (int c = 0; c < bs; c++) A[(size_t)i * n + k0 + c] = ps[i - k0][c];
+      A[(size_t)i * n + k0 + c] = ps[i - k0][c];
       continue;
     }
-    double v[GJB];
+    double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < GJB; k++) v[k] = k < bs ? A[(size_t)i * n + k0 + k] : 0.0;
-    for (int c = 0; c < bs; c++) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < GJB; k++) s += v[k] * ps[k][c];
-      A[(size_t)i * n + k0 + c] = -s;
-    }
+    for (int k = 0; k < GJB; k++) s += vt[ii][k] * ps[k][c];
+    A[(size_t)i * n + k0 + c] = -s;
   }
 }
 
@@ -2763,18 +2904,25 @@ int mis_cluster_size() {
   return c;
 }
 
-// with SGPU_MIS=cluster, graphs of at most this many nodes run their
-// independent-set rounds in one cluster launch.  Not the default: on the
-// 1.01M-DOF cantilever the set-up took 0.02-0.07 ms longer with it in every
-// run (the coarse levels' rounds are cheap once the level-0 bound no longer
-// holds the whole GPU)
+// Graphs of at most kMisClusterDefault nodes run their independent-set
+// rounds in one cluster launch (on the 1.01M-DOF cantilever that is the
+// 945-node level 2: set-up 5.08-5.11 ms against 5.17-5.19 ms with a launch
+// per pass); the larger graphs' rounds run as separate launches over the
+// whole GPU (with the cluster for the 14,586-node level 1 as well, 5.11 ms;
+// up to kMisClusterNodes, 0.02-0.07 ms slower than launches)
+constexpr int kMisClusterDefault = 2048;
 constexpr int kMisClusterNodes = 32768;
 
 int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t, cudaStream_t s) {
   const int nb = L.nb, g = grid_for(nb);
   {
+    // graphs of at most kMisClusterDefault nodes; SGPU_MIS=cluster:N (at
+    // most N nodes), cluster (kMisClusterNodes), rounds (none)
     const char *me = getenv("SGPU_MIS");
-    const int cs = (nb <= kMisClusterNodes && me && !strcmp(me, "cluster")) ? mis_cluster_size() : 0;
+    int most = kMisClusterDefault;
+    if (me && !strncmp(me, "cluster", 7)) most = me[7] == ':' ? atoi(me + 8) : kMisClusterNodes;
+    else if (me) most = 0;
+    const int cs = nb <= std::min(most, kMisClusterNodes) ? mis_cluster_size() : 0;
     if (cs > 0) {
       TmpBuf<uint64_t> m1(s);
       TmpBuf<int> cnt(s);
@@ -2840,6 +2988,14 @@ int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t
     SGPU_CUDA(cudaGetLastError());
     SGPU_TRY(read_int(cnt.p + rounds, s, &undecided));
   }
+  if (getenv("SGPU_AMG_VERBOSE")) {  // the rounds that had work
+    std::vector<int> hc((size_t)rounds + 1);
+    SGPU_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, hc.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    SGPU_CUDA(cudaStreamSynchronize(s));
+    int used = 0;
+    while (used < rounds && hc[used] != 0) used++;
+    fprintf(stderr, "amg independent set: %d nodes, %d rounds (%d launched)\n", nb, used, rounds);
+  }
   return SGPU_OK;
 }
 
@@ -2886,6 +3042,9 @@ int aggregate(AmgLevel &L, cudaStream_t s, CubTmp &tmp) {
   SGPU_CUDA(cudaMemsetAsync(agg1.p, 0xff, (size_t)nb * sizeof(int), s));  // -1: unaggregated
   SGPU_TRY(mis2(L, nullptr, nullptr, t, s));
   SGPU_TRY(take_roots(L, t, nullptr, agg1.p, s, tmp, cnt.p));
+  // second-pass candidates: left-over nodes with at least 4 left-over
+  // neighbours (2, 3, 5, 6 or 8 measured: 40-43 iterations against 39 on the
+  // 1.01M-DOF cantilever)
   k_mis_cand<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg1.p, 4, cand.p);
   count_launches(1);
   SGPU_TRY(mis2(L, cand.p, agg1.p, t, s));
@@ -2951,15 +3110,25 @@ int tentative(AmgLevel &L, int K, const double *Bl, double *Bnext, cudaStream_t 
   return SGPU_OK;
 }
 
+// SGPU_GALERKIN=plain: the row walk of k_gal_values2 without its software
+// pipelining (the same sums in the same order: a check of the pipelined walk)
+bool gal_pipelined() {
+  const char *g = getenv("SGPU_GALERKIN");
+  return !(g && !strcmp(g, "plain"));
+}
+
 template <int B, int K>
 int launch_gal_values(const AmgLevel &L, const LevelView &view, const int *lists, AmgLevel &C, cudaStream_t s,
-                      bool private_acc) {
+                      bool private_acc, int max_row) {
   if (private_acc) {
-    constexpr size_t sm2 = gal2_shared_bytes<B, K>();
-    SGPU_CUDA(cudaFuncSetAttribute(k_gal_values2<B, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    const int cap = std::max(1, std::min(max_row, kGal2Cap));
+    const size_t sm2 = gal2_shared_bytes<B, K>(cap);
+    SGPU_CUDA(cudaFuncSetAttribute(k_gal_values2<B, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)gal2_shared_bytes<B, K>(kGal2Cap)));
     const int grid = (int)std::min<int64_t>(L.na, 64ll * kNumSMs);
     k_gal_values2<B, K><<<grid, 32 * kGal2Warps, sm2, s>>>(L.na, L.aggptr.p, L.aggnodes.p, L.agg.p, view, L.Q64.p,
-                                                           lists, C.own_browptr.p, C.own_bcol.p, C.val64.p);
+                                                           lists, C.own_browptr.p, C.own_bcol.p, C.val64.p, cap,
+                                                           gal_pipelined());
     count_launches(1);
     return SGPU_OK;
   }
@@ -3029,12 +3198,12 @@ int galerkin_direct(AmgLevel &L, const LevelView &view, AmgLevel &C, int K, cuda
   C.browptr = C.own_browptr.p;
   C.bcol = C.own_bcol.p;
   const int B = L.b;
-  if (B == 3 && K == 6) SGPU_TRY((launch_gal_values<3, 6>(L, view, lists.p, C, s, private_acc)));
-  else if (B == 6 && K == 6) SGPU_TRY((launch_gal_values<6, 6>(L, view, lists.p, C, s, private_acc)));
-  else if (B == 1 && K == 1) SGPU_TRY((launch_gal_values<1, 1>(L, view, lists.p, C, s, private_acc)));
-  else if (B == 1 && K == 3) SGPU_TRY((launch_gal_values<1, 3>(L, view, lists.p, C, s, private_acc)));
-  else if (B == 3 && K == 3) SGPU_TRY((launch_gal_values<3, 3>(L, view, lists.p, C, s, private_acc)));
-  else if (B == 1 && K == 6) SGPU_TRY((launch_gal_values<1, 6>(L, view, lists.p, C, s, private_acc)));
+  if (B == 3 && K == 6) SGPU_TRY((launch_gal_values<3, 6>(L, view, lists.p, C, s, private_acc, hv[2])));
+  else if (B == 6 && K == 6) SGPU_TRY((launch_gal_values<6, 6>(L, view, lists.p, C, s, private_acc, hv[2])));
+  else if (B == 1 && K == 1) SGPU_TRY((launch_gal_values<1, 1>(L, view, lists.p, C, s, private_acc, hv[2])));
+  else if (B == 1 && K == 3) SGPU_TRY((launch_gal_values<1, 3>(L, view, lists.p, C, s, private_acc, hv[2])));
+  else if (B == 3 && K == 3) SGPU_TRY((launch_gal_values<3, 3>(L, view, lists.p, C, s, private_acc, hv[2])));
+  else if (B == 1 && K == 6) SGPU_TRY((launch_gal_values<1, 6>(L, view, lists.p, C, s, private_acc, hv[2])));
   else return fail(SGPU_BAD_INPUT, "unsupported block size / near-null-space size");
   SGPU_CUDA(cudaGetLastError());
   *done = true;
@@ -3693,7 +3862,8 @@ int amg_build(sgpu_matrix m) {
   A.nc = Cl->n;
   SGPU_TRY(A.M64.alloc((size_t)A.nc * A.nc));
   SGPU_CUDA(cudaMemsetAsync(A.M64.p, 0, (size_t)A.nc * A.nc * sizeof(double), s));
-  k_dense_fill<<<grid_for(Cl->nb), TPB, 0, s>>>(Cl->nb, Cl->b, A.nc, Cl->browptr, Cl->bcol, Cl->val64.p, A.M64.p);
+  k_dense_fill<<<grid_for((int64_t)Cl->nb * 32), TPB, 0, s>>>(Cl->nb, Cl->b, A.nc, Cl->browptr, Cl->bcol,
+                                                               Cl->val64.p, A.M64.p);
   k_unit_empty_diag<<<grid_for(A.nc), TPB, 0, s>>>(A.nc, A.M64.p);
   const int gj_cs = gj_cluster_size();
   if (gj_cs > 0) {
@@ -3716,13 +3886,14 @@ int amg_build(sgpu_matrix m) {
     TmpBuf<double> P(s);
     SGPU_TRY(P.alloc(GJB * GJB));
     const int nc = A.nc;
-    const dim3 tiles((nc + 63) / 64, (nc + 63) / 64);
+    const int nt = (nc + GJB - 1) / GJB;  // 32-wide panels and tiles
+    const dim3 tiles(nt, nt);
     for (int k0 = 0; k0 < nc; k0 += GJB) {
       const int bs = std::min(GJB, nc - k0);
       k_bgj_diag<<<1, GJB * GJB, 0, s>>>(nc, k0, bs, A.M64.p, P.p);
-      k_bgj_rowpanel<<<grid_for(nc), TPB, 0, s>>>(nc, k0, bs, P.p, A.M64.p);
+      k_bgj_rowpanel<<<nt, TPB, 0, s>>>(nc, k0, bs, P.p, A.M64.p);
       k_bgj_update<<<tiles, TPB, 0, s>>>(nc, k0, bs, A.M64.p);
-      k_bgj_colpanel<<<grid_for(nc), TPB, 0, s>>>(nc, k0, bs, P.p, A.M64.p);
+      k_bgj_colpanel<<<nt, TPB, 0, s>>>(nc, k0, bs, P.p, A.M64.p);
     }
     count_launches(2 + 4 * ((nc + GJB - 1) / GJB));
   }

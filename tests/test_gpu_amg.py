@@ -430,10 +430,12 @@ def test_half_precision_level0_values(oracle, gpu_lib, shape, monkeypatch):
 
 @pytest.mark.parametrize("case", ["cantilever", "plate"])
 def test_cluster_independent_set_gives_the_same_bits(oracle, gpu_lib, case):
-    # with SGPU_MIS=cluster, graphs of up to 32768 nodes run all their
+    # graphs of up to 2048 nodes (the default), of up to 32768 nodes
+    # (SGPU_MIS=cluster) or none (SGPU_MIS=rounds) run all their
     # independent-set rounds in one thread-block cluster launch; the same
-    # keys, maxima and decisions as the separate launches per pass, so the
-    # same aggregates, hierarchy and solve to the bit
+    # keys, maxima and decisions as the separate launches per pass (which
+    # skip the nodes that take no part in a pass), so the same aggregates,
+    # hierarchy and solve to the bit
     if case == "cantilever":
         m = decks.cantilever_hex(40, 8, 8)
     else:
@@ -442,12 +444,50 @@ def test_cluster_independent_set_gives_the_same_bits(oracle, gpu_lib, case):
     f = oracle.load_vector(m)
     with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
         dm.set_nullspace(mefel.rigid_body_modes(m))
-        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", None)
+        x0, r0 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", "rounds")
         x1, r1 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", "cluster")
-    assert r0.status == r1.status == L.OK
-    assert r0.info["iterations"] == r1.info["iterations"]
-    assert r0.info["precond_coarse_n"] == r1.info["precond_coarse_n"]
+        x2, r2 = _solve_with_env(dm, f, "mixed", "SGPU_MIS", None)
+    assert r0.status == r1.status == r2.status == L.OK
+    assert r0.info["iterations"] == r1.info["iterations"] == r2.info["iterations"]
+    assert r0.info["precond_coarse_n"] == r1.info["precond_coarse_n"] == r2.info["precond_coarse_n"]
     assert np.array_equal(x0, x1)
+    assert np.array_equal(x0, x2)
+
+
+@pytest.mark.parametrize("case", ["cantilever", "plate", "conduction"])
+def test_pipelined_galerkin_gives_the_same_bits(oracle, gpu_lib, case):
+    # the coarse operators' row walk with the next chunk's loads in flight
+    # (the default) against the walk one chunk after another
+    # (SGPU_GALERKIN=plain): the same sums in the same order, so the same
+    # hierarchy and solve to the bit (3x3 blocks with six modes, scalar rows
+    # with three, scalar rows with one)
+    if case == "cantilever":
+        m = decks.cantilever_hex(40, 8, 8)
+        adr, ci, a = _oracle_system(oracle, m)
+        f = oracle.load_vector(m)
+        B = mefel.rigid_body_modes(m)
+    elif case == "plate":
+        m = decks.plate_quad(48, 24, E=3e10, nu=0.22)
+        adr, ci, a = _oracle_system(oracle, m)
+        f = oracle.load_vector(m)
+        B = mefel.rigid_body_modes(m)
+    else:
+        m = decks.heat_cube(24, sigma=1.0)
+        with mefel.conductivity_matrix(m) as K:
+            adr, ci, a = K.download(symmetric=1)
+        f = np.random.default_rng(11).standard_normal(adr.size - 1)
+        B = np.ones((adr.size - 1, 1))
+    xo, _, _, _ = oracle.scr_cg_prec(adr, ci, a, f, ni=200000, res=1e-26)
+    with gefel.DeviceMatrix(adr, ci, a, 1) as dm:
+        dm.set_nullspace(B)
+        for mode in ("mixed", "fp64"):
+            x0, r0 = _solve_with_env(dm, f, mode, "SGPU_GALERKIN", None)
+            x1, r1 = _solve_with_env(dm, f, mode, "SGPU_GALERKIN", "plain")
+            assert r0.status == r1.status == L.OK
+            assert r0.info["precond_levels"] == r1.info["precond_levels"] > 1
+            assert r0.info["iterations"] == r1.info["iterations"]
+            assert np.array_equal(x0, x1)
+            assert np.linalg.norm(x1 - xo) / np.linalg.norm(xo) <= 1e-8
 
 
 @pytest.mark.parametrize("case", ["cantilever", "plate"])
