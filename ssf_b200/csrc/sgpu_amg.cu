@@ -3412,7 +3412,10 @@ void level0_h16_shape(int *lanes, int *groups) {
 
 // The padded pattern (once per handle) and the binary16 values (once per
 // FP32 set-up) of level 0; stream-ordered on s, never inside a capture.
-int ensure_level0_h16(sgpu_matrix m, cudaStream_t s) {
+// The padded pattern (once per handle) on s, then the values on vs (none
+// when vs is null): the set-up converts them on its second stream, beside
+// the aggregation, after a fork that follows the pattern.
+int ensure_level0_h16(sgpu_matrix m, cudaStream_t s, cudaStream_t vs) {
   Amg &A = *m->amg;
   Bsr3 &b = m->bsr;
   if (!b.valid || !b.have32 || !level0_h16_enabled()) return SGPU_OK;
@@ -3439,8 +3442,9 @@ int ensure_level0_h16(sgpu_matrix m, cudaStream_t s) {
     A.h16_struct = true;
   }
   if (!A.h16_vals) {
-    k_h16_vals<<<grid_for((int64_t)b.nb * 32), TPB, 0, s>>>(b.nb, b.browptr.p, b.bval32s.p, A.h16ptr.p,
-                                                             A.h16val.p);
+    if (!vs) return SGPU_OK;  // the pattern only
+    k_h16_vals<<<grid_for((int64_t)b.nb * 32), TPB, 0, vs>>>(b.nb, b.browptr.p, b.bval32s.p, A.h16ptr.p,
+                                                              A.h16val.p);
     count_launches(1);
     SGPU_CUDA(cudaGetLastError());
     A.h16_vals = true;
@@ -3774,7 +3778,9 @@ int amg_build(sgpu_matrix m) {
   SGPU_TRY(ensure_bsr3(m));
   SGPU_TRY(ensure_fp32(m));  // scaled FP32 level 0 and S = diag^-1/2
   SGPU_TRY(level0_tile_plan(m, s));
-  if (A.want_fp32) SGPU_TRY(ensure_level0_h16(m, s));  // before the level-0 bound below reads it
+  // the binary16 level 0 before the level-0 bound below reads it: its
+  // values on the second stream when the bound runs there
+  if (A.want_fp32) SGPU_TRY(ensure_level0_h16(m, s, A.l0_bound_wanted ? nullptr : s));
   const int n = (int)m->n;
   keep_pool_memory();
   CubTmp tmp(s);
@@ -3800,17 +3806,19 @@ int amg_build(sgpu_matrix m) {
   L0->n = n;
   L0->unit_diag = true;
   if (A.l0_bound_wanted) {
-    // the FP32 cycle's level-0 smoother bound needs only the scaled FP32
-    // matrix: its Lanczos steps (bandwidth-bound SpMVs) run on a second
-    // stream while the aggregation (latency-bound rounds with host reads)
-    // runs here; amg_prepare_precision collects it.  Neither touches the
-    // other's buffers (the set-up kernels use no reduction partials).
+    // the FP32 cycle's level-0 smoother bound needs only the scaled level 0
+    // (its binary16 values, converted first on the same stream): its
+    // Lanczos steps (bandwidth-bound SpMVs) run on a second stream while
+    // the aggregation (latency-bound rounds with host reads) runs here;
+    // amg_prepare_precision collects it.  Neither touches the other's
+    // buffers (the set-up kernels use no reduction partials).
     if (!A.side) SGPU_CUDA(cudaStreamCreateWithFlags(&A.side, cudaStreamNonBlocking));
     if (!A.fork) SGPU_CUDA(cudaEventCreateWithFlags(&A.fork, cudaEventDisableTiming));
     SGPU_TRY(A.lz32.alloc((size_t)5 * n));
     SGPU_TRY(A.lz_ab.alloc(129));
     SGPU_CUDA(cudaEventRecord(A.fork, s));
     SGPU_CUDA(cudaStreamWaitEvent(A.side, A.fork, 0));
+    SGPU_TRY(ensure_level0_h16(m, s, A.side));
     float *z = A.lz32.p;
     SGPU_TRY(lanczos_enqueue<float>(m, *L0, A.side, std::max(2, std::min(A.lanczos_steps, 63)), z, z + n, z + 2 * n,
                                     z + 3 * (size_t)n, z + 4 * (size_t)n, A.lz_ab.p));
@@ -3918,7 +3926,7 @@ int amg_prepare_precision(sgpu_matrix m, bool fp32) {
   cudaStream_t s = m->stream;
   PhaseClock clk(s);
   if (fp32 && !A.have32) {
-    SGPU_TRY(ensure_level0_h16(m, s));
+    SGPU_TRY(ensure_level0_h16(m, s, s));
     std::vector<double> hc;  // the coarse levels' Lanczos coefficients from the second stream
     for (size_t l = 0; l < A.lv.size(); l++) {
       AmgLevel &L = *A.lv[l];
