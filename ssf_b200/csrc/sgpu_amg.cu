@@ -1365,7 +1365,8 @@ __global__ void k_mis_max(int nb, const int *__restrict__ browptr, const int *__
 template <int LPR, bool DECIDE>
 __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *__restrict__ bcol,
                             const int *__restrict__ agg, const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
-                            const int *go, uint64_t *__restrict__ t, int *__restrict__ undecided) {
+                            const int *go, uint64_t *__restrict__ t, int *__restrict__ undecided,
+                            int *__restrict__ settled) {
   if (*go == 0) return;
   constexpr int RPW = 32 / LPR;
   const int lane = threadIdx.x & 31, g = lane / LPR, sub = lane % LPR;
@@ -1375,17 +1376,25 @@ __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *
   for (int base = warp * RPW; base < nb; base += nwarps * RPW) {
     const int i = base + g;
     uint64_t m = 0;
-    // nodes that take no part: an aggregated node (second pass: no node
-    // reads its maximum, it has nothing to decide) and, in the deciding
-    // pass, a node already decided (its maximum feeds nothing else)
+    // nodes that take no part: an aggregated node (second phase: no node
+    // reads its maximum, it has nothing to decide); in the deciding pass, a
+    // node already decided (its maximum feeds nothing else); in the first
+    // pass, a settled node: one whose closed neighbourhood had no undecided
+    // node at an earlier round (decisions are final, so no undecided node
+    // will read its maximum again)
     uint64_t ti = 0;
     bool on_i = i < nb && (agg == nullptr || __ldg(agg + i) < 0);
     if (DECIDE && on_i) {
       ti = t[i];
       on_i = (ti >> 62) == 1;
     }
+    if (!DECIDE && on_i) on_i = settled[i] == 0;
+    int open = 0;  // first pass: an undecided node in the closed neighbourhood
     if (on_i) {
-      if (sub == 0) m = in[i];
+      if (sub == 0) {
+        m = in[i];
+        open = (m >> 62) == 1;
+      }
       const int re = browptr[i + 1];
       // four neighbours per lane in flight: their columns first, then their
       // keys (and aggregate marks)
@@ -1402,14 +1411,22 @@ __global__ void k_mis_max_w(int nb, const int *__restrict__ browptr, const int *
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
-          if (on[u]) m = max(m, kv[u]);
+          if (on[u]) {
+            m = max(m, kv[u]);
+            if (!DECIDE) open |= (kv[u] >> 62) == 1;
+          }
       }
     }
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) m = max(m, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)m, o, LPR));
+    if (!DECIDE) {
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) open |= __shfl_xor_sync(0xffffffffu, open, o, LPR);
+    }
     if (on_i && sub == 0) {
       if (!DECIDE) {
         out[i] = m;
+        if (!open) settled[i] = 1;
       } else {  // ti undecided
         if (m == ti) t[i] = mis_key(2, i);
         else if ((m >> 62) == 2) t[i] = ti & ~(3ull << 62);
@@ -2957,9 +2974,11 @@ int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t
   const int gw = grid_for((int64_t)nb * 8);
   constexpr int kMaxRounds = 200, kGroup = 16;  // rounds enqueued per host read of the count
   TmpBuf<uint64_t> m1(s), m2(s);
-  TmpBuf<int> cnt(s);
+  TmpBuf<int> cnt(s), settled(s);
   SGPU_TRY(m1.alloc(nb));
   SGPU_TRY(m2.alloc(nb));
+  SGPU_TRY(settled.alloc(nb));
+  SGPU_CUDA(cudaMemsetAsync(settled.p, 0, (size_t)nb * sizeof(int), s));
   // cnt[r]: the nodes round r left undecided; cnt[0] a non-zero start.  A
   // round whose predecessor left none returns at once, so the host enqueues
   // kGroup rounds and reads the count once per group.
@@ -2974,9 +2993,10 @@ int mis2(const AmgLevel &L, const int *cand, const int *agg, TmpBuf<uint64_t> &t
     for (int k = 0; k < kGroup; k++, rounds++) {
       const int *go = cnt.p + rounds;
       if (warp_rows) {
-        k_mis_max_w<8, false><<<gw, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go, nullptr, nullptr);
+        k_mis_max_w<8, false><<<gw, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go, nullptr, nullptr,
+                                                  settled.p);
         k_mis_max_w<8, true><<<gw, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, m1.p, nullptr, go, t.p,
-                                                 cnt.p + rounds + 1);
+                                                 cnt.p + rounds + 1, nullptr);
         count_launches(2);
       } else {
         k_mis_max<<<g, TPB, 0, s>>>(nb, L.browptr, L.bcol, agg, t.p, m1.p, go);
