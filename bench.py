@@ -56,6 +56,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -124,26 +125,53 @@ class Clocks:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 50
+
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.p = None
+        self.lines = []
+        self.reader = None
+        self.first = 0
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line)
 
     def start(self):
+        """Starts the sampler and returns once it has taken its first sample
+        (at most 2 s), so that the samples after that one cover the region."""
+        self.lines = []
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.p = None
+            return
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        t0 = time.time()
+        while not self.lines and self.p.poll() is None and time.time() - t0 < 2.0:
+            time.sleep(0.005)
+        self.first = len(self.lines)  # samples taken before the region
 
     def stop(self):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
-        out, _ = self.p.communicate(timeout=10)
+        try:
+            self.p.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            self.p.wait()
+        self.reader.join(timeout=10)
+        # the samples of the region; the one before it only when the region
+        # ended before the next sample
+        lines = self.lines[self.first:] or self.lines
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
