@@ -2179,7 +2179,7 @@ __global__ void __launch_bounds__(32 * kGal2Warps)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double *accs = gal2_sh;                            // [W][cap][KK]
   double *stages = accs + (size_t)W * cap * KK;      // [W][32][SS]
-  double *qis = stages + (size_t)W * 32 * SS;              // [W][BK]
+  double *qis = stages + (size_t)W * 32 * SS;        // [W][BK]
   GalTable &T = *reinterpret_cast<GalTable *>(qis + (size_t)W * BK);
   int *pnode = reinterpret_cast<int *>(&T + 1);  // [kGal2Nodes] the aggregate's nodes
   int *prs = pnode + kGal2Nodes, *pre = prs + kGal2Nodes;  // their rows' ranges
